@@ -1,0 +1,357 @@
+// Jacobi-preconditioned conjugate gradients, FP64:
+// ConjugateGradients<TSpace>::product (linalg/packages/solvers/impl/ConjugateGradients_impl.hpp:49-201)
+// with DiagonalOperator (DiagonalOperator.cpp:37-53) as preconditioner.
+//
+// One iteration = three kernels over HBM, with the solver scalars on the device:
+//   K1  q = A p (CSR row pass) and p^T q in the same pass; the last CTA forms
+//       alpha = rz / p^T q and flags the p^T A p <= 0 breakdown.
+//   K2  x += alpha p; r -= alpha q; z = D^-1 r; r^T r and r^T z in the same pass;
+//       the last CTA forms beta, the residual norms and the stopping decision.
+//   K3  p = beta p + z (z recomputed from r and D^-1; same rounding as
+//       space.scale(search, beta) followed by space.add(search, z, 1)).
+// Every kernel returns at once when the done flag is set, so a CUDA graph of a
+// fixed number of iterations can be replayed until the host sees the flag.
+#include "pcg.cuh"
+
+#include <string>
+
+namespace ciecu {
+
+namespace {
+
+constexpr int kT = 256;
+
+// r = b - A x (x = initial guess) is formed with the CSR kernel in the host code;
+// this kernel does the rest of the set-up (:100-132): rr, early exit, z, rz, p.
+template <bool PRECOND>
+__global__ void __launch_bounds__(kT) pcg_init_kernel(long n, const double* __restrict__ r,
+                                                      const double* __restrict__ dinv, double* __restrict__ p,
+                                                      PcgScalars* s, double* partials, unsigned* counter) {
+    double rr = 0.0, rz = 0.0;
+    const long stride = static_cast<long>(gridDim.x) * kT;
+    for (long i = static_cast<long>(blockIdx.x) * kT + threadIdx.x; i < n; i += stride) {
+        const double ri = r[i];
+        const double zi = PRECOND ? ri * dinv[i] : ri;
+        p[i] = zi;
+        rr = fma(ri, ri, rr);
+        rz = fma(ri, zi, rz);
+    }
+    double mine[2] = {rr, rz}, tot[2];
+    if (grid_reduce_last<2, kT>(mine, partials, counter, tot) && threadIdx.x == 0) {
+        s->rr = tot[0];
+        s->r0 = sqrt(tot[0]);
+        s->absres = s->r0;
+        s->relres = 1.0;
+        s->iter = 0;
+        s->done = 0;
+        s->error = 0;
+        if (float_less(s->absres, s->absTol) || float_less(s->relres, s->relTol)) {
+            s->done = 1;
+        } else {
+            s->rz = PRECOND ? tot[1] : tot[0];
+            if (!(0.0 < s->rz)) {
+                s->done = 3;
+                s->error = CIECU_ERR_BREAKDOWN;
+                s->errorKind = 1;
+                s->errorIter = 0;
+            } else if (s->maxIter <= 0) {
+                s->done = 2;
+            }
+        }
+    }
+}
+
+// K1: q = A p, p^T q, alpha.
+template <int KERNEL>
+__global__ void __launch_bounds__(csr_threads<KERNEL>())
+    pcg_spmv_kernel(CsrArgs<double> A, const double* __restrict__ p, double* __restrict__ q, PcgScalars* s,
+                    double* partials, unsigned* counter) {
+    if (*reinterpret_cast<volatile int*>(&s->done)) return;
+    constexpr int T = csr_threads<KERNEL>();
+    double acc = 0.0;
+    auto op = [&](int r, double sum) {
+        q[r] = sum;
+        acc = fma(p[r], sum, acc);
+    };
+    csr_rows<KERNEL, double, double, false>(A, p, op);
+    double mine[1] = {acc}, tot[1];
+    if (grid_reduce_last<1, T>(mine, partials, counter, tot) && threadIdx.x == 0) {
+        s->pq = tot[0];
+        if (!(0.0 < tot[0])) {
+            s->done = 3;
+            s->error = CIECU_ERR_BREAKDOWN;
+            s->errorKind = 2;
+            s->errorIter = s->iter;
+        } else {
+            s->alpha = s->rz / tot[0];
+        }
+    }
+}
+
+// K2: x, r update; z; rr, rz; beta and the stopping test (:154-185).
+template <bool PRECOND>
+__global__ void __launch_bounds__(kT) pcg_update_kernel(long n, double* __restrict__ x, double* __restrict__ r,
+                                                        const double* __restrict__ p, const double* __restrict__ q,
+                                                        const double* __restrict__ dinv, PcgScalars* s,
+                                                        double* partials, unsigned* counter) {
+    if (*reinterpret_cast<volatile int*>(&s->done)) return;
+    const double alpha = s->alpha;
+    const double malpha = -alpha;
+    double rr = 0.0, rz = 0.0;
+    const long stride = static_cast<long>(gridDim.x) * kT;
+    for (long i = static_cast<long>(blockIdx.x) * kT + threadIdx.x; i < n; i += stride) {
+        x[i] = fma(alpha, p[i], x[i]);
+        const double ri = fma(malpha, q[i], r[i]);
+        r[i] = ri;
+        rr = fma(ri, ri, rr);
+        if (PRECOND) rz = fma(ri, ri * dinv[i], rz);
+    }
+    double mine[2] = {rr, rz}, tot[2];
+    if (grid_reduce_last<2, kT>(mine, partials, counter, tot) && threadIdx.x == 0) {
+        const double rzNew = PRECOND ? tot[1] : tot[0];
+        s->rr = tot[0];
+        s->beta = rzNew / s->rz;
+        s->rz = rzNew;
+        s->absres = sqrt(tot[0]);
+        s->relres = s->absres / s->r0;
+        if (float_less(s->absres, s->absTol) || float_less(s->relres, s->relTol)) {
+            s->done = 1;
+        } else {
+            s->iter += 1;
+            if (s->iter >= s->maxIter) s->done = 2;
+        }
+    }
+}
+
+// K3: p = beta p + z.  Runs after K2 decided to continue; a converged solve
+// does not need the new search direction.
+template <bool PRECOND>
+__global__ void __launch_bounds__(kT) pcg_direction_kernel(long n, double* __restrict__ p,
+                                                           const double* __restrict__ r,
+                                                           const double* __restrict__ dinv, const PcgScalars* s) {
+    if (*reinterpret_cast<const volatile int*>(&s->done)) return;
+    const double beta = s->beta;
+    const long stride = static_cast<long>(gridDim.x) * kT;
+    for (long i = static_cast<long>(blockIdx.x) * kT + threadIdx.x; i < n; i += stride) {
+        const double zi = PRECOND ? __dmul_rn(r[i], dinv[i]) : r[i];
+        p[i] = __dadd_rn(__dmul_rn(p[i], beta), zi);
+    }
+}
+
+// out = inScale*out + outScale*x with the space ops of :190-198.
+__global__ void pcg_output_kernel(long n, double inScale, double outScale, const double* __restrict__ x,
+                                  double* __restrict__ out) {
+    const long stride = static_cast<long>(gridDim.x) * blockDim.x;
+    for (long i = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const double xi = x[i];
+        double o = out[i];
+        if (inScale == 1.0) {
+            o = outScale == 1.0 ? o + xi : (outScale == -1.0 ? o - xi : o + outScale * xi);
+        } else if (inScale == 0.0) {
+            o = xi * outScale;
+        } else {
+            o *= inScale;
+            o = outScale == 1.0 ? o + xi : (outScale == -1.0 ? o - xi : o + outScale * xi);
+        }
+        out[i] = o;
+    }
+}
+
+}  // namespace
+
+}  // namespace ciecu
+
+struct ciecu_pcg_s {
+    ciecu_csr_s* A = nullptr;
+    const double* dinv = nullptr;
+    ciecu_statistics settings{};
+    int verbosity = 0;
+    long n = 0;
+    double* x = nullptr;
+    double* r = nullptr;
+    double* p = nullptr;
+    double* q = nullptr;
+    ciecu::PcgScalars* d_s = nullptr;
+    ciecu::PcgScalars* h_s = nullptr;
+    double* d_partials = nullptr;
+    unsigned* d_counter = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int graphKernel = -1;
+    int chunk = 16;
+};
+
+namespace ciecu {
+namespace {
+
+int launch_iteration(ciecu_pcg_s* S, cudaStream_t st) {
+    ciecu_csr_s* A = S->A;
+    const int gridA = csr_grid(A, A->kernel);
+    const int gridV = grid_for(S->n, kT, 8);
+    const bool pre = S->dinv != nullptr;
+    CIECU_TRY(with_schedule(A->kernel, [&](auto k) -> int {
+        constexpr int K = decltype(k)::value;
+        pcg_spmv_kernel<K><<<gridA, csr_threads<K>(), 0, st>>>(A->args<double>(), S->p, S->q, S->d_s, S->d_partials,
+                                                               S->d_counter);
+        return CIECU_OK;
+    }));
+    if (pre) {
+        pcg_update_kernel<true><<<gridV, kT, 0, st>>>(S->n, S->x, S->r, S->p, S->q, S->dinv, S->d_s, S->d_partials,
+                                                      S->d_counter);
+        pcg_direction_kernel<true><<<gridV, kT, 0, st>>>(S->n, S->p, S->r, S->dinv, S->d_s);
+    } else {
+        pcg_update_kernel<false><<<gridV, kT, 0, st>>>(S->n, S->x, S->r, S->p, S->q, S->dinv, S->d_s, S->d_partials,
+                                                       S->d_counter);
+        pcg_direction_kernel<false><<<gridV, kT, 0, st>>>(S->n, S->p, S->r, S->dinv, S->d_s);
+    }
+    CIECU_CHECK_LAUNCH("pcg iteration");
+    return CIECU_OK;
+}
+
+int build_graph(ciecu_pcg_s* S) {
+    cudaStream_t st = S->A->space->stream;
+    if (S->graph && S->graphKernel == S->A->kernel) return CIECU_OK;
+    if (S->graph) {
+        cudaGraphExecDestroy(S->graph);
+        S->graph = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    CIECU_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int status = CIECU_OK;
+    for (int i = 0; i < S->chunk && status == CIECU_OK; ++i) status = launch_iteration(S, st);
+    cudaError_t e = cudaStreamEndCapture(st, &g);
+    if (status != CIECU_OK) {
+        if (g) cudaGraphDestroy(g);
+        return status;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "pcg graph capture");
+    e = cudaGraphInstantiate(&S->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(e, "pcg graph instantiate");
+    S->graphKernel = S->A->kernel;
+    return CIECU_OK;
+}
+
+}  // namespace
+}  // namespace ciecu
+
+using namespace ciecu;
+
+extern "C" {
+
+int ciecu_pcg_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_statistics settings, int verbosity,
+                     ciecu_pcg* out) {
+    CIECU_REQUIRE(lhs && out, "pcg_create: null matrix or output");
+    CIECU_REQUIRE(lhs->valueType == CIECU_F64, "pcg_create: the FP64 solver needs an FP64 matrix");
+    CIECU_REQUIRE(lhs->rows == lhs->cols, "pcg_create: the system matrix must be square");
+    auto* S = new ciecu_pcg_s();
+    S->A = lhs;
+    S->dinv = d_inverseDiagonal;
+    S->settings = settings;
+    S->verbosity = verbosity;
+    S->n = lhs->rows;
+    const size_t bytes = sizeof(double) * static_cast<size_t>(std::max<long>(S->n, 1));
+    cudaError_t e = cudaSuccess;
+    for (double** v : {&S->x, &S->r, &S->p, &S->q})
+        if (e == cudaSuccess) e = cudaMalloc(v, bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&S->d_s, sizeof(PcgScalars));
+    if (e == cudaSuccess) e = cudaMallocHost(&S->h_s, sizeof(PcgScalars));
+    if (e == cudaSuccess) e = cudaMalloc(&S->d_partials, sizeof(double) * kMaxPartials * 2);
+    if (e == cudaSuccess) e = cudaMalloc(&S->d_counter, sizeof(unsigned) * 4);
+    if (e == cudaSuccess) e = cudaMemsetAsync(S->d_counter, 0, sizeof(unsigned) * 4, lhs->space->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(S->q, 0, bytes, lhs->space->stream);
+    if (e != cudaSuccess) {
+        ciecu_pcg_destroy(S);
+        return cuda_fail(e, "pcg_create: allocation");
+    }
+    *out = S;
+    return CIECU_OK;
+}
+
+int ciecu_pcg_destroy(ciecu_pcg S) {
+    if (!S) return CIECU_OK;
+    if (S->A && S->A->space) cudaStreamSynchronize(S->A->space->stream);
+    if (S->graph) cudaGraphExecDestroy(S->graph);
+    cudaFree(S->x);
+    cudaFree(S->r);
+    cudaFree(S->p);
+    cudaFree(S->q);
+    cudaFree(S->d_s);
+    if (S->h_s) cudaFreeHost(S->h_s);
+    cudaFree(S->d_partials);
+    cudaFree(S->d_counter);
+    delete S;
+    return CIECU_OK;
+}
+
+int ciecu_pcg_set_graph_chunk(ciecu_pcg S, int iterations) {
+    CIECU_REQUIRE(S && iterations >= 1 && iterations <= 4096, "pcg_set_graph_chunk: chunk must be in [1, 4096]");
+    if (S->chunk != iterations && S->graph) {
+        cudaGraphExecDestroy(S->graph);
+        S->graph = nullptr;
+    }
+    S->chunk = iterations;
+    return CIECU_OK;
+}
+
+int ciecu_pcg_product(ciecu_pcg S, double inScale, const double* d_in, double outScale, double* d_out,
+                      ciecu_statistics* h_stats) {
+    CIECU_REQUIRE(S, "pcg_product: null solver");
+    const long n = S->n;
+    CIECU_REQUIRE(n == 0 || (d_in && d_out), "pcg_product: null vector");
+    ciecu_csr_s* A = S->A;
+    cudaStream_t st = A->space->stream;
+    ciecu_statistics stats{0, 1.7976931348623157e308, 1.7976931348623157e308};
+    if (n == 0) {
+        if (h_stats) *h_stats = ciecu_statistics{0, 0.0, 0.0};
+        return CIECU_OK;
+    }
+    CIECU_TRY(ensure_tuned(A));
+    // solution <- out (initial guess)
+    CIECU_CUDA(cudaMemcpyAsync(S->x, d_out, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    if (S->settings.iterationCount > 0) {
+        PcgScalars init{};
+        init.maxIter = S->settings.iterationCount;
+        init.absTol = S->settings.absoluteResidual;
+        init.relTol = S->settings.relativeResidual;
+        *S->h_s = init;
+        CIECU_CUDA(cudaMemcpyAsync(S->d_s, S->h_s, sizeof(PcgScalars), cudaMemcpyHostToDevice, st));
+        // r = b - A x
+        CIECU_CUDA(cudaMemcpyAsync(S->r, d_in, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+        CIECU_TRY(ciecu_csr_spmv_f64(A, 1.0, S->x, -1.0, S->r));
+        const int gridV = grid_for(n, kT, 8);
+        if (S->dinv)
+            pcg_init_kernel<true><<<gridV, kT, 0, st>>>(n, S->r, S->dinv, S->p, S->d_s, S->d_partials, S->d_counter);
+        else
+            pcg_init_kernel<false><<<gridV, kT, 0, st>>>(n, S->r, S->dinv, S->p, S->d_s, S->d_partials, S->d_counter);
+        count_launch();
+        CIECU_CHECK_LAUNCH("pcg_init_kernel");
+        CIECU_TRY(build_graph(S));
+        // Replay graph chunks until the device reports done.  The scalars are read
+        // back after each chunk; the kernels of a finished solve return at once.
+        for (;;) {
+            CIECU_CUDA(cudaMemcpyAsync(S->h_s, S->d_s, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
+            CIECU_CUDA(cudaStreamSynchronize(st));
+            if (S->h_s->done) break;
+            CIECU_CUDA(cudaGraphLaunch(S->graph, st));
+            count_launch(3LL * S->chunk);
+        }
+        const PcgScalars& s = *S->h_s;
+        if (s.error) {
+            if (h_stats) *h_stats = ciecu_statistics{s.errorIter, s.absres, s.relres};
+            if (s.errorKind == 1)
+                return fail(CIECU_ERR_BREAKDOWN, "preconditioned norm vanished in iteration 0 (r^T @ z = 0)");
+            return fail(CIECU_ERR_BREAKDOWN, "p^T @ A @ p vanished in iteration " + std::to_string(s.errorIter));
+        }
+        stats.iterationCount = s.iter;
+        stats.absoluteResidual = s.absres;
+        stats.relativeResidual = s.relres;
+    }
+    pcg_output_kernel<<<grid_for(n, kT, 8), kT, 0, st>>>(n, inScale, outScale, S->x, d_out);
+    count_launch();
+    CIECU_CHECK_LAUNCH("pcg_output_kernel");
+    CIECU_CUDA(cudaStreamSynchronize(st));
+    if (h_stats) *h_stats = stats;
+    return CIECU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,179 @@
+"""Assembly path over the CUDA backend: structured Q_p meshes, the CSR pattern
+(Assembler::makeCSRMatrix), GPU element stiffness integration + atomic-free
+coloured scatter (IntegrandProcessor + Assembler::addContribution), symmetric
+Dirichlet elimination, and the seeded synthetic Poisson problems.
+
+Seeded inputs (identical host arrays feed the GPU and the oracle):
+  RHS      uniform [-1, 1] from std::mt19937_64(seed)        ((x >> 11) 2^-53) 2 - 1
+  kappa    exp(g), g ~ N(0,1) per cell (Box-Muller, seed+1), convolved with a
+           separable Gaussian kernel (sigma = 1 cell, truncated at +-3 cells,
+           clamped at the boundary) and standardised to unit variance.
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import call, CiecuError
+from .linalg import CSRMatrix, CUDASpace, _ptr, _CSRHandle
+
+__all__ = ["StructuredMesh", "csr_pattern", "Assembler", "random_uniform", "random_normal", "kappa_field",
+           "PoissonProblem", "make_poisson"]
+
+
+def _np_ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def random_uniform(seed, n):
+    out = np.empty(int(n), dtype=np.float64)
+    call("ciecu_random_uniform", int(seed), int(n), _np_ptr(out))
+    return out
+
+
+def random_normal(seed, n):
+    out = np.empty(int(n), dtype=np.float64)
+    call("ciecu_random_normal", int(seed), int(n), _np_ptr(out))
+    return out
+
+
+def kappa_field(seed, cells, sigma=1.0, truncation=3):
+    cells = np.asarray(cells, dtype=np.int32)
+    out = np.empty(int(np.prod(cells)), dtype=np.float64)
+    call("ciecu_kappa_field", int(seed), len(cells), _np_ptr(cells), float(sigma), int(truncation), _np_ptr(out))
+    return out
+
+
+class StructuredMesh:
+    """Uniform grid of Q_order Lagrange cells on the unit box."""
+
+    def __init__(self, dim, order, cells):
+        self.dim = int(dim)
+        self.order = int(order)
+        self.cells = np.asarray(cells, dtype=np.int32)
+        assert self.cells.size == self.dim
+        self.ncells = int(np.prod(self.cells))
+        self.nb = (self.order + 1) ** self.dim
+        self.dofmap = np.empty(self.ncells * self.nb, dtype=np.int32)
+        nd = ctypes.c_int32()
+        call("ciecu_structured_dofmap", self.dim, self.order, _np_ptr(self.cells), _np_ptr(self.dofmap),
+             ctypes.byref(nd))
+        self.ndofs = nd.value
+        self.h = 1.0 / self.cells.astype(np.float64)
+
+    def boundary(self):
+        b = np.empty(self.ndofs, dtype=np.uint8)
+        call("ciecu_structured_boundary", self.dim, self.order, _np_ptr(self.cells), _np_ptr(b))
+        return b
+
+    def colors(self):
+        c = np.empty(self.ncells, dtype=np.int32)
+        call("ciecu_structured_colors", self.dim, _np_ptr(self.cells), _np_ptr(c))
+        return c
+
+
+def csr_pattern(ncells, nb, dofmap, ndofs):
+    """Assembler::makeCSRMatrix (fem/packages/graph/src/Assembler.cpp:55-175)."""
+    dofmap = np.ascontiguousarray(dofmap, dtype=np.int32)
+    rowptr = np.empty(int(ndofs) + 1, dtype=np.int32)
+    nnz = ctypes.c_int64()
+    call("ciecu_csr_pattern", int(ncells), int(nb), _np_ptr(dofmap), int(ndofs), _np_ptr(rowptr), None,
+         ctypes.byref(nnz))
+    col = np.empty(nnz.value, dtype=np.int32)
+    call("ciecu_csr_pattern", int(ncells), int(nb), _np_ptr(dofmap), int(ndofs), _np_ptr(rowptr), _np_ptr(col),
+         ctypes.byref(nnz))
+    return rowptr, col
+
+
+class Assembler:
+    """GPU stiffness assembly into a device CSR pattern (ciecu_assembly_*)."""
+
+    def __init__(self, space, matrix, mesh, quadratureOrder=None, colors=None, csr_handle=None,
+                 d_dofmap=None):
+        self.space = space
+        self.matrix = matrix
+        self.mesh = mesh
+        self.csr = csr_handle if csr_handle is not None else _CSRHandle(matrix, space)
+        self.d_dofmap = d_dofmap if d_dofmap is not None else torch.as_tensor(mesh.dofmap).to(space.device)
+        colors = mesh.colors() if colors is None else np.ascontiguousarray(colors, dtype=np.int32)
+        q = mesh.order + 1 if quadratureOrder is None else int(quadratureOrder)
+        h = ctypes.c_void_p()
+        space.enter()
+        call("ciecu_assembly_create", self.csr.handle, mesh.dim, mesh.order, q, mesh.ncells, _ptr(self.d_dofmap),
+             _np_ptr(colors), ctypes.byref(h))
+        self.handle = h
+        self._work = torch.empty(mesh.nb * mesh.nb, dtype=torch.float64, device=space.device)
+
+    def __del__(self):
+        try:
+            if getattr(self, "handle", None):
+                _lib.load().ciecu_assembly_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+    def assemble(self, kappa, convention=0, accumulate=False, entries=None):
+        entries = self.matrix.entries if entries is None else entries
+        h = np.ascontiguousarray(self.mesh.h, dtype=np.float64)
+        self.space.enter()
+        call("ciecu_assemble_stiffness", self.handle, _ptr(kappa), _np_ptr(h), int(convention), int(bool(accumulate)),
+             _ptr(entries))
+        self.space.leave()
+
+    def dirichlet(self, isBoundary, rhs=None, entries=None):
+        entries = self.matrix.entries if entries is None else entries
+        self.space.enter()
+        call("ciecu_dirichlet_eliminate", self.csr.handle, _ptr(isBoundary), _ptr(entries), _ptr(rhs))
+        self.space.leave()
+
+    def element_gradient(self, lam, u, grad, convention=0):
+        h = np.ascontiguousarray(self.mesh.h, dtype=np.float64)
+        self.space.enter()
+        call("ciecu_element_gradient", self.handle, _np_ptr(h), int(convention), _ptr(lam), _ptr(u), _ptr(grad),
+             _ptr(self._work))
+        self.space.leave()
+
+
+class PoissonProblem:
+    """A seeded Poisson system assembled on the GPU: matrix (device CSR, FP64),
+    rhs (device), kappa (device), boundary flags, plus host copies on request."""
+
+    def __init__(self, space, mesh, matrix, rhs, kappa, boundary, assembler, seed):
+        self.space = space
+        self.mesh = mesh
+        self.matrix = matrix
+        self.rhs = rhs
+        self.kappa = kappa
+        self.boundary = boundary
+        self.assembler = assembler
+        self.seed = seed
+
+    def host_csr(self):
+        m = self.matrix
+        return (m.rowExtents.cpu().numpy(), m.columnIndices.cpu().numpy(), m.entries.cpu().numpy())
+
+
+def make_poisson(space, dim, order, cells, seed=0, kappa="lognormal", convention=0, kappa_seed=None):
+    """Q_order Poisson problem on a cells^dim grid of the unit box, homogeneous
+    Dirichlet boundary by symmetric elimination, RHS uniform [-1, 1] (seed),
+    kappa = 1 or the smoothed log-normal field (seed + 1 unless kappa_seed)."""
+    mesh = StructuredMesh(dim, order, cells)
+    rowptr, col = csr_pattern(mesh.ncells, mesh.nb, mesh.dofmap, mesh.ndofs)
+    dev = space.device
+    matrix = CSRMatrix(mesh.ndofs, torch.as_tensor(rowptr).to(dev), torch.as_tensor(col).to(dev),
+                       torch.zeros(col.size, dtype=torch.float64, device=dev))
+    if isinstance(kappa, str) and kappa == "lognormal":
+        k = kappa_field(seed + 1 if kappa_seed is None else kappa_seed, mesh.cells)
+    elif isinstance(kappa, str) and kappa == "one":
+        k = np.ones(mesh.ncells)
+    else:
+        k = np.asarray(kappa, dtype=np.float64)
+    kappa_d = torch.as_tensor(k).to(dev)
+    rhs = torch.as_tensor(random_uniform(seed, mesh.ndofs)).to(dev)
+    bnd = torch.as_tensor(mesh.boundary()).to(dev)
+    asm = Assembler(space, matrix, mesh)
+    asm.assemble(kappa_d, convention=convention)
+    asm.dirichlet(bnd, rhs)
+    torch.cuda.synchronize()
+    return PoissonProblem(space, mesh, matrix, rhs, kappa_d, bnd, asm, seed)

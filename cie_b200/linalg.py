@@ -1,0 +1,529 @@
+"""Python mirror of the kelofm/cie linalg operator API over the CUDA backend.
+
+Names, argument meaning and error behaviour follow the reference:
+  LinearOperator.product(inScale, in, outScale, out):  out <- inScale*out + outScale*Op(in)
+      (linalg/packages/solvers/inc/LinearOperator.hpp:10-34)
+  CUDASpace satisfies LinalgSpaceLike (linalg/packages/solvers/inc/LinalgSpace.hpp:10-35)
+  CSROperator, MaskedCSROperator, DiagonalOperator / makeDiagonalOperator,
+  JacobiOperator, MaskedIdentityOperator, NestedProductOperator, ConjugateGradients.
+Vectors are torch CUDA tensors (torch provides device memory and streams only);
+every operation runs in the libciecu.so kernels.  Failures raise CiecuError,
+the counterpart of cie::Exception.
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import Statistics, call, CiecuError
+
+__all__ = [
+    "CUDASpace", "CSRMatrix", "LinearOperator", "CSROperator", "MaskedCSROperator", "DiagonalOperator",
+    "makeDiagonalOperator", "JacobiOperator", "MaskedIdentityOperator", "NestedProductOperator",
+    "ChebyshevOperator", "ConjugateGradients", "Statistics", "CiecuError", "launch_count",
+]
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else ctypes.c_void_p(0)
+
+
+def launch_count():
+    """Kernels launched by libciecu.so since it was loaded."""
+    return int(_lib.load().ciecu_kernel_launch_count())
+
+
+class CUDASpace:
+    """Device vector space on one CUDA stream (the SYCLSpace counterpart)."""
+
+    def __init__(self, dtype=torch.float64, device=None):
+        if not torch.cuda.is_available():
+            raise RuntimeError("CUDASpace needs a CUDA device (there is no CPU fallback)")
+        _lib.load()
+        self.dtype = dtype
+        self.device = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+        self.stream = torch.cuda.Stream(self.device)
+        handle = ctypes.c_void_p()
+        call("ciecu_space_create", ctypes.c_void_p(self.stream.cuda_stream), ctypes.byref(handle))
+        self.handle = handle
+        self._sfx = "f64" if dtype == torch.float64 else "f32"
+
+    def __del__(self):
+        try:
+            if getattr(self, "handle", None):
+                _lib.load().ciecu_space_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+    # -- stream ordering with torch's current stream ---------------------------
+    def enter(self):
+        self.stream.wait_stream(torch.cuda.current_stream(self.device))
+
+    def leave(self):
+        torch.cuda.current_stream(self.device).wait_stream(self.stream)
+
+    def synchronize(self):
+        call("ciecu_space_synchronize", self.handle)
+
+    # -- LinalgSpaceLike ---------------------------------------------------------
+    @staticmethod
+    def view(vector):
+        return vector
+
+    @staticmethod
+    def size(view):
+        return int(view.numel())
+
+    def makeVector(self, size):
+        return torch.empty(int(size), dtype=self.dtype, device=self.device)
+
+    def _check(self, *vs):
+        for v in vs:
+            if not (v.is_cuda and v.dtype == self.dtype and v.is_contiguous()):
+                raise CiecuError(1, "expected a contiguous %s CUDA vector" % self.dtype)
+
+    def innerProduct(self, left, right):
+        self._check(left, right)
+        if left.numel() != right.numel():
+            raise CiecuError(1, "incompatible vector sizes %d != %d" % (left.numel(), right.numel()))
+        out = ctypes.c_double()
+        self.enter()
+        call("ciecu_dot_" + self._sfx, self.handle, left.numel(), _ptr(left), _ptr(right), ctypes.byref(out))
+        return out.value
+
+    def scale(self, target, source_or_value, scale=None):
+        """scale(target, source, alpha): target = alpha * target (.) source (elementwise);
+        scale(view, value): view *= value."""
+        self.enter()
+        if scale is None:
+            self._check(target)
+            call("ciecu_scale_" + self._sfx, self.handle, target.numel(), _ptr(target), float(source_or_value))
+        else:
+            self._check(target, source_or_value)
+            call("ciecu_scale_elementwise_" + self._sfx, self.handle, target.numel(), _ptr(target),
+                 _ptr(source_or_value), float(scale))
+        self.leave()
+
+    def add(self, target, source, scale):
+        self._check(target, source)
+        self.enter()
+        call("ciecu_add_" + self._sfx, self.handle, target.numel(), _ptr(target), _ptr(source), float(scale))
+        self.leave()
+
+    def assign(self, target, source):
+        """Device<-device, device<-host (numpy / CPU tensor) and host<-device."""
+        self.enter()
+        if isinstance(target, torch.Tensor) and target.is_cuda and isinstance(source, torch.Tensor) and source.is_cuda:
+            self._check(target, source)
+            call("ciecu_assign_" + self._sfx, self.handle, target.numel(), _ptr(target), _ptr(source))
+        elif isinstance(target, torch.Tensor) and target.is_cuda:
+            host = np.ascontiguousarray(np.asarray(source), dtype=np.float64 if self._sfx == "f64" else np.float32)
+            call("ciecu_memcpy_h2d", self.handle, _ptr(target), host.ctypes.data_as(ctypes.c_void_p), host.nbytes)
+        else:
+            host = np.asarray(target)
+            call("ciecu_memcpy_d2h", self.handle, host.ctypes.data_as(ctypes.c_void_p), _ptr(source),
+                 source.numel() * source.element_size())
+        self.leave()
+
+    def fill(self, view, value):
+        self._check(view)
+        self.enter()
+        call("ciecu_fill_" + self._sfx, self.handle, view.numel(), _ptr(view), float(value))
+        self.leave()
+
+
+class CSRMatrix:
+    """Device CSR arrays (the storage a device CSRView points at,
+    linalg/packages/utilities/inc/CSRView.hpp:11-86)."""
+
+    def __init__(self, columnCount, rowExtents, columnIndices, entries):
+        self.columnCount = int(columnCount)
+        self.rowExtents = rowExtents
+        self.columnIndices = columnIndices
+        self.entries = entries
+
+    @classmethod
+    def from_host(cls, columnCount, rowExtents, columnIndices, entries, dtype=torch.float64, device="cuda"):
+        return cls(columnCount,
+                   torch.as_tensor(np.asarray(rowExtents, dtype=np.int32)).to(device),
+                   torch.as_tensor(np.asarray(columnIndices, dtype=np.int32)).to(device),
+                   torch.as_tensor(np.asarray(entries)).to(device=device, dtype=dtype))
+
+    def rowCount(self):
+        return int(self.rowExtents.numel()) - 1
+
+    def nnz(self):
+        return int(self.columnIndices.numel())
+
+    def astype(self, dtype):
+        return CSRMatrix(self.columnCount, self.rowExtents, self.columnIndices, self.entries.to(dtype))
+
+
+class LinearOperator:
+    def product(self, inScale, in_, outScale, out):
+        raise NotImplementedError
+
+
+class _CSRHandle:
+    def __init__(self, matrix, space):
+        if matrix.columnIndices.numel() != matrix.entries.numel():
+            raise CiecuError(1, "number of column indices (%d) is inconsistent with the number of entries (%d) "
+                                "in the provided CSR matrix" % (matrix.columnIndices.numel(), matrix.entries.numel()))
+        if matrix.rowExtents.numel() < 1:
+            raise CiecuError(1, "expecting the row extents of a CSR matrix to have at least 1 entry, but it has none")
+        self.matrix = matrix
+        self.space = space
+        vt = 0 if matrix.entries.dtype == torch.float64 else 1
+        h = ctypes.c_void_p()
+        space.enter()
+        call("ciecu_csr_create", space.handle, matrix.rowCount(), matrix.columnCount, matrix.nnz(),
+             _ptr(matrix.rowExtents), _ptr(matrix.columnIndices), _ptr(matrix.entries), vt, ctypes.byref(h))
+        self.handle = h
+
+    def __del__(self):
+        try:
+            if getattr(self, "handle", None):
+                _lib.load().ciecu_csr_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+    def kernel(self):
+        k = ctypes.c_int()
+        call("ciecu_csr_get_kernel", self.handle, ctypes.byref(k))
+        return k.value
+
+    def set_kernel(self, k):
+        call("ciecu_csr_set_kernel", self.handle, int(k))
+
+
+class CSROperator(LinearOperator):
+    """CSROperator<int,T>::product (linalg/packages/solvers/src/CSROperator.cpp:33-111)."""
+
+    def __init__(self, lhs, space):
+        self.lhs = lhs
+        self.space = space
+        self.csr = _CSRHandle(lhs, space)
+
+    def product(self, inScale, in_, outScale, out):
+        rows, cols = self.lhs.rowCount(), self.lhs.columnCount
+        if out.numel() != rows or in_.numel() != cols:
+            raise CiecuError(1, "Incompatible matrix-vector product: [%dx%d] * [%d] = [%d]"
+                             % (rows, cols, in_.numel(), out.numel()))
+        self.space._check(in_, out)
+        self.space.enter()
+        if self.space._sfx == "f64":
+            call("ciecu_csr_spmv_f64", self.csr.handle, float(inScale), _ptr(in_), float(outScale), _ptr(out))
+        else:
+            call("ciecu_csr_spmv_f32", self.csr.handle, float(inScale), _ptr(in_), float(outScale), _ptr(out))
+        self.space.leave()
+
+
+def _mask_tensor(mask, device):
+    if isinstance(mask, torch.Tensor) and mask.is_cuda:
+        return mask
+    arr = np.ascontiguousarray(np.asarray(mask, dtype=np.uint16)).view(np.int16)
+    return torch.as_tensor(arr).to(device)
+
+
+class MaskedCSROperator(LinearOperator):
+    """MaskedCSROperator<int,double,double,uint16_t> (MaskedCSROperator.cpp:37-118): rows and
+    columns whose mask is >= threshold are excluded; masked rows get inScale*out."""
+
+    def __init__(self, lhs, mask, threshold, space, csr_handle=None):
+        self.lhs = lhs
+        self.space = space
+        self.mask = _mask_tensor(mask, space.device)
+        self.threshold = int(threshold)
+        self.csr = csr_handle if csr_handle is not None else _CSRHandle(lhs, space)
+
+    def product(self, inScale, in_, outScale, out):
+        rows, cols = self.lhs.rowCount(), self.lhs.columnCount
+        if out.numel() != rows or in_.numel() != cols:
+            raise CiecuError(1, "Incompatible masked matrix-vector product: [%dx%d] * [%d] = [%d]"
+                             % (rows, cols, in_.numel(), out.numel()))
+        self.space._check(in_, out)
+        self.space.enter()
+        call("ciecu_csr_masked_spmv_f64", self.csr.handle, _ptr(self.mask), self.threshold, float(inScale),
+             _ptr(in_), float(outScale), _ptr(out))
+        self.space.leave()
+
+
+class DiagonalOperator(LinearOperator):
+    """DiagonalOperator<CUDASpace> (DiagonalOperator.cpp:37-53); owns the inverse diagonal."""
+
+    def __init__(self, inverseDiagonal, space):
+        self.inverseDiagonal = inverseDiagonal
+        self.space = space
+
+    def product(self, inScale, in_, outScale, out):
+        self.space._check(in_, out)
+        self.space.enter()
+        call("ciecu_diagonal_apply_f64", self.space.handle, out.numel(), _ptr(self.inverseDiagonal),
+             float(inScale), _ptr(in_), float(outScale), _ptr(out))
+        self.space.leave()
+
+
+def makeDiagonalOperator(matrix, space, csr_handle=None):
+    """makeDiagonalOperator (DiagonalOperator.cpp:56-88): raises on a missing or zero diagonal."""
+    handle = csr_handle if csr_handle is not None else _CSRHandle(matrix, space)
+    dinv = space.makeVector(matrix.rowCount())
+    space.enter()
+    call("ciecu_diagonal_inverse_f64", handle.handle, _ptr(dinv))
+    space.leave()
+    op = DiagonalOperator(dinv, space)
+    op._csr = handle
+    return op
+
+
+class JacobiOperator(LinearOperator):
+    """JacobiOperator (JacobiOperator.cpp:36-62).  With a (masked) CSR operator and a
+    DiagonalOperator every sweep is one fused kernel; any other operator pair runs
+    the reference's composition of products and space operations."""
+
+    def __init__(self, space, size, lhs, inverseDiagonal, iterations=1, relaxation=1.0):
+        self.space = space
+        self.size = int(size)
+        self.lhs = lhs
+        self.inverseDiagonal = inverseDiagonal
+        self.iterations = int(iterations)
+        self.relaxation = float(relaxation)
+        self._work = space.makeVector(2 * self.size)
+
+    def product(self, inScale, in_, outScale, out):
+        if in_.numel() != out.numel() or out.numel() != self.size:
+            raise CiecuError(1, "inconsistent input vector sizes")
+        fused = isinstance(self.lhs, (CSROperator, MaskedCSROperator)) and isinstance(
+            self.inverseDiagonal, DiagonalOperator)
+        sp = self.space
+        if fused:
+            mask = self.lhs.mask if isinstance(self.lhs, MaskedCSROperator) else None
+            thr = self.lhs.threshold if mask is not None else 0
+            sp.enter()
+            call("ciecu_jacobi_f64", self.lhs.csr.handle, _ptr(self.inverseDiagonal.inverseDiagonal), _ptr(mask),
+                 thr, self.iterations, self.relaxation, float(inScale), _ptr(in_), float(outScale), _ptr(out),
+                 _ptr(self._work))
+            sp.leave()
+            return
+        memory = sp.makeVector(self.size)
+        previous = sp.makeVector(self.size)
+        residual = sp.makeVector(self.size)
+        sp.assign(memory, out)
+        sp.fill(out, 0)
+        for _ in range(self.iterations):
+            sp.assign(previous, out)
+            sp.assign(residual, in_)
+            self.lhs.product(1, out, -1, residual)
+            self.inverseDiagonal.product(1, residual, self.relaxation, out)
+        sp.scale(out, outScale)
+        sp.add(out, memory, inScale)
+
+
+class MaskedIdentityOperator(LinearOperator):
+    """MaskedIdentityOperator (MaskedIdentityOperator.cpp:14-74)."""
+
+    def __init__(self, space, mask, threshold):
+        self.space = space
+        self.mask = _mask_tensor(mask, space.device)
+        self.threshold = int(threshold)
+
+    def product(self, inScale, in_, outScale, out):
+        self.space._check(in_, out)
+        self.space.enter()
+        call("ciecu_masked_identity_f64", self.space.handle, out.numel(), _ptr(self.mask), self.threshold,
+             float(inScale), _ptr(in_), float(outScale), _ptr(out))
+        self.space.leave()
+
+
+class NestedProductOperator(LinearOperator):
+    """NestedProductOperator (NestedProductOperator_impl.hpp:24-32): lhs(rhs(in))."""
+
+    def __init__(self, space, lhs, rhs, rowCount):
+        self.space = space
+        self.lhs = lhs
+        self.rhs = rhs
+        self._buffer = space.makeVector(rowCount)
+        space.fill(self._buffer, 0)
+
+    def product(self, inScale, in_, outScale, out):
+        self.rhs.product(0, in_, 1, self._buffer)
+        self.lhs.product(inScale, self._buffer, outScale, out)
+
+
+class ChebyshevOperator(LinearOperator):
+    """Chebyshev polynomial smoother of D^-1 A (no reference counterpart)."""
+
+    def __init__(self, lhs, inverseDiagonal, degree=4, lambdaMin=None, lambdaMax=None, ratio=30.0,
+                 powerIterations=20, seed=0):
+        self.lhs = lhs
+        self.space = lhs.space
+        self.inverseDiagonal = inverseDiagonal
+        n = lhs.lhs.rowCount()
+        self._work = self.space.makeVector(4 * n)
+        if lambdaMax is None:
+            lam = ctypes.c_double()
+            self.space.enter()
+            call("ciecu_power_lambda_max_f64", lhs.csr.handle, _ptr(inverseDiagonal.inverseDiagonal),
+                 int(powerIterations), int(seed), _ptr(self._work), ctypes.byref(lam))
+            lambdaMax = 1.1 * lam.value
+        self.lambdaMax = float(lambdaMax)
+        self.lambdaMin = float(lambdaMin) if lambdaMin is not None else self.lambdaMax / ratio
+        self.degree = int(degree)
+
+    def product(self, inScale, in_, outScale, out):
+        self.space.enter()
+        call("ciecu_chebyshev_f64", self.lhs.csr.handle, _ptr(self.inverseDiagonal.inverseDiagonal), self.degree,
+             self.lambdaMin, self.lambdaMax, float(inScale), _ptr(in_), float(outScale), _ptr(out),
+             _ptr(self._work))
+        self.space.leave()
+
+
+def _float_less(a, b):
+    """utils::Comparison<double>::less with default tolerances (Comparison_impl.hpp:32-63)."""
+    norm = min(abs(a) + abs(b), np.finfo(np.float64).max)
+    tol = max(np.finfo(np.float64).tiny, np.finfo(np.float64).eps * norm)
+    return a < b and not abs(a - b) < tol
+
+
+class ConjugateGradients(LinearOperator):
+    """ConjugateGradients<CUDASpace> (ConjugateGradients_impl.hpp:49-201).
+
+    A plain CSROperator with no preconditioner or a DiagonalOperator runs the fused
+    device-resident solver (ciecu_pcg_*).  Any other operator combination (masked
+    operators, multigrid preconditioners) runs the reference algorithm composed of
+    operator products and space operations, all on the GPU."""
+
+    def __init__(self, lhs, space, preconditioner=None, settings=None, verbosity=0):
+        self.lhs = lhs
+        self.space = space
+        self.preconditioner = preconditioner
+        self.settings = settings if settings is not None else Statistics(0, 0.0, 0.0)
+        self.verbosity = verbosity
+        self._stats = None
+        self._solver = None
+        if type(lhs) is CSROperator and space._sfx == "f64" and (
+                preconditioner is None or type(preconditioner) is DiagonalOperator):
+            h = ctypes.c_void_p()
+            dinv = preconditioner.inverseDiagonal if preconditioner is not None else None
+            self._dinv = dinv
+            call("ciecu_pcg_create", lhs.csr.handle, _ptr(dinv), self.settings, int(verbosity), ctypes.byref(h))
+            self._solver = h
+
+    def __del__(self):
+        try:
+            if getattr(self, "_solver", None):
+                _lib.load().ciecu_pcg_destroy(self._solver)
+                self._solver = None
+        except Exception:
+            pass
+
+    def configure(self, settings):
+        self.settings = settings
+        if self._solver is not None:
+            _lib.load().ciecu_pcg_destroy(self._solver)
+            h = ctypes.c_void_p()
+            call("ciecu_pcg_create", self.lhs.csr.handle, _ptr(self._dinv), settings, int(self.verbosity),
+                 ctypes.byref(h))
+            self._solver = h
+
+    def getConfiguration(self):
+        return self.settings
+
+    def getStats(self):
+        return self._stats
+
+    def set_graph_chunk(self, iterations):
+        if self._solver is not None:
+            call("ciecu_pcg_set_graph_chunk", self._solver, int(iterations))
+
+    def product(self, inScale, in_, outScale, out):
+        n = self.space.size(out)
+        if self.space.size(in_) != n:
+            raise CiecuError(1, "incompatible vector sizes %d != %d" % (self.space.size(in_), n))
+        if self._solver is not None:
+            stats = Statistics()
+            self.space._check(in_, out)
+            self.space.enter()
+            try:
+                call("ciecu_pcg_product", self._solver, float(inScale), _ptr(in_), float(outScale), _ptr(out),
+                     ctypes.byref(stats))
+            finally:
+                self._stats = stats
+                self.space.leave()
+            return
+        self._generic_product(inScale, in_, outScale, out)
+
+    def _generic_product(self, inScale, in_, outScale, out):
+        sp = self.space
+        settings = self.settings
+        n = sp.size(out)
+        stats = Statistics(0, np.finfo(np.float64).max, np.finfo(np.float64).max)
+        solution = sp.makeVector(n)
+        sp.assign(solution, out)
+        if settings.iterationCount:
+            search = sp.makeVector(n)
+            searchProduct = sp.makeVector(n)
+            sp.fill(searchProduct, 0)
+            z = None
+            residual = sp.makeVector(n)
+            sp.assign(residual, in_)
+            self.lhs.product(1, solution, -1, residual)
+            residualNorm = sp.innerProduct(residual, residual)
+            initial = float(np.sqrt(residualNorm))
+            stats.absoluteResidual = initial
+            stats.relativeResidual = 1.0
+            if _float_less(stats.absoluteResidual, settings.absoluteResidual) or _float_less(
+                    stats.relativeResidual, settings.relativeResidual):
+                self._finish(inScale, outScale, out, solution, stats)
+                return
+            if self.preconditioner is not None:
+                z = sp.makeVector(n)
+                self.preconditioner.product(0, residual, 1, z)
+                rz = sp.innerProduct(residual, z)
+                sp.assign(search, z)
+                if not 0 < rz:
+                    raise CiecuError(3, "preconditioned norm vanished in iteration 0 (r^T @ z = 0)")
+            else:
+                rz = residualNorm
+                sp.assign(search, residual)
+                if not 0 < rz:
+                    raise CiecuError(3, "residual norm vanished in iteration 0 (r^T @ r = 0)")
+            while stats.iterationCount < settings.iterationCount:
+                self.lhs.product(0, search, 1, searchProduct)
+                den = sp.innerProduct(search, searchProduct)
+                if not 0 < den:
+                    self._stats = stats
+                    raise CiecuError(3, "p^T @ A @ p vanished in iteration %d" % stats.iterationCount)
+                alpha = rz / den
+                sp.add(solution, search, alpha)
+                sp.add(residual, searchProduct, -alpha)
+                residualNorm = sp.innerProduct(residual, residual)
+                previous = rz
+                if z is not None:
+                    self.preconditioner.product(0, residual, 1, z)
+                    rz = sp.innerProduct(residual, z)
+                else:
+                    rz = residualNorm
+                sp.scale(search, rz / previous)
+                sp.add(search, z if z is not None else residual, 1)
+                stats.absoluteResidual = float(np.sqrt(residualNorm))
+                stats.relativeResidual = stats.absoluteResidual / initial
+                if _float_less(stats.absoluteResidual, settings.absoluteResidual) or _float_less(
+                        stats.relativeResidual, settings.relativeResidual):
+                    break
+                stats.iterationCount += 1
+        self._finish(inScale, outScale, out, solution, stats)
+
+    def _finish(self, inScale, outScale, out, solution, stats):
+        sp = self.space
+        if inScale == 1:
+            sp.add(out, solution, outScale)
+        elif inScale == 0:
+            sp.assign(out, solution)
+            sp.scale(out, outScale)
+        else:
+            sp.scale(out, inScale)
+            sp.add(out, solution, outScale)
+        self._stats = stats

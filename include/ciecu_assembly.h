@@ -1,0 +1,56 @@
+/*
+ * ciecu assembly: per-element stiffness integration and CSR scatter on the GPU,
+ * the device counterpart of IntegrandProcessor (SYCLIntegrandProcessor,
+ * fem/packages/utilities/inc/IntegrandProcessor.hpp:138-158) evaluating
+ * TransformedIntegrand<LinearIsotropicStiffnessIntegrand> and of
+ * Assembler::addContribution (fem/packages/graph/impl/Assembler_impl.hpp:156-194).
+ */
+#ifndef CIECU_ASSEMBLY_H
+#define CIECU_ASSEMBLY_H
+
+#include "ciecu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ciecu_assembly_s* ciecu_assembly;
+
+/* Plan for repeated assembly into the pattern of `csr` (FP64 values): tensor
+ * Lagrange Q_order cells on equispaced nodes, quadratureOrder^dim Gauss-Legendre
+ * points (the reference uses order + 1, definitions.hpp:36), device DoF map
+ * (ncells x (order+1)^dim, local index first-1-D-index fastest), host colours
+ * (cells of one colour must share no DoF; NULL = one colour).  Builds the
+ * element -> CSR-entry map once and fails with CIECU_ERR_PATTERN if an element
+ * entry is missing from the pattern (CIE_OUT_OF_RANGE_CHECK of
+ * Assembler_impl.hpp:178-180). */
+int ciecu_assembly_create(ciecu_csr csr, int dim, int order, int quadratureOrder, int64_t ncells,
+                          const int32_t* d_dofmap, const int32_t* h_color, ciecu_assembly* out);
+int ciecu_assembly_destroy(ciecu_assembly plan);
+int ciecu_assembly_color_count(ciecu_assembly plan, int* h_count);
+
+/* d_entries (+)= sum_e K_e scattered into the CSR values, one launch per colour,
+ * no atomics.  K_e = kappa_e * |det J^-1| * sum_q w_q G_q^T G_q with parametric
+ * gradients (convention 0, the reference's TransformedIntegrand.hpp:73-83 with
+ * the inverse Jacobian passed by integration.cpp:92-97) or the physical
+ * kappa_e * det J * sum_q w_q (J^-T G_q)^T (J^-T G_q) (convention 1).
+ * h_cellSize: dim edge lengths of the (uniform) cells.  accumulate = 0 zeroes
+ * d_entries first. */
+int ciecu_assemble_stiffness(ciecu_assembly plan, const double* d_kappa, const double* h_cellSize, int convention,
+                             int accumulate, double* d_entries);
+
+/* Adjoint gradient of J(u) with respect to the cell conductivities:
+ * d_grad[e] = -lambda_e^T (dK_e/dkappa_e) u_e = -lambda_e^T K_e(kappa = 1) u_e.
+ * d_work: nb*nb doubles. */
+int ciecu_element_gradient(ciecu_assembly plan, const double* h_cellSize, int convention, const double* d_lambda,
+                           const double* d_u, double* d_grad, double* d_work);
+
+/* Symmetric elimination of homogeneous Dirichlet DoFs (fem/test/test_1d.cpp:291-313):
+ * rows and columns of boundary DoFs zeroed (structural zeros kept), diagonal 1,
+ * d_rhs[boundary] = 0 (d_rhs may be NULL). */
+int ciecu_dirichlet_eliminate(ciecu_csr csr, const uint8_t* d_isBoundary, double* d_entries, double* d_rhs);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CIECU_ASSEMBLY_H */

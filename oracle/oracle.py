@@ -1,0 +1,283 @@
+"""ORACLE / TEST INFRASTRUCTURE ONLY.
+
+ctypes front end of the two CPU checkers built by oracle/Makefile:
+  Restatement  liboracle.so          plain-C restatement of the reference algorithms
+  Reference    _ref/libcieref.so     the reference's own FP64 CPU solver (compiled in place)
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import this.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+RESTATE_PATH = os.path.join(HERE, "liboracle.so")
+REF_PATH = os.path.join(HERE, "_ref", "libcieref.so")
+
+_P = ctypes.c_void_p
+_i, _l, _d, _u16, _u64 = ctypes.c_int, ctypes.c_long, ctypes.c_double, ctypes.c_uint16, ctypes.c_uint64
+
+
+def p(a):
+    return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
+
+
+def build(reference=True):
+    """Build the restatement (and the reference library when its sources exist)."""
+    target = "all" if reference else "restatement"
+    subprocess.run(["make", "-s", "-C", HERE, target], check=True)
+
+
+class Restatement:
+    def __init__(self):
+        if not os.path.exists(RESTATE_PATH):
+            build(reference=False)
+        L = ctypes.CDLL(RESTATE_PATH)
+        sig = {
+            "ora_spmv": (None, [_i, _P, _P, _P, _d, _P, _d, _P]),
+            "ora_masked_spmv": (None, [_i, _P, _P, _P, _P, _u16, _d, _P, _d, _P]),
+            "ora_diag_inverse": (_i, [_i, _P, _P, _P, _P]),
+            "ora_dot": (_d, [_l, _P, _P]),
+            "ora_pcg": (_i, [_i, _P, _P, _P, _P, _P, _l, _d, _d, _i, _P]),
+            "ora_jacobi": (None, [_i, _P, _P, _P, _P, _l, _d, _d, _P, _d, _P]),
+            "ora_chebyshev": (None, [_i, _P, _P, _P, _P, _i, _d, _d, _P, _P]),
+            "ora_power_lambda_max": (_d, [_i, _P, _P, _P, _P, _i, _u64]),
+            "ora_gauss_legendre": (_i, [_i, _P, _P]),
+            "ora_lagrange_1d": (None, [_i, _P, _d, _P, _P]),
+            "ora_stiffness_point": (None, [_i, _i, _P, _i, _P, _d, _P]),
+            "ora_element_stiffness": (None, [_i, _i, _i, _P, _P, _d, _P, _i, _P]),
+            "ora_structured_dofmap": (None, [_i, _i, _P, _P]),
+            "ora_csr_pattern": (_l, [_l, _i, _P, _i, _P, _P]),
+            "ora_assemble": (_i, [_l, _i, _P, _P, _P, _P, _P]),
+            "ora_element_gradient": (None, [_l, _i, _P, _P, _P, _P, _P]),
+            "ora_dirichlet_eliminate": (None, [_i, _P, _P, _P, _P, _P]),
+            "ora_cut_cell_points": (_i, [_i, _i, _i, _P, _d, _P, _P, _i, _P, _P, _P, _d]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        self.L = L
+
+    # -- linalg --
+    def spmv(self, rowptr, col, val, inScale, x, outScale, y):
+        y = np.array(y, dtype=np.float64, copy=True)
+        self.L.ora_spmv(len(rowptr) - 1, p(rowptr), p(col), p(val), inScale, p(x), outScale, p(y))
+        return y
+
+    def masked_spmv(self, rowptr, col, val, mask, threshold, inScale, x, outScale, y):
+        y = np.array(y, dtype=np.float64, copy=True)
+        mask = np.ascontiguousarray(mask, dtype=np.uint16)
+        self.L.ora_masked_spmv(len(rowptr) - 1, p(rowptr), p(col), p(val), p(mask), threshold, inScale, p(x),
+                               outScale, p(y))
+        return y
+
+    def diag_inverse(self, rowptr, col, val):
+        out = np.zeros(len(rowptr) - 1)
+        bad = self.L.ora_diag_inverse(len(rowptr) - 1, p(rowptr), p(col), p(val), p(out))
+        return out, bad
+
+    def pcg(self, rowptr, col, val, b, x0=None, maxit=5000, abstol=0.0, reltol=1e-10, precondition=True):
+        n = len(rowptr) - 1
+        x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64, copy=True)
+        stats = np.zeros(3)
+        st = self.L.ora_pcg(n, p(rowptr), p(col), p(val), p(b), p(x), maxit, abstol, reltol, int(precondition),
+                            p(stats))
+        return x, stats, st
+
+    def jacobi(self, rowptr, col, val, dinv, iterations, relaxation, inScale, x, outScale, y):
+        y = np.array(y, dtype=np.float64, copy=True)
+        self.L.ora_jacobi(len(rowptr) - 1, p(rowptr), p(col), p(val), p(dinv), iterations, relaxation, inScale, p(x),
+                          outScale, p(y))
+        return y
+
+    def chebyshev(self, rowptr, col, val, dinv, degree, lmin, lmax, x):
+        y = np.zeros(len(rowptr) - 1)
+        self.L.ora_chebyshev(len(rowptr) - 1, p(rowptr), p(col), p(val), p(dinv), degree, lmin, lmax, p(x), p(y))
+        return y
+
+    def power_lambda_max(self, rowptr, col, val, dinv, iterations, seed):
+        return self.L.ora_power_lambda_max(len(rowptr) - 1, p(rowptr), p(col), p(val), p(dinv), iterations, seed)
+
+    # -- fem --
+    def gauss_legendre(self, order):
+        n, w = np.zeros(order), np.zeros(order)
+        st = self.L.ora_gauss_legendre(order, p(n), p(w))
+        assert st == 0
+        return n, w
+
+    def stiffness_point(self, dim, coefficients, point, modulus):
+        coefficients = np.ascontiguousarray(coefficients, dtype=np.float64)
+        setSize, deg1 = coefficients.shape
+        out = np.zeros((setSize ** dim) ** 2)
+        self.L.ora_stiffness_point(dim, setSize, p(coefficients), deg1 - 1, p(np.asarray(point, dtype=np.float64)),
+                                   modulus, p(out))
+        return out
+
+    def tensor_gauss(self, dim, order):
+        """Tensor Gauss points, first 1-D index fastest (OuterProduct_impl.hpp:27-45)."""
+        n, w = self.gauss_legendre(order)
+        q = np.arange(order ** dim)
+        idx = (q[:, None] // order ** np.arange(dim)[None, :]) % order
+        return np.ascontiguousarray(n[idx]), np.ascontiguousarray(np.prod(w[idx], axis=1))
+
+    def element_stiffness(self, dim, order, kappa, h, convention=0, points=None, weights=None):
+        if points is None:
+            points, weights = self.tensor_gauss(dim, order + 1)
+        nb = (order + 1) ** dim
+        K = np.zeros(nb * nb)
+        self.L.ora_element_stiffness(dim, order, len(weights), p(points), p(weights), kappa,
+                                     p(np.asarray(h, dtype=np.float64)), convention, p(K))
+        return K
+
+    def structured_dofmap(self, dim, order, cells):
+        cells = np.asarray(cells, dtype=np.int32)
+        nb = (order + 1) ** dim
+        out = np.zeros(int(np.prod(cells)) * nb, dtype=np.int32)
+        self.L.ora_structured_dofmap(dim, order, p(cells), p(out))
+        return out
+
+    def csr_pattern(self, ncells, nb, dofmap, ndofs):
+        rowptr = np.zeros(ndofs + 1, dtype=np.int32)
+        nnz = self.L.ora_csr_pattern(ncells, nb, p(dofmap), ndofs, p(rowptr), None)
+        col = np.zeros(nnz, dtype=np.int32)
+        self.L.ora_csr_pattern(ncells, nb, p(dofmap), ndofs, p(rowptr), p(col))
+        return rowptr, col
+
+    def assemble(self, ncells, nb, dofmap, Ke, rowptr, col, val=None):
+        val = np.zeros(len(col)) if val is None else np.array(val, dtype=np.float64, copy=True)
+        st = self.L.ora_assemble(ncells, nb, p(dofmap), p(np.ascontiguousarray(Ke, dtype=np.float64)), p(rowptr),
+                                 p(col), p(val))
+        return val, st
+
+    def element_gradient(self, ncells, nb, dofmap, Kunit, lam, u):
+        g = np.zeros(ncells)
+        self.L.ora_element_gradient(ncells, nb, p(dofmap), p(np.ascontiguousarray(Kunit)), p(lam), p(u), p(g))
+        return g
+
+    def dirichlet(self, rowptr, col, val, isBoundary, rhs=None):
+        val = np.array(val, dtype=np.float64, copy=True)
+        rhs = None if rhs is None else np.array(rhs, dtype=np.float64, copy=True)
+        self.L.ora_dirichlet_eliminate(len(rowptr) - 1, p(rowptr), p(col), p(val),
+                                       p(np.ascontiguousarray(isBoundary, dtype=np.uint8)), p(rhs))
+        return val, rhs
+
+    def cut_cell_points(self, dim, depth, order, center, radius, origin, size, alpha, maxPoints=1 << 16):
+        pts = np.zeros(maxPoints * dim)
+        w = np.zeros(maxPoints)
+        s = np.zeros(maxPoints)
+        n = self.L.ora_cut_cell_points(dim, depth, order, p(np.asarray(center, dtype=np.float64)), radius,
+                                       p(np.asarray(origin, dtype=np.float64)), p(np.asarray(size, dtype=np.float64)),
+                                       maxPoints, p(pts), p(w), p(s), alpha)
+        assert n >= 0
+        return pts[: n * dim].reshape(n, dim), w[:n], s[:n]
+
+
+class Reference:
+    """The reference's compiled CPU solver (oracle/_ref/libcieref.so)."""
+
+    def __init__(self, threads=None):
+        if not os.path.exists(REF_PATH):
+            raise FileNotFoundError("oracle/_ref/libcieref.so is not built (needs the reference sources)")
+        L = ctypes.CDLL(REF_PATH)
+        sig = {
+            "cieref_last_error": (_i, [ctypes.c_char_p, _i]),
+            "cieref_max_threads": (_i, []),
+            "cieref_pool_create": (_P, [_i]),
+            "cieref_pool_destroy": (None, [_P]),
+            "cieref_spmv": (_i, [_P, _i, _i, _P, _P, _P, _d, _P, _d, _P]),
+            "cieref_masked_spmv": (_i, [_P, _i, _i, _P, _P, _P, _P, _u16, _d, _P, _d, _P]),
+            "cieref_diag_inverse": (_i, [_i, _P, _P, _P, _P]),
+            "cieref_pcg": (_i, [_P, _i, _P, _P, _P, _P, _P, _l, _d, _d, _i, _i, _P, _P]),
+            "cieref_jacobi": (_i, [_P, _i, _P, _P, _P, _l, _d, _d, _P, _d, _P]),
+            "cieref_pmg": (_i, [_P, _i, _P, _P, _P, _P, _i, _P, _P, _d, _l, _P, _P]),
+            "cieref_space_dot": (_i, [_P, _l, _P, _P, _P]),
+            "cieref_space_op": (_i, [_P, _i, _l, _P, _P, _d]),
+            "cieref_gauss_legendre": (_i, [_i, _P, _P]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        self.L = L
+        self.threads = int(threads) if threads else int(L.cieref_max_threads())
+        self.pool = L.cieref_pool_create(self.threads) if self.threads > 1 else None
+
+    def close(self):
+        if self.pool:
+            self.L.cieref_pool_destroy(self.pool)
+            self.pool = None
+
+    def _err(self):
+        b = ctypes.create_string_buffer(2048)
+        self.L.cieref_last_error(b, 2048)
+        return b.value.decode()
+
+    def _check(self, st):
+        if st:
+            raise RuntimeError("reference: " + self._err())
+
+    def spmv(self, rowptr, col, val, inScale, x, outScale, y, ncols=None):
+        y = np.array(y, dtype=np.float64, copy=True)
+        n = len(rowptr) - 1
+        self._check(self.L.cieref_spmv(self.pool, n, ncols if ncols is not None else len(x), p(rowptr), p(col),
+                                       p(val), inScale, p(x), outScale, p(y)))
+        return y
+
+    def masked_spmv(self, rowptr, col, val, mask, threshold, inScale, x, outScale, y):
+        y = np.array(y, dtype=np.float64, copy=True)
+        mask = np.ascontiguousarray(mask, dtype=np.uint16)
+        self._check(self.L.cieref_masked_spmv(self.pool, len(rowptr) - 1, len(x), p(rowptr), p(col), p(val),
+                                              p(mask), threshold, inScale, p(x), outScale, p(y)))
+        return y
+
+    def diag_inverse(self, rowptr, col, val):
+        out = np.zeros(len(rowptr) - 1)
+        st = self.L.cieref_diag_inverse(len(rowptr) - 1, p(rowptr), p(col), p(val), p(out))
+        return out, (self._err() if st else None)
+
+    def pcg(self, rowptr, col, val, b, x0=None, maxit=5000, abstol=0.0, reltol=1e-10, precondition=True):
+        n = len(rowptr) - 1
+        x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64, copy=True)
+        stats = np.zeros(3)
+        secs = ctypes.c_double()
+        st = self.L.cieref_pcg(self.pool, n, p(rowptr), p(col), p(val), p(b), p(x), maxit, abstol, reltol,
+                               int(precondition), 0, p(stats), ctypes.byref(secs))
+        return x, stats, (self._err() if st else None), secs.value
+
+    def jacobi(self, rowptr, col, val, iterations, relaxation, inScale, x, outScale, y):
+        y = np.array(y, dtype=np.float64, copy=True)
+        self._check(self.L.cieref_jacobi(self.pool, len(rowptr) - 1, p(rowptr), p(col), p(val), iterations,
+                                         relaxation, inScale, p(x), outScale, p(y)))
+        return y
+
+    def pmg(self, rowptr, col, val, mask, order, b, tol=1e-6, maxCycles=200):
+        n = len(rowptr) - 1
+        x = np.zeros(n)
+        cycles = ctypes.c_long()
+        rel = ctypes.c_double()
+        self._check(self.L.cieref_pmg(self.pool, n, p(rowptr), p(col), p(val),
+                                      p(np.ascontiguousarray(mask, dtype=np.uint16)), order, p(b), p(x), tol,
+                                      maxCycles, ctypes.byref(cycles), ctypes.byref(rel)))
+        return x, cycles.value, rel.value
+
+    def dot(self, a, b):
+        out = ctypes.c_double()
+        self._check(self.L.cieref_space_dot(self.pool, len(a), p(a), p(b), ctypes.byref(out)))
+        return out.value
+
+    def space_op(self, op, target, source, alpha):
+        t = np.array(target, dtype=np.float64, copy=True)
+        self._check(self.L.cieref_space_op(self.pool, op, len(t), p(t), p(source), alpha))
+        return t
+
+    def gauss_legendre(self, order):
+        n, w = np.zeros(order), np.zeros(order)
+        self._check(self.L.cieref_gauss_legendre(order, p(n), p(w)))
+        return n, w
+
+
+def reference_available():
+    return os.path.exists(REF_PATH)

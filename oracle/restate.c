@@ -1,0 +1,613 @@
+/* ORACLE / TEST INFRASTRUCTURE ONLY -- see restate.h.
+ *
+ * Each function cites the kelofm/cie source it restates (paths relative to the
+ * reference project root).  Compiled with -ffp-contract=off so that the
+ * restatement evaluates every expression exactly as written.
+ */
+#include "restate.h"
+
+#define ORA_PI 3.14159265358979323846
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include <float.h>
+
+/* out = inScale*out + outScale*sum, with the reference's special cases for
+ * scales in {-1, 0, 1}, including the (-1, -1) quirk that yields sum - out.
+ * linalg/packages/solvers/src/CSROperator.cpp:78-110 */
+static double combine(double inScale, double old, double outScale, double sum) {
+    if (inScale == 1.0) {
+        if (outScale == 1.0) return old + sum;
+        if (outScale == -1.0) return old - sum;
+        return old + outScale * sum;
+    }
+    if (inScale == 0.0) {
+        if (outScale == 1.0) return sum;
+        if (outScale == -1.0) return -sum;
+        return outScale * sum;
+    }
+    if (inScale == -1.0) {
+        if (outScale == 1.0 || outScale == -1.0) return sum - old;
+        return outScale * sum - old;
+    }
+    if (outScale == 1.0) return inScale * old + sum;
+    if (outScale == -1.0) return inScale * old - sum;
+    return inScale * old + outScale * sum;
+}
+
+/* linalg/packages/solvers/src/CSROperator.cpp:46-58 (row loop), :78-110 (combine) */
+void ora_spmv(int nrows, const int* rowptr, const int* col, const double* val,
+              double inScale, const double* in, double outScale, double* out) {
+    for (int i = 0; i < nrows; ++i) {
+        double s = 0.0;
+        for (int k = rowptr[i]; k < rowptr[i + 1]; ++k) s += val[k] * in[col[k]];
+        out[i] = combine(inScale, out[i], outScale, s);
+    }
+}
+
+/* linalg/packages/solvers/src/MaskedCSROperator.cpp:51-66: masked rows contribute 0
+ * (CPU semantics), masked columns are skipped. */
+void ora_masked_spmv(int nrows, const int* rowptr, const int* col, const double* val,
+                     const uint16_t* mask, uint16_t threshold, double inScale,
+                     const double* in, double outScale, double* out) {
+    for (int i = 0; i < nrows; ++i) {
+        double s = 0.0;
+        if (mask[i] < threshold)
+            for (int k = rowptr[i]; k < rowptr[i + 1]; ++k)
+                if (mask[col[k]] < threshold) s += val[k] * in[col[k]];
+        out[i] = combine(inScale, out[i], outScale, s);
+    }
+}
+
+/* linalg/packages/solvers/src/DiagonalOperator.cpp:56-88.  Returns -1 on success,
+ * else the first row with a missing or zero diagonal. */
+int ora_diag_inverse(int n, const int* rowptr, const int* col, const double* val, double* dinv) {
+    for (int i = 0; i < n; ++i) {
+        int found = 0;
+        for (int k = rowptr[i]; k < rowptr[i + 1]; ++k)
+            if (col[k] == i) {
+                if (val[k] == 0.0) return i;
+                dinv[i] = 1.0 / val[k];
+                found = 1;
+                break;
+            }
+        if (!found) return i;
+    }
+    return -1;
+}
+
+/* linalg/packages/solvers/src/DefaultSpace.cpp:71-76 (serial inner_product) */
+double ora_dot(long n, const double* a, const double* b) {
+    double s = 0.0;
+    for (long i = 0; i < n; ++i) s += a[i] * b[i];
+    return s;
+}
+
+/* cieutils/packages/maths/impl/Comparison_impl.hpp:32-63 with the default
+ * tolerances (DBL_MIN, DBL_EPSILON). */
+static int float_less(double a, double b) {
+    double norm = fabs(a) + fabs(b);
+    if (norm > DBL_MAX) norm = DBL_MAX;
+    double tol = DBL_EPSILON * norm;
+    if (tol < DBL_MIN) tol = DBL_MIN;
+    const int equal = fabs(a - b) < tol;
+    return a < b && !equal;
+}
+
+/* linalg/packages/solvers/impl/ConjugateGradients_impl.hpp:49-201, Jacobi
+ * preconditioner from DiagonalOperator.cpp:37-53.  out (x) is the initial guess
+ * and receives the solution (inScale 0, outScale 1).  stats = {iterations,
+ * absolute residual, relative residual}.  Returns 0, or 1 (r^T z <= 0 at start),
+ * 2 (p^T A p <= 0), 3 (missing/zero diagonal). */
+int ora_pcg(int n, const int* rowptr, const int* col, const double* val, const double* b,
+            double* x, long maxIterations, double absoluteTolerance, double relativeTolerance,
+            int precondition, double* stats) {
+    double* r = (double*)malloc(sizeof(double) * (size_t)n);
+    double* p = (double*)malloc(sizeof(double) * (size_t)n);
+    double* q = (double*)calloc((size_t)n, sizeof(double));
+    double* z = (double*)malloc(sizeof(double) * (size_t)n);
+    double* dinv = (double*)malloc(sizeof(double) * (size_t)n);
+    int status = 0;
+    long it = 0;
+    double absres = DBL_MAX, relres = DBL_MAX;
+    if (precondition && ora_diag_inverse(n, rowptr, col, val, dinv) >= 0) {
+        status = 3;
+        goto done;
+    }
+    if (maxIterations > 0) {
+        memcpy(r, b, sizeof(double) * (size_t)n);
+        ora_spmv(n, rowptr, col, val, 1.0, x, -1.0, r); /* r = b - A x  (:86-88) */
+        double rr = ora_dot(n, r, r);
+        const double r0 = sqrt(rr);
+        absres = r0;
+        relres = 1.0;
+        if (float_less(absres, absoluteTolerance) || float_less(relres, relativeTolerance)) goto done;
+        double rz;
+        if (precondition) {
+            for (int i = 0; i < n; ++i) z[i] = r[i] * dinv[i];
+            rz = ora_dot(n, r, z);
+            memcpy(p, z, sizeof(double) * (size_t)n);
+        } else {
+            rz = rr;
+            memcpy(p, r, sizeof(double) * (size_t)n);
+        }
+        if (!(0.0 < rz)) { status = 1; goto done; }
+        for (; it < maxIterations; ++it) {
+            ora_spmv(n, rowptr, col, val, 0.0, p, 1.0, q); /* :136 */
+            const double pq = ora_dot(n, p, q);
+            if (!(0.0 < pq)) { status = 2; goto done; }
+            const double alpha = rz / pq;
+            for (int i = 0; i < n; ++i) x[i] = x[i] + alpha * p[i];
+            const double malpha = -alpha;
+            for (int i = 0; i < n; ++i) r[i] = r[i] + malpha * q[i];
+            rr = ora_dot(n, r, r);
+            const double rzOld = rz;
+            if (precondition) {
+                for (int i = 0; i < n; ++i) z[i] = r[i] * dinv[i];
+                rz = ora_dot(n, r, z);
+            } else {
+                rz = rr;
+            }
+            const double beta = rz / rzOld;
+            const double* zz = precondition ? z : r;
+            for (int i = 0; i < n; ++i) p[i] = p[i] * beta;
+            for (int i = 0; i < n; ++i) p[i] = p[i] + zz[i];
+            absres = sqrt(rr);
+            relres = absres / r0;
+            if (float_less(absres, absoluteTolerance) || float_less(relres, relativeTolerance)) break;
+        }
+    }
+done:
+    if (stats) {
+        stats[0] = (double)it;
+        stats[1] = absres;
+        stats[2] = relres;
+    }
+    free(r); free(p); free(q); free(z); free(dinv);
+    return status;
+}
+
+/* linalg/packages/solvers/src/JacobiOperator.cpp:36-62 with a DiagonalOperator
+ * as inverse diagonal: starting from 0, x <- x + w * D^-1 (in - A x), then
+ * out = inScale*out_old + outScale*x (scale(out,outScale); add(out,memory,inScale)). */
+void ora_jacobi(int n, const int* rowptr, const int* col, const double* val, const double* dinv,
+                long iterations, double relaxation, double inScale, const double* in,
+                double outScale, double* out) {
+    double* memory = (double*)malloc(sizeof(double) * (size_t)n);
+    double* x = (double*)calloc((size_t)n, sizeof(double));
+    double* res = (double*)malloc(sizeof(double) * (size_t)n);
+    memcpy(memory, out, sizeof(double) * (size_t)n);
+    for (long s = 0; s < iterations; ++s) {
+        memcpy(res, in, sizeof(double) * (size_t)n);
+        ora_spmv(n, rowptr, col, val, 1.0, x, -1.0, res); /* res = in - A x */
+        for (int i = 0; i < n; ++i) {
+            /* DiagonalOperator::product(1, res, w, x): buffer = res*dinv*w; x += buffer */
+            const double t = relaxation == 1.0 ? res[i] * dinv[i]
+                             : (relaxation == -1.0 ? -res[i] * dinv[i] : relaxation * res[i] * dinv[i]);
+            x[i] = x[i] + t;
+        }
+    }
+    for (int i = 0; i < n; ++i) {
+        const double sx = x[i] * outScale;
+        out[i] = inScale == 1.0 ? sx + memory[i]
+               : (inScale == -1.0 ? sx - memory[i] : sx + inScale * memory[i]);
+    }
+    free(memory); free(x); free(res);
+}
+
+/* Chebyshev polynomial smoother for D^-1 A on [lambdaMin, lambdaMax], applied to
+ * in from a zero initial guess (no reference counterpart).  Three-term recurrence
+ * of Saad, "Iterative Methods for Sparse Linear Systems", 2nd ed., Alg. 12.1:
+ *   theta = (lmax+lmin)/2, delta = (lmax-lmin)/2, sigma = theta/delta, rho_0 = 1/sigma
+ *   d_0 = D^-1 r_0 / theta;  x_1 = d_0
+ *   rho_k = 1/(2 sigma - rho_{k-1});  d_k = rho_k rho_{k-1} d_{k-1} + 2 rho_k/delta D^-1 r_k
+ *   x_{k+1} = x_k + d_k,  r_{k+1} = r_k - A d_k. */
+void ora_chebyshev(int n, const int* rowptr, const int* col, const double* val,
+                   const double* dinv, int degree, double lambdaMin, double lambdaMax,
+                   const double* in, double* out) {
+    double* r = (double*)malloc(sizeof(double) * (size_t)n);
+    double* d = (double*)malloc(sizeof(double) * (size_t)n);
+    double* ad = (double*)malloc(sizeof(double) * (size_t)n);
+    const double theta = 0.5 * (lambdaMax + lambdaMin);
+    const double delta = 0.5 * (lambdaMax - lambdaMin);
+    const double sigma = theta / delta;
+    double rho = 1.0 / sigma;
+    memcpy(r, in, sizeof(double) * (size_t)n);
+    for (int i = 0; i < n; ++i) {
+        d[i] = dinv[i] * r[i] / theta;
+        out[i] = 0.0;
+    }
+    for (int k = 0; k < degree; ++k) {
+        for (int i = 0; i < n; ++i) out[i] += d[i];
+        if (k + 1 == degree) break;
+        ora_spmv(n, rowptr, col, val, 0.0, d, 1.0, ad);
+        for (int i = 0; i < n; ++i) r[i] -= ad[i];
+        const double rhoNew = 1.0 / (2.0 * sigma - rho);
+        for (int i = 0; i < n; ++i) d[i] = rhoNew * rho * d[i] + 2.0 * rhoNew / delta * dinv[i] * r[i];
+        rho = rhoNew;
+    }
+    free(r); free(d); free(ad);
+}
+
+static uint64_t splitmix(uint64_t* s) {
+    uint64_t z = (*s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+/* Largest eigenvalue of D^-1 A by power iteration (Chebyshev bounds). */
+double ora_power_lambda_max(int n, const int* rowptr, const int* col, const double* val,
+                            const double* dinv, int iterations, uint64_t seed) {
+    double* v = (double*)malloc(sizeof(double) * (size_t)n);
+    double* w = (double*)malloc(sizeof(double) * (size_t)n);
+    uint64_t s = seed;
+    for (int i = 0; i < n; ++i) v[i] = (double)(splitmix(&s) >> 11) * 0x1.0p-53 + 0.5;
+    double lambda = 0.0;
+    for (int it = 0; it < iterations; ++it) {
+        double nv = sqrt(ora_dot(n, v, v));
+        for (int i = 0; i < n; ++i) v[i] /= nv;
+        ora_spmv(n, rowptr, col, val, 0.0, v, 1.0, w);
+        for (int i = 0; i < n; ++i) w[i] *= dinv[i];
+        lambda = ora_dot(n, v, w);
+        memcpy(v, w, sizeof(double) * (size_t)n);
+    }
+    free(v); free(w);
+    return lambda;
+}
+
+/* ---- fem ------------------------------------------------------------- */
+
+/* Legendre P_n(x) by the three-term recurrence (std::legendre in the reference). */
+static double legendre(int n, double x) {
+    if (n == 0) return 1.0;
+    double p0 = 1.0, p1 = x;
+    for (int k = 2; k <= n; ++k) {
+        const double p2 = ((2.0 * k - 1.0) * x * p1 - (k - 1.0) * p0) / k;
+        p0 = p1;
+        p1 = p2;
+    }
+    return p1;
+}
+
+/* fem/packages/numeric/src/GaussLegendreQuadrature.cpp:82-175: Newton iteration on
+ * P_n from the initial guess (1 - (1/8 - 1/(8n))/n^2) cos(pi (4i-1)/(4n+2)), i = n-index,
+ * convergence when |P_n| is "equal" to 0 under Comparison(256 eps, 256 eps);
+ * weight = 2 / P_n'^2 / (1 - x^2); nodes ascending, mirrored. */
+int ora_gauss_legendre(int order, double* nodes, double* weights) {
+    if (order < 1) return 1;
+    const double tol = 256.0 * DBL_EPSILON;
+    int pivot;
+    if (order % 2 == 1 && order > 1) {
+        pivot = order / 2 + 1;
+        nodes[pivot] = 0.0;
+        double w = order * legendre(order - 1, 0.0);
+        weights[pivot] = 2.0 / w / w;
+        --pivot;
+    } else {
+        pivot = order / 2;
+    }
+    for (int index = 0; index <= pivot && index < order; ++index) {
+        const int i = order - index;
+        double node = (1.0 - (0.125 - 0.125 / order) / ((double)order * order)) *
+                      cos(ORA_PI * (4.0 * i - 1.0) / (4.0 * order + 2.0));
+        double omx2 = 1.0 - node * node;
+        double value = 0.0, deriv = 0.0;
+        int converged = 0;
+        for (int k = 0; k < 50; ++k) {
+            value = legendre(order, node);
+            deriv = order * (-node * value + legendre(order - 1, node)) / omx2;
+            /* Comparison::equal(|value|, 0) */
+            double t = tol * fabs(value);
+            if (t < tol) t = tol;
+            if (fabs(value) < t) { converged = 1; break; }
+            node -= value / deriv;
+            omx2 = 1.0 - node * node;
+        }
+        if (!converged) return 2;
+        const double w = 2.0 / deriv / deriv / omx2;
+        nodes[index] = node;
+        weights[index] = w;
+        nodes[order - index - 1] = -node;
+        weights[order - index - 1] = w;
+    }
+    return 0;
+}
+
+/* Lagrange basis on the given nodes in product form and its derivative
+ * (fem/packages/maths/src/LagrangePolynomial.cpp:18-72 builds the same
+ * polynomials as coefficient vectors). */
+void ora_lagrange_1d(int count, const double* nodes, double x, double* values, double* derivatives) {
+    for (int i = 0; i < count; ++i) {
+        double v = 1.0;
+        for (int j = 0; j < count; ++j)
+            if (j != i) v *= (x - nodes[j]) / (nodes[i] - nodes[j]);
+        double d = 0.0;
+        for (int k = 0; k < count; ++k) {
+            if (k == i) continue;
+            double t = 1.0 / (nodes[i] - nodes[k]);
+            for (int j = 0; j < count; ++j)
+                if (j != i && j != k) t *= (x - nodes[j]) / (nodes[i] - nodes[j]);
+            d += t;
+        }
+        values[i] = v;
+        derivatives[i] = d;
+    }
+}
+
+/* Horner evaluation of a polynomial with ascending coefficients and of its
+ * derivative (fem/packages/maths/impl/Polynomial_impl.hpp:83-105). */
+static void horner(const double* c, int degree, double x, double* value, double* deriv) {
+    double v = c[degree], d = 0.0;
+    for (int k = degree - 1; k >= 0; --k) {
+        d = d * x + v;
+        v = v * x + c[k];
+    }
+    *value = v;
+    *deriv = d;
+}
+
+/* Parametric gradient matrix G (dim x setSize^dim, row-major) of the tensor-product
+ * basis, first 1-D index fastest (fem/packages/maths/impl/AnsatzSpace_impl.hpp:231-328). */
+static void tensor_gradients(int dim, int setSize, const double* values /*dim x setSize*/,
+                             const double* derivs /*dim x setSize*/, double* G) {
+    int nb = 1;
+    for (int d = 0; d < dim; ++d) nb *= setSize;
+    for (int dd = 0; dd < dim; ++dd)
+        for (int a = 0; a < nb; ++a) {
+            int rest = a;
+            double g = 1.0;
+            for (int d = 0; d < dim; ++d) {
+                const int i = rest % setSize;
+                rest /= setSize;
+                g *= (d == dd) ? derivs[d * setSize + i] : values[d * setSize + i];
+            }
+            G[dd * nb + a] = g;
+        }
+}
+
+/* LinearIsotropicStiffnessIntegrand::evaluate at one point:
+ * out = modulus * G^T G (fem/packages/integrands/impl/LinearIsotropicStiffnessIntegrand_impl.hpp:62-75)
+ * with a 1-D basis given as ascending monomial coefficients. */
+void ora_stiffness_point(int dim, int setSize, const double* coefficients, int degree,
+                         const double* point, double modulus, double* out) {
+    double values[3 * 16], derivs[3 * 16];
+    int nb = 1;
+    for (int d = 0; d < dim; ++d) nb *= setSize;
+    for (int d = 0; d < dim; ++d)
+        for (int i = 0; i < setSize; ++i)
+            horner(coefficients + i * (degree + 1), degree, point[d], &values[d * setSize + i],
+                   &derivs[d * setSize + i]);
+    double* G = (double*)malloc(sizeof(double) * (size_t)(dim * nb));
+    tensor_gradients(dim, setSize, values, derivs, G);
+    for (int a = 0; a < nb; ++a)
+        for (int b = 0; b < nb; ++b) {
+            double s = 0.0;
+            for (int d = 0; d < dim; ++d) s += G[d * nb + a] * G[d * nb + b];
+            out[a * nb + b] = modulus * s;
+        }
+    free(G);
+}
+
+/* Element stiffness for a Lagrange basis of the given order on equispaced nodes
+ * -1 + 2i/order, integrated over the supplied parametric points (nq x dim) and
+ * weights:
+ *  convention 0 (reference): K = kappa * prod_d(2/h_d) * sum_q w_q G_q^T G_q
+ *     (TransformedIntegrand.hpp:73-83 scales by |det| of the passed inverse
+ *      Jacobian; QuadraturePoint.hpp:84-90 multiplies by the weight)
+ *  convention 1 (physical): K = kappa * prod_d(h_d/2) * sum_q w_q (J^-T G)^T (J^-T G). */
+void ora_element_stiffness(int dim, int order, int nq, const double* points,
+                           const double* weights, double kappa, const double* h, int convention,
+                           double* K) {
+    const int setSize = order + 1;
+    int nb = 1;
+    for (int d = 0; d < dim; ++d) nb *= setSize;
+    double nodes[16];
+    for (int i = 0; i < setSize; ++i) nodes[i] = -1.0 + 2.0 * i / order;
+    double values[3 * 16], derivs[3 * 16];
+    double* G = (double*)malloc(sizeof(double) * (size_t)(dim * nb));
+    memset(K, 0, sizeof(double) * (size_t)(nb * nb));
+    for (int q = 0; q < nq; ++q) {
+        for (int d = 0; d < dim; ++d)
+            ora_lagrange_1d(setSize, nodes, points[q * dim + d], &values[d * setSize], &derivs[d * setSize]);
+        tensor_gradients(dim, setSize, values, derivs, G);
+        if (convention == 1)
+            for (int d = 0; d < dim; ++d)
+                for (int a = 0; a < nb; ++a) G[d * nb + a] *= 2.0 / h[d];
+        for (int a = 0; a < nb; ++a)
+            for (int b = 0; b < nb; ++b) {
+                double s = 0.0;
+                for (int d = 0; d < dim; ++d) s += G[d * nb + a] * G[d * nb + b];
+                K[a * nb + b] += weights[q] * s;
+            }
+    }
+    double scale = kappa;
+    for (int d = 0; d < dim; ++d) scale *= convention == 1 ? 0.5 * h[d] : 2.0 / h[d];
+    for (int k = 0; k < nb * nb; ++k) K[k] *= scale;
+    free(G);
+}
+
+/* DoF map of a structured grid of cells[0] x cells[1] (x cells[2]) elements of the
+ * given order: nodes numbered lexicographically (x fastest), local basis index
+ * a = i0 + (p+1) i1 + (p+1)^2 i2 (first index fastest). */
+void ora_structured_dofmap(int dim, int order, const int* cells, int* dofmap) {
+    const int setSize = order + 1;
+    int nb = 1, ncells = 1;
+    int nodesPerAxis[3] = {1, 1, 1}, c[3] = {1, 1, 1};
+    for (int d = 0; d < dim; ++d) {
+        nb *= setSize;
+        ncells *= cells[d];
+        nodesPerAxis[d] = order * cells[d] + 1;
+        c[d] = cells[d];
+    }
+    for (int e = 0; e < ncells; ++e) {
+        const int ex = e % c[0], ey = (e / c[0]) % c[1], ez = e / (c[0] * c[1]);
+        for (int a = 0; a < nb; ++a) {
+            const int i0 = a % setSize, i1 = (a / setSize) % setSize, i2 = a / (setSize * setSize);
+            int g = order * ex + i0;
+            if (dim >= 2) g += nodesPerAxis[0] * (order * ey + i1);
+            if (dim >= 3) g += nodesPerAxis[0] * nodesPerAxis[1] * (order * ez + i2);
+            dofmap[(long)e * nb + a] = g;
+        }
+    }
+}
+
+static int cmp_int(const void* a, const void* b) {
+    const int x = *(const int*)a, y = *(const int*)b;
+    return (x > y) - (x < y);
+}
+
+/* Sparsity pattern = per row, the sorted unique union of the DoFs of every cell
+ * that contains the row's DoF (fem/packages/graph/src/Assembler.cpp:55-175).
+ * Returns nnz; fills rowptr/col when col is non-NULL (rowptr must then hold the
+ * counts from a first call with col == NULL ... simplest: always recomputes). */
+long ora_csr_pattern(long ncells, int nb, const int* dofmap, int ndofs, int* rowptr, int* col) {
+    /* bucket (row, col) pairs per row */
+    long* count = (long*)calloc((size_t)ndofs + 1, sizeof(long));
+    for (long e = 0; e < ncells; ++e)
+        for (int a = 0; a < nb; ++a) count[dofmap[e * nb + a] + 1] += nb;
+    for (int i = 0; i < ndofs; ++i) count[i + 1] += count[i];
+    int* buf = (int*)malloc(sizeof(int) * (size_t)count[ndofs]);
+    long* fill = (long*)malloc(sizeof(long) * (size_t)ndofs);
+    for (int i = 0; i < ndofs; ++i) fill[i] = count[i];
+    for (long e = 0; e < ncells; ++e)
+        for (int a = 0; a < nb; ++a) {
+            const int row = dofmap[e * nb + a];
+            for (int b = 0; b < nb; ++b) buf[fill[row]++] = dofmap[e * nb + b];
+        }
+    long nnz = 0;
+    if (rowptr) rowptr[0] = 0;
+    for (int i = 0; i < ndofs; ++i) {
+        int* seg = buf + count[i];
+        const long len = count[i + 1] - count[i];
+        qsort(seg, (size_t)len, sizeof(int), cmp_int);
+        long u = 0;
+        for (long k = 0; k < len; ++k)
+            if (k == 0 || seg[k] != seg[k - 1]) {
+                if (col) col[nnz + u] = seg[k];
+                ++u;
+            }
+        nnz += u;
+        if (rowptr) rowptr[i + 1] = (int)nnz;
+    }
+    free(count); free(buf); free(fill);
+    return nnz;
+}
+
+/* Assembler::addContribution (fem/packages/graph/impl/Assembler_impl.hpp:156-194):
+ * for every local (i, j), lower_bound the global column inside the global row and
+ * add K_e[i*nb + j].  Returns 0, or 1 when an entry is missing from the pattern. */
+int ora_assemble(long ncells, int nb, const int* dofmap, const double* Ke, const int* rowptr,
+                 const int* col, double* val) {
+    for (long e = 0; e < ncells; ++e) {
+        const int* dofs = dofmap + e * nb;
+        const double* K = Ke + e * (long)nb * nb;
+        for (int i = 0; i < nb; ++i) {
+            const int row = dofs[i];
+            for (int j = 0; j < nb; ++j) {
+                int lo = rowptr[row], hi = rowptr[row + 1];
+                const int target = dofs[j];
+                while (lo < hi) {
+                    const int mid = lo + (hi - lo) / 2;
+                    if (col[mid] < target) lo = mid + 1; else hi = mid;
+                }
+                if (lo == rowptr[row + 1] || col[lo] != target) return 1;
+                val[lo] += K[i * nb + j];
+            }
+        }
+    }
+    return 0;
+}
+
+/* Per-element adjoint gradient dJ/dkappa_e = -lambda_e^T (dK_e/dkappa_e) u_e with
+ * K_e linear in kappa_e, i.e. -lambda_e^T K_e(kappa=1) u_e. */
+void ora_element_gradient(long ncells, int nb, const int* dofmap, const double* Kunit,
+                          const double* lambda, const double* u, double* grad) {
+    for (long e = 0; e < ncells; ++e) {
+        const int* dofs = dofmap + e * nb;
+        double s = 0.0;
+        for (int i = 0; i < nb; ++i) {
+            double t = 0.0;
+            for (int j = 0; j < nb; ++j) t += Kunit[i * nb + j] * u[dofs[j]];
+            s += lambda[dofs[i]] * t;
+        }
+        grad[e] = -s;
+    }
+}
+
+/* Symmetric elimination of homogeneous Dirichlet DoFs (fem/test/test_1d.cpp:291-313):
+ * boundary rows and columns zeroed (structural zeros kept), diagonal 1, rhs 0. */
+void ora_dirichlet_eliminate(int n, const int* rowptr, const int* col, double* val,
+                             const uint8_t* isBoundary, double* rhs) {
+    for (int i = 0; i < n; ++i)
+        for (int k = rowptr[i]; k < rowptr[i + 1]; ++k)
+            if (isBoundary[i] || isBoundary[col[k]]) val[k] = (i == col[k]) ? 1.0 : 0.0;
+    if (rhs)
+        for (int i = 0; i < n; ++i)
+            if (isBoundary[i]) rhs[i] = 0.0;
+}
+
+/* Cut-cell quadrature of fem/packages/numeric/inc/KDTreeQuadraturePointFactory.hpp:67-173
+ * for a sphere domain (inside: |x - center|^2 < radius^2), depth range [0, depth],
+ * a (order)^dim Gauss-Legendre base rule per tree node.  Keep rule (:156-160):
+ * keep = (homogeneous && inside) || depth == max || (depth == min && homogeneous);
+ * descend while not homogeneous.  points: parametric coordinates in [-1,1]^dim,
+ * weights scaled by the node's Jacobian determinant (length/2)^dim, scales:
+ * 1 inside, alpha outside (ScaledMultiMaterialIntegrand_impl.hpp:33-60 with the
+ * material map {(0, alpha), (1, 1)}).  Returns the number of points, or -1 when
+ * maxPoints is exceeded. */
+static int cut_visit(int dim, int depth, int maxDepth, const double* base, double length,
+                     int order, const double* gn, const double* gw, const double* center,
+                     double radius, const double* cellOrigin, const double* cellSize,
+                     int maxPoints, int count, double* points, double* weights, double* scales,
+                     double alpha) {
+    int nbase = 1;
+    for (int d = 0; d < dim; ++d) nbase *= order;
+    if (count + nbase > maxPoints) return -1;
+    int inside0 = -1, homogeneous = 1;
+    const double jac = pow(0.5 * length, dim);
+    for (int q = 0; q < nbase; ++q) {
+        int rest = q;
+        double w = 1.0, r2 = 0.0;
+        for (int d = 0; d < dim; ++d) {
+            const int i = rest % order;
+            rest /= order;
+            const double xi = base[d] + 0.5 * length * (gn[i] + 1.0);
+            points[(long)(count + q) * dim + d] = xi;
+            w *= gw[i];
+            const double x = cellOrigin[d] + 0.5 * (xi + 1.0) * cellSize[d];
+            r2 += (x - center[d]) * (x - center[d]);
+        }
+        weights[count + q] = w * jac;
+        const int inside = r2 < radius * radius;
+        scales[count + q] = inside ? 1.0 : alpha;
+        if (inside0 < 0) inside0 = inside;
+        else if (inside != inside0) homogeneous = 0;
+    }
+    int keep = homogeneous && inside0;
+    keep |= depth == maxDepth;
+    keep |= depth == 0 && homogeneous;
+    if (keep) count += nbase;
+    if (homogeneous || depth == maxDepth) return count;
+    const double half = 0.5 * length;
+    const int children = 1 << dim;
+    for (int c = 0; c < children; ++c) {
+        double childBase[3];
+        for (int d = 0; d < dim; ++d) childBase[d] = base[d] + ((c >> d) & 1) * half;
+        count = cut_visit(dim, depth + 1, maxDepth, childBase, half, order, gn, gw, center, radius,
+                          cellOrigin, cellSize, maxPoints, count, points, weights, scales, alpha);
+        if (count < 0) return -1;
+    }
+    return count;
+}
+
+int ora_cut_cell_points(int dim, int depth, int order, const double* center, double radius,
+                        const double* cellOrigin, const double* cellSize, int maxPoints,
+                        double* points, double* weights, double* scales, double alpha) {
+    double gn[16], gw[16];
+    if (ora_gauss_legendre(order, gn, gw)) return -1;
+    const double base[3] = {-1.0, -1.0, -1.0};
+    return cut_visit(dim, 0, depth, base, 2.0, order, gn, gw, center, radius, cellOrigin, cellSize,
+                     maxPoints, 0, points, weights, scales, alpha);
+}
