@@ -6,13 +6,15 @@ kappa = exp(smoothed unit-variance Gaussian field), RHS uniform [-1, 1] (seed 0)
 homogeneous Dirichlet boundary by symmetric elimination, Jacobi-preconditioned CG
 to ||r||/||b|| <= 1e-10 from x = 0.  Matrix assembled on the GPU (untimed set-up).
 
-Metric: PCG time-to-1e-10 in seconds (lower is better); value = the headline
-solver's device time per solve with inputs resident in HBM (inputs are larger than
-L2, so no flush is needed); e2e = the same through the public API with host
-buffers (H2D of CSR + RHS from pinned memory and D2H of the solution inside the
-timed region).  The line also carries the FP64 solver's time, the roofline of the
-dominant kernel (CSR SpMV, timed live with CUDA events) and of the whole PCG
-iteration, and the reference's threaded CPU solver on a bounded sample.
+Metric: PCG time-to-1e-10 in seconds (lower is better).  value = the headline
+mixed-precision solver (FP32 inner CG with FP64 reliable updates, stopping on the
+true FP64 residual) per solve with inputs resident in HBM (inputs are larger than
+L2, so no flush is needed); the plain FP64 PCG (the drop-in) is timed beside it.
+e2e = the mixed solve through the public API with host buffers (H2D of CSR + RHS
+from pinned memory, operator set-up, solve, D2H of the solution, all timed).
+roofline = the headline's dominant kernel (the FP32 CSR SpMV) timed live with CUDA
+events; the FP64 SpMV and whole-iteration rooflines are reported beside it, and
+the reference's threaded CPU solver is timed on the same system.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cie_b200|reference]
 """
@@ -33,6 +35,8 @@ sys.path.insert(0, ROOT)
 WORKLOAD = {"workload": "poisson3d_q1_128^3_lognormal_kappa_jacobi_pcg_rel1e-10", "cells": [128, 128, 128],
             "dofs": 2146689, "nnz": 57066625, "seed": 0, "tolerance": 1e-10, "index": "int32",
             "l2": "inputs larger than L2 (no flush needed)"}
+# Smaller case of the same workload for ncu captures (matrix 290 MB, still above L2).
+PROFILE_CELLS = [96, 96, 96]
 METRIC = "PCG time-to-1e-10 (s), 3D Q1 128^3 Poisson"
 
 
@@ -100,9 +104,9 @@ def cpu_problem_arrays(prob):
 
 
 def cpu_reference_sample(rp, col, val, b, full_iterations, budget_s=15.0, threads=None):
-    """The reference's threaded FP64 CG (oracle/_ref) on a bounded number of
-    iterations of the same system; the per-iteration time is scaled to the
-    iteration count of a complete solve."""
+    """The reference's threaded FP64 CG (oracle/_ref) on the same system: a complete
+    solve when it fits the budget, else a bounded number of iterations whose
+    per-iteration time is scaled to the iteration count of a complete solve."""
     from oracle.oracle import Reference, reference_available
     if not reference_available():
         return None
@@ -110,61 +114,58 @@ def cpu_reference_sample(rp, col, val, b, full_iterations, budget_s=15.0, thread
     try:
         _, _, err, t_probe = ref.pcg(rp, col, val, b, maxit=2, reltol=1e-10)
         per_it = max(t_probe / 3.0, 1e-6)
-        m = int(max(3, min(full_iterations, budget_s / per_it - 1)))
+        if per_it * (full_iterations + 1) <= budget_s:
+            _, stats, err, t = ref.pcg(rp, col, val, b, maxit=20000, reltol=1e-10)
+            return {"value": t, "unit": "s", "cores": ref.threads, "kind": "reference",
+                    "sample": "one complete solve to 1e-10 (%d iterations, true stop) with the reference's "
+                              "ConjugateGradients<DefaultSpace<double>> + CSROperator + DiagonalOperator compiled "
+                              "from its own sources (oracle/_ref), same system" % int(stats[0]),
+                    "iterations": int(stats[0])}
+        m = int(max(3, budget_s / per_it - 1))
         _, stats, err, t = ref.pcg(rp, col, val, b, maxit=m, reltol=1e-10)
         per_it = t / (stats[0] + 1)
-        est = per_it * (full_iterations + 1)
-        return {"value": est, "unit": "s", "cores": ref.threads, "kind": "reference",
-                "sample": "%d CG iterations of the reference's ConjugateGradients<DefaultSpace<double>> + "
-                          "CSROperator + DiagonalOperator (oracle/_ref) on the same system: %.3f s, i.e. %.2f ms per "
-                          "iteration, scaled to the %d iterations of a complete solve"
-                          % (stats[0] + 1, t, 1e3 * per_it, full_iterations + 1),
-                "seconds_per_iteration": per_it}
+        return {"value": per_it * (full_iterations + 1), "unit": "s", "cores": ref.threads, "kind": "reference",
+                "sample": "%d CG iterations of the reference's CPU solver (oracle/_ref) on the same system: "
+                          "%.3f s, %.2f ms per iteration, scaled to the %d iterations of a complete solve"
+                          % (stats[0] + 1, t, 1e3 * per_it, full_iterations + 1)}
     finally:
         ref.close()
 
 
 def run_reference_arm(args):
+    """The reference's own threaded FP64 CPU solver (oracle/_ref: ConjugateGradients<
+    DefaultSpace<double>> + CSROperator + DiagonalOperator over mp::ThreadPoolBase with
+    every host thread) on the same seeded system; each step is a complete solve."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    import torch  # noqa: F401  (only for problem construction on the GPU, not timed)
     from cie_b200.fem import make_poisson
     from cie_b200.linalg import CUDASpace
-    space = CUDASpace()
+    space = CUDASpace()  # builds the identical system (GPU assembly, untimed)
     prob = make_poisson(space, 3, 1, WORKLOAD["cells"], seed=WORKLOAD["seed"])
     rp, col, val, b = cpu_problem_arrays(prob)
     del prob, space
     from oracle.oracle import Reference
     ref = Reference()
-    full = FULL_ITERATIONS_FP64
-    times = []
-    per_its = []
-    budget = max(2.0, 150.0 / max(1, args.steps + args.warmup))
-    _, _, _, t_probe = ref.pcg(rp, col, val, b, maxit=2, reltol=1e-10)
-    m = int(max(3, min(full, budget / max(t_probe / 3.0, 1e-6) - 1)))
+    times, its = [], []
     for step in range(args.warmup + args.steps):
-        _, stats, err, t = ref.pcg(rp, col, val, b, maxit=m, reltol=1e-10)
+        _, stats, err, t = ref.pcg(rp, col, val, b, maxit=20000, reltol=WORKLOAD["tolerance"])
+        if err:
+            raise RuntimeError(err)
         if step >= args.warmup:
-            per_its.append(t / (stats[0] + 1))
+            times.append(t)
+            its.append(int(stats[0]))
     ref.close()
-    per_it = statistics.median(per_its)
-    value = per_it * (full + 1)
+    value = statistics.median(times)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * value, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-            "config": dict(WORKLOAD, parallelism="replicas"),
+            "config": dict(WORKLOAD, parallelism="replicas", iterations=its[-1]),
             "cpu_baseline": {"value": value, "unit": "s", "cores": ref.threads, "kind": "reference",
-                             "sample": "each step: %d CG iterations of the reference's CPU solver (oracle/_ref), "
-                                       "per-iteration time scaled to the %d iterations of a complete solve"
-                                       % (m + 1, full + 1)},
+                             "sample": "each step: one complete solve to 1e-10 (%d iterations) with the reference's "
+                                       "CPU solver compiled from its own sources (oracle/_ref)" % its[-1]},
             "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
-
-
-# Iterations of the FP64 Jacobi-PCG on this seeded system (GPU solver; the compiled
-# reference agrees within +-2 on the parity cases); used to scale CPU samples.
-FULL_ITERATIONS_FP64 = 1000
 
 
 def main():
@@ -175,6 +176,8 @@ def main():
     ap.add_argument("--impl", default="cie_b200", choices=["cie_b200", "reference"])
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="ncu target: 96^3 case, solves only (no e2e, no CPU baseline, no clock sampling)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -186,8 +189,8 @@ def main():
     import torch.distributed as dist
     from cie_b200 import _lib
     from cie_b200.fem import make_poisson
-    from cie_b200.linalg import (CUDASpace, CSRMatrix, CSROperator, ConjugateGradients, Statistics,
-                                 launch_count, makeDiagonalOperator)
+    from cie_b200.linalg import (CUDASpace, CSRMatrix, CSROperator, ConjugateGradients, MixedPrecisionCG,
+                                 Statistics, launch_count, makeDiagonalOperator)
 
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
@@ -200,65 +203,89 @@ def main():
         torch.cuda.synchronize()
 
     space = CUDASpace()
-    prob = make_poisson(space, 3, 1, WORKLOAD["cells"], seed=WORKLOAD["seed"])
+    cells = PROFILE_CELLS if args.profile else WORKLOAD["cells"]
+    prob = make_poisson(space, 3, 1, cells, seed=WORKLOAD["seed"])
     n, nnz = prob.mesh.ndofs, prob.matrix.nnz()
     A = CSROperator(prob.matrix, space)
     D = makeDiagonalOperator(prob.matrix, space, csr_handle=A.csr)
     settings = Statistics(20000, 0.0, WORKLOAD["tolerance"])
     cg = ConjugateGradients(A, space, D, settings)
-    x = torch.zeros_like(prob.rhs)
+    mixed = MixedPrecisionCG(A, D, settings, mode=0, delta=0.1)
+    x64 = torch.zeros_like(prob.rhs)
+    xmx = torch.zeros_like(prob.rhs)
     stream = torch.cuda.ExternalStream(space.stream.cuda_stream)
 
-    def solve():
-        x.zero_()
-        cg.product(0.0, prob.rhs, 1.0, x)
+    def solve_fp64():
+        x64.zero_()
+        cg.product(0.0, prob.rhs, 1.0, x64)
+
+    def solve_mixed():
+        xmx.zero_()
+        mixed.product(0.0, prob.rhs, 1.0, xmx)
 
     for _ in range(args.warmup):
-        solve()
-    iters = cg.getStats().iterationCount
+        solve_mixed()
+        solve_fp64()
+    it64 = cg.getStats().iterationCount
+    mst = mixed.getStats()
+    if args.profile:
+        for _ in range(args.steps):
+            solve_mixed()
+            solve_fp64()
+        torch.cuda.synchronize()
+        print(json.dumps({"profile": True, "cells": cells, "fp64_iterations": it64,
+                          "mixed_inner": mst.innerIterations, "mixed_refinements": mst.refinements}), flush=True)
+        return
     hbm, peak_kind = peaks()
+
+    def timed(fn, reps):
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        barrier()
+        return e0.elapsed_time(e1) / 1e3 / reps
+
     sampler = ClockSampler(local)
     sampler.start()
     launches0 = launch_count()
-    barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        solve()
-    e1.record(stream)
-    barrier()
-    t_solve = e0.elapsed_time(e1) / 1e3 / args.steps
+    t_mixed = timed(solve_mixed, args.steps)
+    t_fp64 = timed(solve_fp64, args.steps)
     launches = launch_count() - launches0
 
-    # dominant kernel: the CSR row pass (SpMV), timed live with CUDA events
-    y = torch.empty_like(prob.rhs)
-    spmv_reps = 20
-    for _ in range(3):
-        A.product(0.0, x, 1.0, y)
-    torch.cuda.synchronize()
-    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    s0.record(stream)
-    for _ in range(spmv_reps):
-        A.product(0.0, x, 1.0, y)
-    s1.record(stream)
-    torch.cuda.synchronize()
-    t_spmv = s0.elapsed_time(s1) / 1e3 / spmv_reps
+    # dominant kernels, timed live with CUDA events on the launching stream
+    lib = _lib.load()
+    from cie_b200.linalg import _ptr
+    y64 = torch.empty_like(prob.rhs)
+    x32 = xmx.float()
+    y32 = torch.empty_like(x32)
+    reps = 20
+    t_spmv32 = timed(lambda: [lib.ciecu_mixed_apply_f32(mixed._solver, _ptr(x32), _ptr(y32)) for _ in range(reps)],
+                     1) / reps
+    t_spmv64 = timed(lambda: [lib.ciecu_csr_spmv_f64(A.csr.handle, 0.0, _ptr(x64), 1.0, _ptr(y64))
+                              for _ in range(reps)], 1) / reps
     clocks = sampler.stop()
 
-    t_tensor = torch.tensor([t_solve, t_spmv], device="cuda", dtype=torch.float64)
+    t_tensor = torch.tensor([t_mixed, t_fp64, t_spmv32, t_spmv64], device="cuda", dtype=torch.float64)
     if world > 1:
         dist.all_reduce(t_tensor, op=dist.ReduceOp.MAX)
-    t_solve, t_spmv = t_tensor.tolist()
+    t_mixed, t_fp64, t_spmv32, t_spmv64 = t_tensor.tolist()
+    info = mixed.info()
 
-    spmv_bytes = 12 * nnz + 4 * (n + 1) + 16 * n
-    iter_bytes = 12 * nnz + 4 * (n + 1) + 104 * n
-    solve_bytes = (iters + 1) * iter_bytes + (12 * nnz + 4 * (n + 1) + 24 * n)
-    spmv_gbs = spmv_bytes / t_spmv / 1e9
-    iter_gbs = solve_bytes / t_solve / 1e9
+    idx_bytes = 2 if info["compressed_columns"] else 4
+    spmv32_bytes = (4 + idx_bytes) * nnz + 4 * (n + 1) + 8 * n
+    spmv64_bytes = 12 * nnz + 4 * (n + 1) + 16 * n
+    iter64_bytes = 12 * nnz + 4 * (n + 1) + 104 * n
+    inner_bytes = (4 + idx_bytes) * nnz + 4 * (n + 1) + 52 * n
+    fp64_solve_bytes = (it64 + 1) * iter64_bytes + (12 * nnz + 4 * (n + 1) + 24 * n)
+    refine_bytes = 12 * nnz + 4 * (n + 1) + 28 * n  # FP64 residual pass: x64, b read, r32 written, dinv32
+    mixed_solve_bytes = mst.innerIterations * inner_bytes + (mst.refinements + 1) * refine_bytes
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
-        traffic = json.load(open(tpath)).get("spmv_f64_poisson3d_q1_128", None)
+        traffic = json.load(open(tpath)).get("mixed_spmv_f32_idx16_poisson3d_q1_128", None)
 
     # end to end through the public API with host buffers
     rp_h, col_h, val_h = [t.cpu().pin_memory() for t in (prob.matrix.rowExtents, prob.matrix.columnIndices,
@@ -273,45 +300,65 @@ def main():
                       val_h.to("cuda", non_blocking=True))
         b = rhs_h.to("cuda", non_blocking=True)
         A2 = CSROperator(m, space)
-        cg2 = ConjugateGradients(A2, space, makeDiagonalOperator(m, space, csr_handle=A2.csr), settings)
+        D2 = makeDiagonalOperator(m, space, csr_handle=A2.csr)
+        M2 = MixedPrecisionCG(A2, D2, settings, mode=0, delta=0.1)
         xe = torch.zeros(n, dtype=torch.float64, device="cuda")
-        cg2.product(0.0, b, 1.0, xe)
+        M2.product(0.0, b, 1.0, xe)
         sol_h.copy_(xe, non_blocking=True)
         torch.cuda.synchronize()
         if step >= 2:
             e2e_times.append(time.perf_counter() - t0)
-        del cg2, A2, m
+        del M2, D2, A2, m
     e2e = statistics.median(e2e_times)
     h2d = 4 * (n + 1) + 12 * nnz + 8 * n
     d2h = 8 * n
 
-    # parity of the timed solve: true residual in FP64 on the GPU
-    r = prob.rhs.clone()
-    A.product(1.0, x, -1.0, r)
-    true_rel = float(torch.linalg.norm(r) / torch.linalg.norm(prob.rhs))
+    # accuracy of the timed solves: true FP64 residuals and agreement of the two solvers
+    def true_rel(x):
+        r = prob.rhs.clone()
+        A.product(1.0, x, -1.0, r)
+        return float(torch.linalg.norm(r) / torch.linalg.norm(prob.rhs))
+    rel_mixed, rel_fp64 = true_rel(xmx), true_rel(x64)
+    agree = float(torch.linalg.norm(xmx - x64) / torch.linalg.norm(x64))
 
     cpu = None
     if rank == 0 and not args.no_cpu:
         rp, col, val, bh = cpu_problem_arrays(prob)
-        cpu = cpu_reference_sample(rp, col, val, bh, iters, budget_s=args.cpu_budget)
+        cpu = cpu_reference_sample(rp, col, val, bh, it64, budget_s=args.cpu_budget)
 
     if rank == 0:
+        g32 = spmv32_bytes / t_spmv32 / 1e9
         line = {
-            "metric": METRIC, "value": t_solve, "unit": "s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * t_solve, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded mt19937_64 RHS and kappa field)",
+            "metric": METRIC, "value": t_mixed, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t_mixed, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 inner / f64 refinement",
+            "data": "synthetic (seeded mt19937_64 RHS and kappa field)",
             "config": dict(WORKLOAD, parallelism="replicas" if world > 1 else "single_gpu",
-                           solver="fp64 jacobi-pcg", iterations=iters, true_relative_residual=true_rel),
-            "fp64": {"seconds": t_solve, "iterations": iters, "true_relative_residual": true_rel},
-            "roofline": {"bound": "hbm", "kernel": "csr spmv (ciecu spmv_kernel, schedule %d)" % A.csr.kernel(),
-                         "achieved": spmv_gbs, "peak": hbm, "unit": "GB/s", "frac": spmv_gbs / hbm,
-                         "peak_kind": peak_kind, "traffic": traffic, "algorithmic_bytes": spmv_bytes,
-                         "launch_ms": 1e3 * t_spmv},
-            "pcg_iteration_roofline": {"achieved": iter_gbs, "peak": hbm, "unit": "GB/s", "frac": iter_gbs / hbm,
-                                       "algorithmic_bytes_per_iteration": iter_bytes,
-                                       "us_per_iteration": 1e6 * t_solve / (iters + 1)},
+                           solver="mixed-precision jacobi-pcg, reliable updates delta=0.1",
+                           compressed_columns=info["compressed_columns"]),
+            "mixed": {"seconds": t_mixed, "inner_iterations": mst.innerIterations,
+                      "refinements": mst.refinements, "true_relative_residual": rel_mixed,
+                      "rel_diff_vs_fp64_solution": agree,
+                      "achieved_gbs": mixed_solve_bytes / t_mixed / 1e9},
+            "fp64": {"seconds": t_fp64, "iterations": it64, "true_relative_residual": rel_fp64,
+                     "achieved_gbs": fp64_solve_bytes / t_fp64 / 1e9,
+                     "us_per_iteration": 1e6 * t_fp64 / (it64 + 1)},
+            "speedup_mixed_vs_fp64": t_fp64 / t_mixed,
+            "roofline": {"bound": "hbm", "kernel": "mixed_apply_kernel (FP32 CSR SpMV, %s columns, %d lanes/row)"
+                         % ("16-bit" if info["compressed_columns"] else "int32", info["lanes_per_row"]),
+                         "achieved": g32, "peak": hbm, "unit": "GB/s", "frac": g32 / hbm, "peak_kind": peak_kind,
+                         "traffic": traffic, "algorithmic_bytes": spmv32_bytes, "launch_ms": 1e3 * t_spmv32},
+            "fp64_spmv_roofline": {"kernel": "spmv_kernel (FP64 CSR, schedule %d)" % A.csr.kernel(),
+                                   "achieved": spmv64_bytes / t_spmv64 / 1e9, "peak": hbm,
+                                   "frac": spmv64_bytes / t_spmv64 / 1e9 / hbm, "algorithmic_bytes": spmv64_bytes,
+                                   "launch_ms": 1e3 * t_spmv64},
+            "pcg_iteration_roofline": {"fp64_frac": fp64_solve_bytes / t_fp64 / 1e9 / hbm,
+                                       "mixed_frac": mixed_solve_bytes / t_mixed / 1e9 / hbm,
+                                       "fp64_bytes_per_iteration": iter64_bytes,
+                                       "mixed_inner_bytes_per_iteration": inner_bytes},
             "clocks": clocks,
-            "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "solver": "mixed"},
             "gpu_launches": int(launches),
             "cpu_baseline": cpu,
         }

@@ -2,12 +2,9 @@
 
 The CUDA kernels and the C-ABI live in libciecu.so (include/ciecu*.h); this
 package is the Python mirror of the reference's operator API on top of it.
-Importing it loads the library and fails loudly if it has not been built.
+The library is loaded on first use (cie_b200.load()); a missing build fails
+loudly -- there is no CPU fallback.
 """
-from . import _lib
+from ._lib import CiecuError, Statistics, load  # noqa: F401
 
-_lib.load()
-
-from ._lib import CiecuError, Statistics  # noqa: E402
-
-__all__ = ["CiecuError", "Statistics"]
+__all__ = ["CiecuError", "Statistics", "load"]

@@ -22,6 +22,10 @@ class Statistics(ctypes.Structure):
             self.iterationCount, self.absoluteResidual, self.relativeResidual)
 
 
+class MixedOptions(ctypes.Structure):
+    _fields_ = [("mode", c_int), ("delta", c_double), ("compressColumns", c_int)]
+
+
 class MixedStatistics(ctypes.Structure):
     _fields_ = [("iterationCount", c_int64), ("absoluteResidual", c_double), ("relativeResidual", c_double),
                 ("innerIterations", c_int64), ("refinements", c_int64), ("trueRelativeResidual", c_double)]
@@ -73,6 +77,12 @@ SIGNATURES = {
     "ciecu_pcg_destroy": (c_int, [P]),
     "ciecu_pcg_product": (c_int, [P, c_double, P, c_double, P, P]),
     "ciecu_pcg_set_graph_chunk": (c_int, [P, c_int]),
+    "ciecu_mixed_create": (c_int, [P, P, Statistics, MixedOptions, P]),
+    "ciecu_mixed_destroy": (c_int, [P]),
+    "ciecu_mixed_info": (c_int, [P, P, P]),
+    "ciecu_mixed_set_graph_chunk": (c_int, [P, c_int]),
+    "ciecu_mixed_product": (c_int, [P, c_double, P, c_double, P, P]),
+    "ciecu_mixed_apply_f32": (c_int, [P, P, P]),
     # host utilities
     "ciecu_structured_dofmap": (c_int, [c_int, c_int, P, P, P]),
     "ciecu_structured_boundary": (c_int, [c_int, c_int, P, P]),

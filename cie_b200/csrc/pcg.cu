@@ -89,6 +89,7 @@ __global__ void __launch_bounds__(csr_threads<KERNEL>())
 }
 
 // K2: x, r update; z; rr, rz; beta and the stopping test (:154-185).
+// Two elements per thread with 16-byte loads (all operands 16-byte aligned).
 template <bool PRECOND>
 __global__ void __launch_bounds__(kT) pcg_update_kernel(long n, double* __restrict__ x, double* __restrict__ r,
                                                         const double* __restrict__ p, const double* __restrict__ q,
@@ -98,8 +99,29 @@ __global__ void __launch_bounds__(kT) pcg_update_kernel(long n, double* __restri
     const double alpha = s->alpha;
     const double malpha = -alpha;
     double rr = 0.0, rz = 0.0;
+    const long pairs = n >> 1;
     const long stride = static_cast<long>(gridDim.x) * kT;
-    for (long i = static_cast<long>(blockIdx.x) * kT + threadIdx.x; i < n; i += stride) {
+    for (long j = static_cast<long>(blockIdx.x) * kT + threadIdx.x; j < pairs; j += stride) {
+        const double2 pj = reinterpret_cast<const double2*>(p)[j];
+        const double2 qj = reinterpret_cast<const double2*>(q)[j];
+        double2 xj = reinterpret_cast<const double2*>(x)[j];
+        double2 rj = reinterpret_cast<const double2*>(r)[j];
+        xj.x = fma(alpha, pj.x, xj.x);
+        xj.y = fma(alpha, pj.y, xj.y);
+        rj.x = fma(malpha, qj.x, rj.x);
+        rj.y = fma(malpha, qj.y, rj.y);
+        reinterpret_cast<double2*>(x)[j] = xj;
+        reinterpret_cast<double2*>(r)[j] = rj;
+        rr = fma(rj.x, rj.x, rr);
+        rr = fma(rj.y, rj.y, rr);
+        if (PRECOND) {
+            const double2 dj = reinterpret_cast<const double2*>(dinv)[j];
+            rz = fma(rj.x, rj.x * dj.x, rz);
+            rz = fma(rj.y, rj.y * dj.y, rz);
+        }
+    }
+    if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+        const long i = n - 1;
         x[i] = fma(alpha, p[i], x[i]);
         const double ri = fma(malpha, q[i], r[i]);
         r[i] = ri;
@@ -131,8 +153,23 @@ __global__ void __launch_bounds__(kT) pcg_direction_kernel(long n, double* __res
                                                            const double* __restrict__ dinv, const PcgScalars* s) {
     if (*reinterpret_cast<const volatile int*>(&s->done)) return;
     const double beta = s->beta;
+    const long pairs = n >> 1;
     const long stride = static_cast<long>(gridDim.x) * kT;
-    for (long i = static_cast<long>(blockIdx.x) * kT + threadIdx.x; i < n; i += stride) {
+    for (long j = static_cast<long>(blockIdx.x) * kT + threadIdx.x; j < pairs; j += stride) {
+        const double2 rj = reinterpret_cast<const double2*>(r)[j];
+        double2 pj = reinterpret_cast<const double2*>(p)[j];
+        double2 zj = rj;
+        if (PRECOND) {
+            const double2 dj = reinterpret_cast<const double2*>(dinv)[j];
+            zj.x = __dmul_rn(rj.x, dj.x);
+            zj.y = __dmul_rn(rj.y, dj.y);
+        }
+        pj.x = __dadd_rn(__dmul_rn(pj.x, beta), zj.x);
+        pj.y = __dadd_rn(__dmul_rn(pj.y, beta), zj.y);
+        reinterpret_cast<double2*>(p)[j] = pj;
+    }
+    if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+        const long i = n - 1;
         const double zi = PRECOND ? __dmul_rn(r[i], dinv[i]) : r[i];
         p[i] = __dadd_rn(__dmul_rn(p[i], beta), zi);
     }
@@ -186,7 +223,7 @@ namespace {
 int launch_iteration(ciecu_pcg_s* S, cudaStream_t st) {
     ciecu_csr_s* A = S->A;
     const int gridA = csr_grid(A, A->kernel);
-    const int gridV = grid_for(S->n, kT, 8);
+    const int gridV = grid_for((S->n + 1) / 2, kT, 8);
     const bool pre = S->dinv != nullptr;
     CIECU_TRY(with_schedule(A->kernel, [&](auto k) -> int {
         constexpr int K = decltype(k)::value;
@@ -243,6 +280,8 @@ int ciecu_pcg_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_stati
     CIECU_REQUIRE(lhs && out, "pcg_create: null matrix or output");
     CIECU_REQUIRE(lhs->valueType == CIECU_F64, "pcg_create: the FP64 solver needs an FP64 matrix");
     CIECU_REQUIRE(lhs->rows == lhs->cols, "pcg_create: the system matrix must be square");
+    CIECU_REQUIRE(reinterpret_cast<uintptr_t>(d_inverseDiagonal) % 16 == 0,
+                  "pcg_create: the inverse diagonal must be 16-byte aligned");
     auto* S = new ciecu_pcg_s();
     S->A = lhs;
     S->dinv = d_inverseDiagonal;

@@ -18,7 +18,10 @@ namespace {
 template <int KERNEL, typename T, typename V, bool MASKED>
 __global__ void __launch_bounds__(csr_threads<KERNEL>())
     spmv_kernel(CsrArgs<V> A, T inScale, const T* __restrict__ x, T outScale, T* __restrict__ y) {
-    auto op = [&](int r, T sum) { y[r] = combine(inScale, y[r], outScale, sum); };
+    auto op = [&](int r, T sum) {
+        const T old = inScale == T(0) ? T(0) : y[r];
+        y[r] = combine(inScale, old, outScale, sum);
+    };
     csr_rows<KERNEL, T, V, MASKED>(A, x, op);
 }
 

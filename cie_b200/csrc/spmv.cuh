@@ -165,9 +165,27 @@ __device__ __forceinline__ void vector_rows(const CsrArgs<V>& A, const T* __rest
         const int r = valid ? static_cast<int>(rowL) : 0;
         T sum = T(0);
         if (valid && (!MASKED || A.mask[r] < A.threshold)) {
+            // Issue the loads of UNROLL strided entries before the FMA chain so
+            // each lane keeps UNROLL value/index loads and gathers in flight.
+            constexpr int UNROLL = VS <= 4 ? 8 : 4;
             const int k1 = A.rowptr[r + 1];
-            for (int k = A.rowptr[r] + sub; k < k1; k += VS)
-                sum = fma(static_cast<T>(A.val[k]), gather<MASKED>(A, x, A.col[k]), sum);
+            int k = A.rowptr[r] + sub;
+            for (; k < k1; k += UNROLL * VS) {
+                V v[UNROLL];
+                int c[UNROLL];
+#pragma unroll
+                for (int u = 0; u < UNROLL; ++u) {
+                    const int kk = k + u * VS;
+                    const bool in = kk < k1;
+                    v[u] = in ? __ldg(A.val + kk) : V(0);
+                    c[u] = in ? __ldg(A.col + kk) : -1;
+                }
+                T xv[UNROLL];
+#pragma unroll
+                for (int u = 0; u < UNROLL; ++u) xv[u] = c[u] >= 0 ? gather<MASKED>(A, x, c[u]) : T(0);
+#pragma unroll
+                for (int u = 0; u < UNROLL; ++u) sum = fma(static_cast<T>(v[u]), xv[u], sum);
+            }
         }
 #pragma unroll
         for (int offset = VS / 2; offset > 0; offset >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, offset, VS);

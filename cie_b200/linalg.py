@@ -16,12 +16,12 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._lib import Statistics, call, CiecuError
+from ._lib import Statistics, MixedOptions, MixedStatistics, call, CiecuError
 
 __all__ = [
     "CUDASpace", "CSRMatrix", "LinearOperator", "CSROperator", "MaskedCSROperator", "DiagonalOperator",
     "makeDiagonalOperator", "JacobiOperator", "MaskedIdentityOperator", "NestedProductOperator",
-    "ChebyshevOperator", "ConjugateGradients", "Statistics", "CiecuError", "launch_count",
+    "ChebyshevOperator", "ConjugateGradients", "MixedPrecisionCG", "Statistics", "CiecuError", "launch_count",
 ]
 
 
@@ -527,3 +527,63 @@ class ConjugateGradients(LinearOperator):
             sp.scale(out, inScale)
             sp.add(out, solution, outScale)
         self._stats = stats
+
+
+class MixedPrecisionCG(LinearOperator):
+    """FP32-inner Jacobi-PCG with FP64 refinement (ciecu_mixed_*): the FP32 matrix
+    copy (16-bit column offsets where the bandwidth allows), FP32 vectors with FP64
+    dot accumulators, FP64 residual r = b - A x and FP64 solution.  mode 0 =
+    reliable updates (delta = replacement trigger), mode 1 = restarted iterative
+    refinement (delta = inner tolerance).  Stops on the true FP64 residual."""
+
+    def __init__(self, lhs, inverseDiagonal, settings=None, mode=0, delta=None, compressColumns=True):
+        if type(lhs) is not CSROperator or lhs.space._sfx != "f64":
+            raise CiecuError(1, "MixedPrecisionCG needs an FP64 CSROperator")
+        self.lhs = lhs
+        self.space = lhs.space
+        self.inverseDiagonal = inverseDiagonal
+        self.settings = settings if settings is not None else Statistics(5000, 0.0, 1e-10)
+        delta = (0.1 if mode == 0 else 1e-4) if delta is None else float(delta)
+        self.options = MixedOptions(int(mode), delta, int(bool(compressColumns)))
+        h = ctypes.c_void_p()
+        self.space.enter()
+        call("ciecu_mixed_create", lhs.csr.handle, _ptr(inverseDiagonal.inverseDiagonal), self.settings, self.options,
+             ctypes.byref(h))
+        self._solver = h
+        self._stats = None
+
+    def __del__(self):
+        try:
+            if getattr(self, "_solver", None):
+                _lib.load().ciecu_mixed_destroy(self._solver)
+                self._solver = None
+        except Exception:
+            pass
+
+    def info(self):
+        c, v = ctypes.c_int(), ctypes.c_int()
+        call("ciecu_mixed_info", self._solver, ctypes.byref(c), ctypes.byref(v))
+        return {"compressed_columns": bool(c.value), "lanes_per_row": v.value}
+
+    def set_graph_chunk(self, iterations):
+        call("ciecu_mixed_set_graph_chunk", self._solver, int(iterations))
+
+    def apply_inner(self, in32, out32):
+        """out32 = A32 in32 with the solver's FP32 inner operator."""
+        self.space.enter()
+        call("ciecu_mixed_apply_f32", self._solver, _ptr(in32), _ptr(out32))
+        self.space.leave()
+
+    def getStats(self):
+        return self._stats
+
+    def product(self, inScale, in_, outScale, out):
+        self.space._check(in_, out)
+        stats = MixedStatistics()
+        self.space.enter()
+        try:
+            call("ciecu_mixed_product", self._solver, float(inScale), _ptr(in_), float(outScale), _ptr(out),
+                 ctypes.byref(stats))
+        finally:
+            self._stats = stats
+            self.space.leave()

@@ -1,0 +1,60 @@
+/*
+ * ciecu mixed precision: FP32-inner Jacobi-PCG with FP64 refinement.
+ * No counterpart in the reference, which solves in one precision
+ * (ConjugateGradients<DefaultSpace<float|double>>, ConjugateGradients.cpp:10-17);
+ * the settings, stopping rule and output combination follow
+ * ConjugateGradients_impl.hpp:49-201, with the stop decided on the TRUE FP64
+ * residual ||b - A x|| of the FP64 matrix.
+ */
+#ifndef CIECU_MIXED_H
+#define CIECU_MIXED_H
+
+#include "ciecu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ciecu_mixed_s* ciecu_mixed;
+
+typedef struct ciecu_mixed_options {
+    /* 0: reliable updates (residual replacement keeping the search direction);
+     * 1: classic iterative refinement (inner CG restarted after each correction). */
+    int mode;
+    /* mode 0: replace the residual when the FP32 residual norm fell below
+     *         delta * its maximum since the last replacement (e.g. 0.1);
+     * mode 1: inner relative tolerance of each correction solve (e.g. 1e-4). */
+    double delta;
+    /* 1: store column indices as 16-bit offsets from the row when the matrix
+     * bandwidth is below 2^15 (checked; int32 otherwise). */
+    int compressColumns;
+} ciecu_mixed_options;
+
+typedef struct ciecu_mixed_statistics {
+    int64_t iterationCount;       /* FP32 inner iterations (FP32 SpMVs) */
+    double absoluteResidual;      /* ||b - A64 x64|| at the last refinement */
+    double relativeResidual;      /* ... / ||b - A64 x0|| */
+    int64_t innerIterations;      /* = iterationCount */
+    int64_t refinements;          /* FP64 residual recomputations */
+    double trueRelativeResidual;  /* = relativeResidual */
+} ciecu_mixed_statistics;
+
+/* Builds the FP32 value copy, the (16-bit or int32) column copy and the FP32
+ * inverse diagonal from the FP64 matrix and its inverse diagonal (both device).
+ * settings: iteration limit (FP32 inner iterations) and tolerances. */
+int ciecu_mixed_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_statistics settings,
+                       ciecu_mixed_options options, ciecu_mixed* out);
+int ciecu_mixed_destroy(ciecu_mixed solver);
+int ciecu_mixed_info(ciecu_mixed solver, int* compressedColumns, int* lanesPerRow);
+int ciecu_mixed_set_graph_chunk(ciecu_mixed solver, int iterations);
+/* d_out = A32 d_in: the solver's FP32 inner operator (FP32 values, 16-bit or
+ * int32 columns) on its own, e.g. to time it. */
+int ciecu_mixed_apply_f32(ciecu_mixed solver, const float* d_in, float* d_out);
+/* out = inScale*out + outScale*x, x the refined solution (initial guess = out). */
+int ciecu_mixed_product(ciecu_mixed solver, double inScale, const double* d_in, double outScale, double* d_out,
+                        ciecu_mixed_statistics* h_stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CIECU_MIXED_H */

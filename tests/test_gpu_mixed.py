@@ -1,0 +1,105 @@
+"""GPU parity of the mixed-precision (FP32-inner, FP64-refined) PCG against the
+reference's compiled FP64 CPU solver: at ||r||/||b|| <= 1e-10 (the TRUE FP64
+residual) the solution is within 1e-9 relative of the FP64 oracle's."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+from tests.test_gpu_linalg import dev, host, matrix  # noqa: E402
+from tests.test_gpu_pcg import true_residual  # noqa: E402
+
+
+@pytest.fixture(scope="module")
+def space():
+    from cie_b200.linalg import CUDASpace
+    return CUDASpace()
+
+
+def mixed_solve(space, m, b, mode=0, delta=None, compress=True, x0=None, settings=None):
+    from cie_b200.linalg import CSROperator, MixedPrecisionCG, Statistics, makeDiagonalOperator
+    A = CSROperator(m, space)
+    D = makeDiagonalOperator(m, space, csr_handle=A.csr)
+    solver = MixedPrecisionCG(A, D, settings or Statistics(20000, 0.0, 1e-10), mode=mode, delta=delta,
+                              compressColumns=compress)
+    x = dev(np.zeros(len(b)) if x0 is None else x0)
+    solver.product(0.0, dev(b), 1.0, x)
+    return host(x), solver.getStats(), solver.info()
+
+
+@pytest.mark.parametrize("mode,compress", [(0, True), (0, False), (1, True)])
+def test_mixed_3d_lognormal_vs_reference(space, reference, mode, compress):
+    from cie_b200.fem import make_poisson
+    prob = make_poisson(space, 3, 1, [40, 40, 40], seed=2)
+    rp, col, val = prob.host_csr()
+    b = host(prob.rhs)
+    x, st, info = mixed_solve(space, prob.matrix, b, mode=mode, compress=compress)
+    xr, sr, err, _ = reference.pcg(rp, col, val, b, maxit=20000, abstol=0.0, reltol=1e-10)
+    rel = np.linalg.norm(x - xr) / np.linalg.norm(xr)
+    tr = true_residual(rp, col, val, x, b)
+    print("mixed mode %d compress %s: %d inner iterations, %d refinements (FP64 reference: %d), "
+          "|x-x_ref|/|x_ref| = %.3e, true rel residual %.3e, %s"
+          % (mode, compress, st.innerIterations, st.refinements, sr[0], rel, tr, info))
+    assert info["compressed_columns"] == compress
+    assert st.trueRelativeResidual < 1e-10 and tr <= 1.01e-10
+    assert rel <= 1e-9
+    if mode == 0:
+        assert st.innerIterations <= 1.2 * sr[0] + 10
+
+
+def test_mixed_cfg1_vs_reference(space, reference):
+    from cie_b200.fem import make_poisson
+    prob = make_poisson(space, 2, 1, [256, 256], seed=0, kappa="one")
+    rp, col, val = prob.host_csr()
+    b = host(prob.rhs)
+    x, st, info = mixed_solve(space, prob.matrix, b)
+    xr, sr, _, _ = reference.pcg(rp, col, val, b, maxit=5000, abstol=0.0, reltol=1e-10)
+    rel = np.linalg.norm(x - xr) / np.linalg.norm(xr)
+    print("cfg1 mixed: %d inner it, %d refinements, ref %d it, rel %.3e" % (st.innerIterations, st.refinements,
+                                                                             sr[0], rel))
+    assert rel <= 1e-9 and true_residual(rp, col, val, x, b) <= 1.01e-10
+
+
+def test_mixed_wide_bandwidth_falls_back_to_int32(space, reference):
+    # a symmetric matrix coupling row i with row i + 40000: 16-bit offsets impossible
+    n = 50000
+    rows, cols, vals = [], [], []
+    for i in range(n):
+        rows.append(i); cols.append(i); vals.append(4.0)
+        if i + 40000 < n:
+            rows += [i, i + 40000]; cols += [i + 40000, i]; vals += [-1.0, -1.0]
+        if i + 1 < n:
+            rows += [i, i + 1]; cols += [i + 1, i]; vals += [-1.0, -1.0]
+    order = np.lexsort((cols, rows))
+    rows, cols, vals = np.array(rows)[order], np.array(cols, np.int32)[order], np.array(vals)[order]
+    rp = np.zeros(n + 1, np.int32)
+    np.add.at(rp, rows + 1, 1)
+    rp = np.cumsum(rp).astype(np.int32)
+    b = np.random.default_rng(3).uniform(-1, 1, n)
+    x, st, info = mixed_solve(space, matrix(rp, cols, vals, n), b)
+    assert info["compressed_columns"] is False
+    xr, sr, _, _ = reference.pcg(rp, cols, vals, b, maxit=5000, abstol=0.0, reltol=1e-10)
+    assert np.linalg.norm(x - xr) <= 1e-9 * np.linalg.norm(xr)
+
+
+def test_mixed_settings_and_output_scales(space):
+    from cie_b200.fem import make_poisson
+    from cie_b200.linalg import Statistics
+    prob = make_poisson(space, 2, 1, [48, 48], seed=4)
+    b = host(prob.rhs)
+    rng = np.random.default_rng(5)
+    y0 = rng.uniform(-1, 1, len(b))
+    x_full, st, _ = mixed_solve(space, prob.matrix, b)
+    from cie_b200.linalg import CSROperator, MixedPrecisionCG, makeDiagonalOperator
+    A = CSROperator(prob.matrix, space)
+    M = MixedPrecisionCG(A, makeDiagonalOperator(prob.matrix, space), Statistics(20000, 0.0, 1e-10))
+    out = dev(y0)
+    M.product(2.0, dev(b), -0.5, out)
+    # initial guess y0, then out = 2 y0 - 0.5 x
+    x_from_y0, _, _ = mixed_solve(space, prob.matrix, b, x0=y0)
+    assert np.allclose(host(out), 2.0 * y0 - 0.5 * x_from_y0, rtol=1e-12, atol=1e-14)
+    assert np.linalg.norm(x_from_y0 - x_full) <= 1e-8 * np.linalg.norm(x_full)
+    # iteration limit: stops with done = limit and the statistics say so
+    x7, st7, _ = mixed_solve(space, prob.matrix, b, settings=Statistics(7, 0.0, 1e-10))
+    assert st7.innerIterations == 7 and st7.refinements >= 1 and st7.relativeResidual > 1e-10
