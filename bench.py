@@ -275,10 +275,12 @@ def main():
     info = mixed.info()
 
     idx_bytes = 2 if info["compressed_columns"] else 4
-    spmv32_bytes = (4 + idx_bytes) * nnz + 4 * (n + 1) + 8 * n
+    # FP32 SELL-32 SpMV: values + column offsets of the nonzeros, x read, y written
+    # (padding entries and the per-slice descriptors are reported, not counted)
+    spmv32_bytes = (4 + idx_bytes) * nnz + 8 * n
     spmv64_bytes = 12 * nnz + 4 * (n + 1) + 16 * n
     iter64_bytes = 12 * nnz + 4 * (n + 1) + 104 * n
-    inner_bytes = (4 + idx_bytes) * nnz + 4 * (n + 1) + 52 * n
+    inner_bytes = (4 + idx_bytes) * nnz + 52 * n
     fp64_solve_bytes = (it64 + 1) * iter64_bytes + (12 * nnz + 4 * (n + 1) + 24 * n)
     refine_bytes = 12 * nnz + 4 * (n + 1) + 28 * n  # FP64 residual pass: x64, b read, r32 written, dinv32
     mixed_solve_bytes = mst.innerIterations * inner_bytes + (mst.refinements + 1) * refine_bytes
@@ -344,8 +346,9 @@ def main():
                      "achieved_gbs": fp64_solve_bytes / t_fp64 / 1e9,
                      "us_per_iteration": 1e6 * t_fp64 / (it64 + 1)},
             "speedup_mixed_vs_fp64": t_fp64 / t_mixed,
-            "roofline": {"bound": "hbm", "kernel": "mixed_apply_kernel (FP32 CSR SpMV, %s columns, %d lanes/row)"
-                         % ("16-bit" if info["compressed_columns"] else "int32", info["lanes_per_row"]),
+            "roofline": {"bound": "hbm", "kernel": "mixed_apply_kernel (FP32 SELL-32 SpMV, %s columns, %d stored "
+                         "entries for %d nonzeros)" % ("16-bit" if info["compressed_columns"] else "int32",
+                                                       info["padded_entries"], nnz),
                          "achieved": g32, "peak": hbm, "unit": "GB/s", "frac": g32 / hbm, "peak_kind": peak_kind,
                          "traffic": traffic, "algorithmic_bytes": spmv32_bytes, "launch_ms": 1e3 * t_spmv32},
             "fp64_spmv_roofline": {"kernel": "spmv_kernel (FP64 CSR, schedule %d)" % A.csr.kernel(),

@@ -341,7 +341,7 @@ int ciecu_assembly_create(ciecu_csr csr, int dim, int order, int quadratureOrder
 
 int ciecu_assembly_destroy(ciecu_assembly P) {
     if (!P) return CIECU_OK;
-    if (P->csr && P->csr->space) cudaStreamSynchronize(P->csr->space->stream);
+    // No access to P->csr (it may already be gone); cudaFree synchronises the device.
     cudaFree(P->d_cellOrder);
     cudaFree(P->d_slots);
     cudaFree(P->d_gtab);

@@ -7,10 +7,12 @@
 //   FP64 (kept on the GPU only here): the solution x64, the residual
 //        r = b - A64 x64 recomputed with the FP64 matrix, and every dot-product
 //        accumulator (the FP32 vectors are reduced in double).
-//   FP32: the matrix values (a converted copy), the vectors r, p, q, x-increment
-//        and the inverse diagonal.  Column indices are stored as 16-bit offsets
-//        from the row (col - row) when the matrix bandwidth allows -- a lossless,
-//        checked re-encoding of the int32 CSR that halves the index bytes.
+//   FP32: the matrix values (a converted copy in the SELL-32 layout of sell.cuh:
+//        one thread per row, every load warp-coalesced), the vectors r, p, q,
+//        x-increment and the inverse diagonal.  Column indices are stored as
+//        16-bit offsets from the row (col - row) when the matrix bandwidth allows
+//        -- a lossless, checked re-encoding of the int32 CSR that halves the
+//        index bytes (int32 otherwise).
 //
 // mode 0 (reliable updates; Sleijpen & van der Vorst 1996, the residual
 //   replacement used for mixed-precision CG by Clark et al. 2010): whenever the
@@ -28,9 +30,12 @@
 // M3 direction); the two refinement kernels (R1 fold, R2 FP64 residual) are in
 // the same CUDA graph and return at once unless M2 asked for a replacement.
 #include "ciecu_mixed.h"
+#include "graph.cuh"
 #include "pcg.cuh"
+#include "sell.cuh"
 
 #include <string>
+#include <vector>
 
 namespace ciecu {
 namespace {
@@ -45,98 +50,112 @@ struct MixedScalars {
     double absTol, relTol, delta;
     long long iter, maxIter, refinements;
     int done, error, update, updateX, mode, pad;
+    long long chunkIter, chunkLimit;  // iterations of the current graph launch / per launch
 };
 
-// ---- compressed FP32 matrix ---------------------------------------------------
+__device__ __forceinline__ void set_cond(bool useCond, cudaGraphConditionalHandle cond, unsigned value) {
+    if (useCond) cudaGraphSetConditional(cond, value);
+}
 
-__global__ void compress_kernel(int nrows, const int* __restrict__ rowptr, const int* __restrict__ col,
-                                const double* __restrict__ val, float* __restrict__ val32,
-                                short* __restrict__ col16, unsigned* tooFar) {
-    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nrows; r += gridDim.x * blockDim.x) {
-        for (int k = rowptr[r]; k < rowptr[r + 1]; ++k) {
-            val32[k] = static_cast<float>(val[k]);
-            const int off = col[k] - r;
-            if (col16) {
-                if (off < -32768 || off > 32767) atomicOr(tooFar, 1u);
-                col16[k] = static_cast<short>(off);
-            }
+constexpr int kUnroll = 9;  // entries per thread in flight in the SELL row loop
+
+// ---- SELL-32 FP32 matrix ------------------------------------------------------
+
+// Padded length of each 32-row slice; negative when its rows differ in length.
+__global__ void sell_len_kernel(int nrows, const int* __restrict__ rowptr, int* __restrict__ sliceLen,
+                                unsigned* tooLong) {
+    const int nslices = (nrows + 31) >> 5;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nslices; s += gridDim.x * blockDim.x) {
+        int mx = 0, mn = 0x7fffffff;
+        for (int r = s << 5; r < min(nrows, (s << 5) + 32); ++r) {
+            const int len = rowptr[r + 1] - rowptr[r];
+            mx = max(mx, len);
+            mn = min(mn, len);
         }
+        if (mx > 65535) atomicOr(tooLong, 1u);
+        sliceLen[s] = (mn == mx) ? mx : -mx;
     }
 }
 
-// Row sums over the FP32 matrix, VS lanes per row, UNROLL strided entries per
-// lane loaded before the FMA chain.  IDX16: columns are 16-bit row offsets.
-template <int VS, bool IDX16, typename Op>
-__device__ __forceinline__ void f32_rows(int nrows, const int* __restrict__ rowptr, const void* __restrict__ colv,
-                                         const float* __restrict__ val, const float* __restrict__ x, Op& op) {
-    constexpr int ROWS_PER_WARP = 32 / VS;
-    constexpr int UNROLL = VS <= 4 ? 8 : 4;
-    const int lane = threadIdx.x & 31;
-    const int sub = lane % VS;
-    const long warpGlobal = (static_cast<long>(blockIdx.x) * kT + threadIdx.x) >> 5;
-    const long warps = (static_cast<long>(gridDim.x) * kT) >> 5;
-    const long groups = (nrows + ROWS_PER_WARP - 1) / ROWS_PER_WARP;
-    const short* col16 = static_cast<const short*>(colv);
-    const int* col32 = static_cast<const int*>(colv);
-    for (long g = warpGlobal; g < groups; g += warps) {
-        const long rowL = g * ROWS_PER_WARP + lane / VS;
-        const bool valid = rowL < nrows;
-        const int r = valid ? static_cast<int>(rowL) : 0;
-        float sum = 0.0f;
-        if (valid) {
-            const int k1 = rowptr[r + 1];
-            for (int k = rowptr[r] + sub; k < k1; k += UNROLL * VS) {
-                float v[UNROLL];
-                int c[UNROLL];
-#pragma unroll
-                for (int u = 0; u < UNROLL; ++u) {
-                    const int kk = k + u * VS;
-                    const bool in = kk < k1;
-                    v[u] = in ? __ldg(val + kk) : 0.0f;
-                    if (IDX16) c[u] = in ? r + static_cast<int>(__ldg(col16 + kk)) : -1;
-                    else c[u] = in ? __ldg(col32 + kk) : -1;
+// Copies row r into its slice (values in FP32, columns as 16-bit row offsets or
+// int32) and zero-fills its padding.
+template <typename CI>
+__global__ void sell_fill_kernel(int nrows, const int* __restrict__ rowptr, const int* __restrict__ col,
+                                 const double* __restrict__ val, const int* __restrict__ sliceLen,
+                                 const long long* __restrict__ sliceStart, float* __restrict__ sval,
+                                 CI* __restrict__ scol, unsigned short* __restrict__ rowLen, unsigned* tooFar) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nrows; r += gridDim.x * blockDim.x) {
+        const int s = r >> 5;
+        const int padded = abs(sliceLen[s]);
+        const int k0 = rowptr[r], len = rowptr[r + 1] - k0;
+        rowLen[r] = static_cast<unsigned short>(len);
+        const long long base = sliceStart[s] + (r & 31);
+        for (int j = 0; j < padded; ++j) {
+            const long long idx = base + 32LL * j;
+            if (j < len) {
+                sval[idx] = static_cast<float>(val[k0 + j]);
+                const int c = col[k0 + j];
+                if constexpr (sizeof(CI) == 2) {
+                    const int off = c - r;
+                    if (off < -32768 || off > 32767) atomicOr(tooFar, 1u);
+                    scol[idx] = static_cast<CI>(off);
+                } else {
+                    scol[idx] = c;
                 }
-                float xv[UNROLL];
-#pragma unroll
-                for (int u = 0; u < UNROLL; ++u) xv[u] = c[u] >= 0 ? __ldg(x + c[u]) : 0.0f;
-#pragma unroll
-                for (int u = 0; u < UNROLL; ++u) sum = fmaf(v[u], xv[u], sum);
+            } else {
+                sval[idx] = 0.0f;
+                scol[idx] = sizeof(CI) == 2 ? CI(0) : static_cast<CI>(r);
             }
         }
-#pragma unroll
-        for (int offset = VS / 2; offset > 0; offset >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, offset, VS);
-        if (valid && sub == 0) op(r, sum);
     }
 }
 
 // out = A32 in (the inner operator on its own).
-template <int VS, bool IDX16>
-__global__ void __launch_bounds__(kT) mixed_apply_kernel(int nrows, const int* __restrict__ rowptr,
-                                                         const void* __restrict__ col, const float* __restrict__ val,
-                                                         const float* __restrict__ x, float* __restrict__ y) {
-    auto op = [&](int r, float sum) { y[r] = sum; };
-    f32_rows<VS, IDX16>(nrows, rowptr, col, val, x, op);
+struct StoreOp {
+    using Pre = NoPre;
+    float* __restrict__ y;
+    __device__ __forceinline__ NoPre pre(int) const { return NoPre{}; }
+    __device__ __forceinline__ void post(int r, NoPre, float sum) const { y[r] = sum; }
+};
+
+template <typename CI>
+__global__ void __launch_bounds__(kT) mixed_apply_kernel(SellArgs<float, CI> A, const float* __restrict__ x,
+                                                         float* __restrict__ y) {
+    StoreOp op{y};
+    sell_rows<kUnroll, float, float, CI>(A, x, op);
 }
 
 // M1: q = A32 p, p^T q (FP64 accumulation), alpha.
-template <int VS, bool IDX16>
-__global__ void __launch_bounds__(kT) mixed_spmv_kernel(int nrows, const int* __restrict__ rowptr,
-                                                        const void* __restrict__ col, const float* __restrict__ val,
-                                                        const float* __restrict__ p, float* __restrict__ q,
-                                                        MixedScalars* s, double* partials, unsigned* counter) {
-    if (*reinterpret_cast<volatile int*>(&s->done)) return;
-    double acc = 0.0;
-    auto op = [&](int r, float sum) {
+struct MixedPqOp {
+    using Pre = float;
+    const float* __restrict__ p;
+    float* __restrict__ q;
+    double acc;
+    __device__ __forceinline__ float pre(int r) const { return p[r]; }
+    __device__ __forceinline__ void post(int r, float pr, float sum) {
         q[r] = sum;
-        acc = fma(static_cast<double>(p[r]), static_cast<double>(sum), acc);
-    };
-    f32_rows<VS, IDX16>(nrows, rowptr, col, val, p, op);
-    double mine[1] = {acc}, tot[1];
+        acc = fma(static_cast<double>(pr), static_cast<double>(sum), acc);
+    }
+};
+
+template <typename CI>
+__global__ void __launch_bounds__(kT) mixed_spmv_kernel(SellArgs<float, CI> A, const float* __restrict__ p,
+                                                        float* __restrict__ q, MixedScalars* s, double* partials,
+                                                        unsigned* counter, cudaGraphConditionalHandle loop,
+                                                        bool useCond) {
+    if (*reinterpret_cast<volatile int*>(&s->done)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) set_cond(useCond, loop, 0);
+        return;
+    }
+    MixedPqOp op{p, q, 0.0};
+    sell_rows<kUnroll, float, float, CI>(A, p, op);
+    double mine[1] = {op.acc}, tot[1];
     if (grid_reduce_last<1, kT>(mine, partials, counter, tot) && threadIdx.x == 0) {
         s->pq = tot[0];
         if (!(0.0 < tot[0])) {
             s->done = 3;
             s->error = CIECU_ERR_BREAKDOWN;
+            set_cond(useCond, loop, 0);
         } else {
             s->alpha = s->rz / tot[0];
         }
@@ -147,8 +166,16 @@ __global__ void __launch_bounds__(kT) mixed_spmv_kernel(int nrows, const int* __
 __global__ void __launch_bounds__(kT) mixed_update_kernel(long n, float* __restrict__ x, float* __restrict__ r,
                                                           const float* __restrict__ p, const float* __restrict__ q,
                                                           const float* __restrict__ dinv, MixedScalars* s,
-                                                          double* partials, unsigned* counter) {
-    if (*reinterpret_cast<volatile int*>(&s->done)) return;
+                                                          double* partials, unsigned* counter,
+                                                          cudaGraphConditionalHandle loop,
+                                                          cudaGraphConditionalHandle refine, bool useCond) {
+    if (*reinterpret_cast<volatile int*>(&s->done)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            set_cond(useCond, loop, 0);
+            set_cond(useCond, refine, 0);
+        }
+        return;
+    }
     const float alpha = static_cast<float>(s->alpha);
     double rr = 0.0, rz = 0.0;
     const long quads = n >> 2;
@@ -202,6 +229,9 @@ __global__ void __launch_bounds__(kT) mixed_update_kernel(long n, float* __restr
             s->beta = tot[1] / s->rz;
             s->rz = tot[1];
         }
+        s->chunkIter += 1;
+        set_cond(useCond, refine, update ? 1u : 0u);
+        set_cond(useCond, loop, s->chunkIter < s->chunkLimit ? 1u : 0u);
     }
 }
 
@@ -216,24 +246,37 @@ __global__ void __launch_bounds__(kT) mixed_fold_kernel(long n, double* __restri
     }
 }
 
+struct ResidualOp {
+    struct Pre {
+        double b;
+        float d;
+    };
+    const double* __restrict__ b;
+    const float* __restrict__ dinv;
+    float* __restrict__ r32;
+    double rr, rz;
+    __device__ __forceinline__ Pre pre(int row) const { return Pre{b[row], dinv[row]}; }
+    __device__ __forceinline__ void post(int row, const Pre& p, double sum) {
+        const double ri = p.b - sum;
+        const float rf = static_cast<float>(ri);
+        r32[row] = rf;
+        rr = fma(ri, ri, rr);
+        rz = fma(double(rf), double(rf * p.d), rz);
+    }
+};
+
 // R2 (and set-up): r = b - A64 x64 in FP64; r32 = float(r); ||r||^2 and r32^T z32
 // in FP64.  INIT: first residual of a solve.
 template <int KERNEL, bool INIT>
 __global__ void __launch_bounds__(csr_threads<KERNEL>())
     mixed_residual_kernel(CsrArgs<double> A, const double* __restrict__ b, const double* __restrict__ x64,
                           const float* __restrict__ dinv, float* __restrict__ r32, MixedScalars* s,
-                          double* partials, unsigned* counter) {
+                          double* partials, unsigned* counter, cudaGraphConditionalHandle loop, bool useCond) {
     if (!INIT && !*reinterpret_cast<volatile int*>(&s->update)) return;
     constexpr int T = csr_threads<KERNEL>();
-    double rr = 0.0, rz = 0.0;
-    auto op = [&](int row, double sum) {
-        const double ri = b[row] - sum;
-        const float rf = static_cast<float>(ri);
-        r32[row] = rf;
-        rr = fma(ri, ri, rr);
-        rz = fma(double(rf), double(rf * dinv[row]), rz);
-    };
+    ResidualOp op{b, dinv, r32, 0.0, 0.0};
     csr_rows<KERNEL, double, double, false>(A, x64, op);
+    const double rr = op.rr, rz = op.rz;
     double mine[2] = {rr, rz}, tot[2];
     if (grid_reduce_last<2, T>(mine, partials, counter, tot) && threadIdx.x == 0) {
         const double rnorm = sqrt(tot[0]);
@@ -282,6 +325,7 @@ __global__ void __launch_bounds__(csr_threads<KERNEL>())
             }
             s->rz = tot[1];
         }
+        if (s->done) set_cond(useCond, loop, 0);
     }
 }
 
@@ -341,10 +385,17 @@ struct ciecu_mixed_s {
     ciecu_statistics settings{};
     ciecu_mixed_options options{};
     long n = 0;
-    int vs = 4;
     bool idx16 = false;
+    // SELL-32 inner matrix
+    int nslices = 0;
+    long long paddedEntries = 0;
+    int* sliceLen = nullptr;
+    long long* sliceStart = nullptr;
+    unsigned short* rowLen = nullptr;
     float* val32 = nullptr;
     void* col32or16 = nullptr;
+    ciecu::SellArgs<float, short> a16{};
+    ciecu::SellArgs<float, int> a32{};
     float* dinv32 = nullptr;
     float *x32 = nullptr, *r32 = nullptr, *p32 = nullptr, *q32 = nullptr;
     double* x64 = nullptr;
@@ -355,55 +406,49 @@ struct ciecu_mixed_s {
     unsigned* d_counter = nullptr;
     cudaGraphExec_t graph = nullptr;
     const double* graphB = nullptr;
+    bool deviceLoop = false;
+    cudaStream_t side = nullptr;  // captures the IF body of the refinement
     int chunk = 16;
 };
 
 namespace ciecu {
 namespace {
 
-template <typename F>
-int with_vs(int vs, F&& f) {
-    switch (vs) {
-        case 2: return f(std::integral_constant<int, 2>{});
-        case 8: return f(std::integral_constant<int, 8>{});
-        case 16: return f(std::integral_constant<int, 16>{});
-        case 32: return f(std::integral_constant<int, 32>{});
-        default: return f(std::integral_constant<int, 4>{});
-    }
-}
+int sell_grid(const ciecu_mixed_s* M) { return grid_for(M->n, kT, 8); }
 
-int f32_grid(const ciecu_mixed_s* M) {
-    const long rowsPerCta = static_cast<long>(kT / 32) * (32 / M->vs);
-    const long need = (M->n + rowsPerCta - 1) / rowsPerCta;
-    return static_cast<int>(std::max(1L, std::min(need, static_cast<long>(sm_count()) * 8)));
-}
-
-int launch_inner(ciecu_mixed_s* M, cudaStream_t st) {
-    const int gridA = f32_grid(M);
+// One inner iteration.  With conditional nodes (useCond) the refinement pair
+// R1/R2 sits under IF(refine); otherwise it is launched unconditionally and
+// returns at once unless M2 requested a replacement.
+int launch_inner(ciecu_mixed_s* M, cudaStream_t st, cudaGraph_t root, cudaGraphConditionalHandle loop,
+                 bool useCond) {
+    const int gridA = sell_grid(M);
     const int gridV = grid_for((M->n + 3) / 4, kT, 8);
     ciecu_csr_s* A = M->A;
-    CIECU_TRY(with_vs(M->vs, [&](auto v) -> int {
-        constexpr int VS = decltype(v)::value;
-        if (M->idx16)
-            mixed_spmv_kernel<VS, true><<<gridA, kT, 0, st>>>(static_cast<int>(M->n), A->rowptr, M->col32or16,
-                                                              M->val32, M->p32, M->q32, M->d_s, M->d_partials,
-                                                              M->d_counter);
-        else
-            mixed_spmv_kernel<VS, false><<<gridA, kT, 0, st>>>(static_cast<int>(M->n), A->rowptr, M->col32or16,
-                                                               M->val32, M->p32, M->q32, M->d_s, M->d_partials,
-                                                               M->d_counter);
-        return CIECU_OK;
-    }));
+    cudaGraphConditionalHandle refine = 0;
+    if (useCond) CIECU_CUDA(cudaGraphConditionalHandleCreate(&refine, root, 0, cudaGraphCondAssignDefault));
+    if (M->idx16)
+        mixed_spmv_kernel<short><<<gridA, kT, 0, st>>>(M->a16, M->p32, M->q32, M->d_s, M->d_partials, M->d_counter,
+                                                       loop, useCond);
+    else
+        mixed_spmv_kernel<int><<<gridA, kT, 0, st>>>(M->a32, M->p32, M->q32, M->d_s, M->d_partials, M->d_counter,
+                                                     loop, useCond);
     mixed_update_kernel<<<gridV, kT, 0, st>>>(M->n, M->x32, M->r32, M->p32, M->q32, M->dinv32, M->d_s, M->d_partials,
-                                              M->d_counter);
-    mixed_fold_kernel<<<grid_for(M->n, kT, 8), kT, 0, st>>>(M->n, M->x64, M->x32, M->d_s);
-    const int gridR = csr_grid(A, A->kernel);
-    CIECU_TRY(with_schedule(A->kernel, [&](auto k) -> int {
-        constexpr int K = decltype(k)::value;
-        mixed_residual_kernel<K, false><<<gridR, csr_threads<K>(), 0, st>>>(
-            A->args<double>(), M->b, M->x64, M->dinv32, M->r32, M->d_s, M->d_partials, M->d_counter);
-        return CIECU_OK;
-    }));
+                                              M->d_counter, loop, refine, useCond);
+    auto refinement = [&](cudaStream_t s2) -> int {
+        mixed_fold_kernel<<<grid_for(M->n, kT, 8), kT, 0, s2>>>(M->n, M->x64, M->x32, M->d_s);
+        const int gridR = csr_grid(A, A->kernel);
+        return with_schedule(A->kernel, [&](auto k) -> int {
+            constexpr int K = decltype(k)::value;
+            mixed_residual_kernel<K, false><<<gridR, csr_threads<K>(), 0, s2>>>(
+                A->args<double>(), M->b, M->x64, M->dinv32, M->r32, M->d_s, M->d_partials, M->d_counter, loop,
+                useCond);
+            return CIECU_OK;
+        });
+    };
+    if (useCond)
+        CIECU_TRY(capture_if(st, M->side, refine, refinement));
+    else
+        CIECU_TRY(refinement(st));
     mixed_direction_kernel<<<gridV, kT, 0, st>>>(M->n, M->p32, M->r32, M->dinv32, M->d_s);
     CIECU_CHECK_LAUNCH("mixed inner iteration");
     return CIECU_OK;
@@ -416,10 +461,20 @@ int build_mixed_graph(ciecu_mixed_s* M) {
         M->graph = nullptr;
     }
     cudaStream_t st = M->A->space->stream;
+    int status = build_while_graph(st, [&](cudaGraph_t root, cudaGraphConditionalHandle loop) {
+        return launch_inner(M, st, root, loop, true);
+    }, &M->graph);
+    if (status == CIECU_OK) {
+        M->deviceLoop = true;
+        M->graphB = M->b;
+        return CIECU_OK;
+    }
+    cudaGetLastError();
+    M->deviceLoop = false;
     cudaGraph_t g = nullptr;
     CIECU_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    int status = CIECU_OK;
-    for (int i = 0; i < M->chunk && status == CIECU_OK; ++i) status = launch_inner(M, st);
+    status = CIECU_OK;
+    for (int i = 0; i < M->chunk && status == CIECU_OK; ++i) status = launch_inner(M, st, nullptr, 0, false);
     cudaError_t e = cudaStreamEndCapture(st, &g);
     if (status != CIECU_OK) {
         if (g) cudaGraphDestroy(g);
@@ -453,13 +508,10 @@ int ciecu_mixed_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_sta
     M->settings = settings;
     M->options = options;
     M->n = lhs->rows;
-    M->vs = lhs->avgRow > 12 ? 4 : 2;
     cudaStream_t st = lhs->space->stream;
     const size_t n = static_cast<size_t>(std::max<long>(M->n, 1)) + 4;
-    const size_t nnz = static_cast<size_t>(std::max<long>(lhs->nnz, 1));
-    cudaError_t e = cudaMalloc(&M->val32, sizeof(float) * nnz);
-    const bool try16 = options.compressColumns != 0;
-    if (e == cudaSuccess) e = cudaMalloc(&M->col32or16, (try16 ? sizeof(short) : sizeof(int)) * nnz);
+    M->nslices = static_cast<int>((M->n + 31) / 32);
+    cudaError_t e = cudaSuccess;
     for (float** v : {&M->dinv32, &M->x32, &M->r32, &M->p32, &M->q32})
         if (e == cudaSuccess) e = cudaMalloc(v, sizeof(float) * n);
     if (e == cudaSuccess) e = cudaMalloc(&M->x64, sizeof(double) * n);
@@ -468,48 +520,103 @@ int ciecu_mixed_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_sta
     if (e == cudaSuccess) e = cudaMalloc(&M->d_partials, sizeof(double) * kMaxPartials * 2);
     if (e == cudaSuccess) e = cudaMalloc(&M->d_counter, sizeof(unsigned) * 4);
     if (e == cudaSuccess) e = cudaMemsetAsync(M->d_counter, 0, sizeof(unsigned) * 4, st);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&M->side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&M->sliceLen, sizeof(int) * std::max(1, M->nslices));
+    if (e == cudaSuccess) e = cudaMalloc(&M->sliceStart, sizeof(long long) * (M->nslices + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&M->rowLen, sizeof(unsigned short) * n);
     if (e != cudaSuccess) {
         ciecu_mixed_destroy(M);
         return cuda_fail(e, "mixed_create: allocation");
     }
-    unsigned* d_far = reinterpret_cast<unsigned*>(lhs->space->d_result);
-    unsigned far = 0;
-    e = cudaMemsetAsync(d_far, 0, sizeof(unsigned), st);
-    if (M->n > 0) {
-        compress_kernel<<<grid_for(M->n, kT, 8), kT, 0, st>>>(
-            static_cast<int>(M->n), lhs->rowptr, lhs->col, static_cast<const double*>(lhs->val), M->val32,
-            try16 ? static_cast<short*>(M->col32or16) : nullptr, d_far);
-        to_f32_kernel<<<grid_for(M->n, kT, 8), kT, 0, st>>>(M->n, d_inverseDiagonal, M->dinv32);
-        count_launch(2);
+    // Slice lengths on the device, their prefix sum on the host.
+    unsigned* d_flag = reinterpret_cast<unsigned*>(lhs->space->d_result);
+    unsigned flags[2] = {0, 0};
+    e = cudaMemsetAsync(d_flag, 0, 2 * sizeof(unsigned), st);
+    if (M->n > 0 && e == cudaSuccess) {
+        sell_len_kernel<<<grid_for(M->nslices, kT, 8), kT, 0, st>>>(static_cast<int>(M->n), lhs->rowptr, M->sliceLen,
+                                                                    d_flag);
+        count_launch();
+        e = cudaGetLastError();
     }
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&far, d_far, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
+    std::vector<int> lens(static_cast<size_t>(M->nslices));
+    std::vector<long long> starts(static_cast<size_t>(M->nslices) + 1, 0);
+    if (e == cudaSuccess && M->nslices)
+        e = cudaMemcpyAsync(lens.data(), M->sliceLen, sizeof(int) * lens.size(), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(flags, d_flag, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        ciecu_mixed_destroy(M);
+        return cuda_fail(e, "mixed_create: slice lengths");
+    }
+    if (flags[0]) {
+        ciecu_mixed_destroy(M);
+        return fail(CIECU_ERR_ARGUMENT, "mixed_create: rows longer than 65535 entries are not supported");
+    }
+    for (int sl = 0; sl < M->nslices; ++sl) starts[sl + 1] = starts[sl] + 32LL * std::abs(lens[sl]);
+    M->paddedEntries = starts.back();
+    e = cudaMemcpyAsync(M->sliceStart, starts.data(), sizeof(long long) * starts.size(), cudaMemcpyHostToDevice, st);
+    const size_t padded = static_cast<size_t>(std::max<long long>(1, M->paddedEntries));
+    if (e == cudaSuccess) e = cudaMalloc(&M->val32, sizeof(float) * padded);
+    const bool try16 = options.compressColumns != 0;
+    if (e == cudaSuccess) e = cudaMalloc(&M->col32or16, (try16 ? sizeof(short) : sizeof(int)) * padded);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_flag, 0, sizeof(unsigned), st);
+    if (e == cudaSuccess && M->n > 0) {
+        const int grid = grid_for(M->n, kT, 8);
+        if (try16)
+            sell_fill_kernel<short><<<grid, kT, 0, st>>>(static_cast<int>(M->n), lhs->rowptr, lhs->col,
+                                                         static_cast<const double*>(lhs->val), M->sliceLen,
+                                                         M->sliceStart, M->val32, static_cast<short*>(M->col32or16),
+                                                         M->rowLen, d_flag);
+        else
+            sell_fill_kernel<int><<<grid, kT, 0, st>>>(static_cast<int>(M->n), lhs->rowptr, lhs->col,
+                                                       static_cast<const double*>(lhs->val), M->sliceLen,
+                                                       M->sliceStart, M->val32, static_cast<int*>(M->col32or16),
+                                                       M->rowLen, d_flag);
+        to_f32_kernel<<<grid, kT, 0, st>>>(M->n, d_inverseDiagonal, M->dinv32);
+        count_launch(2);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(flags, d_flag, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {
         ciecu_mixed_destroy(M);
         return cuda_fail(e, "mixed_create: conversion");
     }
-    M->idx16 = try16 && !far;
-    if (!M->idx16) {
-        // bandwidth too large for 16-bit offsets (or not requested): int32 columns
+    M->idx16 = try16 && !flags[0];
+    if (try16 && flags[0]) {
+        // bandwidth too large for 16-bit offsets: int32 columns
         cudaFree(M->col32or16);
         M->col32or16 = nullptr;
-        e = cudaMalloc(&M->col32or16, sizeof(int) * nnz);
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync(M->col32or16, lhs->col, sizeof(int) * lhs->nnz, cudaMemcpyDeviceToDevice, st);
+        e = cudaMalloc(&M->col32or16, sizeof(int) * padded);
+        if (e == cudaSuccess && M->n > 0) {
+            sell_fill_kernel<int><<<grid_for(M->n, kT, 8), kT, 0, st>>>(
+                static_cast<int>(M->n), lhs->rowptr, lhs->col, static_cast<const double*>(lhs->val), M->sliceLen,
+                M->sliceStart, M->val32, static_cast<int*>(M->col32or16), M->rowLen, d_flag);
+            count_launch();
+            e = cudaGetLastError();
+        }
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) {
             ciecu_mixed_destroy(M);
             return cuda_fail(e, "mixed_create: int32 columns");
         }
     }
+    M->a16 = SellArgs<float, short>{static_cast<int>(M->n), M->sliceLen, M->sliceStart, M->rowLen, M->val32,
+                                    static_cast<const short*>(M->col32or16)};
+    M->a32 = SellArgs<float, int>{static_cast<int>(M->n), M->sliceLen, M->sliceStart, M->rowLen, M->val32,
+                                  static_cast<const int*>(M->col32or16)};
     *out = M;
     return CIECU_OK;
 }
 
 int ciecu_mixed_destroy(ciecu_mixed M) {
     if (!M) return CIECU_OK;
-    if (M->A && M->A->space) cudaStreamSynchronize(M->A->space->stream);
+    // No access to M->A (it may already be gone); cudaFree synchronises the device.
     if (M->graph) cudaGraphExecDestroy(M->graph);
+    if (M->side) cudaStreamDestroy(M->side);
+    cudaFree(M->sliceLen);
+    cudaFree(M->sliceStart);
+    cudaFree(M->rowLen);
     cudaFree(M->val32);
     cudaFree(M->col32or16);
     cudaFree(M->dinv32);
@@ -529,7 +636,7 @@ int ciecu_mixed_destroy(ciecu_mixed M) {
 int ciecu_mixed_info(ciecu_mixed M, int* compressedColumns, int* lanesPerRow) {
     CIECU_REQUIRE(M, "mixed_info: null solver");
     if (compressedColumns) *compressedColumns = M->idx16 ? 1 : 0;
-    if (lanesPerRow) *lanesPerRow = M->vs;
+    if (lanesPerRow) *lanesPerRow = 1;  // SELL-32: one thread per row
     return CIECU_OK;
 }
 
@@ -537,19 +644,19 @@ int ciecu_mixed_apply_f32(ciecu_mixed M, const float* d_in, float* d_out) {
     CIECU_REQUIRE(M && (M->n == 0 || (d_in && d_out)), "mixed_apply_f32: null argument");
     if (M->n == 0) return CIECU_OK;
     cudaStream_t st = M->A->space->stream;
-    const int grid = f32_grid(M);
-    CIECU_TRY(with_vs(M->vs, [&](auto v) -> int {
-        constexpr int VS = decltype(v)::value;
-        if (M->idx16)
-            mixed_apply_kernel<VS, true><<<grid, kT, 0, st>>>(static_cast<int>(M->n), M->A->rowptr, M->col32or16,
-                                                              M->val32, d_in, d_out);
-        else
-            mixed_apply_kernel<VS, false><<<grid, kT, 0, st>>>(static_cast<int>(M->n), M->A->rowptr, M->col32or16,
-                                                               M->val32, d_in, d_out);
-        return CIECU_OK;
-    }));
+    const int grid = sell_grid(M);
+    if (M->idx16)
+        mixed_apply_kernel<short><<<grid, kT, 0, st>>>(M->a16, d_in, d_out);
+    else
+        mixed_apply_kernel<int><<<grid, kT, 0, st>>>(M->a32, d_in, d_out);
     count_launch();
     CIECU_CHECK_LAUNCH("mixed_apply_kernel");
+    return CIECU_OK;
+}
+
+int ciecu_mixed_padded_entries(ciecu_mixed M, int64_t* h_entries) {
+    CIECU_REQUIRE(M && h_entries, "mixed_padded_entries: null argument");
+    *h_entries = M->paddedEntries;
     return CIECU_OK;
 }
 
@@ -592,19 +699,29 @@ int ciecu_mixed_product(ciecu_mixed M, double inScale, const double* d_in, doubl
         CIECU_TRY(with_schedule(A->kernel, [&](auto k) -> int {
             constexpr int K = decltype(k)::value;
             mixed_residual_kernel<K, true><<<gridR, csr_threads<K>(), 0, st>>>(
-                A->args<double>(), d_in, M->x64, M->dinv32, M->r32, M->d_s, M->d_partials, M->d_counter);
+                A->args<double>(), d_in, M->x64, M->dinv32, M->r32, M->d_s, M->d_partials, M->d_counter, 0, false);
             return CIECU_OK;
         }));
         mixed_direction_kernel<<<grid_for((n + 3) / 4, kT, 8), kT, 0, st>>>(n, M->p32, M->r32, M->dinv32, M->d_s);
         count_launch(2);
         CIECU_CHECK_LAUNCH("mixed set-up");
         CIECU_TRY(build_mixed_graph(M));
+        const long long limit = M->deviceLoop ? 4096 : M->chunk;
         for (;;) {
             CIECU_CUDA(cudaMemcpyAsync(M->h_s, M->d_s, sizeof(MixedScalars), cudaMemcpyDeviceToHost, st));
             CIECU_CUDA(cudaStreamSynchronize(st));
             if (M->h_s->done) break;
+            const long long before = M->h_s->iter, refBefore = M->h_s->refinements;
+            M->h_s->chunkIter = 0;
+            M->h_s->chunkLimit = limit;
+            CIECU_CUDA(cudaMemcpyAsync(&M->d_s->chunkIter, &M->h_s->chunkIter, 2 * sizeof(long long),
+                                       cudaMemcpyHostToDevice, st));
             CIECU_CUDA(cudaGraphLaunch(M->graph, st));
-            count_launch(5LL * M->chunk);
+            CIECU_CUDA(cudaMemcpyAsync(M->h_s, M->d_s, sizeof(MixedScalars), cudaMemcpyDeviceToHost, st));
+            CIECU_CUDA(cudaStreamSynchronize(st));
+            count_launch(M->deviceLoop ? 3LL * (M->h_s->iter - before) + 2LL * (M->h_s->refinements - refBefore)
+                                       : 5LL * M->chunk);
+            if (M->h_s->done) break;
         }
         const MixedScalars& s = *M->h_s;
         if (s.error) {

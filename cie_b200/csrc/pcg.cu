@@ -11,6 +11,7 @@
 //       space.scale(search, beta) followed by space.add(search, z, 1)).
 // Every kernel returns at once when the done flag is set, so a CUDA graph of a
 // fixed number of iterations can be replayed until the host sees the flag.
+#include "graph.cuh"
 #include "pcg.cuh"
 
 #include <string>
@@ -62,19 +63,35 @@ __global__ void __launch_bounds__(kT) pcg_init_kernel(long n, const double* __re
 }
 
 // K1: q = A p, p^T q, alpha.
+struct PqOp {
+    using Pre = double;
+    const double* __restrict__ p;
+    double* __restrict__ q;
+    double acc;
+    __device__ __forceinline__ double pre(int r) const { return p[r]; }
+    __device__ __forceinline__ void post(int r, double pr, double sum) {
+        q[r] = sum;
+        acc = fma(pr, sum, acc);
+    }
+};
+
+// Ends the device-side loop (graph WHILE node) when `cond` is a live handle.
+__device__ __forceinline__ void set_loop(bool useCond, cudaGraphConditionalHandle cond, unsigned value) {
+    if (useCond) cudaGraphSetConditional(cond, value);
+}
+
 template <int KERNEL>
 __global__ void __launch_bounds__(csr_threads<KERNEL>())
     pcg_spmv_kernel(CsrArgs<double> A, const double* __restrict__ p, double* __restrict__ q, PcgScalars* s,
-                    double* partials, unsigned* counter) {
-    if (*reinterpret_cast<volatile int*>(&s->done)) return;
+                    double* partials, unsigned* counter, cudaGraphConditionalHandle cond, bool useCond) {
+    if (*reinterpret_cast<volatile int*>(&s->done)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) set_loop(useCond, cond, 0);
+        return;
+    }
     constexpr int T = csr_threads<KERNEL>();
-    double acc = 0.0;
-    auto op = [&](int r, double sum) {
-        q[r] = sum;
-        acc = fma(p[r], sum, acc);
-    };
+    PqOp op{p, q, 0.0};
     csr_rows<KERNEL, double, double, false>(A, p, op);
-    double mine[1] = {acc}, tot[1];
+    double mine[1] = {op.acc}, tot[1];
     if (grid_reduce_last<1, T>(mine, partials, counter, tot) && threadIdx.x == 0) {
         s->pq = tot[0];
         if (!(0.0 < tot[0])) {
@@ -82,6 +99,7 @@ __global__ void __launch_bounds__(csr_threads<KERNEL>())
             s->error = CIECU_ERR_BREAKDOWN;
             s->errorKind = 2;
             s->errorIter = s->iter;
+            set_loop(useCond, cond, 0);
         } else {
             s->alpha = s->rz / tot[0];
         }
@@ -94,8 +112,12 @@ template <bool PRECOND>
 __global__ void __launch_bounds__(kT) pcg_update_kernel(long n, double* __restrict__ x, double* __restrict__ r,
                                                         const double* __restrict__ p, const double* __restrict__ q,
                                                         const double* __restrict__ dinv, PcgScalars* s,
-                                                        double* partials, unsigned* counter) {
-    if (*reinterpret_cast<volatile int*>(&s->done)) return;
+                                                        double* partials, unsigned* counter,
+                                                        cudaGraphConditionalHandle cond, bool useCond) {
+    if (*reinterpret_cast<volatile int*>(&s->done)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) set_loop(useCond, cond, 0);
+        return;
+    }
     const double alpha = s->alpha;
     const double malpha = -alpha;
     double rr = 0.0, rz = 0.0;
@@ -142,6 +164,8 @@ __global__ void __launch_bounds__(kT) pcg_update_kernel(long n, double* __restri
             s->iter += 1;
             if (s->iter >= s->maxIter) s->done = 2;
         }
+        s->chunkIter += 1;
+        set_loop(useCond, cond, (s->done == 0 && s->chunkIter < s->chunkLimit) ? 1u : 0u);
     }
 }
 
@@ -214,13 +238,14 @@ struct ciecu_pcg_s {
     unsigned* d_counter = nullptr;
     cudaGraphExec_t graph = nullptr;
     int graphKernel = -1;
+    bool deviceLoop = false;  // graph = WHILE loop (else `chunk` unrolled iterations)
     int chunk = 16;
 };
 
 namespace ciecu {
 namespace {
 
-int launch_iteration(ciecu_pcg_s* S, cudaStream_t st) {
+int launch_iteration(ciecu_pcg_s* S, cudaStream_t st, cudaGraphConditionalHandle cond, bool useCond) {
     ciecu_csr_s* A = S->A;
     const int gridA = csr_grid(A, A->kernel);
     const int gridV = grid_for((S->n + 1) / 2, kT, 8);
@@ -228,22 +253,25 @@ int launch_iteration(ciecu_pcg_s* S, cudaStream_t st) {
     CIECU_TRY(with_schedule(A->kernel, [&](auto k) -> int {
         constexpr int K = decltype(k)::value;
         pcg_spmv_kernel<K><<<gridA, csr_threads<K>(), 0, st>>>(A->args<double>(), S->p, S->q, S->d_s, S->d_partials,
-                                                               S->d_counter);
+                                                               S->d_counter, cond, useCond);
         return CIECU_OK;
     }));
     if (pre) {
         pcg_update_kernel<true><<<gridV, kT, 0, st>>>(S->n, S->x, S->r, S->p, S->q, S->dinv, S->d_s, S->d_partials,
-                                                      S->d_counter);
+                                                      S->d_counter, cond, useCond);
         pcg_direction_kernel<true><<<gridV, kT, 0, st>>>(S->n, S->p, S->r, S->dinv, S->d_s);
     } else {
         pcg_update_kernel<false><<<gridV, kT, 0, st>>>(S->n, S->x, S->r, S->p, S->q, S->dinv, S->d_s, S->d_partials,
-                                                       S->d_counter);
+                                                       S->d_counter, cond, useCond);
         pcg_direction_kernel<false><<<gridV, kT, 0, st>>>(S->n, S->p, S->r, S->dinv, S->d_s);
     }
     CIECU_CHECK_LAUNCH("pcg iteration");
     return CIECU_OK;
 }
 
+// The solve loop as a graph: a device-side WHILE loop over one iteration when the
+// driver supports conditional nodes, else `chunk` captured iterations that the
+// host replays until the done flag is set.
 int build_graph(ciecu_pcg_s* S) {
     cudaStream_t st = S->A->space->stream;
     if (S->graph && S->graphKernel == S->A->kernel) return CIECU_OK;
@@ -251,10 +279,20 @@ int build_graph(ciecu_pcg_s* S) {
         cudaGraphExecDestroy(S->graph);
         S->graph = nullptr;
     }
+    int status = build_while_graph(st, [&](cudaGraph_t, cudaGraphConditionalHandle cond) {
+        return launch_iteration(S, st, cond, true);
+    }, &S->graph);
+    if (status == CIECU_OK) {
+        S->deviceLoop = true;
+        S->graphKernel = S->A->kernel;
+        return CIECU_OK;
+    }
+    cudaGetLastError();  // clear a sticky launch error of the failed attempt
+    S->deviceLoop = false;
     cudaGraph_t g = nullptr;
     CIECU_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    int status = CIECU_OK;
-    for (int i = 0; i < S->chunk && status == CIECU_OK; ++i) status = launch_iteration(S, st);
+    status = CIECU_OK;
+    for (int i = 0; i < S->chunk && status == CIECU_OK; ++i) status = launch_iteration(S, st, 0, false);
     cudaError_t e = cudaStreamEndCapture(st, &g);
     if (status != CIECU_OK) {
         if (g) cudaGraphDestroy(g);
@@ -308,7 +346,8 @@ int ciecu_pcg_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_stati
 
 int ciecu_pcg_destroy(ciecu_pcg S) {
     if (!S) return CIECU_OK;
-    if (S->A && S->A->space) cudaStreamSynchronize(S->A->space->stream);
+    // No access to S->A: the matrix handle may already be gone.  cudaFree
+    // synchronises the device before releasing memory.
     if (S->graph) cudaGraphExecDestroy(S->graph);
     cudaFree(S->x);
     cudaFree(S->r);
@@ -367,12 +406,23 @@ int ciecu_pcg_product(ciecu_pcg S, double inScale, const double* d_in, double ou
         CIECU_TRY(build_graph(S));
         // Replay graph chunks until the device reports done.  The scalars are read
         // back after each chunk; the kernels of a finished solve return at once.
+        // Device loop: one launch runs up to chunkLimit iterations; the host only
+        // looks at the scalars between launches.
+        const long long limit = S->deviceLoop ? 4096 : S->chunk;
         for (;;) {
             CIECU_CUDA(cudaMemcpyAsync(S->h_s, S->d_s, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
             CIECU_CUDA(cudaStreamSynchronize(st));
             if (S->h_s->done) break;
+            const long long before = S->h_s->iter;
+            S->h_s->chunkIter = 0;
+            S->h_s->chunkLimit = limit;
+            CIECU_CUDA(cudaMemcpyAsync(&S->d_s->chunkIter, &S->h_s->chunkIter, 2 * sizeof(long long),
+                                       cudaMemcpyHostToDevice, st));
             CIECU_CUDA(cudaGraphLaunch(S->graph, st));
-            count_launch(3LL * S->chunk);
+            CIECU_CUDA(cudaMemcpyAsync(S->h_s, S->d_s, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
+            CIECU_CUDA(cudaStreamSynchronize(st));
+            count_launch(3LL * std::max<long long>(1, S->deviceLoop ? S->h_s->iter - before + 1 : S->chunk));
+            if (S->h_s->done) break;
         }
         const PcgScalars& s = *S->h_s;
         if (s.error) {

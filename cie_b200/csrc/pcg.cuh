@@ -25,6 +25,8 @@ struct PcgScalars {
     long long errorIter;
     int errorKind;      // 1: r^T z <= 0 at start, 2: p^T A p <= 0
     int pad;
+    long long chunkIter;   // iterations run by the current graph launch
+    long long chunkLimit;  // iterations one graph launch may run
 };
 
 // Comparison::less with the default tolerances

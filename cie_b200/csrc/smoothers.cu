@@ -79,15 +79,28 @@ __global__ void jacobi_first_kernel(long n, const double* __restrict__ in, const
 }
 
 // One sweep: res = in - A x_old; x_new = x_old + (w res) D^-1.
+struct JacobiOp {
+    struct Pre {
+        double in, d, xo;
+    };
+    const double* __restrict__ in;
+    const double* __restrict__ dinv;
+    const double* __restrict__ xold;
+    double* __restrict__ xnew;
+    double w;
+    __device__ __forceinline__ Pre pre(int r) const { return Pre{in[r], dinv[r], xold[r]}; }
+    __device__ __forceinline__ void post(int r, const Pre& p, double sum) const {
+        const double res = p.in - sum;
+        const double t = w == 1.0 ? res * p.d : (w == -1.0 ? -res * p.d : w * res * p.d);
+        xnew[r] = p.xo + t;
+    }
+};
+
 template <int KERNEL, bool MASKED>
 __global__ void __launch_bounds__(csr_threads<KERNEL>())
     jacobi_sweep_kernel(CsrArgs<double> A, const double* __restrict__ in, const double* __restrict__ dinv, double w,
                         const double* __restrict__ xold, double* __restrict__ xnew) {
-    auto op = [&](int r, double sum) {
-        const double res = in[r] - sum;
-        const double t = w == 1.0 ? res * dinv[r] : (w == -1.0 ? -res * dinv[r] : w * res * dinv[r]);
-        xnew[r] = xold[r] + t;
-    };
+    JacobiOp op{in, dinv, xold, xnew, w};
     csr_rows<KERNEL, double, double, MASKED>(A, xold, op);
 }
 
@@ -117,18 +130,32 @@ __global__ void cheb_first_kernel(long n, const double* __restrict__ in, const d
 }
 
 // Chebyshev step: r -= A d_old; d_new = c1 d_old + c2 D^-1 r; x += d_new.
+struct ChebOp {
+    struct Pre {
+        double r, d, dinv, x;
+    };
+    const double* __restrict__ dinv;
+    double c1, c2;
+    double* __restrict__ r;
+    const double* __restrict__ dold;
+    double* __restrict__ dnew;
+    double* __restrict__ x;
+    __device__ __forceinline__ Pre pre(int i) const { return Pre{r[i], dold[i], dinv[i], x[i]}; }
+    __device__ __forceinline__ void post(int i, const Pre& p, double sum) const {
+        const double ri = p.r - sum;
+        r[i] = ri;
+        const double di = c1 * p.d + c2 * p.dinv * ri;
+        dnew[i] = di;
+        x[i] = p.x + di;
+    }
+};
+
 template <int KERNEL>
 __global__ void __launch_bounds__(csr_threads<KERNEL>())
     cheb_step_kernel(CsrArgs<double> A, const double* __restrict__ dinv, double c1, double c2,
                      double* __restrict__ r, const double* __restrict__ dold, double* __restrict__ dnew,
                      double* __restrict__ x) {
-    auto op = [&](int i, double sum) {
-        const double ri = r[i] - sum;
-        r[i] = ri;
-        const double di = c1 * dold[i] + c2 * dinv[i] * ri;
-        dnew[i] = di;
-        x[i] += di;
-    };
+    ChebOp op{dinv, c1, c2, r, dold, dnew, x};
     csr_rows<KERNEL, double, double, false>(A, dold, op);
 }
 
@@ -159,11 +186,19 @@ __global__ void power_normalize_kernel(long n, double* __restrict__ v, const dou
     for (long i = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) v[i] *= inv;
 }
 
+struct PowerOp {
+    using Pre = double;
+    const double* __restrict__ dinv;
+    double* __restrict__ w;
+    __device__ __forceinline__ double pre(int i) const { return dinv[i]; }
+    __device__ __forceinline__ void post(int i, double d, double sum) const { w[i] = sum * d; }
+};
+
 template <int KERNEL>
 __global__ void __launch_bounds__(csr_threads<KERNEL>())
     power_apply_kernel(CsrArgs<double> A, const double* __restrict__ dinv, const double* __restrict__ v,
                        double* __restrict__ w) {
-    auto op = [&](int i, double sum) { w[i] = sum * dinv[i]; };
+    PowerOp op{dinv, w};
     csr_rows<KERNEL, double, double, false>(A, v, op);
 }
 

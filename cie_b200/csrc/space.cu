@@ -189,7 +189,9 @@ int ciecu_space_create(void* cudaStream, ciecu_space* out) {
 
 int ciecu_space_destroy(ciecu_space space) {
     if (!space) return CIECU_OK;
-    if (space->stream) cudaStreamSynchronize(space->stream);
+    // Only a stream this space created is touched (a borrowed one may already be
+    // gone); cudaFree synchronises the device.
+    if (space->ownsStream && space->stream) cudaStreamSynchronize(space->stream);
     cudaFree(space->d_partials);
     cudaFree(space->d_counter);
     cudaFree(space->d_result);

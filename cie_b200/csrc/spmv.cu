@@ -15,13 +15,20 @@ namespace ciecu {
 
 namespace {
 
+// out = combine(inScale, out, outScale, A in); out is only read when inScale != 0.
+template <typename T>
+struct AxpbyOp {
+    using Pre = T;
+    T inScale, outScale;
+    T* __restrict__ y;
+    __device__ __forceinline__ T pre(int r) const { return inScale == T(0) ? T(0) : y[r]; }
+    __device__ __forceinline__ void post(int r, T old, T sum) const { y[r] = combine(inScale, old, outScale, sum); }
+};
+
 template <int KERNEL, typename T, typename V, bool MASKED>
 __global__ void __launch_bounds__(csr_threads<KERNEL>())
     spmv_kernel(CsrArgs<V> A, T inScale, const T* __restrict__ x, T outScale, T* __restrict__ y) {
-    auto op = [&](int r, T sum) {
-        const T old = inScale == T(0) ? T(0) : y[r];
-        y[r] = combine(inScale, old, outScale, sum);
-    };
+    AxpbyOp<T> op{inScale, outScale, y};
     csr_rows<KERNEL, T, V, MASKED>(A, x, op);
 }
 
@@ -257,7 +264,7 @@ int ciecu_csr_create(ciecu_space space, int32_t rowCount, int32_t columnCount, i
 
 int ciecu_csr_destroy(ciecu_csr csr) {
     if (!csr) return CIECU_OK;
-    if (csr->space) cudaStreamSynchronize(csr->space->stream);
+    // No access to csr->space (it may already be gone); cudaFree synchronises the device.
     cudaFree(csr->d_blocks);
     delete csr;
     return CIECU_OK;

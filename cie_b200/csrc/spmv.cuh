@@ -1,18 +1,26 @@
 // CSR SpMV device engine shared by the operator kernels and the fused solver
 // kernels.  Two schedules:
 //
+//  * vector_rows<VS>: VS lanes per row (VS = 2..32; the sub-group-per-row scheme
+//    of SYCLCSROperator.cpp:55-86).  Lane j of a row handles entries j, j + VS,
+//    ...; a warp load instruction covers VS consecutive entries of each of its
+//    32/VS rows, each lane keeps UNROLL loads in flight, and the lanes of a row
+//    reduce with shuffles.
 //  * stream_rows: rows are grouped host-side into row blocks of at most TILE
-//    entries.  A CTA stages its block's column indices (int4 loads), values
-//    (16-byte loads) and the gathered x[col] into shared memory, then one thread
-//    per row accumulates the row in CSR order with FMA -- the summation order of
-//    CSROperator.cpp:49-56, so row sums match the reference's FMA-contracted
-//    build bit for bit.  Rows longer than TILE form single-row blocks that the
-//    whole CTA reduces cooperatively.
-//  * vector_rows<VS>: VS lanes per row (VS = 2..32), lanes stride the row and
-//    reduce with shuffles (the sub-group-per-row scheme of SYCLCSROperator.cpp:55-86).
+//    entries.  A CTA stages its block's column indices, values and the gathered
+//    x[col] into shared memory, then one thread per row accumulates the row in
+//    CSR order with FMA -- the summation order of CSROperator.cpp:49-56, so row
+//    sums match the reference's FMA-contracted build bit for bit.  Rows longer
+//    than TILE form single-row blocks that the whole CTA reduces cooperatively.
 //
-// Both call op(row, sum) exactly once per row, so fused epilogues (scaled
-// update, dot products of the solver) need no second pass over the output.
+// Epilogues are structs with pre(row) -> Pre and post(row, Pre, sum): pre() is
+// issued before the row's loads so that operands the epilogue needs (p[r],
+// b[r], D^-1[r], ...) are in flight with them instead of adding a dependent
+// memory latency after the reduction; post() runs exactly once per row, so fused
+// epilogues (scaled update, solver dot products) need no second pass.
+//
+// Column indices: CI = int (absolute) or short (offset from the row, the 16-bit
+// encoding of the mixed-precision inner matrix).
 #pragma once
 
 #include "common.cuh"
@@ -29,18 +37,21 @@ constexpr int kStreamTile = 2048;       // entries per row block
 constexpr int kStreamMaxRows = 1024;    // rows per row block
 constexpr int kVectorThreads = 256;
 
-template <typename V>
+template <typename V, typename CI = int>
 struct CsrArgs {
     const int* __restrict__ rowptr;
-    const int* __restrict__ col;
+    const CI* __restrict__ col;
     const V* __restrict__ val;
     int nrows;
+    long nnz;
     const int* __restrict__ blocks;  // row-block boundaries (nblocks + 1)
     int nblocks;
     const uint16_t* __restrict__ mask;  // optional (masked operator)
     uint16_t threshold;
     bool aligned16;  // col and val base pointers are 16-byte aligned
 };
+
+struct NoPre {};
 
 template <typename V>
 struct Vec4;
@@ -60,8 +71,34 @@ struct Vec4<float> {
     }
 };
 
-template <bool MASKED, typename T, typename V>
-__device__ __forceinline__ T gather(const CsrArgs<V>& A, const T* __restrict__ x, int c) {
+template <typename CI>
+struct Col4;
+template <>
+struct Col4<int> {
+    static __device__ __forceinline__ void load(const int* p, int row, int (&c)[4]) {
+        const int4 a = __ldg(reinterpret_cast<const int4*>(p));
+        c[0] = a.x; c[1] = a.y; c[2] = a.z; c[3] = a.w;
+        (void)row;
+    }
+    static __device__ __forceinline__ int one(const int* p, int row) {
+        (void)row;
+        return __ldg(p);
+    }
+};
+template <>
+struct Col4<short> {
+    static __device__ __forceinline__ void load(const short* p, int row, int (&c)[4]) {
+        const uint2 a = __ldg(reinterpret_cast<const uint2*>(p));
+        c[0] = row + static_cast<short>(a.x & 0xffffu);
+        c[1] = row + static_cast<short>(a.x >> 16);
+        c[2] = row + static_cast<short>(a.y & 0xffffu);
+        c[3] = row + static_cast<short>(a.y >> 16);
+    }
+    static __device__ __forceinline__ int one(const short* p, int row) { return row + __ldg(p); }
+};
+
+template <bool MASKED, typename T, typename V, typename CI>
+__device__ __forceinline__ T gather(const CsrArgs<V, CI>& A, const T* __restrict__ x, int c) {
     if constexpr (MASKED) {
         return A.mask[c] < A.threshold ? __ldg(x + c) : T(0);
     } else {
@@ -71,7 +108,7 @@ __device__ __forceinline__ T gather(const CsrArgs<V>& A, const T* __restrict__ x
 
 // Stages entries [e0, e1) of the row block: s_val[k] = val[e0+k], s_x[k] = x[col[e0+k]].
 template <typename T, typename V, int THREADS, bool MASKED>
-__device__ __forceinline__ void stage_block(const CsrArgs<V>& A, const T* __restrict__ x, int e0, int e1,
+__device__ __forceinline__ void stage_block(const CsrArgs<V, int>& A, const T* __restrict__ x, int e0, int e1,
                                             V* s_val, T* s_x) {
     const int tid = threadIdx.x;
     if (A.aligned16) {
@@ -90,22 +127,19 @@ __device__ __forceinline__ void stage_block(const CsrArgs<V>& A, const T* __rest
             s_val[k - e0] = A.val[k];
             s_x[k - e0] = gather<MASKED>(A, x, A.col[k]);
         }
-        const int4* cols4 = reinterpret_cast<const int4*>(A.col + a0);
         const int base = a0 - e0;
 #pragma unroll 2
         for (int g = tid; g < groups; g += THREADS) {
-            const int4 c = __ldg(cols4 + g);
+            int c[4];
+            Col4<int>::load(A.col + a0 + 4 * g, 0, c);
             V v[4];
             Vec4<V>::load(A.val + a0 + 4 * g, v);
             const int k = base + 4 * g;
-            s_x[k + 0] = gather<MASKED>(A, x, c.x);
-            s_x[k + 1] = gather<MASKED>(A, x, c.y);
-            s_x[k + 2] = gather<MASKED>(A, x, c.z);
-            s_x[k + 3] = gather<MASKED>(A, x, c.w);
-            s_val[k + 0] = v[0];
-            s_val[k + 1] = v[1];
-            s_val[k + 2] = v[2];
-            s_val[k + 3] = v[3];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                s_x[k + u] = gather<MASKED>(A, x, c[u]);
+                s_val[k + u] = v[u];
+            }
         }
     } else {
         for (int k = e0 + tid; k < e1; k += THREADS) {
@@ -117,7 +151,7 @@ __device__ __forceinline__ void stage_block(const CsrArgs<V>& A, const T* __rest
 
 // Row sums of every row block assigned to this CTA (persistent loop over blocks).
 template <typename T, typename V, int THREADS, int TILE, bool MASKED, typename Op>
-__device__ __forceinline__ void stream_rows(const CsrArgs<V>& A, const T* __restrict__ x, Op& op) {
+__device__ __forceinline__ void stream_rows(const CsrArgs<V, int>& A, const T* __restrict__ x, Op& op) {
     __shared__ __align__(16) V s_val[TILE];
     __shared__ __align__(16) T s_x[TILE];
     __shared__ T s_red[32];
@@ -128,32 +162,36 @@ __device__ __forceinline__ void stream_rows(const CsrArgs<V>& A, const T* __rest
             stage_block<T, V, THREADS, MASKED>(A, x, e0, e1, s_val, s_x);
             __syncthreads();
             for (int r = r0 + threadIdx.x; r < r1; r += THREADS) {
+                const auto pre = op.pre(r);
                 const int k0 = A.rowptr[r] - e0, k1 = A.rowptr[r + 1] - e0;
                 T sum = T(0);
                 if (!MASKED || A.mask[r] < A.threshold)
                     for (int k = k0; k < k1; ++k) sum = fma(static_cast<T>(s_val[k]), s_x[k], sum);
-                op(r, sum);
+                op.post(r, pre, sum);
             }
             __syncthreads();
         } else {
             // one long row: the whole CTA reduces it (fixed order)
+            const auto pre = op.pre(r0);
             T sum = T(0);
             const bool active = !MASKED || A.mask[r0] < A.threshold;
             if (active)
                 for (int k = e0 + threadIdx.x; k < e1; k += THREADS)
                     sum = fma(static_cast<T>(A.val[k]), gather<MASKED>(A, x, A.col[k]), sum);
             sum = block_sum<T, THREADS>(sum, s_red);
-            if (threadIdx.x == 0) op(r0, sum);
+            if (threadIdx.x == 0) op.post(r0, pre, sum);
             __syncthreads();
         }
     }
 }
 
 // VS lanes per row.  Loop bounds are uniform per warp so the shuffles always see
-// all 32 lanes.
-template <typename T, typename V, int VS, int THREADS, bool MASKED, typename Op>
-__device__ __forceinline__ void vector_rows(const CsrArgs<V>& A, const T* __restrict__ x, Op& op) {
+// all 32 lanes.  Each lane issues the loads of UNROLL strided entries (a warp
+// instruction covers VS consecutive entries of 32/VS rows) before the FMA chain.
+template <typename T, typename V, typename CI, int VS, int THREADS, bool MASKED, typename Op>
+__device__ __forceinline__ void vector_rows(const CsrArgs<V, CI>& A, const T* __restrict__ x, Op& op) {
     constexpr int ROWS_PER_WARP = 32 / VS;
+    constexpr int UNROLL = VS <= 4 ? 8 : 4;
     const int lane = threadIdx.x & 31;
     const int sub = lane % VS;
     const long warpGlobal = (static_cast<long>(blockIdx.x) * THREADS + threadIdx.x) >> 5;
@@ -163,14 +201,12 @@ __device__ __forceinline__ void vector_rows(const CsrArgs<V>& A, const T* __rest
         const long rowL = g * ROWS_PER_WARP + lane / VS;
         const bool valid = rowL < A.nrows;
         const int r = valid ? static_cast<int>(rowL) : 0;
+        typename Op::Pre pre{};
+        if (valid && sub == 0) pre = op.pre(r);
         T sum = T(0);
         if (valid && (!MASKED || A.mask[r] < A.threshold)) {
-            // Issue the loads of UNROLL strided entries before the FMA chain so
-            // each lane keeps UNROLL value/index loads and gathers in flight.
-            constexpr int UNROLL = VS <= 4 ? 8 : 4;
             const int k1 = A.rowptr[r + 1];
-            int k = A.rowptr[r] + sub;
-            for (; k < k1; k += UNROLL * VS) {
+            for (int k = A.rowptr[r] + sub; k < k1; k += UNROLL * VS) {
                 V v[UNROLL];
                 int c[UNROLL];
 #pragma unroll
@@ -178,7 +214,7 @@ __device__ __forceinline__ void vector_rows(const CsrArgs<V>& A, const T* __rest
                     const int kk = k + u * VS;
                     const bool in = kk < k1;
                     v[u] = in ? __ldg(A.val + kk) : V(0);
-                    c[u] = in ? __ldg(A.col + kk) : -1;
+                    c[u] = in ? Col4<CI>::one(A.col + kk, r) : -1;
                 }
                 T xv[UNROLL];
 #pragma unroll
@@ -189,17 +225,18 @@ __device__ __forceinline__ void vector_rows(const CsrArgs<V>& A, const T* __rest
         }
 #pragma unroll
         for (int offset = VS / 2; offset > 0; offset >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, offset, VS);
-        if (valid && sub == 0) op(r, sum);
+        if (valid && sub == 0) op.post(r, pre, sum);
     }
 }
 
 // Row pass with the schedule fixed at compile time: KERNEL = 1 (stream) or VS.
-template <int KERNEL, typename T, typename V, bool MASKED, typename Op>
-__device__ __forceinline__ void csr_rows(const CsrArgs<V>& A, const T* __restrict__ x, Op& op) {
+template <int KERNEL, typename T, typename V, bool MASKED, typename CI = int, typename Op>
+__device__ __forceinline__ void csr_rows(const CsrArgs<V, CI>& A, const T* __restrict__ x, Op& op) {
     if constexpr (KERNEL == 1) {
+        static_assert(std::is_same<CI, int>::value, "the stream schedule reads int32 columns");
         stream_rows<T, V, kStreamThreads, kStreamTile, MASKED>(A, x, op);
     } else {
-        vector_rows<T, V, KERNEL, kVectorThreads, MASKED>(A, x, op);
+        vector_rows<T, V, CI, KERNEL, kVectorThreads, MASKED>(A, x, op);
     }
 }
 
@@ -240,7 +277,7 @@ struct ciecu_csr_s {
 
     template <typename V>
     ciecu::CsrArgs<V> args(const uint16_t* mask = nullptr, uint16_t threshold = 0) const {
-        return ciecu::CsrArgs<V>{rowptr, col, static_cast<const V*>(val), rows, d_blocks, nblocks,
+        return ciecu::CsrArgs<V>{rowptr, col, static_cast<const V*>(val), rows, nnz, d_blocks, nblocks,
                                  mask, threshold, aligned16};
     }
 };

@@ -563,7 +563,9 @@ class MixedPrecisionCG(LinearOperator):
     def info(self):
         c, v = ctypes.c_int(), ctypes.c_int()
         call("ciecu_mixed_info", self._solver, ctypes.byref(c), ctypes.byref(v))
-        return {"compressed_columns": bool(c.value), "lanes_per_row": v.value}
+        e = ctypes.c_int64()
+        call("ciecu_mixed_padded_entries", self._solver, ctypes.byref(e))
+        return {"compressed_columns": bool(c.value), "format": "sell-32", "padded_entries": e.value}
 
     def set_graph_chunk(self, iterations):
         call("ciecu_mixed_set_graph_chunk", self._solver, int(iterations))

@@ -39,8 +39,10 @@ typedef struct ciecu_mixed_statistics {
     double trueRelativeResidual;  /* = relativeResidual */
 } ciecu_mixed_statistics;
 
-/* Builds the FP32 value copy, the (16-bit or int32) column copy and the FP32
- * inverse diagonal from the FP64 matrix and its inverse diagonal (both device).
+/* Builds the FP32 inner matrix -- SELL-32 layout (slices of 32 rows, one thread
+ * per row, coalesced loads), FP32 values, 16-bit row-relative or int32 columns --
+ * and the FP32 inverse diagonal from the FP64 matrix and its inverse diagonal
+ * (both device).
  * settings: iteration limit (FP32 inner iterations) and tolerances. */
 int ciecu_mixed_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_statistics settings,
                        ciecu_mixed_options options, ciecu_mixed* out);
@@ -50,6 +52,8 @@ int ciecu_mixed_set_graph_chunk(ciecu_mixed solver, int iterations);
 /* d_out = A32 d_in: the solver's FP32 inner operator (FP32 values, 16-bit or
  * int32 columns) on its own, e.g. to time it. */
 int ciecu_mixed_apply_f32(ciecu_mixed solver, const float* d_in, float* d_out);
+/* Stored entries of the SELL-32 inner matrix, padding included (>= nnz). */
+int ciecu_mixed_padded_entries(ciecu_mixed solver, int64_t* h_entries);
 /* out = inScale*out + outScale*x, x the refined solution (initial guess = out). */
 int ciecu_mixed_product(ciecu_mixed solver, double inScale, const double* d_in, double outScale, double* d_out,
                         ciecu_mixed_statistics* h_stats);
