@@ -229,9 +229,15 @@ def main():
     it64 = cg.getStats().iterationCount
     mst = mixed.getStats()
     if args.profile:
+        from cie_b200.linalg import _ptr
+        lib = _lib.load()
+        x32, y32 = xmx.float(), torch.empty(n, dtype=torch.float32, device="cuda")
         for _ in range(args.steps):
             solve_mixed()
             solve_fp64()
+            for _ in range(3):
+                lib.ciecu_mixed_apply_f32(mixed._solver, _ptr(x32), _ptr(y32))
+                lib.ciecu_csr_spmv_f64(A.csr.handle, 0.0, _ptr(x64), 1.0, _ptr(prob.rhs.clone()))
         torch.cuda.synchronize()
         print(json.dumps({"profile": True, "cells": cells, "fp64_iterations": it64,
                           "mixed_inner": mst.innerIterations, "mixed_refinements": mst.refinements}), flush=True)

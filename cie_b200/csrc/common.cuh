@@ -126,6 +126,17 @@ __device__ __forceinline__ T combine(T inScale, T old, T outScale, T sum) {
     return inScale * old + outScale * sum;
 }
 
+// Largest grid of `kernel` whose blocks are all resident at once (one wave),
+// capped by the blocks the work needs; cached per kernel.
+int resident_blocks(const void* kernel, int threads, size_t smem);
+
+template <typename K>
+inline int fit_grid(K* kernel, int threads, long needBlocks, size_t smem = 0) {
+    const long cap = static_cast<long>(resident_blocks(reinterpret_cast<const void*>(kernel), threads, smem));
+    long g = needBlocks < cap ? needBlocks : cap;
+    return static_cast<int>(g < 1 ? 1 : g);
+}
+
 inline int grid_for(long n, int threads, int perSM = 8) {
     long blocks = (n + threads - 1) / threads;
     const long cap = static_cast<long>(sm_count()) * perSM;

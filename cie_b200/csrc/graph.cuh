@@ -7,7 +7,19 @@
 
 #include "common.cuh"
 
+#include <cstdlib>
+
 namespace ciecu {
+
+// CIECU_GRAPH_LOOP=0 selects the plain captured-chunk graphs (same kernels,
+// host-polled) -- profilers cannot attribute kernels inside conditional graphs.
+inline bool device_loop_enabled() {
+    static const bool enabled = [] {
+        const char* v = std::getenv("CIECU_GRAPH_LOOP");
+        return !(v && v[0] == '0');
+    }();
+    return enabled;
+}
 
 template <typename F>
 int build_while_graph(cudaStream_t st, F&& body, cudaGraphExec_t* exec) {

@@ -53,11 +53,13 @@ struct MixedScalars {
     long long chunkIter, chunkLimit;  // iterations of the current graph launch / per launch
 };
 
-__device__ __forceinline__ void set_cond(bool useCond, cudaGraphConditionalHandle cond, unsigned value) {
-    if (useCond) cudaGraphSetConditional(cond, value);
+// COND selects the instantiation with conditional-node calls (device loop) or
+// without any (plain captured graphs, profilable).
+template <bool COND>
+__device__ __forceinline__ void set_cond(cudaGraphConditionalHandle cond, unsigned value) {
+    if constexpr (COND) cudaGraphSetConditional(cond, value);
 }
 
-constexpr int kUnroll = 9;  // entries per thread in flight in the SELL row loop
 
 // ---- SELL-32 FP32 matrix ------------------------------------------------------
 
@@ -78,7 +80,7 @@ __global__ void sell_len_kernel(int nrows, const int* __restrict__ rowptr, int* 
 }
 
 // Copies row r into its slice (values in FP32, columns as 16-bit row offsets or
-// int32) and zero-fills its padding.
+// int32) and zero-fills its padding; layout of sell.cuh.
 template <typename CI>
 __global__ void sell_fill_kernel(int nrows, const int* __restrict__ rowptr, const int* __restrict__ col,
                                  const double* __restrict__ val, const int* __restrict__ sliceLen,
@@ -86,12 +88,12 @@ __global__ void sell_fill_kernel(int nrows, const int* __restrict__ rowptr, cons
                                  CI* __restrict__ scol, unsigned short* __restrict__ rowLen, unsigned* tooFar) {
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nrows; r += gridDim.x * blockDim.x) {
         const int s = r >> 5;
-        const int padded = abs(sliceLen[s]);
+        const int padded = ((abs(sliceLen[s]) + 3) >> 2) << 2;
         const int k0 = rowptr[r], len = rowptr[r + 1] - k0;
         rowLen[r] = static_cast<unsigned short>(len);
-        const long long base = sliceStart[s] + (r & 31);
+        const long long base = sliceStart[s] + 4 * (r & 31);
         for (int j = 0; j < padded; ++j) {
-            const long long idx = base + 32LL * j;
+            const long long idx = base + 128LL * (j >> 2) + (j & 3);
             if (j < len) {
                 sval[idx] = static_cast<float>(val[k0 + j]);
                 const int c = col[k0 + j];
@@ -118,11 +120,11 @@ struct StoreOp {
     __device__ __forceinline__ void post(int r, NoPre, float sum) const { y[r] = sum; }
 };
 
-template <typename CI>
+template <int U, typename CI>
 __global__ void __launch_bounds__(kT) mixed_apply_kernel(SellArgs<float, CI> A, const float* __restrict__ x,
                                                          float* __restrict__ y) {
     StoreOp op{y};
-    sell_rows<kUnroll, float, float, CI>(A, x, op);
+    sell_rows<U, float, float, CI>(A, x, op);
 }
 
 // M1: q = A32 p, p^T q (FP64 accumulation), alpha.
@@ -138,24 +140,23 @@ struct MixedPqOp {
     }
 };
 
-template <typename CI>
+template <int U, typename CI, bool COND>
 __global__ void __launch_bounds__(kT) mixed_spmv_kernel(SellArgs<float, CI> A, const float* __restrict__ p,
                                                         float* __restrict__ q, MixedScalars* s, double* partials,
-                                                        unsigned* counter, cudaGraphConditionalHandle loop,
-                                                        bool useCond) {
+                                                        unsigned* counter, cudaGraphConditionalHandle loop) {
     if (*reinterpret_cast<volatile int*>(&s->done)) {
-        if (blockIdx.x == 0 && threadIdx.x == 0) set_cond(useCond, loop, 0);
+        if (blockIdx.x == 0 && threadIdx.x == 0) set_cond<COND>(loop, 0);
         return;
     }
     MixedPqOp op{p, q, 0.0};
-    sell_rows<kUnroll, float, float, CI>(A, p, op);
+    sell_rows<U, float, float, CI>(A, p, op);
     double mine[1] = {op.acc}, tot[1];
     if (grid_reduce_last<1, kT>(mine, partials, counter, tot) && threadIdx.x == 0) {
         s->pq = tot[0];
         if (!(0.0 < tot[0])) {
             s->done = 3;
             s->error = CIECU_ERR_BREAKDOWN;
-            set_cond(useCond, loop, 0);
+            set_cond<COND>(loop, 0);
         } else {
             s->alpha = s->rz / tot[0];
         }
@@ -163,16 +164,17 @@ __global__ void __launch_bounds__(kT) mixed_spmv_kernel(SellArgs<float, CI> A, c
 }
 
 // M2: x32 += alpha p; r32 -= alpha q; rr, rz in FP64; replacement decision.
+template <bool COND>
 __global__ void __launch_bounds__(kT) mixed_update_kernel(long n, float* __restrict__ x, float* __restrict__ r,
                                                           const float* __restrict__ p, const float* __restrict__ q,
                                                           const float* __restrict__ dinv, MixedScalars* s,
                                                           double* partials, unsigned* counter,
                                                           cudaGraphConditionalHandle loop,
-                                                          cudaGraphConditionalHandle refine, bool useCond) {
+                                                          cudaGraphConditionalHandle refine) {
     if (*reinterpret_cast<volatile int*>(&s->done)) {
         if (blockIdx.x == 0 && threadIdx.x == 0) {
-            set_cond(useCond, loop, 0);
-            set_cond(useCond, refine, 0);
+            set_cond<COND>(loop, 0);
+            set_cond<COND>(refine, 0);
         }
         return;
     }
@@ -230,8 +232,8 @@ __global__ void __launch_bounds__(kT) mixed_update_kernel(long n, float* __restr
             s->rz = tot[1];
         }
         s->chunkIter += 1;
-        set_cond(useCond, refine, update ? 1u : 0u);
-        set_cond(useCond, loop, s->chunkIter < s->chunkLimit ? 1u : 0u);
+        set_cond<COND>(refine, update ? 1u : 0u);
+        set_cond<COND>(loop, s->chunkIter < s->chunkLimit ? 1u : 0u);
     }
 }
 
@@ -267,11 +269,11 @@ struct ResidualOp {
 
 // R2 (and set-up): r = b - A64 x64 in FP64; r32 = float(r); ||r||^2 and r32^T z32
 // in FP64.  INIT: first residual of a solve.
-template <int KERNEL, bool INIT>
+template <int KERNEL, bool INIT, bool COND>
 __global__ void __launch_bounds__(csr_threads<KERNEL>())
     mixed_residual_kernel(CsrArgs<double> A, const double* __restrict__ b, const double* __restrict__ x64,
                           const float* __restrict__ dinv, float* __restrict__ r32, MixedScalars* s,
-                          double* partials, unsigned* counter, cudaGraphConditionalHandle loop, bool useCond) {
+                          double* partials, unsigned* counter, cudaGraphConditionalHandle loop) {
     if (!INIT && !*reinterpret_cast<volatile int*>(&s->update)) return;
     constexpr int T = csr_threads<KERNEL>();
     ResidualOp op{b, dinv, r32, 0.0, 0.0};
@@ -325,7 +327,7 @@ __global__ void __launch_bounds__(csr_threads<KERNEL>())
             }
             s->rz = tot[1];
         }
-        if (s->done) set_cond(useCond, loop, 0);
+        if (s->done) set_cond<COND>(loop, 0);
     }
 }
 
@@ -386,6 +388,7 @@ struct ciecu_mixed_s {
     ciecu_mixed_options options{};
     long n = 0;
     bool idx16 = false;
+    int unroll = 2;  // SELL groups of four entries in flight per thread (autotuned)
     // SELL-32 inner matrix
     int nslices = 0;
     long long paddedEntries = 0;
@@ -414,34 +417,48 @@ struct ciecu_mixed_s {
 namespace ciecu {
 namespace {
 
-int sell_grid(const ciecu_mixed_s* M) { return grid_for(M->n, kT, 8); }
+// Calls f(std::integral_constant<int, U>) for the group unroll U in {1, 2, 4}.
+template <typename F>
+int with_unroll(int u, F&& f) {
+    switch (u) {
+        case 1: return f(std::integral_constant<int, 1>{});
+        case 4: return f(std::integral_constant<int, 4>{});
+        default: return f(std::integral_constant<int, 2>{});
+    }
+}
 
 // One inner iteration.  With conditional nodes (useCond) the refinement pair
 // R1/R2 sits under IF(refine); otherwise it is launched unconditionally and
 // returns at once unless M2 requested a replacement.
-int launch_inner(ciecu_mixed_s* M, cudaStream_t st, cudaGraph_t root, cudaGraphConditionalHandle loop,
-                 bool useCond) {
-    const int gridA = sell_grid(M);
-    const int gridV = grid_for((M->n + 3) / 4, kT, 8);
+template <bool COND>
+int launch_inner(ciecu_mixed_s* M, cudaStream_t st, cudaGraph_t root, cudaGraphConditionalHandle loop) {
+    constexpr bool useCond = COND;
+    const long needA = (M->n + kT - 1) / kT;
+    const long needV = ((M->n + 3) / 4 + kT - 1) / kT;
     ciecu_csr_s* A = M->A;
     cudaGraphConditionalHandle refine = 0;
     if (useCond) CIECU_CUDA(cudaGraphConditionalHandleCreate(&refine, root, 0, cudaGraphCondAssignDefault));
-    if (M->idx16)
-        mixed_spmv_kernel<short><<<gridA, kT, 0, st>>>(M->a16, M->p32, M->q32, M->d_s, M->d_partials, M->d_counter,
-                                                       loop, useCond);
-    else
-        mixed_spmv_kernel<int><<<gridA, kT, 0, st>>>(M->a32, M->p32, M->q32, M->d_s, M->d_partials, M->d_counter,
-                                                     loop, useCond);
-    mixed_update_kernel<<<gridV, kT, 0, st>>>(M->n, M->x32, M->r32, M->p32, M->q32, M->dinv32, M->d_s, M->d_partials,
-                                              M->d_counter, loop, refine, useCond);
+    CIECU_TRY(with_unroll(M->unroll, [&](auto uu) -> int {
+        constexpr int U = decltype(uu)::value;
+        if (M->idx16)
+            mixed_spmv_kernel<U, short, COND><<<fit_grid(mixed_spmv_kernel<U, short, COND>, kT, needA), kT, 0, st>>>(
+                M->a16, M->p32, M->q32, M->d_s, M->d_partials, M->d_counter, loop);
+        else
+            mixed_spmv_kernel<U, int, COND><<<fit_grid(mixed_spmv_kernel<U, int, COND>, kT, needA), kT, 0, st>>>(
+                M->a32, M->p32, M->q32, M->d_s, M->d_partials, M->d_counter, loop);
+        return CIECU_OK;
+    }));
+    mixed_update_kernel<COND><<<fit_grid(mixed_update_kernel<COND>, kT, needV), kT, 0, st>>>(M->n, M->x32, M->r32, M->p32, M->q32, M->dinv32, M->d_s,
+                                                    M->d_partials, M->d_counter, loop, refine);
     auto refinement = [&](cudaStream_t s2) -> int {
-        mixed_fold_kernel<<<grid_for(M->n, kT, 8), kT, 0, s2>>>(M->n, M->x64, M->x32, M->d_s);
-        const int gridR = csr_grid(A, A->kernel);
+        mixed_fold_kernel<<<fit_grid(mixed_fold_kernel, kT, needA), kT, 0, s2>>>(M->n, M->x64, M->x32, M->d_s);
+        const int needR = csr_grid(A, A->kernel);
         return with_schedule(A->kernel, [&](auto k) -> int {
             constexpr int K = decltype(k)::value;
-            mixed_residual_kernel<K, false><<<gridR, csr_threads<K>(), 0, s2>>>(
-                A->args<double>(), M->b, M->x64, M->dinv32, M->r32, M->d_s, M->d_partials, M->d_counter, loop,
-                useCond);
+            mixed_residual_kernel<K, false, COND><<<fit_grid(mixed_residual_kernel<K, false, COND>, csr_threads<K>(),
+                                                             needR),
+                                                    csr_threads<K>(), 0, s2>>>(
+                A->args<double>(), M->b, M->x64, M->dinv32, M->r32, M->d_s, M->d_partials, M->d_counter, loop);
             return CIECU_OK;
         });
     };
@@ -449,7 +466,8 @@ int launch_inner(ciecu_mixed_s* M, cudaStream_t st, cudaGraph_t root, cudaGraphC
         CIECU_TRY(capture_if(st, M->side, refine, refinement));
     else
         CIECU_TRY(refinement(st));
-    mixed_direction_kernel<<<gridV, kT, 0, st>>>(M->n, M->p32, M->r32, M->dinv32, M->d_s);
+    mixed_direction_kernel<<<fit_grid(mixed_direction_kernel, kT, needV), kT, 0, st>>>(M->n, M->p32, M->r32,
+                                                                                       M->dinv32, M->d_s);
     CIECU_CHECK_LAUNCH("mixed inner iteration");
     return CIECU_OK;
 }
@@ -461,8 +479,10 @@ int build_mixed_graph(ciecu_mixed_s* M) {
         M->graph = nullptr;
     }
     cudaStream_t st = M->A->space->stream;
-    int status = build_while_graph(st, [&](cudaGraph_t root, cudaGraphConditionalHandle loop) {
-        return launch_inner(M, st, root, loop, true);
+    int status = CIECU_ERR_ARGUMENT;
+    if (device_loop_enabled())
+        status = build_while_graph(st, [&](cudaGraph_t root, cudaGraphConditionalHandle loop) {
+        return launch_inner<true>(M, st, root, loop);
     }, &M->graph);
     if (status == CIECU_OK) {
         M->deviceLoop = true;
@@ -474,7 +494,7 @@ int build_mixed_graph(ciecu_mixed_s* M) {
     cudaGraph_t g = nullptr;
     CIECU_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     status = CIECU_OK;
-    for (int i = 0; i < M->chunk && status == CIECU_OK; ++i) status = launch_inner(M, st, nullptr, 0, false);
+    for (int i = 0; i < M->chunk && status == CIECU_OK; ++i) status = launch_inner<false>(M, st, nullptr, 0);
     cudaError_t e = cudaStreamEndCapture(st, &g);
     if (status != CIECU_OK) {
         if (g) cudaGraphDestroy(g);
@@ -552,7 +572,7 @@ int ciecu_mixed_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_sta
         ciecu_mixed_destroy(M);
         return fail(CIECU_ERR_ARGUMENT, "mixed_create: rows longer than 65535 entries are not supported");
     }
-    for (int sl = 0; sl < M->nslices; ++sl) starts[sl + 1] = starts[sl] + 32LL * std::abs(lens[sl]);
+    for (int sl = 0; sl < M->nslices; ++sl) starts[sl + 1] = starts[sl] + 128LL * ((std::abs(lens[sl]) + 3) / 4);
     M->paddedEntries = starts.back();
     e = cudaMemcpyAsync(M->sliceStart, starts.data(), sizeof(long long) * starts.size(), cudaMemcpyHostToDevice, st);
     const size_t padded = static_cast<size_t>(std::max<long long>(1, M->paddedEntries));
@@ -605,6 +625,38 @@ int ciecu_mixed_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_sta
                                     static_cast<const short*>(M->col32or16)};
     M->a32 = SellArgs<float, int>{static_cast<int>(M->n), M->sliceLen, M->sliceStart, M->rowLen, M->val32,
                                   static_cast<const int*>(M->col32or16)};
+    // Autotune the group unroll of the inner operator on the solver's own matrix
+    // (scratch vectors p32 -> q32).
+    if (M->n > 0) {
+        e = cudaMemsetAsync(M->p32, 0, sizeof(float) * M->n, st);
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        if (e == cudaSuccess) e = cudaEventCreate(&e0);
+        if (e == cudaSuccess) e = cudaEventCreate(&e1);
+        float best = 1e30f;
+        int bestU = 2;
+        for (int u : {1, 2, 4}) {
+            if (e != cudaSuccess) break;
+            M->unroll = u;
+            for (int rep = 0; rep < 2; ++rep) ciecu_mixed_apply_f32(M, M->p32, M->q32);
+            cudaEventRecord(e0, st);
+            for (int rep = 0; rep < 5; ++rep) ciecu_mixed_apply_f32(M, M->p32, M->q32);
+            cudaEventRecord(e1, st);
+            e = cudaEventSynchronize(e1);
+            float ms = 0.f;
+            if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+            if (e == cudaSuccess && ms < best) {
+                best = ms;
+                bestU = u;
+            }
+        }
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        if (e != cudaSuccess) {
+            ciecu_mixed_destroy(M);
+            return cuda_fail(e, "mixed_create: autotune");
+        }
+        M->unroll = bestU;
+    }
     *out = M;
     return CIECU_OK;
 }
@@ -636,7 +688,7 @@ int ciecu_mixed_destroy(ciecu_mixed M) {
 int ciecu_mixed_info(ciecu_mixed M, int* compressedColumns, int* lanesPerRow) {
     CIECU_REQUIRE(M, "mixed_info: null solver");
     if (compressedColumns) *compressedColumns = M->idx16 ? 1 : 0;
-    if (lanesPerRow) *lanesPerRow = 1;  // SELL-32: one thread per row
+    if (lanesPerRow) *lanesPerRow = M->unroll;  // SELL: one thread per row, `unroll` groups of 4 in flight
     return CIECU_OK;
 }
 
@@ -644,11 +696,17 @@ int ciecu_mixed_apply_f32(ciecu_mixed M, const float* d_in, float* d_out) {
     CIECU_REQUIRE(M && (M->n == 0 || (d_in && d_out)), "mixed_apply_f32: null argument");
     if (M->n == 0) return CIECU_OK;
     cudaStream_t st = M->A->space->stream;
-    const int grid = sell_grid(M);
-    if (M->idx16)
-        mixed_apply_kernel<short><<<grid, kT, 0, st>>>(M->a16, d_in, d_out);
-    else
-        mixed_apply_kernel<int><<<grid, kT, 0, st>>>(M->a32, d_in, d_out);
+    const long need = (M->n + kT - 1) / kT;
+    CIECU_TRY(with_unroll(M->unroll, [&](auto uu) -> int {
+        constexpr int U = decltype(uu)::value;
+        if (M->idx16)
+            mixed_apply_kernel<U, short><<<fit_grid(mixed_apply_kernel<U, short>, kT, need), kT, 0, st>>>(M->a16, d_in,
+                                                                                                       d_out);
+        else
+            mixed_apply_kernel<U, int><<<fit_grid(mixed_apply_kernel<U, int>, kT, need), kT, 0, st>>>(M->a32, d_in,
+                                                                                                   d_out);
+        return CIECU_OK;
+    }));
     count_launch();
     CIECU_CHECK_LAUNCH("mixed_apply_kernel");
     return CIECU_OK;
@@ -695,14 +753,17 @@ int ciecu_mixed_product(ciecu_mixed M, double inScale, const double* d_in, doubl
         CIECU_CUDA(cudaMemcpyAsync(M->d_s, M->h_s, sizeof(MixedScalars), cudaMemcpyHostToDevice, st));
         CIECU_CUDA(cudaMemsetAsync(M->x32, 0, sizeof(float) * n, st));
         CIECU_CUDA(cudaMemsetAsync(M->p32, 0, sizeof(float) * n, st));
-        const int gridR = csr_grid(A, A->kernel);
+        const int needR = csr_grid(A, A->kernel);
         CIECU_TRY(with_schedule(A->kernel, [&](auto k) -> int {
             constexpr int K = decltype(k)::value;
-            mixed_residual_kernel<K, true><<<gridR, csr_threads<K>(), 0, st>>>(
-                A->args<double>(), d_in, M->x64, M->dinv32, M->r32, M->d_s, M->d_partials, M->d_counter, 0, false);
+            mixed_residual_kernel<K, true, false><<<fit_grid(mixed_residual_kernel<K, true, false>, csr_threads<K>(),
+                                                             needR),
+                                                    csr_threads<K>(), 0, st>>>(
+                A->args<double>(), d_in, M->x64, M->dinv32, M->r32, M->d_s, M->d_partials, M->d_counter, 0);
             return CIECU_OK;
         }));
-        mixed_direction_kernel<<<grid_for((n + 3) / 4, kT, 8), kT, 0, st>>>(n, M->p32, M->r32, M->dinv32, M->d_s);
+        mixed_direction_kernel<<<fit_grid(mixed_direction_kernel, kT, ((n + 3) / 4 + kT - 1) / kT), kT, 0, st>>>(
+            n, M->p32, M->r32, M->dinv32, M->d_s);
         count_launch(2);
         CIECU_CHECK_LAUNCH("mixed set-up");
         CIECU_TRY(build_mixed_graph(M));

@@ -75,17 +75,20 @@ struct PqOp {
     }
 };
 
-// Ends the device-side loop (graph WHILE node) when `cond` is a live handle.
-__device__ __forceinline__ void set_loop(bool useCond, cudaGraphConditionalHandle cond, unsigned value) {
-    if (useCond) cudaGraphSetConditional(cond, value);
+// Ends the device-side loop (graph WHILE node).  COND is a template parameter so
+// that the instantiation used by the plain captured graphs contains no
+// conditional-node call at all (profilers skip kernels that have one).
+template <bool COND>
+__device__ __forceinline__ void set_loop(cudaGraphConditionalHandle cond, unsigned value) {
+    if constexpr (COND) cudaGraphSetConditional(cond, value);
 }
 
-template <int KERNEL>
+template <int KERNEL, bool COND>
 __global__ void __launch_bounds__(csr_threads<KERNEL>())
     pcg_spmv_kernel(CsrArgs<double> A, const double* __restrict__ p, double* __restrict__ q, PcgScalars* s,
-                    double* partials, unsigned* counter, cudaGraphConditionalHandle cond, bool useCond) {
+                    double* partials, unsigned* counter, cudaGraphConditionalHandle cond) {
     if (*reinterpret_cast<volatile int*>(&s->done)) {
-        if (blockIdx.x == 0 && threadIdx.x == 0) set_loop(useCond, cond, 0);
+        if (blockIdx.x == 0 && threadIdx.x == 0) set_loop<COND>(cond, 0);
         return;
     }
     constexpr int T = csr_threads<KERNEL>();
@@ -99,7 +102,7 @@ __global__ void __launch_bounds__(csr_threads<KERNEL>())
             s->error = CIECU_ERR_BREAKDOWN;
             s->errorKind = 2;
             s->errorIter = s->iter;
-            set_loop(useCond, cond, 0);
+            set_loop<COND>(cond, 0);
         } else {
             s->alpha = s->rz / tot[0];
         }
@@ -108,14 +111,14 @@ __global__ void __launch_bounds__(csr_threads<KERNEL>())
 
 // K2: x, r update; z; rr, rz; beta and the stopping test (:154-185).
 // Two elements per thread with 16-byte loads (all operands 16-byte aligned).
-template <bool PRECOND>
+template <bool PRECOND, bool COND>
 __global__ void __launch_bounds__(kT) pcg_update_kernel(long n, double* __restrict__ x, double* __restrict__ r,
                                                         const double* __restrict__ p, const double* __restrict__ q,
                                                         const double* __restrict__ dinv, PcgScalars* s,
                                                         double* partials, unsigned* counter,
-                                                        cudaGraphConditionalHandle cond, bool useCond) {
+                                                        cudaGraphConditionalHandle cond) {
     if (*reinterpret_cast<volatile int*>(&s->done)) {
-        if (blockIdx.x == 0 && threadIdx.x == 0) set_loop(useCond, cond, 0);
+        if (blockIdx.x == 0 && threadIdx.x == 0) set_loop<COND>(cond, 0);
         return;
     }
     const double alpha = s->alpha;
@@ -165,7 +168,7 @@ __global__ void __launch_bounds__(kT) pcg_update_kernel(long n, double* __restri
             if (s->iter >= s->maxIter) s->done = 2;
         }
         s->chunkIter += 1;
-        set_loop(useCond, cond, (s->done == 0 && s->chunkIter < s->chunkLimit) ? 1u : 0u);
+        set_loop<COND>(cond, (s->done == 0 && s->chunkIter < s->chunkLimit) ? 1u : 0u);
     }
 }
 
@@ -245,25 +248,28 @@ struct ciecu_pcg_s {
 namespace ciecu {
 namespace {
 
-int launch_iteration(ciecu_pcg_s* S, cudaStream_t st, cudaGraphConditionalHandle cond, bool useCond) {
+template <bool COND>
+int launch_iteration(ciecu_pcg_s* S, cudaStream_t st, cudaGraphConditionalHandle cond) {
     ciecu_csr_s* A = S->A;
-    const int gridA = csr_grid(A, A->kernel);
-    const int gridV = grid_for((S->n + 1) / 2, kT, 8);
+    const int needA = csr_grid(A, A->kernel);
+    const long needV = ((S->n + 1) / 2 + kT - 1) / kT;
     const bool pre = S->dinv != nullptr;
     CIECU_TRY(with_schedule(A->kernel, [&](auto k) -> int {
         constexpr int K = decltype(k)::value;
-        pcg_spmv_kernel<K><<<gridA, csr_threads<K>(), 0, st>>>(A->args<double>(), S->p, S->q, S->d_s, S->d_partials,
-                                                               S->d_counter, cond, useCond);
+        pcg_spmv_kernel<K, COND><<<fit_grid(pcg_spmv_kernel<K, COND>, csr_threads<K>(), needA), csr_threads<K>(), 0,
+                                   st>>>(A->args<double>(), S->p, S->q, S->d_s, S->d_partials, S->d_counter, cond);
         return CIECU_OK;
     }));
     if (pre) {
-        pcg_update_kernel<true><<<gridV, kT, 0, st>>>(S->n, S->x, S->r, S->p, S->q, S->dinv, S->d_s, S->d_partials,
-                                                      S->d_counter, cond, useCond);
-        pcg_direction_kernel<true><<<gridV, kT, 0, st>>>(S->n, S->p, S->r, S->dinv, S->d_s);
+        pcg_update_kernel<true, COND><<<fit_grid(pcg_update_kernel<true, COND>, kT, needV), kT, 0, st>>>(
+            S->n, S->x, S->r, S->p, S->q, S->dinv, S->d_s, S->d_partials, S->d_counter, cond);
+        pcg_direction_kernel<true><<<fit_grid(pcg_direction_kernel<true>, kT, needV), kT, 0, st>>>(S->n, S->p, S->r,
+                                                                                                   S->dinv, S->d_s);
     } else {
-        pcg_update_kernel<false><<<gridV, kT, 0, st>>>(S->n, S->x, S->r, S->p, S->q, S->dinv, S->d_s, S->d_partials,
-                                                       S->d_counter, cond, useCond);
-        pcg_direction_kernel<false><<<gridV, kT, 0, st>>>(S->n, S->p, S->r, S->dinv, S->d_s);
+        pcg_update_kernel<false, COND><<<fit_grid(pcg_update_kernel<false, COND>, kT, needV), kT, 0, st>>>(
+            S->n, S->x, S->r, S->p, S->q, S->dinv, S->d_s, S->d_partials, S->d_counter, cond);
+        pcg_direction_kernel<false><<<fit_grid(pcg_direction_kernel<false>, kT, needV), kT, 0, st>>>(S->n, S->p, S->r,
+                                                                                                    S->dinv, S->d_s);
     }
     CIECU_CHECK_LAUNCH("pcg iteration");
     return CIECU_OK;
@@ -279,8 +285,10 @@ int build_graph(ciecu_pcg_s* S) {
         cudaGraphExecDestroy(S->graph);
         S->graph = nullptr;
     }
-    int status = build_while_graph(st, [&](cudaGraph_t, cudaGraphConditionalHandle cond) {
-        return launch_iteration(S, st, cond, true);
+    int status = CIECU_ERR_ARGUMENT;
+    if (device_loop_enabled())
+        status = build_while_graph(st, [&](cudaGraph_t, cudaGraphConditionalHandle cond) {
+        return launch_iteration<true>(S, st, cond);
     }, &S->graph);
     if (status == CIECU_OK) {
         S->deviceLoop = true;
@@ -292,7 +300,7 @@ int build_graph(ciecu_pcg_s* S) {
     cudaGraph_t g = nullptr;
     CIECU_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     status = CIECU_OK;
-    for (int i = 0; i < S->chunk && status == CIECU_OK; ++i) status = launch_iteration(S, st, 0, false);
+    for (int i = 0; i < S->chunk && status == CIECU_OK; ++i) status = launch_iteration<false>(S, st, 0);
     cudaError_t e = cudaStreamEndCapture(st, &g);
     if (status != CIECU_OK) {
         if (g) cudaGraphDestroy(g);
@@ -396,11 +404,13 @@ int ciecu_pcg_product(ciecu_pcg S, double inScale, const double* d_in, double ou
         // r = b - A x
         CIECU_CUDA(cudaMemcpyAsync(S->r, d_in, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
         CIECU_TRY(ciecu_csr_spmv_f64(A, 1.0, S->x, -1.0, S->r));
-        const int gridV = grid_for(n, kT, 8);
+        const long needV = (n + kT - 1) / kT;
         if (S->dinv)
-            pcg_init_kernel<true><<<gridV, kT, 0, st>>>(n, S->r, S->dinv, S->p, S->d_s, S->d_partials, S->d_counter);
+            pcg_init_kernel<true><<<fit_grid(pcg_init_kernel<true>, kT, needV), kT, 0, st>>>(
+                n, S->r, S->dinv, S->p, S->d_s, S->d_partials, S->d_counter);
         else
-            pcg_init_kernel<false><<<gridV, kT, 0, st>>>(n, S->r, S->dinv, S->p, S->d_s, S->d_partials, S->d_counter);
+            pcg_init_kernel<false><<<fit_grid(pcg_init_kernel<false>, kT, needV), kT, 0, st>>>(
+                n, S->r, S->dinv, S->p, S->d_s, S->d_partials, S->d_counter);
         count_launch();
         CIECU_CHECK_LAUNCH("pcg_init_kernel");
         CIECU_TRY(build_graph(S));

@@ -277,10 +277,12 @@ int ciecu_jacobi_f64(ciecu_csr csr, const double* d_inverse, const uint16_t* d_m
             CIECU_TRY(with_schedule(csr->kernel, [&](auto k) -> int {
                 constexpr int K = decltype(k)::value;
                 if (d_mask)
-                    jacobi_sweep_kernel<K, true><<<grid, csr_threads<K>(), 0, st>>>(
+                    jacobi_sweep_kernel<K, true><<<fit_grid(jacobi_sweep_kernel<K, true>, csr_threads<K>(), grid),
+                                                   csr_threads<K>(), 0, st>>>(
                         csr->args<double>(d_mask, threshold), d_in, d_inverse, relaxation, xa, xb);
                 else
-                    jacobi_sweep_kernel<K, false><<<grid, csr_threads<K>(), 0, st>>>(
+                    jacobi_sweep_kernel<K, false><<<fit_grid(jacobi_sweep_kernel<K, false>, csr_threads<K>(), grid),
+                                                    csr_threads<K>(), 0, st>>>(
                         csr->args<double>(), d_in, d_inverse, relaxation, xa, xb);
                 return CIECU_OK;
             }));
@@ -322,7 +324,7 @@ int ciecu_chebyshev_f64(ciecu_csr csr, const double* d_inverse, int degree, doub
         const double c2 = 2.0 * rhoNew / delta;
         CIECU_TRY(with_schedule(csr->kernel, [&](auto kk) -> int {
             constexpr int K = decltype(kk)::value;
-            cheb_step_kernel<K><<<grid, csr_threads<K>(), 0, st>>>(csr->args<double>(), d_inverse, c1, c2, r, da, db, x);
+            cheb_step_kernel<K><<<fit_grid(cheb_step_kernel<K>, csr_threads<K>(), grid), csr_threads<K>(), 0, st>>>(csr->args<double>(), d_inverse, c1, c2, r, da, db, x);
             return CIECU_OK;
         }));
         count_launch();
@@ -359,7 +361,7 @@ int ciecu_power_lambda_max_f64(ciecu_csr csr, const double* d_inverse, int itera
         count_launch();
         CIECU_TRY(with_schedule(csr->kernel, [&](auto kk) -> int {
             constexpr int K = decltype(kk)::value;
-            power_apply_kernel<K><<<grid, csr_threads<K>(), 0, st>>>(csr->args<double>(), d_inverse, v, w);
+            power_apply_kernel<K><<<fit_grid(power_apply_kernel<K>, csr_threads<K>(), grid), csr_threads<K>(), 0, st>>>(csr->args<double>(), d_inverse, v, w);
             return CIECU_OK;
         }));
         count_launch();

@@ -4,7 +4,9 @@
 #include "space.cuh"
 
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <string>
 
 namespace ciecu {
@@ -36,6 +38,21 @@ int sm_count() {
         return count > 0 ? count : kFallbackSMs;
     }();
     return cached;
+}
+
+int resident_blocks(const void* kernel, int threads, size_t smem) {
+    static std::mutex mutex;
+    static std::map<std::tuple<const void*, int, size_t>, int> cache;
+    const auto key = std::make_tuple(kernel, threads, smem);
+    std::lock_guard<std::mutex> lock(mutex);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    int perSM = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kernel, threads, smem) != cudaSuccess || perSM < 1)
+        perSM = 1;
+    const int blocks = perSM * sm_count();
+    cache[key] = blocks;
+    return blocks;
 }
 
 // ---- kernels -----------------------------------------------------------------

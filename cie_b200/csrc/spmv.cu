@@ -72,11 +72,13 @@ int launch_spmv(ciecu_csr_s* csr, int kernel, const uint16_t* mask, uint16_t thr
     return with_schedule(kernel, [&](auto k) -> int {
         constexpr int K = decltype(k)::value;
         if (mask)
-            spmv_kernel<K, T, T, true><<<grid, csr_threads<K>(), 0, csr->space->stream>>>(
-                csr->args<T>(mask, threshold), inScale, x, outScale, y);
+            spmv_kernel<K, T, T, true><<<fit_grid(spmv_kernel<K, T, T, true>, csr_threads<K>(), grid),
+                                         csr_threads<K>(), 0, csr->space->stream>>>(csr->args<T>(mask, threshold),
+                                                                                    inScale, x, outScale, y);
         else
-            spmv_kernel<K, T, T, false><<<grid, csr_threads<K>(), 0, csr->space->stream>>>(
-                csr->args<T>(), inScale, x, outScale, y);
+            spmv_kernel<K, T, T, false><<<fit_grid(spmv_kernel<K, T, T, false>, csr_threads<K>(), grid),
+                                          csr_threads<K>(), 0, csr->space->stream>>>(csr->args<T>(), inScale, x,
+                                                                                     outScale, y);
         count_launch();
         CIECU_CHECK_LAUNCH("spmv_kernel");
         return CIECU_OK;
@@ -140,15 +142,11 @@ int autotune(ciecu_csr_s* csr) {
 
 }  // namespace
 
+// Blocks a CSR row pass needs for the schedule (callers cap it with fit_grid).
 int csr_grid(const ciecu_csr_s* csr, int kernel) {
-    if (kernel == 1) {
-        const int cap = sm_count() * 6;
-        return std::max(1, std::min(csr->nblocks, cap));
-    }
+    if (kernel == 1) return std::max(1, csr->nblocks);
     const long rowsPerCta = static_cast<long>(kVectorThreads / 32) * (32 / kernel);
-    const long need = (csr->rows + rowsPerCta - 1) / rowsPerCta;
-    const long cap = static_cast<long>(sm_count()) * 8;
-    return static_cast<int>(std::max(1L, std::min(need, cap)));
+    return static_cast<int>(std::max(1L, (csr->rows + rowsPerCta - 1) / rowsPerCta));
 }
 
 int ensure_tuned(ciecu_csr_s* csr) {

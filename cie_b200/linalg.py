@@ -565,7 +565,8 @@ class MixedPrecisionCG(LinearOperator):
         call("ciecu_mixed_info", self._solver, ctypes.byref(c), ctypes.byref(v))
         e = ctypes.c_int64()
         call("ciecu_mixed_padded_entries", self._solver, ctypes.byref(e))
-        return {"compressed_columns": bool(c.value), "format": "sell-32", "padded_entries": e.value}
+        return {"compressed_columns": bool(c.value), "format": "sell-32x4", "padded_entries": e.value,
+                "group_unroll": v.value}
 
     def set_graph_chunk(self, iterations):
         call("ciecu_mixed_set_graph_chunk", self._solver, int(iterations))

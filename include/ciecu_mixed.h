@@ -47,7 +47,9 @@ typedef struct ciecu_mixed_statistics {
 int ciecu_mixed_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_statistics settings,
                        ciecu_mixed_options options, ciecu_mixed* out);
 int ciecu_mixed_destroy(ciecu_mixed solver);
-int ciecu_mixed_info(ciecu_mixed solver, int* compressedColumns, int* lanesPerRow);
+/* compressedColumns: 1 when the inner matrix stores 16-bit offsets; groupUnroll:
+ * groups of four entries each thread keeps in flight (chosen by the autotuner). */
+int ciecu_mixed_info(ciecu_mixed solver, int* compressedColumns, int* groupUnroll);
 int ciecu_mixed_set_graph_chunk(ciecu_mixed solver, int iterations);
 /* d_out = A32 d_in: the solver's FP32 inner operator (FP32 values, 16-bit or
  * int32 columns) on its own, e.g. to time it. */
