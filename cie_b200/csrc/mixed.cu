@@ -51,6 +51,8 @@ struct MixedScalars {
     long long iter, maxIter, refinements;
     int done, error, update, updateX, mode, pad;
     long long chunkIter, chunkLimit;  // iterations of the current graph launch / per launch
+    unsigned generation;              // grid-release counter of the fused update/direction kernel
+    int needDirection;                // R2 replaced r: the gated direction kernel must run
 };
 
 // COND selects the instantiation with conditional-node calls (device loop) or
@@ -237,6 +239,113 @@ __global__ void __launch_bounds__(kT) mixed_update_kernel(long n, float* __restr
     }
 }
 
+// M2+M3 fused (cooperative launch, all blocks resident): phase 1 is M2 and its
+// decision; the last block releases the grid; phase 2 is M3 unless a residual
+// replacement is due -- then the gated direction kernel runs after R2 instead.
+template <bool COND>
+__global__ void __launch_bounds__(kT) mixed_update_direction_kernel(long n, float* __restrict__ x,
+                                                                    float* __restrict__ r, float* __restrict__ p,
+                                                                    const float* __restrict__ q,
+                                                                    const float* __restrict__ dinv, MixedScalars* s,
+                                                                    double* partials, unsigned* counter,
+                                                                    cudaGraphConditionalHandle loop,
+                                                                    cudaGraphConditionalHandle refine) {
+    if (*reinterpret_cast<volatile int*>(&s->done)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            set_cond<COND>(loop, 0);
+            set_cond<COND>(refine, 0);
+        }
+        return;
+    }
+    const unsigned gen = *reinterpret_cast<volatile unsigned*>(&s->generation);
+    const float alpha = static_cast<float>(s->alpha);
+    double rr = 0.0, rz = 0.0;
+    const long quads = n >> 2;
+    const long stride = static_cast<long>(gridDim.x) * kT;
+    for (long j = static_cast<long>(blockIdx.x) * kT + threadIdx.x; j < quads; j += stride) {
+        const float4 pj = reinterpret_cast<const float4*>(p)[j];
+        const float4 qj = reinterpret_cast<const float4*>(q)[j];
+        const float4 dj = reinterpret_cast<const float4*>(dinv)[j];
+        float4 xj = reinterpret_cast<const float4*>(x)[j];
+        float4 rj = reinterpret_cast<const float4*>(r)[j];
+        xj.x = fmaf(alpha, pj.x, xj.x); xj.y = fmaf(alpha, pj.y, xj.y);
+        xj.z = fmaf(alpha, pj.z, xj.z); xj.w = fmaf(alpha, pj.w, xj.w);
+        rj.x = fmaf(-alpha, qj.x, rj.x); rj.y = fmaf(-alpha, qj.y, rj.y);
+        rj.z = fmaf(-alpha, qj.z, rj.z); rj.w = fmaf(-alpha, qj.w, rj.w);
+        reinterpret_cast<float4*>(x)[j] = xj;
+        reinterpret_cast<float4*>(r)[j] = rj;
+        rr = fma(double(rj.x), double(rj.x), rr); rr = fma(double(rj.y), double(rj.y), rr);
+        rr = fma(double(rj.z), double(rj.z), rr); rr = fma(double(rj.w), double(rj.w), rr);
+        rz = fma(double(rj.x), double(rj.x * dj.x), rz); rz = fma(double(rj.y), double(rj.y * dj.y), rz);
+        rz = fma(double(rj.z), double(rj.z * dj.z), rz); rz = fma(double(rj.w), double(rj.w * dj.w), rz);
+    }
+    if (blockIdx.x == 0 && threadIdx.x < (n & 3)) {
+        const long i = (quads << 2) + threadIdx.x;
+        x[i] = fmaf(alpha, p[i], x[i]);
+        const float ri = fmaf(-alpha, q[i], r[i]);
+        r[i] = ri;
+        rr = fma(double(ri), double(ri), rr);
+        rz = fma(double(ri), double(ri * dinv[i]), rz);
+    }
+    double mine[2] = {rr, rz}, tot[2];
+    if (grid_reduce_last<2, kT>(mine, partials, counter, tot)) {
+        if (threadIdx.x == 0) {
+            const double rnorm = sqrt(tot[0]);
+            s->sloppy = rnorm;
+            s->iter += 1;
+            bool update;
+            s->updateX = 0;
+            if (s->mode == 0) {
+                if (rnorm > s->maxrx) s->maxrx = rnorm;
+                if (rnorm > s->maxrr) s->maxrr = rnorm;
+                const bool updateX = rnorm < s->delta * s->maxrx;
+                update = updateX || rnorm < s->delta * s->maxrr;
+                s->updateX = updateX ? 1 : 0;
+            } else {
+                update = rnorm < s->delta * s->cycleStart;
+            }
+            update = update || rnorm < s->relTol * s->r0 || rnorm < s->absTol || s->iter >= s->maxIter;
+            s->needDirection = 0;
+            if (update) {
+                s->rzPending = tot[1];
+                s->update = 1;
+            } else {
+                s->beta = tot[1] / s->rz;
+                s->rz = tot[1];
+            }
+            s->chunkIter += 1;
+            set_cond<COND>(refine, update ? 1u : 0u);
+            set_cond<COND>(loop, s->chunkIter < s->chunkLimit ? 1u : 0u);
+            release_grid(&s->generation);
+        }
+        __syncthreads();
+    } else if (!wait_release(&s->generation, gen, kReleaseSpins)) {
+        if (threadIdx.x == 0) {
+            s->error = CIECU_ERR_TIMEOUT;
+            s->done = 3;
+            set_cond<COND>(loop, 0);
+            set_cond<COND>(refine, 0);
+        }
+        return;
+    }
+    if (*reinterpret_cast<volatile int*>(&s->update) || *reinterpret_cast<volatile int*>(&s->done)) return;
+    const float beta = static_cast<float>(*reinterpret_cast<volatile double*>(&s->beta));
+    for (long j = static_cast<long>(blockIdx.x) * kT + threadIdx.x; j < quads; j += stride) {
+        const float4 rj = reinterpret_cast<const float4*>(r)[j];
+        const float4 dj = reinterpret_cast<const float4*>(dinv)[j];
+        float4 pj = reinterpret_cast<const float4*>(p)[j];
+        pj.x = fmaf(beta, pj.x, rj.x * dj.x);
+        pj.y = fmaf(beta, pj.y, rj.y * dj.y);
+        pj.z = fmaf(beta, pj.z, rj.z * dj.z);
+        pj.w = fmaf(beta, pj.w, rj.w * dj.w);
+        reinterpret_cast<float4*>(p)[j] = pj;
+    }
+    if (blockIdx.x == 0 && threadIdx.x < (n & 3)) {
+        const long i = (quads << 2) + threadIdx.x;
+        p[i] = fmaf(beta, p[i], r[i] * dinv[i]);
+    }
+}
+
 // R1: x64 += x32; x32 = 0 (only when a replacement was requested).
 __global__ void __launch_bounds__(kT) mixed_fold_kernel(long n, double* __restrict__ x64, float* __restrict__ x32,
                                                         const MixedScalars* s) {
@@ -326,15 +435,19 @@ __global__ void __launch_bounds__(csr_threads<KERNEL>())
                 s->beta = 0.0;  // restart the inner CG: p = z
             }
             s->rz = tot[1];
+            s->needDirection = 1;
         }
         if (s->done) set_cond<COND>(loop, 0);
     }
 }
 
-// M3: p = z + beta p, z = D^-1 r (FP32).
+// M3: p = z + beta p, z = D^-1 r (FP32).  GATED: only after a residual
+// replacement (the fused kernel updates p in all other iterations).
+template <bool GATED>
 __global__ void __launch_bounds__(kT) mixed_direction_kernel(long n, float* __restrict__ p, const float* __restrict__ r,
                                                              const float* __restrict__ dinv, const MixedScalars* s) {
     if (*reinterpret_cast<const volatile int*>(&s->done)) return;
+    if (GATED && !*reinterpret_cast<const volatile int*>(&s->needDirection)) return;
     const float beta = static_cast<float>(s->beta);
     const long quads = n >> 2;
     const long stride = static_cast<long>(gridDim.x) * kT;
@@ -410,6 +523,7 @@ struct ciecu_mixed_s {
     cudaGraphExec_t graph = nullptr;
     const double* graphB = nullptr;
     bool deviceLoop = false;
+    bool fused = true;            // cooperative update/direction kernel
     cudaStream_t side = nullptr;  // captures the IF body of the refinement
     int chunk = 16;
 };
@@ -448,26 +562,40 @@ int launch_inner(ciecu_mixed_s* M, cudaStream_t st, cudaGraph_t root, cudaGraphC
                 M->a32, M->p32, M->q32, M->d_s, M->d_partials, M->d_counter, loop);
         return CIECU_OK;
     }));
-    mixed_update_kernel<COND><<<fit_grid(mixed_update_kernel<COND>, kT, needV), kT, 0, st>>>(M->n, M->x32, M->r32, M->p32, M->q32, M->dinv32, M->d_s,
-                                                    M->d_partials, M->d_counter, loop, refine);
+    if (M->fused) {
+        cudaError_t e = launch_cooperative(mixed_update_direction_kernel<COND>,
+                                           fit_grid(mixed_update_direction_kernel<COND>, kT, needV), kT, st, M->n,
+                                           M->x32, M->r32, M->p32, static_cast<const float*>(M->q32),
+                                           static_cast<const float*>(M->dinv32), M->d_s, M->d_partials, M->d_counter,
+                                           loop, refine);
+        if (e != cudaSuccess) return cuda_fail(e, "fused mixed update/direction launch");
+    } else {
+        mixed_update_kernel<COND><<<fit_grid(mixed_update_kernel<COND>, kT, needV), kT, 0, st>>>(
+            M->n, M->x32, M->r32, M->p32, M->q32, M->dinv32, M->d_s, M->d_partials, M->d_counter, loop, refine);
+    }
     auto refinement = [&](cudaStream_t s2) -> int {
         mixed_fold_kernel<<<fit_grid(mixed_fold_kernel, kT, needA), kT, 0, s2>>>(M->n, M->x64, M->x32, M->d_s);
         const int needR = csr_grid(A, A->kernel);
-        return with_schedule(A->kernel, [&](auto k) -> int {
+        CIECU_TRY(with_schedule(A->kernel, [&](auto k) -> int {
             constexpr int K = decltype(k)::value;
             mixed_residual_kernel<K, false, COND><<<fit_grid(mixed_residual_kernel<K, false, COND>, csr_threads<K>(),
                                                              needR),
                                                     csr_threads<K>(), 0, s2>>>(
                 A->args<double>(), M->b, M->x64, M->dinv32, M->r32, M->d_s, M->d_partials, M->d_counter, loop);
             return CIECU_OK;
-        });
+        }));
+        if (M->fused)
+            mixed_direction_kernel<true><<<fit_grid(mixed_direction_kernel<true>, kT, needV), kT, 0, s2>>>(
+                M->n, M->p32, M->r32, M->dinv32, M->d_s);
+        return CIECU_OK;
     };
     if (useCond)
         CIECU_TRY(capture_if(st, M->side, refine, refinement));
     else
         CIECU_TRY(refinement(st));
-    mixed_direction_kernel<<<fit_grid(mixed_direction_kernel, kT, needV), kT, 0, st>>>(M->n, M->p32, M->r32,
-                                                                                       M->dinv32, M->d_s);
+    if (!M->fused)
+        mixed_direction_kernel<false><<<fit_grid(mixed_direction_kernel<false>, kT, needV), kT, 0, st>>>(
+            M->n, M->p32, M->r32, M->dinv32, M->d_s);
     CIECU_CHECK_LAUNCH("mixed inner iteration");
     return CIECU_OK;
 }
@@ -479,6 +607,7 @@ int build_mixed_graph(ciecu_mixed_s* M) {
         M->graph = nullptr;
     }
     cudaStream_t st = M->A->space->stream;
+    M->fused = fused_update_enabled();
     int status = CIECU_ERR_ARGUMENT;
     if (device_loop_enabled())
         status = build_while_graph(st, [&](cudaGraph_t root, cudaGraphConditionalHandle loop) {
@@ -762,7 +891,7 @@ int ciecu_mixed_product(ciecu_mixed M, double inScale, const double* d_in, doubl
                 A->args<double>(), d_in, M->x64, M->dinv32, M->r32, M->d_s, M->d_partials, M->d_counter, 0);
             return CIECU_OK;
         }));
-        mixed_direction_kernel<<<fit_grid(mixed_direction_kernel, kT, ((n + 3) / 4 + kT - 1) / kT), kT, 0, st>>>(
+        mixed_direction_kernel<false><<<fit_grid(mixed_direction_kernel<false>, kT, ((n + 3) / 4 + kT - 1) / kT), kT, 0, st>>>(
             n, M->p32, M->r32, M->dinv32, M->d_s);
         count_launch(2);
         CIECU_CHECK_LAUNCH("mixed set-up");
@@ -785,6 +914,8 @@ int ciecu_mixed_product(ciecu_mixed M, double inScale, const double* d_in, doubl
             if (M->h_s->done) break;
         }
         const MixedScalars& s = *M->h_s;
+        if (s.error == CIECU_ERR_TIMEOUT)
+            return fail(CIECU_ERR_TIMEOUT, "mixed-precision CG: a device-side grid release timed out");
         if (s.error) {
             if (h_stats) *h_stats = ciecu_mixed_statistics{s.iter, s.absres, s.relres, s.iter, s.refinements, s.relres};
             return fail(CIECU_ERR_BREAKDOWN, "mixed-precision CG breakdown (p^T A p <= 0 or r^T z <= 0) in iteration " +

@@ -202,6 +202,104 @@ __global__ void __launch_bounds__(kT) pcg_direction_kernel(long n, double* __res
     }
 }
 
+// K2+K3 fused (cooperative launch, all blocks resident): phase 1 is K2; the last
+// block to finish the r^T r / r^T z reduction takes the stopping decision and
+// releases the grid; phase 2 is K3, reading r, D^-1 and p back while they are
+// still in L2.  One kernel boundary less per iteration.
+template <bool PRECOND, bool COND>
+__global__ void __launch_bounds__(kT) pcg_update_direction_kernel(long n, double* __restrict__ x,
+                                                                  double* __restrict__ r, double* __restrict__ p,
+                                                                  const double* __restrict__ q,
+                                                                  const double* __restrict__ dinv, PcgScalars* s,
+                                                                  double* partials, unsigned* counter,
+                                                                  cudaGraphConditionalHandle cond) {
+    if (*reinterpret_cast<volatile int*>(&s->done)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) set_loop<COND>(cond, 0);
+        return;
+    }
+    const unsigned gen = *reinterpret_cast<volatile unsigned*>(&s->generation);
+    const double alpha = s->alpha;
+    const double malpha = -alpha;
+    double rr = 0.0, rz = 0.0;
+    const long pairs = n >> 1;
+    const long stride = static_cast<long>(gridDim.x) * kT;
+    for (long j = static_cast<long>(blockIdx.x) * kT + threadIdx.x; j < pairs; j += stride) {
+        const double2 pj = reinterpret_cast<const double2*>(p)[j];
+        const double2 qj = reinterpret_cast<const double2*>(q)[j];
+        double2 xj = reinterpret_cast<const double2*>(x)[j];
+        double2 rj = reinterpret_cast<const double2*>(r)[j];
+        xj.x = fma(alpha, pj.x, xj.x);
+        xj.y = fma(alpha, pj.y, xj.y);
+        rj.x = fma(malpha, qj.x, rj.x);
+        rj.y = fma(malpha, qj.y, rj.y);
+        reinterpret_cast<double2*>(x)[j] = xj;
+        reinterpret_cast<double2*>(r)[j] = rj;
+        rr = fma(rj.x, rj.x, rr);
+        rr = fma(rj.y, rj.y, rr);
+        if (PRECOND) {
+            const double2 dj = reinterpret_cast<const double2*>(dinv)[j];
+            rz = fma(rj.x, rj.x * dj.x, rz);
+            rz = fma(rj.y, rj.y * dj.y, rz);
+        }
+    }
+    if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+        const long i = n - 1;
+        x[i] = fma(alpha, p[i], x[i]);
+        const double ri = fma(malpha, q[i], r[i]);
+        r[i] = ri;
+        rr = fma(ri, ri, rr);
+        if (PRECOND) rz = fma(ri, ri * dinv[i], rz);
+    }
+    double mine[2] = {rr, rz}, tot[2];
+    if (grid_reduce_last<2, kT>(mine, partials, counter, tot)) {
+        if (threadIdx.x == 0) {
+            const double rzNew = PRECOND ? tot[1] : tot[0];
+            s->rr = tot[0];
+            s->beta = rzNew / s->rz;
+            s->rz = rzNew;
+            s->absres = sqrt(tot[0]);
+            s->relres = s->absres / s->r0;
+            if (float_less(s->absres, s->absTol) || float_less(s->relres, s->relTol)) {
+                s->done = 1;
+            } else {
+                s->iter += 1;
+                if (s->iter >= s->maxIter) s->done = 2;
+            }
+            s->chunkIter += 1;
+            set_loop<COND>(cond, (s->done == 0 && s->chunkIter < s->chunkLimit) ? 1u : 0u);
+            release_grid(&s->generation);
+        }
+        __syncthreads();
+    } else if (!wait_release(&s->generation, gen, kReleaseSpins)) {
+        if (threadIdx.x == 0) {
+            s->error = CIECU_ERR_TIMEOUT;
+            s->done = 3;
+            set_loop<COND>(cond, 0);
+        }
+        return;
+    }
+    if (*reinterpret_cast<volatile int*>(&s->done)) return;
+    const double beta = *reinterpret_cast<volatile double*>(&s->beta);
+    for (long j = static_cast<long>(blockIdx.x) * kT + threadIdx.x; j < pairs; j += stride) {
+        const double2 rj = reinterpret_cast<const double2*>(r)[j];
+        double2 pj = reinterpret_cast<const double2*>(p)[j];
+        double2 zj = rj;
+        if (PRECOND) {
+            const double2 dj = reinterpret_cast<const double2*>(dinv)[j];
+            zj.x = __dmul_rn(rj.x, dj.x);
+            zj.y = __dmul_rn(rj.y, dj.y);
+        }
+        pj.x = __dadd_rn(__dmul_rn(pj.x, beta), zj.x);
+        pj.y = __dadd_rn(__dmul_rn(pj.y, beta), zj.y);
+        reinterpret_cast<double2*>(p)[j] = pj;
+    }
+    if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+        const long i = n - 1;
+        const double zi = PRECOND ? __dmul_rn(r[i], dinv[i]) : r[i];
+        p[i] = __dadd_rn(__dmul_rn(p[i], beta), zi);
+    }
+}
+
 // out = inScale*out + outScale*x with the space ops of :190-198.
 __global__ void pcg_output_kernel(long n, double inScale, double outScale, const double* __restrict__ x,
                                   double* __restrict__ out) {
@@ -242,6 +340,7 @@ struct ciecu_pcg_s {
     cudaGraphExec_t graph = nullptr;
     int graphKernel = -1;
     bool deviceLoop = false;  // graph = WHILE loop (else `chunk` unrolled iterations)
+    bool fused = true;        // cooperative update/direction kernel (else K2 and K3)
     int chunk = 16;
 };
 
@@ -260,7 +359,20 @@ int launch_iteration(ciecu_pcg_s* S, cudaStream_t st, cudaGraphConditionalHandle
                                    st>>>(A->args<double>(), S->p, S->q, S->d_s, S->d_partials, S->d_counter, cond);
         return CIECU_OK;
     }));
-    if (pre) {
+    if (S->fused) {
+        cudaError_t e;
+        if (pre)
+            e = launch_cooperative(pcg_update_direction_kernel<true, COND>,
+                                   fit_grid(pcg_update_direction_kernel<true, COND>, kT, needV), kT, st, S->n, S->x,
+                                   S->r, S->p, static_cast<const double*>(S->q), S->dinv, S->d_s, S->d_partials,
+                                   S->d_counter, cond);
+        else
+            e = launch_cooperative(pcg_update_direction_kernel<false, COND>,
+                                   fit_grid(pcg_update_direction_kernel<false, COND>, kT, needV), kT, st, S->n, S->x,
+                                   S->r, S->p, static_cast<const double*>(S->q), S->dinv, S->d_s, S->d_partials,
+                                   S->d_counter, cond);
+        if (e != cudaSuccess) return cuda_fail(e, "fused update/direction launch");
+    } else if (pre) {
         pcg_update_kernel<true, COND><<<fit_grid(pcg_update_kernel<true, COND>, kT, needV), kT, 0, st>>>(
             S->n, S->x, S->r, S->p, S->q, S->dinv, S->d_s, S->d_partials, S->d_counter, cond);
         pcg_direction_kernel<true><<<fit_grid(pcg_direction_kernel<true>, kT, needV), kT, 0, st>>>(S->n, S->p, S->r,
@@ -285,6 +397,7 @@ int build_graph(ciecu_pcg_s* S) {
         cudaGraphExecDestroy(S->graph);
         S->graph = nullptr;
     }
+    S->fused = fused_update_enabled();
     int status = CIECU_ERR_ARGUMENT;
     if (device_loop_enabled())
         status = build_while_graph(st, [&](cudaGraph_t, cudaGraphConditionalHandle cond) {
@@ -435,6 +548,8 @@ int ciecu_pcg_product(ciecu_pcg S, double inScale, const double* d_in, double ou
             if (S->h_s->done) break;
         }
         const PcgScalars& s = *S->h_s;
+        if (s.error == CIECU_ERR_TIMEOUT)
+            return fail(CIECU_ERR_TIMEOUT, "pcg: a device-side grid release timed out");
         if (s.error) {
             if (h_stats) *h_stats = ciecu_statistics{s.errorIter, s.absres, s.relres};
             if (s.errorKind == 1)
