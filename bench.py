@@ -177,7 +177,9 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile", action="store_true",
-                    help="ncu target: 96^3 case, solves only (no e2e, no CPU baseline, no clock sampling)")
+                    help="ncu target: solves only (no e2e, no CPU baseline, no clock sampling)")
+    ap.add_argument("--profile-cells", type=int, default=PROFILE_CELLS[0],
+                    help="cells per axis of the --profile case (96: 290 MB matrix; 128: the full workload)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -203,7 +205,7 @@ def main():
         torch.cuda.synchronize()
 
     space = CUDASpace()
-    cells = PROFILE_CELLS if args.profile else WORKLOAD["cells"]
+    cells = [args.profile_cells] * 3 if args.profile else WORKLOAD["cells"]
     prob = make_poisson(space, 3, 1, cells, seed=WORKLOAD["seed"])
     n, nnz = prob.mesh.ndofs, prob.matrix.nnz()
     A = CSROperator(prob.matrix, space)
@@ -239,7 +241,8 @@ def main():
                 lib.ciecu_mixed_apply_f32(mixed._solver, _ptr(x32), _ptr(y32))
                 lib.ciecu_csr_spmv_f64(A.csr.handle, 0.0, _ptr(x64), 1.0, _ptr(prob.rhs.clone()))
         torch.cuda.synchronize()
-        print(json.dumps({"profile": True, "cells": cells, "fp64_iterations": it64,
+        print(json.dumps({"profile": True, "cells": cells, "fp64_iterations": it64, "fp64_info": cg.info(),
+                          "mixed_info": mixed.info(),
                           "mixed_inner": mst.innerIterations, "mixed_refinements": mst.refinements}), flush=True)
         return
     hbm, peak_kind = peaks()
@@ -349,6 +352,7 @@ def main():
                       "rel_diff_vs_fp64_solution": agree,
                       "achieved_gbs": mixed_solve_bytes / t_mixed / 1e9},
             "fp64": {"seconds": t_fp64, "iterations": it64, "true_relative_residual": rel_fp64,
+                     "spmv_schedule": cg.info().get("spmv_schedule"), "device_loop": cg.info().get("device_loop"),
                      "achieved_gbs": fp64_solve_bytes / t_fp64 / 1e9,
                      "us_per_iteration": 1e6 * t_fp64 / (it64 + 1)},
             "speedup_mixed_vs_fp64": t_fp64 / t_mixed,

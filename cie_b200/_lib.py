@@ -23,7 +23,7 @@ class Statistics(ctypes.Structure):
 
 
 class MixedOptions(ctypes.Structure):
-    _fields_ = [("mode", c_int), ("delta", c_double), ("compressColumns", c_int)]
+    _fields_ = [("mode", c_int), ("delta", c_double), ("compressColumns", c_int), ("innerKernel", c_int)]
 
 
 class MixedStatistics(ctypes.Structure):
@@ -77,6 +77,7 @@ SIGNATURES = {
     "ciecu_pcg_destroy": (c_int, [P]),
     "ciecu_pcg_product": (c_int, [P, c_double, P, c_double, P, P]),
     "ciecu_pcg_set_graph_chunk": (c_int, [P, c_int]),
+    "ciecu_pcg_info": (c_int, [P, P, P]),
     "ciecu_mixed_create": (c_int, [P, P, Statistics, MixedOptions, P]),
     "ciecu_mixed_destroy": (c_int, [P]),
     "ciecu_mixed_info": (c_int, [P, P, P]),

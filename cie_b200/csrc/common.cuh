@@ -103,56 +103,6 @@ __device__ __forceinline__ bool grid_reduce_last(const double (&mine)[K], double
     return true;
 }
 
-// Grid-wide release that follows grid_reduce_last inside a COOPERATIVE launch
-// (all blocks resident): the last block publishes its results and then calls
-// release_grid(); every other block calls wait_release() with the generation it
-// read at kernel start.  The wait is bounded: after maxSpins polls it gives up
-// and returns false, so a lost release can never hang the GPU.
-__device__ __forceinline__ void release_grid(unsigned* generation) {
-    __threadfence();
-    atomicAdd(generation, 1u);
-}
-
-__device__ __forceinline__ bool wait_release(const unsigned* generation, unsigned seen, long long maxSpins) {
-    __shared__ int s_ok;
-    if (threadIdx.x == 0) {
-        int ok = 1;
-        long long spins = 0;
-        while (*reinterpret_cast<const volatile unsigned*>(generation) == seen) {
-            if (++spins > maxSpins) {
-                ok = 0;
-                break;
-            }
-            __nanosleep(32);
-        }
-        s_ok = ok;
-        __threadfence();
-    }
-    __syncthreads();
-    return s_ok != 0;
-}
-
-// ~1 s of polling at 32 ns per poll: far beyond any legitimate wait.
-constexpr long long kReleaseSpins = 30000000LL;
-
-// cudaLaunchKernelEx with the cooperative attribute (co-residency of all blocks,
-// required by wait_release); valid inside stream capture.
-template <typename... KArgs, typename... Args>
-inline cudaError_t launch_cooperative(void (*kernel)(KArgs...), int grid, int threads, cudaStream_t st,
-                                      Args&&... args) {
-    cudaLaunchConfig_t cfg{};
-    cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(threads);
-    cfg.dynamicSmemBytes = 0;
-    cfg.stream = st;
-    cudaLaunchAttribute attr{};
-    attr.id = cudaLaunchAttributeCooperative;
-    attr.val.cooperative = 1;
-    cfg.attrs = &attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
-}
-
 // out = inScale*out + outScale*sum with the special cases of the reference
 // operators (linalg/packages/solvers/src/CSROperator.cpp:78-110), including the
 // (-1, -1) combination that yields sum - out.

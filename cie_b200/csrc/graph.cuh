@@ -21,16 +21,6 @@ inline bool device_loop_enabled() {
     return enabled;
 }
 
-// CIECU_FUSED_UPDATE=0 selects the separate update and direction kernels instead
-// of the cooperative fused one.
-inline bool fused_update_enabled() {
-    static const bool enabled = [] {
-        const char* v = std::getenv("CIECU_FUSED_UPDATE");
-        return !(v && v[0] == '0');
-    }();
-    return enabled;
-}
-
 template <typename F>
 int build_while_graph(cudaStream_t st, F&& body, cudaGraphExec_t* exec) {
     *exec = nullptr;

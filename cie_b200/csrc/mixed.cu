@@ -33,6 +33,7 @@
 #include "graph.cuh"
 #include "pcg.cuh"
 #include "sell.cuh"
+#include "sell_tma.cuh"
 
 #include <string>
 #include <vector>
@@ -51,8 +52,8 @@ struct MixedScalars {
     long long iter, maxIter, refinements;
     int done, error, update, updateX, mode, pad;
     long long chunkIter, chunkLimit;  // iterations of the current graph launch / per launch
-    unsigned generation;              // grid-release counter of the fused update/direction kernel
-    int needDirection;                // R2 replaced r: the gated direction kernel must run
+    unsigned tmaError;                // a bounded TMA pipeline wait gave up
+    unsigned pad2;
 };
 
 // COND selects the instantiation with conditional-node calls (device loop) or
@@ -165,6 +166,56 @@ __global__ void __launch_bounds__(kT) mixed_spmv_kernel(SellArgs<float, CI> A, c
     }
 }
 
+// TMA-pipelined variants of the two kernels above (sell_tma.cuh): one CTA of
+// kTmaWarps warps per SM, the matrix streamed through shared memory.
+template <typename CI>
+__global__ void __launch_bounds__(kTmaWarps * 32) mixed_apply_tma_kernel(SellArgs<float, CI> A,
+                                                                         const float* __restrict__ x,
+                                                                         float* __restrict__ y, unsigned* error) {
+    extern __shared__ __align__(128) unsigned char tma_smem[];
+    StoreOp op{y};
+    sell_rows_tma<CI>(A, x, op, tma_smem, error);
+}
+
+template <typename CI, bool COND>
+__global__ void __launch_bounds__(kTmaWarps * 32) mixed_spmv_tma_kernel(SellArgs<float, CI> A,
+                                                                        const float* __restrict__ p,
+                                                                        float* __restrict__ q, MixedScalars* s,
+                                                                        double* partials, unsigned* counter,
+                                                                        cudaGraphConditionalHandle loop) {
+    extern __shared__ __align__(128) unsigned char tma_smem[];
+    if (*reinterpret_cast<volatile int*>(&s->done)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) set_cond<COND>(loop, 0);
+        return;
+    }
+    MixedPqOp op{p, q, 0.0};
+    sell_rows_tma<CI>(A, p, op, tma_smem, &s->tmaError);
+    double mine[1] = {op.acc}, tot[1];
+    if (grid_reduce_last<1, kTmaWarps * 32>(mine, partials, counter, tot) && threadIdx.x == 0) {
+        s->pq = tot[0];
+        if (s->tmaError) {
+            s->done = 3;
+            s->error = CIECU_ERR_TIMEOUT;
+            set_cond<COND>(loop, 0);
+        } else if (!(0.0 < tot[0])) {
+            s->done = 3;
+            s->error = CIECU_ERR_BREAKDOWN;
+            set_cond<COND>(loop, 0);
+        } else {
+            s->alpha = s->rz / tot[0];
+        }
+    }
+}
+
+// Raises the dynamic shared memory limit of a TMA kernel once (before any
+// occupancy query, launch or capture).
+template <typename K>
+int allow_tma_smem(K* kernel, int bytes) {
+    CIECU_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(kernel), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    bytes));
+    return CIECU_OK;
+}
+
 // M2: x32 += alpha p; r32 -= alpha q; rr, rz in FP64; replacement decision.
 template <bool COND>
 __global__ void __launch_bounds__(kT) mixed_update_kernel(long n, float* __restrict__ x, float* __restrict__ r,
@@ -236,113 +287,6 @@ __global__ void __launch_bounds__(kT) mixed_update_kernel(long n, float* __restr
         s->chunkIter += 1;
         set_cond<COND>(refine, update ? 1u : 0u);
         set_cond<COND>(loop, s->chunkIter < s->chunkLimit ? 1u : 0u);
-    }
-}
-
-// M2+M3 fused (cooperative launch, all blocks resident): phase 1 is M2 and its
-// decision; the last block releases the grid; phase 2 is M3 unless a residual
-// replacement is due -- then the gated direction kernel runs after R2 instead.
-template <bool COND>
-__global__ void __launch_bounds__(kT) mixed_update_direction_kernel(long n, float* __restrict__ x,
-                                                                    float* __restrict__ r, float* __restrict__ p,
-                                                                    const float* __restrict__ q,
-                                                                    const float* __restrict__ dinv, MixedScalars* s,
-                                                                    double* partials, unsigned* counter,
-                                                                    cudaGraphConditionalHandle loop,
-                                                                    cudaGraphConditionalHandle refine) {
-    if (*reinterpret_cast<volatile int*>(&s->done)) {
-        if (blockIdx.x == 0 && threadIdx.x == 0) {
-            set_cond<COND>(loop, 0);
-            set_cond<COND>(refine, 0);
-        }
-        return;
-    }
-    const unsigned gen = *reinterpret_cast<volatile unsigned*>(&s->generation);
-    const float alpha = static_cast<float>(s->alpha);
-    double rr = 0.0, rz = 0.0;
-    const long quads = n >> 2;
-    const long stride = static_cast<long>(gridDim.x) * kT;
-    for (long j = static_cast<long>(blockIdx.x) * kT + threadIdx.x; j < quads; j += stride) {
-        const float4 pj = reinterpret_cast<const float4*>(p)[j];
-        const float4 qj = reinterpret_cast<const float4*>(q)[j];
-        const float4 dj = reinterpret_cast<const float4*>(dinv)[j];
-        float4 xj = reinterpret_cast<const float4*>(x)[j];
-        float4 rj = reinterpret_cast<const float4*>(r)[j];
-        xj.x = fmaf(alpha, pj.x, xj.x); xj.y = fmaf(alpha, pj.y, xj.y);
-        xj.z = fmaf(alpha, pj.z, xj.z); xj.w = fmaf(alpha, pj.w, xj.w);
-        rj.x = fmaf(-alpha, qj.x, rj.x); rj.y = fmaf(-alpha, qj.y, rj.y);
-        rj.z = fmaf(-alpha, qj.z, rj.z); rj.w = fmaf(-alpha, qj.w, rj.w);
-        reinterpret_cast<float4*>(x)[j] = xj;
-        reinterpret_cast<float4*>(r)[j] = rj;
-        rr = fma(double(rj.x), double(rj.x), rr); rr = fma(double(rj.y), double(rj.y), rr);
-        rr = fma(double(rj.z), double(rj.z), rr); rr = fma(double(rj.w), double(rj.w), rr);
-        rz = fma(double(rj.x), double(rj.x * dj.x), rz); rz = fma(double(rj.y), double(rj.y * dj.y), rz);
-        rz = fma(double(rj.z), double(rj.z * dj.z), rz); rz = fma(double(rj.w), double(rj.w * dj.w), rz);
-    }
-    if (blockIdx.x == 0 && threadIdx.x < (n & 3)) {
-        const long i = (quads << 2) + threadIdx.x;
-        x[i] = fmaf(alpha, p[i], x[i]);
-        const float ri = fmaf(-alpha, q[i], r[i]);
-        r[i] = ri;
-        rr = fma(double(ri), double(ri), rr);
-        rz = fma(double(ri), double(ri * dinv[i]), rz);
-    }
-    double mine[2] = {rr, rz}, tot[2];
-    if (grid_reduce_last<2, kT>(mine, partials, counter, tot)) {
-        if (threadIdx.x == 0) {
-            const double rnorm = sqrt(tot[0]);
-            s->sloppy = rnorm;
-            s->iter += 1;
-            bool update;
-            s->updateX = 0;
-            if (s->mode == 0) {
-                if (rnorm > s->maxrx) s->maxrx = rnorm;
-                if (rnorm > s->maxrr) s->maxrr = rnorm;
-                const bool updateX = rnorm < s->delta * s->maxrx;
-                update = updateX || rnorm < s->delta * s->maxrr;
-                s->updateX = updateX ? 1 : 0;
-            } else {
-                update = rnorm < s->delta * s->cycleStart;
-            }
-            update = update || rnorm < s->relTol * s->r0 || rnorm < s->absTol || s->iter >= s->maxIter;
-            s->needDirection = 0;
-            if (update) {
-                s->rzPending = tot[1];
-                s->update = 1;
-            } else {
-                s->beta = tot[1] / s->rz;
-                s->rz = tot[1];
-            }
-            s->chunkIter += 1;
-            set_cond<COND>(refine, update ? 1u : 0u);
-            set_cond<COND>(loop, s->chunkIter < s->chunkLimit ? 1u : 0u);
-            release_grid(&s->generation);
-        }
-        __syncthreads();
-    } else if (!wait_release(&s->generation, gen, kReleaseSpins)) {
-        if (threadIdx.x == 0) {
-            s->error = CIECU_ERR_TIMEOUT;
-            s->done = 3;
-            set_cond<COND>(loop, 0);
-            set_cond<COND>(refine, 0);
-        }
-        return;
-    }
-    if (*reinterpret_cast<volatile int*>(&s->update) || *reinterpret_cast<volatile int*>(&s->done)) return;
-    const float beta = static_cast<float>(*reinterpret_cast<volatile double*>(&s->beta));
-    for (long j = static_cast<long>(blockIdx.x) * kT + threadIdx.x; j < quads; j += stride) {
-        const float4 rj = reinterpret_cast<const float4*>(r)[j];
-        const float4 dj = reinterpret_cast<const float4*>(dinv)[j];
-        float4 pj = reinterpret_cast<const float4*>(p)[j];
-        pj.x = fmaf(beta, pj.x, rj.x * dj.x);
-        pj.y = fmaf(beta, pj.y, rj.y * dj.y);
-        pj.z = fmaf(beta, pj.z, rj.z * dj.z);
-        pj.w = fmaf(beta, pj.w, rj.w * dj.w);
-        reinterpret_cast<float4*>(p)[j] = pj;
-    }
-    if (blockIdx.x == 0 && threadIdx.x < (n & 3)) {
-        const long i = (quads << 2) + threadIdx.x;
-        p[i] = fmaf(beta, p[i], r[i] * dinv[i]);
     }
 }
 
@@ -435,19 +379,15 @@ __global__ void __launch_bounds__(csr_threads<KERNEL>())
                 s->beta = 0.0;  // restart the inner CG: p = z
             }
             s->rz = tot[1];
-            s->needDirection = 1;
         }
         if (s->done) set_cond<COND>(loop, 0);
     }
 }
 
-// M3: p = z + beta p, z = D^-1 r (FP32).  GATED: only after a residual
-// replacement (the fused kernel updates p in all other iterations).
-template <bool GATED>
+// M3: p = z + beta p, z = D^-1 r (FP32).
 __global__ void __launch_bounds__(kT) mixed_direction_kernel(long n, float* __restrict__ p, const float* __restrict__ r,
                                                              const float* __restrict__ dinv, const MixedScalars* s) {
     if (*reinterpret_cast<const volatile int*>(&s->done)) return;
-    if (GATED && !*reinterpret_cast<const volatile int*>(&s->needDirection)) return;
     const float beta = static_cast<float>(s->beta);
     const long quads = n >> 2;
     const long stride = static_cast<long>(gridDim.x) * kT;
@@ -501,7 +441,7 @@ struct ciecu_mixed_s {
     ciecu_mixed_options options{};
     long n = 0;
     bool idx16 = false;
-    int unroll = 2;  // SELL groups of four entries in flight per thread (autotuned)
+    int unroll = 2;  // SELL groups of four entries in flight per thread (autotuned; 0 = TMA pipeline)
     // SELL-32 inner matrix
     int nslices = 0;
     long long paddedEntries = 0;
@@ -523,7 +463,6 @@ struct ciecu_mixed_s {
     cudaGraphExec_t graph = nullptr;
     const double* graphB = nullptr;
     bool deviceLoop = false;
-    bool fused = true;            // cooperative update/direction kernel
     cudaStream_t side = nullptr;  // captures the IF body of the refinement
     int chunk = 16;
 };
@@ -541,6 +480,39 @@ int with_unroll(int u, F&& f) {
     }
 }
 
+// M1 with the autotuned variant: TMA pipeline (unroll == 0) or U register groups.
+template <bool COND>
+int launch_inner_spmv(ciecu_mixed_s* M, cudaStream_t st, cudaGraphConditionalHandle loop) {
+    const long needA = (M->n + kT - 1) / kT;
+    if (M->unroll == 0) {
+        if (M->idx16) {
+            constexpr int smem = TmaShape<float, short>::SMEM;
+            mixed_spmv_tma_kernel<short, COND><<<fit_grid(mixed_spmv_tma_kernel<short, COND>, kTmaWarps * 32,
+                                                          (M->n + 511) / 512, smem),
+                                                 kTmaWarps * 32, smem, st>>>(M->a16, M->p32, M->q32, M->d_s,
+                                                                             M->d_partials, M->d_counter, loop);
+        } else {
+            constexpr int smem = TmaShape<float, int>::SMEM;
+            mixed_spmv_tma_kernel<int, COND><<<fit_grid(mixed_spmv_tma_kernel<int, COND>, kTmaWarps * 32,
+                                                        (M->n + 511) / 512, smem),
+                                               kTmaWarps * 32, smem, st>>>(M->a32, M->p32, M->q32, M->d_s,
+                                                                           M->d_partials, M->d_counter, loop);
+        }
+        CIECU_CHECK_LAUNCH("mixed_spmv_tma_kernel");
+        return CIECU_OK;
+    }
+    return with_unroll(M->unroll, [&](auto uu) -> int {
+        constexpr int U = decltype(uu)::value;
+        if (M->idx16)
+            mixed_spmv_kernel<U, short, COND><<<fit_grid(mixed_spmv_kernel<U, short, COND>, kT, needA), kT, 0, st>>>(
+                M->a16, M->p32, M->q32, M->d_s, M->d_partials, M->d_counter, loop);
+        else
+            mixed_spmv_kernel<U, int, COND><<<fit_grid(mixed_spmv_kernel<U, int, COND>, kT, needA), kT, 0, st>>>(
+                M->a32, M->p32, M->q32, M->d_s, M->d_partials, M->d_counter, loop);
+        return CIECU_OK;
+    });
+}
+
 // One inner iteration.  With conditional nodes (useCond) the refinement pair
 // R1/R2 sits under IF(refine); otherwise it is launched unconditionally and
 // returns at once unless M2 requested a replacement.
@@ -552,27 +524,9 @@ int launch_inner(ciecu_mixed_s* M, cudaStream_t st, cudaGraph_t root, cudaGraphC
     ciecu_csr_s* A = M->A;
     cudaGraphConditionalHandle refine = 0;
     if (useCond) CIECU_CUDA(cudaGraphConditionalHandleCreate(&refine, root, 0, cudaGraphCondAssignDefault));
-    CIECU_TRY(with_unroll(M->unroll, [&](auto uu) -> int {
-        constexpr int U = decltype(uu)::value;
-        if (M->idx16)
-            mixed_spmv_kernel<U, short, COND><<<fit_grid(mixed_spmv_kernel<U, short, COND>, kT, needA), kT, 0, st>>>(
-                M->a16, M->p32, M->q32, M->d_s, M->d_partials, M->d_counter, loop);
-        else
-            mixed_spmv_kernel<U, int, COND><<<fit_grid(mixed_spmv_kernel<U, int, COND>, kT, needA), kT, 0, st>>>(
-                M->a32, M->p32, M->q32, M->d_s, M->d_partials, M->d_counter, loop);
-        return CIECU_OK;
-    }));
-    if (M->fused) {
-        cudaError_t e = launch_cooperative(mixed_update_direction_kernel<COND>,
-                                           fit_grid(mixed_update_direction_kernel<COND>, kT, needV), kT, st, M->n,
-                                           M->x32, M->r32, M->p32, static_cast<const float*>(M->q32),
-                                           static_cast<const float*>(M->dinv32), M->d_s, M->d_partials, M->d_counter,
-                                           loop, refine);
-        if (e != cudaSuccess) return cuda_fail(e, "fused mixed update/direction launch");
-    } else {
-        mixed_update_kernel<COND><<<fit_grid(mixed_update_kernel<COND>, kT, needV), kT, 0, st>>>(
-            M->n, M->x32, M->r32, M->p32, M->q32, M->dinv32, M->d_s, M->d_partials, M->d_counter, loop, refine);
-    }
+    CIECU_TRY(launch_inner_spmv<COND>(M, st, loop));
+    mixed_update_kernel<COND><<<fit_grid(mixed_update_kernel<COND>, kT, needV), kT, 0, st>>>(
+        M->n, M->x32, M->r32, M->p32, M->q32, M->dinv32, M->d_s, M->d_partials, M->d_counter, loop, refine);
     auto refinement = [&](cudaStream_t s2) -> int {
         mixed_fold_kernel<<<fit_grid(mixed_fold_kernel, kT, needA), kT, 0, s2>>>(M->n, M->x64, M->x32, M->d_s);
         const int needR = csr_grid(A, A->kernel);
@@ -584,18 +538,14 @@ int launch_inner(ciecu_mixed_s* M, cudaStream_t st, cudaGraph_t root, cudaGraphC
                 A->args<double>(), M->b, M->x64, M->dinv32, M->r32, M->d_s, M->d_partials, M->d_counter, loop);
             return CIECU_OK;
         }));
-        if (M->fused)
-            mixed_direction_kernel<true><<<fit_grid(mixed_direction_kernel<true>, kT, needV), kT, 0, s2>>>(
-                M->n, M->p32, M->r32, M->dinv32, M->d_s);
         return CIECU_OK;
     };
     if (useCond)
         CIECU_TRY(capture_if(st, M->side, refine, refinement));
     else
         CIECU_TRY(refinement(st));
-    if (!M->fused)
-        mixed_direction_kernel<false><<<fit_grid(mixed_direction_kernel<false>, kT, needV), kT, 0, st>>>(
-            M->n, M->p32, M->r32, M->dinv32, M->d_s);
+    mixed_direction_kernel<<<fit_grid(mixed_direction_kernel, kT, needV), kT, 0, st>>>(M->n, M->p32, M->r32,
+                                                                                       M->dinv32, M->d_s);
     CIECU_CHECK_LAUNCH("mixed inner iteration");
     return CIECU_OK;
 }
@@ -607,7 +557,6 @@ int build_mixed_graph(ciecu_mixed_s* M) {
         M->graph = nullptr;
     }
     cudaStream_t st = M->A->space->stream;
-    M->fused = fused_update_enabled();
     int status = CIECU_ERR_ARGUMENT;
     if (device_loop_enabled())
         status = build_while_graph(st, [&](cudaGraph_t root, cudaGraphConditionalHandle loop) {
@@ -650,6 +599,9 @@ int ciecu_mixed_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_sta
     CIECU_REQUIRE(lhs->valueType == CIECU_F64 && lhs->rows == lhs->cols, "mixed_create: square FP64 matrix expected");
     CIECU_REQUIRE(options.mode == 0 || options.mode == 1, "mixed_create: mode must be 0 or 1");
     CIECU_REQUIRE(options.delta > 0.0 && options.delta < 1.0, "mixed_create: delta must be in (0, 1)");
+    CIECU_REQUIRE(options.innerKernel == 0 || options.innerKernel == 1 || options.innerKernel == 2 ||
+                      options.innerKernel == 4 || options.innerKernel == -1,
+                  "mixed_create: innerKernel must be 0 (autotune), 1, 2, 4 or -1 (TMA pipeline)");
     CIECU_TRY(ensure_tuned(lhs));
     auto* M = new ciecu_mixed_s();
     M->A = lhs;
@@ -708,6 +660,9 @@ int ciecu_mixed_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_sta
     if (e == cudaSuccess) e = cudaMalloc(&M->val32, sizeof(float) * padded);
     const bool try16 = options.compressColumns != 0;
     if (e == cudaSuccess) e = cudaMalloc(&M->col32or16, (try16 ? sizeof(short) : sizeof(int)) * padded);
+    // lanes past the last row of the final slice are never written by the fill
+    if (e == cudaSuccess) e = cudaMemsetAsync(M->val32, 0, sizeof(float) * padded, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(M->col32or16, 0, (try16 ? sizeof(short) : sizeof(int)) * padded, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(d_flag, 0, sizeof(unsigned), st);
     if (e == cudaSuccess && M->n > 0) {
         const int grid = grid_for(M->n, kT, 8);
@@ -737,6 +692,7 @@ int ciecu_mixed_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_sta
         cudaFree(M->col32or16);
         M->col32or16 = nullptr;
         e = cudaMalloc(&M->col32or16, sizeof(int) * padded);
+        if (e == cudaSuccess) e = cudaMemsetAsync(M->col32or16, 0, sizeof(int) * padded, st);
         if (e == cudaSuccess && M->n > 0) {
             sell_fill_kernel<int><<<grid_for(M->n, kT, 8), kT, 0, st>>>(
                 static_cast<int>(M->n), lhs->rowptr, lhs->col, static_cast<const double*>(lhs->val), M->sliceLen,
@@ -754,32 +710,62 @@ int ciecu_mixed_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_sta
                                     static_cast<const short*>(M->col32or16)};
     M->a32 = SellArgs<float, int>{static_cast<int>(M->n), M->sliceLen, M->sliceStart, M->rowLen, M->val32,
                                   static_cast<const int*>(M->col32or16)};
-    // Autotune the group unroll of the inner operator on the solver's own matrix
-    // (scratch vectors p32 -> q32).
-    if (M->n > 0) {
-        e = cudaMemsetAsync(M->p32, 0, sizeof(float) * M->n, st);
+    {
+        int st2 = allow_tma_smem(mixed_spmv_tma_kernel<short, false>, TmaShape<float, short>::SMEM);
+        if (st2 == CIECU_OK) st2 = allow_tma_smem(mixed_spmv_tma_kernel<short, true>, TmaShape<float, short>::SMEM);
+        if (st2 == CIECU_OK) st2 = allow_tma_smem(mixed_spmv_tma_kernel<int, false>, TmaShape<float, int>::SMEM);
+        if (st2 == CIECU_OK) st2 = allow_tma_smem(mixed_spmv_tma_kernel<int, true>, TmaShape<float, int>::SMEM);
+        if (st2 == CIECU_OK) st2 = allow_tma_smem(mixed_apply_tma_kernel<short>, TmaShape<float, short>::SMEM);
+        if (st2 == CIECU_OK) st2 = allow_tma_smem(mixed_apply_tma_kernel<int>, TmaShape<float, int>::SMEM);
+        if (st2 != CIECU_OK) {
+            ciecu_mixed_destroy(M);
+            return st2;
+        }
+    }
+    // Autotune the group unroll of the inner SpMV on the solver's own matrix,
+    // timing the fused kernel the iteration runs (q = A32 p with the p^T q
+    // reduction) on scratch vectors p32 = 0 -> q32.
+    if (options.innerKernel != 0) M->unroll = options.innerKernel < 0 ? 0 : options.innerKernel;
+    if (M->n > 0 && options.innerKernel == 0) {
+        // p = D^-1 > 0: p^T A p > 0 for an SPD matrix, so no timed launch trips the
+        // breakdown flag (which would make the later candidates return at once).
+        MixedScalars scratch{};
+        scratch.rz = 1.0;
+        e = cudaMemcpyAsync(M->d_s, &scratch, sizeof(MixedScalars), cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(M->p32, M->dinv32, sizeof(float) * M->n, cudaMemcpyDeviceToDevice, st);
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         if (e == cudaSuccess) e = cudaEventCreate(&e0);
         if (e == cudaSuccess) e = cudaEventCreate(&e1);
-        float best = 1e30f;
+        float best = 1e30f, bestTma = 1e30f;
         int bestU = 2;
-        for (int u : {1, 2, 4}) {
+        for (int u : {1, 2, 4, 0}) {
             if (e != cudaSuccess) break;
             M->unroll = u;
-            for (int rep = 0; rep < 2; ++rep) ciecu_mixed_apply_f32(M, M->p32, M->q32);
-            cudaEventRecord(e0, st);
-            for (int rep = 0; rep < 5; ++rep) ciecu_mixed_apply_f32(M, M->p32, M->q32);
-            cudaEventRecord(e1, st);
-            e = cudaEventSynchronize(e1);
-            float ms = 0.f;
-            if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
-            if (e == cudaSuccess && ms < best) {
-                best = ms;
-                bestU = u;
+            auto launch = [&]() { launch_inner_spmv<false>(M, st, 0); };
+            for (int rep = 0; rep < 2; ++rep) launch();
+            for (int trial = 0; trial < 3 && e == cudaSuccess; ++trial) {  // best of three
+                cudaEventRecord(e0, st);
+                for (int rep = 0; rep < 3; ++rep) launch();
+                cudaEventRecord(e1, st);
+                e = cudaEventSynchronize(e1);
+                float ms = 0.f;
+                if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+                if (e == cudaSuccess && u == 0 && ms < bestTma) bestTma = ms;
+                if (e == cudaSuccess && u != 0 && ms < best) {
+                    best = ms;
+                    bestU = u;
+                }
             }
         }
+        count_launch(44);
+        // the TMA pipeline competes only when every one of its waits completed
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&scratch, M->d_s, sizeof(MixedScalars), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e == cudaSuccess && scratch.tmaError == 0 && scratch.done == 0 && bestTma < best) bestU = 0;
         if (e0) cudaEventDestroy(e0);
         if (e1) cudaEventDestroy(e1);
+        if (e == cudaSuccess) e = cudaGetLastError();
         if (e != cudaSuccess) {
             ciecu_mixed_destroy(M);
             return cuda_fail(e, "mixed_create: autotune");
@@ -818,6 +804,14 @@ int ciecu_mixed_info(ciecu_mixed M, int* compressedColumns, int* lanesPerRow) {
     CIECU_REQUIRE(M, "mixed_info: null solver");
     if (compressedColumns) *compressedColumns = M->idx16 ? 1 : 0;
     if (lanesPerRow) *lanesPerRow = M->unroll;  // SELL: one thread per row, `unroll` groups of 4 in flight
+    if (M->unroll == 0) {
+        // error word of ciecu_mixed_apply_f32's TMA pipeline (sticky)
+        unsigned flag = 0;
+        cudaStream_t st = M->A->space->stream;
+        CIECU_CUDA(cudaMemcpyAsync(&flag, M->d_counter + 3, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+        CIECU_CUDA(cudaStreamSynchronize(st));
+        if (flag) return fail(CIECU_ERR_TIMEOUT, "mixed_apply_f32: a bounded TMA pipeline wait gave up");
+    }
     return CIECU_OK;
 }
 
@@ -826,6 +820,22 @@ int ciecu_mixed_apply_f32(ciecu_mixed M, const float* d_in, float* d_out) {
     if (M->n == 0) return CIECU_OK;
     cudaStream_t st = M->A->space->stream;
     const long need = (M->n + kT - 1) / kT;
+    if (M->unroll == 0) {
+        if (M->idx16) {
+            constexpr int smem = TmaShape<float, short>::SMEM;
+            mixed_apply_tma_kernel<short><<<fit_grid(mixed_apply_tma_kernel<short>, kTmaWarps * 32, (M->n + 511) / 512,
+                                                     smem),
+                                            kTmaWarps * 32, smem, st>>>(M->a16, d_in, d_out, M->d_counter + 3);
+        } else {
+            constexpr int smem = TmaShape<float, int>::SMEM;
+            mixed_apply_tma_kernel<int><<<fit_grid(mixed_apply_tma_kernel<int>, kTmaWarps * 32, (M->n + 511) / 512,
+                                                   smem),
+                                          kTmaWarps * 32, smem, st>>>(M->a32, d_in, d_out, M->d_counter + 3);
+        }
+        count_launch();
+        CIECU_CHECK_LAUNCH("mixed_apply_tma_kernel");
+        return CIECU_OK;
+    }
     CIECU_TRY(with_unroll(M->unroll, [&](auto uu) -> int {
         constexpr int U = decltype(uu)::value;
         if (M->idx16)
@@ -891,7 +901,7 @@ int ciecu_mixed_product(ciecu_mixed M, double inScale, const double* d_in, doubl
                 A->args<double>(), d_in, M->x64, M->dinv32, M->r32, M->d_s, M->d_partials, M->d_counter, 0);
             return CIECU_OK;
         }));
-        mixed_direction_kernel<false><<<fit_grid(mixed_direction_kernel<false>, kT, ((n + 3) / 4 + kT - 1) / kT), kT, 0, st>>>(
+        mixed_direction_kernel<<<fit_grid(mixed_direction_kernel, kT, ((n + 3) / 4 + kT - 1) / kT), kT, 0, st>>>(
             n, M->p32, M->r32, M->dinv32, M->d_s);
         count_launch(2);
         CIECU_CHECK_LAUNCH("mixed set-up");
@@ -915,7 +925,7 @@ int ciecu_mixed_product(ciecu_mixed M, double inScale, const double* d_in, doubl
         }
         const MixedScalars& s = *M->h_s;
         if (s.error == CIECU_ERR_TIMEOUT)
-            return fail(CIECU_ERR_TIMEOUT, "mixed-precision CG: a device-side grid release timed out");
+            return fail(CIECU_ERR_TIMEOUT, "mixed-precision CG: a bounded TMA pipeline wait gave up");
         if (s.error) {
             if (h_stats) *h_stats = ciecu_mixed_statistics{s.iter, s.absres, s.relres, s.iter, s.refinements, s.relres};
             return fail(CIECU_ERR_BREAKDOWN, "mixed-precision CG breakdown (p^T A p <= 0 or r^T z <= 0) in iteration " +

@@ -202,102 +202,9 @@ __global__ void __launch_bounds__(kT) pcg_direction_kernel(long n, double* __res
     }
 }
 
-// K2+K3 fused (cooperative launch, all blocks resident): phase 1 is K2; the last
-// block to finish the r^T r / r^T z reduction takes the stopping decision and
-// releases the grid; phase 2 is K3, reading r, D^-1 and p back while they are
-// still in L2.  One kernel boundary less per iteration.
-template <bool PRECOND, bool COND>
-__global__ void __launch_bounds__(kT) pcg_update_direction_kernel(long n, double* __restrict__ x,
-                                                                  double* __restrict__ r, double* __restrict__ p,
-                                                                  const double* __restrict__ q,
-                                                                  const double* __restrict__ dinv, PcgScalars* s,
-                                                                  double* partials, unsigned* counter,
-                                                                  cudaGraphConditionalHandle cond) {
-    if (*reinterpret_cast<volatile int*>(&s->done)) {
-        if (blockIdx.x == 0 && threadIdx.x == 0) set_loop<COND>(cond, 0);
-        return;
-    }
-    const unsigned gen = *reinterpret_cast<volatile unsigned*>(&s->generation);
-    const double alpha = s->alpha;
-    const double malpha = -alpha;
-    double rr = 0.0, rz = 0.0;
-    const long pairs = n >> 1;
-    const long stride = static_cast<long>(gridDim.x) * kT;
-    for (long j = static_cast<long>(blockIdx.x) * kT + threadIdx.x; j < pairs; j += stride) {
-        const double2 pj = reinterpret_cast<const double2*>(p)[j];
-        const double2 qj = reinterpret_cast<const double2*>(q)[j];
-        double2 xj = reinterpret_cast<const double2*>(x)[j];
-        double2 rj = reinterpret_cast<const double2*>(r)[j];
-        xj.x = fma(alpha, pj.x, xj.x);
-        xj.y = fma(alpha, pj.y, xj.y);
-        rj.x = fma(malpha, qj.x, rj.x);
-        rj.y = fma(malpha, qj.y, rj.y);
-        reinterpret_cast<double2*>(x)[j] = xj;
-        reinterpret_cast<double2*>(r)[j] = rj;
-        rr = fma(rj.x, rj.x, rr);
-        rr = fma(rj.y, rj.y, rr);
-        if (PRECOND) {
-            const double2 dj = reinterpret_cast<const double2*>(dinv)[j];
-            rz = fma(rj.x, rj.x * dj.x, rz);
-            rz = fma(rj.y, rj.y * dj.y, rz);
-        }
-    }
-    if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
-        const long i = n - 1;
-        x[i] = fma(alpha, p[i], x[i]);
-        const double ri = fma(malpha, q[i], r[i]);
-        r[i] = ri;
-        rr = fma(ri, ri, rr);
-        if (PRECOND) rz = fma(ri, ri * dinv[i], rz);
-    }
-    double mine[2] = {rr, rz}, tot[2];
-    if (grid_reduce_last<2, kT>(mine, partials, counter, tot)) {
-        if (threadIdx.x == 0) {
-            const double rzNew = PRECOND ? tot[1] : tot[0];
-            s->rr = tot[0];
-            s->beta = rzNew / s->rz;
-            s->rz = rzNew;
-            s->absres = sqrt(tot[0]);
-            s->relres = s->absres / s->r0;
-            if (float_less(s->absres, s->absTol) || float_less(s->relres, s->relTol)) {
-                s->done = 1;
-            } else {
-                s->iter += 1;
-                if (s->iter >= s->maxIter) s->done = 2;
-            }
-            s->chunkIter += 1;
-            set_loop<COND>(cond, (s->done == 0 && s->chunkIter < s->chunkLimit) ? 1u : 0u);
-            release_grid(&s->generation);
-        }
-        __syncthreads();
-    } else if (!wait_release(&s->generation, gen, kReleaseSpins)) {
-        if (threadIdx.x == 0) {
-            s->error = CIECU_ERR_TIMEOUT;
-            s->done = 3;
-            set_loop<COND>(cond, 0);
-        }
-        return;
-    }
-    if (*reinterpret_cast<volatile int*>(&s->done)) return;
-    const double beta = *reinterpret_cast<volatile double*>(&s->beta);
-    for (long j = static_cast<long>(blockIdx.x) * kT + threadIdx.x; j < pairs; j += stride) {
-        const double2 rj = reinterpret_cast<const double2*>(r)[j];
-        double2 pj = reinterpret_cast<const double2*>(p)[j];
-        double2 zj = rj;
-        if (PRECOND) {
-            const double2 dj = reinterpret_cast<const double2*>(dinv)[j];
-            zj.x = __dmul_rn(rj.x, dj.x);
-            zj.y = __dmul_rn(rj.y, dj.y);
-        }
-        pj.x = __dadd_rn(__dmul_rn(pj.x, beta), zj.x);
-        pj.y = __dadd_rn(__dmul_rn(pj.y, beta), zj.y);
-        reinterpret_cast<double2*>(p)[j] = pj;
-    }
-    if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
-        const long i = n - 1;
-        const double zi = PRECOND ? __dmul_rn(r[i], dinv[i]) : r[i];
-        p[i] = __dadd_rn(__dmul_rn(p[i], beta), zi);
-    }
+__global__ void fill_ones_kernel(long n, double* __restrict__ v) {
+    const long stride = static_cast<long>(gridDim.x) * blockDim.x;
+    for (long i = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) v[i] = 1.0;
 }
 
 // out = inScale*out + outScale*x with the space ops of :190-198.
@@ -340,7 +247,7 @@ struct ciecu_pcg_s {
     cudaGraphExec_t graph = nullptr;
     int graphKernel = -1;
     bool deviceLoop = false;  // graph = WHILE loop (else `chunk` unrolled iterations)
-    bool fused = true;        // cooperative update/direction kernel (else K2 and K3)
+    int kernel = 0;           // K1 schedule, autotuned on the fused SpMV kernel itself
     int chunk = 16;
 };
 
@@ -350,29 +257,16 @@ namespace {
 template <bool COND>
 int launch_iteration(ciecu_pcg_s* S, cudaStream_t st, cudaGraphConditionalHandle cond) {
     ciecu_csr_s* A = S->A;
-    const int needA = csr_grid(A, A->kernel);
+    const int needA = csr_grid(A, S->kernel);
     const long needV = ((S->n + 1) / 2 + kT - 1) / kT;
     const bool pre = S->dinv != nullptr;
-    CIECU_TRY(with_schedule(A->kernel, [&](auto k) -> int {
+    CIECU_TRY(with_schedule(S->kernel, [&](auto k) -> int {
         constexpr int K = decltype(k)::value;
         pcg_spmv_kernel<K, COND><<<fit_grid(pcg_spmv_kernel<K, COND>, csr_threads<K>(), needA), csr_threads<K>(), 0,
                                    st>>>(A->args<double>(), S->p, S->q, S->d_s, S->d_partials, S->d_counter, cond);
         return CIECU_OK;
     }));
-    if (S->fused) {
-        cudaError_t e;
-        if (pre)
-            e = launch_cooperative(pcg_update_direction_kernel<true, COND>,
-                                   fit_grid(pcg_update_direction_kernel<true, COND>, kT, needV), kT, st, S->n, S->x,
-                                   S->r, S->p, static_cast<const double*>(S->q), S->dinv, S->d_s, S->d_partials,
-                                   S->d_counter, cond);
-        else
-            e = launch_cooperative(pcg_update_direction_kernel<false, COND>,
-                                   fit_grid(pcg_update_direction_kernel<false, COND>, kT, needV), kT, st, S->n, S->x,
-                                   S->r, S->p, static_cast<const double*>(S->q), S->dinv, S->d_s, S->d_partials,
-                                   S->d_counter, cond);
-        if (e != cudaSuccess) return cuda_fail(e, "fused update/direction launch");
-    } else if (pre) {
+    if (pre) {
         pcg_update_kernel<true, COND><<<fit_grid(pcg_update_kernel<true, COND>, kT, needV), kT, 0, st>>>(
             S->n, S->x, S->r, S->p, S->q, S->dinv, S->d_s, S->d_partials, S->d_counter, cond);
         pcg_direction_kernel<true><<<fit_grid(pcg_direction_kernel<true>, kT, needV), kT, 0, st>>>(S->n, S->p, S->r,
@@ -387,17 +281,80 @@ int launch_iteration(ciecu_pcg_s* S, cudaStream_t st, cudaGraphConditionalHandle
     return CIECU_OK;
 }
 
+// Picks the K1 schedule by timing the fused SpMV + p^T q kernel itself on the
+// solver's buffers (p = 0 -> q); its register use, and so the best schedule,
+// differs from the plain operator's.
+int tune_solver_spmv(ciecu_pcg_s* S) {
+    if (S->kernel != 0) return CIECU_OK;
+    ciecu_csr_s* A = S->A;
+    cudaStream_t st = A->space->stream;
+    // p = D^-1 (or 1): positive, so p^T A p > 0 for an SPD matrix and the timed
+    // kernel never trips the breakdown flag (which would make later candidates
+    // return at once and win).
+    PcgScalars scratch{};
+    scratch.rz = 1.0;
+    CIECU_CUDA(cudaMemcpyAsync(S->d_s, &scratch, sizeof(PcgScalars), cudaMemcpyHostToDevice, st));
+    if (S->dinv)
+        CIECU_CUDA(cudaMemcpyAsync(S->p, S->dinv, sizeof(double) * S->n, cudaMemcpyDeviceToDevice, st));
+    else
+        fill_ones_kernel<<<grid_for(S->n, kT, 8), kT, 0, st>>>(S->n, S->p);
+    cudaEvent_t e0, e1;
+    CIECU_CUDA(cudaEventCreate(&e0));
+    CIECU_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    int bestK = A->kernel;
+    cudaError_t e = cudaSuccess;
+    for (int k : {1, 2, 4, 8, 16, 32}) {
+        if (k >= 16 && A->avgRow < k) continue;
+        auto launch = [&]() {
+            with_schedule(k, [&](auto kk) -> int {
+                constexpr int K = decltype(kk)::value;
+                pcg_spmv_kernel<K, false><<<fit_grid(pcg_spmv_kernel<K, false>, csr_threads<K>(), csr_grid(A, k)),
+                                            csr_threads<K>(), 0, st>>>(A->args<double>(), S->p, S->q, S->d_s,
+                                                                       S->d_partials, S->d_counter, 0);
+                return CIECU_OK;
+            });
+        };
+        for (int rep = 0; rep < 2; ++rep) launch();
+        for (int trial = 0; trial < 3 && e == cudaSuccess; ++trial) {  // best of three: robust to noise
+            cudaEventRecord(e0, st);
+            for (int rep = 0; rep < 3; ++rep) launch();
+            cudaEventRecord(e1, st);
+            count_launch(3);
+            e = cudaEventSynchronize(e1);
+            if (e != cudaSuccess) break;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms < best) {
+                best = ms;
+                bestK = k;
+            }
+        }
+        count_launch(2);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "pcg: K1 autotune");
+    // A breakdown during tuning (matrix not SPD) invalidates the timings: keep
+    // the operator's own schedule.
+    int flag = 0;
+    CIECU_CUDA(cudaMemcpyAsync(&flag, &S->d_s->done, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CIECU_CUDA(cudaStreamSynchronize(st));
+    S->kernel = flag ? A->kernel : bestK;
+    return CIECU_OK;
+}
+
 // The solve loop as a graph: a device-side WHILE loop over one iteration when the
 // driver supports conditional nodes, else `chunk` captured iterations that the
 // host replays until the done flag is set.
 int build_graph(ciecu_pcg_s* S) {
     cudaStream_t st = S->A->space->stream;
-    if (S->graph && S->graphKernel == S->A->kernel) return CIECU_OK;
+    if (S->graph && S->graphKernel == S->kernel) return CIECU_OK;
     if (S->graph) {
         cudaGraphExecDestroy(S->graph);
         S->graph = nullptr;
     }
-    S->fused = fused_update_enabled();
     int status = CIECU_ERR_ARGUMENT;
     if (device_loop_enabled())
         status = build_while_graph(st, [&](cudaGraph_t, cudaGraphConditionalHandle cond) {
@@ -405,7 +362,7 @@ int build_graph(ciecu_pcg_s* S) {
     }, &S->graph);
     if (status == CIECU_OK) {
         S->deviceLoop = true;
-        S->graphKernel = S->A->kernel;
+        S->graphKernel = S->kernel;
         return CIECU_OK;
     }
     cudaGetLastError();  // clear a sticky launch error of the failed attempt
@@ -423,7 +380,7 @@ int build_graph(ciecu_pcg_s* S) {
     e = cudaGraphInstantiate(&S->graph, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return cuda_fail(e, "pcg graph instantiate");
-    S->graphKernel = S->A->kernel;
+    S->graphKernel = S->kernel;
     return CIECU_OK;
 }
 
@@ -482,6 +439,13 @@ int ciecu_pcg_destroy(ciecu_pcg S) {
     return CIECU_OK;
 }
 
+int ciecu_pcg_info(ciecu_pcg S, int* spmvSchedule, int* deviceLoop) {
+    CIECU_REQUIRE(S, "pcg_info: null solver");
+    if (spmvSchedule) *spmvSchedule = S->kernel;
+    if (deviceLoop) *deviceLoop = S->deviceLoop ? 1 : 0;
+    return CIECU_OK;
+}
+
 int ciecu_pcg_set_graph_chunk(ciecu_pcg S, int iterations) {
     CIECU_REQUIRE(S && iterations >= 1 && iterations <= 4096, "pcg_set_graph_chunk: chunk must be in [1, 4096]");
     if (S->chunk != iterations && S->graph) {
@@ -505,6 +469,7 @@ int ciecu_pcg_product(ciecu_pcg S, double inScale, const double* d_in, double ou
         return CIECU_OK;
     }
     CIECU_TRY(ensure_tuned(A));
+    CIECU_TRY(tune_solver_spmv(S));
     // solution <- out (initial guess)
     CIECU_CUDA(cudaMemcpyAsync(S->x, d_out, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
     if (S->settings.iterationCount > 0) {
@@ -548,8 +513,6 @@ int ciecu_pcg_product(ciecu_pcg S, double inScale, const double* d_in, double ou
             if (S->h_s->done) break;
         }
         const PcgScalars& s = *S->h_s;
-        if (s.error == CIECU_ERR_TIMEOUT)
-            return fail(CIECU_ERR_TIMEOUT, "pcg: a device-side grid release timed out");
         if (s.error) {
             if (h_stats) *h_stats = ciecu_statistics{s.errorIter, s.absres, s.relres};
             if (s.errorKind == 1)

@@ -27,8 +27,6 @@ struct PcgScalars {
     int pad;
     long long chunkIter;   // iterations run by the current graph launch
     long long chunkLimit;  // iterations one graph launch may run
-    unsigned generation;   // grid-release counter of the fused update/direction kernel
-    unsigned pad2;
 };
 
 // Comparison::less with the default tolerances

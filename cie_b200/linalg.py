@@ -438,6 +438,15 @@ class ConjugateGradients(LinearOperator):
         if self._solver is not None:
             call("ciecu_pcg_set_graph_chunk", self._solver, int(iterations))
 
+    def info(self):
+        """SpMV schedule chosen for the fused solver kernel and whether the solve
+        runs as a device-side graph loop (fused device solver only)."""
+        if self._solver is None:
+            return {"fused": False}
+        k, d = ctypes.c_int(), ctypes.c_int()
+        call("ciecu_pcg_info", self._solver, ctypes.byref(k), ctypes.byref(d))
+        return {"fused": True, "spmv_schedule": k.value, "device_loop": bool(d.value)}
+
     def product(self, inScale, in_, outScale, out):
         n = self.space.size(out)
         if self.space.size(in_) != n:
@@ -536,7 +545,8 @@ class MixedPrecisionCG(LinearOperator):
     reliable updates (delta = replacement trigger), mode 1 = restarted iterative
     refinement (delta = inner tolerance).  Stops on the true FP64 residual."""
 
-    def __init__(self, lhs, inverseDiagonal, settings=None, mode=0, delta=None, compressColumns=True):
+    def __init__(self, lhs, inverseDiagonal, settings=None, mode=0, delta=None, compressColumns=True,
+                 innerKernel=0):
         if type(lhs) is not CSROperator or lhs.space._sfx != "f64":
             raise CiecuError(1, "MixedPrecisionCG needs an FP64 CSROperator")
         self.lhs = lhs
@@ -544,7 +554,7 @@ class MixedPrecisionCG(LinearOperator):
         self.inverseDiagonal = inverseDiagonal
         self.settings = settings if settings is not None else Statistics(5000, 0.0, 1e-10)
         delta = (0.1 if mode == 0 else 1e-4) if delta is None else float(delta)
-        self.options = MixedOptions(int(mode), delta, int(bool(compressColumns)))
+        self.options = MixedOptions(int(mode), delta, int(bool(compressColumns)), int(innerKernel))
         h = ctypes.c_void_p()
         self.space.enter()
         call("ciecu_mixed_create", lhs.csr.handle, _ptr(inverseDiagonal.inverseDiagonal), self.settings, self.options,
@@ -566,7 +576,7 @@ class MixedPrecisionCG(LinearOperator):
         e = ctypes.c_int64()
         call("ciecu_mixed_padded_entries", self._solver, ctypes.byref(e))
         return {"compressed_columns": bool(c.value), "format": "sell-32x4", "padded_entries": e.value,
-                "group_unroll": v.value}
+                "group_unroll": v.value, "inner_kernel": "tma-pipeline" if v.value == 0 else "registers"}
 
     def set_graph_chunk(self, iterations):
         call("ciecu_mixed_set_graph_chunk", self._solver, int(iterations))

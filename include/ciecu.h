@@ -169,8 +169,13 @@ int ciecu_pcg_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_stati
 int ciecu_pcg_destroy(ciecu_pcg solver);
 int ciecu_pcg_product(ciecu_pcg solver, double inScale, const double* d_in, double outScale,
                       double* d_out, ciecu_statistics* h_stats);
-/* Iterations captured per CUDA graph launch between host convergence checks. */
+/* Iterations captured per CUDA graph launch between host convergence checks
+ * (used when the device-side loop of conditional graph nodes is unavailable). */
 int ciecu_pcg_set_graph_chunk(ciecu_pcg solver, int iterations);
+/* SpMV schedule the solver's autotuner chose for its fused q = A p kernel (0 before
+ * the first solve; 1 = row-block stream kernel, else lanes per row) and whether the
+ * solve runs as a device-side graph loop (1) or host-polled graph chunks (0). */
+int ciecu_pcg_info(ciecu_pcg solver, int* spmvSchedule, int* deviceLoop);
 
 #ifdef __cplusplus
 }

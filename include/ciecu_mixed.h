@@ -28,6 +28,10 @@ typedef struct ciecu_mixed_options {
     /* 1: store column indices as 16-bit offsets from the row when the matrix
      * bandwidth is below 2^15 (checked; int32 otherwise). */
     int compressColumns;
+    /* Inner SpMV kernel: 0 lets the autotuner choose; 1, 2 or 4 fixes the groups
+     * of four entries each thread keeps in flight; -1 fixes the TMA-pipelined
+     * kernel (matrix streamed through shared memory by bulk copies). */
+    int innerKernel;
 } ciecu_mixed_options;
 
 typedef struct ciecu_mixed_statistics {
@@ -48,7 +52,10 @@ int ciecu_mixed_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_sta
                        ciecu_mixed_options options, ciecu_mixed* out);
 int ciecu_mixed_destroy(ciecu_mixed solver);
 /* compressedColumns: 1 when the inner matrix stores 16-bit offsets; groupUnroll:
- * groups of four entries each thread keeps in flight (chosen by the autotuner). */
+ * groups of four entries each thread keeps in flight (chosen by the autotuner),
+ * 0 when the autotuner chose the TMA-pipelined inner SpMV (the matrix streamed
+ * through shared memory by bulk copies).  Synchronises the solver's stream and
+ * returns CIECU_ERR_TIMEOUT if a pipelined ciecu_mixed_apply_f32 gave up a wait. */
 int ciecu_mixed_info(ciecu_mixed solver, int* compressedColumns, int* groupUnroll);
 int ciecu_mixed_set_graph_chunk(ciecu_mixed solver, int iterations);
 /* d_out = A32 d_in: the solver's FP32 inner operator (FP32 values, 16-bit or

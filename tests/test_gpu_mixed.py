@@ -17,24 +17,27 @@ def space():
     return CUDASpace()
 
 
-def mixed_solve(space, m, b, mode=0, delta=None, compress=True, x0=None, settings=None):
+def mixed_solve(space, m, b, mode=0, delta=None, compress=True, x0=None, settings=None, inner=0):
     from cie_b200.linalg import CSROperator, MixedPrecisionCG, Statistics, makeDiagonalOperator
     A = CSROperator(m, space)
     D = makeDiagonalOperator(m, space, csr_handle=A.csr)
     solver = MixedPrecisionCG(A, D, settings or Statistics(20000, 0.0, 1e-10), mode=mode, delta=delta,
-                              compressColumns=compress)
+                              compressColumns=compress, innerKernel=inner)
     x = dev(np.zeros(len(b)) if x0 is None else x0)
     solver.product(0.0, dev(b), 1.0, x)
     return host(x), solver.getStats(), solver.info()
 
 
-@pytest.mark.parametrize("mode,compress", [(0, True), (0, False), (1, True)])
-def test_mixed_3d_lognormal_vs_reference(space, reference, mode, compress):
+@pytest.mark.parametrize("mode,compress,inner", [(0, True, 0), (0, False, 0), (1, True, 0), (0, True, -1),
+                                                 (0, False, -1), (1, True, -1), (0, True, 1), (0, True, 4)])
+def test_mixed_3d_lognormal_vs_reference(space, reference, mode, compress, inner):
     from cie_b200.fem import make_poisson
     prob = make_poisson(space, 3, 1, [40, 40, 40], seed=2)
     rp, col, val = prob.host_csr()
     b = host(prob.rhs)
-    x, st, info = mixed_solve(space, prob.matrix, b, mode=mode, compress=compress)
+    x, st, info = mixed_solve(space, prob.matrix, b, mode=mode, compress=compress, inner=inner)
+    if inner:
+        assert info["group_unroll"] == max(inner, 0)
     xr, sr, err, _ = reference.pcg(rp, col, val, b, maxit=20000, abstol=0.0, reltol=1e-10)
     rel = np.linalg.norm(x - xr) / np.linalg.norm(xr)
     tr = true_residual(rp, col, val, x, b)
@@ -109,13 +112,16 @@ def test_mixed_settings_and_output_scales(space):
     assert st7.innerIterations == 7 and st7.refinements >= 1 and st7.relativeResidual > 1e-10
 
 
-def test_sell_inner_operator_on_ragged_rows(space, restatement):
+@pytest.mark.parametrize("compress", [True, False])
+@pytest.mark.parametrize("inner", [0, 1, 2, 4, -1])
+def test_sell_inner_operator_on_ragged_rows(space, restatement, inner, compress):
     """The FP32 SELL-32 inner operator on rows of very different lengths (empty rows,
-    ragged slices, a row longer than a slice), against the oracle SpMV of the same
-    FP32-rounded values."""
+    ragged slices, a row longer than a slice, a partial last slice), against the
+    oracle SpMV of the same FP32-rounded values; every inner kernel sums each row
+    in entry order, so all of them agree bit for bit."""
     from cie_b200.linalg import CSROperator, MixedPrecisionCG, Statistics, makeDiagonalOperator
     rng = np.random.default_rng(7)
-    n = 1000
+    n = 1003
     lens = rng.integers(0, 12, n)
     lens[::97] = 0
     lens[500] = 700
@@ -130,12 +136,19 @@ def test_sell_inner_operator_on_ragged_rows(space, restatement):
     val[rp[:-1] + np.array([r.index(i) for i, r in enumerate(rows)])] = 50.0  # dominant diagonal
     m = matrix(rp, col, val, n)
     A = CSROperator(m, space)
-    M = MixedPrecisionCG(A, makeDiagonalOperator(m, space, csr_handle=A.csr), Statistics(100, 0.0, 1e-10))
+    D = makeDiagonalOperator(m, space, csr_handle=A.csr)
+    M = MixedPrecisionCG(A, D, Statistics(100, 0.0, 1e-10), compressColumns=compress, innerKernel=inner)
     info = M.info()
     assert info["padded_entries"] >= len(col)
+    assert info["compressed_columns"] == compress
     x = rng.uniform(-1, 1, n).astype(np.float32)
     y = torch.empty(n, dtype=torch.float32, device="cuda")
     M.apply_inner(dev(x, torch.float32), y)
+    M.info()  # raises if a pipelined wait gave up
+    base = MixedPrecisionCG(A, D, Statistics(100, 0.0, 1e-10), compressColumns=compress, innerKernel=1)
+    y1 = torch.empty(n, dtype=torch.float32, device="cuda")
+    base.apply_inner(dev(x, torch.float32), y1)
+    assert torch.equal(y, y1)
     ref = restatement.spmv(rp, col, val.astype(np.float32).astype(np.float64), 0, x.astype(np.float64), 1,
                            np.zeros(n))
     scale = np.array([np.sum(np.abs(val[rp[i]:rp[i + 1]] * x[col[rp[i]:rp[i + 1]]])) for i in range(n)]) + 1e-30
