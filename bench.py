@@ -178,6 +178,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="ncu target: solves only (no e2e, no CPU baseline, no clock sampling)")
+    ap.add_argument("--profile-kernels", action="store_true",
+                    help="with --profile: no solves, only three launches each of the FP32 SELL and FP64 CSR SpMV "
+                         "after set-up (a short target for a full ncu capture)")
     ap.add_argument("--profile-cells", type=int, default=PROFILE_CELLS[0],
                     help="cells per axis of the --profile case (96: 290 MB matrix; 128: the full workload)")
     args = ap.parse_args()
@@ -225,6 +228,23 @@ def main():
         xmx.zero_()
         mixed.product(0.0, prob.rhs, 1.0, xmx)
 
+    if args.profile and args.profile_kernels:
+        from cie_b200.linalg import _ptr
+        lib = _lib.load()
+        x32, y32 = torch.rand(n, dtype=torch.float32, device="cuda"), torch.empty(n, dtype=torch.float32,
+                                                                                   device="cuda")
+        xr, yr = torch.rand(n, dtype=torch.float64, device="cuda"), torch.empty_like(prob.rhs)
+        _lib.check(lib.ciecu_csr_spmv_f64(A.csr.handle, 0.0, _ptr(xr), 1.0, _ptr(yr)))  # schedule tuned here
+        space.synchronize()
+        torch.cuda.nvtx.range_push("profile_kernels")  # ncu --nvtx --nvtx-include "profile_kernels/"
+        for _ in range(3):
+            _lib.check(lib.ciecu_mixed_apply_f32(mixed._solver, _ptr(x32), _ptr(y32)))
+            _lib.check(lib.ciecu_csr_spmv_f64(A.csr.handle, 0.0, _ptr(xr), 1.0, _ptr(yr)))
+        space.synchronize()
+        torch.cuda.nvtx.range_pop()
+        print(json.dumps({"profile": True, "kernels_only": True, "cells": cells, "fp64_info": cg.info(),
+                          "mixed_info": mixed.info()}), flush=True)
+        return
     for _ in range(args.warmup):
         solve_mixed()
         solve_fp64()
