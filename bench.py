@@ -313,10 +313,14 @@ def main():
     fp64_solve_bytes = (it64 + 1) * iter64_bytes + (12 * nnz + 4 * (n + 1) + 24 * n)
     refine_bytes = 12 * nnz + 4 * (n + 1) + 28 * n  # FP64 residual pass: x64, b read, r32 written, dinv32
     mixed_solve_bytes = mst.innerIterations * inner_bytes + (mst.refinements + 1) * refine_bytes
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tpath):
-        traffic = json.load(open(tpath)).get("mixed_spmv_f32_idx16_poisson3d_q1_128", None)
+    # DRAM bytes per launch from the committed ncu capture of the same kernel on the same workload
+    traffic = traffic64 = None
+    tpath = os.path.join(ROOT, "profiles", "dram_traffic_poisson3d_q1_128.txt")
+    if os.path.exists(tpath) and cells == [128, 128, 128]:
+        figures = dict(line.split() for line in open(tpath) if line.strip() and not line.startswith("#"))
+        if info["compressed_columns"] and info["group_unroll"] > 0:
+            traffic = int(figures.get("mixed_apply_kernel_f32_sell16", 0)) or None
+        traffic64 = int(figures.get("spmv_kernel_f64_csr", 0)) or None
 
     # end to end through the public API with host buffers
     rp_h, col_h, val_h = [t.cpu().pin_memory() for t in (prob.matrix.rowExtents, prob.matrix.columnIndices,
@@ -376,14 +380,17 @@ def main():
                      "achieved_gbs": fp64_solve_bytes / t_fp64 / 1e9,
                      "us_per_iteration": 1e6 * t_fp64 / (it64 + 1)},
             "speedup_mixed_vs_fp64": t_fp64 / t_mixed,
-            "roofline": {"bound": "hbm", "kernel": "mixed_apply_kernel (FP32 SELL-32 SpMV, %s columns, %d stored "
-                         "entries for %d nonzeros)" % ("16-bit" if info["compressed_columns"] else "int32",
-                                                       info["padded_entries"], nnz),
+            "roofline": {"bound": "hbm", "kernel": "%s (FP32 SELL-32 SpMV, %s columns, %d stored "
+                         "entries for %d nonzeros)" % (
+                             "mixed_apply_kernel<%d>" % info["group_unroll"] if info["group_unroll"] > 0
+                             else "mixed_apply_tma_kernel", "16-bit" if info["compressed_columns"] else "int32",
+                             info["padded_entries"], nnz),
                          "achieved": g32, "peak": hbm, "unit": "GB/s", "frac": g32 / hbm, "peak_kind": peak_kind,
                          "traffic": traffic, "algorithmic_bytes": spmv32_bytes, "launch_ms": 1e3 * t_spmv32},
             "fp64_spmv_roofline": {"kernel": "spmv_kernel (FP64 CSR, schedule %d)" % A.csr.kernel(),
                                    "achieved": spmv64_bytes / t_spmv64 / 1e9, "peak": hbm,
                                    "frac": spmv64_bytes / t_spmv64 / 1e9 / hbm, "algorithmic_bytes": spmv64_bytes,
+                                   "traffic": traffic64,
                                    "launch_ms": 1e3 * t_spmv64},
             "pcg_iteration_roofline": {"fp64_frac": fp64_solve_bytes / t_fp64 / 1e9 / hbm,
                                        "mixed_frac": mixed_solve_bytes / t_mixed / 1e9 / hbm,

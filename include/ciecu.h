@@ -7,7 +7,7 @@
  * Conventions
  *  - Every function returns 0 (CIECU_OK) or a CIECU_ERR_* code; the message of the
  *    last failure on the calling thread is available through ciecu_last_error.
- *    No C++ exception crosses this boundary; the C++ wrapper (cie_cuda/*.hpp)
+ *    No C++ exception crosses this boundary; the C++ wrapper (cie_cuda/linalg.hpp)
  *    turns a non-zero status into an exception, like CIE_CHECK / CIE_THROW
  *    (cieutils/packages/macros/inc/checks.hpp:17-23).
  *  - Pointers named d_* are device pointers, h_* host pointers.  Sizes are element
