@@ -70,6 +70,7 @@ SIGNATURES = {
     "ciecu_diagonal_inverse_f64": (c_int, [P, P]),
     "ciecu_diagonal_apply_f64": (c_int, [P, c_int64, P, c_double, P, c_double, P]),
     "ciecu_jacobi_f64": (c_int, [P, P, P, c_uint16, c_int64, c_double, c_double, P, c_double, P, P]),
+    "ciecu_jacobi_f64_static": (c_int, [P, P, P, c_uint16, c_int64, c_double, c_double, P, c_double, P]),
     "ciecu_masked_identity_f64": (c_int, [P, c_int64, P, c_uint16, c_double, P, c_double, P]),
     "ciecu_chebyshev_f64": (c_int, [P, P, c_int, c_double, c_double, c_double, P, c_double, P, P]),
     "ciecu_power_lambda_max_f64": (c_int, [P, P, c_int, c_uint64, P, P]),

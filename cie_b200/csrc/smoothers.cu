@@ -8,7 +8,14 @@
 #include "spmv.cuh"
 #include "space.cuh"
 
+#include <mutex>
 #include <string>
+
+// Scratch of ciecu_jacobi_f64_static: the two Jacobi iterates of a matrix of at
+// most CIECU_JACOBI_STATIC_MAX_ROWS rows (2 x 262144 doubles = 4 MiB), part of
+// this library's device image, so using it needs no allocation.  One array per
+// device, shared by every call on that device.
+static __device__ __align__(256) double g_jacobiStaticScratch[2 * CIECU_JACOBI_STATIC_MAX_ROWS];
 
 namespace ciecu {
 namespace {
@@ -202,6 +209,35 @@ __global__ void __launch_bounds__(csr_threads<KERNEL>())
     csr_rows<KERNEL, double, double, false>(A, v, op);
 }
 
+// Device address of g_jacobiStaticScratch on `device` (which must be current),
+// looked up on the first call for that device and remembered.  Allocates nothing.
+constexpr int kStaticScratchDevices = 64;
+
+int jacobi_static_scratch(int device, double** out) {
+    static std::mutex mutex;
+    static double* table[kStaticScratchDevices] = {};
+    if (device < 0 || device >= kStaticScratchDevices)
+        return fail(CIECU_ERR_ARGUMENT, "jacobi_f64_static: device ordinal " + std::to_string(device) +
+                                            " is beyond the " + std::to_string(kStaticScratchDevices) +
+                                            " devices this entry point supports");
+    std::lock_guard<std::mutex> lock(mutex);
+    if (!table[device]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_jacobiStaticScratch);
+        if (e != cudaSuccess) return cuda_fail(e, "jacobi_f64_static: cudaGetSymbolAddress(static scratch)");
+        table[device] = static_cast<double*>(p);
+    }
+    *out = table[device];
+    return CIECU_OK;
+}
+
+// Row schedule for a matrix whose SpMV schedule was never tuned (tuning
+// allocates): lanes per row from the mean row length.
+int untuned_schedule(const ciecu_csr_s* csr) {
+    const double avg = csr->rows > 0 ? static_cast<double>(csr->nnz) / csr->rows : 0.0;
+    return avg < 6.0 ? 2 : avg < 12.0 ? 4 : avg < 24.0 ? 8 : avg < 48.0 ? 16 : 32;
+}
+
 }  // namespace
 }  // namespace ciecu
 
@@ -372,6 +408,60 @@ int ciecu_power_lambda_max_f64(ciecu_csr csr, const double* d_inverse, int itera
     CIECU_CUDA(cudaStreamSynchronize(st));
     *h_lambda = space->h_result[3];
     CIECU_CHECK_LAUNCH("power");
+    return CIECU_OK;
+}
+
+int ciecu_jacobi_f64_static(ciecu_csr csr, const double* d_inverse, const uint16_t* d_mask, uint16_t threshold,
+                            int64_t iterations, double relaxation, double inScale, const double* d_in,
+                            double outScale, double* d_out) {
+    CIECU_REQUIRE(csr && csr->valueType == CIECU_F64, "jacobi_f64_static: FP64 matrix expected");
+    CIECU_REQUIRE(csr->rows == csr->cols, "inconsistent input vector sizes");
+    CIECU_REQUIRE(iterations >= 0, "jacobi_f64_static: negative iteration count");
+    const long n = csr->rows;
+    if (n > CIECU_JACOBI_STATIC_MAX_ROWS)
+        return fail(CIECU_ERR_ARGUMENT, "jacobi_f64_static: " + std::to_string(n) +
+                                            " rows exceed the static scratch of " +
+                                            std::to_string(CIECU_JACOBI_STATIC_MAX_ROWS) +
+                                            " rows; use ciecu_jacobi_f64 with caller-provided scratch");
+    if (n == 0) return CIECU_OK;
+    CIECU_REQUIRE(d_inverse && d_in && d_out, "jacobi_f64_static: null vector");
+    int device = -1;
+    CIECU_CUDA(cudaGetDevice(&device));
+    CIECU_REQUIRE(device == csr->space->device, "jacobi_f64_static: the matrix's device must be the current device");
+    double* scratch = nullptr;
+    CIECU_TRY(jacobi_static_scratch(device, &scratch));
+    cudaStream_t st = csr->space->stream;
+    double* xa = scratch;
+    double* xb = scratch + n;
+    const int gridV = grid_for(n, kT, 8);
+    if (iterations == 0) {
+        CIECU_CUDA(cudaMemsetAsync(xa, 0, sizeof(double) * n, st));
+    } else {
+        jacobi_first_kernel<<<gridV, kT, 0, st>>>(n, d_in, d_inverse, relaxation, xa);
+        count_launch();
+        const int schedule = csr->kernel != 0 ? csr->kernel : untuned_schedule(csr);
+        for (int64_t s = 1; s < iterations; ++s) {
+            CIECU_TRY(with_schedule(schedule, [&](auto k) -> int {
+                constexpr int K = decltype(k)::value;
+                // no occupancy query: a fixed multiple of the SM count (the row
+                // passes stride over the grid, so any grid size is correct)
+                const long cap = static_cast<long>(sm_count()) * (2048 / csr_threads<K>());
+                const int grid = static_cast<int>(std::min<long>(csr_grid(csr, K), cap));
+                if (d_mask)
+                    jacobi_sweep_kernel<K, true><<<grid, csr_threads<K>(), 0, st>>>(
+                        csr->args<double>(d_mask, threshold), d_in, d_inverse, relaxation, xa, xb);
+                else
+                    jacobi_sweep_kernel<K, false><<<grid, csr_threads<K>(), 0, st>>>(
+                        csr->args<double>(), d_in, d_inverse, relaxation, xa, xb);
+                return CIECU_OK;
+            }));
+            count_launch();
+            std::swap(xa, xb);
+        }
+    }
+    jacobi_output_kernel<<<gridV, kT, 0, st>>>(n, xa, inScale, outScale, d_out);
+    count_launch();
+    CIECU_CHECK_LAUNCH("jacobi_f64_static");
     return CIECU_OK;
 }
 

@@ -141,6 +141,29 @@ int ciecu_diagonal_apply_f64(ciecu_space space, int64_t n, const double* d_inver
 int ciecu_jacobi_f64(ciecu_csr csr, const double* d_inverse, const uint16_t* d_mask, uint16_t threshold,
                      int64_t iterations, double relaxation, double inScale, const double* d_in,
                      double outScale, double* d_out, double* d_work);
+/* Allocation-free ciecu_jacobi_f64: the same sweeps and result, without d_work.
+ * No counterpart in the reference.
+ * It is for callers that cannot allocate device memory at the call: hosts whose
+ * own pool owns every byte of device memory and that forbid a library from
+ * calling cudaMalloc behind their back, and code on a path where cudaMalloc or
+ * cudaFree would fail or stall -- both are refused while a stream is being
+ * captured in global mode, and cudaFree waits for the whole device.
+ * The two iterates live in a static device array inside this library, 4 MiB:
+ * matrices of more than CIECU_JACOBI_STATIC_MAX_ROWS rows are rejected with
+ * CIECU_ERR_ARGUMENT.  The call makes no cudaMalloc, cudaFree or other
+ * allocating call (an untuned matrix is not tuned, since tuning allocates; its
+ * row schedule then follows from the mean row length).
+ * The first call on a device looks up the array's device address once, with
+ * that device current (it must be the matrix's device): make the first call
+ * before any stream capture.  All calls on a device share the one array, which
+ * keeps the last call's contents; every iterate is written in full before it is
+ * read, so nothing has to start at zero.  Calls that overlap on the GPU (other
+ * streams, other host threads, other matrices on the same device) race on the
+ * array and corrupt each other's results: serialise them. */
+#define CIECU_JACOBI_STATIC_MAX_ROWS 262144
+int ciecu_jacobi_f64_static(ciecu_csr csr, const double* d_inverse, const uint16_t* d_mask, uint16_t threshold,
+                            int64_t iterations, double relaxation, double inScale, const double* d_in,
+                            double outScale, double* d_out);
 /* MaskedIdentityOperator<..>::product (MaskedIdentityOperator.cpp:14-74):
  * out = combine(inScale, out, outScale, mask < threshold ? in : 0). */
 int ciecu_masked_identity_f64(ciecu_space space, int64_t n, const uint16_t* d_mask, uint16_t threshold,
