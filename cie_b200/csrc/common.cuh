@@ -45,6 +45,13 @@ int sm_count();
         if (_s != CIECU_OK) return _s;                                \
     } while (0)
 
+// Loads of matrix values and indices: read once per pass over a matrix larger than
+// L2, so they are marked evict-first and leave the cache to the gathered vector.
+template <typename T>
+__device__ __forceinline__ T stream_ld(const T* p) {
+    return __ldcs(p);
+}
+
 // ---- reductions ------------------------------------------------------------
 
 template <typename T>

@@ -29,15 +29,15 @@ struct Group4;
 template <>
 struct Group4<float> {
     static __device__ __forceinline__ void load(const float* p, float (&v)[4]) {
-        const float4 a = __ldg(reinterpret_cast<const float4*>(p));
+        const float4 a = stream_ld(reinterpret_cast<const float4*>(p));
         v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
     }
 };
 template <>
 struct Group4<double> {
     static __device__ __forceinline__ void load(const double* p, double (&v)[4]) {
-        const double2 a = __ldg(reinterpret_cast<const double2*>(p));
-        const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+        const double2 a = stream_ld(reinterpret_cast<const double2*>(p));
+        const double2 b = stream_ld(reinterpret_cast<const double2*>(p) + 1);
         v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
     }
 };
@@ -47,7 +47,7 @@ struct GroupCols;
 template <>
 struct GroupCols<short> {
     static __device__ __forceinline__ void load(const short* p, int row, int (&c)[4]) {
-        const uint2 a = __ldg(reinterpret_cast<const uint2*>(p));
+        const uint2 a = stream_ld(reinterpret_cast<const uint2*>(p));
         c[0] = row + static_cast<short>(a.x & 0xffffu);
         c[1] = row + static_cast<short>(a.x >> 16);
         c[2] = row + static_cast<short>(a.y & 0xffffu);
@@ -57,17 +57,24 @@ struct GroupCols<short> {
 template <>
 struct GroupCols<int> {
     static __device__ __forceinline__ void load(const int* p, int, int (&c)[4]) {
-        const int4 a = __ldg(reinterpret_cast<const int4*>(p));
+        const int4 a = stream_ld(reinterpret_cast<const int4*>(p));
         c[0] = a.x; c[1] = a.y; c[2] = a.z; c[3] = a.w;
     }
 };
 
-// Row sums with the pre/post epilogue interface of spmv.cuh.  The grid-stride loop
-// moves whole warps (blockDim and the grid are multiples of 32), so a warp always
-// covers 32 consecutive rows of one slice.  U groups (4U entries) per lane are in
-// flight before the FMA chain.
-template <int U, typename T, typename V, typename CI, typename Op>
-__device__ __forceinline__ void sell_rows(const SellArgs<V, CI>& A, const T* __restrict__ x, Op& op) {
+// x[c] read through the read-only path: the operand of a plain SpMV.
+template <typename T>
+struct LoadGather {
+    const T* __restrict__ x;
+    __device__ __forceinline__ T operator()(int c) const { return __ldg(x + c); }
+};
+
+// Row sums with the pre/post epilogue interface of spmv.cuh, the operand entry of
+// column c given by gather(c).  The grid-stride loop moves whole warps (blockDim
+// and the grid are multiples of 32), so a warp always covers 32 consecutive rows
+// of one slice.  U groups (4U entries) per lane are in flight before the FMA chain.
+template <int U, typename T, typename V, typename CI, typename Op, typename TGather>
+__device__ __forceinline__ void sell_rows_gather(const SellArgs<V, CI>& A, const TGather& gather, Op& op) {
     const long stride = static_cast<long>(gridDim.x) * blockDim.x;
     for (long rl = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; rl < A.nrows; rl += stride) {
         const int r = static_cast<int>(rl);
@@ -99,7 +106,7 @@ __device__ __forceinline__ void sell_rows(const SellArgs<V, CI>& A, const T* __r
 #pragma unroll
             for (int u = 0; u < U; ++u)
 #pragma unroll
-                for (int e = 0; e < 4; ++e) xv[u][e] = 4 * (g + u) + e < len ? __ldg(x + c[u][e]) : T(0);
+                for (int e = 0; e < 4; ++e) xv[u][e] = 4 * (g + u) + e < len ? gather(c[u][e]) : T(0);
 #pragma unroll
             for (int u = 0; u < U; ++u)
 #pragma unroll
@@ -107,6 +114,11 @@ __device__ __forceinline__ void sell_rows(const SellArgs<V, CI>& A, const T* __r
         }
         op.post(r, pre, sum);
     }
+}
+
+template <int U, typename T, typename V, typename CI, typename Op>
+__device__ __forceinline__ void sell_rows(const SellArgs<V, CI>& A, const T* __restrict__ x, Op& op) {
+    sell_rows_gather<U, T, V, CI>(A, LoadGather<T>{x}, op);
 }
 
 }  // namespace ciecu

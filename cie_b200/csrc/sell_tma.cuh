@@ -93,11 +93,12 @@ __device__ __forceinline__ void smem_cols4<int>(const int* sc, int idx, int, int
 }
 
 // Row sums of every slice assigned to this warp (slices warp, warp + nwarps, ...),
-// calling op.pre at a slice's first chunk and op.post after its last.  `smem` is
-// the CTA's dynamic shared memory of TmaShape<float, CI>::SMEM bytes.
-template <typename CI, typename Op>
-__device__ __forceinline__ void sell_rows_tma(const SellArgs<float, CI>& A, const float* __restrict__ x, Op& op,
-                                              unsigned char* smem, unsigned* errorFlag) {
+// the operand entry of column c given by gather(c), calling op.pre at a slice's
+// first chunk and op.post after its last.  `smem` is the CTA's dynamic shared
+// memory of TmaShape<float, CI>::SMEM bytes.
+template <typename CI, typename Op, typename TGather>
+__device__ __forceinline__ void sell_rows_tma_gather(const SellArgs<float, CI>& A, const TGather& gather, Op& op,
+                                                     unsigned char* smem, unsigned* errorFlag) {
     using Shape = TmaShape<float, CI>;
     constexpr int S = Shape::STAGES;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -193,10 +194,10 @@ __device__ __forceinline__ void sell_rows_tma(const SellArgs<float, CI>& A, cons
                 int c[4];
                 smem_cols4<CI>(sc, gl * 32 + lane, row, c);
                 const int base = 4 * (g0 + gl);
-                const float xv0 = base + 0 < len ? __ldg(x + c[0]) : 0.0f;
-                const float xv1 = base + 1 < len ? __ldg(x + c[1]) : 0.0f;
-                const float xv2 = base + 2 < len ? __ldg(x + c[2]) : 0.0f;
-                const float xv3 = base + 3 < len ? __ldg(x + c[3]) : 0.0f;
+                const float xv0 = base + 0 < len ? gather(c[0]) : 0.0f;
+                const float xv1 = base + 1 < len ? gather(c[1]) : 0.0f;
+                const float xv2 = base + 2 < len ? gather(c[2]) : 0.0f;
+                const float xv3 = base + 3 < len ? gather(c[3]) : 0.0f;
                 sum = fmaf(v.x, xv0, sum);
                 sum = fmaf(v.y, xv1, sum);
                 sum = fmaf(v.z, xv2, sum);
@@ -221,6 +222,12 @@ __device__ __forceinline__ void sell_rows_tma(const SellArgs<float, CI>& A, cons
         }
         __syncwarp();
     }
+}
+
+template <typename CI, typename Op>
+__device__ __forceinline__ void sell_rows_tma(const SellArgs<float, CI>& A, const float* __restrict__ x, Op& op,
+                                              unsigned char* smem, unsigned* errorFlag) {
+    sell_rows_tma_gather<CI>(A, LoadGather<float>{x}, op, smem, errorFlag);
 }
 
 }  // namespace ciecu

@@ -82,7 +82,7 @@ struct Col4<int> {
     }
     static __device__ __forceinline__ int one(const int* p, int row) {
         (void)row;
-        return __ldg(p);
+        return stream_ld(p);
     }
 };
 template <>
@@ -94,7 +94,7 @@ struct Col4<short> {
         c[2] = row + static_cast<short>(a.y & 0xffffu);
         c[3] = row + static_cast<short>(a.y >> 16);
     }
-    static __device__ __forceinline__ int one(const short* p, int row) { return row + __ldg(p); }
+    static __device__ __forceinline__ int one(const short* p, int row) { return row + stream_ld(p); }
 };
 
 template <bool MASKED, typename T, typename V, typename CI>
@@ -213,7 +213,7 @@ __device__ __forceinline__ void vector_rows(const CsrArgs<V, CI>& A, const T* __
                 for (int u = 0; u < UNROLL; ++u) {
                     const int kk = k + u * VS;
                     const bool in = kk < k1;
-                    v[u] = in ? __ldg(A.val + kk) : V(0);
+                    v[u] = in ? stream_ld(A.val + kk) : V(0);
                     c[u] = in ? Col4<CI>::one(A.col + kk, r) : -1;
                 }
                 T xv[UNROLL];
