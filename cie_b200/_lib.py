@@ -101,6 +101,7 @@ SIGNATURES = {
     "ciecu_assembly_color_count": (c_int, [P, P]),
     "ciecu_assemble_stiffness": (c_int, [P, P, P, c_int, c_int, P]),
     "ciecu_element_gradient": (c_int, [P, P, c_int, P, P, P, P]),
+    "ciecu_adjoint_gradient": (c_int, [P, P, P, c_int, P, P, P, P, P, P, P]),
     "ciecu_dirichlet_eliminate": (c_int, [P, P, P, P]),
 }
 

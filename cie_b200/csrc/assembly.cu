@@ -220,6 +220,13 @@ __global__ void dirichlet_kernel(int n, const int* __restrict__ rowptr, const in
     }
 }
 
+// out = v with the entries of eliminated (boundary) DoFs set to zero.
+__global__ void interior_kernel(int n, const double* __restrict__ v, const uint8_t* __restrict__ bnd,
+                                double* __restrict__ out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        out[i] = bnd[i] ? 0.0 : v[i];
+}
+
 void convention_factors(int dim, const double* h, int convention, double& scale, double f[3]) {
     scale = 1.0;
     for (int d = 0; d < 3; ++d) f[d] = 1.0;
@@ -405,6 +412,39 @@ int ciecu_element_gradient(ciecu_assembly P, const double* h_cellSize, int conve
     }
     CIECU_CHECK_LAUNCH("element_gradient_kernel");
     return CIECU_OK;
+}
+
+int ciecu_adjoint_gradient(ciecu_pcg solver, ciecu_assembly P, const double* h_cellSize, int convention,
+                           const uint8_t* d_isBoundary, const double* d_u, const double* d_dJdu, double* d_lambda,
+                           double* d_gradKappa, double* d_work, ciecu_statistics* h_stats) {
+    CIECU_REQUIRE(solver && P && h_cellSize && d_u && d_dJdu && d_lambda && d_gradKappa && d_work,
+                  "adjoint_gradient: null argument");
+    const int n = P->csr->rows;
+    cudaStream_t st = P->csr->space->stream;
+    double* lamMasked = d_work;
+    double* uMasked = d_work + n;
+    double* unit = d_work + 2L * n;
+    const double* rhs = d_dJdu;
+    if (d_isBoundary && n > 0) {
+        interior_kernel<<<grid_for(n, kT, 8), kT, 0, st>>>(n, d_dJdu, d_isBoundary, lamMasked);
+        count_launch();
+        CIECU_CHECK_LAUNCH("interior_kernel");
+        rhs = lamMasked;
+    }
+    // adjoint solve from lambda = 0; A is symmetric, so A^T lambda = P dJ/du is the same PCG
+    if (n > 0) CIECU_CUDA(cudaMemsetAsync(d_lambda, 0, sizeof(double) * n, st));
+    CIECU_TRY(ciecu_pcg_product(solver, 0.0, rhs, 1.0, d_lambda, h_stats));
+    const double* lam = d_lambda;
+    const double* u = d_u;
+    if (d_isBoundary && n > 0) {
+        interior_kernel<<<grid_for(n, kT, 8), kT, 0, st>>>(n, d_lambda, d_isBoundary, lamMasked);
+        interior_kernel<<<grid_for(n, kT, 8), kT, 0, st>>>(n, d_u, d_isBoundary, uMasked);
+        count_launch(2);
+        CIECU_CHECK_LAUNCH("interior_kernel");
+        lam = lamMasked;
+        u = uMasked;
+    }
+    return ciecu_element_gradient(P, h_cellSize, convention, lam, u, d_gradKappa, unit);
 }
 
 int ciecu_dirichlet_eliminate(ciecu_csr csr, const uint8_t* d_isBoundary, double* d_entries, double* d_rhs) {

@@ -45,6 +45,22 @@ int ciecu_assemble_stiffness(ciecu_assembly plan, const double* d_kappa, const d
 int ciecu_element_gradient(ciecu_assembly plan, const double* h_cellSize, int convention, const double* d_lambda,
                            const double* d_u, double* d_grad, double* d_work);
 
+/* Adjoint sensitivities of an objective J(u) of u = A(kappa)^-1 P b, where
+ * A(kappa) = sum_e kappa_e K_e with the DoFs flagged in d_isBoundary eliminated
+ * symmetrically and P zeroes those DoFs (homogeneous Dirichlet).  The method of
+ * the reference's 1-D adjoint model (fem/python/modules/fem/optcontrol/
+ * adjointmodel.py:16-126, adjointelement.py:70-84), for the Q_p stiffness here:
+ *     lambda        = A^-1 P dJ/du     (the transposed solve: A is symmetric, so
+ *                                       the same PCG `solver`, started from 0)
+ *     dJ/db         = lambda           (written to d_lambda)
+ *     dJ/dkappa_e   = -(P lambda)_e^T K_e(kappa = 1) (P u)_e   (d_gradKappa)
+ * d_isBoundary may be NULL (nothing eliminated).  solver and plan must use the
+ * same space.  d_work: 2n + nb*nb doubles.  h_stats (may be NULL): statistics of
+ * the adjoint solve. */
+int ciecu_adjoint_gradient(ciecu_pcg solver, ciecu_assembly plan, const double* h_cellSize, int convention,
+                           const uint8_t* d_isBoundary, const double* d_u, const double* d_dJdu, double* d_lambda,
+                           double* d_gradKappa, double* d_work, ciecu_statistics* h_stats);
+
 /* Symmetric elimination of homogeneous Dirichlet DoFs (fem/test/test_1d.cpp:291-313):
  * rows and columns of boundary DoFs zeroed (structural zeros kept), diagonal 1,
  * d_rhs[boundary] = 0 (d_rhs may be NULL). */
