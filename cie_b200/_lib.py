@@ -102,6 +102,10 @@ SIGNATURES = {
     "ciecu_assemble_stiffness": (c_int, [P, P, P, c_int, c_int, P]),
     "ciecu_element_gradient": (c_int, [P, P, c_int, P, P, P, P]),
     "ciecu_adjoint_gradient": (c_int, [P, P, P, c_int, P, P, P, P, P, P, P]),
+    "ciecu_batch_create": (c_int, [P, c_int64, P, P, Statistics, P]),
+    "ciecu_batch_destroy": (c_int, [P]),
+    "ciecu_batch_info": (c_int, [P, P, P, P]),
+    "ciecu_batch_product": (c_int, [P, c_double, P, c_double, P, P]),
     "ciecu_dirichlet_eliminate": (c_int, [P, P, P, P]),
 }
 

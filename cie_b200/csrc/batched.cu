@@ -1,0 +1,637 @@
+// Batched Jacobi-preconditioned CG: many independent SPD systems of different
+// sizes solved together, each with its own scalars and stopping test
+// (ConjugateGradients_impl.hpp:49-201 per system; the reference runs one solver
+// object per system).
+//
+// The systems are one block-diagonal CSR matrix: system s owns rows and columns
+// rowOffsets[s] .. rowOffsets[s+1]-1.  The rows are cut into tiles of at most
+// kTileRows rows that never cross a system, so one CTA handles one tile at a
+// time and every tile belongs to exactly one system.  A dot product of system s
+// is reduced deterministically: each tile writes its partial, and the last of the
+// system's tiles to finish (a per-system ticket) sums them in tile order and
+// forms the system's alpha / beta / stopping decision.  Tiles of finished systems
+// return at once, so the work shrinks as systems converge.
+//
+// One iteration = three kernels over all systems (K1 SpMV + p^T q, K2 update +
+// dots + decision, K3 direction), run by the same device-side graph loop as the
+// single-system solver; K3 ends the loop when every system is finished.
+#include "graph.cuh"
+#include "pcg.cuh"
+#include "ciecu_batch.h"
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+namespace ciecu {
+namespace {
+
+constexpr int kT = 256;
+constexpr int kTileRows = 2048;
+
+struct BatchScalars {
+    double rz, pq, alpha, beta, rr, r0, absres, relres;
+    long long iter;
+    int done;   // 0 running, 1 converged, 2 iteration limit, 3 breakdown
+    int errorKind;  // 1: r^T z <= 0 at start, 2: p^T A p <= 0
+    long long errorIter;
+};
+
+struct BatchGlobal {
+    unsigned finished;   // systems that are done
+    unsigned pad;
+    long long chunkIter, chunkLimit;
+    long long maxIter;
+    double absTol, relTol;
+    int badColumn;       // an entry outside its system's block (set-up check)
+    int pad2;
+};
+
+struct Tile {
+    int system;
+    int rowBegin, rowEnd;
+    int slot;  // position among the system's tiles
+};
+
+template <bool COND>
+__device__ __forceinline__ void set_loop(cudaGraphConditionalHandle cond, unsigned value) {
+    if constexpr (COND) cudaGraphSetConditional(cond, value);
+}
+
+// Tile-level reduction of K values; the CTA holding the system's last tile gets
+// the system totals (in tile order) in every thread and returns true.
+template <int K>
+__device__ __forceinline__ bool system_reduce_last(const double (&mine)[K], const Tile& t, const int* tileBegin,
+                                                   const int* tileCount, double* partials, unsigned* counter,
+                                                   double (&out)[K]) {
+    __shared__ double s_red[32];
+    __shared__ bool s_last;
+    double sums[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) sums[k] = block_sum<double, kT>(mine[k], s_red);
+    const int first = tileBegin[t.system];
+    const int count = tileCount[t.system];
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) partials[static_cast<long>(first + t.slot) * K + k] = sums[k];
+        __threadfence();
+        const unsigned ticket = atomicAdd(&counter[t.system], 1u);
+        s_last = ticket == static_cast<unsigned>(count - 1);
+    }
+    __syncthreads();
+    if (!s_last) return false;
+    __threadfence();
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        double acc = 0.0;
+        const volatile double* p = partials;
+        for (int j = threadIdx.x; j < count; j += kT) acc += p[static_cast<long>(first + j) * K + k];
+        out[k] = block_sum<double, kT>(acc, s_red);
+    }
+    if (threadIdx.x == 0) counter[t.system] = 0u;
+    return true;
+}
+
+// Rows [rb, re) of the tile: VS lanes per row, the CTA's warps striding over rows.
+template <int VS, typename Op>
+__device__ __forceinline__ void tile_rows(const CsrArgs<double>& A, int rb, int re, const double* __restrict__ x,
+                                          Op& op) {
+    constexpr int RPW = 32 / VS;
+    constexpr int UNROLL = VS <= 4 ? 8 : 4;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int sub = lane % VS, slot = lane / VS;
+    for (int base = rb + warp * RPW; base < re; base += (kT / 32) * RPW) {
+        const int r = base + slot;
+        const bool valid = r < re;
+        typename Op::Pre pre{};
+        if (valid && sub == 0) pre = op.pre(r);
+        double sum = 0.0;
+        if (valid) {
+            const int k1 = A.rowptr[r + 1];
+            for (int k = A.rowptr[r] + sub; k < k1; k += UNROLL * VS) {
+                double v[UNROLL];
+                int c[UNROLL];
+#pragma unroll
+                for (int u = 0; u < UNROLL; ++u) {
+                    const int kk = k + u * VS;
+                    const bool in = kk < k1;
+                    v[u] = in ? stream_ld(A.val + kk) : 0.0;
+                    c[u] = in ? stream_ld(A.col + kk) : -1;
+                }
+                double xv[UNROLL];
+#pragma unroll
+                for (int u = 0; u < UNROLL; ++u) xv[u] = c[u] >= 0 ? __ldg(x + c[u]) : 0.0;
+#pragma unroll
+                for (int u = 0; u < UNROLL; ++u) sum = fma(v[u], xv[u], sum);
+            }
+        }
+#pragma unroll
+        for (int offset = VS / 2; offset > 0; offset >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, offset, VS);
+        if (valid && sub == 0) op.post(r, pre, sum);
+    }
+}
+
+struct PqOp {
+    using Pre = double;
+    const double* __restrict__ p;
+    double* __restrict__ q;
+    double acc;
+    __device__ __forceinline__ double pre(int r) const { return p[r]; }
+    __device__ __forceinline__ void post(int r, double pr, double sum) {
+        q[r] = sum;
+        acc = fma(pr, sum, acc);
+    }
+};
+
+// Set-up check: every entry of row r lies in the column block of r's system.
+__global__ void batch_check_kernel(CsrArgs<double> A, const Tile* __restrict__ tiles, int ntiles,
+                                   const long long* __restrict__ rowOffsets, BatchGlobal* g) {
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const Tile tile = tiles[t];
+        const long long c0 = rowOffsets[tile.system], c1 = rowOffsets[tile.system + 1];
+        for (int r = tile.rowBegin + threadIdx.x; r < tile.rowEnd; r += kT)
+            for (int k = A.rowptr[r]; k < A.rowptr[r + 1]; ++k)
+                if (A.col[k] < c0 || A.col[k] >= c1) atomicMin(&g->badColumn, r);
+    }
+}
+
+// r = b - A x is formed before; z = D^-1 r, p = z, rr, rz and the initial test.
+__global__ void __launch_bounds__(kT) batch_init_kernel(const Tile* __restrict__ tiles, int ntiles,
+                                                        const int* tileBegin, const int* tileCount,
+                                                        const double* __restrict__ r, const double* __restrict__ dinv,
+                                                        double* __restrict__ p, BatchScalars* S, BatchGlobal* g,
+                                                        double* partials, unsigned* counter) {
+    for (int ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
+        const Tile t = tiles[ti];
+        double rr = 0.0, rz = 0.0;
+        for (int i = t.rowBegin + threadIdx.x; i < t.rowEnd; i += kT) {
+            const double ri = r[i];
+            const double zi = ri * dinv[i];
+            p[i] = zi;
+            rr = fma(ri, ri, rr);
+            rz = fma(ri, zi, rz);
+        }
+        double mine[2] = {rr, rz}, tot[2];
+        if (system_reduce_last<2>(mine, t, tileBegin, tileCount, partials, counter, tot) && threadIdx.x == 0) {
+            BatchScalars& s = S[t.system];
+            s.rr = tot[0];
+            s.r0 = sqrt(tot[0]);
+            s.absres = s.r0;
+            s.relres = 1.0;
+            s.iter = 0;
+            s.done = 0;
+            s.errorKind = 0;
+            s.errorIter = 0;
+            if (float_less(s.absres, g->absTol) || float_less(s.relres, g->relTol)) {
+                s.done = 1;
+            } else {
+                s.rz = tot[1];
+                if (!(0.0 < s.rz)) {
+                    s.done = 3;
+                    s.errorKind = 1;
+                } else if (g->maxIter <= 0) {
+                    s.done = 2;
+                }
+            }
+            if (s.done) atomicAdd(&g->finished, 1u);
+        }
+        __syncthreads();
+    }
+}
+
+// K1: q = A p and p^T q per system; alpha.
+template <int VS>
+__global__ void __launch_bounds__(kT) batch_spmv_kernel(CsrArgs<double> A, const Tile* __restrict__ tiles, int ntiles,
+                                                        const int* tileBegin, const int* tileCount,
+                                                        const double* __restrict__ p, double* __restrict__ q,
+                                                        BatchScalars* S, BatchGlobal* g, double* partials,
+                                                        unsigned* counter) {
+    for (int ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
+        const Tile t = tiles[ti];
+        if (*reinterpret_cast<volatile int*>(&S[t.system].done)) continue;
+        PqOp op{p, q, 0.0};
+        tile_rows<VS>(A, t.rowBegin, t.rowEnd, p, op);
+        double mine[1] = {op.acc}, tot[1];
+        if (system_reduce_last<1>(mine, t, tileBegin, tileCount, partials, counter, tot) && threadIdx.x == 0) {
+            BatchScalars& s = S[t.system];
+            s.pq = tot[0];
+            if (!(0.0 < tot[0])) {
+                s.done = 3;
+                s.errorKind = 2;
+                s.errorIter = s.iter;
+                atomicAdd(&g->finished, 1u);
+            } else {
+                s.alpha = s.rz / tot[0];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// K2: x += alpha p; r -= alpha q; rr, rz; beta and the stopping test per system.
+__global__ void __launch_bounds__(kT) batch_update_kernel(const Tile* __restrict__ tiles, int ntiles,
+                                                          const int* tileBegin, const int* tileCount,
+                                                          double* __restrict__ x, double* __restrict__ r,
+                                                          const double* __restrict__ p, const double* __restrict__ q,
+                                                          const double* __restrict__ dinv, BatchScalars* S,
+                                                          BatchGlobal* g, double* partials, unsigned* counter) {
+    for (int ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
+        const Tile t = tiles[ti];
+        BatchScalars& s = S[t.system];
+        if (*reinterpret_cast<volatile int*>(&s.done)) continue;
+        const double alpha = s.alpha, malpha = -alpha;
+        double rr = 0.0, rz = 0.0;
+        for (int i = t.rowBegin + threadIdx.x; i < t.rowEnd; i += kT) {
+            x[i] = fma(alpha, p[i], x[i]);
+            const double ri = fma(malpha, q[i], r[i]);
+            r[i] = ri;
+            rr = fma(ri, ri, rr);
+            rz = fma(ri, ri * dinv[i], rz);
+        }
+        double mine[2] = {rr, rz}, tot[2];
+        if (system_reduce_last<2>(mine, t, tileBegin, tileCount, partials, counter, tot) && threadIdx.x == 0) {
+            s.rr = tot[0];
+            s.beta = tot[1] / s.rz;
+            s.rz = tot[1];
+            s.absres = sqrt(tot[0]);
+            s.relres = s.absres / s.r0;
+            if (float_less(s.absres, g->absTol) || float_less(s.relres, g->relTol)) {
+                s.done = 1;
+            } else {
+                s.iter += 1;
+                if (s.iter >= g->maxIter) s.done = 2;
+            }
+            if (s.done) atomicAdd(&g->finished, 1u);
+        }
+        __syncthreads();
+    }
+}
+
+// K3: p = beta p + z (the rounding of space.scale + space.add, as the single
+// solver); ends the loop when every system is finished.
+template <bool COND>
+__global__ void __launch_bounds__(kT) batch_direction_kernel(const Tile* __restrict__ tiles, int ntiles, int systems,
+                                                             double* __restrict__ p, const double* __restrict__ r,
+                                                             const double* __restrict__ dinv,
+                                                             const BatchScalars* S, BatchGlobal* g,
+                                                             cudaGraphConditionalHandle cond) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        g->chunkIter += 1;
+        const bool more = *reinterpret_cast<volatile unsigned*>(&g->finished) < static_cast<unsigned>(systems);
+        set_loop<COND>(cond, (more && g->chunkIter < g->chunkLimit) ? 1u : 0u);
+    }
+    for (int ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
+        const Tile t = tiles[ti];
+        const BatchScalars& s = S[t.system];
+        if (*reinterpret_cast<const volatile int*>(&s.done)) continue;
+        const double beta = s.beta;
+        for (int i = t.rowBegin + threadIdx.x; i < t.rowEnd; i += kT)
+            p[i] = __dadd_rn(__dmul_rn(p[i], beta), __dmul_rn(r[i], dinv[i]));
+    }
+}
+
+__global__ void batch_output_kernel(long n, double inScale, double outScale, const double* __restrict__ x,
+                                    double* __restrict__ out) {
+    const long stride = static_cast<long>(gridDim.x) * blockDim.x;
+    for (long i = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const double xi = x[i];
+        double o = out[i];
+        if (inScale == 1.0) {
+            o = outScale == 1.0 ? o + xi : (outScale == -1.0 ? o - xi : o + outScale * xi);
+        } else if (inScale == 0.0) {
+            o = xi * outScale;
+        } else {
+            o *= inScale;
+            o = outScale == 1.0 ? o + xi : (outScale == -1.0 ? o - xi : o + outScale * xi);
+        }
+        out[i] = o;
+    }
+}
+
+// Calls f(std::integral_constant<int, VS>) for VS in {2, 4, 8, 16, 32}.
+template <typename F>
+int with_lanes(int vs, F&& f) {
+    switch (vs) {
+        case 2: return f(std::integral_constant<int, 2>{});
+        case 8: return f(std::integral_constant<int, 8>{});
+        case 16: return f(std::integral_constant<int, 16>{});
+        case 32: return f(std::integral_constant<int, 32>{});
+        default: return f(std::integral_constant<int, 4>{});
+    }
+}
+
+}  // namespace
+}  // namespace ciecu
+
+struct ciecu_batch_s {
+    ciecu_csr_s* A = nullptr;
+    const double* dinv = nullptr;
+    ciecu_statistics settings{};
+    long n = 0;
+    int systems = 0, ntiles = 0;
+    int lanes = 4;  // lanes per row of K1 (autotuned)
+    ciecu::Tile* d_tiles = nullptr;
+    int* d_tileBegin = nullptr;
+    int* d_tileCount = nullptr;
+    long long* d_rowOffsets = nullptr;
+    double *x = nullptr, *r = nullptr, *p = nullptr, *q = nullptr;
+    ciecu::BatchScalars* d_s = nullptr;
+    ciecu::BatchGlobal* d_g = nullptr;
+    ciecu::BatchGlobal* h_g = nullptr;
+    double* d_partials = nullptr;
+    unsigned* d_counter = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    bool deviceLoop = false;
+    int chunk = 16;
+    int grid = 1;
+};
+
+namespace ciecu {
+namespace {
+
+template <bool COND>
+int launch_batch_iteration(ciecu_batch_s* B, cudaStream_t st, cudaGraphConditionalHandle cond) {
+    CIECU_TRY(with_lanes(B->lanes, [&](auto v) -> int {
+        constexpr int VS = decltype(v)::value;
+        batch_spmv_kernel<VS><<<B->grid, kT, 0, st>>>(B->A->args<double>(), B->d_tiles, B->ntiles, B->d_tileBegin,
+                                                      B->d_tileCount, B->p, B->q, B->d_s, B->d_g, B->d_partials,
+                                                      B->d_counter);
+        return CIECU_OK;
+    }));
+    batch_update_kernel<<<B->grid, kT, 0, st>>>(B->d_tiles, B->ntiles, B->d_tileBegin, B->d_tileCount, B->x, B->r,
+                                                B->p, B->q, B->dinv, B->d_s, B->d_g, B->d_partials, B->d_counter);
+    batch_direction_kernel<COND><<<B->grid, kT, 0, st>>>(B->d_tiles, B->ntiles, B->systems, B->p, B->r, B->dinv,
+                                                         B->d_s, B->d_g, cond);
+    CIECU_CHECK_LAUNCH("batched pcg iteration");
+    return CIECU_OK;
+}
+
+int build_batch_graph(ciecu_batch_s* B) {
+    if (B->graph) return CIECU_OK;
+    cudaStream_t st = B->A->space->stream;
+    if (device_loop_enabled()) {
+        const int status = build_while_graph(st, [&](cudaGraph_t, cudaGraphConditionalHandle cond) {
+            return launch_batch_iteration<true>(B, st, cond);
+        }, &B->graph);
+        if (status == CIECU_OK) {
+            B->deviceLoop = true;
+            return CIECU_OK;
+        }
+        cudaGetLastError();
+    }
+    B->deviceLoop = false;
+    cudaGraph_t g = nullptr;
+    CIECU_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int status = CIECU_OK;
+    for (int i = 0; i < B->chunk && status == CIECU_OK; ++i) status = launch_batch_iteration<false>(B, st, 0);
+    cudaError_t e = cudaStreamEndCapture(st, &g);
+    if (status != CIECU_OK) {
+        if (g) cudaGraphDestroy(g);
+        return status;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "batched graph capture");
+    e = cudaGraphInstantiate(&B->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(e, "batched graph instantiate");
+    return CIECU_OK;
+}
+
+// Times K1 for each lane count on the solver's buffers (p = D^-1 > 0, every
+// system running) and keeps the fastest.
+int tune_batch(ciecu_batch_s* B) {
+    cudaStream_t st = B->A->space->stream;
+    std::vector<BatchScalars> scratch(B->systems);
+    for (auto& s : scratch) {
+        s = BatchScalars{};
+        s.rz = 1.0;
+    }
+    CIECU_CUDA(cudaMemcpyAsync(B->d_s, scratch.data(), sizeof(BatchScalars) * B->systems, cudaMemcpyHostToDevice, st));
+    CIECU_CUDA(cudaMemcpyAsync(B->p, B->dinv, sizeof(double) * B->n, cudaMemcpyDeviceToDevice, st));
+    cudaEvent_t e0, e1;
+    CIECU_CUDA(cudaEventCreate(&e0));
+    CIECU_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    int bestLanes = 4;
+    cudaError_t e = cudaSuccess;
+    const double avg = B->n > 0 ? static_cast<double>(B->A->nnz) / B->n : 0.0;
+    for (int vs : {2, 4, 8, 16, 32}) {
+        if (vs >= 16 && avg < vs) continue;
+        auto launch = [&]() {
+            with_lanes(vs, [&](auto v) -> int {
+                constexpr int VS = decltype(v)::value;
+                batch_spmv_kernel<VS><<<B->grid, kT, 0, st>>>(B->A->args<double>(), B->d_tiles, B->ntiles,
+                                                              B->d_tileBegin, B->d_tileCount, B->p, B->q, B->d_s,
+                                                              B->d_g, B->d_partials, B->d_counter);
+                return CIECU_OK;
+            });
+        };
+        launch();
+        for (int trial = 0; trial < 3 && e == cudaSuccess; ++trial) {
+            cudaEventRecord(e0, st);
+            for (int rep = 0; rep < 3; ++rep) launch();
+            cudaEventRecord(e1, st);
+            e = cudaEventSynchronize(e1);
+            float ms = 0.f;
+            if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+            if (e == cudaSuccess && ms < best) {
+                best = ms;
+                bestLanes = vs;
+            }
+        }
+        count_launch(10);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "batched pcg: autotune");
+    B->lanes = bestLanes;
+    return CIECU_OK;
+}
+
+}  // namespace
+}  // namespace ciecu
+
+using namespace ciecu;
+
+extern "C" {
+
+int ciecu_batch_create(ciecu_csr lhs, int64_t systems, const int64_t* h_rowOffsets, const double* d_inverseDiagonal,
+                       ciecu_statistics settings, ciecu_batch* out) {
+    CIECU_REQUIRE(lhs && out && h_rowOffsets && d_inverseDiagonal, "batch_create: null argument");
+    CIECU_REQUIRE(lhs->valueType == CIECU_F64 && lhs->rows == lhs->cols, "batch_create: square FP64 matrix expected");
+    CIECU_REQUIRE(systems >= 1 && systems <= (1 << 24), "batch_create: system count out of range");
+    CIECU_REQUIRE(h_rowOffsets[0] == 0 && h_rowOffsets[systems] == lhs->rows,
+                  "batch_create: row offsets must start at 0 and end at the row count");
+    std::vector<Tile> tiles;
+    std::vector<int> tileBegin(static_cast<size_t>(systems)), tileCount(static_cast<size_t>(systems));
+    for (int64_t s = 0; s < systems; ++s) {
+        CIECU_REQUIRE(h_rowOffsets[s + 1] > h_rowOffsets[s], "batch_create: every system needs at least one row");
+        tileBegin[s] = static_cast<int>(tiles.size());
+        int slot = 0;
+        for (int64_t r = h_rowOffsets[s]; r < h_rowOffsets[s + 1]; r += kTileRows)
+            tiles.push_back(Tile{static_cast<int>(s), static_cast<int>(r),
+                                 static_cast<int>(std::min<int64_t>(r + kTileRows, h_rowOffsets[s + 1])), slot++});
+        tileCount[s] = slot;
+    }
+    auto* B = new ciecu_batch_s();
+    B->A = lhs;
+    B->dinv = d_inverseDiagonal;
+    B->settings = settings;
+    B->n = lhs->rows;
+    B->systems = static_cast<int>(systems);
+    B->ntiles = static_cast<int>(tiles.size());
+    cudaStream_t st = lhs->space->stream;
+    const size_t n = static_cast<size_t>(B->n);
+    cudaError_t e = cudaMalloc(&B->d_tiles, sizeof(Tile) * tiles.size());
+    if (e == cudaSuccess) e = cudaMalloc(&B->d_tileBegin, sizeof(int) * systems);
+    if (e == cudaSuccess) e = cudaMalloc(&B->d_tileCount, sizeof(int) * systems);
+    if (e == cudaSuccess) e = cudaMalloc(&B->d_rowOffsets, sizeof(long long) * (systems + 1));
+    for (double** v : {&B->x, &B->r, &B->p, &B->q})
+        if (e == cudaSuccess) e = cudaMalloc(v, sizeof(double) * std::max<size_t>(1, n));
+    if (e == cudaSuccess) e = cudaMalloc(&B->d_s, sizeof(BatchScalars) * systems);
+    if (e == cudaSuccess) e = cudaMalloc(&B->d_g, sizeof(BatchGlobal));
+    if (e == cudaSuccess) e = cudaMallocHost(&B->h_g, sizeof(BatchGlobal));
+    if (e == cudaSuccess) e = cudaMalloc(&B->d_partials, sizeof(double) * 2 * tiles.size());
+    if (e == cudaSuccess) e = cudaMalloc(&B->d_counter, sizeof(unsigned) * systems);
+    if (e == cudaSuccess) e = cudaMemsetAsync(B->d_counter, 0, sizeof(unsigned) * systems, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(B->d_tiles, tiles.data(), sizeof(Tile) * tiles.size(), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(B->d_tileBegin, tileBegin.data(), sizeof(int) * systems, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(B->d_tileCount, tileCount.data(), sizeof(int) * systems, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(B->d_rowOffsets, h_rowOffsets, sizeof(long long) * (systems + 1), cudaMemcpyHostToDevice,
+                            st);
+    if (e != cudaSuccess) {
+        ciecu_batch_destroy(B);
+        return cuda_fail(e, "batch_create: allocation");
+    }
+    // every entry inside its system's block
+    BatchGlobal g{};
+    g.badColumn = 0x7fffffff;
+    e = cudaMemcpyAsync(B->d_g, &g, sizeof(BatchGlobal), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        batch_check_kernel<<<grid_for(B->ntiles * static_cast<long>(kT), kT, 8), kT, 0, st>>>(
+            lhs->args<double>(), B->d_tiles, B->ntiles, B->d_rowOffsets, B->d_g);
+        count_launch();
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&g, B->d_g, sizeof(BatchGlobal), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        ciecu_batch_destroy(B);
+        return cuda_fail(e, "batch_create: block check");
+    }
+    if (g.badColumn != 0x7fffffff) {
+        const int row = g.badColumn;
+        ciecu_batch_destroy(B);
+        return fail(CIECU_ERR_ARGUMENT, "batch_create: row " + std::to_string(row) +
+                                            " has an entry outside its system's column block");
+    }
+    B->grid = std::max(1, std::min(B->ntiles, resident_blocks(reinterpret_cast<const void*>(
+                                                                   batch_spmv_kernel<4>), kT, 0)));
+    const int status = tune_batch(B);
+    if (status != CIECU_OK) {
+        ciecu_batch_destroy(B);
+        return status;
+    }
+    *out = B;
+    return CIECU_OK;
+}
+
+int ciecu_batch_destroy(ciecu_batch B) {
+    if (!B) return CIECU_OK;
+    if (B->graph) cudaGraphExecDestroy(B->graph);
+    cudaFree(B->d_tiles);
+    cudaFree(B->d_tileBegin);
+    cudaFree(B->d_tileCount);
+    cudaFree(B->d_rowOffsets);
+    cudaFree(B->x);
+    cudaFree(B->r);
+    cudaFree(B->p);
+    cudaFree(B->q);
+    cudaFree(B->d_s);
+    cudaFree(B->d_g);
+    if (B->h_g) cudaFreeHost(B->h_g);
+    cudaFree(B->d_partials);
+    cudaFree(B->d_counter);
+    delete B;
+    return CIECU_OK;
+}
+
+int ciecu_batch_info(ciecu_batch B, int* lanesPerRow, int* deviceLoop, int64_t* tiles) {
+    CIECU_REQUIRE(B, "batch_info: null solver");
+    if (lanesPerRow) *lanesPerRow = B->lanes;
+    if (deviceLoop) *deviceLoop = B->deviceLoop ? 1 : 0;
+    if (tiles) *tiles = B->ntiles;
+    return CIECU_OK;
+}
+
+int ciecu_batch_product(ciecu_batch B, double inScale, const double* d_in, double outScale, double* d_out,
+                        ciecu_statistics* h_stats) {
+    CIECU_REQUIRE(B && d_in && d_out, "batch_product: null argument");
+    ciecu_csr_s* A = B->A;
+    cudaStream_t st = A->space->stream;
+    const long n = B->n;
+    CIECU_CUDA(cudaMemcpyAsync(B->x, d_out, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    std::vector<BatchScalars> s(static_cast<size_t>(B->systems));
+    if (B->settings.iterationCount > 0) {
+        BatchGlobal g{};
+        g.maxIter = B->settings.iterationCount;
+        g.absTol = B->settings.absoluteResidual;
+        g.relTol = B->settings.relativeResidual;
+        g.badColumn = 0x7fffffff;
+        *B->h_g = g;
+        CIECU_CUDA(cudaMemcpyAsync(B->d_g, B->h_g, sizeof(BatchGlobal), cudaMemcpyHostToDevice, st));
+        CIECU_CUDA(cudaMemcpyAsync(B->r, d_in, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+        CIECU_TRY(ciecu_csr_spmv_f64(A, 1.0, B->x, -1.0, B->r));  // r = b - A x0 (block diagonal: per system)
+        batch_init_kernel<<<B->grid, kT, 0, st>>>(B->d_tiles, B->ntiles, B->d_tileBegin, B->d_tileCount, B->r,
+                                                   B->dinv, B->p, B->d_s, B->d_g, B->d_partials, B->d_counter);
+        count_launch();
+        CIECU_CHECK_LAUNCH("batch_init_kernel");
+        CIECU_TRY(build_batch_graph(B));
+        const long long limit = B->deviceLoop ? 4096 : B->chunk;
+        for (;;) {
+            CIECU_CUDA(cudaMemcpyAsync(B->h_g, B->d_g, sizeof(BatchGlobal), cudaMemcpyDeviceToHost, st));
+            CIECU_CUDA(cudaStreamSynchronize(st));
+            if (B->h_g->finished >= static_cast<unsigned>(B->systems)) break;
+            B->h_g->chunkIter = 0;
+            B->h_g->chunkLimit = limit;
+            CIECU_CUDA(cudaMemcpyAsync(&B->d_g->chunkIter, &B->h_g->chunkIter, 2 * sizeof(long long),
+                                       cudaMemcpyHostToDevice, st));
+            CIECU_CUDA(cudaGraphLaunch(B->graph, st));
+            CIECU_CUDA(cudaMemcpyAsync(B->h_g, B->d_g, sizeof(BatchGlobal), cudaMemcpyDeviceToHost, st));
+            CIECU_CUDA(cudaStreamSynchronize(st));
+            count_launch(3LL * (B->deviceLoop ? B->h_g->chunkIter : B->chunk));
+            if (B->h_g->finished >= static_cast<unsigned>(B->systems)) break;
+        }
+        CIECU_CUDA(cudaMemcpyAsync(s.data(), B->d_s, sizeof(BatchScalars) * B->systems, cudaMemcpyDeviceToHost, st));
+        CIECU_CUDA(cudaStreamSynchronize(st));
+    }
+    batch_output_kernel<<<grid_for(n, kT, 8), kT, 0, st>>>(n, inScale, outScale, B->x, d_out);
+    count_launch();
+    CIECU_CHECK_LAUNCH("batch_output_kernel");
+    CIECU_CUDA(cudaStreamSynchronize(st));
+    int firstError = -1;
+    for (int i = 0; i < B->systems; ++i) {
+        const BatchScalars& si = s[i];
+        if (h_stats) {
+            if (B->settings.iterationCount > 0)
+                h_stats[i] = ciecu_statistics{si.done == 3 ? si.errorIter : si.iter, si.absres, si.relres};
+            else
+                h_stats[i] = ciecu_statistics{0, 1.7976931348623157e308, 1.7976931348623157e308};
+        }
+        if (si.done == 3 && firstError < 0) firstError = i;
+    }
+    if (firstError >= 0) {
+        const BatchScalars& si = s[firstError];
+        return fail(CIECU_ERR_BREAKDOWN,
+                    "system " + std::to_string(firstError) + ": " +
+                        (si.errorKind == 1 ? std::string("preconditioned norm vanished in iteration 0 (r^T @ z = 0)")
+                                           : "p^T @ A @ p vanished in iteration " + std::to_string(si.errorIter)));
+    }
+    return CIECU_OK;
+}
+
+}  // extern "C"

@@ -600,3 +600,78 @@ class MixedPrecisionCG(LinearOperator):
         finally:
             self._stats = stats
             self.space.leave()
+
+
+def block_diagonal(matrices):
+    """One block-diagonal CSRMatrix holding the given square device CSR matrices
+    (system s in rows/columns offsets[s] .. offsets[s+1]-1), and the row offsets."""
+    if not matrices:
+        raise CiecuError(1, "block_diagonal: no matrices")
+    rowptrs, cols, vals, offsets = [], [], [], [0]
+    nnz = 0
+    for m in matrices:
+        if m.rowCount() != m.columnCount:
+            raise CiecuError(1, "block_diagonal: square matrices expected")
+        rowptrs.append(m.rowExtents[:-1].to(torch.int64) + nnz)
+        cols.append(m.columnIndices.to(torch.int64) + offsets[-1])
+        vals.append(m.entries)
+        nnz += m.nnz()
+        offsets.append(offsets[-1] + m.rowCount())
+    if nnz >= 2 ** 31 or offsets[-1] >= 2 ** 31:
+        raise CiecuError(1, "block_diagonal: more than 2^31 rows or entries")
+    dev = matrices[0].rowExtents.device
+    rowptr = torch.cat(rowptrs + [torch.tensor([nnz], dtype=torch.int64, device=dev)]).to(torch.int32)
+    return (CSRMatrix(offsets[-1], rowptr, torch.cat(cols).to(torch.int32), torch.cat(vals)),
+            np.asarray(offsets, dtype=np.int64))
+
+
+class BatchedConjugateGradients(LinearOperator):
+    """Independent Jacobi-PCG solves of all systems of a block-diagonal matrix in
+    shared kernel launches (ciecu_batch_*); every system follows
+    ConjugateGradients_impl.hpp:49-201 with its own scalars and stopping test.
+    getStats() returns one Statistics per system."""
+
+    def __init__(self, lhs, rowOffsets, space, inverseDiagonal, settings=None):
+        self.lhs = lhs
+        self.space = space
+        self.rowOffsets = np.ascontiguousarray(rowOffsets, dtype=np.int64)
+        self.systems = len(self.rowOffsets) - 1
+        self.settings = settings if settings is not None else Statistics(0, 0.0, 0.0)
+        self.csr = inverseDiagonal._csr if getattr(inverseDiagonal, "_csr", None) is not None else _CSRHandle(
+            lhs, space)
+        self.inverseDiagonal = inverseDiagonal
+        h = ctypes.c_void_p()
+        space.enter()
+        call("ciecu_batch_create", self.csr.handle, self.systems, self.rowOffsets.ctypes.data_as(ctypes.c_void_p),
+             _ptr(inverseDiagonal.inverseDiagonal), self.settings, ctypes.byref(h))
+        space.leave()
+        self._solver = h
+        self._stats = None
+
+    def __del__(self):
+        try:
+            if getattr(self, "_solver", None):
+                _lib.load().ciecu_batch_destroy(self._solver)
+                self._solver = None
+        except Exception:
+            pass
+
+    def info(self):
+        v, d, t = ctypes.c_int(), ctypes.c_int(), ctypes.c_int64()
+        call("ciecu_batch_info", self._solver, ctypes.byref(v), ctypes.byref(d), ctypes.byref(t))
+        return {"lanes_per_row": v.value, "device_loop": bool(d.value), "tiles": t.value}
+
+    def getStats(self):
+        return self._stats
+
+    def product(self, inScale, in_, outScale, out):
+        self.space._check(in_, out)
+        if in_.numel() != out.numel() or out.numel() != self.lhs.rowCount():
+            raise CiecuError(1, "incompatible vector sizes")
+        stats = (Statistics * self.systems)()
+        self.space.enter()
+        try:
+            call("ciecu_batch_product", self._solver, float(inScale), _ptr(in_), float(outScale), _ptr(out), stats)
+        finally:
+            self._stats = list(stats)
+            self.space.leave()

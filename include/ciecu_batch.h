@@ -1,0 +1,45 @@
+/*
+ * ciecu batched solvers: many independent SPD systems in one device-resident
+ * Jacobi-preconditioned CG.  No reference counterpart as one object: the reference
+ * runs one ConjugateGradients per system
+ * (linalg/packages/solvers/impl/ConjugateGradients_impl.hpp:49-201); here every
+ * system follows that algorithm -- its own alpha, beta, stopping test
+ * (Comparison::less on the recursive residual, relative to its own ||r0||) and
+ * iteration count -- while all systems share each kernel launch.
+ */
+#ifndef CIECU_BATCH_H
+#define CIECU_BATCH_H
+
+#include "ciecu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ciecu_batch_s* ciecu_batch;
+
+/* lhs: the systems' matrices as one block-diagonal FP64 CSR; system s owns rows
+ * and columns h_rowOffsets[s] .. h_rowOffsets[s+1]-1 (systems + 1 offsets, the
+ * first 0, the last the row count; every system at least one row).  An entry
+ * outside its system's column block is rejected (CIECU_ERR_ARGUMENT).
+ * d_inverseDiagonal: the Jacobi preconditioner of all rows (ciecu_diagonal_inverse_f64).
+ * settings apply to every system.  Creation autotunes the lanes per row of the
+ * SpMV on lhs. */
+int ciecu_batch_create(ciecu_csr lhs, int64_t systems, const int64_t* h_rowOffsets,
+                       const double* d_inverseDiagonal, ciecu_statistics settings, ciecu_batch* out);
+int ciecu_batch_destroy(ciecu_batch solver);
+/* Lanes per row chosen by the autotuner, whether the solve loop runs on the device
+ * (conditional graph nodes), and the number of row tiles. */
+int ciecu_batch_info(ciecu_batch solver, int* lanesPerRow, int* deviceLoop, int64_t* tiles);
+/* All systems at once: initial guess = d_out; on return out = inScale*out +
+ * outScale*x per row.  h_stats (may be NULL): one ciecu_statistics per system.
+ * A breakdown in any system returns CIECU_ERR_BREAKDOWN naming the first such
+ * system; the other systems are solved and their statistics filled. */
+int ciecu_batch_product(ciecu_batch solver, double inScale, const double* d_in, double outScale,
+                        double* d_out, ciecu_statistics* h_stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CIECU_BATCH_H */
