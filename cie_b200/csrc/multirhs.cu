@@ -1,0 +1,539 @@
+// Multi-right-hand-side Jacobi-PCG (SpMM-CG): k <= 32 independent conjugate-
+// gradient solves against ONE matrix, each following ConjugateGradients_impl.hpp:
+// 49-201 with its own alpha, beta and stopping test, while every iteration reads
+// the matrix once for all k.  No reference counterpart as one object (the
+// reference would run k solver objects, one per right-hand side).
+//
+// Vectors are row-major n x k blocks (entry (i, c) at i*k + c).  A group of KP
+// lanes (KP = the power of two >= k) owns a row: it loads KP (value, column)
+// pairs of the row at a time, broadcasts each pair within the group by shuffle,
+// and lane c gathers P[j][c] -- k consecutive doubles, one coalesced access per
+// matrix entry for the group.  Each row sum runs over the entries in CSR order.
+// Dot products are per column, reduced in a fixed order (per-block column sums,
+// then the last block sums the blocks in block order).
+//
+// One iteration = three kernels (K1 SpMM + p_c^T q_c, K2 update + dots +
+// decision, K3 direction) in the device-side graph loop of the other solvers;
+// a column that has converged is left unchanged by K2/K3.
+#include "graph.cuh"
+#include "pcg.cuh"
+#include "ciecu_multi.h"
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+namespace ciecu {
+namespace {
+
+constexpr int kT = 256;
+constexpr int kWarps = kT / 32;
+
+struct ColumnScalars {
+    double rz, pq, alpha, beta, rr, r0, absres, relres;
+    long long iter;
+    int done;       // 0 running, 1 converged, 2 iteration limit, 3 breakdown
+    int errorKind;  // 1: r^T z <= 0 at start, 2: p^T A p <= 0
+    long long errorIter;
+};
+
+struct MultiGlobal {
+    unsigned finished;
+    unsigned pad;
+    long long chunkIter, chunkLimit, maxIter;
+    double absTol, relTol;
+};
+
+template <bool COND>
+__device__ __forceinline__ void set_loop(cudaGraphConditionalHandle cond, unsigned value) {
+    if constexpr (COND) cudaGraphSetConditional(cond, value);
+}
+
+// Per-column sums of NV values over the grid.  Every thread holds the values of
+// its column (lane % KP); the CTA holding the last block gets the totals of
+// column c in thread c (c < k) and returns true.  partials: NV x grid x 32.
+template <int KP, int NV>
+__device__ __forceinline__ bool column_reduce_last(const double (&mine)[NV], int k, double* partials,
+                                                   unsigned* counter, double (&out)[NV]) {
+    __shared__ double s_red[NV][kT];
+    __shared__ bool s_last;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) s_red[v][threadIdx.x] = mine[v];
+    __syncthreads();
+    if (threadIdx.x < k) {
+        const int c = threadIdx.x;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            double acc = 0.0;
+            for (int t = c; t < kT; t += KP) acc += s_red[v][t];  // fixed order: warps, then slots
+            partials[(static_cast<long>(v) * gridDim.x + blockIdx.x) * 32 + c] = acc;
+        }
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!s_last) return false;
+    __threadfence();
+    // column c = lane, blocks split over the warps, then the warps' sums in order
+    const int c = threadIdx.x & 31, part = threadIdx.x >> 5;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        double acc = 0.0;
+        const volatile double* p = partials + static_cast<long>(v) * gridDim.x * 32;
+        if (c < k)
+            for (unsigned b = part; b < gridDim.x; b += kWarps) acc += p[static_cast<long>(b) * 32 + c];
+        __syncthreads();
+        s_red[v][threadIdx.x] = acc;
+        __syncthreads();
+        if (threadIdx.x < k) {
+            double tot = 0.0;
+            for (int w = 0; w < kWarps; ++w) tot += s_red[v][w * 32 + threadIdx.x];
+            out[v] = tot;
+        }
+    }
+    if (threadIdx.x == 0) *counter = 0u;
+    return true;
+}
+
+// Row sums of A times the n x k block X for the rows of this group; calls
+// op(row, c, sum) for each row and active column.
+template <int KP, typename Op>
+__device__ __forceinline__ void multi_rows(const CsrArgs<double>& A, int k, const double* __restrict__ X, Op& op) {
+    constexpr int RPW = 32 / KP;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int slot = lane / KP, c = lane % KP;
+    const bool active = c < k;
+    const unsigned gmask = KP == 32 ? 0xffffffffu : (((1u << KP) - 1u) << (slot * KP));
+    const long n = A.nrows;
+    const long stride = static_cast<long>(gridDim.x) * kWarps * RPW;
+    for (long base = (static_cast<long>(blockIdx.x) * kWarps + warp) * RPW; base < n; base += stride) {
+        const long row = base + slot;
+        const bool valid = row < n;
+        const int k0 = valid ? A.rowptr[row] : 0;
+        const int k1 = valid ? A.rowptr[row + 1] : 0;
+        double acc = 0.0;
+        for (int e0 = k0; e0 < k1; e0 += KP) {
+            const int m = min(KP, k1 - e0);
+            const double a = c < m ? stream_ld(A.val + e0 + c) : 0.0;
+            const int col = c < m ? stream_ld(A.col + e0 + c) : 0;
+            for (int j = 0; j < m; j += 4) {
+                double av[4], pv[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int jj = j + u < m ? j + u : m - 1;
+                    av[u] = __shfl_sync(gmask, a, jj, KP);
+                    const int cj = __shfl_sync(gmask, col, jj, KP);
+                    pv[u] = (active && j + u < m) ? __ldg(X + static_cast<long>(cj) * k + c) : 0.0;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) acc = fma(av[u], pv[u], acc);
+            }
+        }
+        if (valid && active) op(row, c, acc);
+    }
+}
+
+struct ResidualOp {  // R = B - A X
+    const double* __restrict__ b;
+    double* __restrict__ r;
+    int k;
+    __device__ __forceinline__ void operator()(long row, int c, double sum) const {
+        r[row * k + c] = b[row * k + c] - sum;
+    }
+};
+
+template <int KP>
+__global__ void __launch_bounds__(kT) multi_residual_kernel(CsrArgs<double> A, int k, const double* __restrict__ X,
+                                                            const double* __restrict__ B, double* __restrict__ R) {
+    ResidualOp op{B, R, k};
+    multi_rows<KP>(A, k, X, op);
+}
+
+// Initial set-up per column: z = D^-1 r, p = z, rr, rz and the initial test.
+template <int KP>
+__global__ void __launch_bounds__(kT) multi_init_kernel(long n, int k, const double* __restrict__ R,
+                                                        const double* __restrict__ dinv, double* __restrict__ P,
+                                                        ColumnScalars* S, MultiGlobal* g, double* partials,
+                                                        unsigned* counter) {
+    constexpr int RPW = 32 / KP;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int slot = lane / KP, c = lane % KP;
+    double rr = 0.0, rz = 0.0;
+    const long stride = static_cast<long>(gridDim.x) * kWarps * RPW;
+    if (c < k)
+        for (long i = (static_cast<long>(blockIdx.x) * kWarps + warp) * RPW + slot; i < n; i += stride) {
+            const double ri = R[i * k + c];
+            const double zi = ri * dinv[i];
+            P[i * k + c] = zi;
+            rr = fma(ri, ri, rr);
+            rz = fma(ri, zi, rz);
+        }
+    double mine[2] = {rr, rz}, tot[2];
+    if (column_reduce_last<KP, 2>(mine, k, partials, counter, tot) && threadIdx.x < k) {
+        ColumnScalars& s = S[threadIdx.x];
+        s.rr = tot[0];
+        s.r0 = sqrt(tot[0]);
+        s.absres = s.r0;
+        s.relres = 1.0;
+        s.iter = 0;
+        s.done = 0;
+        s.errorKind = 0;
+        s.errorIter = 0;
+        if (float_less(s.absres, g->absTol) || float_less(s.relres, g->relTol)) {
+            s.done = 1;
+        } else {
+            s.rz = tot[1];
+            if (!(0.0 < s.rz)) {
+                s.done = 3;
+                s.errorKind = 1;
+            } else if (g->maxIter <= 0) {
+                s.done = 2;
+            }
+        }
+        if (s.done) atomicAdd(&g->finished, 1u);
+    }
+}
+
+struct PqOp {
+    const double* __restrict__ p;
+    double* __restrict__ q;
+    int k;
+    double acc;
+    __device__ __forceinline__ void operator()(long row, int c, double sum) {
+        q[row * k + c] = sum;
+        acc = fma(p[row * k + c], sum, acc);
+    }
+};
+
+// K1: Q = A P and p_c^T q_c; alpha per column.
+template <int KP, bool COND>
+__global__ void __launch_bounds__(kT) multi_spmv_kernel(CsrArgs<double> A, int k, const double* __restrict__ P,
+                                                        double* __restrict__ Q, ColumnScalars* S, MultiGlobal* g,
+                                                        double* partials, unsigned* counter,
+                                                        cudaGraphConditionalHandle cond) {
+    if (*reinterpret_cast<volatile unsigned*>(&g->finished) >= static_cast<unsigned>(k)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) set_loop<COND>(cond, 0);
+        return;
+    }
+    PqOp op{P, Q, k, 0.0};
+    multi_rows<KP>(A, k, P, op);
+    double mine[1] = {op.acc}, tot[1];
+    if (column_reduce_last<KP, 1>(mine, k, partials, counter, tot) && threadIdx.x < k) {
+        ColumnScalars& s = S[threadIdx.x];
+        if (!s.done) {
+            s.pq = tot[0];
+            if (!(0.0 < tot[0])) {
+                s.done = 3;
+                s.errorKind = 2;
+                s.errorIter = s.iter;
+                atomicAdd(&g->finished, 1u);
+            } else {
+                s.alpha = s.rz / tot[0];
+            }
+        }
+    }
+}
+
+// K2: X += alpha P; R -= alpha Q; rr, rz; beta and the stopping test per column.
+template <int KP>
+__global__ void __launch_bounds__(kT) multi_update_kernel(long n, int k, double* __restrict__ X,
+                                                          double* __restrict__ R, const double* __restrict__ P,
+                                                          const double* __restrict__ Q,
+                                                          const double* __restrict__ dinv, ColumnScalars* S,
+                                                          MultiGlobal* g, double* partials, unsigned* counter) {
+    if (*reinterpret_cast<volatile unsigned*>(&g->finished) >= static_cast<unsigned>(k)) return;
+    constexpr int RPW = 32 / KP;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int slot = lane / KP, c = lane % KP;
+    double rr = 0.0, rz = 0.0;
+    if (c < k && !S[c].done) {
+        const double alpha = S[c].alpha, malpha = -alpha;
+        const long stride = static_cast<long>(gridDim.x) * kWarps * RPW;
+        for (long i = (static_cast<long>(blockIdx.x) * kWarps + warp) * RPW + slot; i < n; i += stride) {
+            const long e = i * k + c;
+            X[e] = fma(alpha, P[e], X[e]);
+            const double ri = fma(malpha, Q[e], R[e]);
+            R[e] = ri;
+            rr = fma(ri, ri, rr);
+            rz = fma(ri, ri * dinv[i], rz);
+        }
+    }
+    double mine[2] = {rr, rz}, tot[2];
+    if (column_reduce_last<KP, 2>(mine, k, partials, counter, tot) && threadIdx.x < k) {
+        ColumnScalars& s = S[threadIdx.x];
+        if (!s.done) {
+            s.rr = tot[0];
+            s.beta = tot[1] / s.rz;
+            s.rz = tot[1];
+            s.absres = sqrt(tot[0]);
+            s.relres = s.absres / s.r0;
+            if (float_less(s.absres, g->absTol) || float_less(s.relres, g->relTol)) {
+                s.done = 1;
+            } else {
+                s.iter += 1;
+                if (s.iter >= g->maxIter) s.done = 2;
+            }
+            if (s.done) atomicAdd(&g->finished, 1u);
+        }
+    }
+}
+
+// K3: P = beta P + D^-1 R per running column; ends the loop when all are done.
+template <int KP, bool COND>
+__global__ void __launch_bounds__(kT) multi_direction_kernel(long n, int k, double* __restrict__ P,
+                                                             const double* __restrict__ R,
+                                                             const double* __restrict__ dinv,
+                                                             const ColumnScalars* S, MultiGlobal* g,
+                                                             cudaGraphConditionalHandle cond) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        g->chunkIter += 1;
+        const bool more = *reinterpret_cast<volatile unsigned*>(&g->finished) < static_cast<unsigned>(k);
+        set_loop<COND>(cond, (more && g->chunkIter < g->chunkLimit) ? 1u : 0u);
+    }
+    constexpr int RPW = 32 / KP;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int slot = lane / KP, c = lane % KP;
+    if (c >= k || S[c].done) return;
+    const double beta = S[c].beta;
+    const long stride = static_cast<long>(gridDim.x) * kWarps * RPW;
+    for (long i = (static_cast<long>(blockIdx.x) * kWarps + warp) * RPW + slot; i < n; i += stride) {
+        const long e = i * k + c;
+        P[e] = __dadd_rn(__dmul_rn(P[e], beta), __dmul_rn(R[e], dinv[i]));
+    }
+}
+
+__global__ void multi_output_kernel(long count, double inScale, double outScale, const double* __restrict__ x,
+                                    double* __restrict__ out) {
+    const long stride = static_cast<long>(gridDim.x) * blockDim.x;
+    for (long i = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += stride) {
+        const double xi = x[i];
+        double o = out[i];
+        if (inScale == 1.0) {
+            o = outScale == 1.0 ? o + xi : (outScale == -1.0 ? o - xi : o + outScale * xi);
+        } else if (inScale == 0.0) {
+            o = xi * outScale;
+        } else {
+            o *= inScale;
+            o = outScale == 1.0 ? o + xi : (outScale == -1.0 ? o - xi : o + outScale * xi);
+        }
+        out[i] = o;
+    }
+}
+
+template <typename F>
+int with_group(int kp, F&& f) {
+    switch (kp) {
+        case 1: return f(std::integral_constant<int, 1>{});
+        case 2: return f(std::integral_constant<int, 2>{});
+        case 4: return f(std::integral_constant<int, 4>{});
+        case 8: return f(std::integral_constant<int, 8>{});
+        case 16: return f(std::integral_constant<int, 16>{});
+        default: return f(std::integral_constant<int, 32>{});
+    }
+}
+
+}  // namespace
+}  // namespace ciecu
+
+struct ciecu_multi_s {
+    ciecu_csr_s* A = nullptr;
+    const double* dinv = nullptr;
+    ciecu_statistics settings{};
+    long n = 0;
+    int k = 0, kp = 1;
+    double *x = nullptr, *r = nullptr, *p = nullptr, *q = nullptr;
+    ciecu::ColumnScalars* d_s = nullptr;
+    ciecu::MultiGlobal* d_g = nullptr;
+    ciecu::MultiGlobal* h_g = nullptr;
+    double* d_partials = nullptr;
+    unsigned* d_counter = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    bool deviceLoop = false;
+    int chunk = 16;
+    int grid = 1;
+};
+
+namespace ciecu {
+namespace {
+
+template <bool COND>
+int launch_multi_iteration(ciecu_multi_s* M, cudaStream_t st, cudaGraphConditionalHandle cond) {
+    CIECU_TRY(with_group(M->kp, [&](auto kk) -> int {
+        constexpr int KP = decltype(kk)::value;
+        multi_spmv_kernel<KP, COND><<<M->grid, kT, 0, st>>>(M->A->args<double>(), M->k, M->p, M->q, M->d_s, M->d_g,
+                                                            M->d_partials, M->d_counter, cond);
+        multi_update_kernel<KP><<<M->grid, kT, 0, st>>>(M->n, M->k, M->x, M->r, M->p, M->q, M->dinv, M->d_s,
+                                                        M->d_g, M->d_partials, M->d_counter);
+        multi_direction_kernel<KP, COND><<<M->grid, kT, 0, st>>>(M->n, M->k, M->p, M->r, M->dinv, M->d_s, M->d_g,
+                                                                 cond);
+        return CIECU_OK;
+    }));
+    CIECU_CHECK_LAUNCH("multi-rhs pcg iteration");
+    return CIECU_OK;
+}
+
+int build_multi_graph(ciecu_multi_s* M) {
+    if (M->graph) return CIECU_OK;
+    cudaStream_t st = M->A->space->stream;
+    if (device_loop_enabled()) {
+        const int status = build_while_graph(st, [&](cudaGraph_t, cudaGraphConditionalHandle cond) {
+            return launch_multi_iteration<true>(M, st, cond);
+        }, &M->graph);
+        if (status == CIECU_OK) {
+            M->deviceLoop = true;
+            return CIECU_OK;
+        }
+        cudaGetLastError();
+    }
+    M->deviceLoop = false;
+    cudaGraph_t g = nullptr;
+    CIECU_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int status = CIECU_OK;
+    for (int i = 0; i < M->chunk && status == CIECU_OK; ++i) status = launch_multi_iteration<false>(M, st, 0);
+    cudaError_t e = cudaStreamEndCapture(st, &g);
+    if (status != CIECU_OK) {
+        if (g) cudaGraphDestroy(g);
+        return status;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "multi-rhs graph capture");
+    e = cudaGraphInstantiate(&M->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(e, "multi-rhs graph instantiate");
+    return CIECU_OK;
+}
+
+}  // namespace
+}  // namespace ciecu
+
+using namespace ciecu;
+
+extern "C" {
+
+int ciecu_multi_create(ciecu_csr lhs, int rhsCount, const double* d_inverseDiagonal, ciecu_statistics settings,
+                       ciecu_multi* out) {
+    CIECU_REQUIRE(lhs && out && d_inverseDiagonal, "multi_create: null argument");
+    CIECU_REQUIRE(lhs->valueType == CIECU_F64 && lhs->rows == lhs->cols, "multi_create: square FP64 matrix expected");
+    CIECU_REQUIRE(rhsCount >= 1 && rhsCount <= 32, "multi_create: 1 to 32 right-hand sides");
+    auto* M = new ciecu_multi_s();
+    M->A = lhs;
+    M->dinv = d_inverseDiagonal;
+    M->settings = settings;
+    M->n = lhs->rows;
+    M->k = rhsCount;
+    while (M->kp < rhsCount) M->kp <<= 1;
+    cudaStream_t st = lhs->space->stream;
+    const size_t count = std::max<size_t>(1, static_cast<size_t>(M->n) * M->k);
+    cudaError_t e = cudaSuccess;
+    for (double** v : {&M->x, &M->r, &M->p, &M->q})
+        if (e == cudaSuccess) e = cudaMalloc(v, sizeof(double) * count);
+    if (e == cudaSuccess) e = cudaMalloc(&M->d_s, sizeof(ColumnScalars) * 32);
+    if (e == cudaSuccess) e = cudaMalloc(&M->d_g, sizeof(MultiGlobal));
+    if (e == cudaSuccess) e = cudaMallocHost(&M->h_g, sizeof(MultiGlobal));
+    M->grid = resident_blocks(reinterpret_cast<const void*>(multi_spmv_kernel<32, false>), kT, 0);
+    const long needed = (M->n + static_cast<long>(kWarps) * (32 / M->kp) - 1) / (static_cast<long>(kWarps) * (32 / M->kp));
+    M->grid = static_cast<int>(std::max<long>(1, std::min<long>(M->grid, needed)));
+    if (e == cudaSuccess) e = cudaMalloc(&M->d_partials, sizeof(double) * 2 * 32 * M->grid);
+    if (e == cudaSuccess) e = cudaMalloc(&M->d_counter, sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMemsetAsync(M->d_counter, 0, sizeof(unsigned), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(M->d_s, 0, sizeof(ColumnScalars) * 32, st);
+    if (e != cudaSuccess) {
+        ciecu_multi_destroy(M);
+        return cuda_fail(e, "multi_create: allocation");
+    }
+    *out = M;
+    return CIECU_OK;
+}
+
+int ciecu_multi_destroy(ciecu_multi M) {
+    if (!M) return CIECU_OK;
+    if (M->graph) cudaGraphExecDestroy(M->graph);
+    cudaFree(M->x);
+    cudaFree(M->r);
+    cudaFree(M->p);
+    cudaFree(M->q);
+    cudaFree(M->d_s);
+    cudaFree(M->d_g);
+    if (M->h_g) cudaFreeHost(M->h_g);
+    cudaFree(M->d_partials);
+    cudaFree(M->d_counter);
+    delete M;
+    return CIECU_OK;
+}
+
+int ciecu_multi_info(ciecu_multi M, int* lanesPerRow, int* deviceLoop) {
+    CIECU_REQUIRE(M, "multi_info: null solver");
+    if (lanesPerRow) *lanesPerRow = M->kp;
+    if (deviceLoop) *deviceLoop = M->deviceLoop ? 1 : 0;
+    return CIECU_OK;
+}
+
+int ciecu_multi_product(ciecu_multi M, double inScale, const double* d_in, double outScale, double* d_out,
+                        ciecu_statistics* h_stats) {
+    CIECU_REQUIRE(M && d_in && d_out, "multi_product: null argument");
+    cudaStream_t st = M->A->space->stream;
+    const long n = M->n;
+    const long count = n * M->k;
+    CIECU_CUDA(cudaMemcpyAsync(M->x, d_out, sizeof(double) * count, cudaMemcpyDeviceToDevice, st));
+    std::vector<ColumnScalars> s(static_cast<size_t>(M->k));
+    if (M->settings.iterationCount > 0) {
+        MultiGlobal g{};
+        g.maxIter = M->settings.iterationCount;
+        g.absTol = M->settings.absoluteResidual;
+        g.relTol = M->settings.relativeResidual;
+        *M->h_g = g;
+        CIECU_CUDA(cudaMemcpyAsync(M->d_g, M->h_g, sizeof(MultiGlobal), cudaMemcpyHostToDevice, st));
+        CIECU_TRY(with_group(M->kp, [&](auto kk) -> int {
+            constexpr int KP = decltype(kk)::value;
+            multi_residual_kernel<KP><<<M->grid, kT, 0, st>>>(M->A->args<double>(), M->k, M->x, d_in, M->r);
+            multi_init_kernel<KP><<<M->grid, kT, 0, st>>>(n, M->k, M->r, M->dinv, M->p, M->d_s, M->d_g,
+                                                          M->d_partials, M->d_counter);
+            return CIECU_OK;
+        }));
+        count_launch(2);
+        CIECU_CHECK_LAUNCH("multi-rhs set-up");
+        CIECU_TRY(build_multi_graph(M));
+        const long long limit = M->deviceLoop ? 4096 : M->chunk;
+        for (;;) {
+            CIECU_CUDA(cudaMemcpyAsync(M->h_g, M->d_g, sizeof(MultiGlobal), cudaMemcpyDeviceToHost, st));
+            CIECU_CUDA(cudaStreamSynchronize(st));
+            if (M->h_g->finished >= static_cast<unsigned>(M->k)) break;
+            M->h_g->chunkIter = 0;
+            M->h_g->chunkLimit = limit;
+            CIECU_CUDA(cudaMemcpyAsync(&M->d_g->chunkIter, &M->h_g->chunkIter, 2 * sizeof(long long),
+                                       cudaMemcpyHostToDevice, st));
+            CIECU_CUDA(cudaGraphLaunch(M->graph, st));
+            CIECU_CUDA(cudaMemcpyAsync(M->h_g, M->d_g, sizeof(MultiGlobal), cudaMemcpyDeviceToHost, st));
+            CIECU_CUDA(cudaStreamSynchronize(st));
+            count_launch(3LL * (M->deviceLoop ? M->h_g->chunkIter : M->chunk));
+            if (M->h_g->finished >= static_cast<unsigned>(M->k)) break;
+        }
+        CIECU_CUDA(cudaMemcpyAsync(s.data(), M->d_s, sizeof(ColumnScalars) * M->k, cudaMemcpyDeviceToHost, st));
+        CIECU_CUDA(cudaStreamSynchronize(st));
+    }
+    multi_output_kernel<<<grid_for(count, kT, 8), kT, 0, st>>>(count, inScale, outScale, M->x, d_out);
+    count_launch();
+    CIECU_CHECK_LAUNCH("multi_output_kernel");
+    CIECU_CUDA(cudaStreamSynchronize(st));
+    int firstError = -1;
+    for (int c = 0; c < M->k; ++c) {
+        const ColumnScalars& sc = s[c];
+        if (h_stats) {
+            if (M->settings.iterationCount > 0)
+                h_stats[c] = ciecu_statistics{sc.done == 3 ? sc.errorIter : sc.iter, sc.absres, sc.relres};
+            else
+                h_stats[c] = ciecu_statistics{0, 1.7976931348623157e308, 1.7976931348623157e308};
+        }
+        if (sc.done == 3 && firstError < 0) firstError = c;
+    }
+    if (firstError >= 0) {
+        const ColumnScalars& sc = s[firstError];
+        return fail(CIECU_ERR_BREAKDOWN,
+                    "right-hand side " + std::to_string(firstError) + ": " +
+                        (sc.errorKind == 1 ? std::string("preconditioned norm vanished in iteration 0 (r^T @ z = 0)")
+                                           : "p^T @ A @ p vanished in iteration " + std::to_string(sc.errorIter)));
+    }
+    return CIECU_OK;
+}
+
+}  // extern "C"

@@ -675,3 +675,52 @@ class BatchedConjugateGradients(LinearOperator):
         finally:
             self._stats = list(stats)
             self.space.leave()
+
+
+class MultiRHSConjugateGradients(LinearOperator):
+    """k <= 32 independent Jacobi-PCG solves against one CSR matrix in shared
+    SpMM launches (ciecu_multi_*).  product() takes row-major n x k blocks (a
+    (n, k) tensor); getStats() returns one Statistics per right-hand side."""
+
+    def __init__(self, lhs, inverseDiagonal, rhsCount, settings=None):
+        if type(lhs) is not CSROperator or lhs.space._sfx != "f64":
+            raise CiecuError(1, "MultiRHSConjugateGradients needs an FP64 CSROperator")
+        self.lhs = lhs
+        self.space = lhs.space
+        self.k = int(rhsCount)
+        self.inverseDiagonal = inverseDiagonal
+        self.settings = settings if settings is not None else Statistics(0, 0.0, 0.0)
+        h = ctypes.c_void_p()
+        call("ciecu_multi_create", lhs.csr.handle, self.k, _ptr(inverseDiagonal.inverseDiagonal), self.settings,
+             ctypes.byref(h))
+        self._solver = h
+        self._stats = None
+
+    def __del__(self):
+        try:
+            if getattr(self, "_solver", None):
+                _lib.load().ciecu_multi_destroy(self._solver)
+                self._solver = None
+        except Exception:
+            pass
+
+    def info(self):
+        v, d = ctypes.c_int(), ctypes.c_int()
+        call("ciecu_multi_info", self._solver, ctypes.byref(v), ctypes.byref(d))
+        return {"lanes_per_row": v.value, "device_loop": bool(d.value)}
+
+    def getStats(self):
+        return self._stats
+
+    def product(self, inScale, in_, outScale, out):
+        n = self.lhs.lhs.rowCount()
+        for v in (in_, out):
+            if not (v.is_cuda and v.dtype == torch.float64 and v.is_contiguous() and v.numel() == n * self.k):
+                raise CiecuError(1, "expected contiguous float64 CUDA blocks of %d x %d" % (n, self.k))
+        stats = (Statistics * self.k)()
+        self.space.enter()
+        try:
+            call("ciecu_multi_product", self._solver, float(inScale), _ptr(in_), float(outScale), _ptr(out), stats)
+        finally:
+            self._stats = list(stats)
+            self.space.leave()

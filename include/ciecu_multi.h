@@ -1,0 +1,38 @@
+/*
+ * ciecu multi-right-hand-side solver (SpMM-CG): k <= 32 independent
+ * Jacobi-preconditioned CG solves against one FP64 CSR matrix, sharing every
+ * matrix read.  Each right-hand side follows ConjugateGradients::product
+ * (linalg/packages/solvers/impl/ConjugateGradients_impl.hpp:49-201) with its own
+ * scalars, stopping test and statistics; no reference counterpart as one object
+ * (the reference would run one solver per right-hand side).
+ * Blocks of vectors are row-major n x k: entry (i, c) at i*k + c.
+ */
+#ifndef CIECU_MULTI_H
+#define CIECU_MULTI_H
+
+#include "ciecu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ciecu_multi_s* ciecu_multi;
+
+int ciecu_multi_create(ciecu_csr lhs, int rhsCount, const double* d_inverseDiagonal, ciecu_statistics settings,
+                       ciecu_multi* out);
+int ciecu_multi_destroy(ciecu_multi solver);
+/* Lanes per row group (the power of two >= rhsCount) and whether the solve loop
+ * runs on the device (conditional graph nodes). */
+int ciecu_multi_info(ciecu_multi solver, int* lanesPerRow, int* deviceLoop);
+/* Initial guesses = d_out (n x k); on return out = inScale*out + outScale*X.
+ * h_stats (may be NULL): one ciecu_statistics per right-hand side.  A breakdown
+ * returns CIECU_ERR_BREAKDOWN naming the first such right-hand side; the others
+ * are solved and reported. */
+int ciecu_multi_product(ciecu_multi solver, double inScale, const double* d_in, double outScale, double* d_out,
+                        ciecu_statistics* h_stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CIECU_MULTI_H */
