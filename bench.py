@@ -181,11 +181,16 @@ def main():
     ap.add_argument("--impl", default="cie_b200", choices=["cie_b200", "reference"])
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the other workloads (2D Q1 256^2, batched Q2 systems, 32 right-hand sides, adjoint)")
     ap.add_argument("--profile", action="store_true",
                     help="ncu target: solves only (no e2e, no CPU baseline, no clock sampling)")
     ap.add_argument("--profile-kernels", action="store_true",
                     help="with --profile: no solves, only three launches each of the FP32 SELL and FP64 CSR SpMV "
                          "after set-up (a short target for a full ncu capture)")
+    ap.add_argument("--pin", default=None,
+                    help="with --profile: FP64-solver,mixed-unroll,CSR schedules to use instead of autotuning "
+                         "(the choices a bench run without the profiler reports), e.g. 4,1,4")
     ap.add_argument("--profile-cells", type=int, default=PROFILE_CELLS[0],
                     help="cells per axis of the --profile case (96: 290 MB matrix; 128: the full workload)")
     args = ap.parse_args()
@@ -220,7 +225,13 @@ def main():
     D = makeDiagonalOperator(prob.matrix, space, csr_handle=A.csr)
     settings = Statistics(20000, 0.0, WORKLOAD["tolerance"])
     cg = ConjugateGradients(A, space, D, settings)
-    mixed = MixedPrecisionCG(A, D, settings, mode=0, delta=DELTA)
+    if args.profile and args.pin:
+        pin_fp64, pin_unroll, pin_csr = (int(v) for v in args.pin.split(","))
+        A.csr.set_kernel(pin_csr)
+        cg.set_schedule(pin_fp64)
+        mixed = MixedPrecisionCG(A, D, settings, mode=0, delta=DELTA, innerKernel=pin_unroll)
+    else:
+        mixed = MixedPrecisionCG(A, D, settings, mode=0, delta=DELTA)
     x64 = torch.zeros_like(prob.rhs)
     xmx = torch.zeros_like(prob.rhs)
     stream = torch.cuda.ExternalStream(space.stream.cuda_stream)
@@ -370,6 +381,10 @@ def main():
     rel_mixed, rel_fp64 = true_rel(xmx), true_rel(x64)
     agree = float(torch.linalg.norm(xmx - x64) / torch.linalg.norm(x64))
 
+    extra = None
+    if not args.no_extra:
+        extra = extra_workloads(space, A, D, settings, t_fp64, it64)
+
     cpu = None
     if rank == 0 and not args.no_cpu:
         rp, col, val, bh = cpu_problem_arrays(prob)
@@ -415,10 +430,138 @@ def main():
                     "solver": "mixed"},
             "gpu_launches": int(launches),
             "cpu_baseline": cpu,
+            "workloads": extra,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def extra_workloads(space, A, D, settings, t_fp64, it64):
+    """The other workloads of the path, each timed with CUDA events around complete
+    solves (inputs resident on the device):
+      * 2D Q1 Poisson 256^2, kappa = 1: FP64 Jacobi-PCG to 1e-10;
+      * 512 independent 2D Q2 systems on n x n meshes, n ~ U{16..128} (seeded), each
+        with its own log-normal kappa: one batched solve vs the same systems solved
+        one after another with the single-system solver;
+      * 32 right-hand sides (uniform [-1, 1]) on the 128^3 Q1 matrix: one SpMM-CG
+        vs 32 single solves (the FP64 time measured above, times 32);
+      * adjoint gradient of J = 1/2 ||u - u_t||^2 on 3D Q1 64^3: forward solve and
+        backward (transposed solve + per-element gradient)."""
+    import torch
+    from cie_b200.adjoint import DifferentiablePoisson
+    from cie_b200.fem import kappa_field, make_poisson, random_uniform
+    from cie_b200.linalg import (BatchedConjugateGradients, CSROperator, ConjugateGradients,
+                                 MultiRHSConjugateGradients, Statistics, block_diagonal, makeDiagonalOperator)
+    stream = torch.cuda.current_stream()
+
+    def timed(fn, reps, warm=1):
+        for _ in range(warm):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3 / reps
+
+    out = {}
+    tight = Statistics(5000, 0.0, 1e-10)
+    # 2D Q1 256^2
+    p1 = make_poisson(space, 2, 1, [256, 256], seed=0, kappa="one")
+    A1 = CSROperator(p1.matrix, space)
+    cg1 = ConjugateGradients(A1, space, makeDiagonalOperator(p1.matrix, space, csr_handle=A1.csr), tight)
+    x1 = torch.zeros_like(p1.rhs)
+
+    def solve1():
+        x1.zero_()
+        cg1.product(0.0, p1.rhs, 1.0, x1)
+    t1 = timed(solve1, 5, warm=3)
+    out["poisson2d_q1_256^2_fp64_pcg"] = {"seconds": t1, "iterations": cg1.getStats().iterationCount,
+                                         "dofs": p1.rhs.numel(), "nnz": p1.matrix.nnz(),
+                                         "us_per_iteration": 1e6 * t1 / (cg1.getStats().iterationCount + 1)}
+    del cg1, A1, p1, x1
+
+    # 512 uneven 2D Q2 systems
+    rng = np.random.default_rng(0)
+    sizes = rng.integers(16, 129, 512)
+    probs = [make_poisson(space, 2, 2, [int(m), int(m)], seed=1000 + 3 * i) for i, m in enumerate(sizes)]
+    bd, offsets = block_diagonal([p.matrix for p in probs])
+    rhs = torch.cat([p.rhs for p in probs])
+    Dbd = makeDiagonalOperator(bd, space)
+    batch = BatchedConjugateGradients(bd, offsets, space, Dbd, tight)
+    xb = torch.zeros_like(rhs)
+
+    def solveb():
+        xb.zero_()
+        batch.product(0.0, rhs, 1.0, xb)
+    tb = timed(solveb, 3)
+    its = [s.iterationCount for s in batch.getStats()]
+    rels = [s.relativeResidual for s in batch.getStats()]
+    # the same systems one after another (one solver object per system)
+    singles = []
+    for p in probs:
+        Ap = CSROperator(p.matrix, space)
+        singles.append((ConjugateGradients(Ap, space, makeDiagonalOperator(p.matrix, space, csr_handle=Ap.csr),
+                                           tight), p, torch.zeros_like(p.rhs), Ap))
+
+    def solve_each():
+        for cg, p, xs, _ in singles:
+            xs.zero_()
+            cg.product(0.0, p.rhs, 1.0, xs)
+    ts = timed(solve_each, 1)
+    agree = float(torch.linalg.norm(xb - torch.cat([xs for _, _, xs, _ in singles])) / torch.linalg.norm(xb))
+    out["batched_512_poisson2d_q2_fp64_pcg"] = {
+        "seconds": tb, "systems": len(probs), "total_dofs": int(rhs.numel()), "total_nnz": bd.nnz(),
+        "iterations_min": int(min(its)), "iterations_max": int(max(its)), "max_relative_residual": max(rels),
+        "sequential_single_solves_seconds": ts, "speedup_vs_sequential": ts / tb,
+        "rel_diff_vs_single_solves": agree, "solver": batch.info()}
+    del singles, batch, Dbd, bd, rhs, xb, probs
+
+    # 32 right-hand sides on the 128^3 matrix
+    n = A.lhs.rowCount()
+    k = 32
+    B = torch.as_tensor(np.stack([random_uniform(2000 + c, n) for c in range(k)], axis=1)).cuda().contiguous()
+    mrhs = MultiRHSConjugateGradients(A, D, k, settings)
+    X = torch.zeros_like(B)
+
+    def solvem():
+        X.zero_()
+        mrhs.product(0.0, B, 1.0, X)
+    tm = timed(solvem, 2)
+    its = [s.iterationCount for s in mrhs.getStats()]
+    out["multi_rhs_32_poisson3d_q1_128^3_fp64_pcg"] = {
+        "seconds": tm, "rhs": k, "iterations_min": int(min(its)), "iterations_max": int(max(its)),
+        "max_relative_residual": max(s.relativeResidual for s in mrhs.getStats()),
+        "seconds_per_rhs": tm / k, "single_solve_seconds": t_fp64, "speedup_vs_32_single_solves": 32 * t_fp64 / tm,
+        "note": "random right-hand sides, boundary rows included (identity rows of the eliminated system)"}
+    del mrhs, X, B
+
+    # adjoint gradient, 3D Q1 64^3
+    cells = [64, 64, 64]
+    prob = DifferentiablePoisson(space, 3, 1, cells, settings=Statistics(20000, 0.0, 1e-10))
+    kappa = torch.as_tensor(kappa_field(1, cells)).cuda()
+    kappa_t = torch.as_tensor(kappa_field(2, cells)).cuda()
+    b = torch.as_tensor(random_uniform(0, prob.n)).cuda()
+    u_t = prob(kappa_t, b).detach()
+    k_req = kappa.clone().requires_grad_(True)
+
+    def forward():
+        return 0.5 * torch.sum((prob(k_req, b) - u_t) ** 2)
+    tf = timed(forward, 3)
+    J = forward()
+
+    def backward():
+        k_req.grad = None
+        J.backward(retain_graph=True)
+    tbk = timed(backward, 3)
+    out["adjoint_poisson3d_q1_64^3"] = {
+        "forward_seconds": tf, "backward_seconds": tbk, "cells": int(np.prod(cells)), "dofs": prob.n,
+        "forward_iterations": prob.forward_stats.iterationCount,
+        "adjoint_iterations": prob.adjoint_stats.iterationCount}
+    return out
 
 
 if __name__ == "__main__":

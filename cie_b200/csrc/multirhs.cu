@@ -117,18 +117,15 @@ __device__ __forceinline__ void multi_rows(const CsrArgs<double>& A, int k, cons
             const int m = min(KP, k1 - e0);
             const double a = c < m ? stream_ld(A.val + e0 + c) : 0.0;
             const int col = c < m ? stream_ld(A.col + e0 + c) : 0;
-            for (int j = 0; j < m; j += 4) {
-                double av[4], pv[4];
+            // all KP gathers of the chunk in flight before the FMA chain
+            double pv[KP];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int jj = j + u < m ? j + u : m - 1;
-                    av[u] = __shfl_sync(gmask, a, jj, KP);
-                    const int cj = __shfl_sync(gmask, col, jj, KP);
-                    pv[u] = (active && j + u < m) ? __ldg(X + static_cast<long>(cj) * k + c) : 0.0;
-                }
-#pragma unroll
-                for (int u = 0; u < 4; ++u) acc = fma(av[u], pv[u], acc);
+            for (int u = 0; u < KP; ++u) {
+                const int cj = __shfl_sync(gmask, col, u, KP);
+                pv[u] = (active && u < m) ? __ldg(X + static_cast<long>(cj) * k + c) : 0.0;
             }
+#pragma unroll
+            for (int u = 0; u < KP; ++u) acc = fma(__shfl_sync(gmask, a, u, KP), pv[u], acc);
         }
         if (valid && active) op(row, c, acc);
     }
@@ -162,6 +159,7 @@ __global__ void __launch_bounds__(kT) multi_init_kernel(long n, int k, const dou
     double rr = 0.0, rz = 0.0;
     const long stride = static_cast<long>(gridDim.x) * kWarps * RPW;
     if (c < k)
+#pragma unroll 4
         for (long i = (static_cast<long>(blockIdx.x) * kWarps + warp) * RPW + slot; i < n; i += stride) {
             const double ri = R[i * k + c];
             const double zi = ri * dinv[i];
@@ -250,6 +248,7 @@ __global__ void __launch_bounds__(kT) multi_update_kernel(long n, int k, double*
     if (c < k && !S[c].done) {
         const double alpha = S[c].alpha, malpha = -alpha;
         const long stride = static_cast<long>(gridDim.x) * kWarps * RPW;
+#pragma unroll 4
         for (long i = (static_cast<long>(blockIdx.x) * kWarps + warp) * RPW + slot; i < n; i += stride) {
             const long e = i * k + c;
             X[e] = fma(alpha, P[e], X[e]);
@@ -297,6 +296,7 @@ __global__ void __launch_bounds__(kT) multi_direction_kernel(long n, int k, doub
     if (c >= k || S[c].done) return;
     const double beta = S[c].beta;
     const long stride = static_cast<long>(gridDim.x) * kWarps * RPW;
+#pragma unroll 4
     for (long i = (static_cast<long>(blockIdx.x) * kWarps + warp) * RPW + slot; i < n; i += stride) {
         const long e = i * k + c;
         P[e] = __dadd_rn(__dmul_rn(P[e], beta), __dmul_rn(R[e], dinv[i]));
@@ -351,7 +351,8 @@ struct ciecu_multi_s {
     cudaGraphExec_t graph = nullptr;
     bool deviceLoop = false;
     int chunk = 16;
-    int grid = 1;
+    int grid = 1;   // SpMM kernels (register-limited occupancy)
+    int gridV = 1;  // vector kernels
 };
 
 namespace ciecu {
@@ -363,9 +364,9 @@ int launch_multi_iteration(ciecu_multi_s* M, cudaStream_t st, cudaGraphCondition
         constexpr int KP = decltype(kk)::value;
         multi_spmv_kernel<KP, COND><<<M->grid, kT, 0, st>>>(M->A->args<double>(), M->k, M->p, M->q, M->d_s, M->d_g,
                                                             M->d_partials, M->d_counter, cond);
-        multi_update_kernel<KP><<<M->grid, kT, 0, st>>>(M->n, M->k, M->x, M->r, M->p, M->q, M->dinv, M->d_s,
-                                                        M->d_g, M->d_partials, M->d_counter);
-        multi_direction_kernel<KP, COND><<<M->grid, kT, 0, st>>>(M->n, M->k, M->p, M->r, M->dinv, M->d_s, M->d_g,
+        multi_update_kernel<KP><<<M->gridV, kT, 0, st>>>(M->n, M->k, M->x, M->r, M->p, M->q, M->dinv, M->d_s,
+                                                         M->d_g, M->d_partials, M->d_counter);
+        multi_direction_kernel<KP, COND><<<M->gridV, kT, 0, st>>>(M->n, M->k, M->p, M->r, M->dinv, M->d_s, M->d_g,
                                                                  cond);
         return CIECU_OK;
     }));
@@ -430,10 +431,16 @@ int ciecu_multi_create(ciecu_csr lhs, int rhsCount, const double* d_inverseDiago
     if (e == cudaSuccess) e = cudaMalloc(&M->d_s, sizeof(ColumnScalars) * 32);
     if (e == cudaSuccess) e = cudaMalloc(&M->d_g, sizeof(MultiGlobal));
     if (e == cudaSuccess) e = cudaMallocHost(&M->h_g, sizeof(MultiGlobal));
-    M->grid = resident_blocks(reinterpret_cast<const void*>(multi_spmv_kernel<32, false>), kT, 0);
     const long needed = (M->n + static_cast<long>(kWarps) * (32 / M->kp) - 1) / (static_cast<long>(kWarps) * (32 / M->kp));
+    with_group(M->kp, [&](auto kk) -> int {
+        constexpr int KP = decltype(kk)::value;
+        M->grid = resident_blocks(reinterpret_cast<const void*>(multi_spmv_kernel<KP, true>), kT, 0);
+        M->gridV = resident_blocks(reinterpret_cast<const void*>(multi_update_kernel<KP>), kT, 0);
+        return CIECU_OK;
+    });
     M->grid = static_cast<int>(std::max<long>(1, std::min<long>(M->grid, needed)));
-    if (e == cudaSuccess) e = cudaMalloc(&M->d_partials, sizeof(double) * 2 * 32 * M->grid);
+    M->gridV = static_cast<int>(std::max<long>(1, std::min<long>(M->gridV, needed)));
+    if (e == cudaSuccess) e = cudaMalloc(&M->d_partials, sizeof(double) * 2 * 32 * std::max(M->grid, M->gridV));
     if (e == cudaSuccess) e = cudaMalloc(&M->d_counter, sizeof(unsigned));
     if (e == cudaSuccess) e = cudaMemsetAsync(M->d_counter, 0, sizeof(unsigned), st);
     if (e == cudaSuccess) e = cudaMemsetAsync(M->d_s, 0, sizeof(ColumnScalars) * 32, st);
@@ -486,7 +493,7 @@ int ciecu_multi_product(ciecu_multi M, double inScale, const double* d_in, doubl
         CIECU_TRY(with_group(M->kp, [&](auto kk) -> int {
             constexpr int KP = decltype(kk)::value;
             multi_residual_kernel<KP><<<M->grid, kT, 0, st>>>(M->A->args<double>(), M->k, M->x, d_in, M->r);
-            multi_init_kernel<KP><<<M->grid, kT, 0, st>>>(n, M->k, M->r, M->dinv, M->p, M->d_s, M->d_g,
+            multi_init_kernel<KP><<<M->gridV, kT, 0, st>>>(n, M->k, M->r, M->dinv, M->p, M->d_s, M->d_g,
                                                           M->d_partials, M->d_counter);
             return CIECU_OK;
         }));

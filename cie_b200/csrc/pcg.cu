@@ -456,6 +456,15 @@ int ciecu_pcg_set_graph_chunk(ciecu_pcg S, int iterations) {
     return CIECU_OK;
 }
 
+int ciecu_pcg_set_schedule(ciecu_pcg S, int schedule) {
+    CIECU_REQUIRE(S, "pcg_set_schedule: null solver");
+    CIECU_REQUIRE(schedule == 0 || schedule == 1 || schedule == 2 || schedule == 4 || schedule == 8 ||
+                      schedule == 16 || schedule == 32,
+                  "pcg_set_schedule: schedule must be 0 (autotune), 1, 2, 4, 8, 16 or 32");
+    S->kernel = schedule;  // the graph is rebuilt when it was built for another schedule
+    return CIECU_OK;
+}
+
 int ciecu_pcg_product(ciecu_pcg S, double inScale, const double* d_in, double outScale, double* d_out,
                       ciecu_statistics* h_stats) {
     CIECU_REQUIRE(S, "pcg_product: null solver");

@@ -438,6 +438,11 @@ class ConjugateGradients(LinearOperator):
         if self._solver is not None:
             call("ciecu_pcg_set_graph_chunk", self._solver, int(iterations))
 
+    def set_schedule(self, schedule):
+        """Pins the fused solver's SpMV schedule (0: autotune at the next solve)."""
+        if self._solver is not None:
+            call("ciecu_pcg_set_schedule", self._solver, int(schedule))
+
     def info(self):
         """SpMV schedule chosen for the fused solver kernel and whether the solve
         runs as a device-side graph loop (fused device solver only)."""

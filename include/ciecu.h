@@ -195,6 +195,11 @@ int ciecu_pcg_product(ciecu_pcg solver, double inScale, const double* d_in, doub
 /* Iterations captured per CUDA graph launch between host convergence checks
  * (used when the device-side loop of conditional graph nodes is unavailable). */
 int ciecu_pcg_set_graph_chunk(ciecu_pcg solver, int iterations);
+/* Pins the schedule of the solver's fused q = A p kernel (1 = row-block stream
+ * kernel, 2..32 = lanes per row) instead of autotuning it at the first solve;
+ * 0 returns to autotuning.  For runs whose timings would mislead the autotuner
+ * (under a profiler). */
+int ciecu_pcg_set_schedule(ciecu_pcg solver, int schedule);
 /* SpMV schedule the solver's autotuner chose for its fused q = A p kernel (0 before
  * the first solve; 1 = row-block stream kernel, else lanes per row) and whether the
  * solve runs as a device-side graph loop (1) or host-polled graph chunks (0). */
