@@ -4,11 +4,12 @@
 // the matrix once for all k.  No reference counterpart as one object (the
 // reference would run k solver objects, one per right-hand side).
 //
-// Vectors are row-major n x k blocks (entry (i, c) at i*k + c).  A group of KP
-// lanes (KP = the power of two >= k) owns a row: it loads KP (value, column)
-// pairs of the row at a time, broadcasts each pair within the group by shuffle,
-// and lane c gathers P[j][c] -- k consecutive doubles, one coalesced access per
-// matrix entry for the group.  Each row sum runs over the entries in CSR order.
+// Vectors are row-major n x k blocks (entry (i, c) at i*k + c).  A CTA stages a
+// row block's (value, column) pairs in shared memory; a group of KP lanes (KP =
+// the power of two >= k) owns a row, reads each pair as a shared-memory
+// broadcast, and lane c gathers P[j][c] -- k consecutive doubles, one coalesced
+// access per matrix entry for the group.  Each row sum runs over the entries in
+// CSR order.
 // Dot products are per column, reduced in a fixed order (per-block column sums,
 // then the last block sums the blocks in block order).
 //
@@ -96,38 +97,68 @@ __device__ __forceinline__ bool column_reduce_last(const double (&mine)[NV], int
     return true;
 }
 
-// Row sums of A times the n x k block X for the rows of this group; calls
-// op(row, c, sum) for each row and active column.
+// Row sums of A times the n x k block X; calls op(row, c, sum) for each row and
+// active column.  The CTA takes the row blocks of the CSR handle (at most
+// kStreamTile entries each) in turn, interleaved over the grid so that all CTAs
+// advance through the rows together and the gathered X rows stay in L2; it
+// stages a block's values and column indices in shared memory with coalesced
+// loads, then every lane of a row group reads (a_ij, j) as a shared-memory
+// broadcast and gathers X[j][c]: one load and one FMA per entry and lane, the
+// entries of a row summed in CSR order.  A row longer than the tile (a block of
+// its own) is read straight from global memory.
+struct __align__(16) Entry {
+    double a;
+    int col;
+    int pad;
+};
+
 template <int KP, typename Op>
 __device__ __forceinline__ void multi_rows(const CsrArgs<double>& A, int k, const double* __restrict__ X, Op& op) {
+    __shared__ Entry s_e[kStreamTile];  // one 16-byte broadcast read per entry
     constexpr int RPW = 32 / KP;
+    constexpr int UNROLL = 8;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int slot = lane / KP, c = lane % KP;
     const bool active = c < k;
-    const unsigned gmask = KP == 32 ? 0xffffffffu : (((1u << KP) - 1u) << (slot * KP));
-    const long n = A.nrows;
-    const long stride = static_cast<long>(gridDim.x) * kWarps * RPW;
-    for (long base = (static_cast<long>(blockIdx.x) * kWarps + warp) * RPW; base < n; base += stride) {
-        const long row = base + slot;
-        const bool valid = row < n;
-        const int k0 = valid ? A.rowptr[row] : 0;
-        const int k1 = valid ? A.rowptr[row + 1] : 0;
-        double acc = 0.0;
-        for (int e0 = k0; e0 < k1; e0 += KP) {
-            const int m = min(KP, k1 - e0);
-            const double a = c < m ? stream_ld(A.val + e0 + c) : 0.0;
-            const int col = c < m ? stream_ld(A.col + e0 + c) : 0;
-            // all KP gathers of the chunk in flight before the FMA chain
-            double pv[KP];
-#pragma unroll
-            for (int u = 0; u < KP; ++u) {
-                const int cj = __shfl_sync(gmask, col, u, KP);
-                pv[u] = (active && u < m) ? __ldg(X + static_cast<long>(cj) * k + c) : 0.0;
-            }
-#pragma unroll
-            for (int u = 0; u < KP; ++u) acc = fma(__shfl_sync(gmask, a, u, KP), pv[u], acc);
+    const double* __restrict__ xc = X + c;
+    for (int b = blockIdx.x; b < A.nblocks; b += gridDim.x) {
+        const int r0 = A.blocks[b], r1 = A.blocks[b + 1];
+        const int e0 = A.rowptr[r0], e1 = A.rowptr[r1];
+        const bool staged = e1 - e0 <= kStreamTile;
+        if (staged) {
+            for (int j = threadIdx.x; j < e1 - e0; j += kT)
+                s_e[j] = Entry{stream_ld(A.val + e0 + j), stream_ld(A.col + e0 + j), 0};
+            __syncthreads();
         }
-        if (valid && active) op(row, c, acc);
+        for (int rbase = r0 + warp * RPW; rbase < r1; rbase += kWarps * RPW) {
+            const int row = rbase + slot;
+            if (row >= r1) continue;
+            const int k0 = A.rowptr[row] - e0, k1 = A.rowptr[row + 1] - e0;
+            double acc = 0.0;
+            if (staged) {
+                int j = k0;
+                for (; j + UNROLL <= k1; j += UNROLL) {
+                    Entry e[UNROLL];
+                    double pv[UNROLL];
+#pragma unroll
+                    for (int u = 0; u < UNROLL; ++u) {
+                        e[u] = s_e[j + u];
+                        pv[u] = active ? __ldg(xc + static_cast<long>(e[u].col) * k) : 0.0;
+                    }
+#pragma unroll
+                    for (int u = 0; u < UNROLL; ++u) acc = fma(e[u].a, pv[u], acc);
+                }
+                for (; j < k1; ++j) {
+                    const Entry e = s_e[j];
+                    acc = fma(e.a, active ? __ldg(xc + static_cast<long>(e.col) * k) : 0.0, acc);
+                }
+            } else {
+                for (int j = e0 + k0; j < e0 + k1; ++j)
+                    acc = fma(A.val[j], active ? __ldg(xc + static_cast<long>(A.col[j]) * k) : 0.0, acc);
+            }
+            if (active) op(row, c, acc);
+        }
+        if (staged) __syncthreads();
     }
 }
 
