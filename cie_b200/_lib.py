@@ -103,6 +103,7 @@ SIGNATURES = {
     "ciecu_assemble_stiffness": (c_int, [P, P, P, c_int, c_int, P]),
     "ciecu_element_gradient": (c_int, [P, P, c_int, P, P, P, P]),
     "ciecu_adjoint_gradient": (c_int, [P, P, P, c_int, P, P, P, P, P, P, P]),
+    "ciecu_assemble_embedded": (c_int, [P, P, P, P, P, P, c_double, c_double, c_int, c_int, c_int, P, P, P]),
     "ciecu_batch_create": (c_int, [P, c_int64, P, P, Statistics, P]),
     "ciecu_batch_destroy": (c_int, [P]),
     "ciecu_batch_info": (c_int, [P, P, P, P]),

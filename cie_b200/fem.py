@@ -19,7 +19,7 @@ from ._lib import call, CiecuError
 from .linalg import CSRMatrix, CUDASpace, _ptr, _CSRHandle
 
 __all__ = ["StructuredMesh", "csr_pattern", "Assembler", "random_uniform", "random_normal", "kappa_field",
-           "PoissonProblem", "make_poisson"]
+           "PoissonProblem", "make_poisson", "make_embedded_poisson"]
 
 
 def _np_ptr(a):
@@ -121,6 +121,25 @@ class Assembler:
              _ptr(entries))
         self.space.leave()
 
+    def assemble_embedded(self, center, radius, alpha, maxDepth, kappa=None, convention=0, accumulate=False,
+                          entries=None, origin=None):
+        """Finite-cell stiffness of the sphere |x - center| < radius inside the grid
+        (fictitious part scaled by alpha, cut cells on a depth-maxDepth quadrature
+        tree; ciecu_assemble_embedded).  Returns the number of cut cells."""
+        entries = self.matrix.entries if entries is None else entries
+        m = self.mesh
+        h = np.ascontiguousarray(m.h, dtype=np.float64)
+        cells = np.ascontiguousarray(m.cells, dtype=np.int32)
+        org = np.zeros(m.dim) if origin is None else np.asarray(origin, dtype=np.float64)
+        cen = np.ascontiguousarray(center, dtype=np.float64)
+        cut = ctypes.c_int64()
+        self.space.enter()
+        call("ciecu_assemble_embedded", self.handle, _ptr(kappa), _np_ptr(h), _np_ptr(cells), _np_ptr(org),
+             _np_ptr(cen), float(radius), float(alpha), int(maxDepth), int(convention), int(bool(accumulate)),
+             _ptr(entries), _ptr(self._work), ctypes.byref(cut))
+        self.space.leave()
+        return cut.value
+
     def dirichlet(self, isBoundary, rhs=None, entries=None):
         entries = self.matrix.entries if entries is None else entries
         self.space.enter()
@@ -152,6 +171,29 @@ class PoissonProblem:
     def host_csr(self):
         m = self.matrix
         return (m.rowExtents.cpu().numpy(), m.columnIndices.cpu().numpy(), m.entries.cpu().numpy())
+
+
+def make_embedded_poisson(space, dim, order, cells, center=None, radius=0.4, alpha=1e-6, depth=2, seed=0):
+    """Finite-cell Poisson problem: Q_order cells on the unit box, the physical
+    domain the sphere |x - center| < radius (center: the box centre), the rest
+    scaled by alpha, cut cells integrated on a depth-`depth` quadrature tree with
+    the (order+1)^dim Gauss rule per node; kappa = 1, homogeneous Dirichlet on the
+    box boundary, RHS uniform [-1, 1] (seed)."""
+    mesh = StructuredMesh(dim, order, cells)
+    rowptr, col = csr_pattern(mesh.ncells, mesh.nb, mesh.dofmap, mesh.ndofs)
+    dev = space.device
+    matrix = CSRMatrix(mesh.ndofs, torch.as_tensor(rowptr).to(dev), torch.as_tensor(col).to(dev),
+                       torch.zeros(col.size, dtype=torch.float64, device=dev))
+    rhs = torch.as_tensor(random_uniform(seed, mesh.ndofs)).to(dev)
+    bnd = torch.as_tensor(mesh.boundary()).to(dev)
+    asm = Assembler(space, matrix, mesh)
+    center = [0.5] * dim if center is None else center
+    cut = asm.assemble_embedded(center, radius, alpha, depth)
+    asm.dirichlet(bnd, rhs)
+    torch.cuda.synchronize()
+    prob = PoissonProblem(space, mesh, matrix, rhs, None, bnd, asm, seed)
+    prob.cut_cells = cut
+    return prob
 
 
 def make_poisson(space, dim, order, cells, seed=0, kappa="lognormal", convention=0, kappa_seed=None):

@@ -39,6 +39,25 @@ int ciecu_assembly_color_count(ciecu_assembly plan, int* h_count);
 int ciecu_assemble_stiffness(ciecu_assembly plan, const double* d_kappa, const double* h_cellSize, int convention,
                              int accumulate, double* d_entries);
 
+/* Embedded-domain (finite-cell) stiffness on a structured grid of h_cells cells of
+ * size h_cellSize starting at h_origin (cell e at index (e % cells[0], ...), first
+ * axis fastest): the physical domain is the sphere |x - h_center| < radius, the
+ * rest is fictitious with material factor alpha
+ * (ScaledMultiMaterialIntegrand_impl.hpp:33-60).  A cell whose base quadrature
+ * points (the plan's quadratureOrder^dim Gauss rule) all lie on one side is
+ * integrated with that rule; a cut cell with the tree of
+ * KDTreeQuadraturePointFactory.hpp:67-173 over depths [0, maxDepth]: the base
+ * rule on every tree node, weights times the node's Jacobian, nodes kept when
+ * homogeneous and inside, at the maximum depth, or homogeneous at depth 0, and
+ * refined while not homogeneous.  K_e in FP64, convention as
+ * ciecu_assemble_stiffness; d_kappa may be NULL (kappa = 1).  The plan's basis has
+ * at most 64 functions.  d_work: nb*nb doubles.  h_cutCells (may be NULL): the
+ * number of cut cells (synchronises the stream). */
+int ciecu_assemble_embedded(ciecu_assembly plan, const double* d_kappa, const double* h_cellSize,
+                            const int32_t* h_cells, const double* h_origin, const double* h_center, double radius,
+                            double alpha, int maxDepth, int convention, int accumulate, double* d_entries,
+                            double* d_work, int64_t* h_cutCells);
+
 /* Adjoint gradient of J(u) with respect to the cell conductivities:
  * d_grad[e] = -lambda_e^T (dK_e/dkappa_e) u_e = -lambda_e^T K_e(kappa = 1) u_e.
  * d_work: nb*nb doubles. */
