@@ -23,7 +23,8 @@ class Statistics(ctypes.Structure):
 
 
 class MixedOptions(ctypes.Structure):
-    _fields_ = [("mode", c_int), ("delta", c_double), ("compressColumns", c_int), ("innerKernel", c_int)]
+    _fields_ = [("mode", c_int), ("delta", c_double), ("compressColumns", c_int), ("innerKernel", c_int),
+                ("scaleInner", c_int)]
 
 
 class MixedStatistics(ctypes.Structure):

@@ -53,8 +53,27 @@ struct MixedScalars {
     int done, error, update, updateX, mode, pad;
     long long chunkIter, chunkLimit;  // iterations of the current graph launch / per launch
     unsigned tmaError;                // a bounded TMA pipeline wait gave up
-    unsigned pad2;
+    int scaled;                       // inner system symmetrically Jacobi-scaled
+    double r0s;                       // initial residual norm in the inner (scaled) units
+    int restart;                      // an FP32 breakdown asked for a replacement + restart
+    int breakdowns;                   // FP32 breakdowns of this solve
 };
+
+// FP32 breakdowns (p^T q <= 0 in the inner precision) a solve survives by a
+// residual replacement and a restarted direction before it reports a breakdown.
+constexpr int kMaxInnerBreakdowns = 64;
+
+// M1 epilogue: alpha, or -- when the FP32 p^T q is not positive -- no step, and a
+// residual replacement with a restarted direction (up to kMaxInnerBreakdowns).
+__device__ __forceinline__ bool inner_breakdown(MixedScalars* s) {
+    s->alpha = 0.0;
+    s->restart = 1;
+    s->breakdowns += 1;
+    if (s->breakdowns <= kMaxInnerBreakdowns) return false;
+    s->done = 3;
+    s->error = CIECU_ERR_BREAKDOWN;
+    return true;
+}
 
 // COND selects the instantiation with conditional-node calls (device loop) or
 // without any (plain captured graphs, profilable).
@@ -88,7 +107,8 @@ template <typename CI>
 __global__ void sell_fill_kernel(int nrows, const int* __restrict__ rowptr, const int* __restrict__ col,
                                  const double* __restrict__ val, const int* __restrict__ sliceLen,
                                  const long long* __restrict__ sliceStart, float* __restrict__ sval,
-                                 CI* __restrict__ scol, unsigned short* __restrict__ rowLen, unsigned* tooFar) {
+                                 CI* __restrict__ scol, unsigned short* __restrict__ rowLen, unsigned* tooFar,
+                                 const double* __restrict__ sdiag) {
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nrows; r += gridDim.x * blockDim.x) {
         const int s = r >> 5;
         const int padded = ((abs(sliceLen[s]) + 3) >> 2) << 2;
@@ -98,8 +118,8 @@ __global__ void sell_fill_kernel(int nrows, const int* __restrict__ rowptr, cons
         for (int j = 0; j < padded; ++j) {
             const long long idx = base + 128LL * (j >> 2) + (j & 3);
             if (j < len) {
-                sval[idx] = static_cast<float>(val[k0 + j]);
                 const int c = col[k0 + j];
+                sval[idx] = static_cast<float>(sdiag ? val[k0 + j] * sdiag[r] * sdiag[c] : val[k0 + j]);
                 if constexpr (sizeof(CI) == 2) {
                     const int off = c - r;
                     if (off < -32768 || off > 32767) atomicOr(tooFar, 1u);
@@ -157,9 +177,7 @@ __global__ void __launch_bounds__(kT) mixed_spmv_kernel(SellArgs<float, CI> A, c
     if (grid_reduce_last<1, kT>(mine, partials, counter, tot) && threadIdx.x == 0) {
         s->pq = tot[0];
         if (!(0.0 < tot[0])) {
-            s->done = 3;
-            s->error = CIECU_ERR_BREAKDOWN;
-            set_cond<COND>(loop, 0);
+            if (inner_breakdown(s)) set_cond<COND>(loop, 0);
         } else {
             s->alpha = s->rz / tot[0];
         }
@@ -198,9 +216,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32) mixed_spmv_tma_kernel(SellArgs
             s->error = CIECU_ERR_TIMEOUT;
             set_cond<COND>(loop, 0);
         } else if (!(0.0 < tot[0])) {
-            s->done = 3;
-            s->error = CIECU_ERR_BREAKDOWN;
-            set_cond<COND>(loop, 0);
+            if (inner_breakdown(s)) set_cond<COND>(loop, 0);
         } else {
             s->alpha = s->rz / tot[0];
         }
@@ -232,21 +248,24 @@ __global__ void __launch_bounds__(kT) mixed_update_kernel(long n, float* __restr
         return;
     }
     const float alpha = static_cast<float>(s->alpha);
+    const bool step = !s->restart;  // after an FP32 breakdown: no step (p may not be finite)
     double rr = 0.0, rz = 0.0;
     const long quads = n >> 2;
     const long stride = static_cast<long>(gridDim.x) * kT;
     for (long j = static_cast<long>(blockIdx.x) * kT + threadIdx.x; j < quads; j += stride) {
-        const float4 pj = reinterpret_cast<const float4*>(p)[j];
-        const float4 qj = reinterpret_cast<const float4*>(q)[j];
         const float4 dj = reinterpret_cast<const float4*>(dinv)[j];
-        float4 xj = reinterpret_cast<const float4*>(x)[j];
         float4 rj = reinterpret_cast<const float4*>(r)[j];
-        xj.x = fmaf(alpha, pj.x, xj.x); xj.y = fmaf(alpha, pj.y, xj.y);
-        xj.z = fmaf(alpha, pj.z, xj.z); xj.w = fmaf(alpha, pj.w, xj.w);
-        rj.x = fmaf(-alpha, qj.x, rj.x); rj.y = fmaf(-alpha, qj.y, rj.y);
-        rj.z = fmaf(-alpha, qj.z, rj.z); rj.w = fmaf(-alpha, qj.w, rj.w);
-        reinterpret_cast<float4*>(x)[j] = xj;
-        reinterpret_cast<float4*>(r)[j] = rj;
+        if (step) {
+            const float4 pj = reinterpret_cast<const float4*>(p)[j];
+            const float4 qj = reinterpret_cast<const float4*>(q)[j];
+            float4 xj = reinterpret_cast<const float4*>(x)[j];
+            xj.x = fmaf(alpha, pj.x, xj.x); xj.y = fmaf(alpha, pj.y, xj.y);
+            xj.z = fmaf(alpha, pj.z, xj.z); xj.w = fmaf(alpha, pj.w, xj.w);
+            rj.x = fmaf(-alpha, qj.x, rj.x); rj.y = fmaf(-alpha, qj.y, rj.y);
+            rj.z = fmaf(-alpha, qj.z, rj.z); rj.w = fmaf(-alpha, qj.w, rj.w);
+            reinterpret_cast<float4*>(x)[j] = xj;
+            reinterpret_cast<float4*>(r)[j] = rj;
+        }
         rr = fma(double(rj.x), double(rj.x), rr); rr = fma(double(rj.y), double(rj.y), rr);
         rr = fma(double(rj.z), double(rj.z), rr); rr = fma(double(rj.w), double(rj.w), rr);
         rz = fma(double(rj.x), double(rj.x * dj.x), rz); rz = fma(double(rj.y), double(rj.y * dj.y), rz);
@@ -254,9 +273,12 @@ __global__ void __launch_bounds__(kT) mixed_update_kernel(long n, float* __restr
     }
     if (blockIdx.x == 0 && threadIdx.x < (n & 3)) {
         const long i = (quads << 2) + threadIdx.x;
-        x[i] = fmaf(alpha, p[i], x[i]);
-        const float ri = fmaf(-alpha, q[i], r[i]);
-        r[i] = ri;
+        float ri = r[i];
+        if (step) {
+            x[i] = fmaf(alpha, p[i], x[i]);
+            ri = fmaf(-alpha, q[i], ri);
+            r[i] = ri;
+        }
         rr = fma(double(ri), double(ri), rr);
         rz = fma(double(ri), double(ri * dinv[i]), rz);
     }
@@ -276,7 +298,7 @@ __global__ void __launch_bounds__(kT) mixed_update_kernel(long n, float* __restr
         } else {
             update = rnorm < s->delta * s->cycleStart;
         }
-        update = update || rnorm < s->relTol * s->r0 || rnorm < s->absTol || s->iter >= s->maxIter;
+        update = update || rnorm < s->relTol * s->r0s || rnorm < s->absTol || s->iter >= s->maxIter || s->restart;
         if (update) {
             s->rzPending = tot[1];
             s->update = 1;
@@ -292,11 +314,11 @@ __global__ void __launch_bounds__(kT) mixed_update_kernel(long n, float* __restr
 
 // R1: x64 += x32; x32 = 0 (only when a replacement was requested).
 __global__ void __launch_bounds__(kT) mixed_fold_kernel(long n, double* __restrict__ x64, float* __restrict__ x32,
-                                                        const MixedScalars* s) {
+                                                        const double* __restrict__ sdiag, const MixedScalars* s) {
     if (!*reinterpret_cast<const volatile int*>(&s->update)) return;
     const long stride = static_cast<long>(gridDim.x) * kT;
     for (long i = static_cast<long>(blockIdx.x) * kT + threadIdx.x; i < n; i += stride) {
-        x64[i] += static_cast<double>(x32[i]);
+        x64[i] += sdiag ? static_cast<double>(x32[i]) * sdiag[i] : static_cast<double>(x32[i]);
         x32[i] = 0.0f;
     }
 }
@@ -305,15 +327,17 @@ struct ResidualOp {
     struct Pre {
         double b;
         float d;
+        double s;
     };
     const double* __restrict__ b;
     const float* __restrict__ dinv;
     float* __restrict__ r32;
+    const double* __restrict__ sdiag;  // inner scaling (or null)
     double rr, rz;
-    __device__ __forceinline__ Pre pre(int row) const { return Pre{b[row], dinv[row]}; }
+    __device__ __forceinline__ Pre pre(int row) const { return Pre{b[row], dinv[row], sdiag ? sdiag[row] : 1.0}; }
     __device__ __forceinline__ void post(int row, const Pre& p, double sum) {
         const double ri = p.b - sum;
-        const float rf = static_cast<float>(ri);
+        const float rf = static_cast<float>(sdiag ? ri * p.s : ri);
         r32[row] = rf;
         rr = fma(ri, ri, rr);
         rz = fma(double(rf), double(rf * p.d), rz);
@@ -325,22 +349,26 @@ struct ResidualOp {
 template <int KERNEL, bool INIT, bool COND>
 __global__ void __launch_bounds__(csr_threads<KERNEL>())
     mixed_residual_kernel(CsrArgs<double> A, const double* __restrict__ b, const double* __restrict__ x64,
-                          const float* __restrict__ dinv, float* __restrict__ r32, MixedScalars* s,
-                          double* partials, unsigned* counter, cudaGraphConditionalHandle loop) {
+                          const float* __restrict__ dinv, float* __restrict__ r32, const double* __restrict__ sdiag,
+                          MixedScalars* s, double* partials, unsigned* counter, cudaGraphConditionalHandle loop) {
     if (!INIT && !*reinterpret_cast<volatile int*>(&s->update)) return;
     constexpr int T = csr_threads<KERNEL>();
-    ResidualOp op{b, dinv, r32, 0.0, 0.0};
+    ResidualOp op{b, dinv, r32, sdiag, 0.0, 0.0};
     csr_rows<KERNEL, double, double, false>(A, x64, op);
     const double rr = op.rr, rz = op.rz;
     double mine[2] = {rr, rz}, tot[2];
     if (grid_reduce_last<2, T>(mine, partials, counter, tot) && threadIdx.x == 0) {
         const double rnorm = sqrt(tot[0]);
+        // the FP32 recursion's norms are in the inner units: scaled when the inner
+        // system is scaled (then z32 = r32 and tot[1] = ||r32||^2)
+        const double rs = s->scaled ? sqrt(tot[1]) : rnorm;
         s->rnorm = rnorm;
         if (INIT) {
             s->r0 = rnorm;
+            s->r0s = rs;
             s->absres = rnorm;
             s->relres = 1.0;
-            s->maxrx = s->maxrr = s->cycleStart = rnorm;
+            s->maxrx = s->maxrr = s->cycleStart = rs;
             s->iter = 0;
             s->refinements = 0;
             s->update = 0;
@@ -371,15 +399,16 @@ __global__ void __launch_bounds__(csr_threads<KERNEL>())
             s->error = CIECU_ERR_BREAKDOWN;
         } else {
             if (s->mode == 0) {
-                s->maxrr = rnorm;
-                if (s->updateX) s->maxrx = rnorm;
-                s->beta = tot[1] / s->rz;
+                s->maxrr = rs;
+                if (s->updateX) s->maxrx = rs;
+                s->beta = s->restart ? 0.0 : tot[1] / s->rz;  // after an FP32 breakdown: p = z
             } else {
-                s->cycleStart = rnorm;
+                s->cycleStart = rs;
                 s->beta = 0.0;  // restart the inner CG: p = z
             }
             s->rz = tot[1];
         }
+        s->restart = 0;
         if (s->done) set_cond<COND>(loop, 0);
     }
 }
@@ -405,6 +434,16 @@ __global__ void __launch_bounds__(kT) mixed_direction_kernel(long n, float* __re
         const long i = (quads << 2) + threadIdx.x;
         p[i] = fmaf(beta, p[i], r[i] * dinv[i]);
     }
+}
+
+__global__ void fill_f32_kernel(long n, float v, float* __restrict__ b) {
+    const long stride = static_cast<long>(gridDim.x) * blockDim.x;
+    for (long i = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) b[i] = v;
+}
+
+__global__ void sqrt_kernel(long n, const double* __restrict__ a, double* __restrict__ b) {
+    const long stride = static_cast<long>(gridDim.x) * blockDim.x;
+    for (long i = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) b[i] = sqrt(a[i]);
 }
 
 __global__ void to_f32_kernel(long n, const double* __restrict__ a, float* __restrict__ b) {
@@ -453,6 +492,7 @@ struct ciecu_mixed_s {
     ciecu::SellArgs<float, short> a16{};
     ciecu::SellArgs<float, int> a32{};
     float* dinv32 = nullptr;
+    double* sdiag = nullptr;  // sqrt(D^-1) when the inner system is scaled
     float *x32 = nullptr, *r32 = nullptr, *p32 = nullptr, *q32 = nullptr;
     double* x64 = nullptr;
     const double* b = nullptr;
@@ -528,14 +568,16 @@ int launch_inner(ciecu_mixed_s* M, cudaStream_t st, cudaGraph_t root, cudaGraphC
     mixed_update_kernel<COND><<<fit_grid(mixed_update_kernel<COND>, kT, needV), kT, 0, st>>>(
         M->n, M->x32, M->r32, M->p32, M->q32, M->dinv32, M->d_s, M->d_partials, M->d_counter, loop, refine);
     auto refinement = [&](cudaStream_t s2) -> int {
-        mixed_fold_kernel<<<fit_grid(mixed_fold_kernel, kT, needA), kT, 0, s2>>>(M->n, M->x64, M->x32, M->d_s);
+        mixed_fold_kernel<<<fit_grid(mixed_fold_kernel, kT, needA), kT, 0, s2>>>(M->n, M->x64, M->x32, M->sdiag,
+                                                                                M->d_s);
         const int needR = csr_grid(A, A->kernel);
         CIECU_TRY(with_schedule(A->kernel, [&](auto k) -> int {
             constexpr int K = decltype(k)::value;
             mixed_residual_kernel<K, false, COND><<<fit_grid(mixed_residual_kernel<K, false, COND>, csr_threads<K>(),
                                                              needR),
                                                     csr_threads<K>(), 0, s2>>>(
-                A->args<double>(), M->b, M->x64, M->dinv32, M->r32, M->d_s, M->d_partials, M->d_counter, loop);
+                A->args<double>(), M->b, M->x64, M->dinv32, M->r32, M->sdiag, M->d_s, M->d_partials, M->d_counter,
+                loop);
             return CIECU_OK;
         }));
         return CIECU_OK;
@@ -598,6 +640,7 @@ int ciecu_mixed_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_sta
     CIECU_REQUIRE(lhs && out && d_inverseDiagonal, "mixed_create: null argument");
     CIECU_REQUIRE(lhs->valueType == CIECU_F64 && lhs->rows == lhs->cols, "mixed_create: square FP64 matrix expected");
     CIECU_REQUIRE(options.mode == 0 || options.mode == 1, "mixed_create: mode must be 0 or 1");
+    CIECU_REQUIRE(options.scaleInner == 0 || options.scaleInner == 1, "mixed_create: scaleInner must be 0 or 1");
     CIECU_REQUIRE(options.delta > 0.0 && options.delta < 1.0, "mixed_create: delta must be in (0, 1)");
     CIECU_REQUIRE(options.innerKernel == 0 || options.innerKernel == 1 || options.innerKernel == 2 ||
                       options.innerKernel == 4 || options.innerKernel == -1,
@@ -622,6 +665,14 @@ int ciecu_mixed_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_sta
     if (e == cudaSuccess) e = cudaMalloc(&M->d_counter, sizeof(unsigned) * 4);
     if (e == cudaSuccess) e = cudaMemsetAsync(M->d_counter, 0, sizeof(unsigned) * 4, st);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&M->side, cudaStreamNonBlocking);
+    if (e == cudaSuccess && options.scaleInner) {
+        e = cudaMalloc(&M->sdiag, sizeof(double) * n);
+        if (e == cudaSuccess && M->n > 0) {
+            sqrt_kernel<<<grid_for(M->n, kT, 8), kT, 0, st>>>(M->n, d_inverseDiagonal, M->sdiag);
+            count_launch();
+            e = cudaGetLastError();
+        }
+    }
     if (e == cudaSuccess) e = cudaMalloc(&M->sliceLen, sizeof(int) * std::max(1, M->nslices));
     if (e == cudaSuccess) e = cudaMalloc(&M->sliceStart, sizeof(long long) * (M->nslices + 1));
     if (e == cudaSuccess) e = cudaMalloc(&M->rowLen, sizeof(unsigned short) * n);
@@ -670,13 +721,16 @@ int ciecu_mixed_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_sta
             sell_fill_kernel<short><<<grid, kT, 0, st>>>(static_cast<int>(M->n), lhs->rowptr, lhs->col,
                                                          static_cast<const double*>(lhs->val), M->sliceLen,
                                                          M->sliceStart, M->val32, static_cast<short*>(M->col32or16),
-                                                         M->rowLen, d_flag);
+                                                         M->rowLen, d_flag, M->sdiag);
         else
             sell_fill_kernel<int><<<grid, kT, 0, st>>>(static_cast<int>(M->n), lhs->rowptr, lhs->col,
                                                        static_cast<const double*>(lhs->val), M->sliceLen,
                                                        M->sliceStart, M->val32, static_cast<int*>(M->col32or16),
-                                                       M->rowLen, d_flag);
-        to_f32_kernel<<<grid, kT, 0, st>>>(M->n, d_inverseDiagonal, M->dinv32);
+                                                       M->rowLen, d_flag, M->sdiag);
+        if (M->sdiag)
+            fill_f32_kernel<<<grid, kT, 0, st>>>(M->n, 1.0f, M->dinv32);  // D^-1 of the scaled matrix
+        else
+            to_f32_kernel<<<grid, kT, 0, st>>>(M->n, d_inverseDiagonal, M->dinv32);
         count_launch(2);
         e = cudaGetLastError();
     }
@@ -696,7 +750,7 @@ int ciecu_mixed_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_sta
         if (e == cudaSuccess && M->n > 0) {
             sell_fill_kernel<int><<<grid_for(M->n, kT, 8), kT, 0, st>>>(
                 static_cast<int>(M->n), lhs->rowptr, lhs->col, static_cast<const double*>(lhs->val), M->sliceLen,
-                M->sliceStart, M->val32, static_cast<int*>(M->col32or16), M->rowLen, d_flag);
+                M->sliceStart, M->val32, static_cast<int*>(M->col32or16), M->rowLen, d_flag, M->sdiag);
             count_launch();
             e = cudaGetLastError();
         }
@@ -787,6 +841,7 @@ int ciecu_mixed_destroy(ciecu_mixed M) {
     cudaFree(M->val32);
     cudaFree(M->col32or16);
     cudaFree(M->dinv32);
+    cudaFree(M->sdiag);
     cudaFree(M->x32);
     cudaFree(M->r32);
     cudaFree(M->p32);
@@ -888,6 +943,7 @@ int ciecu_mixed_product(ciecu_mixed M, double inScale, const double* d_in, doubl
         init.relTol = M->settings.relativeResidual;
         init.delta = M->options.delta;
         init.mode = M->options.mode;
+        init.scaled = M->sdiag ? 1 : 0;
         *M->h_s = init;
         CIECU_CUDA(cudaMemcpyAsync(M->d_s, M->h_s, sizeof(MixedScalars), cudaMemcpyHostToDevice, st));
         CIECU_CUDA(cudaMemsetAsync(M->x32, 0, sizeof(float) * n, st));
@@ -898,7 +954,7 @@ int ciecu_mixed_product(ciecu_mixed M, double inScale, const double* d_in, doubl
             mixed_residual_kernel<K, true, false><<<fit_grid(mixed_residual_kernel<K, true, false>, csr_threads<K>(),
                                                              needR),
                                                     csr_threads<K>(), 0, st>>>(
-                A->args<double>(), d_in, M->x64, M->dinv32, M->r32, M->d_s, M->d_partials, M->d_counter, 0);
+                A->args<double>(), d_in, M->x64, M->dinv32, M->r32, M->sdiag, M->d_s, M->d_partials, M->d_counter, 0);
             return CIECU_OK;
         }));
         mixed_direction_kernel<<<fit_grid(mixed_direction_kernel, kT, ((n + 3) / 4 + kT - 1) / kT), kT, 0, st>>>(

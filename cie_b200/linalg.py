@@ -551,7 +551,7 @@ class MixedPrecisionCG(LinearOperator):
     refinement (delta = inner tolerance).  Stops on the true FP64 residual."""
 
     def __init__(self, lhs, inverseDiagonal, settings=None, mode=0, delta=None, compressColumns=True,
-                 innerKernel=0):
+                 innerKernel=0, scaleInner=False):
         if type(lhs) is not CSROperator or lhs.space._sfx != "f64":
             raise CiecuError(1, "MixedPrecisionCG needs an FP64 CSROperator")
         self.lhs = lhs
@@ -559,7 +559,8 @@ class MixedPrecisionCG(LinearOperator):
         self.inverseDiagonal = inverseDiagonal
         self.settings = settings if settings is not None else Statistics(5000, 0.0, 1e-10)
         delta = (0.1 if mode == 0 else 1e-4) if delta is None else float(delta)
-        self.options = MixedOptions(int(mode), delta, int(bool(compressColumns)), int(innerKernel))
+        self.options = MixedOptions(int(mode), delta, int(bool(compressColumns)), int(innerKernel),
+                                    int(bool(scaleInner)))
         h = ctypes.c_void_p()
         self.space.enter()
         call("ciecu_mixed_create", lhs.csr.handle, _ptr(inverseDiagonal.inverseDiagonal), self.settings, self.options,

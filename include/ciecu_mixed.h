@@ -32,6 +32,12 @@ typedef struct ciecu_mixed_options {
      * of four entries each thread keeps in flight; -1 fixes the TMA-pipelined
      * kernel (matrix streamed through shared memory by bulk copies). */
     int innerKernel;
+    /* 1: the FP32 inner system is the symmetrically Jacobi-scaled matrix
+     * D^-1/2 A D^-1/2 (unit diagonal), for matrices whose entries span many orders
+     * of magnitude (embedded domains with a small material factor), where an
+     * unscaled FP32 copy loses the small couplings and definiteness; the FP64
+     * residuals, solution and stopping test are unchanged.  0: the unscaled copy. */
+    int scaleInner;
 } ciecu_mixed_options;
 
 typedef struct ciecu_mixed_statistics {

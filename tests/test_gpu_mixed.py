@@ -153,3 +153,31 @@ def test_sell_inner_operator_on_ragged_rows(space, restatement, inner, compress)
                            np.zeros(n))
     scale = np.array([np.sum(np.abs(val[rp[i]:rp[i + 1]] * x[col[rp[i]:rp[i + 1]]])) for i in range(n)]) + 1e-30
     assert np.max(np.abs(host(y) - ref) / scale) <= 2e-6
+
+
+@pytest.mark.parametrize("embedded", [False, True])
+def test_mixed_scaled_inner_vs_reference(space, reference, embedded):
+    """The Jacobi-scaled FP32 inner system (scaleInner): same accuracy bar, on a
+    log-normal problem and on an embedded sphere with material factor 1e-6, whose
+    unscaled FP32 copy loses the small couplings."""
+    from cie_b200.fem import make_embedded_poisson, make_poisson
+    from cie_b200.linalg import CSROperator, MixedPrecisionCG, Statistics, makeDiagonalOperator
+    if embedded:
+        prob = make_embedded_poisson(space, 3, 3, [6, 6, 6], radius=0.4, alpha=1e-6, depth=2)
+    else:
+        prob = make_poisson(space, 3, 1, [40, 40, 40], seed=2)
+    rp, col, val = prob.host_csr()
+    b = host(prob.rhs)
+    A = CSROperator(prob.matrix, space)
+    D = makeDiagonalOperator(prob.matrix, space, csr_handle=A.csr)
+    solver = MixedPrecisionCG(A, D, Statistics(200000, 0.0, 1e-10), scaleInner=True)
+    x = dev(np.zeros(len(b)))
+    solver.product(0.0, dev(b), 1.0, x)
+    x, st = host(x), solver.getStats()
+    xr, sr, err, _ = reference.pcg(rp, col, val, b, maxit=200000, abstol=0.0, reltol=1e-10)
+    rel = np.linalg.norm(x - xr) / np.linalg.norm(xr)
+    tr = true_residual(rp, col, val, x, b)
+    print("scaled inner (%s): %d inner iterations, %d refinements (FP64 reference %d), rel %.3e, true residual %.3e"
+          % ("embedded" if embedded else "lognormal", st.innerIterations, st.refinements, sr[0], rel, tr))
+    assert st.trueRelativeResidual < 1e-10 and tr <= 1.05e-10
+    assert rel <= 1e-9
