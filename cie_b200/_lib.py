@@ -109,6 +109,7 @@ SIGNATURES = {
     "ciecu_batch_destroy": (c_int, [P]),
     "ciecu_batch_info": (c_int, [P, P, P, P]),
     "ciecu_batch_product": (c_int, [P, c_double, P, c_double, P, P]),
+    "ciecu_batch_set_refinement": (c_int, [P, c_double]),
     "ciecu_multi_create": (c_int, [P, c_int, P, Statistics, P]),
     "ciecu_multi_destroy": (c_int, [P]),
     "ciecu_multi_info": (c_int, [P, P, P]),

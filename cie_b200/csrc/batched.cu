@@ -20,6 +20,8 @@
 #include "ciecu_batch.h"
 
 #include <algorithm>
+#include <cmath>
+#include <limits>
 #include <string>
 #include <vector>
 
@@ -58,6 +60,11 @@ __device__ __forceinline__ void set_loop(cudaGraphConditionalHandle cond, unsign
     if constexpr (COND) cudaGraphSetConditional(cond, value);
 }
 
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+
 // Tile-level reduction of K values; the CTA holding the system's last tile gets
 // the system totals (in tile order) in every thread and returns true.
 template <int K>
@@ -93,9 +100,8 @@ __device__ __forceinline__ bool system_reduce_last(const double (&mine)[K], cons
 }
 
 // Rows [rb, re) of the tile: VS lanes per row, the CTA's warps striding over rows.
-template <int VS, typename Op>
-__device__ __forceinline__ void tile_rows(const CsrArgs<double>& A, int rb, int re, const double* __restrict__ x,
-                                          Op& op) {
+template <int VS, typename T, typename Op>
+__device__ __forceinline__ void tile_rows(const CsrArgs<T>& A, int rb, int re, const T* __restrict__ x, Op& op) {
     constexpr int RPW = 32 / VS;
     constexpr int UNROLL = VS <= 4 ? 8 : 4;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -105,22 +111,22 @@ __device__ __forceinline__ void tile_rows(const CsrArgs<double>& A, int rb, int 
         const bool valid = r < re;
         typename Op::Pre pre{};
         if (valid && sub == 0) pre = op.pre(r);
-        double sum = 0.0;
+        T sum = T(0);
         if (valid) {
             const int k1 = A.rowptr[r + 1];
             for (int k = A.rowptr[r] + sub; k < k1; k += UNROLL * VS) {
-                double v[UNROLL];
+                T v[UNROLL];
                 int c[UNROLL];
 #pragma unroll
                 for (int u = 0; u < UNROLL; ++u) {
                     const int kk = k + u * VS;
                     const bool in = kk < k1;
-                    v[u] = in ? stream_ld(A.val + kk) : 0.0;
+                    v[u] = in ? stream_ld(A.val + kk) : T(0);
                     c[u] = in ? stream_ld(A.col + kk) : -1;
                 }
-                double xv[UNROLL];
+                T xv[UNROLL];
 #pragma unroll
-                for (int u = 0; u < UNROLL; ++u) xv[u] = c[u] >= 0 ? __ldg(x + c[u]) : 0.0;
+                for (int u = 0; u < UNROLL; ++u) xv[u] = c[u] >= 0 ? __ldg(x + c[u]) : T(0);
 #pragma unroll
                 for (int u = 0; u < UNROLL; ++u) sum = fma(v[u], xv[u], sum);
             }
@@ -131,15 +137,16 @@ __device__ __forceinline__ void tile_rows(const CsrArgs<double>& A, int rb, int 
     }
 }
 
+template <typename T>
 struct PqOp {
-    using Pre = double;
-    const double* __restrict__ p;
-    double* __restrict__ q;
+    using Pre = T;
+    const T* __restrict__ p;
+    T* __restrict__ q;
     double acc;
-    __device__ __forceinline__ double pre(int r) const { return p[r]; }
-    __device__ __forceinline__ void post(int r, double pr, double sum) {
+    __device__ __forceinline__ T pre(int r) const { return p[r]; }
+    __device__ __forceinline__ void post(int r, T pr, T sum) {
         q[r] = sum;
-        acc = fma(pr, sum, acc);
+        acc = fma(static_cast<double>(pr), static_cast<double>(sum), acc);
     }
 };
 
@@ -156,20 +163,24 @@ __global__ void batch_check_kernel(CsrArgs<double> A, const Tile* __restrict__ t
 }
 
 // r = b - A x is formed before; z = D^-1 r, p = z, rr, rz and the initial test.
+// Systems preset to done = 4 (skipped: already converged in the outer FP64
+// refinement) take no work.
+template <typename T>
 __global__ void __launch_bounds__(kT) batch_init_kernel(const Tile* __restrict__ tiles, int ntiles,
                                                         const int* tileBegin, const int* tileCount,
-                                                        const double* __restrict__ r, const double* __restrict__ dinv,
-                                                        double* __restrict__ p, BatchScalars* S, BatchGlobal* g,
+                                                        const T* __restrict__ r, const T* __restrict__ dinv,
+                                                        T* __restrict__ p, BatchScalars* S, BatchGlobal* g,
                                                         double* partials, unsigned* counter) {
     for (int ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
         const Tile t = tiles[ti];
+        if (S[t.system].done == 4) continue;
         double rr = 0.0, rz = 0.0;
         for (int i = t.rowBegin + threadIdx.x; i < t.rowEnd; i += kT) {
-            const double ri = r[i];
-            const double zi = ri * dinv[i];
+            const T ri = r[i];
+            const T zi = ri * dinv[i];
             p[i] = zi;
-            rr = fma(ri, ri, rr);
-            rz = fma(ri, zi, rz);
+            rr = fma(static_cast<double>(ri), static_cast<double>(ri), rr);
+            rz = fma(static_cast<double>(ri), static_cast<double>(zi), rz);
         }
         double mine[2] = {rr, rz}, tot[2];
         if (system_reduce_last<2>(mine, t, tileBegin, tileCount, partials, counter, tot) && threadIdx.x == 0) {
@@ -200,16 +211,16 @@ __global__ void __launch_bounds__(kT) batch_init_kernel(const Tile* __restrict__
 }
 
 // K1: q = A p and p^T q per system; alpha.
-template <int VS>
-__global__ void __launch_bounds__(kT) batch_spmv_kernel(CsrArgs<double> A, const Tile* __restrict__ tiles, int ntiles,
+template <int VS, typename T>
+__global__ void __launch_bounds__(kT) batch_spmv_kernel(CsrArgs<T> A, const Tile* __restrict__ tiles, int ntiles,
                                                         const int* tileBegin, const int* tileCount,
-                                                        const double* __restrict__ p, double* __restrict__ q,
+                                                        const T* __restrict__ p, T* __restrict__ q,
                                                         BatchScalars* S, BatchGlobal* g, double* partials,
                                                         unsigned* counter) {
     for (int ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
         const Tile t = tiles[ti];
         if (*reinterpret_cast<volatile int*>(&S[t.system].done)) continue;
-        PqOp op{p, q, 0.0};
+        PqOp<T> op{p, q, 0.0};
         tile_rows<VS>(A, t.rowBegin, t.rowEnd, p, op);
         double mine[1] = {op.acc}, tot[1];
         if (system_reduce_last<1>(mine, t, tileBegin, tileCount, partials, counter, tot) && threadIdx.x == 0) {
@@ -229,24 +240,25 @@ __global__ void __launch_bounds__(kT) batch_spmv_kernel(CsrArgs<double> A, const
 }
 
 // K2: x += alpha p; r -= alpha q; rr, rz; beta and the stopping test per system.
+template <typename T>
 __global__ void __launch_bounds__(kT) batch_update_kernel(const Tile* __restrict__ tiles, int ntiles,
                                                           const int* tileBegin, const int* tileCount,
-                                                          double* __restrict__ x, double* __restrict__ r,
-                                                          const double* __restrict__ p, const double* __restrict__ q,
-                                                          const double* __restrict__ dinv, BatchScalars* S,
+                                                          T* __restrict__ x, T* __restrict__ r,
+                                                          const T* __restrict__ p, const T* __restrict__ q,
+                                                          const T* __restrict__ dinv, BatchScalars* S,
                                                           BatchGlobal* g, double* partials, unsigned* counter) {
     for (int ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
         const Tile t = tiles[ti];
         BatchScalars& s = S[t.system];
         if (*reinterpret_cast<volatile int*>(&s.done)) continue;
-        const double alpha = s.alpha, malpha = -alpha;
+        const T alpha = static_cast<T>(s.alpha), malpha = -alpha;
         double rr = 0.0, rz = 0.0;
         for (int i = t.rowBegin + threadIdx.x; i < t.rowEnd; i += kT) {
             x[i] = fma(alpha, p[i], x[i]);
-            const double ri = fma(malpha, q[i], r[i]);
+            const T ri = fma(malpha, q[i], r[i]);
             r[i] = ri;
-            rr = fma(ri, ri, rr);
-            rz = fma(ri, ri * dinv[i], rz);
+            rr = fma(static_cast<double>(ri), static_cast<double>(ri), rr);
+            rz = fma(static_cast<double>(ri), static_cast<double>(ri * dinv[i]), rz);
         }
         double mine[2] = {rr, rz}, tot[2];
         if (system_reduce_last<2>(mine, t, tileBegin, tileCount, partials, counter, tot) && threadIdx.x == 0) {
@@ -269,10 +281,10 @@ __global__ void __launch_bounds__(kT) batch_update_kernel(const Tile* __restrict
 
 // K3: p = beta p + z (the rounding of space.scale + space.add, as the single
 // solver); ends the loop when every system is finished.
-template <bool COND>
+template <typename T, bool COND>
 __global__ void __launch_bounds__(kT) batch_direction_kernel(const Tile* __restrict__ tiles, int ntiles, int systems,
-                                                             double* __restrict__ p, const double* __restrict__ r,
-                                                             const double* __restrict__ dinv,
+                                                             T* __restrict__ p, const T* __restrict__ r,
+                                                             const T* __restrict__ dinv,
                                                              const BatchScalars* S, BatchGlobal* g,
                                                              cudaGraphConditionalHandle cond) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -284,9 +296,9 @@ __global__ void __launch_bounds__(kT) batch_direction_kernel(const Tile* __restr
         const Tile t = tiles[ti];
         const BatchScalars& s = S[t.system];
         if (*reinterpret_cast<const volatile int*>(&s.done)) continue;
-        const double beta = s.beta;
+        const T beta = static_cast<T>(s.beta);
         for (int i = t.rowBegin + threadIdx.x; i < t.rowEnd; i += kT)
-            p[i] = __dadd_rn(__dmul_rn(p[i], beta), __dmul_rn(r[i], dinv[i]));
+            p[i] = add_rn(mul_rn(p[i], beta), mul_rn(r[i], dinv[i]));
     }
 }
 
@@ -323,25 +335,80 @@ int with_lanes(int vs, F&& f) {
 }  // namespace
 }  // namespace ciecu
 
+namespace ciecu {
+namespace {
+
+// Comparison::less with the default tolerances (Comparison_impl.hpp:32-63), on the host.
+bool host_float_less(double a, double b) {
+    const double norm = std::fmin(std::fabs(a) + std::fabs(b), std::numeric_limits<double>::max());
+    const double tol = std::fmax(std::numeric_limits<double>::min(), std::numeric_limits<double>::epsilon() * norm);
+    return a < b && !(std::fabs(a - b) < tol);
+}
+
+// FP64 residual norms per system (outer refinement): norm2[s] = ||r_s||^2.
+__global__ void __launch_bounds__(kT) batch_norm_kernel(const Tile* __restrict__ tiles, int ntiles,
+                                                        const int* tileBegin, const int* tileCount,
+                                                        const double* __restrict__ r, double* __restrict__ norm2,
+                                                        double* partials, unsigned* counter) {
+    for (int ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
+        const Tile t = tiles[ti];
+        double rr = 0.0;
+        for (int i = t.rowBegin + threadIdx.x; i < t.rowEnd; i += kT) rr = fma(r[i], r[i], rr);
+        double mine[1] = {rr}, tot[1];
+        if (system_reduce_last<1>(mine, t, tileBegin, tileCount, partials, counter, tot) && threadIdx.x == 0)
+            norm2[t.system] = tot[0];
+        __syncthreads();
+    }
+}
+
+__global__ void batch_to_f32_kernel(long n, const double* __restrict__ a, float* __restrict__ b) {
+    const long stride = static_cast<long>(gridDim.x) * blockDim.x;
+    for (long i = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+        b[i] = static_cast<float>(a[i]);
+}
+
+// x64 += x32 (the correction of one refinement round)
+__global__ void batch_fold_kernel(long n, double* __restrict__ x64, const float* __restrict__ x32) {
+    const long stride = static_cast<long>(gridDim.x) * blockDim.x;
+    for (long i = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+        x64[i] += static_cast<double>(x32[i]);
+}
+
+// One precision of the batched iteration: the matrix values, the vectors, the
+// tuned lanes per row and the graph of the loop.
+template <typename T>
+struct Level {
+    CsrArgs<T> A{};
+    const T* dinv = nullptr;
+    T *x = nullptr, *r = nullptr, *p = nullptr, *q = nullptr;
+    int lanes = 4;
+    cudaGraphExec_t graph = nullptr;
+    bool deviceLoop = false;
+};
+
+}  // namespace
+}  // namespace ciecu
+
 struct ciecu_batch_s {
     ciecu_csr_s* A = nullptr;
-    const double* dinv = nullptr;
     ciecu_statistics settings{};
     long n = 0;
     int systems = 0, ntiles = 0;
-    int lanes = 4;  // lanes per row of K1 (autotuned)
     ciecu::Tile* d_tiles = nullptr;
     int* d_tileBegin = nullptr;
     int* d_tileCount = nullptr;
     long long* d_rowOffsets = nullptr;
-    double *x = nullptr, *r = nullptr, *p = nullptr, *q = nullptr;
+    ciecu::Level<double> f64;
+    ciecu::Level<float> f32;  // FP32 inner level of the refined solve (allocated by set_refinement)
+    float* val32 = nullptr;
+    float* dinv32 = nullptr;
+    double* norm2 = nullptr;  // per-system ||r||^2 of the outer refinement
+    double innerTolerance = 0.0;  // > 0: FP32 inner solves with FP64 refinement
     ciecu::BatchScalars* d_s = nullptr;
     ciecu::BatchGlobal* d_g = nullptr;
     ciecu::BatchGlobal* h_g = nullptr;
     double* d_partials = nullptr;
     unsigned* d_counter = nullptr;
-    cudaGraphExec_t graph = nullptr;
-    bool deviceLoop = false;
     int chunk = 16;
     int grid = 1;
 };
@@ -349,56 +416,57 @@ struct ciecu_batch_s {
 namespace ciecu {
 namespace {
 
-template <bool COND>
-int launch_batch_iteration(ciecu_batch_s* B, cudaStream_t st, cudaGraphConditionalHandle cond) {
-    CIECU_TRY(with_lanes(B->lanes, [&](auto v) -> int {
+template <typename T, bool COND>
+int launch_batch_iteration(ciecu_batch_s* B, Level<T>& L, cudaStream_t st, cudaGraphConditionalHandle cond) {
+    CIECU_TRY(with_lanes(L.lanes, [&](auto v) -> int {
         constexpr int VS = decltype(v)::value;
-        batch_spmv_kernel<VS><<<B->grid, kT, 0, st>>>(B->A->args<double>(), B->d_tiles, B->ntiles, B->d_tileBegin,
-                                                      B->d_tileCount, B->p, B->q, B->d_s, B->d_g, B->d_partials,
-                                                      B->d_counter);
+        batch_spmv_kernel<VS, T><<<B->grid, kT, 0, st>>>(L.A, B->d_tiles, B->ntiles, B->d_tileBegin, B->d_tileCount,
+                                                         L.p, L.q, B->d_s, B->d_g, B->d_partials, B->d_counter);
         return CIECU_OK;
     }));
-    batch_update_kernel<<<B->grid, kT, 0, st>>>(B->d_tiles, B->ntiles, B->d_tileBegin, B->d_tileCount, B->x, B->r,
-                                                B->p, B->q, B->dinv, B->d_s, B->d_g, B->d_partials, B->d_counter);
-    batch_direction_kernel<COND><<<B->grid, kT, 0, st>>>(B->d_tiles, B->ntiles, B->systems, B->p, B->r, B->dinv,
-                                                         B->d_s, B->d_g, cond);
+    batch_update_kernel<T><<<B->grid, kT, 0, st>>>(B->d_tiles, B->ntiles, B->d_tileBegin, B->d_tileCount, L.x, L.r,
+                                                   L.p, L.q, L.dinv, B->d_s, B->d_g, B->d_partials, B->d_counter);
+    batch_direction_kernel<T, COND><<<B->grid, kT, 0, st>>>(B->d_tiles, B->ntiles, B->systems, L.p, L.r, L.dinv,
+                                                            B->d_s, B->d_g, cond);
     CIECU_CHECK_LAUNCH("batched pcg iteration");
     return CIECU_OK;
 }
 
-int build_batch_graph(ciecu_batch_s* B) {
-    if (B->graph) return CIECU_OK;
+template <typename T>
+int build_batch_graph(ciecu_batch_s* B, Level<T>& L) {
+    if (L.graph) return CIECU_OK;
     cudaStream_t st = B->A->space->stream;
     if (device_loop_enabled()) {
         const int status = build_while_graph(st, [&](cudaGraph_t, cudaGraphConditionalHandle cond) {
-            return launch_batch_iteration<true>(B, st, cond);
-        }, &B->graph);
+            return launch_batch_iteration<T, true>(B, L, st, cond);
+        }, &L.graph);
         if (status == CIECU_OK) {
-            B->deviceLoop = true;
+            L.deviceLoop = true;
             return CIECU_OK;
         }
         cudaGetLastError();
     }
-    B->deviceLoop = false;
+    L.deviceLoop = false;
     cudaGraph_t g = nullptr;
     CIECU_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     int status = CIECU_OK;
-    for (int i = 0; i < B->chunk && status == CIECU_OK; ++i) status = launch_batch_iteration<false>(B, st, 0);
+    for (int i = 0; i < B->chunk && status == CIECU_OK; ++i) status = launch_batch_iteration<T, false>(B, L, st, 0);
     cudaError_t e = cudaStreamEndCapture(st, &g);
     if (status != CIECU_OK) {
         if (g) cudaGraphDestroy(g);
         return status;
     }
     if (e != cudaSuccess) return cuda_fail(e, "batched graph capture");
-    e = cudaGraphInstantiate(&B->graph, g, 0);
+    e = cudaGraphInstantiate(&L.graph, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return cuda_fail(e, "batched graph instantiate");
     return CIECU_OK;
 }
 
-// Times K1 for each lane count on the solver's buffers (p = D^-1 > 0, every
+// Times K1 for each lane count on the level's buffers (p = D^-1 > 0, every
 // system running) and keeps the fastest.
-int tune_batch(ciecu_batch_s* B) {
+template <typename T>
+int tune_batch(ciecu_batch_s* B, Level<T>& L) {
     cudaStream_t st = B->A->space->stream;
     std::vector<BatchScalars> scratch(B->systems);
     for (auto& s : scratch) {
@@ -406,7 +474,7 @@ int tune_batch(ciecu_batch_s* B) {
         s.rz = 1.0;
     }
     CIECU_CUDA(cudaMemcpyAsync(B->d_s, scratch.data(), sizeof(BatchScalars) * B->systems, cudaMemcpyHostToDevice, st));
-    CIECU_CUDA(cudaMemcpyAsync(B->p, B->dinv, sizeof(double) * B->n, cudaMemcpyDeviceToDevice, st));
+    CIECU_CUDA(cudaMemcpyAsync(L.p, L.dinv, sizeof(T) * B->n, cudaMemcpyDeviceToDevice, st));
     cudaEvent_t e0, e1;
     CIECU_CUDA(cudaEventCreate(&e0));
     CIECU_CUDA(cudaEventCreate(&e1));
@@ -419,9 +487,9 @@ int tune_batch(ciecu_batch_s* B) {
         auto launch = [&]() {
             with_lanes(vs, [&](auto v) -> int {
                 constexpr int VS = decltype(v)::value;
-                batch_spmv_kernel<VS><<<B->grid, kT, 0, st>>>(B->A->args<double>(), B->d_tiles, B->ntiles,
-                                                              B->d_tileBegin, B->d_tileCount, B->p, B->q, B->d_s,
-                                                              B->d_g, B->d_partials, B->d_counter);
+                batch_spmv_kernel<VS, T><<<B->grid, kT, 0, st>>>(L.A, B->d_tiles, B->ntiles, B->d_tileBegin,
+                                                                 B->d_tileCount, L.p, L.q, B->d_s, B->d_g,
+                                                                 B->d_partials, B->d_counter);
                 return CIECU_OK;
             });
         };
@@ -444,7 +512,39 @@ int tune_batch(ciecu_batch_s* B) {
     cudaEventDestroy(e1);
     if (e == cudaSuccess) e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "batched pcg: autotune");
-    B->lanes = bestLanes;
+    L.lanes = bestLanes;
+    return CIECU_OK;
+}
+
+// One batched PCG solve on level L from x = 0 (or the level's current x) for
+// every system whose scalars are not preset to done = 4; the right-hand side is
+// in L.r on entry (it becomes the residual).  Returns when every system is done.
+template <typename T>
+int run_level(ciecu_batch_s* B, Level<T>& L, const BatchGlobal& g0, unsigned preset) {
+    cudaStream_t st = B->A->space->stream;
+    *B->h_g = g0;
+    B->h_g->finished = preset;
+    CIECU_CUDA(cudaMemcpyAsync(B->d_g, B->h_g, sizeof(BatchGlobal), cudaMemcpyHostToDevice, st));
+    batch_init_kernel<T><<<B->grid, kT, 0, st>>>(B->d_tiles, B->ntiles, B->d_tileBegin, B->d_tileCount, L.r, L.dinv,
+                                                 L.p, B->d_s, B->d_g, B->d_partials, B->d_counter);
+    count_launch();
+    CIECU_CHECK_LAUNCH("batch_init_kernel");
+    CIECU_TRY(build_batch_graph(B, L));
+    const long long limit = L.deviceLoop ? 4096 : B->chunk;
+    for (;;) {
+        CIECU_CUDA(cudaMemcpyAsync(B->h_g, B->d_g, sizeof(BatchGlobal), cudaMemcpyDeviceToHost, st));
+        CIECU_CUDA(cudaStreamSynchronize(st));
+        if (B->h_g->finished >= static_cast<unsigned>(B->systems)) break;
+        B->h_g->chunkIter = 0;
+        B->h_g->chunkLimit = limit;
+        CIECU_CUDA(cudaMemcpyAsync(&B->d_g->chunkIter, &B->h_g->chunkIter, 2 * sizeof(long long),
+                                   cudaMemcpyHostToDevice, st));
+        CIECU_CUDA(cudaGraphLaunch(L.graph, st));
+        CIECU_CUDA(cudaMemcpyAsync(B->h_g, B->d_g, sizeof(BatchGlobal), cudaMemcpyDeviceToHost, st));
+        CIECU_CUDA(cudaStreamSynchronize(st));
+        count_launch(3LL * (L.deviceLoop ? B->h_g->chunkIter : B->chunk));
+        if (B->h_g->finished >= static_cast<unsigned>(B->systems)) break;
+    }
     return CIECU_OK;
 }
 
@@ -475,7 +575,8 @@ int ciecu_batch_create(ciecu_csr lhs, int64_t systems, const int64_t* h_rowOffse
     }
     auto* B = new ciecu_batch_s();
     B->A = lhs;
-    B->dinv = d_inverseDiagonal;
+    B->f64.dinv = d_inverseDiagonal;
+    B->f64.A = lhs->args<double>();
     B->settings = settings;
     B->n = lhs->rows;
     B->systems = static_cast<int>(systems);
@@ -486,7 +587,7 @@ int ciecu_batch_create(ciecu_csr lhs, int64_t systems, const int64_t* h_rowOffse
     if (e == cudaSuccess) e = cudaMalloc(&B->d_tileBegin, sizeof(int) * systems);
     if (e == cudaSuccess) e = cudaMalloc(&B->d_tileCount, sizeof(int) * systems);
     if (e == cudaSuccess) e = cudaMalloc(&B->d_rowOffsets, sizeof(long long) * (systems + 1));
-    for (double** v : {&B->x, &B->r, &B->p, &B->q})
+    for (double** v : {&B->f64.x, &B->f64.r, &B->f64.p, &B->f64.q})
         if (e == cudaSuccess) e = cudaMalloc(v, sizeof(double) * std::max<size_t>(1, n));
     if (e == cudaSuccess) e = cudaMalloc(&B->d_s, sizeof(BatchScalars) * systems);
     if (e == cudaSuccess) e = cudaMalloc(&B->d_g, sizeof(BatchGlobal));
@@ -530,8 +631,8 @@ int ciecu_batch_create(ciecu_csr lhs, int64_t systems, const int64_t* h_rowOffse
                                             " has an entry outside its system's column block");
     }
     B->grid = std::max(1, std::min(B->ntiles, resident_blocks(reinterpret_cast<const void*>(
-                                                                   batch_spmv_kernel<4>), kT, 0)));
-    const int status = tune_batch(B);
+                                                                   batch_spmv_kernel<4, double>), kT, 0)));
+    const int status = tune_batch(B, B->f64);
     if (status != CIECU_OK) {
         ciecu_batch_destroy(B);
         return status;
@@ -542,15 +643,17 @@ int ciecu_batch_create(ciecu_csr lhs, int64_t systems, const int64_t* h_rowOffse
 
 int ciecu_batch_destroy(ciecu_batch B) {
     if (!B) return CIECU_OK;
-    if (B->graph) cudaGraphExecDestroy(B->graph);
+    if (B->f64.graph) cudaGraphExecDestroy(B->f64.graph);
+    if (B->f32.graph) cudaGraphExecDestroy(B->f32.graph);
     cudaFree(B->d_tiles);
     cudaFree(B->d_tileBegin);
     cudaFree(B->d_tileCount);
     cudaFree(B->d_rowOffsets);
-    cudaFree(B->x);
-    cudaFree(B->r);
-    cudaFree(B->p);
-    cudaFree(B->q);
+    for (double* v : {B->f64.x, B->f64.r, B->f64.p, B->f64.q}) cudaFree(v);
+    for (float* v : {B->f32.x, B->f32.r, B->f32.p, B->f32.q}) cudaFree(v);
+    cudaFree(B->val32);
+    cudaFree(B->dinv32);
+    cudaFree(B->norm2);
     cudaFree(B->d_s);
     cudaFree(B->d_g);
     if (B->h_g) cudaFreeHost(B->h_g);
@@ -562,10 +665,36 @@ int ciecu_batch_destroy(ciecu_batch B) {
 
 int ciecu_batch_info(ciecu_batch B, int* lanesPerRow, int* deviceLoop, int64_t* tiles) {
     CIECU_REQUIRE(B, "batch_info: null solver");
-    if (lanesPerRow) *lanesPerRow = B->lanes;
-    if (deviceLoop) *deviceLoop = B->deviceLoop ? 1 : 0;
+    if (lanesPerRow) *lanesPerRow = B->f64.lanes;
+    if (deviceLoop) *deviceLoop = B->f64.deviceLoop ? 1 : 0;
     if (tiles) *tiles = B->ntiles;
     return CIECU_OK;
+}
+
+int ciecu_batch_set_refinement(ciecu_batch B, double innerTolerance) {
+    CIECU_REQUIRE(B, "batch_set_refinement: null solver");
+    CIECU_REQUIRE(innerTolerance >= 0.0 && innerTolerance < 1.0, "batch_set_refinement: tolerance must be in [0, 1)");
+    B->innerTolerance = innerTolerance;
+    if (innerTolerance == 0.0 || B->val32) return CIECU_OK;
+    cudaStream_t st = B->A->space->stream;
+    const size_t n = static_cast<size_t>(std::max<long>(1, B->n));
+    cudaError_t e = cudaMalloc(&B->val32, sizeof(float) * std::max<long>(1, B->A->nnz));
+    if (e == cudaSuccess) e = cudaMalloc(&B->dinv32, sizeof(float) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&B->norm2, sizeof(double) * B->systems);
+    for (float** v : {&B->f32.x, &B->f32.r, &B->f32.p, &B->f32.q})
+        if (e == cudaSuccess) e = cudaMalloc(v, sizeof(float) * n);
+    if (e == cudaSuccess && B->A->nnz > 0) {
+        batch_to_f32_kernel<<<grid_for(B->A->nnz, kT, 8), kT, 0, st>>>(
+            B->A->nnz, static_cast<const double*>(B->A->val), B->val32);
+        batch_to_f32_kernel<<<grid_for(B->n, kT, 8), kT, 0, st>>>(B->n, B->f64.dinv, B->dinv32);
+        count_launch(2);
+        e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "batch_set_refinement: FP32 copies");
+    B->f32.A = CsrArgs<float>{B->A->rowptr, B->A->col, B->val32, B->A->rows, B->A->nnz, B->A->d_blocks,
+                              B->A->nblocks, nullptr, 0, B->A->aligned16};
+    B->f32.dinv = B->dinv32;
+    return tune_batch(B, B->f32);
 }
 
 int ciecu_batch_product(ciecu_batch B, double inScale, const double* d_in, double outScale, double* d_out,
@@ -574,63 +703,114 @@ int ciecu_batch_product(ciecu_batch B, double inScale, const double* d_in, doubl
     ciecu_csr_s* A = B->A;
     cudaStream_t st = A->space->stream;
     const long n = B->n;
-    CIECU_CUDA(cudaMemcpyAsync(B->x, d_out, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    Level<double>& L = B->f64;
+    CIECU_CUDA(cudaMemcpyAsync(L.x, d_out, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
     std::vector<BatchScalars> s(static_cast<size_t>(B->systems));
+    std::vector<ciecu_statistics> out(static_cast<size_t>(B->systems),
+                                      ciecu_statistics{0, 1.7976931348623157e308, 1.7976931348623157e308});
+    std::vector<int> failedKind(static_cast<size_t>(B->systems), 0);
+    std::vector<long long> failedIter(static_cast<size_t>(B->systems), 0);
     if (B->settings.iterationCount > 0) {
         BatchGlobal g{};
         g.maxIter = B->settings.iterationCount;
         g.absTol = B->settings.absoluteResidual;
         g.relTol = B->settings.relativeResidual;
         g.badColumn = 0x7fffffff;
-        *B->h_g = g;
-        CIECU_CUDA(cudaMemcpyAsync(B->d_g, B->h_g, sizeof(BatchGlobal), cudaMemcpyHostToDevice, st));
-        CIECU_CUDA(cudaMemcpyAsync(B->r, d_in, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-        CIECU_TRY(ciecu_csr_spmv_f64(A, 1.0, B->x, -1.0, B->r));  // r = b - A x0 (block diagonal: per system)
-        batch_init_kernel<<<B->grid, kT, 0, st>>>(B->d_tiles, B->ntiles, B->d_tileBegin, B->d_tileCount, B->r,
-                                                   B->dinv, B->p, B->d_s, B->d_g, B->d_partials, B->d_counter);
-        count_launch();
-        CIECU_CHECK_LAUNCH("batch_init_kernel");
-        CIECU_TRY(build_batch_graph(B));
-        const long long limit = B->deviceLoop ? 4096 : B->chunk;
-        for (;;) {
-            CIECU_CUDA(cudaMemcpyAsync(B->h_g, B->d_g, sizeof(BatchGlobal), cudaMemcpyDeviceToHost, st));
+        CIECU_CUDA(cudaMemcpyAsync(L.r, d_in, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+        CIECU_TRY(ciecu_csr_spmv_f64(A, 1.0, L.x, -1.0, L.r));  // r = b - A x0 (block diagonal: per system)
+        if (B->innerTolerance == 0.0) {
+            // FP64: every system runs ConjugateGradients_impl.hpp:49-201 as it is
+            CIECU_CUDA(cudaMemsetAsync(B->d_s, 0, sizeof(BatchScalars) * B->systems, st));
+            CIECU_TRY(run_level(B, L, g, 0u));
+            CIECU_CUDA(cudaMemcpyAsync(s.data(), B->d_s, sizeof(BatchScalars) * B->systems, cudaMemcpyDeviceToHost,
+                                       st));
             CIECU_CUDA(cudaStreamSynchronize(st));
-            if (B->h_g->finished >= static_cast<unsigned>(B->systems)) break;
-            B->h_g->chunkIter = 0;
-            B->h_g->chunkLimit = limit;
-            CIECU_CUDA(cudaMemcpyAsync(&B->d_g->chunkIter, &B->h_g->chunkIter, 2 * sizeof(long long),
-                                       cudaMemcpyHostToDevice, st));
-            CIECU_CUDA(cudaGraphLaunch(B->graph, st));
-            CIECU_CUDA(cudaMemcpyAsync(B->h_g, B->d_g, sizeof(BatchGlobal), cudaMemcpyDeviceToHost, st));
-            CIECU_CUDA(cudaStreamSynchronize(st));
-            count_launch(3LL * (B->deviceLoop ? B->h_g->chunkIter : B->chunk));
-            if (B->h_g->finished >= static_cast<unsigned>(B->systems)) break;
+            for (int i = 0; i < B->systems; ++i) {
+                out[i] = ciecu_statistics{s[i].done == 3 ? s[i].errorIter : s[i].iter, s[i].absres, s[i].relres};
+                if (s[i].done == 3) {
+                    failedKind[i] = s[i].errorKind;
+                    failedIter[i] = s[i].errorIter;
+                }
+            }
+        } else {
+            // FP32 inner solves, FP64 refinement: each round solves A32 c = float(r) to
+            // innerTolerance for the systems not yet converged, x += c, r = b - A x in FP64;
+            // a system stops on its true FP64 residual (Comparison::less against the
+            // absolute or the relative limit, relative to its initial residual).
+            Level<float>& F = B->f32;
+            std::vector<double> r0(static_cast<size_t>(B->systems)), nrm(static_cast<size_t>(B->systems));
+            std::vector<int> state(static_cast<size_t>(B->systems), 0);  // 0 running, 1 converged, 2 limit, 3 failed
+            std::vector<long long> used(static_cast<size_t>(B->systems), 0);
+            BatchGlobal gi = g;
+            gi.relTol = B->innerTolerance;
+            gi.absTol = 0.0;
+            for (int round = 0;; ++round) {
+                batch_norm_kernel<<<B->grid, kT, 0, st>>>(B->d_tiles, B->ntiles, B->d_tileBegin, B->d_tileCount, L.r,
+                                                           B->norm2, B->d_partials, B->d_counter);
+                count_launch();
+                CIECU_CHECK_LAUNCH("batch_norm_kernel");
+                CIECU_CUDA(cudaMemcpyAsync(nrm.data(), B->norm2, sizeof(double) * B->systems,
+                                           cudaMemcpyDeviceToHost, st));
+                CIECU_CUDA(cudaStreamSynchronize(st));
+                unsigned preset = 0;
+                for (int i = 0; i < B->systems; ++i) {
+                    const double absres = std::sqrt(nrm[i]);
+                    if (round == 0) r0[i] = absres;
+                    const double relres = r0[i] > 0.0 ? absres / r0[i] : 0.0;
+                    if (state[i] == 0) {
+                        out[i] = ciecu_statistics{used[i], absres, relres};
+                        if (host_float_less(absres, g.absTol) || host_float_less(relres, g.relTol)) state[i] = 1;
+                        else if (used[i] >= g.maxIter) state[i] = 2;
+                    }
+                    s[i] = BatchScalars{};
+                    if (state[i] != 0) {
+                        s[i].done = 4;
+                        ++preset;
+                    }
+                }
+                if (preset == static_cast<unsigned>(B->systems)) break;
+                long long budget = g.maxIter;
+                for (int i = 0; i < B->systems; ++i)
+                    if (state[i] == 0) budget = std::min(budget, g.maxIter - used[i]);
+                gi.maxIter = std::max<long long>(1, budget);
+                CIECU_CUDA(cudaMemcpyAsync(B->d_s, s.data(), sizeof(BatchScalars) * B->systems, cudaMemcpyHostToDevice,
+                                           st));
+                batch_to_f32_kernel<<<grid_for(n, kT, 8), kT, 0, st>>>(n, L.r, F.r);
+                CIECU_CUDA(cudaMemsetAsync(F.x, 0, sizeof(float) * n, st));
+                count_launch();
+                CIECU_TRY(run_level(B, F, gi, preset));
+                batch_fold_kernel<<<grid_for(n, kT, 8), kT, 0, st>>>(n, L.x, F.x);
+                count_launch();
+                CIECU_CUDA(cudaMemcpyAsync(L.r, d_in, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+                CIECU_TRY(ciecu_csr_spmv_f64(A, 1.0, L.x, -1.0, L.r));
+                std::vector<BatchScalars> si(static_cast<size_t>(B->systems));
+                CIECU_CUDA(cudaMemcpyAsync(si.data(), B->d_s, sizeof(BatchScalars) * B->systems,
+                                           cudaMemcpyDeviceToHost, st));
+                CIECU_CUDA(cudaStreamSynchronize(st));
+                for (int i = 0; i < B->systems; ++i) {
+                    if (state[i] != 0) continue;
+                    used[i] += si[i].done == 3 ? si[i].errorIter : si[i].iter;
+                    if (si[i].done == 3 && si[i].iter == 0 && si[i].errorIter == 0) {
+                        state[i] = 3;  // no progress possible in FP32
+                        failedKind[i] = si[i].errorKind;
+                        failedIter[i] = used[i];
+                    }
+                }
+            }
         }
-        CIECU_CUDA(cudaMemcpyAsync(s.data(), B->d_s, sizeof(BatchScalars) * B->systems, cudaMemcpyDeviceToHost, st));
-        CIECU_CUDA(cudaStreamSynchronize(st));
     }
-    batch_output_kernel<<<grid_for(n, kT, 8), kT, 0, st>>>(n, inScale, outScale, B->x, d_out);
+    batch_output_kernel<<<grid_for(n, kT, 8), kT, 0, st>>>(n, inScale, outScale, L.x, d_out);
     count_launch();
     CIECU_CHECK_LAUNCH("batch_output_kernel");
     CIECU_CUDA(cudaStreamSynchronize(st));
-    int firstError = -1;
-    for (int i = 0; i < B->systems; ++i) {
-        const BatchScalars& si = s[i];
-        if (h_stats) {
-            if (B->settings.iterationCount > 0)
-                h_stats[i] = ciecu_statistics{si.done == 3 ? si.errorIter : si.iter, si.absres, si.relres};
-            else
-                h_stats[i] = ciecu_statistics{0, 1.7976931348623157e308, 1.7976931348623157e308};
-        }
-        if (si.done == 3 && firstError < 0) firstError = i;
-    }
-    if (firstError >= 0) {
-        const BatchScalars& si = s[firstError];
-        return fail(CIECU_ERR_BREAKDOWN,
-                    "system " + std::to_string(firstError) + ": " +
-                        (si.errorKind == 1 ? std::string("preconditioned norm vanished in iteration 0 (r^T @ z = 0)")
-                                           : "p^T @ A @ p vanished in iteration " + std::to_string(si.errorIter)));
-    }
+    if (h_stats)
+        for (int i = 0; i < B->systems; ++i) h_stats[i] = out[i];
+    for (int i = 0; i < B->systems; ++i)
+        if (failedKind[i])
+            return fail(CIECU_ERR_BREAKDOWN,
+                        "system " + std::to_string(i) + ": " +
+                            (failedKind[i] == 1 ? std::string("preconditioned norm vanished in iteration 0 (r^T @ z = 0)")
+                                                : "p^T @ A @ p vanished in iteration " + std::to_string(failedIter[i])));
     return CIECU_OK;
 }
 

@@ -667,6 +667,14 @@ class BatchedConjugateGradients(LinearOperator):
         call("ciecu_batch_info", self._solver, ctypes.byref(v), ctypes.byref(d), ctypes.byref(t))
         return {"lanes_per_row": v.value, "device_loop": bool(d.value), "tiles": t.value}
 
+    def set_refinement(self, innerTolerance):
+        """innerTolerance > 0: FP32 inner solves with FP64 refinement (0: FP64)."""
+        self.space.enter()
+        try:
+            call("ciecu_batch_set_refinement", self._solver, float(innerTolerance))
+        finally:
+            self.space.leave()
+
     def getStats(self):
         return self._stats
 

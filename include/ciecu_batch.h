@@ -37,6 +37,14 @@ int ciecu_batch_info(ciecu_batch solver, int* lanesPerRow, int* deviceLoop, int6
  * system; the other systems are solved and their statistics filled. */
 int ciecu_batch_product(ciecu_batch solver, double inScale, const double* d_in, double outScale,
                         double* d_out, ciecu_statistics* h_stats);
+/* innerTolerance > 0: later products run FP32 inner solves with FP64 refinement
+ * -- each round solves the FP32 copy of the matrix to innerTolerance relative
+ * to the current residual for the systems not yet converged, adds the
+ * correction to the FP64 solution and recomputes r = b - A x in FP64; a system
+ * stops on its true FP64 residual.  statistics: inner (FP32) iterations and the
+ * true residuals.  0 (the default): the FP64 solve.  The first call with a
+ * positive tolerance allocates the FP32 copies and autotunes their SpMV. */
+int ciecu_batch_set_refinement(ciecu_batch solver, double innerTolerance);
 
 #ifdef __cplusplus
 }

@@ -107,3 +107,30 @@ def test_batched_pcg_breakdown_names_the_system(space):
         solver.product(0.0, rhs, 1.0, x)
     stats = solver.getStats()
     assert stats[0].relativeResidual <= 1e-10 and stats[2].relativeResidual <= 1e-10
+
+
+def test_batched_fp32_refined_vs_reference(space, reference):
+    """FP32 inner solves with FP64 refinement (set_refinement): every system reaches
+    its true FP64 relative residual 1e-10 and lands within 1e-9 of the reference
+    CG's solution."""
+    from cie_b200.linalg import BatchedConjugateGradients, Statistics, block_diagonal, makeDiagonalOperator
+    probs = systems(space, 10, seed=17)
+    bd, offsets = block_diagonal([p.matrix for p in probs])
+    rhs = torch.cat([p.rhs for p in probs])
+    D = makeDiagonalOperator(bd, space)
+    solver = BatchedConjugateGradients(bd, offsets, space, D, Statistics(20000, 0.0, 1e-10))
+    solver.set_refinement(1e-3)
+    x = torch.zeros_like(rhs)
+    solver.product(0.0, rhs, 1.0, x)
+    stats = solver.getStats()
+    xh = x.cpu().numpy()
+    for s, p in enumerate(probs):
+        rp, col, val = p.host_csr()
+        b = p.rhs.cpu().numpy()
+        xs = xh[offsets[s]:offsets[s + 1]]
+        xr, sr, err, _ = reference.pcg(rp, col, val, b, maxit=20000, abstol=0.0, reltol=1e-10)
+        r = b - np.array([val[rp[i]:rp[i + 1]] @ xs[col[rp[i]:rp[i + 1]]] for i in range(len(b))])
+        assert stats[s].relativeResidual <= 1e-10, (s, stats[s].relativeResidual)
+        assert np.linalg.norm(r) <= 1.05e-10 * np.linalg.norm(b)
+        assert np.linalg.norm(xs - xr) <= 1e-9 * np.linalg.norm(xr)
+    print("refined: inner iterations %s (FP64 reference %s)" % ([st.iterationCount for st in stats[:4]], int(sr[0])))
