@@ -500,6 +500,18 @@ def extra_workloads(space, A, D, settings, t_fp64, it64):
     tb = timed(solveb, 3)
     its = [s.iterationCount for s in batch.getStats()]
     rels = [s.relativeResidual for s in batch.getStats()]
+    # the same batch with FP32 inner solves and FP64 refinement
+    refined = BatchedConjugateGradients(bd, offsets, space, Dbd, tight)
+    refined.set_refinement(1e-2)
+    xr = torch.zeros_like(rhs)
+
+    def solver_refined():
+        xr.zero_()
+        refined.product(0.0, rhs, 1.0, xr)
+    tr = timed(solver_refined, 2)
+    rits = [s.iterationCount for s in refined.getStats()]
+    rrel = max(s.relativeResidual for s in refined.getStats())
+    del refined
     # the same systems one after another (one solver object per system)
     singles = []
     for p in probs:
@@ -517,8 +529,11 @@ def extra_workloads(space, A, D, settings, t_fp64, it64):
         "seconds": tb, "systems": len(probs), "total_dofs": int(rhs.numel()), "total_nnz": bd.nnz(),
         "iterations_min": int(min(its)), "iterations_max": int(max(its)), "max_relative_residual": max(rels),
         "sequential_single_solves_seconds": ts, "speedup_vs_sequential": ts / tb,
-        "rel_diff_vs_single_solves": agree, "solver": batch.info()}
-    del singles, batch, Dbd, bd, rhs, xb, probs
+        "rel_diff_vs_single_solves": agree, "solver": batch.info(),
+        "fp32_refined_seconds": tr, "fp32_refined_inner_iterations_max": int(max(rits)),
+        "fp32_refined_max_relative_residual": rrel,
+        "fp32_refined_rel_diff_vs_fp64": float(torch.linalg.norm(xr - xb) / torch.linalg.norm(xb))}
+    del singles, batch, Dbd, bd, rhs, xb, xr, probs
 
     # 32 right-hand sides on the 128^3 matrix
     n = A.lhs.rowCount()
