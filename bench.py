@@ -191,6 +191,11 @@ def main():
     ap.add_argument("--pin", default=None,
                     help="with --profile: FP64-solver,mixed-unroll,CSR schedules to use instead of autotuning "
                          "(the choices a bench run without the profiler reports), e.g. 4,1,4")
+    ap.add_argument("--profile-target", default="pcg", choices=["pcg", "batch", "spmm", "embedded", "gradient"],
+                    help="with --profile: the solver the ncu target runs (pcg: the headline solves; batch: a "
+                         "batched solve of 128 Q2 systems; spmm: a 32-RHS solve on the Q1 grid of --profile-cells; "
+                         "embedded: the finite-cell Q3 assembly on 16^3 cells; gradient: one adjoint gradient on "
+                         "the Q1 grid of --profile-cells)")
     ap.add_argument("--profile-cells", type=int, default=PROFILE_CELLS[0],
                     help="cells per axis of the --profile case (96: 290 MB matrix; 128: the full workload)")
     args = ap.parse_args()
@@ -218,6 +223,9 @@ def main():
         torch.cuda.synchronize()
 
     space = CUDASpace()
+    if args.profile and args.profile_target != "pcg":
+        profile_target(space, args.profile_target, args.profile_cells)
+        return
     cells = [args.profile_cells] * 3 if args.profile else WORKLOAD["cells"]
     prob = make_poisson(space, 3, 1, cells, seed=WORKLOAD["seed"])
     n, nnz = prob.mesh.ndofs, prob.matrix.nnz()
@@ -433,6 +441,49 @@ def main():
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def profile_target(space, target, cells):
+    """Short runs of the other solvers for ncu (inputs built first, one solve or
+    assembly, no timing)."""
+    import torch
+    from cie_b200.fem import kappa_field, make_embedded_poisson, make_poisson, random_uniform
+    from cie_b200.linalg import (BatchedConjugateGradients, CSROperator, MultiRHSConjugateGradients, Statistics,
+                                 block_diagonal, makeDiagonalOperator)
+    tight = Statistics(20000, 0.0, 1e-10)
+    if target == "batch":
+        rng = np.random.default_rng(0)
+        sizes = rng.integers(16, 129, 128)
+        probs = [make_poisson(space, 2, 2, [int(m), int(m)], seed=1000 + 3 * i) for i, m in enumerate(sizes)]
+        bd, offsets = block_diagonal([p.matrix for p in probs])
+        rhs = torch.cat([p.rhs for p in probs])
+        solver = BatchedConjugateGradients(bd, offsets, space, makeDiagonalOperator(bd, space), tight)
+        x = torch.zeros_like(rhs)
+        solver.product(0.0, rhs, 1.0, x)
+        info = solver.info()
+    elif target == "spmm":
+        prob = make_poisson(space, 3, 1, [cells] * 3, seed=0)
+        n = prob.rhs.numel()
+        A = CSROperator(prob.matrix, space)
+        D = makeDiagonalOperator(prob.matrix, space, csr_handle=A.csr)
+        B = torch.as_tensor(np.stack([random_uniform(2000 + c, n) for c in range(32)], axis=1)).cuda().contiguous()
+        solver = MultiRHSConjugateGradients(A, D, 32, tight)
+        X = torch.zeros_like(B)
+        solver.product(0.0, B, 1.0, X)
+        info = solver.info()
+    elif target == "embedded":
+        prob = make_embedded_poisson(space, 3, 3, [16, 16, 16], radius=0.4, alpha=1e-6, depth=2)
+        info = {"cut_cells": prob.cut_cells}
+    else:
+        from cie_b200.adjoint import DifferentiablePoisson
+        prob = DifferentiablePoisson(space, 3, 1, [cells] * 3, settings=tight)
+        kappa = torch.as_tensor(kappa_field(1, [cells] * 3)).cuda().requires_grad_(True)
+        b = torch.as_tensor(random_uniform(0, prob.n)).cuda()
+        u = prob(kappa, b)
+        (0.5 * torch.sum(u ** 2)).backward()
+        info = {"adjoint_iterations": prob.adjoint_stats.iterationCount}
+    torch.cuda.synchronize()
+    print(json.dumps({"profile": True, "target": target, "info": info}), flush=True)
 
 
 def extra_workloads(space, A, D, settings, t_fp64, it64, rank=0, world=1):

@@ -112,14 +112,24 @@ struct __align__(16) Entry {
     int pad;
 };
 
-template <int KP, typename Op>
+// One 16-byte shared-memory read of an entry.
+__device__ __forceinline__ void load_entry(const Entry* e, double& a, int& col) {
+    const double2 raw = *reinterpret_cast<const double2*>(e);
+    a = raw.x;
+    col = static_cast<int>(__double_as_longlong(raw.y) & 0xffffffffLL);
+}
+
+// FULL: k == KP, so every lane is active and the row stride of X is the
+// compile-time KP (the gather address is a shift and an add).
+template <int KP, bool FULL, typename Op>
 __device__ __forceinline__ void multi_rows(const CsrArgs<double>& A, int k, const double* __restrict__ X, Op& op) {
     __shared__ Entry s_e[kStreamTile];  // one 16-byte broadcast read per entry
     constexpr int RPW = 32 / KP;
     constexpr int UNROLL = 8;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int slot = lane / KP, c = lane % KP;
-    const bool active = c < k;
+    const bool active = FULL || c < k;
+    const long ld = FULL ? KP : k;
     const double* __restrict__ xc = X + c;
     for (int b = blockIdx.x; b < A.nblocks; b += gridDim.x) {
         const int r0 = A.blocks[b], r1 = A.blocks[b + 1];
@@ -138,23 +148,25 @@ __device__ __forceinline__ void multi_rows(const CsrArgs<double>& A, int k, cons
             if (staged) {
                 int j = k0;
                 for (; j + UNROLL <= k1; j += UNROLL) {
-                    Entry e[UNROLL];
-                    double pv[UNROLL];
+                    double av[UNROLL], pv[UNROLL];
 #pragma unroll
                     for (int u = 0; u < UNROLL; ++u) {
-                        e[u] = s_e[j + u];
-                        pv[u] = active ? __ldg(xc + static_cast<long>(e[u].col) * k) : 0.0;
+                        int col;
+                        load_entry(s_e + j + u, av[u], col);
+                        pv[u] = active ? __ldg(xc + static_cast<long>(col) * ld) : 0.0;
                     }
 #pragma unroll
-                    for (int u = 0; u < UNROLL; ++u) acc = fma(e[u].a, pv[u], acc);
+                    for (int u = 0; u < UNROLL; ++u) acc = fma(av[u], pv[u], acc);
                 }
                 for (; j < k1; ++j) {
-                    const Entry e = s_e[j];
-                    acc = fma(e.a, active ? __ldg(xc + static_cast<long>(e.col) * k) : 0.0, acc);
+                    double a;
+                    int col;
+                    load_entry(s_e + j, a, col);
+                    acc = fma(a, active ? __ldg(xc + static_cast<long>(col) * ld) : 0.0, acc);
                 }
             } else {
                 for (int j = e0 + k0; j < e0 + k1; ++j)
-                    acc = fma(A.val[j], active ? __ldg(xc + static_cast<long>(A.col[j]) * k) : 0.0, acc);
+                    acc = fma(A.val[j], active ? __ldg(xc + static_cast<long>(A.col[j]) * ld) : 0.0, acc);
             }
             if (active) op(row, c, acc);
         }
@@ -171,11 +183,11 @@ struct ResidualOp {  // R = B - A X
     }
 };
 
-template <int KP>
+template <int KP, bool FULL>
 __global__ void __launch_bounds__(kT) multi_residual_kernel(CsrArgs<double> A, int k, const double* __restrict__ X,
                                                             const double* __restrict__ B, double* __restrict__ R) {
     ResidualOp op{B, R, k};
-    multi_rows<KP>(A, k, X, op);
+    multi_rows<KP, FULL>(A, k, X, op);
 }
 
 // Initial set-up per column: z = D^-1 r, p = z, rr, rz and the initial test.
@@ -236,7 +248,7 @@ struct PqOp {
 };
 
 // K1: Q = A P and p_c^T q_c; alpha per column.
-template <int KP, bool COND>
+template <int KP, bool FULL, bool COND>
 __global__ void __launch_bounds__(kT) multi_spmv_kernel(CsrArgs<double> A, int k, const double* __restrict__ P,
                                                         double* __restrict__ Q, ColumnScalars* S, MultiGlobal* g,
                                                         double* partials, unsigned* counter,
@@ -246,7 +258,7 @@ __global__ void __launch_bounds__(kT) multi_spmv_kernel(CsrArgs<double> A, int k
         return;
     }
     PqOp op{P, Q, k, 0.0};
-    multi_rows<KP>(A, k, P, op);
+    multi_rows<KP, FULL>(A, k, P, op);
     double mine[1] = {op.acc}, tot[1];
     if (column_reduce_last<KP, 1>(mine, k, partials, counter, tot) && threadIdx.x < k) {
         ColumnScalars& s = S[threadIdx.x];
@@ -393,8 +405,13 @@ template <bool COND>
 int launch_multi_iteration(ciecu_multi_s* M, cudaStream_t st, cudaGraphConditionalHandle cond) {
     CIECU_TRY(with_group(M->kp, [&](auto kk) -> int {
         constexpr int KP = decltype(kk)::value;
-        multi_spmv_kernel<KP, COND><<<M->grid, kT, 0, st>>>(M->A->args<double>(), M->k, M->p, M->q, M->d_s, M->d_g,
-                                                            M->d_partials, M->d_counter, cond);
+        if (M->k == KP)
+            multi_spmv_kernel<KP, true, COND><<<M->grid, kT, 0, st>>>(M->A->args<double>(), M->k, M->p, M->q, M->d_s,
+                                                                      M->d_g, M->d_partials, M->d_counter, cond);
+        else
+            multi_spmv_kernel<KP, false, COND><<<M->grid, kT, 0, st>>>(M->A->args<double>(), M->k, M->p, M->q,
+                                                                       M->d_s, M->d_g, M->d_partials, M->d_counter,
+                                                                       cond);
         multi_update_kernel<KP><<<M->gridV, kT, 0, st>>>(M->n, M->k, M->x, M->r, M->p, M->q, M->dinv, M->d_s,
                                                          M->d_g, M->d_partials, M->d_counter);
         multi_direction_kernel<KP, COND><<<M->gridV, kT, 0, st>>>(M->n, M->k, M->p, M->r, M->dinv, M->d_s, M->d_g,
@@ -465,7 +482,8 @@ int ciecu_multi_create(ciecu_csr lhs, int rhsCount, const double* d_inverseDiago
     const long needed = (M->n + static_cast<long>(kWarps) * (32 / M->kp) - 1) / (static_cast<long>(kWarps) * (32 / M->kp));
     with_group(M->kp, [&](auto kk) -> int {
         constexpr int KP = decltype(kk)::value;
-        M->grid = resident_blocks(reinterpret_cast<const void*>(multi_spmv_kernel<KP, true>), kT, 0);
+        M->grid = std::min(resident_blocks(reinterpret_cast<const void*>(multi_spmv_kernel<KP, true, true>), kT, 0),
+                           resident_blocks(reinterpret_cast<const void*>(multi_spmv_kernel<KP, false, true>), kT, 0));
         M->gridV = resident_blocks(reinterpret_cast<const void*>(multi_update_kernel<KP>), kT, 0);
         return CIECU_OK;
     });
@@ -523,7 +541,11 @@ int ciecu_multi_product(ciecu_multi M, double inScale, const double* d_in, doubl
         CIECU_CUDA(cudaMemcpyAsync(M->d_g, M->h_g, sizeof(MultiGlobal), cudaMemcpyHostToDevice, st));
         CIECU_TRY(with_group(M->kp, [&](auto kk) -> int {
             constexpr int KP = decltype(kk)::value;
-            multi_residual_kernel<KP><<<M->grid, kT, 0, st>>>(M->A->args<double>(), M->k, M->x, d_in, M->r);
+            if (M->k == KP)
+                multi_residual_kernel<KP, true><<<M->grid, kT, 0, st>>>(M->A->args<double>(), M->k, M->x, d_in, M->r);
+            else
+                multi_residual_kernel<KP, false><<<M->grid, kT, 0, st>>>(M->A->args<double>(), M->k, M->x, d_in,
+                                                                         M->r);
             multi_init_kernel<KP><<<M->gridV, kT, 0, st>>>(n, M->k, M->r, M->dinv, M->p, M->d_s, M->d_g,
                                                           M->d_partials, M->d_counter);
             return CIECU_OK;
