@@ -81,6 +81,7 @@ SIGNATURES = {
     "ciecu_pcg_set_graph_chunk": (c_int, [P, c_int]),
     "ciecu_pcg_set_schedule": (c_int, [P, c_int]),
     "ciecu_pcg_info": (c_int, [P, P, P]),
+    "ciecu_pcg_set_loop": (c_int, [P, c_int]),
     "ciecu_mixed_create": (c_int, [P, P, Statistics, MixedOptions, P]),
     "ciecu_mixed_destroy": (c_int, [P]),
     "ciecu_mixed_info": (c_int, [P, P, P]),

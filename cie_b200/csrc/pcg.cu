@@ -15,6 +15,7 @@
 #include "pcg.cuh"
 
 #include <string>
+#include <vector>
 
 namespace ciecu {
 
@@ -202,6 +203,300 @@ __global__ void __launch_bounds__(kT) pcg_direction_kernel(long n, double* __res
     }
 }
 
+// ---- single-launch solve -----------------------------------------------------
+// For a system whose matrix fits in the shared memory of the whole chip, the three
+// launches per iteration cost more than their work.  Here one cooperative launch
+// (every block resident, one per SM) runs the iterations.  Each block owns one
+// contiguous row range (balanced by nonzeros) and keeps its rows of the matrix
+// and its own x, r, D^-1, q, p and z in shared memory for the whole launch.  An
+// iteration has two grid-wide exchanges:
+//   S  q = A p_k with p_k = beta p_{k-1} + z_k formed on the fly for each gathered
+//      column (p is double-buffered in global memory, so no block overwrites a
+//      p_{k-1} another block still reads); the owner of row i stores p_k,i;
+//      partial p^T q.  -> exchange 1: alpha = rz / p^T q in every block.
+//   U  x += alpha p_k, r -= alpha q, z = D^-1 r on the own rows (z also to global
+//      memory for the other blocks' gathers); partial r^T r, r^T z.
+//      -> exchange 2: beta, norms and the stopping test.
+// An exchange publishes the block's partial sums with a release store of an
+// epoch number; every block then reads all blocks' epochs (relaxed loads and one
+// acquire fence) and sums the partials in block order, so all blocks hold
+// bit-identical scalars and take the same branches.  Global vectors written
+// during the launch are read with ld.global.cg (L2), never through the
+// non-coherent L1 or texture paths.  Every wait is bounded (kExchangeWaitCycles
+// SM clock cycles, 2 to 4 s); a wait that gives up sets the abort flag, every
+// block leaves, and the host reports CIECU_ERR_TIMEOUT.  One exchange costs about
+// 5 us on B200 (148 blocks), about a quarter of what three launches per
+// iteration cost together.
+constexpr int kPT = 1024;
+constexpr long long kExchangeWaitCycles = 4000000000LL;
+
+struct alignas(32) ExchangeSlot {
+    double v[2];
+    unsigned long long epoch;
+    unsigned long long pad;
+};
+
+struct PersistentArgs {
+    CsrArgs<double> A;
+    const int2* __restrict__ split;  // (first row, its first entry) of each block; grid + 1 entries
+    const double* __restrict__ dinv;
+    double* x;
+    double* r;
+    double* z;
+    double* p0;  // p_k for even k
+    double* p1;  // p_k for odd k
+    ExchangeSlot* slotsS;
+    ExchangeSlot* slotsU;
+    int* abortFlag;
+    PcgScalars* s;
+    unsigned long long epoch0;
+};
+
+// Shared memory of a block with ne entries and nr rows: doubles (values, then x,
+// r, D^-1, q, p, z of the own rows) followed by ints (columns, local row offsets).
+__host__ __device__ inline size_t persistent_smem(long ne, long nr) {
+    return static_cast<size_t>(8 * (ne + 6 * nr) + 4 * (ne + nr + 1));
+}
+
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
+// Publishes the block's K partial sums under `epoch` and returns in `out` the
+// grid-wide sums (blocks in index order, identical in every block).  False when a
+// wait gave up or another block aborted; the block then leaves the launch.
+template <int K>
+__device__ bool grid_exchange(const double (&mine)[K], ExchangeSlot* slots, unsigned long long epoch,
+                              int* abortFlag, double (&out)[K], double* s_red) {
+    double sums[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) sums[k] = block_sum<double, kPT>(mine[k], s_red);  // orders the block's stores
+    if (threadIdx.x == 0) {
+        ExchangeSlot* m = slots + blockIdx.x;
+#pragma unroll
+        for (int k = 0; k < K; ++k) m->v[k] = sums[k];
+        st_release_u64(&m->epoch, epoch);  // cumulative: also releases the block's stores before the barrier
+    }
+    double acc[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) acc[k] = 0.0;
+    bool ok = true;
+    for (unsigned b = threadIdx.x; b < gridDim.x && ok; b += kPT) {
+        const ExchangeSlot* o = slots + b;
+        const long long t0 = clock64();
+        unsigned spin = 0;
+        while (ld_relaxed_u64(&o->epoch) != epoch) {
+            __nanosleep(20);
+            if ((++spin & 63u) == 0u &&
+                (*reinterpret_cast<volatile int*>(abortFlag) || clock64() - t0 > kExchangeWaitCycles)) {
+                atomicExch(abortFlag, 1);
+                ok = false;
+                break;
+            }
+        }
+        if (ok) {
+            fence_acq_rel_gpu();  // acquire: the partials and the block's vector stores are visible
+#pragma unroll
+            for (int k = 0; k < K; ++k) acc[k] += __ldcg(&o->v[k]);
+        }
+    }
+    if (!__syncthreads_and(ok)) return false;
+#pragma unroll
+    for (int k = 0; k < K; ++k) out[k] = block_sum<double, kPT>(acc[k], s_red);
+    return true;
+}
+
+// First row of block b when the rows are split into `blocks` ranges of about equal
+// nonzero count; entry b of `out` = (first row, its first entry).
+__global__ void persistent_split_kernel(const int* __restrict__ rowptr, int n, long nnz, int blocks,
+                                        int2* __restrict__ out) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b > blocks) return;
+    int row;
+    if (b == 0) {
+        row = 0;
+    } else if (b == blocks) {
+        row = n;
+    } else {
+        const long target = nnz * b / blocks;
+        int lo = 0, hi = n;  // first row with rowptr[row] >= target
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (rowptr[mid] < target) lo = mid + 1;
+            else hi = mid;
+        }
+        row = lo;
+    }
+    out[b] = make_int2(row, rowptr[row]);
+}
+
+template <int VS, bool PRECOND>
+__global__ void __launch_bounds__(kPT, 1) pcg_persistent_kernel(PersistentArgs P) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ double s_red[32];
+    const CsrArgs<double>& A = P.A;
+    PcgScalars* s = P.s;
+    const int2 lo = P.split[blockIdx.x], hi = P.split[blockIdx.x + 1];
+    const int rb = lo.x, nr = hi.x - lo.x;
+    const int eb = lo.y, ne = hi.y - lo.y;
+    double* s_val = reinterpret_cast<double*>(smem);
+    double* s_x = s_val + ne;
+    double* s_r = s_x + nr;
+    double* s_d = s_r + nr;
+    double* s_q = s_d + nr;
+    double* s_p = s_q + nr;
+    double* s_z = s_p + nr;
+    int* s_col = reinterpret_cast<int*>(s_z + nr);
+    int* s_rp = s_col + ne;
+    // Scalars of the iteration, identical in every block.  All reads of *s happen
+    // before this block's first exchange, and block 0 writes *s back only after the
+    // last one, so no block reads a scalar block 0 has already overwritten.
+    long long iter = s->iter;
+    const long long maxIter = s->maxIter;
+    const long long chunkLimit = s->chunkLimit;
+    long long chunkIter = 0;
+    const double absTol = s->absTol, relTol = s->relTol, r0 = s->r0;
+    double rz = s->rz, beta = s->beta, pq = s->pq, alpha = s->alpha, rr = s->rr;
+    double absres = s->absres, relres = s->relres;
+    int done = s->done, error = 0, errorKind = 0;
+    long long errorIter = 0;
+    // Stage the block's matrix rows and own vectors.
+    {
+        const double* pprev = (iter & 1) ? P.p0 : P.p1;
+        for (int e = threadIdx.x; e < ne; e += kPT) {
+            s_val[e] = __ldg(A.val + eb + e);
+            s_col[e] = __ldg(A.col + eb + e);
+        }
+        for (int i = threadIdx.x; i <= nr; i += kPT) s_rp[i] = A.rowptr[rb + i] - eb;
+        for (int i = threadIdx.x; i < nr; i += kPT) {
+            s_x[i] = P.x[rb + i];
+            s_r[i] = P.r[rb + i];
+            s_d[i] = PRECOND ? P.dinv[rb + i] : 1.0;
+            s_z[i] = P.z[rb + i];
+            s_p[i] = iter > 0 ? pprev[rb + i] : 0.0;
+        }
+        __syncthreads();
+    }
+    unsigned long long epoch = P.epoch0;
+    const int lane = threadIdx.x % VS;
+    const int group = threadIdx.x / VS;
+    constexpr int kGroups = kPT / VS;
+    bool aborted = false;
+    while (done == 0) {
+        // ---- S: q = A p_k; p_k of the own rows to shared and global memory -----
+        const bool first = iter == 0;
+        const double* pprev = (iter & 1) ? P.p0 : P.p1;
+        double* pcur = (iter & 1) ? P.p1 : P.p0;
+        double pqPart = 0.0;
+        for (int base = 0; base < nr; base += kGroups) {  // warp-uniform trip count
+            const int row = base + group;
+            double sum = 0.0;
+            if (row < nr) {
+                const int e1 = s_rp[row + 1];
+#pragma unroll 4
+                for (int e = s_rp[row] + lane; e < e1; e += VS) {
+                    const int c = s_col[e];
+                    const double zc = __ldcg(P.z + c);
+                    const double pc = first ? zc : __dadd_rn(__dmul_rn(__ldcg(pprev + c), beta), zc);
+                    sum = fma(s_val[e], pc, sum);
+                }
+            }
+#pragma unroll
+            for (int off = VS / 2; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off, VS);
+            if (row < nr && lane == 0) {
+                const double zi = s_z[row];
+                const double pi = first ? zi : __dadd_rn(__dmul_rn(s_p[row], beta), zi);
+                s_p[row] = pi;
+                pcur[rb + row] = pi;
+                s_q[row] = sum;
+                pqPart = fma(pi, sum, pqPart);
+            }
+        }
+        {
+            double mine[1] = {pqPart}, tot[1];
+            if (!grid_exchange<1>(mine, P.slotsS, ++epoch, P.abortFlag, tot, s_red)) {
+                aborted = true;
+                break;
+            }
+            pq = tot[0];
+        }
+        if (!(0.0 < pq)) {
+            done = 3;
+            error = CIECU_ERR_BREAKDOWN;
+            errorKind = 2;
+            errorIter = iter;
+            break;
+        }
+        alpha = rz / pq;
+        // ---- U: x, r, z on the own rows ----------------------------------------
+        const double malpha = -alpha;
+        double rrPart = 0.0, rzPart = 0.0;
+        for (int i = threadIdx.x; i < nr; i += kPT) {
+            s_x[i] = fma(alpha, s_p[i], s_x[i]);
+            const double ri = fma(malpha, s_q[i], s_r[i]);
+            s_r[i] = ri;
+            rrPart = fma(ri, ri, rrPart);
+            double zi = ri;
+            if (PRECOND) {
+                zi = __dmul_rn(ri, s_d[i]);
+                rzPart = fma(ri, zi, rzPart);
+            }
+            s_z[i] = zi;
+            P.z[rb + i] = zi;
+        }
+        {
+            double mine[2] = {rrPart, rzPart}, tot[2];
+            if (!grid_exchange<2>(mine, P.slotsU, ++epoch, P.abortFlag, tot, s_red)) {
+                aborted = true;
+                break;
+            }
+            const double rzNew = PRECOND ? tot[1] : tot[0];
+            rr = tot[0];
+            beta = rzNew / rz;
+            rz = rzNew;
+            absres = sqrt(tot[0]);
+            relres = absres / r0;
+        }
+        if (float_less(absres, absTol) || float_less(relres, relTol)) {
+            done = 1;
+        } else {
+            iter += 1;
+            if (iter >= maxIter) done = 2;
+        }
+        chunkIter += 1;
+        if (chunkIter >= chunkLimit) break;
+    }
+    if (aborted) return;
+    for (int i = threadIdx.x; i < nr; i += kPT) {
+        P.x[rb + i] = s_x[i];
+        P.r[rb + i] = s_r[i];
+    }
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    s->iter = iter;
+    s->chunkIter = chunkIter;
+    s->rz = rz;
+    s->beta = beta;
+    s->pq = pq;
+    s->alpha = alpha;
+    s->rr = rr;
+    s->absres = absres;
+    s->relres = relres;
+    s->done = done;
+    if (error) {
+        s->error = error;
+        s->errorKind = errorKind;
+        s->errorIter = errorIter;
+    }
+}
+
 __global__ void fill_ones_kernel(long n, double* __restrict__ v) {
     const long stride = static_cast<long>(gridDim.x) * blockDim.x;
     for (long i = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) v[i] = 1.0;
@@ -249,6 +544,19 @@ struct ciecu_pcg_s {
     bool deviceLoop = false;  // graph = WHILE loop (else `chunk` unrolled iterations)
     int kernel = 0;           // K1 schedule, autotuned on the fused SpMV kernel itself
     int chunk = 16;
+    // Single-launch solve (allocated at its first use).
+    int loopMode = 0;     // 0 auto (single launch when the system fits in L2), 1 graph, 2 single launch
+    bool persistent = false;  // the last solve ran as a single launch
+    bool planned = false;     // row split and shared-memory size computed
+    bool fits = false;        // every block's rows fit in shared memory
+    size_t smem = 0;          // dynamic shared memory of the single launch
+    int maxRows = 0;          // rows of the largest block
+    int2* split = nullptr;
+    double* z = nullptr;
+    double* p2 = nullptr;
+    void* slots = nullptr;  // 2 x SMs exchange slots
+    int* abortFlag = nullptr;
+    unsigned long long epoch = 1;
 };
 
 namespace ciecu {
@@ -279,6 +587,136 @@ int launch_iteration(ciecu_pcg_s* S, cudaStream_t st, cudaGraphConditionalHandle
     }
     CIECU_CHECK_LAUNCH("pcg iteration");
     return CIECU_OK;
+}
+
+// Splits the rows into one range per SM (balanced by nonzeros) and sizes the
+// shared memory of the single launch from the largest range.
+int plan_persistent(ciecu_pcg_s* S) {
+    if (S->planned) return CIECU_OK;
+    ciecu_csr_s* A = S->A;
+    cudaStream_t st = A->space->stream;
+    const int G = sm_count();
+    if (!S->split) CIECU_CUDA(cudaMalloc(&S->split, sizeof(int2) * (G + 1)));
+    persistent_split_kernel<<<(G + 1 + 127) / 128, 128, 0, st>>>(A->rowptr, A->rows, A->nnz, G, S->split);
+    count_launch();
+    CIECU_CHECK_LAUNCH("persistent_split_kernel");
+    std::vector<int2> h(G + 1);
+    CIECU_CUDA(cudaMemcpyAsync(h.data(), S->split, sizeof(int2) * (G + 1), cudaMemcpyDeviceToHost, st));
+    CIECU_CUDA(cudaStreamSynchronize(st));
+    size_t smem = 0;
+    int maxRows = 0;
+    for (int b = 0; b < G; ++b) {
+        const long nr = h[b + 1].x - h[b].x, ne = static_cast<long>(h[b + 1].y) - h[b].y;
+        smem = std::max(smem, persistent_smem(ne, nr));
+        maxRows = std::max<int>(maxRows, static_cast<int>(nr));
+    }
+    int device = 0, optin = 0;
+    CIECU_CUDA(cudaGetDevice(&device));
+    CIECU_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+    S->smem = std::max<size_t>(smem, 16);
+    S->maxRows = maxRows;
+    S->fits = S->smem + 1024 <= static_cast<size_t>(optin);  // 1 KB for the static reduction scratch
+    S->planned = true;
+    return CIECU_OK;
+}
+
+int use_persistent(ciecu_pcg_s* S, bool* out) {
+    *out = false;
+    if (S->loopMode == 1) return CIECU_OK;
+    CIECU_TRY(plan_persistent(S));
+    if (S->loopMode == 2 && !S->fits)
+        return fail(CIECU_ERR_ARGUMENT, "pcg: the single-launch solve needs each SM's rows of the matrix in shared "
+                                        "memory; this matrix is too large for it");
+    *out = S->fits;
+    return CIECU_OK;
+}
+
+int ensure_persistent_buffers(ciecu_pcg_s* S) {
+    if (S->slots) return CIECU_OK;
+    const size_t bytes = sizeof(double) * static_cast<size_t>(std::max<long>(S->n, 1));
+    const size_t slotBytes = sizeof(ExchangeSlot) * 2 * static_cast<size_t>(sm_count());
+    cudaStream_t st = S->A->space->stream;
+    cudaError_t e = cudaMalloc(&S->z, bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&S->p2, bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&S->slots, slotBytes);
+    if (e == cudaSuccess) e = cudaMalloc(&S->abortFlag, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemsetAsync(S->slots, 0, slotBytes, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(S->abortFlag, 0, sizeof(int), st);
+    if (e != cudaSuccess) {
+        cudaFree(S->z);
+        cudaFree(S->p2);
+        cudaFree(S->slots);
+        cudaFree(S->abortFlag);
+        S->z = S->p2 = nullptr;
+        S->slots = nullptr;
+        S->abortFlag = nullptr;
+        return cuda_fail(e, "pcg: single-launch buffers");
+    }
+    S->epoch = 1;
+    return CIECU_OK;
+}
+
+template <int VS, bool PRE>
+int launch_persistent(ciecu_pcg_s* S, cudaStream_t st) {
+    auto kernel = pcg_persistent_kernel<VS, PRE>;
+    CIECU_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S->smem)));
+    int occ = 0;
+    CIECU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, kPT, S->smem));
+    if (occ < 1) return fail(CIECU_ERR_CUDA, "pcg: the single-launch kernel does not fit on an SM");
+    const int G = sm_count();
+    ExchangeSlot* slots = static_cast<ExchangeSlot*>(S->slots);
+    PersistentArgs args{S->A->args<double>(), S->split, S->dinv, S->x, S->r, S->z, S->p, S->p2,
+                        slots, slots + G, S->abortFlag, S->d_s, S->epoch};
+    void* params[] = {&args};
+    CIECU_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kernel), dim3(G), dim3(kPT), params,
+                                           S->smem, st));
+    count_launch();
+    return CIECU_OK;
+}
+
+// Lanes per row: as many as leave one lane group per row of the largest block,
+// and no more than the average row needs.
+template <bool PRE>
+int launch_persistent_rows(ciecu_pcg_s* S, cudaStream_t st) {
+    int vs = 32;
+    while (vs > 1 && (kPT / vs < S->maxRows || vs / 2 >= S->A->avgRow)) vs >>= 1;
+    switch (vs) {
+        case 32: return launch_persistent<32, PRE>(S, st);
+        case 16: return launch_persistent<16, PRE>(S, st);
+        case 8: return launch_persistent<8, PRE>(S, st);
+        case 4: return launch_persistent<4, PRE>(S, st);
+        case 2: return launch_persistent<2, PRE>(S, st);
+        default: return launch_persistent<1, PRE>(S, st);
+    }
+}
+
+int launch_persistent_any(ciecu_pcg_s* S, cudaStream_t st) {
+    return S->dinv ? launch_persistent_rows<true>(S, st) : launch_persistent_rows<false>(S, st);
+}
+
+// Runs the iterations as single launches of up to 2^16 iterations each until the
+// device reports done.  On entry z holds z_0 (written by the init kernel).
+int run_persistent(ciecu_pcg_s* S, cudaStream_t st) {
+    constexpr long long kLimit = 1LL << 16;
+    for (;;) {
+        CIECU_CUDA(cudaMemcpyAsync(S->h_s, S->d_s, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
+        CIECU_CUDA(cudaStreamSynchronize(st));
+        if (S->h_s->done) return CIECU_OK;
+        S->h_s->chunkIter = 0;
+        S->h_s->chunkLimit = kLimit;
+        CIECU_CUDA(cudaMemcpyAsync(&S->d_s->chunkIter, &S->h_s->chunkIter, 2 * sizeof(long long),
+                                   cudaMemcpyHostToDevice, st));
+        CIECU_TRY(launch_persistent_any(S, st));
+        S->epoch += 2 * kLimit + 2;  // exchanges of one launch never reuse an epoch
+        int aborted = 0;
+        CIECU_CUDA(cudaMemcpyAsync(&aborted, S->abortFlag, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CIECU_CUDA(cudaStreamSynchronize(st));
+        if (aborted) {
+            CIECU_CUDA(cudaMemsetAsync(S->abortFlag, 0, sizeof(int), st));
+            CIECU_CUDA(cudaStreamSynchronize(st));
+            return fail(CIECU_ERR_TIMEOUT, "pcg: a grid-wide exchange of the single-launch solve gave up waiting");
+        }
+    }
 }
 
 // Picks the K1 schedule by timing the fused SpMV + p^T q kernel itself on the
@@ -435,6 +873,11 @@ int ciecu_pcg_destroy(ciecu_pcg S) {
     if (S->h_s) cudaFreeHost(S->h_s);
     cudaFree(S->d_partials);
     cudaFree(S->d_counter);
+    cudaFree(S->z);
+    cudaFree(S->p2);
+    cudaFree(S->slots);
+    cudaFree(S->abortFlag);
+    cudaFree(S->split);
     delete S;
     return CIECU_OK;
 }
@@ -442,7 +885,14 @@ int ciecu_pcg_destroy(ciecu_pcg S) {
 int ciecu_pcg_info(ciecu_pcg S, int* spmvSchedule, int* deviceLoop) {
     CIECU_REQUIRE(S, "pcg_info: null solver");
     if (spmvSchedule) *spmvSchedule = S->kernel;
-    if (deviceLoop) *deviceLoop = S->deviceLoop ? 1 : 0;
+    if (deviceLoop) *deviceLoop = S->persistent ? 2 : (S->deviceLoop ? 1 : 0);
+    return CIECU_OK;
+}
+
+int ciecu_pcg_set_loop(ciecu_pcg S, int mode) {
+    CIECU_REQUIRE(S, "pcg_set_loop: null solver");
+    CIECU_REQUIRE(mode >= 0 && mode <= 2, "pcg_set_loop: mode must be 0 (auto), 1 (graph) or 2 (single launch)");
+    S->loopMode = mode;
     return CIECU_OK;
 }
 
@@ -478,7 +928,13 @@ int ciecu_pcg_product(ciecu_pcg S, double inScale, const double* d_in, double ou
         return CIECU_OK;
     }
     CIECU_TRY(ensure_tuned(A));
-    CIECU_TRY(tune_solver_spmv(S));
+    bool persistent = false;
+    CIECU_TRY(use_persistent(S, &persistent));
+    if (persistent)
+        CIECU_TRY(ensure_persistent_buffers(S));
+    else
+        CIECU_TRY(tune_solver_spmv(S));
+    S->persistent = persistent;
     // solution <- out (initial guess)
     CIECU_CUDA(cudaMemcpyAsync(S->x, d_out, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
     if (S->settings.iterationCount > 0) {
@@ -492,14 +948,19 @@ int ciecu_pcg_product(ciecu_pcg S, double inScale, const double* d_in, double ou
         CIECU_CUDA(cudaMemcpyAsync(S->r, d_in, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
         CIECU_TRY(ciecu_csr_spmv_f64(A, 1.0, S->x, -1.0, S->r));
         const long needV = (n + kT - 1) / kT;
+        double* p0 = persistent ? S->z : S->p;  // the single launch forms p_0 from z_0
         if (S->dinv)
             pcg_init_kernel<true><<<fit_grid(pcg_init_kernel<true>, kT, needV), kT, 0, st>>>(
-                n, S->r, S->dinv, S->p, S->d_s, S->d_partials, S->d_counter);
+                n, S->r, S->dinv, p0, S->d_s, S->d_partials, S->d_counter);
         else
             pcg_init_kernel<false><<<fit_grid(pcg_init_kernel<false>, kT, needV), kT, 0, st>>>(
-                n, S->r, S->dinv, S->p, S->d_s, S->d_partials, S->d_counter);
+                n, S->r, S->dinv, p0, S->d_s, S->d_partials, S->d_counter);
         count_launch();
         CIECU_CHECK_LAUNCH("pcg_init_kernel");
+    }
+    if (S->settings.iterationCount > 0 && persistent) {
+        CIECU_TRY(run_persistent(S, st));
+    } else if (S->settings.iterationCount > 0) {
         CIECU_TRY(build_graph(S));
         // Replay graph chunks until the device reports done.  The scalars are read
         // back after each chunk; the kernels of a finished solve return at once.
@@ -521,6 +982,8 @@ int ciecu_pcg_product(ciecu_pcg S, double inScale, const double* d_in, double ou
             count_launch(3LL * std::max<long long>(1, S->deviceLoop ? S->h_s->iter - before + 1 : S->chunk));
             if (S->h_s->done) break;
         }
+    }
+    if (S->settings.iterationCount > 0) {
         const PcgScalars& s = *S->h_s;
         if (s.error) {
             if (h_stats) *h_stats = ciecu_statistics{s.errorIter, s.absres, s.relres};

@@ -443,14 +443,22 @@ class ConjugateGradients(LinearOperator):
         if self._solver is not None:
             call("ciecu_pcg_set_schedule", self._solver, int(schedule))
 
+    def set_loop(self, mode):
+        """How the fused solver runs its iterations: 0 auto (a single cooperative
+        launch when every SM's rows of the matrix fit in its shared memory), 1 the
+        graph of three kernels per iteration, 2 the single launch."""
+        if self._solver is not None:
+            call("ciecu_pcg_set_loop", self._solver, int(mode))
+
     def info(self):
-        """SpMV schedule chosen for the fused solver kernel and whether the solve
-        runs as a device-side graph loop (fused device solver only)."""
+        """SpMV schedule chosen for the fused solver kernel and how the last solve
+        ran (fused device solver only)."""
         if self._solver is None:
             return {"fused": False}
         k, d = ctypes.c_int(), ctypes.c_int()
         call("ciecu_pcg_info", self._solver, ctypes.byref(k), ctypes.byref(d))
-        return {"fused": True, "spmv_schedule": k.value, "device_loop": bool(d.value)}
+        return {"fused": True, "spmv_schedule": k.value, "device_loop": d.value >= 1,
+                "loop": ("graph chunks", "graph loop", "single launch")[d.value]}
 
     def product(self, inScale, in_, outScale, out):
         n = self.space.size(out)

@@ -201,9 +201,18 @@ int ciecu_pcg_set_graph_chunk(ciecu_pcg solver, int iterations);
  * (under a profiler). */
 int ciecu_pcg_set_schedule(ciecu_pcg solver, int schedule);
 /* SpMV schedule the solver's autotuner chose for its fused q = A p kernel (0 before
- * the first solve; 1 = row-block stream kernel, else lanes per row) and whether the
- * solve runs as a device-side graph loop (1) or host-polled graph chunks (0). */
+ * the first solve or when the solve ran as a single launch; 1 = row-block stream
+ * kernel, else lanes per row) and how the last solve ran: host-polled graph chunks
+ * (0), a device-side graph loop (1) or a single cooperative launch (2). */
 int ciecu_pcg_info(ciecu_pcg solver, int* spmvSchedule, int* deviceLoop);
+/* How the iterations run.  mode 0 (default): a single cooperative launch, one
+ * block per SM holding its rows of the matrix in shared memory, when every SM's
+ * share fits there, else the graph of three kernels per iteration; 1: always the
+ * graph; 2: always the single launch (CIECU_ERR_ARGUMENT at the next solve when
+ * the matrix does not fit).  The single launch gives results within rounding of
+ * the graph's (its dot products are summed over another grid); a grid-wide wait
+ * that gives up fails with CIECU_ERR_TIMEOUT. */
+int ciecu_pcg_set_loop(ciecu_pcg solver, int mode);
 
 #ifdef __cplusplus
 }

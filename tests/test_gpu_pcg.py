@@ -28,24 +28,33 @@ def true_residual(rp, col, val, x, b):
     return np.linalg.norm(r) / np.linalg.norm(b)
 
 
-def solve_gpu(space, m, b, settings, precond=True, x0=None, si=0.0, so=1.0):
+# Loop modes of the fused solver: 1 = graph of three kernels per iteration,
+# 2 = single cooperative launch with grid-wide exchanges.
+LOOPS = [1, 2]
+
+
+def solve_gpu(space, m, b, settings, precond=True, x0=None, si=0.0, so=1.0, loop=0):
     from cie_b200.linalg import CSROperator, ConjugateGradients, makeDiagonalOperator
     A = CSROperator(m, space)
     P = makeDiagonalOperator(m, space) if precond else None
     cg = ConjugateGradients(A, space, P, settings)
+    cg.set_loop(loop)
     x = dev(np.zeros(len(b)) if x0 is None else x0)
     cg.product(si, dev(b), so, x)
+    if loop:
+        assert (cg.info()["loop"] == "single launch") == (loop == 2)
     return host(x), cg.getStats()
 
 
-def test_pcg_cfg1_vs_reference(space, reference):
+@pytest.mark.parametrize("loop", LOOPS)
+def test_pcg_cfg1_vs_reference(space, reference, loop):
     """2D Q1 Poisson, 256 x 256 cells (66,049 DoFs), Jacobi-PCG to 1e-10."""
     from cie_b200.fem import make_poisson
     from cie_b200.linalg import Statistics
     prob = make_poisson(space, 2, 1, [256, 256], seed=0, kappa="one")
     rp, col, val = prob.host_csr()
     b = host(prob.rhs)
-    x, st = solve_gpu(space, prob.matrix, b, Statistics(5000, 0.0, 1e-10))
+    x, st = solve_gpu(space, prob.matrix, b, Statistics(5000, 0.0, 1e-10), loop=loop)
     xr, sr, err, secs = reference.pcg(rp, col, val, b, maxit=5000, abstol=0.0, reltol=1e-10)
     assert err is None
     rel = np.linalg.norm(x - xr) / np.linalg.norm(xr)
@@ -57,22 +66,24 @@ def test_pcg_cfg1_vs_reference(space, reference):
     assert true_residual(rp, col, val, x, b) <= 2e-10
 
 
-def test_pcg_3d_lognormal_vs_reference(space, reference):
+@pytest.mark.parametrize("loop", LOOPS)
+def test_pcg_3d_lognormal_vs_reference(space, reference, loop):
     """3D Q1, 32^3 cells with the smoothed log-normal kappa field."""
     from cie_b200.fem import make_poisson
     from cie_b200.linalg import Statistics
     prob = make_poisson(space, 3, 1, [32, 32, 32], seed=3)
     rp, col, val = prob.host_csr()
     b = host(prob.rhs)
-    x, st = solve_gpu(space, prob.matrix, b, Statistics(5000, 0.0, 1e-10))
+    x, st = solve_gpu(space, prob.matrix, b, Statistics(5000, 0.0, 1e-10), loop=loop)
     xr, sr, err, _ = reference.pcg(rp, col, val, b, maxit=5000, abstol=0.0, reltol=1e-10)
     rel = np.linalg.norm(x - xr) / np.linalg.norm(xr)
     print("3D lognormal: GPU %d it, reference %d it, rel diff %.3e" % (st.iterationCount, sr[0], rel))
     assert abs(st.iterationCount - sr[0]) <= 2 and rel <= 1e-9
 
 
+@pytest.mark.parametrize("loop", LOOPS)
 @pytest.mark.parametrize("case", ["unpreconditioned", "maxit", "abstol", "maxit0", "guess", "scales", "scales2"])
-def test_pcg_settings_vs_reference(space, reference, case):
+def test_pcg_settings_vs_reference(space, reference, case, loop):
     from cie_b200.linalg import Statistics
     rp, col, val = poisson2d(30)
     n = len(rp) - 1
@@ -91,7 +102,7 @@ def test_pcg_settings_vs_reference(space, reference, case):
         kw["maxit"] = 0
     m = matrix(rp, col, val, n)
     settings = Statistics(kw["maxit"], kw["abstol"], kw["reltol"])
-    x, st = solve_gpu(space, m, b, settings, precond=kw["precondition"], x0=x0)
+    x, st = solve_gpu(space, m, b, settings, precond=kw["precondition"], x0=x0, loop=loop)
     xr, sr, err, _ = reference.pcg(rp, col, val, b, x0=x0, **kw)
     assert err is None
     assert abs(st.iterationCount - sr[0]) <= 1
@@ -101,23 +112,28 @@ def test_pcg_settings_vs_reference(space, reference, case):
     if case in ("scales", "scales2"):
         si, so = (1.0, -2.0) if case == "scales" else (0.5, 3.0)
         y0 = rng.uniform(-1, 1, n)
-        y, _ = solve_gpu(space, m, b, settings, x0=y0, si=si, so=so)
+        y, _ = solve_gpu(space, m, b, settings, x0=y0, si=si, so=so, loop=loop)
         xr2, _, _, _ = reference.pcg(rp, col, val, b, x0=y0, **kw)
         assert np.allclose(y, si * y0 + so * xr2, rtol=1e-9, atol=1e-11)
 
 
-def test_pcg_breakdown_raises(space):
+@pytest.mark.parametrize("loop", LOOPS)
+def test_pcg_breakdown_raises(space, loop):
     from cie_b200.linalg import Statistics
     from cie_b200._lib import CiecuError
     m = matrix([0, 1, 2], [0, 1], [1.0, -1.0], 2)
     with pytest.raises(CiecuError, match=r"p\^T @ A @ p vanished in iteration 0"):
-        solve_gpu(space, m, np.array([0.0, 1.0]), Statistics(100, 0.0, 1e-10), precond=False)
+        solve_gpu(space, m, np.array([0.0, 1.0]), Statistics(100, 0.0, 1e-10), precond=False, loop=loop)
+    # indefinite: diag(1, 2, 3, -4) with b = 1 breaks down in a later iteration
+    m = matrix([0, 1, 2, 3, 4], [0, 1, 2, 3], [1.0, 2.0, 3.0, -4.0], 4)
+    with pytest.raises(CiecuError, match=r"p\^T @ A @ p vanished in iteration"):
+        solve_gpu(space, m, np.ones(4), Statistics(100, 0.0, 1e-10), precond=False, loop=loop)
     # zero right-hand side with no absolute tolerance: r^T z = 0 like the reference
     rp, col, val = poisson2d(5)
     with pytest.raises(CiecuError, match="vanished in iteration 0"):
-        solve_gpu(space, matrix(rp, col, val, 25), np.zeros(25), Statistics(100, 0.0, 1e-10))
+        solve_gpu(space, matrix(rp, col, val, 25), np.zeros(25), Statistics(100, 0.0, 1e-10), loop=loop)
     # ... and an early exit with an absolute tolerance
-    x, st = solve_gpu(space, matrix(rp, col, val, 25), np.zeros(25), Statistics(100, 1e-12, 1e-10))
+    x, st = solve_gpu(space, matrix(rp, col, val, 25), np.zeros(25), Statistics(100, 1e-12, 1e-10), loop=loop)
     assert st.iterationCount == 0 and np.all(x == 0)
 
 
