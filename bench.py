@@ -191,11 +191,14 @@ def main():
     ap.add_argument("--pin", default=None,
                     help="with --profile: FP64-solver,mixed-unroll,CSR schedules to use instead of autotuning "
                          "(the choices a bench run without the profiler reports), e.g. 4,1,4")
-    ap.add_argument("--profile-target", default="pcg", choices=["pcg", "batch", "spmm", "embedded", "gradient"],
+    ap.add_argument("--profile-target", default="pcg",
+                    choices=["pcg", "batch", "spmm", "embedded", "cut", "gradient"],
                     help="with --profile: the solver the ncu target runs (pcg: the headline solves; batch: a "
                          "batched solve of 128 Q2 systems; spmm: a 32-RHS solve on the Q1 grid of --profile-cells; "
-                         "embedded: the finite-cell Q3 assembly on 16^3 cells; gradient: one adjoint gradient on "
-                         "the Q1 grid of --profile-cells)")
+                         "embedded: the finite-cell Q3 assembly on 16^3 cells; cut: 30 FP64 Jacobi-PCG iterations "
+                         "on that finite-cell system, on --profile-cells^3 cells when that is at most 24 "
+                         "(--pin's first value pins the SpMV schedule); gradient: one "
+                         "adjoint gradient on the Q1 grid of --profile-cells)")
     ap.add_argument("--profile-cells", type=int, default=PROFILE_CELLS[0],
                     help="cells per axis of the --profile case (96: 290 MB matrix; 128: the full workload)")
     args = ap.parse_args()
@@ -224,7 +227,8 @@ def main():
 
     space = CUDASpace()
     if args.profile and args.profile_target != "pcg":
-        profile_target(space, args.profile_target, args.profile_cells)
+        profile_target(space, args.profile_target, args.profile_cells,
+                       int(args.pin.split(",")[0]) if args.pin else 0)
         return
     cells = [args.profile_cells] * 3 if args.profile else WORKLOAD["cells"]
     prob = make_poisson(space, 3, 1, cells, seed=WORKLOAD["seed"])
@@ -443,13 +447,13 @@ def main():
         dist.destroy_process_group()
 
 
-def profile_target(space, target, cells):
+def profile_target(space, target, cells, schedule=0):
     """Short runs of the other solvers for ncu (inputs built first, one solve or
     assembly, no timing)."""
     import torch
     from cie_b200.fem import kappa_field, make_embedded_poisson, make_poisson, random_uniform
-    from cie_b200.linalg import (BatchedConjugateGradients, CSROperator, MultiRHSConjugateGradients, Statistics,
-                                 block_diagonal, makeDiagonalOperator)
+    from cie_b200.linalg import (BatchedConjugateGradients, ConjugateGradients, CSROperator,
+                                 MultiRHSConjugateGradients, Statistics, block_diagonal, makeDiagonalOperator)
     tight = Statistics(20000, 0.0, 1e-10)
     if target == "batch":
         rng = np.random.default_rng(0)
@@ -474,6 +478,18 @@ def profile_target(space, target, cells):
     elif target == "embedded":
         prob = make_embedded_poisson(space, 3, 3, [16, 16, 16], radius=0.4, alpha=1e-6, depth=2)
         info = {"cut_cells": prob.cut_cells}
+    elif target == "cut":
+        c = cells if cells <= 24 else 16
+        prob = make_embedded_poisson(space, 3, 3, [c, c, c], radius=0.4, alpha=1e-6, depth=2)
+        A = CSROperator(prob.matrix, space)
+        cg = ConjugateGradients(A, space, makeDiagonalOperator(prob.matrix, space, csr_handle=A.csr),
+                                Statistics(30, 0.0, 1e-10))
+        cg.set_loop(1)
+        if schedule:
+            cg.set_schedule(schedule)
+        x = torch.zeros_like(prob.rhs)
+        cg.product(0.0, prob.rhs, 1.0, x)
+        info = dict(cg.info(), nnz=prob.matrix.nnz(), dofs=prob.rhs.numel())
     else:
         from cie_b200.adjoint import DifferentiablePoisson
         prob = DifferentiablePoisson(space, 3, 1, [cells] * 3, settings=tight)
