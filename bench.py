@@ -338,13 +338,22 @@ def main():
     t_mixed, t_fp64, t_spmv32, t_spmv64 = max_over_ranks([t_mixed, t_fp64, t_spmv32, t_spmv64])
     info = mixed.info()
 
-    idx_bytes = 2 if info["compressed_columns"] else 4
-    # FP32 SELL-32 SpMV: values + column offsets of the nonzeros, x read, y written
-    # (padding entries and the per-slice descriptors are reported, not counted)
-    spmv32_bytes = (4 + idx_bytes) * nnz + 8 * n
+    ndiag = A.csr.diagonals()
+    dia32 = info.get("format") == "dia"
+    dia64 = cg.info().get("spmv_schedule") == 64
+    idx_bytes = 2 if info.get("compressed_columns") else 4
+    if dia32:
+        # FP32 DIA SpMV: the stored diagonals (nonzeros and the zeros that pad the
+        # diagonals), x read, y written; no column indices
+        spmv32_bytes = 4 * ndiag * n + 8 * n
+        inner_bytes = 4 * ndiag * n + 52 * n
+    else:
+        # FP32 SELL-32 SpMV: values + column offsets of the nonzeros, x read, y written
+        # (padding entries and the per-slice descriptors are reported, not counted)
+        spmv32_bytes = (4 + idx_bytes) * nnz + 8 * n
+        inner_bytes = (4 + idx_bytes) * nnz + 52 * n
     spmv64_bytes = 12 * nnz + 4 * (n + 1) + 16 * n
-    iter64_bytes = 12 * nnz + 4 * (n + 1) + 104 * n
-    inner_bytes = (4 + idx_bytes) * nnz + 52 * n
+    iter64_bytes = (8 * ndiag * n if dia64 else 12 * nnz + 4 * (n + 1)) + 104 * n
     fp64_solve_bytes = (it64 + 1) * iter64_bytes + (12 * nnz + 4 * (n + 1) + 24 * n)
     refine_bytes = 12 * nnz + 4 * (n + 1) + 28 * n  # FP64 residual pass: x64, b read, r32 written, dinv32
     mixed_solve_bytes = mst.innerIterations * inner_bytes + (mst.refinements + 1) * refine_bytes
@@ -353,7 +362,9 @@ def main():
     tpath = os.path.join(ROOT, "profiles", "dram_traffic_poisson3d_q1_128.txt")
     if os.path.exists(tpath) and cells == [128, 128, 128]:
         figures = dict(line.split() for line in open(tpath) if line.strip() and not line.startswith("#"))
-        if info["compressed_columns"] and info["group_unroll"] > 0:
+        if dia32:
+            traffic = int(figures.get("mixed_apply_dia_kernel_f32", 0)) or None
+        elif info["compressed_columns"] and info["group_unroll"] > 0:
             traffic = int(figures.get("mixed_apply_kernel_f32_sell16", 0)) or None
         traffic64 = int(figures.get("spmv_kernel_f64_csr", 0)) or None
 
@@ -409,7 +420,7 @@ def main():
             "data": "synthetic (seeded mt19937_64 RHS and kappa field)",
             "config": dict(WORKLOAD, parallelism="replicas" if world > 1 else "single_gpu",
                            solver="mixed-precision jacobi-pcg, reliable updates delta=%g" % DELTA,
-                           compressed_columns=info["compressed_columns"]),
+                           inner_format=info["format"], fp64_k1="dia" if dia64 else "csr"),
             "mixed": {"seconds": t_mixed, "inner_iterations": mst.innerIterations,
                       "refinements": mst.refinements, "true_relative_residual": rel_mixed,
                       "rel_diff_vs_fp64_solution": agree,
@@ -419,11 +430,13 @@ def main():
                      "achieved_gbs": fp64_solve_bytes / t_fp64 / 1e9,
                      "us_per_iteration": 1e6 * t_fp64 / (it64 + 1)},
             "speedup_mixed_vs_fp64": t_fp64 / t_mixed,
-            "roofline": {"bound": "hbm", "kernel": "%s (FP32 SELL-32 SpMV, %s columns, %d stored "
-                         "entries for %d nonzeros)" % (
-                             "mixed_apply_kernel<%d>" % info["group_unroll"] if info["group_unroll"] > 0
-                             else "mixed_apply_tma_kernel", "16-bit" if info["compressed_columns"] else "int32",
-                             info["padded_entries"], nnz),
+            "roofline": {"bound": "hbm", "kernel": (
+                             "mixed_apply_dia_kernel (FP32 DIA SpMV, %d diagonals, %d stored entries for %d "
+                             "nonzeros)" % (ndiag, ndiag * n, nnz)) if dia32 else (
+                             "%s (FP32 SELL-32 SpMV, %s columns, %d stored entries for %d nonzeros)" % (
+                                 "mixed_apply_kernel<%d>" % info["group_unroll"] if info["group_unroll"] > 0
+                                 else "mixed_apply_tma_kernel", "16-bit" if info["compressed_columns"] else "int32",
+                                 info["padded_entries"], nnz)),
                          "achieved": g32, "peak": hbm, "unit": "GB/s", "frac": g32 / hbm, "peak_kind": peak_kind,
                          "traffic": traffic, "algorithmic_bytes": spmv32_bytes, "launch_ms": 1e3 * t_spmv32},
             "fp64_spmv_roofline": {"kernel": "spmv_kernel (FP64 CSR, schedule %d)" % A.csr.kernel(),

@@ -64,6 +64,7 @@ SIGNATURES = {
     "ciecu_csr_destroy": (c_int, [P]),
     "ciecu_csr_set_kernel": (c_int, [P, c_int]),
     "ciecu_csr_get_kernel": (c_int, [P, P]),
+    "ciecu_csr_diagonals": (c_int, [P, P]),
     "ciecu_csr_autotune": (c_int, [P]),
     "ciecu_csr_spmv_f64": (c_int, [P, c_double, P, c_double, P]),
     "ciecu_csr_spmv_f32": (c_int, [P, c_float, P, c_float, P]),

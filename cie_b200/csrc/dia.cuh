@@ -1,0 +1,115 @@
+// Diagonal (DIA) storage of a CSR matrix whose nonzeros lie on few diagonals:
+// the Q1 stiffness matrices of structured grids (9 diagonals in 2D, 27 in 3D,
+// lexicographic node order).  Entry (r, c) with c - r = off[d] is stored at
+// val[d * ld + r]; entries of a diagonal that are not in the CSR pattern are
+// zero.  No column indices are stored, so a row pass reads 8 (FP64) or 4 (FP32)
+// bytes per stored entry instead of 12 or 6, and the gathers x[r + off[d]] of
+// consecutive rows are consecutive addresses.
+//
+// Row sums run over the diagonals in ascending offset order, i.e. in the
+// column order of the CSR row, one FMA per diagonal (a padded zero adds
+// nothing), so they equal the sequential CSR-order FMA sums of
+// CSROperator.cpp:49-56 up to the sign of zero.
+//
+// The CSR view stays the source of truth: the offsets are found once per CSR
+// handle (the pattern is fixed for its lifetime, as the row-block schedule
+// already assumes), and solvers refill the values from the CSR arrays.
+#pragma once
+
+#include "spmv.cuh"
+
+#include <vector>
+
+namespace ciecu {
+
+constexpr int kMaxDiagonals = 32;
+
+template <typename V>
+struct DiaArgs {
+    int nrows;
+    int ndiag;
+    long ld;  // stride between diagonals (rows rounded up to a multiple of 32)
+    const V* __restrict__ val;
+    int off[kMaxDiagonals];  // ascending
+};
+
+// One thread per row (grid-stride); epilogue interface of the CSR engines.
+template <typename T, typename V, typename Op>
+__device__ __forceinline__ void dia_rows(const DiaArgs<V>& A, const T* __restrict__ x, Op& op) {
+    const long stride = static_cast<long>(gridDim.x) * blockDim.x;
+    for (long rl = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; rl < A.nrows; rl += stride) {
+        const int r = static_cast<int>(rl);
+        const auto pre = op.pre(r);
+        T sum = T(0);
+#pragma unroll 9
+        for (int d = 0; d < A.ndiag; ++d) {
+            const int c = r + A.off[d];
+            const V v = stream_ld(A.val + static_cast<long>(d) * A.ld + r);
+            const T xv = static_cast<unsigned>(c) < static_cast<unsigned>(A.nrows) ? __ldg(x + c) : T(0);
+            sum = fma(static_cast<T>(v), xv, sum);
+        }
+        op.post(r, pre, sum);
+    }
+}
+
+// Four consecutive rows per thread with 16-byte loads of each diagonal (FP32:
+// a warp reads 512 contiguous bytes per diagonal instead of 128).  Rows past
+// nrows (up to ld, zero-filled) are computed and dropped; the gathers of x stay
+// inside [0, nrows).
+template <typename Op>
+__device__ __forceinline__ void dia_rows4(const DiaArgs<float>& A, const float* __restrict__ x, Op& op) {
+    const long stride = static_cast<long>(gridDim.x) * blockDim.x * 4;
+    for (long r0 = (static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x) * 4; r0 < A.nrows; r0 += stride) {
+        const int r = static_cast<int>(r0);
+        typename Op::Pre pre[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            if (r + i < A.nrows) pre[i] = op.pre(r + i);
+        float sum[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll 9
+        for (int d = 0; d < A.ndiag; ++d) {
+            const float4 v = __ldcs(reinterpret_cast<const float4*>(A.val + static_cast<long>(d) * A.ld + r));
+            const int c = r + A.off[d];
+            float xv[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+                xv[i] = static_cast<unsigned>(c + i) < static_cast<unsigned>(A.nrows) ? __ldg(x + c + i) : 0.f;
+            sum[0] = fmaf(v.x, xv[0], sum[0]);
+            sum[1] = fmaf(v.y, xv[1], sum[1]);
+            sum[2] = fmaf(v.z, xv[2], sum[2]);
+            sum[3] = fmaf(v.w, xv[3], sum[3]);
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            if (r + i < A.nrows) op.post(r + i, pre[i], sum[i]);
+    }
+}
+
+// Distinct diagonal offsets of a square CSR matrix, ascending, cached in the
+// handle.  Empty when there are more than kMaxDiagonals or when DIA storage would
+// hold less than 60 % nonzeros.
+int dia_offsets(ciecu_csr_s* csr, const std::vector<int>** out);
+
+// Diagonal stride for n rows.
+inline long dia_ld(long n) { return ((n + 31) / 32) * 32; }
+
+// Shape of the DIA copy of csr (values pointer left null).
+template <typename V>
+DiaArgs<V> dia_shape(const ciecu_csr_s* csr, const std::vector<int>& offsets) {
+    DiaArgs<V> a{};
+    a.nrows = csr->rows;
+    a.ndiag = static_cast<int>(offsets.size());
+    a.ld = dia_ld(csr->rows);
+    a.val = nullptr;
+    for (int d = 0; d < a.ndiag; ++d) a.off[d] = offsets[static_cast<size_t>(d)];
+    return a;
+}
+
+// Writes the CSR values of csr into the DIA array `out` of shape `a` (entries of
+// the pattern only; the caller zero-fills `out` once).  With sdiag, entry (r, c)
+// is scaled by sdiag[r] * sdiag[c] (the symmetric Jacobi scaling of the mixed
+// solver's inner matrix) before the conversion to V.
+int dia_fill_f64(const ciecu_csr_s* csr, const DiaArgs<double>& a, double* out, cudaStream_t st);
+int dia_fill_f32(const ciecu_csr_s* csr, const DiaArgs<float>& a, float* out, const double* sdiag, cudaStream_t st);
+
+}  // namespace ciecu

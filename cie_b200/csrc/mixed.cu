@@ -33,6 +33,7 @@
 #include "graph.cuh"
 #include "pcg.cuh"
 #include "sell.cuh"
+#include "dia.cuh"
 #include "sell_tma.cuh"
 
 #include <string>
@@ -42,6 +43,7 @@ namespace ciecu {
 namespace {
 
 constexpr int kT = 256;
+constexpr int kDiaInner = -2;  // innerKernel / unroll code of the DIA inner kernels
 
 struct MixedScalars {
     double rz, pq, alpha, beta, rzPending;
@@ -173,6 +175,35 @@ __global__ void __launch_bounds__(kT) mixed_spmv_kernel(SellArgs<float, CI> A, c
     }
     MixedPqOp op{p, q, 0.0};
     sell_rows<U, float, float, CI>(A, p, op);
+    double mine[1] = {op.acc}, tot[1];
+    if (grid_reduce_last<1, kT>(mine, partials, counter, tot) && threadIdx.x == 0) {
+        s->pq = tot[0];
+        if (!(0.0 < tot[0])) {
+            if (inner_breakdown(s)) set_cond<COND>(loop, 0);
+        } else {
+            s->alpha = s->rz / tot[0];
+        }
+    }
+}
+
+// DIA variants of the two kernels above, for inner matrices of at most 32
+// diagonals (dia.cuh): FP32 values only, no column indices.
+__global__ void __launch_bounds__(kT) mixed_apply_dia_kernel(DiaArgs<float> A, const float* __restrict__ x,
+                                                            float* __restrict__ y) {
+    StoreOp op{y};
+    dia_rows4(A, x, op);
+}
+
+template <bool COND>
+__global__ void __launch_bounds__(kT) mixed_spmv_dia_kernel(DiaArgs<float> A, const float* __restrict__ p,
+                                                           float* __restrict__ q, MixedScalars* s, double* partials,
+                                                           unsigned* counter, cudaGraphConditionalHandle loop) {
+    if (*reinterpret_cast<volatile int*>(&s->done)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) set_cond<COND>(loop, 0);
+        return;
+    }
+    MixedPqOp op{p, q, 0.0};
+    dia_rows4(A, p, op);
     double mine[1] = {op.acc}, tot[1];
     if (grid_reduce_last<1, kT>(mine, partials, counter, tot) && threadIdx.x == 0) {
         s->pq = tot[0];
@@ -480,7 +511,10 @@ struct ciecu_mixed_s {
     ciecu_mixed_options options{};
     long n = 0;
     bool idx16 = false;
-    int unroll = 2;  // SELL groups of four entries in flight per thread (autotuned; 0 = TMA pipeline)
+    int unroll = 2;  // SELL groups of four entries in flight per thread (autotuned; 0 = TMA pipeline,
+                     // kDiaInner = the DIA copy)
+    float* dia32 = nullptr;  // DIA copy of the inner matrix (few-diagonal matrices only)
+    ciecu::DiaArgs<float> dia{};
     // SELL-32 inner matrix
     int nslices = 0;
     long long paddedEntries = 0;
@@ -520,10 +554,17 @@ int with_unroll(int u, F&& f) {
     }
 }
 
-// M1 with the autotuned variant: TMA pipeline (unroll == 0) or U register groups.
+// M1 with the autotuned variant: TMA pipeline (unroll == 0), the DIA copy
+// (unroll == kDiaInner) or U register groups.
 template <bool COND>
 int launch_inner_spmv(ciecu_mixed_s* M, cudaStream_t st, cudaGraphConditionalHandle loop) {
     const long needA = (M->n + kT - 1) / kT;
+    if (M->unroll == kDiaInner) {
+        mixed_spmv_dia_kernel<COND><<<fit_grid(mixed_spmv_dia_kernel<COND>, kT, (needA + 3) / 4), kT, 0, st>>>(
+            M->dia, M->p32, M->q32, M->d_s, M->d_partials, M->d_counter, loop);
+        CIECU_CHECK_LAUNCH("mixed_spmv_dia_kernel");
+        return CIECU_OK;
+    }
     if (M->unroll == 0) {
         if (M->idx16) {
             constexpr int smem = TmaShape<float, short>::SMEM;
@@ -643,8 +684,8 @@ int ciecu_mixed_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_sta
     CIECU_REQUIRE(options.scaleInner == 0 || options.scaleInner == 1, "mixed_create: scaleInner must be 0 or 1");
     CIECU_REQUIRE(options.delta > 0.0 && options.delta < 1.0, "mixed_create: delta must be in (0, 1)");
     CIECU_REQUIRE(options.innerKernel == 0 || options.innerKernel == 1 || options.innerKernel == 2 ||
-                      options.innerKernel == 4 || options.innerKernel == -1,
-                  "mixed_create: innerKernel must be 0 (autotune), 1, 2, 4 or -1 (TMA pipeline)");
+                      options.innerKernel == 4 || options.innerKernel == -1 || options.innerKernel == kDiaInner,
+                  "mixed_create: innerKernel must be 0 (autotune), 1, 2, 4, -1 (TMA pipeline) or -2 (DIA copy)");
     CIECU_TRY(ensure_tuned(lhs));
     auto* M = new ciecu_mixed_s();
     M->A = lhs;
@@ -760,6 +801,33 @@ int ciecu_mixed_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_sta
             return cuda_fail(e, "mixed_create: int32 columns");
         }
     }
+    // DIA copy of the inner matrix when its nonzeros lie on few diagonals.
+    if (M->n > 0 && (options.innerKernel == 0 || options.innerKernel == kDiaInner)) {
+        const std::vector<int>* offsets = nullptr;
+        int status = dia_offsets(lhs, &offsets);
+        if (status == CIECU_OK && !offsets->empty()) {
+            DiaArgs<float> a = dia_shape<float>(lhs, *offsets);
+            const size_t bytes = sizeof(float) * static_cast<size_t>(a.ndiag) * static_cast<size_t>(a.ld);
+            if (cudaMalloc(&M->dia32, bytes) == cudaSuccess) {
+                e = cudaMemsetAsync(M->dia32, 0, bytes, st);
+                a.val = M->dia32;
+                M->dia = a;
+                if (e == cudaSuccess) status = dia_fill_f32(lhs, M->dia, M->dia32, M->sdiag, st);
+                if (e != cudaSuccess) status = cuda_fail(e, "mixed_create: DIA copy");
+            } else {
+                cudaGetLastError();  // no room for the copy: the SELL kernels stay
+                M->dia32 = nullptr;
+            }
+        }
+        if (status != CIECU_OK) {
+            ciecu_mixed_destroy(M);
+            return status;
+        }
+        if (options.innerKernel == kDiaInner && !M->dia32) {
+            ciecu_mixed_destroy(M);
+            return fail(CIECU_ERR_ARGUMENT, "mixed_create: innerKernel -2 needs a matrix of at most 32 diagonals");
+        }
+    }
     M->a16 = SellArgs<float, short>{static_cast<int>(M->n), M->sliceLen, M->sliceStart, M->rowLen, M->val32,
                                     static_cast<const short*>(M->col32or16)};
     M->a32 = SellArgs<float, int>{static_cast<int>(M->n), M->sliceLen, M->sliceStart, M->rowLen, M->val32,
@@ -779,7 +847,8 @@ int ciecu_mixed_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_sta
     // Autotune the group unroll of the inner SpMV on the solver's own matrix,
     // timing the fused kernel the iteration runs (q = A32 p with the p^T q
     // reduction) on scratch vectors p32 = 0 -> q32.
-    if (options.innerKernel != 0) M->unroll = options.innerKernel < 0 ? 0 : options.innerKernel;
+    if (options.innerKernel != 0)
+        M->unroll = options.innerKernel == kDiaInner ? kDiaInner : (options.innerKernel < 0 ? 0 : options.innerKernel);
     if (M->n > 0 && options.innerKernel == 0) {
         // p = D^-1 > 0: p^T A p > 0 for an SPD matrix, so no timed launch trips the
         // breakdown flag (which would make the later candidates return at once).
@@ -793,8 +862,9 @@ int ciecu_mixed_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_sta
         if (e == cudaSuccess) e = cudaEventCreate(&e1);
         float best = 1e30f, bestTma = 1e30f;
         int bestU = 2;
-        for (int u : {1, 2, 4, 0}) {
+        for (int u : {1, 2, 4, 0, kDiaInner}) {
             if (e != cudaSuccess) break;
+            if (u == kDiaInner && !M->dia32) continue;
             M->unroll = u;
             auto launch = [&]() { launch_inner_spmv<false>(M, st, 0); };
             for (int rep = 0; rep < 2; ++rep) launch();
@@ -840,6 +910,7 @@ int ciecu_mixed_destroy(ciecu_mixed M) {
     cudaFree(M->rowLen);
     cudaFree(M->val32);
     cudaFree(M->col32or16);
+    cudaFree(M->dia32);
     cudaFree(M->dinv32);
     cudaFree(M->sdiag);
     cudaFree(M->x32);
@@ -875,6 +946,13 @@ int ciecu_mixed_apply_f32(ciecu_mixed M, const float* d_in, float* d_out) {
     if (M->n == 0) return CIECU_OK;
     cudaStream_t st = M->A->space->stream;
     const long need = (M->n + kT - 1) / kT;
+    if (M->unroll == kDiaInner) {
+        mixed_apply_dia_kernel<<<fit_grid(mixed_apply_dia_kernel, kT, (need + 3) / 4), kT, 0, st>>>(M->dia, d_in,
+                                                                                                 d_out);
+        count_launch();
+        CIECU_CHECK_LAUNCH("mixed_apply_dia_kernel");
+        return CIECU_OK;
+    }
     if (M->unroll == 0) {
         if (M->idx16) {
             constexpr int smem = TmaShape<float, short>::SMEM;

@@ -12,6 +12,7 @@
 // Every kernel returns at once when the done flag is set, so a CUDA graph of a
 // fixed number of iterations can be replayed until the host sees the flag.
 #include "graph.cuh"
+#include "dia.cuh"
 #include "pcg.cuh"
 
 #include <string>
@@ -97,6 +98,33 @@ __global__ void __launch_bounds__(csr_threads<KERNEL>())
     csr_rows<KERNEL, double, double, false>(A, p, op);
     double mine[1] = {op.acc}, tot[1];
     if (grid_reduce_last<1, T>(mine, partials, counter, tot) && threadIdx.x == 0) {
+        s->pq = tot[0];
+        if (!(0.0 < tot[0])) {
+            s->done = 3;
+            s->error = CIECU_ERR_BREAKDOWN;
+            s->errorKind = 2;
+            s->errorIter = s->iter;
+            set_loop<COND>(cond, 0);
+        } else {
+            s->alpha = s->rz / tot[0];
+        }
+    }
+}
+
+// K1 over the DIA copy of a few-diagonal matrix (dia.cuh): no column indices,
+// 8 bytes per stored entry.
+template <bool COND>
+__global__ void __launch_bounds__(kT) pcg_spmv_dia_kernel(DiaArgs<double> A, const double* __restrict__ p,
+                                                         double* __restrict__ q, PcgScalars* s, double* partials,
+                                                         unsigned* counter, cudaGraphConditionalHandle cond) {
+    if (*reinterpret_cast<volatile int*>(&s->done)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) set_loop<COND>(cond, 0);
+        return;
+    }
+    PqOp op{p, q, 0.0};
+    dia_rows<double, double>(A, p, op);
+    double mine[1] = {op.acc}, tot[1];
+    if (grid_reduce_last<1, kT>(mine, partials, counter, tot) && threadIdx.x == 0) {
         s->pq = tot[0];
         if (!(0.0 < tot[0])) {
             s->done = 3;
@@ -544,6 +572,11 @@ struct ciecu_pcg_s {
     bool deviceLoop = false;  // graph = WHILE loop (else `chunk` unrolled iterations)
     int kernel = 0;           // K1 schedule, autotuned on the fused SpMV kernel itself
     int chunk = 16;
+    // DIA copy of a few-diagonal matrix (K1 schedule kDiaSchedule), refilled from
+    // the CSR values at every solve.
+    bool diaChecked = false;
+    double* diaBuf = nullptr;
+    ciecu::DiaArgs<double> dia{};
     // Single-launch solve (allocated at its first use).
     int loopMode = 0;     // 0 auto (single launch when the system fits in L2), 1 graph, 2 single launch
     bool persistent = false;  // the last solve ran as a single launch
@@ -562,18 +595,58 @@ struct ciecu_pcg_s {
 namespace ciecu {
 namespace {
 
+// K1 schedules: 1 (row-block stream kernel), 2..32 (lanes per row) and
+// kDiaSchedule (the DIA copy).
+constexpr int kDiaSchedule = 64;
+
 template <bool COND>
-int launch_iteration(ciecu_pcg_s* S, cudaStream_t st, cudaGraphConditionalHandle cond) {
+int launch_k1(ciecu_pcg_s* S, cudaStream_t st, int schedule, cudaGraphConditionalHandle cond) {
     ciecu_csr_s* A = S->A;
-    const int needA = csr_grid(A, S->kernel);
-    const long needV = ((S->n + 1) / 2 + kT - 1) / kT;
-    const bool pre = S->dinv != nullptr;
-    CIECU_TRY(with_schedule(S->kernel, [&](auto k) -> int {
+    if (schedule == kDiaSchedule) {
+        if (!S->diaBuf) return fail(CIECU_ERR_ARGUMENT, "pcg: the DIA schedule needs a matrix of at most 32 diagonals");
+        pcg_spmv_dia_kernel<COND><<<fit_grid(pcg_spmv_dia_kernel<COND>, kT, (S->n + kT - 1) / kT), kT, 0, st>>>(
+            S->dia, S->p, S->q, S->d_s, S->d_partials, S->d_counter, cond);
+        return CIECU_OK;
+    }
+    const int needA = csr_grid(A, schedule);
+    return with_schedule(schedule, [&](auto k) -> int {
         constexpr int K = decltype(k)::value;
         pcg_spmv_kernel<K, COND><<<fit_grid(pcg_spmv_kernel<K, COND>, csr_threads<K>(), needA), csr_threads<K>(), 0,
                                    st>>>(A->args<double>(), S->p, S->q, S->d_s, S->d_partials, S->d_counter, cond);
         return CIECU_OK;
-    }));
+    });
+}
+
+// Finds the diagonals once per solver and refills the DIA copy from the CSR
+// values (which the caller may have changed since the last solve).
+int refresh_dia(ciecu_pcg_s* S, cudaStream_t st) {
+    if (!S->diaChecked) {
+        S->diaChecked = true;
+        const std::vector<int>* offsets = nullptr;
+        CIECU_TRY(dia_offsets(S->A, &offsets));
+        if (!offsets->empty()) {
+            DiaArgs<double> a = dia_shape<double>(S->A, *offsets);
+            const size_t bytes = sizeof(double) * static_cast<size_t>(a.ndiag) * static_cast<size_t>(a.ld);
+            double* buf = nullptr;
+            if (cudaMalloc(&buf, bytes) != cudaSuccess) {
+                cudaGetLastError();  // no room for the copy: the CSR schedules stay
+                return CIECU_OK;
+            }
+            CIECU_CUDA(cudaMemsetAsync(buf, 0, bytes, st));
+            a.val = buf;
+            S->dia = a;
+            S->diaBuf = buf;
+        }
+    }
+    if (S->diaBuf) CIECU_TRY(dia_fill_f64(S->A, S->dia, S->diaBuf, st));
+    return CIECU_OK;
+}
+
+template <bool COND>
+int launch_iteration(ciecu_pcg_s* S, cudaStream_t st, cudaGraphConditionalHandle cond) {
+    const long needV = ((S->n + 1) / 2 + kT - 1) / kT;
+    const bool pre = S->dinv != nullptr;
+    CIECU_TRY(launch_k1<COND>(S, st, S->kernel, cond));
     if (pre) {
         pcg_update_kernel<true, COND><<<fit_grid(pcg_update_kernel<true, COND>, kT, needV), kT, 0, st>>>(
             S->n, S->x, S->r, S->p, S->q, S->dinv, S->d_s, S->d_partials, S->d_counter, cond);
@@ -742,17 +815,10 @@ int tune_solver_spmv(ciecu_pcg_s* S) {
     float best = 1e30f;
     int bestK = A->kernel;
     cudaError_t e = cudaSuccess;
-    for (int k : {1, 2, 4, 8, 16, 32}) {
-        if (k >= 16 && A->avgRow < k) continue;
-        auto launch = [&]() {
-            with_schedule(k, [&](auto kk) -> int {
-                constexpr int K = decltype(kk)::value;
-                pcg_spmv_kernel<K, false><<<fit_grid(pcg_spmv_kernel<K, false>, csr_threads<K>(), csr_grid(A, k)),
-                                            csr_threads<K>(), 0, st>>>(A->args<double>(), S->p, S->q, S->d_s,
-                                                                       S->d_partials, S->d_counter, 0);
-                return CIECU_OK;
-            });
-        };
+    for (int k : {1, 2, 4, 8, 16, 32, kDiaSchedule}) {
+        if (k >= 16 && k <= 32 && A->avgRow < k) continue;
+        if (k == kDiaSchedule && !S->diaBuf) continue;
+        auto launch = [&]() { launch_k1<false>(S, st, k, 0); };
         for (int rep = 0; rep < 2; ++rep) launch();
         for (int trial = 0; trial < 3 && e == cudaSuccess; ++trial) {  // best of three: robust to noise
             cudaEventRecord(e0, st);
@@ -873,6 +939,7 @@ int ciecu_pcg_destroy(ciecu_pcg S) {
     if (S->h_s) cudaFreeHost(S->h_s);
     cudaFree(S->d_partials);
     cudaFree(S->d_counter);
+    cudaFree(S->diaBuf);
     cudaFree(S->z);
     cudaFree(S->p2);
     cudaFree(S->slots);
@@ -909,8 +976,8 @@ int ciecu_pcg_set_graph_chunk(ciecu_pcg S, int iterations) {
 int ciecu_pcg_set_schedule(ciecu_pcg S, int schedule) {
     CIECU_REQUIRE(S, "pcg_set_schedule: null solver");
     CIECU_REQUIRE(schedule == 0 || schedule == 1 || schedule == 2 || schedule == 4 || schedule == 8 ||
-                      schedule == 16 || schedule == 32,
-                  "pcg_set_schedule: schedule must be 0 (autotune), 1, 2, 4, 8, 16 or 32");
+                      schedule == 16 || schedule == 32 || schedule == kDiaSchedule,
+                  "pcg_set_schedule: schedule must be 0 (autotune), 1, 2, 4, 8, 16, 32 or 64 (DIA)");
     S->kernel = schedule;  // the graph is rebuilt when it was built for another schedule
     return CIECU_OK;
 }
@@ -930,10 +997,12 @@ int ciecu_pcg_product(ciecu_pcg S, double inScale, const double* d_in, double ou
     CIECU_TRY(ensure_tuned(A));
     bool persistent = false;
     CIECU_TRY(use_persistent(S, &persistent));
-    if (persistent)
+    if (persistent) {
         CIECU_TRY(ensure_persistent_buffers(S));
-    else
+    } else {
+        CIECU_TRY(refresh_dia(S, st));
         CIECU_TRY(tune_solver_spmv(S));
+    }
     S->persistent = persistent;
     // solution <- out (initial guess)
     CIECU_CUDA(cudaMemcpyAsync(S->x, d_out, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));

@@ -27,6 +27,7 @@
 
 #include <cstdint>
 #include <type_traits>
+#include <vector>
 
 struct ciecu_csr_s;
 
@@ -274,6 +275,8 @@ struct ciecu_csr_s {
     int nblocks = 0;
     int maxRow = 0;
     double avgRow = 0.0;
+    int diaState = 0;             // 0 not analysed, 1 DIA offsets found, 2 not a few-diagonal matrix
+    std::vector<int> diaOffsets;  // ascending diagonal offsets (dia.cuh)
 
     template <typename V>
     ciecu::CsrArgs<V> args(const uint16_t* mask = nullptr, uint16_t threshold = 0) const {

@@ -198,6 +198,12 @@ class _CSRHandle:
     def set_kernel(self, k):
         call("ciecu_csr_set_kernel", self.handle, int(k))
 
+    def diagonals(self):
+        """Diagonals of the matrix's diagonal-storage copy (0: not a few-diagonal matrix)."""
+        d = ctypes.c_int()
+        call("ciecu_csr_diagonals", self.handle, ctypes.byref(d))
+        return d.value
+
 
 class CSROperator(LinearOperator):
     """CSROperator<int,T>::product (linalg/packages/solvers/src/CSROperator.cpp:33-111)."""
@@ -589,6 +595,10 @@ class MixedPrecisionCG(LinearOperator):
         call("ciecu_mixed_info", self._solver, ctypes.byref(c), ctypes.byref(v))
         e = ctypes.c_int64()
         call("ciecu_mixed_padded_entries", self._solver, ctypes.byref(e))
+        if v.value == -2:
+            # the SELL copy (compressed_columns, padded_entries) is kept beside the DIA one
+            return {"format": "dia", "inner_kernel": "dia", "group_unroll": v.value,
+                    "compressed_columns": bool(c.value), "padded_entries": e.value}
         return {"compressed_columns": bool(c.value), "format": "sell-32x4", "padded_entries": e.value,
                 "group_unroll": v.value, "inner_kernel": "tma-pipeline" if v.value == 0 else "registers"}
 

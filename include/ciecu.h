@@ -109,6 +109,12 @@ int ciecu_csr_destroy(ciecu_csr csr);
  * (bit-compatible row sums), 2/4/8/16/32 = that many lanes per row. */
 int ciecu_csr_set_kernel(ciecu_csr csr, int kernel);
 int ciecu_csr_get_kernel(ciecu_csr csr, int* kernel);
+/* Number of diagonals of the matrix's diagonal-storage copy, used by the FP64
+ * PCG (schedule 64) and the mixed solver's inner matrix (innerKernel -2): the
+ * distinct offsets c - r when there are at most 32 of them, the columns of every
+ * row strictly ascend and at least 60 % of the stored entries are nonzeros; 0
+ * otherwise.  The analysis runs once per handle (one pass over the pattern). */
+int ciecu_csr_diagonals(ciecu_csr csr, int* ndiag);
 /* Runs the autotuner now (otherwise it runs on the first product). */
 int ciecu_csr_autotune(ciecu_csr csr);
 
@@ -196,9 +202,13 @@ int ciecu_pcg_product(ciecu_pcg solver, double inScale, const double* d_in, doub
  * (used when the device-side loop of conditional graph nodes is unavailable). */
 int ciecu_pcg_set_graph_chunk(ciecu_pcg solver, int iterations);
 /* Pins the schedule of the solver's fused q = A p kernel (1 = row-block stream
- * kernel, 2..32 = lanes per row) instead of autotuning it at the first solve;
- * 0 returns to autotuning.  For runs whose timings would mislead the autotuner
- * (under a profiler). */
+ * kernel, 2..32 = lanes per row, 64 = a diagonal-storage copy of the matrix, for
+ * square matrices with strictly ascending columns whose nonzeros lie on at most
+ * 32 diagonals, at least 60 % filled; the copy is refilled from the CSR values at
+ * every solve) instead of autotuning it at the first solve; 0 returns to
+ * autotuning.  For runs whose timings would mislead the autotuner (under a
+ * profiler).  A pinned 64 on a matrix without a diagonal copy fails at the solve
+ * with CIECU_ERR_ARGUMENT. */
 int ciecu_pcg_set_schedule(ciecu_pcg solver, int schedule);
 /* SpMV schedule the solver's autotuner chose for its fused q = A p kernel (0 before
  * the first solve or when the solve ran as a single launch; 1 = row-block stream

@@ -30,7 +30,11 @@ typedef struct ciecu_mixed_options {
     int compressColumns;
     /* Inner SpMV kernel: 0 lets the autotuner choose; 1, 2 or 4 fixes the groups
      * of four entries each thread keeps in flight; -1 fixes the TMA-pipelined
-     * kernel (matrix streamed through shared memory by bulk copies). */
+     * kernel (matrix streamed through shared memory by bulk copies); -2 fixes a
+     * diagonal-storage FP32 copy (square matrices with strictly ascending
+     * columns whose nonzeros lie on at most 32 diagonals, at least 60 % filled;
+     * CIECU_ERR_ARGUMENT otherwise).  The autotuner considers the diagonal copy
+     * whenever the matrix qualifies. */
     int innerKernel;
     /* 1: the FP32 inner system is the symmetrically Jacobi-scaled matrix
      * D^-1/2 A D^-1/2 (unit diagonal), for matrices whose entries span many orders

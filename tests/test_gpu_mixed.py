@@ -29,7 +29,8 @@ def mixed_solve(space, m, b, mode=0, delta=None, compress=True, x0=None, setting
 
 
 @pytest.mark.parametrize("mode,compress,inner", [(0, True, 0), (0, False, 0), (1, True, 0), (0, True, -1),
-                                                 (0, False, -1), (1, True, -1), (0, True, 1), (0, True, 4)])
+                                                 (0, False, -1), (1, True, -1), (0, True, 1), (0, True, 4),
+                                                 (0, True, -2), (1, True, -2)])
 def test_mixed_3d_lognormal_vs_reference(space, reference, mode, compress, inner):
     from cie_b200.fem import make_poisson
     prob = make_poisson(space, 3, 1, [40, 40, 40], seed=2)
@@ -37,7 +38,7 @@ def test_mixed_3d_lognormal_vs_reference(space, reference, mode, compress, inner
     b = host(prob.rhs)
     x, st, info = mixed_solve(space, prob.matrix, b, mode=mode, compress=compress, inner=inner)
     if inner:
-        assert info["group_unroll"] == max(inner, 0)
+        assert info["group_unroll"] == (inner if inner == -2 else max(inner, 0))
     xr, sr, err, _ = reference.pcg(rp, col, val, b, maxit=20000, abstol=0.0, reltol=1e-10)
     rel = np.linalg.norm(x - xr) / np.linalg.norm(xr)
     tr = true_residual(rp, col, val, x, b)
@@ -153,6 +154,48 @@ def test_sell_inner_operator_on_ragged_rows(space, restatement, inner, compress)
                            np.zeros(n))
     scale = np.array([np.sum(np.abs(val[rp[i]:rp[i + 1]] * x[col[rp[i]:rp[i + 1]]])) for i in range(n)]) + 1e-30
     assert np.max(np.abs(host(y) - ref) / scale) <= 2e-6
+
+
+@pytest.mark.parametrize("scale", [False, True])
+@pytest.mark.parametrize("dims", [(2, [48, 48]), (3, [20, 20, 20])])
+def test_dia_inner_operator_matches_sell(space, dims, scale):
+    """The DIA copy of a structured-grid Q1 matrix (9 / 27 diagonals) sums every
+    row in column order like the SELL kernels, so both FP32 inner operators agree
+    bit for bit, scaled or not; the solver reaches the same FP64 accuracy."""
+    from cie_b200.fem import make_poisson
+    from cie_b200.linalg import CSROperator, MixedPrecisionCG, Statistics, makeDiagonalOperator
+    dim, cells = dims
+    prob = make_poisson(space, dim, 1, cells, seed=6)
+    A = CSROperator(prob.matrix, space)
+    assert A.csr.diagonals() == 3 ** dim
+    D = makeDiagonalOperator(prob.matrix, space, csr_handle=A.csr)
+    dia = MixedPrecisionCG(A, D, Statistics(20000, 0.0, 1e-10), innerKernel=-2, scaleInner=scale)
+    sell = MixedPrecisionCG(A, D, Statistics(20000, 0.0, 1e-10), innerKernel=1, scaleInner=scale)
+    assert dia.info()["format"] == "dia" and sell.info()["format"] == "sell-32x4"
+    n = prob.rhs.numel()
+    x = torch.rand(n, dtype=torch.float32, device="cuda") * 2 - 1
+    y1 = torch.empty_like(x)
+    y2 = torch.empty_like(x)
+    dia.apply_inner(x, y1)
+    sell.apply_inner(x, y2)
+    assert torch.equal(y1, y2)
+    xs = torch.zeros_like(prob.rhs)
+    dia.product(0.0, prob.rhs, 1.0, xs)
+    r = prob.rhs.clone()
+    A.product(1.0, xs, -1.0, r)
+    assert float(torch.linalg.norm(r) / torch.linalg.norm(prob.rhs)) <= 1.01e-10
+
+
+def test_dia_refused_for_scattered_pattern(space):
+    """innerKernel -2 on a matrix with more than 32 diagonals is an argument error."""
+    from cie_b200._lib import CiecuError
+    from cie_b200.fem import make_poisson
+    from cie_b200.linalg import CSROperator, MixedPrecisionCG, Statistics, makeDiagonalOperator
+    prob = make_poisson(space, 3, 2, [6, 6, 6], seed=1)  # Q2: 125 diagonals
+    A = CSROperator(prob.matrix, space)
+    assert A.csr.diagonals() == 0
+    with pytest.raises(CiecuError, match="at most 32 diagonals"):
+        MixedPrecisionCG(A, makeDiagonalOperator(prob.matrix, space), Statistics(10, 0.0, 1e-10), innerKernel=-2)
 
 
 @pytest.mark.parametrize("embedded", [False, True])

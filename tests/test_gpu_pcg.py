@@ -117,6 +117,47 @@ def test_pcg_settings_vs_reference(space, reference, case, loop):
         assert np.allclose(y, si * y0 + so * xr2, rtol=1e-9, atol=1e-11)
 
 
+@pytest.mark.parametrize("schedule", [64, 4])
+def test_pcg_dia_schedule_vs_reference(space, reference, schedule):
+    """The FP64 K1 over the diagonal-storage copy (27 diagonals of the 3D Q1 grid)
+    against the reference solver; the copy follows changed CSR values."""
+    from cie_b200.fem import make_poisson
+    from cie_b200.linalg import CSROperator, ConjugateGradients, Statistics, makeDiagonalOperator
+    prob = make_poisson(space, 3, 1, [48, 48, 48], seed=3)
+    rp, col, val = prob.host_csr()
+    b = host(prob.rhs)
+    A = CSROperator(prob.matrix, space)
+    assert A.csr.diagonals() == 27
+    cg = ConjugateGradients(A, space, makeDiagonalOperator(prob.matrix, space, csr_handle=A.csr),
+                            Statistics(5000, 0.0, 1e-10))
+    cg.set_loop(1)
+    cg.set_schedule(schedule)
+    x = dev(np.zeros(len(b)))
+    cg.product(0.0, dev(b), 1.0, x)
+    assert cg.info()["spmv_schedule"] == schedule
+    xr, sr, err, _ = reference.pcg(rp, col, val, b, maxit=5000, abstol=0.0, reltol=1e-10)
+    rel = np.linalg.norm(host(x) - xr) / np.linalg.norm(xr)
+    assert abs(cg.getStats().iterationCount - sr[0]) <= 2 and rel <= 1e-9
+    # scale the matrix in place: the next solve must see the new values
+    prob.matrix.entries.mul_(2.0)
+    x2 = dev(np.zeros(len(b)))
+    cg.product(0.0, dev(b), 1.0, x2)
+    assert np.linalg.norm(2.0 * host(x2) - host(x)) <= 1e-9 * np.linalg.norm(host(x))
+
+
+def test_pcg_dia_schedule_refused_without_diagonals(space):
+    from cie_b200._lib import CiecuError
+    from cie_b200.fem import make_poisson
+    from cie_b200.linalg import CSROperator, ConjugateGradients, Statistics, makeDiagonalOperator
+    prob = make_poisson(space, 3, 2, [6, 6, 6], seed=1)
+    A = CSROperator(prob.matrix, space)
+    cg = ConjugateGradients(A, space, makeDiagonalOperator(prob.matrix, space), Statistics(50, 0.0, 1e-10))
+    cg.set_loop(1)
+    cg.set_schedule(64)
+    with pytest.raises(CiecuError, match="at most 32 diagonals"):
+        cg.product(0.0, prob.rhs, 1.0, torch.zeros_like(prob.rhs))
+
+
 @pytest.mark.parametrize("loop", LOOPS)
 def test_pcg_breakdown_raises(space, loop):
     from cie_b200.linalg import Statistics
