@@ -33,21 +33,34 @@ struct DiaArgs {
     int off[kMaxDiagonals];  // ascending
 };
 
+// Calls step(d) for every diagonal: fully unrolled when the count ND is known at
+// compile time (27 and 9, the 3D and 2D Q1 stencils: every load of a row in
+// flight at once), else over the runtime count.
+template <int ND, typename V, typename F>
+__device__ __forceinline__ void for_diagonals(const DiaArgs<V>& A, F&& step) {
+    if constexpr (ND > 0) {
+#pragma unroll
+        for (int d = 0; d < ND; ++d) step(d);
+    } else {
+#pragma unroll 9
+        for (int d = 0; d < A.ndiag; ++d) step(d);
+    }
+}
+
 // One thread per row (grid-stride); epilogue interface of the CSR engines.
-template <typename T, typename V, typename Op>
+template <int ND, typename T, typename V, typename Op>
 __device__ __forceinline__ void dia_rows(const DiaArgs<V>& A, const T* __restrict__ x, Op& op) {
     const long stride = static_cast<long>(gridDim.x) * blockDim.x;
     for (long rl = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; rl < A.nrows; rl += stride) {
         const int r = static_cast<int>(rl);
         const auto pre = op.pre(r);
         T sum = T(0);
-#pragma unroll 9
-        for (int d = 0; d < A.ndiag; ++d) {
+        for_diagonals<ND>(A, [&](int d) {
             const int c = r + A.off[d];
             const V v = stream_ld(A.val + static_cast<long>(d) * A.ld + r);
             const T xv = static_cast<unsigned>(c) < static_cast<unsigned>(A.nrows) ? __ldg(x + c) : T(0);
             sum = fma(static_cast<T>(v), xv, sum);
-        }
+        });
         op.post(r, pre, sum);
     }
 }
@@ -56,7 +69,7 @@ __device__ __forceinline__ void dia_rows(const DiaArgs<V>& A, const T* __restric
 // a warp reads 512 contiguous bytes per diagonal instead of 128).  Rows past
 // nrows (up to ld, zero-filled) are computed and dropped; the gathers of x stay
 // inside [0, nrows).
-template <typename Op>
+template <int ND, typename Op>
 __device__ __forceinline__ void dia_rows4(const DiaArgs<float>& A, const float* __restrict__ x, Op& op) {
     const long stride = static_cast<long>(gridDim.x) * blockDim.x * 4;
     for (long r0 = (static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x) * 4; r0 < A.nrows; r0 += stride) {
@@ -66,8 +79,7 @@ __device__ __forceinline__ void dia_rows4(const DiaArgs<float>& A, const float* 
         for (int i = 0; i < 4; ++i)
             if (r + i < A.nrows) pre[i] = op.pre(r + i);
         float sum[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll 9
-        for (int d = 0; d < A.ndiag; ++d) {
+        for_diagonals<ND>(A, [&](int d) {
             const float4 v = __ldcs(reinterpret_cast<const float4*>(A.val + static_cast<long>(d) * A.ld + r));
             const int c = r + A.off[d];
             float xv[4];
@@ -78,10 +90,20 @@ __device__ __forceinline__ void dia_rows4(const DiaArgs<float>& A, const float* 
             sum[1] = fmaf(v.y, xv[1], sum[1]);
             sum[2] = fmaf(v.z, xv[2], sum[2]);
             sum[3] = fmaf(v.w, xv[3], sum[3]);
-        }
+        });
 #pragma unroll
         for (int i = 0; i < 4; ++i)
             if (r + i < A.nrows) op.post(r + i, pre[i], sum[i]);
+    }
+}
+
+// Calls f(std::integral_constant<int, ND>) with ND = 27, 9 or 0 (runtime count).
+template <typename F>
+int with_diagonals(int ndiag, F&& f) {
+    switch (ndiag) {
+        case 27: return f(std::integral_constant<int, 27>{});
+        case 9: return f(std::integral_constant<int, 9>{});
+        default: return f(std::integral_constant<int, 0>{});
     }
 }
 

@@ -188,13 +188,14 @@ __global__ void __launch_bounds__(kT) mixed_spmv_kernel(SellArgs<float, CI> A, c
 
 // DIA variants of the two kernels above, for inner matrices of at most 32
 // diagonals (dia.cuh): FP32 values only, no column indices.
+template <int ND>
 __global__ void __launch_bounds__(kT) mixed_apply_dia_kernel(DiaArgs<float> A, const float* __restrict__ x,
                                                             float* __restrict__ y) {
     StoreOp op{y};
-    dia_rows4(A, x, op);
+    dia_rows4<ND>(A, x, op);
 }
 
-template <bool COND>
+template <int ND, bool COND>
 __global__ void __launch_bounds__(kT) mixed_spmv_dia_kernel(DiaArgs<float> A, const float* __restrict__ p,
                                                            float* __restrict__ q, MixedScalars* s, double* partials,
                                                            unsigned* counter, cudaGraphConditionalHandle loop) {
@@ -203,7 +204,7 @@ __global__ void __launch_bounds__(kT) mixed_spmv_dia_kernel(DiaArgs<float> A, co
         return;
     }
     MixedPqOp op{p, q, 0.0};
-    dia_rows4(A, p, op);
+    dia_rows4<ND>(A, p, op);
     double mine[1] = {op.acc}, tot[1];
     if (grid_reduce_last<1, kT>(mine, partials, counter, tot) && threadIdx.x == 0) {
         s->pq = tot[0];
@@ -560,8 +561,13 @@ template <bool COND>
 int launch_inner_spmv(ciecu_mixed_s* M, cudaStream_t st, cudaGraphConditionalHandle loop) {
     const long needA = (M->n + kT - 1) / kT;
     if (M->unroll == kDiaInner) {
-        mixed_spmv_dia_kernel<COND><<<fit_grid(mixed_spmv_dia_kernel<COND>, kT, (needA + 3) / 4), kT, 0, st>>>(
-            M->dia, M->p32, M->q32, M->d_s, M->d_partials, M->d_counter, loop);
+        CIECU_TRY(with_diagonals(M->dia.ndiag, [&](auto nd) -> int {
+            constexpr int ND = decltype(nd)::value;
+            mixed_spmv_dia_kernel<ND, COND><<<fit_grid(mixed_spmv_dia_kernel<ND, COND>, kT, (needA + 3) / 4), kT, 0,
+                                              st>>>(M->dia, M->p32, M->q32, M->d_s, M->d_partials, M->d_counter,
+                                                    loop);
+            return CIECU_OK;
+        }));
         CIECU_CHECK_LAUNCH("mixed_spmv_dia_kernel");
         return CIECU_OK;
     }
@@ -947,8 +953,12 @@ int ciecu_mixed_apply_f32(ciecu_mixed M, const float* d_in, float* d_out) {
     cudaStream_t st = M->A->space->stream;
     const long need = (M->n + kT - 1) / kT;
     if (M->unroll == kDiaInner) {
-        mixed_apply_dia_kernel<<<fit_grid(mixed_apply_dia_kernel, kT, (need + 3) / 4), kT, 0, st>>>(M->dia, d_in,
-                                                                                                 d_out);
+        CIECU_TRY(with_diagonals(M->dia.ndiag, [&](auto nd) -> int {
+            constexpr int ND = decltype(nd)::value;
+            mixed_apply_dia_kernel<ND><<<fit_grid(mixed_apply_dia_kernel<ND>, kT, (need + 3) / 4), kT, 0, st>>>(
+                M->dia, d_in, d_out);
+            return CIECU_OK;
+        }));
         count_launch();
         CIECU_CHECK_LAUNCH("mixed_apply_dia_kernel");
         return CIECU_OK;
