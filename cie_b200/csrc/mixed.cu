@@ -38,6 +38,9 @@
 
 #include <string>
 #include <vector>
+#include <tuple>
+#include <mutex>
+#include <map>
 
 namespace ciecu {
 namespace {
@@ -514,6 +517,7 @@ struct ciecu_mixed_s {
     bool idx16 = false;
     int unroll = 2;  // SELL groups of four entries in flight per thread (autotuned; 0 = TMA pipeline,
                      // kDiaInner = the DIA copy)
+    bool sellBuilt = false;  // the SELL copy exists (not built when the DIA copy is the known choice)
     float* dia32 = nullptr;  // DIA copy of the inner matrix (few-diagonal matrices only)
     ciecu::DiaArgs<float> dia{};
     // SELL-32 inner matrix
@@ -680,6 +684,98 @@ int build_mixed_graph(ciecu_mixed_s* M) {
 
 using namespace ciecu;
 
+namespace ciecu {
+namespace {
+
+// SELL-32x4 copy of the inner matrix (sell.cuh): slice lengths on the device,
+// their prefix sum on the host, then the FP32 values and 16-bit or int32 columns.
+int build_sell(ciecu_mixed_s* M, ciecu_csr_s* lhs, const ciecu_mixed_options& options, cudaStream_t st) {
+    const size_t n = static_cast<size_t>(std::max<long>(M->n, 1)) + 4;
+    cudaError_t e = cudaMalloc(&M->sliceLen, sizeof(int) * std::max(1, M->nslices));
+    if (e == cudaSuccess) e = cudaMalloc(&M->sliceStart, sizeof(long long) * (M->nslices + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&M->rowLen, sizeof(unsigned short) * n);
+    if (e != cudaSuccess) return cuda_fail(e, "mixed_create: SELL allocation");
+    // Slice lengths on the device, their prefix sum on the host.
+    unsigned* d_flag = reinterpret_cast<unsigned*>(lhs->space->d_result);
+    unsigned flags[2] = {0, 0};
+    e = cudaMemsetAsync(d_flag, 0, 2 * sizeof(unsigned), st);
+    if (M->n > 0 && e == cudaSuccess) {
+        sell_len_kernel<<<grid_for(M->nslices, kT, 8), kT, 0, st>>>(static_cast<int>(M->n), lhs->rowptr, M->sliceLen,
+                                                                    d_flag);
+        count_launch();
+        e = cudaGetLastError();
+    }
+    std::vector<int> lens(static_cast<size_t>(M->nslices));
+    std::vector<long long> starts(static_cast<size_t>(M->nslices) + 1, 0);
+    if (e == cudaSuccess && M->nslices)
+        e = cudaMemcpyAsync(lens.data(), M->sliceLen, sizeof(int) * lens.size(), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(flags, d_flag, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(e, "mixed_create: slice lengths");
+    if (flags[0]) return fail(CIECU_ERR_ARGUMENT, "mixed_create: rows longer than 65535 entries are not supported");
+    for (int sl = 0; sl < M->nslices; ++sl) starts[sl + 1] = starts[sl] + 128LL * ((std::abs(lens[sl]) + 3) / 4);
+    M->paddedEntries = starts.back();
+    e = cudaMemcpyAsync(M->sliceStart, starts.data(), sizeof(long long) * starts.size(), cudaMemcpyHostToDevice, st);
+    const size_t padded = static_cast<size_t>(std::max<long long>(1, M->paddedEntries));
+    if (e == cudaSuccess) e = cudaMalloc(&M->val32, sizeof(float) * padded);
+    const bool try16 = options.compressColumns != 0;
+    if (e == cudaSuccess) e = cudaMalloc(&M->col32or16, (try16 ? sizeof(short) : sizeof(int)) * padded);
+    // lanes past the last row of the final slice are never written by the fill
+    if (e == cudaSuccess) e = cudaMemsetAsync(M->val32, 0, sizeof(float) * padded, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(M->col32or16, 0, (try16 ? sizeof(short) : sizeof(int)) * padded, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_flag, 0, sizeof(unsigned), st);
+    if (e == cudaSuccess && M->n > 0) {
+        const int grid = grid_for(M->n, kT, 8);
+        if (try16)
+            sell_fill_kernel<short><<<grid, kT, 0, st>>>(static_cast<int>(M->n), lhs->rowptr, lhs->col,
+                                                         static_cast<const double*>(lhs->val), M->sliceLen,
+                                                         M->sliceStart, M->val32, static_cast<short*>(M->col32or16),
+                                                         M->rowLen, d_flag, M->sdiag);
+        else
+            sell_fill_kernel<int><<<grid, kT, 0, st>>>(static_cast<int>(M->n), lhs->rowptr, lhs->col,
+                                                       static_cast<const double*>(lhs->val), M->sliceLen,
+                                                       M->sliceStart, M->val32, static_cast<int*>(M->col32or16),
+                                                       M->rowLen, d_flag, M->sdiag);
+        count_launch();
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(flags, d_flag, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(e, "mixed_create: conversion");
+    M->idx16 = try16 && !flags[0];
+    if (try16 && flags[0]) {
+        // bandwidth too large for 16-bit offsets: int32 columns
+        cudaFree(M->col32or16);
+        M->col32or16 = nullptr;
+        e = cudaMalloc(&M->col32or16, sizeof(int) * padded);
+        if (e == cudaSuccess) e = cudaMemsetAsync(M->col32or16, 0, sizeof(int) * padded, st);
+        if (e == cudaSuccess && M->n > 0) {
+            sell_fill_kernel<int><<<grid_for(M->n, kT, 8), kT, 0, st>>>(
+                static_cast<int>(M->n), lhs->rowptr, lhs->col, static_cast<const double*>(lhs->val), M->sliceLen,
+                M->sliceStart, M->val32, static_cast<int*>(M->col32or16), M->rowLen, d_flag, M->sdiag);
+            count_launch();
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return cuda_fail(e, "mixed_create: int32 columns");
+    }
+    M->a16 = SellArgs<float, short>{static_cast<int>(M->n), M->sliceLen, M->sliceStart, M->rowLen, M->val32,
+                                    static_cast<const short*>(M->col32or16)};
+    M->a32 = SellArgs<float, int>{static_cast<int>(M->n), M->sliceLen, M->sliceStart, M->rowLen, M->val32,
+                                  static_cast<const int*>(M->col32or16)};
+    M->sellBuilt = true;
+    return CIECU_OK;
+}
+
+// Inner-kernel choice of the autotuner per matrix shape (rows, nonzeros,
+// diagonals, 16-bit columns requested, scaled inner system): later solvers of the
+// same shape skip the timing and, when the choice is the DIA copy, the SELL copy.
+std::mutex g_innerMutex;
+std::map<std::tuple<int, long, int, int, int>, int> g_innerChoice;
+
+}  // namespace
+}  // namespace ciecu
+
 extern "C" {
 
 int ciecu_mixed_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_statistics settings,
@@ -720,92 +816,17 @@ int ciecu_mixed_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_sta
             e = cudaGetLastError();
         }
     }
-    if (e == cudaSuccess) e = cudaMalloc(&M->sliceLen, sizeof(int) * std::max(1, M->nslices));
-    if (e == cudaSuccess) e = cudaMalloc(&M->sliceStart, sizeof(long long) * (M->nslices + 1));
-    if (e == cudaSuccess) e = cudaMalloc(&M->rowLen, sizeof(unsigned short) * n);
-    if (e != cudaSuccess) {
-        ciecu_mixed_destroy(M);
-        return cuda_fail(e, "mixed_create: allocation");
-    }
-    // Slice lengths on the device, their prefix sum on the host.
-    unsigned* d_flag = reinterpret_cast<unsigned*>(lhs->space->d_result);
-    unsigned flags[2] = {0, 0};
-    e = cudaMemsetAsync(d_flag, 0, 2 * sizeof(unsigned), st);
-    if (M->n > 0 && e == cudaSuccess) {
-        sell_len_kernel<<<grid_for(M->nslices, kT, 8), kT, 0, st>>>(static_cast<int>(M->n), lhs->rowptr, M->sliceLen,
-                                                                    d_flag);
+    if (e == cudaSuccess && M->n > 0) {
+        if (M->sdiag)
+            fill_f32_kernel<<<grid_for(M->n, kT, 8), kT, 0, st>>>(M->n, 1.0f, M->dinv32);  // D^-1 of the scaled matrix
+        else
+            to_f32_kernel<<<grid_for(M->n, kT, 8), kT, 0, st>>>(M->n, d_inverseDiagonal, M->dinv32);
         count_launch();
         e = cudaGetLastError();
     }
-    std::vector<int> lens(static_cast<size_t>(M->nslices));
-    std::vector<long long> starts(static_cast<size_t>(M->nslices) + 1, 0);
-    if (e == cudaSuccess && M->nslices)
-        e = cudaMemcpyAsync(lens.data(), M->sliceLen, sizeof(int) * lens.size(), cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(flags, d_flag, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {
         ciecu_mixed_destroy(M);
-        return cuda_fail(e, "mixed_create: slice lengths");
-    }
-    if (flags[0]) {
-        ciecu_mixed_destroy(M);
-        return fail(CIECU_ERR_ARGUMENT, "mixed_create: rows longer than 65535 entries are not supported");
-    }
-    for (int sl = 0; sl < M->nslices; ++sl) starts[sl + 1] = starts[sl] + 128LL * ((std::abs(lens[sl]) + 3) / 4);
-    M->paddedEntries = starts.back();
-    e = cudaMemcpyAsync(M->sliceStart, starts.data(), sizeof(long long) * starts.size(), cudaMemcpyHostToDevice, st);
-    const size_t padded = static_cast<size_t>(std::max<long long>(1, M->paddedEntries));
-    if (e == cudaSuccess) e = cudaMalloc(&M->val32, sizeof(float) * padded);
-    const bool try16 = options.compressColumns != 0;
-    if (e == cudaSuccess) e = cudaMalloc(&M->col32or16, (try16 ? sizeof(short) : sizeof(int)) * padded);
-    // lanes past the last row of the final slice are never written by the fill
-    if (e == cudaSuccess) e = cudaMemsetAsync(M->val32, 0, sizeof(float) * padded, st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(M->col32or16, 0, (try16 ? sizeof(short) : sizeof(int)) * padded, st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(d_flag, 0, sizeof(unsigned), st);
-    if (e == cudaSuccess && M->n > 0) {
-        const int grid = grid_for(M->n, kT, 8);
-        if (try16)
-            sell_fill_kernel<short><<<grid, kT, 0, st>>>(static_cast<int>(M->n), lhs->rowptr, lhs->col,
-                                                         static_cast<const double*>(lhs->val), M->sliceLen,
-                                                         M->sliceStart, M->val32, static_cast<short*>(M->col32or16),
-                                                         M->rowLen, d_flag, M->sdiag);
-        else
-            sell_fill_kernel<int><<<grid, kT, 0, st>>>(static_cast<int>(M->n), lhs->rowptr, lhs->col,
-                                                       static_cast<const double*>(lhs->val), M->sliceLen,
-                                                       M->sliceStart, M->val32, static_cast<int*>(M->col32or16),
-                                                       M->rowLen, d_flag, M->sdiag);
-        if (M->sdiag)
-            fill_f32_kernel<<<grid, kT, 0, st>>>(M->n, 1.0f, M->dinv32);  // D^-1 of the scaled matrix
-        else
-            to_f32_kernel<<<grid, kT, 0, st>>>(M->n, d_inverseDiagonal, M->dinv32);
-        count_launch(2);
-        e = cudaGetLastError();
-    }
-    if (e == cudaSuccess) e = cudaMemcpyAsync(flags, d_flag, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) {
-        ciecu_mixed_destroy(M);
-        return cuda_fail(e, "mixed_create: conversion");
-    }
-    M->idx16 = try16 && !flags[0];
-    if (try16 && flags[0]) {
-        // bandwidth too large for 16-bit offsets: int32 columns
-        cudaFree(M->col32or16);
-        M->col32or16 = nullptr;
-        e = cudaMalloc(&M->col32or16, sizeof(int) * padded);
-        if (e == cudaSuccess) e = cudaMemsetAsync(M->col32or16, 0, sizeof(int) * padded, st);
-        if (e == cudaSuccess && M->n > 0) {
-            sell_fill_kernel<int><<<grid_for(M->n, kT, 8), kT, 0, st>>>(
-                static_cast<int>(M->n), lhs->rowptr, lhs->col, static_cast<const double*>(lhs->val), M->sliceLen,
-                M->sliceStart, M->val32, static_cast<int*>(M->col32or16), M->rowLen, d_flag, M->sdiag);
-            count_launch();
-            e = cudaGetLastError();
-        }
-        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-        if (e != cudaSuccess) {
-            ciecu_mixed_destroy(M);
-            return cuda_fail(e, "mixed_create: int32 columns");
-        }
+        return cuda_fail(e, "mixed_create: allocation");
     }
     // DIA copy of the inner matrix when its nonzeros lie on few diagonals.
     if (M->n > 0 && (options.innerKernel == 0 || options.innerKernel == kDiaInner)) {
@@ -834,10 +855,22 @@ int ciecu_mixed_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_sta
             return fail(CIECU_ERR_ARGUMENT, "mixed_create: innerKernel -2 needs a matrix of at most 32 diagonals");
         }
     }
-    M->a16 = SellArgs<float, short>{static_cast<int>(M->n), M->sliceLen, M->sliceStart, M->rowLen, M->val32,
-                                    static_cast<const short*>(M->col32or16)};
-    M->a32 = SellArgs<float, int>{static_cast<int>(M->n), M->sliceLen, M->sliceStart, M->rowLen, M->val32,
-                                  static_cast<const int*>(M->col32or16)};
+    const auto key = std::make_tuple(lhs->rows, lhs->nnz, M->dia32 ? M->dia.ndiag : 0, options.compressColumns ? 1 : 0,
+                                     options.scaleInner);
+    int cached = 1000;  // none
+    if (options.innerKernel == 0) {
+        std::lock_guard<std::mutex> lock(g_innerMutex);
+        auto it = g_innerChoice.find(key);
+        if (it != g_innerChoice.end() && (it->second != kDiaInner || M->dia32)) cached = it->second;
+    }
+    const bool diaOnly = (options.innerKernel == kDiaInner) || (cached == kDiaInner);
+    if (!diaOnly) {
+        const int status = build_sell(M, lhs, options, st);
+        if (status != CIECU_OK) {
+            ciecu_mixed_destroy(M);
+            return status;
+        }
+    }
     {
         int st2 = allow_tma_smem(mixed_spmv_tma_kernel<short, false>, TmaShape<float, short>::SMEM);
         if (st2 == CIECU_OK) st2 = allow_tma_smem(mixed_spmv_tma_kernel<short, true>, TmaShape<float, short>::SMEM);
@@ -850,12 +883,13 @@ int ciecu_mixed_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_sta
             return st2;
         }
     }
+    if (cached != 1000) M->unroll = cached;
     // Autotune the group unroll of the inner SpMV on the solver's own matrix,
     // timing the fused kernel the iteration runs (q = A32 p with the p^T q
     // reduction) on scratch vectors p32 = 0 -> q32.
     if (options.innerKernel != 0)
         M->unroll = options.innerKernel == kDiaInner ? kDiaInner : (options.innerKernel < 0 ? 0 : options.innerKernel);
-    if (M->n > 0 && options.innerKernel == 0) {
+    if (M->n > 0 && options.innerKernel == 0 && cached == 1000) {
         // p = D^-1 > 0: p^T A p > 0 for an SPD matrix, so no timed launch trips the
         // breakdown flag (which would make the later candidates return at once).
         MixedScalars scratch{};
@@ -901,6 +935,8 @@ int ciecu_mixed_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_sta
             return cuda_fail(e, "mixed_create: autotune");
         }
         M->unroll = bestU;
+        std::lock_guard<std::mutex> lock(g_innerMutex);
+        g_innerChoice[key] = bestU;
     }
     *out = M;
     return CIECU_OK;

@@ -16,6 +16,9 @@
 #include "pcg.cuh"
 
 #include <string>
+#include <tuple>
+#include <mutex>
+#include <map>
 #include <vector>
 
 namespace ciecu {
@@ -798,9 +801,25 @@ int run_persistent(ciecu_pcg_s* S, cudaStream_t st) {
 // Picks the K1 schedule by timing the fused SpMV + p^T q kernel itself on the
 // solver's buffers (p = 0 -> q); its register use, and so the best schedule,
 // differs from the plain operator's.
+// K1 schedule chosen per matrix shape (rows, nonzeros, diagonals of the DIA
+// copy, preconditioned, 16-byte aligned arrays): later solvers of the same shape
+// skip the timing.
+std::mutex g_k1Mutex;
+std::map<std::tuple<int, long, int, int, int>, int> g_k1Choice;
+
 int tune_solver_spmv(ciecu_pcg_s* S) {
     if (S->kernel != 0) return CIECU_OK;
     ciecu_csr_s* A = S->A;
+    const auto key = std::make_tuple(A->rows, A->nnz, S->diaBuf ? S->dia.ndiag : 0, S->dinv ? 1 : 0,
+                                     static_cast<int>(A->aligned16));
+    {
+        std::lock_guard<std::mutex> lock(g_k1Mutex);
+        auto it = g_k1Choice.find(key);
+        if (it != g_k1Choice.end()) {
+            S->kernel = it->second;
+            return CIECU_OK;
+        }
+    }
     cudaStream_t st = A->space->stream;
     // p = D^-1 (or 1): positive, so p^T A p > 0 for an SPD matrix and the timed
     // kernel never trips the breakdown flag (which would make later candidates
@@ -849,6 +868,10 @@ int tune_solver_spmv(ciecu_pcg_s* S) {
     CIECU_CUDA(cudaMemcpyAsync(&flag, &S->d_s->done, sizeof(int), cudaMemcpyDeviceToHost, st));
     CIECU_CUDA(cudaStreamSynchronize(st));
     S->kernel = flag ? A->kernel : bestK;
+    if (!flag) {
+        std::lock_guard<std::mutex> lock(g_k1Mutex);
+        g_k1Choice[key] = S->kernel;
+    }
     return CIECU_OK;
 }
 

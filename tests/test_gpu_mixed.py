@@ -45,7 +45,8 @@ def test_mixed_3d_lognormal_vs_reference(space, reference, mode, compress, inner
     print("mixed mode %d compress %s: %d inner iterations, %d refinements (FP64 reference: %d), "
           "|x-x_ref|/|x_ref| = %.3e, true rel residual %.3e, %s"
           % (mode, compress, st.innerIterations, st.refinements, sr[0], rel, tr, info))
-    assert info["compressed_columns"] == compress
+    if info["format"] != "dia":  # the SELL copy is not built when the DIA copy is the known choice
+        assert info["compressed_columns"] == compress
     assert st.trueRelativeResidual < 1e-10 and tr <= 1.01e-10
     assert rel <= 1e-9
     if mode == 0:
