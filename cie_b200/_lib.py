@@ -115,6 +115,7 @@ SIGNATURES = {
     "ciecu_multi_create": (c_int, [P, c_int, P, Statistics, P]),
     "ciecu_multi_destroy": (c_int, [P]),
     "ciecu_multi_info": (c_int, [P, P, P]),
+    "ciecu_multi_format": (c_int, [P, P]),
     "ciecu_multi_product": (c_int, [P, c_double, P, c_double, P, P]),
     "ciecu_dirichlet_eliminate": (c_int, [P, P, P, P]),
 }

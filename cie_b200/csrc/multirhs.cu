@@ -16,6 +16,7 @@
 // One iteration = three kernels (K1 SpMM + p_c^T q_c, K2 update + dots +
 // decision, K3 direction) in the device-side graph loop of the other solvers;
 // a column that has converged is left unchanged by K2/K3.
+#include "dia.cuh"
 #include "graph.cuh"
 #include "pcg.cuh"
 #include "ciecu_multi.h"
@@ -174,6 +175,36 @@ __device__ __forceinline__ void multi_rows(const CsrArgs<double>& A, int k, cons
     }
 }
 
+// The same row sums over the DIA copy of a few-diagonal matrix (dia.cuh): lane c
+// of a row's group reads the diagonal value (one broadcast load for the group)
+// and X[row + off[d]][c] (k consecutive doubles, coalesced).  No staging, no
+// column indices; the diagonals run in ascending order, i.e. in the CSR column
+// order, so the sums equal those of multi_rows.
+template <int KP, bool FULL, typename Op>
+__device__ __forceinline__ void multi_dia_rows(const DiaArgs<double>& D, int k, const double* __restrict__ X,
+                                               Op& op) {
+    constexpr int RPW = 32 / KP;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int slot = lane / KP, c = lane % KP;
+    const bool active = FULL || c < k;
+    const long ld = FULL ? KP : k;
+    const double* __restrict__ xc = X + c;
+    const long stride = static_cast<long>(gridDim.x) * kWarps * RPW;
+    for (long row = (static_cast<long>(blockIdx.x) * kWarps + warp) * RPW + slot; row < D.nrows; row += stride) {
+        double acc = 0.0;
+#pragma unroll 9
+        for (int d = 0; d < D.ndiag; ++d) {
+            const long col = row + D.off[d];
+            const double a = stream_ld(D.val + static_cast<long>(d) * D.ld + row);
+            const double xv =
+                active && static_cast<unsigned long>(col) < static_cast<unsigned long>(D.nrows) ? __ldg(xc + col * ld)
+                                                                                                 : 0.0;
+            acc = fma(a, xv, acc);
+        }
+        if (active) op(row, c, acc);
+    }
+}
+
 struct ResidualOp {  // R = B - A X
     const double* __restrict__ b;
     double* __restrict__ r;
@@ -188,6 +219,14 @@ __global__ void __launch_bounds__(kT) multi_residual_kernel(CsrArgs<double> A, i
                                                             const double* __restrict__ B, double* __restrict__ R) {
     ResidualOp op{B, R, k};
     multi_rows<KP, FULL>(A, k, X, op);
+}
+
+template <int KP, bool FULL>
+__global__ void __launch_bounds__(kT) multi_residual_dia_kernel(DiaArgs<double> D, int k,
+                                                                const double* __restrict__ X,
+                                                                const double* __restrict__ B, double* __restrict__ R) {
+    ResidualOp op{B, R, k};
+    multi_dia_rows<KP, FULL>(D, k, X, op);
 }
 
 // Initial set-up per column: z = D^-1 r, p = z, rr, rz and the initial test.
@@ -259,6 +298,34 @@ __global__ void __launch_bounds__(kT) multi_spmv_kernel(CsrArgs<double> A, int k
     }
     PqOp op{P, Q, k, 0.0};
     multi_rows<KP, FULL>(A, k, P, op);
+    double mine[1] = {op.acc}, tot[1];
+    if (column_reduce_last<KP, 1>(mine, k, partials, counter, tot) && threadIdx.x < k) {
+        ColumnScalars& s = S[threadIdx.x];
+        if (!s.done) {
+            s.pq = tot[0];
+            if (!(0.0 < tot[0])) {
+                s.done = 3;
+                s.errorKind = 2;
+                s.errorIter = s.iter;
+                atomicAdd(&g->finished, 1u);
+            } else {
+                s.alpha = s.rz / tot[0];
+            }
+        }
+    }
+}
+
+template <int KP, bool FULL, bool COND>
+__global__ void __launch_bounds__(kT) multi_spmv_dia_kernel(DiaArgs<double> D, int k, const double* __restrict__ P,
+                                                            double* __restrict__ Q, ColumnScalars* S, MultiGlobal* g,
+                                                            double* partials, unsigned* counter,
+                                                            cudaGraphConditionalHandle cond) {
+    if (*reinterpret_cast<volatile unsigned*>(&g->finished) >= static_cast<unsigned>(k)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) set_loop<COND>(cond, 0);
+        return;
+    }
+    PqOp op{P, Q, k, 0.0};
+    multi_dia_rows<KP, FULL>(D, k, P, op);
     double mine[1] = {op.acc}, tot[1];
     if (column_reduce_last<KP, 1>(mine, k, partials, counter, tot) && threadIdx.x < k) {
         ColumnScalars& s = S[threadIdx.x];
@@ -396,6 +463,13 @@ struct ciecu_multi_s {
     int chunk = 16;
     int grid = 1;   // SpMM kernels (register-limited occupancy)
     int gridV = 1;  // vector kernels
+    // DIA copy of a few-diagonal matrix, refilled from the CSR values at every
+    // solve; used when it timed faster at the first solve.
+    bool diaChecked = false;
+    bool useDia = false;
+    int gridD = 1;
+    double* diaBuf = nullptr;
+    ciecu::DiaArgs<double> dia{};
 };
 
 namespace ciecu {
@@ -405,7 +479,14 @@ template <bool COND>
 int launch_multi_iteration(ciecu_multi_s* M, cudaStream_t st, cudaGraphConditionalHandle cond) {
     CIECU_TRY(with_group(M->kp, [&](auto kk) -> int {
         constexpr int KP = decltype(kk)::value;
-        if (M->k == KP)
+        if (M->useDia && M->k == KP)
+            multi_spmv_dia_kernel<KP, true, COND><<<M->gridD, kT, 0, st>>>(M->dia, M->k, M->p, M->q, M->d_s, M->d_g,
+                                                                           M->d_partials, M->d_counter, cond);
+        else if (M->useDia)
+            multi_spmv_dia_kernel<KP, false, COND><<<M->gridD, kT, 0, st>>>(M->dia, M->k, M->p, M->q, M->d_s,
+                                                                            M->d_g, M->d_partials, M->d_counter,
+                                                                            cond);
+        else if (M->k == KP)
             multi_spmv_kernel<KP, true, COND><<<M->grid, kT, 0, st>>>(M->A->args<double>(), M->k, M->p, M->q, M->d_s,
                                                                       M->d_g, M->d_partials, M->d_counter, cond);
         else
@@ -419,6 +500,82 @@ int launch_multi_iteration(ciecu_multi_s* M, cudaStream_t st, cudaGraphCondition
         return CIECU_OK;
     }));
     CIECU_CHECK_LAUNCH("multi-rhs pcg iteration");
+    return CIECU_OK;
+}
+
+// R = B - A X with the SpMM of the chosen format.
+int launch_multi_residual(ciecu_multi_s* M, cudaStream_t st, bool dia, const double* B) {
+    return with_group(M->kp, [&](auto kk) -> int {
+        constexpr int KP = decltype(kk)::value;
+        if (dia && M->k == KP)
+            multi_residual_dia_kernel<KP, true><<<M->gridD, kT, 0, st>>>(M->dia, M->k, M->x, B, M->r);
+        else if (dia)
+            multi_residual_dia_kernel<KP, false><<<M->gridD, kT, 0, st>>>(M->dia, M->k, M->x, B, M->r);
+        else if (M->k == KP)
+            multi_residual_kernel<KP, true><<<M->grid, kT, 0, st>>>(M->A->args<double>(), M->k, M->x, B, M->r);
+        else
+            multi_residual_kernel<KP, false><<<M->grid, kT, 0, st>>>(M->A->args<double>(), M->k, M->x, B, M->r);
+        count_launch();
+        return CIECU_OK;
+    });
+}
+
+// At the first solve: build the DIA copy when the matrix has few diagonals and
+// keep it if its SpMM (timed on the residual kernel, best of three) is faster.
+// Later solves refill its values from the CSR arrays.
+int prepare_dia(ciecu_multi_s* M, cudaStream_t st, const double* B) {
+    if (!M->diaChecked) {
+        M->diaChecked = true;
+        const std::vector<int>* offsets = nullptr;
+        CIECU_TRY(dia_offsets(M->A, &offsets));
+        if (offsets->empty()) return CIECU_OK;
+        DiaArgs<double> a = dia_shape<double>(M->A, *offsets);
+        const size_t bytes = sizeof(double) * static_cast<size_t>(a.ndiag) * static_cast<size_t>(a.ld);
+        if (cudaMalloc(&M->diaBuf, bytes) != cudaSuccess) {
+            cudaGetLastError();  // no room for the copy: the CSR SpMM stays
+            M->diaBuf = nullptr;
+            return CIECU_OK;
+        }
+        CIECU_CUDA(cudaMemsetAsync(M->diaBuf, 0, bytes, st));
+        a.val = M->diaBuf;
+        M->dia = a;
+        const long needed = (M->n + static_cast<long>(kWarps) * (32 / M->kp) - 1) /
+                            (static_cast<long>(kWarps) * (32 / M->kp));
+        with_group(M->kp, [&](auto kk) -> int {
+            constexpr int KP = decltype(kk)::value;
+            M->gridD = std::min(
+                resident_blocks(reinterpret_cast<const void*>(multi_spmv_dia_kernel<KP, true, true>), kT, 0),
+                resident_blocks(reinterpret_cast<const void*>(multi_spmv_dia_kernel<KP, false, true>), kT, 0));
+            return CIECU_OK;
+        });
+        M->gridD = static_cast<int>(std::max<long>(1, std::min<long>(M->gridD, needed)));
+        CIECU_TRY(dia_fill_f64(M->A, M->dia, M->diaBuf, st));
+        cudaEvent_t e0, e1;
+        CIECU_CUDA(cudaEventCreate(&e0));
+        CIECU_CUDA(cudaEventCreate(&e1));
+        float best[2] = {1e30f, 1e30f};
+        cudaError_t e = cudaSuccess;
+        for (int variant = 0; variant < 2 && e == cudaSuccess; ++variant) {
+            const bool dia = variant == 1;
+            launch_multi_residual(M, st, dia, B);
+            for (int trial = 0; trial < 3 && e == cudaSuccess; ++trial) {
+                cudaEventRecord(e0, st);
+                launch_multi_residual(M, st, dia, B);
+                cudaEventRecord(e1, st);
+                e = cudaEventSynchronize(e1);
+                float ms = 0.f;
+                if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+                if (ms < best[variant]) best[variant] = ms;
+            }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (e == cudaSuccess) e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_fail(e, "multi: SpMM format choice");
+        M->useDia = best[1] < best[0];
+        return CIECU_OK;
+    }
+    if (M->diaBuf) CIECU_TRY(dia_fill_f64(M->A, M->dia, M->diaBuf, st));
     return CIECU_OK;
 }
 
@@ -513,6 +670,7 @@ int ciecu_multi_destroy(ciecu_multi M) {
     if (M->h_g) cudaFreeHost(M->h_g);
     cudaFree(M->d_partials);
     cudaFree(M->d_counter);
+    cudaFree(M->diaBuf);
     delete M;
     return CIECU_OK;
 }
@@ -521,6 +679,12 @@ int ciecu_multi_info(ciecu_multi M, int* lanesPerRow, int* deviceLoop) {
     CIECU_REQUIRE(M, "multi_info: null solver");
     if (lanesPerRow) *lanesPerRow = M->kp;
     if (deviceLoop) *deviceLoop = M->deviceLoop ? 1 : 0;
+    return CIECU_OK;
+}
+
+int ciecu_multi_format(ciecu_multi M, int* diagonals) {
+    CIECU_REQUIRE(M && diagonals, "multi_format: null argument");
+    *diagonals = M->useDia ? M->dia.ndiag : 0;
     return CIECU_OK;
 }
 
@@ -539,18 +703,15 @@ int ciecu_multi_product(ciecu_multi M, double inScale, const double* d_in, doubl
         g.relTol = M->settings.relativeResidual;
         *M->h_g = g;
         CIECU_CUDA(cudaMemcpyAsync(M->d_g, M->h_g, sizeof(MultiGlobal), cudaMemcpyHostToDevice, st));
+        CIECU_TRY(prepare_dia(M, st, d_in));
+        CIECU_TRY(launch_multi_residual(M, st, M->useDia, d_in));
         CIECU_TRY(with_group(M->kp, [&](auto kk) -> int {
             constexpr int KP = decltype(kk)::value;
-            if (M->k == KP)
-                multi_residual_kernel<KP, true><<<M->grid, kT, 0, st>>>(M->A->args<double>(), M->k, M->x, d_in, M->r);
-            else
-                multi_residual_kernel<KP, false><<<M->grid, kT, 0, st>>>(M->A->args<double>(), M->k, M->x, d_in,
-                                                                         M->r);
             multi_init_kernel<KP><<<M->gridV, kT, 0, st>>>(n, M->k, M->r, M->dinv, M->p, M->d_s, M->d_g,
                                                           M->d_partials, M->d_counter);
             return CIECU_OK;
         }));
-        count_launch(2);
+        count_launch();
         CIECU_CHECK_LAUNCH("multi-rhs set-up");
         CIECU_TRY(build_multi_graph(M));
         const long long limit = M->deviceLoop ? 4096 : M->chunk;

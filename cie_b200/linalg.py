@@ -739,7 +739,10 @@ class MultiRHSConjugateGradients(LinearOperator):
     def info(self):
         v, d = ctypes.c_int(), ctypes.c_int()
         call("ciecu_multi_info", self._solver, ctypes.byref(v), ctypes.byref(d))
-        return {"lanes_per_row": v.value, "device_loop": bool(d.value)}
+        f = ctypes.c_int()
+        call("ciecu_multi_format", self._solver, ctypes.byref(f))
+        return {"lanes_per_row": v.value, "device_loop": bool(d.value),
+                "spmm_format": "dia-%d" % f.value if f.value else "csr"}
 
     def getStats(self):
         return self._stats

@@ -24,6 +24,11 @@ int ciecu_multi_destroy(ciecu_multi solver);
 /* Lanes per row group (the power of two >= rhsCount) and whether the solve loop
  * runs on the device (conditional graph nodes). */
 int ciecu_multi_info(ciecu_multi solver, int* lanesPerRow, int* deviceLoop);
+/* SpMM format chosen at the first solve: the number of diagonals of the
+ * diagonal-storage copy (a matrix of at most 32 diagonals, see
+ * ciecu_csr_diagonals, whose copy timed faster than the CSR SpMM; the copy is
+ * refilled from the CSR values at every solve), or 0 for the CSR SpMM. */
+int ciecu_multi_format(ciecu_multi solver, int* diagonals);
 /* Initial guesses = d_out (n x k); on return out = inScale*out + outScale*X.
  * h_stats (may be NULL): one ciecu_statistics per right-hand side.  A breakdown
  * returns CIECU_ERR_BREAKDOWN naming the first such right-hand side; the others
