@@ -587,6 +587,7 @@ struct ciecu_pcg_s {
     bool fits = false;        // every block's rows fit in shared memory
     size_t smem = 0;          // dynamic shared memory of the single launch
     int maxRows = 0;          // rows of the largest block
+    int grid = 0;             // blocks of the single launch
     int2* split = nullptr;
     double* z = nullptr;
     double* p2 = nullptr;
@@ -668,33 +669,42 @@ int launch_iteration(ciecu_pcg_s* S, cudaStream_t st, cudaGraphConditionalHandle
     return CIECU_OK;
 }
 
-// Splits the rows into one range per SM (balanced by nonzeros) and sizes the
-// shared memory of the single launch from the largest range.
+// Splits the rows into G ranges (balanced by nonzeros) and sizes the shared
+// memory of the single launch from the largest range.  G is the smallest of
+// SMs/4, SMs/2 and SMs whose ranges fit in shared memory: a grid-wide exchange
+// costs less with fewer blocks (measured on B200 per iteration of 2D Q1 128^2:
+// 10.8 us with 37 blocks, 13.2 us with 74; 2D Q1 256^2: 13.4 us with 74 blocks,
+// 14.6 us with 148).
 int plan_persistent(ciecu_pcg_s* S) {
     if (S->planned) return CIECU_OK;
     ciecu_csr_s* A = S->A;
     cudaStream_t st = A->space->stream;
-    const int G = sm_count();
-    if (!S->split) CIECU_CUDA(cudaMalloc(&S->split, sizeof(int2) * (G + 1)));
-    persistent_split_kernel<<<(G + 1 + 127) / 128, 128, 0, st>>>(A->rowptr, A->rows, A->nnz, G, S->split);
-    count_launch();
-    CIECU_CHECK_LAUNCH("persistent_split_kernel");
-    std::vector<int2> h(G + 1);
-    CIECU_CUDA(cudaMemcpyAsync(h.data(), S->split, sizeof(int2) * (G + 1), cudaMemcpyDeviceToHost, st));
-    CIECU_CUDA(cudaStreamSynchronize(st));
-    size_t smem = 0;
-    int maxRows = 0;
-    for (int b = 0; b < G; ++b) {
-        const long nr = h[b + 1].x - h[b].x, ne = static_cast<long>(h[b + 1].y) - h[b].y;
-        smem = std::max(smem, persistent_smem(ne, nr));
-        maxRows = std::max<int>(maxRows, static_cast<int>(nr));
-    }
     int device = 0, optin = 0;
     CIECU_CUDA(cudaGetDevice(&device));
     CIECU_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
-    S->smem = std::max<size_t>(smem, 16);
-    S->maxRows = maxRows;
-    S->fits = S->smem + 1024 <= static_cast<size_t>(optin);  // 1 KB for the static reduction scratch
+    const int sms = sm_count();
+    if (!S->split) CIECU_CUDA(cudaMalloc(&S->split, sizeof(int2) * (sms + 1)));
+    S->fits = false;
+    for (int G : {std::max(1, sms / 4), std::max(1, sms / 2), sms}) {
+        persistent_split_kernel<<<(G + 1 + 127) / 128, 128, 0, st>>>(A->rowptr, A->rows, A->nnz, G, S->split);
+        count_launch();
+        CIECU_CHECK_LAUNCH("persistent_split_kernel");
+        std::vector<int2> h(G + 1);
+        CIECU_CUDA(cudaMemcpyAsync(h.data(), S->split, sizeof(int2) * (G + 1), cudaMemcpyDeviceToHost, st));
+        CIECU_CUDA(cudaStreamSynchronize(st));
+        size_t smem = 0;
+        int maxRows = 0;
+        for (int b = 0; b < G; ++b) {
+            const long nr = h[b + 1].x - h[b].x, ne = static_cast<long>(h[b + 1].y) - h[b].y;
+            smem = std::max(smem, persistent_smem(ne, nr));
+            maxRows = std::max<int>(maxRows, static_cast<int>(nr));
+        }
+        S->smem = std::max<size_t>(smem, 16);
+        S->maxRows = maxRows;
+        S->grid = G;
+        S->fits = S->smem + 1024 <= static_cast<size_t>(optin);  // 1 KB for the static reduction scratch
+        if (S->fits) break;  // S->split holds this G's ranges
+    }
     S->planned = true;
     return CIECU_OK;
 }
@@ -742,7 +752,7 @@ int launch_persistent(ciecu_pcg_s* S, cudaStream_t st) {
     int occ = 0;
     CIECU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, kPT, S->smem));
     if (occ < 1) return fail(CIECU_ERR_CUDA, "pcg: the single-launch kernel does not fit on an SM");
-    const int G = sm_count();
+    const int G = S->grid;
     ExchangeSlot* slots = static_cast<ExchangeSlot*>(S->slots);
     PersistentArgs args{S->A->args<double>(), S->split, S->dinv, S->x, S->r, S->z, S->p, S->p2,
                         slots, slots + G, S->abortFlag, S->d_s, S->epoch};

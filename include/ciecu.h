@@ -215,9 +215,10 @@ int ciecu_pcg_set_schedule(ciecu_pcg solver, int schedule);
  * kernel, else lanes per row) and how the last solve ran: host-polled graph chunks
  * (0), a device-side graph loop (1) or a single cooperative launch (2). */
 int ciecu_pcg_info(ciecu_pcg solver, int* spmvSchedule, int* deviceLoop);
-/* How the iterations run.  mode 0 (default): a single cooperative launch, one
- * block per SM holding its rows of the matrix in shared memory, when every SM's
- * share fits there, else the graph of three kernels per iteration; 1: always the
+/* How the iterations run.  mode 0 (default): a single cooperative launch of at
+ * most one block per SM (the fewest of SMs/4, SMs/2, SMs that fit), each block
+ * holding its rows of the matrix in shared memory, when the rows fit there at one
+ * block per SM, else the graph of three kernels per iteration; 1: always the
  * graph; 2: always the single launch (CIECU_ERR_ARGUMENT at the next solve when
  * the matrix does not fit).  The single launch gives results within rounding of
  * the graph's (its dot products are summed over another grid); a grid-wide wait
