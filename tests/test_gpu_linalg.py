@@ -2,7 +2,7 @@
 reference's known answers and the oracle on identical seeded inputs.
 
 Tolerances: SpMV per row |y_gpu - y_ref| <= 1e-13 * sum_j |a_ij x_j| (+ the
-|inScale * out| term), the north_star's "1e-13 relative per row"; elementwise
+|inScale * out| term), i.e. 1e-13 relative per row; elementwise
 operations exact or 1 ulp."""
 import numpy as np
 import pytest

@@ -1,7 +1,7 @@
 """GPU parity of the conjugate-gradient solver through the C-ABI against the
 reference's own compiled FP64 CPU solver (oracle/_ref) on identical seeded inputs.
 
-Bar (north_star): at ||r||/||b|| <= 1e-10 the solution is within 1e-9 relative of
+Accuracy bar: at ||r||/||b|| <= 1e-10 the solution is within 1e-9 relative of
 the FP64 oracle's; the iteration count matches the reference's up to the
 last-bit differences of its dot products."""
 import numpy as np
