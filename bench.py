@@ -12,9 +12,10 @@ true FP64 residual) per solve with inputs resident in HBM (inputs are larger tha
 L2, so no flush is needed); the plain FP64 PCG (the drop-in) is timed beside it.
 e2e = the mixed solve through the public API with host buffers (H2D of CSR + RHS
 from pinned memory, operator set-up, solve, D2H of the solution, all timed).
-roofline = the headline's dominant kernel (the FP32 CSR SpMV) timed live with CUDA
-events; the FP64 SpMV and whole-iteration rooflines are reported beside it, and
-the reference's threaded CPU solver is timed on the same system.
+roofline = the headline's dominant kernel (the FP32 inner SpMV: over the diagonal-
+storage copy for this 27-diagonal matrix, else SELL-32) timed live with CUDA
+events; the FP64 CSR operator SpMV and whole-iteration rooflines are reported
+beside it, and the reference's threaded CPU solver is timed on the same system.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cie_b200|reference]
 """
