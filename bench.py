@@ -104,36 +104,59 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_problem_arrays(prob):
-    rp, col, val = prob.host_csr()
-    return rp, col, val, prob.rhs.cpu().numpy()
+def common_config(world):
+    """The config both arms print (the workload, nothing about either solver)."""
+    return dict(WORKLOAD, parallelism="replicas" if world > 1 else "single_gpu")
 
 
-def cpu_reference_sample(rp, col, val, b, full_iterations, budget_s=15.0, threads=None):
-    """The reference's threaded FP64 CG (oracle/_ref) on the same system: a complete
-    solve when it fits the budget, else a bounded number of iterations whose
-    per-iteration time is scaled to the iteration count of a complete solve."""
+def compact(v, digits=4):
+    """Floats rounded to `digits` significant digits, recursively (keeps the line short)."""
+    if isinstance(v, float):
+        return float("%.*g" % (digits, v)) if np.isfinite(v) else v
+    if isinstance(v, dict):
+        return {k: compact(x, digits) for k, x in v.items()}
+    if isinstance(v, (list, tuple)):
+        return [compact(x, digits) for x in v]
+    return v
+
+
+def oracle_system():
+    """The workload's system built on the host by the oracle (no CUDA library):
+    the arrays the reference arm solves."""
+    from oracle.oracle import Restatement, system_digest
+    rp, col, val, b, _, _ = Restatement().poisson_system(3, 1, WORKLOAD["cells"], seed=WORKLOAD["seed"])
+    return (rp, col, val, b), system_digest(rp, col, val, b)
+
+
+def reference_solve(rp, col, val, b, full_iterations, budget_s=15.0, threads=None):
+    """The reference's threaded FP64 CG (oracle/_ref) on the same system.  Returns
+    (cpu_baseline, x_ref, iterations): a complete solve when it is expected to
+    end within max(budget, 120 s) -- its solution then anchors the parity of the
+    GPU solutions -- else a bounded number of iterations scaled to a complete
+    solve (no solution)."""
     from oracle.oracle import Reference, reference_available
     if not reference_available():
-        return None
+        return None, None, None
     ref = Reference(threads=threads)
     try:
         _, _, err, t_probe = ref.pcg(rp, col, val, b, maxit=2, reltol=1e-10)
         per_it = max(t_probe / 3.0, 1e-6)
-        if per_it * (full_iterations + 1) <= budget_s:
-            _, stats, err, t = ref.pcg(rp, col, val, b, maxit=20000, reltol=1e-10)
-            return {"value": t, "unit": "s", "cores": ref.threads, "kind": "reference",
-                    "sample": "one complete solve to 1e-10 (%d iterations, true stop) with the reference's "
-                              "ConjugateGradients<DefaultSpace<double>> + CSROperator + DiagonalOperator compiled "
-                              "from its own sources (oracle/_ref), same system" % int(stats[0]),
-                    "iterations": int(stats[0])}
+        if per_it * (full_iterations + 1) <= max(budget_s, 120.0):
+            x, stats, err, t = ref.pcg(rp, col, val, b, maxit=20000, reltol=1e-10)
+            if err:
+                raise RuntimeError(err)
+            base = {"value": t, "unit": "s", "cores": ref.threads, "kind": "reference",
+                    "sample": "one complete solve to 1e-10 (%d iterations) with the reference's ConjugateGradients"
+                              "<DefaultSpace<double>> + CSROperator + DiagonalOperator built from its sources "
+                              "(oracle/_ref), same system" % int(stats[0])}
+            return base, x, int(stats[0])
         m = int(max(3, budget_s / per_it - 1))
         _, stats, err, t = ref.pcg(rp, col, val, b, maxit=m, reltol=1e-10)
         per_it = t / (stats[0] + 1)
-        return {"value": per_it * (full_iterations + 1), "unit": "s", "cores": ref.threads, "kind": "reference",
-                "sample": "%d CG iterations of the reference's CPU solver (oracle/_ref) on the same system: "
-                          "%.3f s, %.2f ms per iteration, scaled to the %d iterations of a complete solve"
-                          % (stats[0] + 1, t, 1e3 * per_it, full_iterations + 1)}
+        return ({"value": per_it * (full_iterations + 1), "unit": "s", "cores": ref.threads, "kind": "reference",
+                 "sample": "%d CG iterations of the reference's CPU solver (oracle/_ref) on the same system, "
+                           "scaled to the %d iterations of a complete solve" % (stats[0] + 1, full_iterations + 1)},
+                None, None)
     finally:
         ref.close()
 
@@ -141,16 +164,13 @@ def cpu_reference_sample(rp, col, val, b, full_iterations, budget_s=15.0, thread
 def run_reference_arm(args):
     """The reference's own threaded FP64 CPU solver (oracle/_ref: ConjugateGradients<
     DefaultSpace<double>> + CSROperator + DiagonalOperator over mp::ThreadPoolBase with
-    every host thread) on the same seeded system; each step is a complete solve."""
+    every host thread) on the workload's system, built on the host by the oracle
+    (bit-identical to the GPU-assembled one: same digest); each step is a complete
+    solve.  No CUDA library is loaded on this arm."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    from cie_b200.fem import make_poisson
-    from cie_b200.linalg import CUDASpace
-    space = CUDASpace()  # builds the identical system (GPU assembly, untimed)
-    prob = make_poisson(space, 3, 1, WORKLOAD["cells"], seed=WORKLOAD["seed"])
-    rp, col, val, b = cpu_problem_arrays(prob)
-    del prob, space
+    (rp, col, val, b), digest = oracle_system()
     from oracle.oracle import Reference
     ref = Reference()
     times, its = [], []
@@ -165,13 +185,14 @@ def run_reference_arm(args):
     value = statistics.median(times)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * value, "higher_is_better": False,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-            "config": dict(WORKLOAD, parallelism="replicas", iterations=its[-1]),
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded mt19937_64 RHS and "
+            "kappa field)", "config": common_config(world),
+            "system_digest": digest, "iterations": its[-1],
             "cpu_baseline": {"value": value, "unit": "s", "cores": ref.threads, "kind": "reference",
                              "sample": "each step: one complete solve to 1e-10 (%d iterations) with the reference's "
-                                       "CPU solver compiled from its own sources (oracle/_ref)" % its[-1]},
+                                       "CPU solver built from its own sources (oracle/_ref)" % its[-1]},
             "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line), flush=True)
+    print(json.dumps(compact(line, 6)), flush=True)
 
 
 def main():
@@ -234,9 +255,37 @@ def main():
     cells = [args.profile_cells] * 3 if args.profile else WORKLOAD["cells"]
     prob = make_poisson(space, 3, 1, cells, seed=WORKLOAD["seed"])
     n, nnz = prob.mesh.ndofs, prob.matrix.nnz()
+    settings = Statistics(20000, 0.0, WORKLOAD["tolerance"])
+    if not args.profile:
+        # host copies of the system (pinned) for the end-to-end runs and the CPU leg
+        rp_h, col_h, val_h = [t.cpu().pin_memory() for t in (prob.matrix.rowExtents, prob.matrix.columnIndices,
+                                                              prob.matrix.entries)]
+        rhs_h = prob.rhs.cpu().pin_memory()
+        sol_h = torch.empty(n, dtype=torch.float64).pin_memory()
+
+        def e2e_solve():
+            """The public API with host buffers: H2D of the CSR arrays and RHS, operator
+            and solver set-up, the mixed solve, D2H of the solution."""
+            m = CSRMatrix(n, rp_h.to("cuda", non_blocking=True), col_h.to("cuda", non_blocking=True),
+                          val_h.to("cuda", non_blocking=True))
+            b = rhs_h.to("cuda", non_blocking=True)
+            A2 = CSROperator(m, space)
+            D2 = makeDiagonalOperator(m, space, csr_handle=A2.csr)
+            M2 = MixedPrecisionCG(A2, D2, settings, mode=0, delta=DELTA)
+            xe = torch.zeros(n, dtype=torch.float64, device="cuda")
+            M2.product(0.0, b, 1.0, xe)
+            sol_h.copy_(xe, non_blocking=True)
+            torch.cuda.synchronize()
+            del M2, D2, A2, m
+
+        # first call of the process on a matrix of this shape: includes the one-off
+        # autotuning and the build of the inner-matrix copy, cached per shape after it
+        barrier()
+        t0 = time.perf_counter()
+        e2e_solve()
+        e2e_cold = time.perf_counter() - t0
     A = CSROperator(prob.matrix, space)
     D = makeDiagonalOperator(prob.matrix, space, csr_handle=A.csr)
-    settings = Statistics(20000, 0.0, WORKLOAD["tolerance"])
     cg = ConjugateGradients(A, space, D, settings)
     if args.profile and args.pin:
         pin_fp64, pin_unroll, pin_csr = (int(v) for v in args.pin.split(","))
@@ -369,28 +418,13 @@ def main():
             traffic = int(figures.get("mixed_apply_kernel_f32_sell16", 0)) or None
         traffic64 = int(figures.get("spmv_kernel_f64_csr", 0)) or None
 
-    # end to end through the public API with host buffers
-    rp_h, col_h, val_h = [t.cpu().pin_memory() for t in (prob.matrix.rowExtents, prob.matrix.columnIndices,
-                                                          prob.matrix.entries)]
-    rhs_h = prob.rhs.cpu().pin_memory()
-    sol_h = torch.empty(n, dtype=torch.float64).pin_memory()
+    # end to end through the public API with host buffers (warm: the shape's tuning is cached)
     e2e_times = []
-    for step in range(2 + max(1, min(args.steps, 3))):
+    for step in range(max(1, min(args.steps, 3))):
         barrier()
         t0 = time.perf_counter()
-        m = CSRMatrix(n, rp_h.to("cuda", non_blocking=True), col_h.to("cuda", non_blocking=True),
-                      val_h.to("cuda", non_blocking=True))
-        b = rhs_h.to("cuda", non_blocking=True)
-        A2 = CSROperator(m, space)
-        D2 = makeDiagonalOperator(m, space, csr_handle=A2.csr)
-        M2 = MixedPrecisionCG(A2, D2, settings, mode=0, delta=DELTA)
-        xe = torch.zeros(n, dtype=torch.float64, device="cuda")
-        M2.product(0.0, b, 1.0, xe)
-        sol_h.copy_(xe, non_blocking=True)
-        torch.cuda.synchronize()
-        if step >= 2:
-            e2e_times.append(time.perf_counter() - t0)
-        del M2, D2, A2, m
+        e2e_solve()
+        e2e_times.append(time.perf_counter() - t0)
     e2e = statistics.median(e2e_times)
     h2d = 4 * (n + 1) + 12 * nnz + 8 * n
     d2h = 8 * n
@@ -407,56 +441,67 @@ def main():
     if not args.no_extra:
         extra = extra_workloads(space, A, D, settings, t_fp64, it64, rank, world)
 
-    cpu = None
+    # CPU leg (rank 0): the oracle rebuilds the system on the host without the CUDA
+    # library (the reference arm's input; same digest = same bits), the reference's
+    # threaded CPU CG solves it, and its solution anchors the parity of both GPU solves
+    cpu = parity = None
     if rank == 0 and not args.no_cpu:
-        rp, col, val, bh = cpu_problem_arrays(prob)
-        cpu = cpu_reference_sample(rp, col, val, bh, it64, budget_s=args.cpu_budget)
+        rp, col, val, bh = (t.numpy() for t in (rp_h, col_h, val_h, rhs_h))
+        from oracle.oracle import system_digest
+        digest = system_digest(rp, col, val, bh)
+        (orp, ocol, oval, ob), odigest = oracle_system()
+        same = digest == odigest
+        cpu, x_ref, it_ref = reference_solve(orp, ocol, oval, ob, it64, budget_s=args.cpu_budget)
+        parity = {"system_digest": digest, "oracle_system_digest": odigest, "bit_identical_to_oracle": same}
+        if not same:
+            parity["max_entry_rel_diff"] = float(np.abs(val - oval).max() / np.abs(oval).max())
+        del orp, ocol, oval, ob
+        if x_ref is not None:
+            xr = np.linalg.norm(x_ref)
+            parity.update({"reference_iterations": it_ref,
+                           "mixed_rel_err_vs_reference": float(np.linalg.norm(xmx.cpu().numpy() - x_ref) / xr),
+                           "fp64_rel_err_vs_reference": float(np.linalg.norm(x64.cpu().numpy() - x_ref) / xr)})
 
     if rank == 0:
         g32 = spmv32_bytes / t_spmv32 / 1e9
+        # key order: the long blocks first, the headline blocks last (the end of the
+        # line is what a log tail shows)
         line = {
             "metric": METRIC, "value": t_mixed, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * t_mixed, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 inner / f64 refinement",
             "data": "synthetic (seeded mt19937_64 RHS and kappa field)",
-            "config": dict(WORKLOAD, parallelism="replicas" if world > 1 else "single_gpu",
-                           solver="mixed-precision jacobi-pcg, reliable updates delta=%g" % DELTA,
-                           inner_format=info["format"], fp64_k1="dia" if dia64 else "csr"),
-            "mixed": {"seconds": t_mixed, "inner_iterations": mst.innerIterations,
-                      "refinements": mst.refinements, "true_relative_residual": rel_mixed,
-                      "rel_diff_vs_fp64_solution": agree,
-                      "achieved_gbs": mixed_solve_bytes / t_mixed / 1e9},
-            "fp64": {"seconds": t_fp64, "iterations": it64, "true_relative_residual": rel_fp64,
-                     "spmv_schedule": cg.info().get("spmv_schedule"), "device_loop": cg.info().get("device_loop"),
-                     "achieved_gbs": fp64_solve_bytes / t_fp64 / 1e9,
-                     "us_per_iteration": 1e6 * t_fp64 / (it64 + 1)},
-            "speedup_mixed_vs_fp64": t_fp64 / t_mixed,
-            "roofline": {"bound": "hbm", "kernel": (
-                             "mixed_apply_dia_kernel (FP32 DIA SpMV, %d diagonals, %d stored entries for %d "
-                             "nonzeros)" % (ndiag, ndiag * n, nnz)) if dia32 else (
-                             "%s (FP32 SELL-32 SpMV, %s columns, %d stored entries for %d nonzeros)" % (
-                                 "mixed_apply_kernel<%d>" % info["group_unroll"] if info["group_unroll"] > 0
-                                 else "mixed_apply_tma_kernel", "16-bit" if info["compressed_columns"] else "int32",
-                                 info["padded_entries"], nnz)),
-                         "achieved": g32, "peak": hbm, "unit": "GB/s", "frac": g32 / hbm, "peak_kind": peak_kind,
-                         "traffic": traffic, "algorithmic_bytes": spmv32_bytes, "launch_ms": 1e3 * t_spmv32},
+            "config": common_config(world),
+            "solver": {"mixed": "jacobi-pcg, FP32 inner over %s, FP64 reliable updates delta=%g" % (info["format"],
+                                                                                                  DELTA),
+                       "fp64": "jacobi-pcg over %s" % ("dia" if dia64 else "csr")},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+            "workloads": extra,
             "fp64_spmv_roofline": {"kernel": "spmv_kernel (FP64 CSR, schedule %d)" % A.csr.kernel(),
                                    "achieved": spmv64_bytes / t_spmv64 / 1e9, "peak": hbm,
                                    "frac": spmv64_bytes / t_spmv64 / 1e9 / hbm, "algorithmic_bytes": spmv64_bytes,
-                                   "traffic": traffic64,
-                                   "launch_ms": 1e3 * t_spmv64},
-            "pcg_iteration_roofline": {"fp64_frac": fp64_solve_bytes / t_fp64 / 1e9 / hbm,
-                                       "mixed_frac": mixed_solve_bytes / t_mixed / 1e9 / hbm,
-                                       "fp64_bytes_per_iteration": iter64_bytes,
-                                       "mixed_inner_bytes_per_iteration": inner_bytes},
-            "clocks": clocks,
-            "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "solver": "mixed"},
-            "gpu_launches": int(launches),
+                                   "traffic": traffic64, "launch_ms": 1e3 * t_spmv64},
             "cpu_baseline": cpu,
-            "workloads": extra,
+            "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "cold_first_call_s": e2e_cold, "solver": "mixed"},
+            "fp64": {"seconds": t_fp64, "iterations": it64, "true_relative_residual": rel_fp64,
+                     "us_per_iteration": 1e6 * t_fp64 / (it64 + 1), "achieved_gbs": fp64_solve_bytes / t_fp64 / 1e9},
+            "mixed": {"seconds": t_mixed, "inner_iterations": mst.innerIterations,
+                      "refinements": mst.refinements, "true_relative_residual": rel_mixed,
+                      "rel_diff_vs_fp64_solution": agree, "achieved_gbs": mixed_solve_bytes / t_mixed / 1e9},
+            "speedup_mixed_vs_fp64": t_fp64 / t_mixed,
+            "pcg_iteration_roofline": {"fp64_frac": fp64_solve_bytes / t_fp64 / 1e9 / hbm,
+                                       "mixed_frac": mixed_solve_bytes / t_mixed / 1e9 / hbm},
+            "parity": parity,
+            "roofline": {"bound": "hbm", "kernel": (
+                             "mixed_apply_dia_kernel (FP32 DIA SpMV, %d diagonals)" % ndiag) if dia32 else (
+                             "%s (FP32 SELL-32 SpMV)" % ("mixed_apply_kernel<%d>" % info["group_unroll"]
+                                                         if info["group_unroll"] > 0 else "mixed_apply_tma_kernel")),
+                         "achieved": g32, "peak": hbm, "unit": "GB/s", "frac": g32 / hbm, "peak_kind": peak_kind,
+                         "traffic": traffic, "algorithmic_bytes": spmv32_bytes, "launch_ms": 1e3 * t_spmv32},
         }
-        print(json.dumps(line), flush=True)
+        print(json.dumps(compact(line)), flush=True)
     if world > 1:
         dist.destroy_process_group()
 

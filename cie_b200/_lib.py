@@ -83,6 +83,7 @@ SIGNATURES = {
     "ciecu_pcg_set_schedule": (c_int, [P, c_int]),
     "ciecu_pcg_info": (c_int, [P, P, P]),
     "ciecu_pcg_set_loop": (c_int, [P, c_int]),
+    "ciecu_pcg_debug_exchange": (c_int, [P, c_int64, c_int64]),
     "ciecu_mixed_create": (c_int, [P, P, Statistics, MixedOptions, P]),
     "ciecu_mixed_destroy": (c_int, [P]),
     "ciecu_mixed_info": (c_int, [P, P, P]),

@@ -164,7 +164,9 @@ __global__ void stiffness_scatter_kernel(long count, int nb, int dim, int nq, co
             s = fma(s_w[q], gg, s);
         }
         const int slot = slots[static_cast<long>(e) * nb2 + ab];
-        val[slot] += kappa[e] * scale * s;
+        // one rounding per contribution, written out so that the host restatement
+        // of this summation order reproduces the matrix bit for bit
+        val[slot] = fma(kappa[e] * scale, s, val[slot]);
     }
 }
 

@@ -52,6 +52,14 @@ __device__ __forceinline__ T stream_ld(const T* p) {
     return __ldcs(p);
 }
 
+// Nanoseconds of the GPU's global timer: a bound on a wait in wall-clock time,
+// independent of the SM clock and of the SM the thread runs on.
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 // ---- reductions ------------------------------------------------------------
 
 template <typename T>

@@ -7,9 +7,11 @@
 // consecutive rows are consecutive addresses.
 //
 // Row sums run over the diagonals in ascending offset order, i.e. in the
-// column order of the CSR row, one FMA per diagonal (a padded zero adds
-// nothing), so they equal the sequential CSR-order FMA sums of
-// CSROperator.cpp:49-56 up to the sign of zero.
+// column order of the CSR row, one FMA per diagonal.  For finite x a padded zero
+// adds nothing, so the sums equal the sequential CSR-order FMA sums of
+// CSROperator.cpp:49-56 up to the sign of zero.  When x holds an Inf or NaN at
+// a column a padded zero points to, 0 * Inf gives NaN in that row where the CSR
+// sum, which never touches that column, stays finite.
 //
 // The CSR view stays the source of truth: the offsets are found once per CSR
 // handle (the pattern is fixed for its lifetime, as the row-block schedule

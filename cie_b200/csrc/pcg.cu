@@ -253,13 +253,12 @@ __global__ void __launch_bounds__(kT) pcg_direction_kernel(long n, double* __res
 // acquire fence) and sums the partials in block order, so all blocks hold
 // bit-identical scalars and take the same branches.  Global vectors written
 // during the launch are read with ld.global.cg (L2), never through the
-// non-coherent L1 or texture paths.  Every wait is bounded (kExchangeWaitCycles
-// SM clock cycles, 2 to 4 s); a wait that gives up sets the abort flag, every
+// non-coherent L1 or texture paths.  Every wait is bounded in time (2 s of the
+// GPU's global timer by default); a wait that gives up sets the abort flag, every
 // block leaves, and the host reports CIECU_ERR_TIMEOUT.  One exchange costs about
 // 5 us on B200 (148 blocks), about a quarter of what three launches per
 // iteration cost together.
 constexpr int kPT = 1024;
-constexpr long long kExchangeWaitCycles = 4000000000LL;
 
 struct alignas(32) ExchangeSlot {
     double v[2];
@@ -281,6 +280,8 @@ struct PersistentArgs {
     int* abortFlag;
     PcgScalars* s;
     unsigned long long epoch0;
+    long long waitNs;                   // bound of one exchange wait
+    unsigned long long withholdEpoch;   // test hook: the last block never publishes this epoch (0: none)
 };
 
 // Shared memory of a block with ne entries and nr rows: doubles (values, then x,
@@ -306,11 +307,12 @@ __device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_re
 // wait gave up or another block aborted; the block then leaves the launch.
 template <int K>
 __device__ bool grid_exchange(const double (&mine)[K], ExchangeSlot* slots, unsigned long long epoch,
-                              int* abortFlag, double (&out)[K], double* s_red) {
+                              const PersistentArgs& P, double (&out)[K], double* s_red) {
+    int* abortFlag = P.abortFlag;
     double sums[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) sums[k] = block_sum<double, kPT>(mine[k], s_red);  // orders the block's stores
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 0 && !(epoch == P.withholdEpoch && blockIdx.x == gridDim.x - 1)) {
         ExchangeSlot* m = slots + blockIdx.x;
 #pragma unroll
         for (int k = 0; k < K; ++k) m->v[k] = sums[k];
@@ -322,12 +324,13 @@ __device__ bool grid_exchange(const double (&mine)[K], ExchangeSlot* slots, unsi
     bool ok = true;
     for (unsigned b = threadIdx.x; b < gridDim.x && ok; b += kPT) {
         const ExchangeSlot* o = slots + b;
-        const long long t0 = clock64();
+        const unsigned long long t0 = global_ns();
         unsigned spin = 0;
         while (ld_relaxed_u64(&o->epoch) != epoch) {
             __nanosleep(20);
             if ((++spin & 63u) == 0u &&
-                (*reinterpret_cast<volatile int*>(abortFlag) || clock64() - t0 > kExchangeWaitCycles)) {
+                (*reinterpret_cast<volatile int*>(abortFlag) ||
+                 global_ns() - t0 > static_cast<unsigned long long>(P.waitNs))) {
                 atomicExch(abortFlag, 1);
                 ok = false;
                 break;
@@ -453,7 +456,7 @@ __global__ void __launch_bounds__(kPT, 1) pcg_persistent_kernel(PersistentArgs P
         }
         {
             double mine[1] = {pqPart}, tot[1];
-            if (!grid_exchange<1>(mine, P.slotsS, ++epoch, P.abortFlag, tot, s_red)) {
+            if (!grid_exchange<1>(mine, P.slotsS, ++epoch, P, tot, s_red)) {
                 aborted = true;
                 break;
             }
@@ -485,7 +488,7 @@ __global__ void __launch_bounds__(kPT, 1) pcg_persistent_kernel(PersistentArgs P
         }
         {
             double mine[2] = {rrPart, rzPart}, tot[2];
-            if (!grid_exchange<2>(mine, P.slotsU, ++epoch, P.abortFlag, tot, s_red)) {
+            if (!grid_exchange<2>(mine, P.slotsU, ++epoch, P, tot, s_red)) {
                 aborted = true;
                 break;
             }
@@ -594,6 +597,9 @@ struct ciecu_pcg_s {
     void* slots = nullptr;  // 2 x SMs exchange slots
     int* abortFlag = nullptr;
     unsigned long long epoch = 1;
+    long long waitNs = 2000000000LL;  // bound of one grid-wide exchange wait (global timer)
+    long long withholdExchange = 0;   // test hook of the timeout path (ciecu_pcg_debug_exchange)
+    bool pinned = false;              // K1 schedule pinned by ciecu_pcg_set_schedule
 };
 
 namespace ciecu {
@@ -712,6 +718,9 @@ int plan_persistent(ciecu_pcg_s* S) {
 int use_persistent(ciecu_pcg_s* S, bool* out) {
     *out = false;
     if (S->loopMode == 1) return CIECU_OK;
+    // A pinned K1 schedule names a kernel of the graph loop: in the automatic mode
+    // it selects that loop, so the pin takes effect.
+    if (S->loopMode == 0 && S->pinned) return CIECU_OK;
     CIECU_TRY(plan_persistent(S));
     if (S->loopMode == 2 && !S->fits)
         return fail(CIECU_ERR_ARGUMENT, "pcg: the single-launch solve needs each SM's rows of the matrix in shared "
@@ -755,7 +764,9 @@ int launch_persistent(ciecu_pcg_s* S, cudaStream_t st) {
     const int G = S->grid;
     ExchangeSlot* slots = static_cast<ExchangeSlot*>(S->slots);
     PersistentArgs args{S->A->args<double>(), S->split, S->dinv, S->x, S->r, S->z, S->p, S->p2,
-                        slots, slots + G, S->abortFlag, S->d_s, S->epoch};
+                        slots, slots + G, S->abortFlag, S->d_s, S->epoch, S->waitNs,
+                        S->withholdExchange > 0 ? S->epoch + static_cast<unsigned long long>(S->withholdExchange)
+                                                : 0ULL};
     void* params[] = {&args};
     CIECU_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kernel), dim3(G), dim3(kPT), params,
                                            S->smem, st));
@@ -1015,6 +1026,17 @@ int ciecu_pcg_set_schedule(ciecu_pcg S, int schedule) {
                       schedule == 16 || schedule == 32 || schedule == kDiaSchedule,
                   "pcg_set_schedule: schedule must be 0 (autotune), 1, 2, 4, 8, 16, 32 or 64 (DIA)");
     S->kernel = schedule;  // the graph is rebuilt when it was built for another schedule
+    S->pinned = schedule != 0;
+    return CIECU_OK;
+}
+
+int ciecu_pcg_debug_exchange(ciecu_pcg S, int64_t waitNanoseconds, int64_t withholdExchange) {
+    CIECU_REQUIRE(S, "pcg_debug_exchange: null solver");
+    CIECU_REQUIRE(waitNanoseconds >= 1000 && waitNanoseconds <= 60000000000LL,
+                  "pcg_debug_exchange: the wait limit must be in [1 us, 60 s]");
+    CIECU_REQUIRE(withholdExchange >= 0, "pcg_debug_exchange: negative exchange index");
+    S->waitNs = waitNanoseconds;
+    S->withholdExchange = withholdExchange;
     return CIECU_OK;
 }
 

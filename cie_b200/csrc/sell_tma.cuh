@@ -6,8 +6,8 @@
 // each) wait for the current stage, gather x and accumulate.  Streaming the
 // matrix no longer waits on the gather/FMA chain of the rows.
 //
-// Every wait is bounded: a stage that does not complete within kMbarSpins polls
-// sets *errorFlag, the warp waits (bounded again) for its copies still in flight
+// Every wait is bounded: a stage that does not complete within kMbarWaitNs
+// nanoseconds of the global timer sets *errorFlag, the warp waits (bounded again) for its copies still in flight
 // and leaves; the caller reports the flag.  No multicast: each CTA reads only the
 // slices it processes.
 #pragma once
@@ -18,7 +18,7 @@ namespace ciecu {
 
 constexpr int kTmaWarps = 16;   // warps per CTA (one CTA per SM: shared memory bound)
 constexpr int kTmaChunk = 4;    // groups of four entries per row per stage
-constexpr long long kMbarSpins = 1LL << 24;
+constexpr unsigned long long kMbarWaitNs = 2000000000ULL;  // 2 s
 
 template <typename V, typename CI>
 struct TmaShape {
@@ -59,9 +59,11 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
 }
 
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
-    for (long long spins = 0; spins < kMbarSpins; ++spins)
+    const unsigned long long t0 = global_ns();
+    for (unsigned spins = 1;; ++spins) {
         if (mbar_try_wait(bar, parity)) return true;
-    return false;
+        if ((spins & 255u) == 0u && global_ns() - t0 > kMbarWaitNs) return false;
+    }
 }
 
 // Global -> shared bulk copy completing on `bar` (16-byte aligned addresses, size

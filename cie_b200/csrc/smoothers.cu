@@ -8,6 +8,8 @@
 #include "spmv.cuh"
 #include "space.cuh"
 
+#include <cuda.h>
+
 #include <mutex>
 #include <string>
 
@@ -210,24 +212,57 @@ __global__ void __launch_bounds__(csr_threads<KERNEL>())
 }
 
 // Device address of g_jacobiStaticScratch on `device` (which must be current),
-// looked up on the first call for that device and remembered.  Allocates nothing.
+// looked up on the first call for that device and remembered together with the
+// identity of the current context.  A reset of the device (cudaDeviceReset or a
+// primary-context reset) loads the library's device image again, possibly at
+// another address; the new context has another identity, so the address is
+// looked up again.  Allocates nothing.
 constexpr int kStaticScratchDevices = 64;
 
+// The two driver calls are fetched through the runtime, so the library keeps no
+// link-time dependency on the driver library.
+int current_context_id(unsigned long long* id) {
+    using GetCurrent = CUresult (*)(CUcontext*);
+    using GetId = CUresult (*)(CUcontext, unsigned long long*);
+    static GetCurrent getCurrent = nullptr;
+    static GetId getId = nullptr;
+    *id = 0;
+    if (!getCurrent || !getId) {
+        void* f = nullptr;
+        void* g = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, nullptr) != cudaSuccess || !f ||
+            cudaGetDriverEntryPoint("cuCtxGetId", &g, cudaEnableDefault, nullptr) != cudaSuccess || !g)
+            return 0;
+        getCurrent = reinterpret_cast<GetCurrent>(f);
+        getId = reinterpret_cast<GetId>(g);
+    }
+    CUcontext ctx = nullptr;
+    if (getCurrent(&ctx) != CUDA_SUCCESS || ctx == nullptr) return 0;
+    return getId(ctx, id) == CUDA_SUCCESS ? 1 : 0;
+}
+
 int jacobi_static_scratch(int device, double** out) {
+    struct Entry {
+        unsigned long long context;
+        double* address;
+    };
     static std::mutex mutex;
-    static double* table[kStaticScratchDevices] = {};
+    static Entry table[kStaticScratchDevices] = {};
     if (device < 0 || device >= kStaticScratchDevices)
         return fail(CIECU_ERR_ARGUMENT, "jacobi_f64_static: device ordinal " + std::to_string(device) +
                                             " is beyond the " + std::to_string(kStaticScratchDevices) +
                                             " devices this entry point supports");
     std::lock_guard<std::mutex> lock(mutex);
-    if (!table[device]) {
+    unsigned long long context = 0;
+    const int known = current_context_id(&context);
+    if (!table[device].address || !known || table[device].context != context) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_jacobiStaticScratch);
         if (e != cudaSuccess) return cuda_fail(e, "jacobi_f64_static: cudaGetSymbolAddress(static scratch)");
-        table[device] = static_cast<double*>(p);
+        current_context_id(&context);  // the lookup made the device's context current
+        table[device] = Entry{context, static_cast<double*>(p)};
     }
-    *out = table[device];
+    *out = table[device].address;
     return CIECU_OK;
 }
 

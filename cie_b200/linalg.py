@@ -456,6 +456,13 @@ class ConjugateGradients(LinearOperator):
         if self._solver is not None:
             call("ciecu_pcg_set_loop", self._solver, int(mode))
 
+    def debug_exchange(self, waitNanoseconds=2_000_000_000, withholdExchange=0):
+        """Test hook of the single-launch solve's bounded waits (ciecu_pcg_debug_exchange):
+        the wait limit in nanoseconds and an exchange at which the last block
+        withholds its partial sums (0: none), which makes the solve time out."""
+        if self._solver is not None:
+            call("ciecu_pcg_debug_exchange", self._solver, int(waitNanoseconds), int(withholdExchange))
+
     def info(self):
         """SpMV schedule chosen for the fused solver kernel and how the last solve
         ran (fused device solver only)."""

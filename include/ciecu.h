@@ -161,7 +161,9 @@ int ciecu_jacobi_f64(ciecu_csr csr, const double* d_inverse, const uint16_t* d_m
  * row schedule then follows from the mean row length).
  * The first call on a device looks up the array's device address once, with
  * that device current (it must be the matrix's device): make the first call
- * before any stream capture.  All calls on a device share the one array, which
+ * before any stream capture.  The address is remembered with the identity of the
+ * device's context; after a reset of the device (cudaDeviceReset) the next call
+ * looks it up again, so that call too belongs before any capture.  All calls on a device share the one array, which
  * keeps the last call's contents; every iterate is written in full before it is
  * read, so nothing has to start at zero.  Calls that overlap on the GPU (other
  * streams, other host threads, other matrices on the same device) race on the
@@ -208,7 +210,9 @@ int ciecu_pcg_set_graph_chunk(ciecu_pcg solver, int iterations);
  * every solve) instead of autotuning it at the first solve; 0 returns to
  * autotuning.  For runs whose timings would mislead the autotuner (under a
  * profiler).  A pinned 64 on a matrix without a diagonal copy fails at the solve
- * with CIECU_ERR_ARGUMENT. */
+ * with CIECU_ERR_ARGUMENT.  The schedules are kernels of the graph loop: with the
+ * loop mode 0 a pinned schedule (non-zero) selects the graph loop, and with mode 2
+ * (single launch) the pin has no effect. */
 int ciecu_pcg_set_schedule(ciecu_pcg solver, int schedule);
 /* SpMV schedule the solver's autotuner chose for its fused q = A p kernel (0 before
  * the first solve or when the solve ran as a single launch; 1 = row-block stream
@@ -224,6 +228,14 @@ int ciecu_pcg_info(ciecu_pcg solver, int* spmvSchedule, int* deviceLoop);
  * the graph's (its dot products are summed over another grid); a grid-wide wait
  * that gives up fails with CIECU_ERR_TIMEOUT. */
 int ciecu_pcg_set_loop(ciecu_pcg solver, int mode);
+/* Controls the bounded waits of the single-launch solve, for tests of its timeout
+ * path (no counterpart in the reference).  waitNanoseconds bounds each grid-wide
+ * exchange wait in global-timer nanoseconds (default 2 s; [1 us, 60 s]);
+ * withholdExchange > 0 makes the last block skip publishing its partial sums at
+ * that exchange of the next launches (counted from 1), so every wait on it runs
+ * out, the launch ends and the solve fails with CIECU_ERR_TIMEOUT; 0 (default)
+ * publishes normally.  The solver stays usable after a timeout. */
+int ciecu_pcg_debug_exchange(ciecu_pcg solver, int64_t waitNanoseconds, int64_t withholdExchange);
 
 #ifdef __cplusplus
 }

@@ -54,6 +54,11 @@ class Restatement:
             "ora_element_gradient": (None, [_l, _i, _P, _P, _P, _P, _P]),
             "ora_dirichlet_eliminate": (None, [_i, _P, _P, _P, _P, _P]),
             "ora_cut_cell_points": (_i, [_i, _i, _i, _P, _d, _P, _P, _i, _P, _P, _P, _d]),
+            "ora_random_uniform": (None, [_u64, _l, _P]),
+            "ora_random_normal": (None, [_u64, _l, _P]),
+            "ora_kappa_field": (None, [_u64, _i, _P, _d, _i, _P]),
+            "ora_structured_boundary": (None, [_i, _i, _P, _P]),
+            "ora_assemble_structured": (_i, [_i, _i, _i, _P, _P, _P, _P, _P, _P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -173,6 +178,67 @@ class Restatement:
                                        maxPoints, p(pts), p(w), p(s), alpha)
         assert n >= 0
         return pts[: n * dim].reshape(n, dim), w[:n], s[:n]
+
+    # -- seeded workload inputs --
+    def random_uniform(self, seed, n):
+        out = np.zeros(int(n))
+        self.L.ora_random_uniform(int(seed), int(n), p(out))
+        return out
+
+    def random_normal(self, seed, n):
+        out = np.zeros(int(n))
+        self.L.ora_random_normal(int(seed), int(n), p(out))
+        return out
+
+    def kappa_field(self, seed, cells, sigma=1.0, truncation=3):
+        cells = np.ascontiguousarray(cells, dtype=np.int32)
+        out = np.zeros(int(np.prod(cells)))
+        self.L.ora_kappa_field(int(seed), len(cells), p(cells), float(sigma), int(truncation), p(out))
+        return out
+
+    def structured_boundary(self, dim, order, cells):
+        cells = np.ascontiguousarray(cells, dtype=np.int32)
+        n = int(np.prod(order * cells + 1))
+        out = np.zeros(n, dtype=np.uint8)
+        self.L.ora_structured_boundary(dim, order, p(cells), p(out))
+        return out
+
+    def poisson_system(self, dim, order, cells, seed=0, kappa="lognormal", kappa_seed=None):
+        """The seeded Poisson system of the workloads, built on the host without the
+        CUDA library: structured Q_order grid of the unit box, CSR pattern, element
+        stiffness scattered in the GPU's colour and summation order (reference
+        convention), symmetric Dirichlet elimination, RHS uniform [-1, 1] (seed),
+        kappa = 1 or the smoothed log-normal field (seed + 1 unless kappa_seed).
+        Returns (rowptr, col, val, rhs, isBoundary, kappa)."""
+        cells = np.ascontiguousarray(cells, dtype=np.int32)
+        assert len(cells) == dim
+        dofmap = self.structured_dofmap(dim, order, cells)
+        ndofs = int(np.prod(order * cells.astype(np.int64) + 1))
+        nb = (order + 1) ** dim
+        rowptr, col = self.csr_pattern(int(np.prod(cells)), nb, dofmap, ndofs)
+        if isinstance(kappa, str) and kappa == "lognormal":
+            k = self.kappa_field(seed + 1 if kappa_seed is None else kappa_seed, cells)
+        elif isinstance(kappa, str) and kappa == "one":
+            k = np.ones(int(np.prod(cells)))
+        else:
+            k = np.ascontiguousarray(kappa, dtype=np.float64)
+        val = np.zeros(len(col))
+        st = self.L.ora_assemble_structured(dim, order, order + 1, p(cells), p(dofmap), p(k), p(rowptr), p(col),
+                                            p(val))
+        assert st == 0, "element entry missing from the pattern"
+        rhs = self.random_uniform(seed, ndofs)
+        bnd = self.structured_boundary(dim, order, cells)
+        self.L.ora_dirichlet_eliminate(ndofs, p(rowptr), p(col), p(val), p(bnd), p(rhs))
+        return rowptr, col, val, rhs, bnd, k
+
+
+def system_digest(rowptr, col, val, rhs):
+    """SHA-256 (first 16 hex digits) over the bytes of a CSR system and its RHS."""
+    import hashlib
+    h = hashlib.sha256()
+    for a, t in ((rowptr, np.int32), (col, np.int32), (val, np.float64), (rhs, np.float64)):
+        h.update(np.ascontiguousarray(a, dtype=t).tobytes())
+    return h.hexdigest()[:16]
 
 
 class Reference:

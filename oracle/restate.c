@@ -611,3 +611,222 @@ int ora_cut_cell_points(int dim, int depth, int order, const double* center, dou
     return cut_visit(dim, 0, depth, base, 2.0, order, gn, gw, center, radius, cellOrigin, cellSize,
                      maxPoints, 0, points, weights, scales, alpha);
 }
+
+/* ---- seeded workload inputs ------------------------------------------------
+ * The benchmark and parity systems are built from seeded host arrays.  These
+ * functions regenerate them without the CUDA library, so that the reference's CPU
+ * solver can run on exactly the system the GPU solves.  They restate published
+ * algorithms (64-bit Mersenne Twister, Box-Muller) and the workload definition
+ * (uniform ((x >> 11) 2^-53) 2 - 1; kappa = exp of a smoothed, standardised
+ * Gaussian field), not reference code. */
+
+/* MT19937-64 (Matsumoto and Nishimura, ACM TOMACS 1998; Nishimura 2000), the
+ * engine of std::mt19937_64: state of 312 words, default seeding
+ * x_i = 6364136223846793005 (x_{i-1} ^ (x_{i-1} >> 62)) + i. */
+typedef struct {
+    uint64_t mt[312];
+    int index;
+} ora_mt64;
+
+static void mt64_seed(ora_mt64* g, uint64_t seed) {
+    g->mt[0] = seed;
+    for (int i = 1; i < 312; ++i)
+        g->mt[i] = 6364136223846793005ULL * (g->mt[i - 1] ^ (g->mt[i - 1] >> 62)) + (uint64_t)i;
+    g->index = 312;
+}
+
+static uint64_t mt64_next(ora_mt64* g) {
+    const uint64_t upper = 0xFFFFFFFF80000000ULL, lower = 0x7FFFFFFFULL;
+    const uint64_t matrixA = 0xB5026F5AA96619E9ULL;
+    if (g->index >= 312) {
+        for (int i = 0; i < 312; ++i) {
+            const uint64_t y = (g->mt[i] & upper) | (g->mt[(i + 1) % 312] & lower);
+            g->mt[i] = g->mt[(i + 156) % 312] ^ (y >> 1) ^ ((y & 1ULL) ? matrixA : 0ULL);
+        }
+        g->index = 0;
+    }
+    uint64_t x = g->mt[g->index++];
+    x ^= (x >> 29) & 0x5555555555555555ULL;
+    x ^= (x << 17) & 0x71D67FFFEDA60000ULL;
+    x ^= (x << 37) & 0xFFF7EEE000000000ULL;
+    x ^= x >> 43;
+    return x;
+}
+
+void ora_random_uniform(uint64_t seed, long n, double* out) {
+    ora_mt64 g;
+    mt64_seed(&g, seed);
+    for (long i = 0; i < n; ++i) out[i] = (double)(mt64_next(&g) >> 11) * 0x1.0p-53 * 2.0 - 1.0;
+}
+
+void ora_random_normal(uint64_t seed, long n, double* out) {
+    ora_mt64 g;
+    mt64_seed(&g, seed);
+    const double twoPi = 6.283185307179586476925286766559;
+    for (long i = 0; i < n; i += 2) {
+        const double u1 = (double)(mt64_next(&g) >> 11) * 0x1.0p-53;
+        const double u2 = (double)(mt64_next(&g) >> 11) * 0x1.0p-53;
+        const double rad = sqrt(-2.0 * log(1.0 - u1));
+        out[i] = rad * cos(twoPi * u2);
+        if (i + 1 < n) out[i + 1] = rad * sin(twoPi * u2);
+    }
+}
+
+/* kappa_e = exp(g_e): N(0,1) per cell, convolved axis by axis (x first) with the
+ * normalised kernel exp(-j^2 / (2 sigma^2)), |j| <= truncation, indices clamped at
+ * the grid boundary, then standardised by the sample mean and variance. */
+void ora_kappa_field(uint64_t seed, int dim, const int* cells, double sigma, int truncation, double* kappa) {
+    long c[3] = {1, 1, 1}, n = 1;
+    for (int d = 0; d < dim; ++d) {
+        c[d] = cells[d];
+        n *= cells[d];
+    }
+    double* g = (double*)malloc(sizeof(double) * (size_t)n);
+    double* tmp = (double*)malloc(sizeof(double) * (size_t)n);
+    double* w = (double*)malloc(sizeof(double) * (size_t)(2 * truncation + 1));
+    ora_random_normal(seed, n, g);
+    double wsum = 0.0;
+    for (int j = -truncation; j <= truncation; ++j) {
+        w[j + truncation] = exp(-0.5 * j * j / (sigma * sigma));
+        wsum += w[j + truncation];
+    }
+    for (int j = 0; j < 2 * truncation + 1; ++j) w[j] /= wsum;
+    const long stride[3] = {1, c[0], c[0] * c[1]};
+    for (int d = 0; d < dim; ++d) {
+        for (long e = 0; e < n; ++e) {
+            const long coord = (e / stride[d]) % c[d];
+            double s = 0.0;
+            for (int j = -truncation; j <= truncation; ++j) {
+                long k = coord + j;
+                k = k < 0 ? 0 : (k >= c[d] ? c[d] - 1 : k);
+                s += w[j + truncation] * g[e + (k - coord) * stride[d]];
+            }
+            tmp[e] = s;
+        }
+        double* t = g;
+        g = tmp;
+        tmp = t;
+    }
+    double mean = 0.0;
+    for (long e = 0; e < n; ++e) mean += g[e];
+    mean /= (double)n;
+    double var = 0.0;
+    for (long e = 0; e < n; ++e) var += (g[e] - mean) * (g[e] - mean);
+    var /= (double)n;
+    const double inv = var > 0.0 ? 1.0 / sqrt(var) : 1.0;
+    for (long e = 0; e < n; ++e) kappa[e] = exp((g[e] - mean) * inv);
+    free(g); free(tmp); free(w);
+}
+
+/* 1 for the nodes of a structured Q_order grid that lie on the box boundary. */
+void ora_structured_boundary(int dim, int order, const int* cells, uint8_t* isBoundary) {
+    long nodes[3] = {1, 1, 1};
+    for (int d = 0; d < dim; ++d) nodes[d] = (long)order * cells[d] + 1;
+    const long n = nodes[0] * nodes[1] * nodes[2];
+    for (long i = 0; i < n; ++i) {
+        const long ix = i % nodes[0], iy = (i / nodes[0]) % nodes[1], iz = i / (nodes[0] * nodes[1]);
+        int b = ix == 0 || ix == nodes[0] - 1;
+        if (dim >= 2) b = b || iy == 0 || iy == nodes[1] - 1;
+        if (dim >= 3) b = b || iz == 0 || iz == nodes[2] - 1;
+        isBoundary[i] = (uint8_t)b;
+    }
+}
+
+/* Element stiffness of a uniform grid scattered colour by colour (colour of a
+ * cell = parity of its coordinates, so no two cells of a colour share a node),
+ * with the summation order the GPU kernel uses, so that the two matrices can be
+ * compared bit for bit:
+ *   S[a][b] = sum_q w_q (sum_d G_q[d][a] G_q[d][b])   (fused multiply-adds, q and d ascending)
+ *   val[slot] = fma(kappa_e * prod_d(2/h_d), S[a][b], val[slot])   (reference convention)
+ * with the Gauss-Legendre rule of ora_gauss_legendre and Lagrange values and
+ * derivatives on equispaced nodes by the running product
+ *   f = (x - x_j)/(x_i - x_j);  dv = dv f + v/(x_i - x_j);  v = v f.
+ * Returns 0, or 1 when an entry is missing from the pattern. */
+int ora_assemble_structured(int dim, int order, int quadratureOrder, const int* cells, const int* dofmap,
+                            const double* kappa, const int* rowptr, const int* col, double* val) {
+    const int n1 = order + 1;
+    int nb = 1, nq = 1;
+    long ncells = 1, c[3] = {1, 1, 1};
+    for (int d = 0; d < dim; ++d) {
+        nb *= n1;
+        nq *= quadratureOrder;
+        ncells *= cells[d];
+        c[d] = cells[d];
+    }
+    double gn[16], gw[16], nodes[16], v1[16 * 16], d1[16 * 16];
+    if (quadratureOrder < 1 || quadratureOrder > 16 || n1 > 16 || ora_gauss_legendre(quadratureOrder, gn, gw)) return 1;
+    for (int i = 0; i < n1; ++i) nodes[i] = -1.0 + 2.0 * i / order;
+    for (int q = 0; q < quadratureOrder; ++q)
+        for (int i = 0; i < n1; ++i) {
+            double value = 1.0, deriv = 0.0;
+            for (int j = 0; j < n1; ++j) {
+                if (j == i) continue;
+                const double f = (gn[q] - nodes[j]) / (nodes[i] - nodes[j]);
+                deriv = deriv * f + value / (nodes[i] - nodes[j]);
+                value *= f;
+            }
+            v1[q * n1 + i] = value;
+            d1[q * n1 + i] = deriv;
+        }
+    double* gtab = (double*)malloc(sizeof(double) * (size_t)nq * dim * nb);
+    double* wq = (double*)malloc(sizeof(double) * (size_t)nq);
+    double* S = (double*)malloc(sizeof(double) * (size_t)nb * nb);
+    for (int q = 0; q < nq; ++q) {
+        int qi[3] = {0, 0, 0}, rest = q;
+        double w = 1.0;
+        for (int d = 0; d < dim; ++d) {
+            qi[d] = rest % quadratureOrder;
+            rest /= quadratureOrder;
+            w *= gw[qi[d]];
+        }
+        wq[q] = w;
+        for (int dd = 0; dd < dim; ++dd)
+            for (int a = 0; a < nb; ++a) {
+                int ra = a;
+                double g = 1.0;
+                for (int d = 0; d < dim; ++d) {
+                    const int i = ra % n1;
+                    ra /= n1;
+                    g *= (d == dd) ? d1[qi[d] * n1 + i] : v1[qi[d] * n1 + i];
+                }
+                gtab[((long)q * dim + dd) * nb + a] = g;
+            }
+    }
+    for (int a = 0; a < nb; ++a)
+        for (int b = 0; b < nb; ++b) {
+            double s = 0.0;
+            for (int q = 0; q < nq; ++q) {
+                const double* g = gtab + (long)q * dim * nb;
+                double gg = 0.0;
+                for (int d = 0; d < dim; ++d) gg = fma(g[d * nb + a], g[d * nb + b], gg);
+                s = fma(wq[q], gg, s);
+            }
+            S[a * nb + b] = s;
+        }
+    double scale = 1.0;
+    for (int d = 0; d < dim; ++d) scale *= 2.0 / (1.0 / (double)cells[d]);
+    int missing = 0;
+    const int colors = 1 << dim;
+    for (int color = 0; color < colors && !missing; ++color)
+        for (long e = 0; e < ncells && !missing; ++e) {
+            const long ex = e % c[0], ey = (e / c[0]) % c[1], ez = e / (c[0] * c[1]);
+            if ((int)((ex & 1) | ((ey & 1) << 1) | ((ez & 1) << 2)) != color) continue;
+            const int* dofs = dofmap + e * nb;
+            const double ks = kappa[e] * scale;
+            for (int a = 0; a < nb && !missing; ++a) {
+                const int row = dofs[a];
+                for (int b = 0; b < nb; ++b) {
+                    int lo = rowptr[row], hi = rowptr[row + 1];
+                    const int target = dofs[b];
+                    while (lo < hi) {
+                        const int mid = lo + (hi - lo) / 2;
+                        if (col[mid] < target) lo = mid + 1; else hi = mid;
+                    }
+                    if (lo == rowptr[row + 1] || col[lo] != target) { missing = 1; break; }
+                    val[lo] = fma(ks, S[a * nb + b], val[lo]);
+                }
+            }
+        }
+    free(gtab); free(wq); free(S);
+    return missing;
+}

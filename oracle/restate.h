@@ -56,6 +56,14 @@ int ora_cut_cell_points(int dim, int depth, int order, const double* center, dou
                         const double* cellOrigin, const double* cellSize, int maxPoints,
                         double* points, double* weights, double* scales, double alpha);
 
+/* ---- seeded workload inputs (no CUDA library needed) ------------------ */
+void ora_random_uniform(uint64_t seed, long n, double* out);
+void ora_random_normal(uint64_t seed, long n, double* out);
+void ora_kappa_field(uint64_t seed, int dim, const int* cells, double sigma, int truncation, double* kappa);
+void ora_structured_boundary(int dim, int order, const int* cells, uint8_t* isBoundary);
+int ora_assemble_structured(int dim, int order, int quadratureOrder, const int* cells, const int* dofmap,
+                            const double* kappa, const int* rowptr, const int* col, double* val);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,181 @@
+"""Parity at the exact benchmark configurations, through the C-ABI, against the
+reference's compiled FP64 CPU solver (ConjugateGradients<DefaultSpace<double>> +
+CSROperator + DiagonalOperator) on identical inputs:
+
+  * the seeded systems the GPU assembles are bit-identical to the ones the oracle
+    builds on the host without the CUDA library (2D Q1 256^2, 3D Q1 32^3 and 128^3),
+    so the reference arm of the benchmark solves exactly the GPU's system;
+  * 3D Q1 128^3, log-normal kappa (2,146,689 rows): plain FP64 PCG and the
+    FP32-inner / FP64-refined PCG to ||r||/||b|| <= 1e-10, each within 1e-9
+    relative of the reference's solution;
+  * 32 right-hand sides on that matrix (SpMM-CG): four columns against the
+    reference solving them alone;
+  * batched uneven 2D Q2 systems, n ~ U{16..128} with the benchmark's seeds: a
+    64-system subset of the 512, FP64 and FP32-refined, every system within 1e-9.
+"""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+TOL = 1e-9           # solution bar: relative 2-norm distance from the reference's solution
+RESIDUAL = 1.01e-10  # true FP64 relative residual bar (1e-10 plus rounding of its own evaluation)
+
+
+def true_residual(rp, col, val, x, b):
+    """||b - A x|| / ||b|| in FP64 with the oracle's row loop."""
+    from oracle.oracle import Restatement
+    r = Restatement().spmv(rp, col, val, 1.0, x, -1.0, b)
+    return np.linalg.norm(r) / np.linalg.norm(b)
+
+
+@pytest.fixture(scope="module")
+def space():
+    from cie_b200.linalg import CUDASpace
+    return CUDASpace()
+
+
+@pytest.fixture(scope="module")
+def reference_all():
+    """The reference CPU solver on every host thread (the 128^3 solves)."""
+    from oracle.oracle import Reference, reference_available
+    if not reference_available():
+        pytest.skip("oracle/_ref/libcieref.so not built")
+    ref = Reference()
+    yield ref
+    ref.close()
+
+
+@pytest.mark.parametrize("dim,cells,kappa", [(2, [256, 256], "one"), (3, [32, 32, 32], "lognormal"),
+                                             (3, [128, 128, 128], "lognormal")])
+def test_workload_system_is_bit_identical_to_oracle(space, restatement, dim, cells, kappa):
+    from cie_b200.fem import make_poisson
+    from oracle.oracle import system_digest
+    prob = make_poisson(space, dim, 1, cells, seed=0, kappa=kappa)
+    rp, col, val = prob.host_csr()
+    b = prob.rhs.cpu().numpy()
+    orp, ocol, oval, ob, _, _ = restatement.poisson_system(dim, 1, cells, seed=0, kappa=kappa)
+    assert np.array_equal(rp, orp) and np.array_equal(col, ocol)
+    assert np.array_equal(b.view(np.uint64), ob.view(np.uint64))
+    diff = np.abs(val - oval).max() / np.abs(oval).max()
+    assert np.array_equal(val.view(np.uint64), oval.view(np.uint64)), "max entry difference %.3e" % diff
+    assert system_digest(rp, col, val, b) == system_digest(orp, ocol, oval, ob)
+
+
+@pytest.fixture(scope="module")
+def cfg2(space, reference_all):
+    """The 128^3 Q1 system with the reference's FP64 solution (one CPU solve)."""
+    from cie_b200.fem import make_poisson
+    prob = make_poisson(space, 3, 1, [128, 128, 128], seed=0)
+    rp, col, val = prob.host_csr()
+    b = prob.rhs.cpu().numpy()
+    xr, sr, err, secs = reference_all.pcg(rp, col, val, b, maxit=20000, abstol=0.0, reltol=1e-10)
+    assert err is None
+    print("reference 128^3: %d iterations, %.2f s on %d threads" % (sr[0], secs, reference_all.threads))
+    return prob, (rp, col, val, b), xr, sr
+
+
+def test_cfg2_fp64_pcg_vs_reference(space, cfg2):
+    from cie_b200.linalg import ConjugateGradients, CSROperator, Statistics, makeDiagonalOperator
+    prob, (rp, col, val, b), xr, sr = cfg2
+    A = CSROperator(prob.matrix, space)
+    cg = ConjugateGradients(A, space, makeDiagonalOperator(prob.matrix, space, csr_handle=A.csr),
+                            Statistics(20000, 0.0, 1e-10))
+    x = torch.zeros_like(prob.rhs)
+    cg.product(0.0, prob.rhs, 1.0, x)
+    xh = x.cpu().numpy()
+    rel = np.linalg.norm(xh - xr) / np.linalg.norm(xr)
+    st = cg.getStats()
+    print("cfg2 FP64: %d iterations (reference %d), |x - x_ref|/|x_ref| = %.3e, %s"
+          % (st.iterationCount, sr[0], rel, cg.info()))
+    assert abs(st.iterationCount - int(sr[0])) <= 2
+    assert rel <= TOL
+    assert true_residual(rp, col, val, xh, b) <= RESIDUAL
+
+
+@pytest.mark.parametrize("delta", [0.1])
+def test_cfg2_mixed_pcg_vs_reference(space, cfg2, delta):
+    from cie_b200.linalg import CSROperator, MixedPrecisionCG, Statistics, makeDiagonalOperator
+    prob, (rp, col, val, b), xr, sr = cfg2
+    A = CSROperator(prob.matrix, space)
+    D = makeDiagonalOperator(prob.matrix, space, csr_handle=A.csr)
+    solver = MixedPrecisionCG(A, D, Statistics(20000, 0.0, 1e-10), mode=0, delta=delta)
+    x = torch.zeros_like(prob.rhs)
+    solver.product(0.0, prob.rhs, 1.0, x)
+    xh = x.cpu().numpy()
+    st = solver.getStats()
+    rel = np.linalg.norm(xh - xr) / np.linalg.norm(xr)
+    print("cfg2 mixed: %d inner iterations, %d replacements, |x - x_ref|/|x_ref| = %.3e, %s"
+          % (st.innerIterations, st.refinements, rel, solver.info()))
+    assert st.trueRelativeResidual < 1e-10
+    assert rel <= TOL
+    assert true_residual(rp, col, val, xh, b) <= RESIDUAL
+
+
+def test_cfg4_multirhs_128_vs_reference(space, cfg2, reference_all):
+    """32 right-hand sides U[-1,1] (seeds 2000 + c, the benchmark's) on the 128^3
+    matrix; columns 0, 9, 21 and 31 against the reference solving them alone."""
+    from cie_b200.fem import random_uniform
+    from cie_b200.linalg import CSROperator, MultiRHSConjugateGradients, Statistics, makeDiagonalOperator
+    prob, (rp, col, val, _), _, _ = cfg2
+    n = prob.rhs.numel()
+    k = 32
+    B = np.stack([random_uniform(2000 + c, n) for c in range(k)], axis=1)
+    A = CSROperator(prob.matrix, space)
+    D = makeDiagonalOperator(prob.matrix, space, csr_handle=A.csr)
+    solver = MultiRHSConjugateGradients(A, D, k, Statistics(20000, 0.0, 1e-10))
+    X = torch.zeros(n, k, dtype=torch.float64, device="cuda")
+    solver.product(0.0, torch.as_tensor(B).cuda().contiguous(), 1.0, X)
+    stats = solver.getStats()
+    Xh = X.cpu().numpy()
+    for c in (0, 9, 21, 31):
+        bc = B[:, c].copy()
+        xr, sr, err, _ = reference_all.pcg(rp, col, val, bc, maxit=20000, abstol=0.0, reltol=1e-10)
+        rel = np.linalg.norm(Xh[:, c] - xr) / np.linalg.norm(xr)
+        print("cfg4 32-RHS column %d: %d iterations (reference %d), rel %.3e" % (c, stats[c].iterationCount,
+                                                                                sr[0], rel))
+        assert err is None
+        assert abs(stats[c].iterationCount - int(sr[0])) <= 2
+        assert rel <= TOL
+
+
+@pytest.fixture(scope="module")
+def cfg4_batch(space):
+    """Every eighth of the benchmark's 512 uneven 2D Q2 systems (sizes from
+    default_rng(0).integers(16, 129, 512), RHS seed 1000 + 3i, kappa seed + 1)."""
+    from cie_b200.fem import make_poisson
+    sizes = np.random.default_rng(0).integers(16, 129, 512)
+    pick = list(range(0, 512, 8))
+    return [make_poisson(space, 2, 2, [int(sizes[i]), int(sizes[i])], seed=1000 + 3 * i) for i in pick]
+
+
+@pytest.mark.parametrize("refined", [False, True])
+def test_cfg4_batched_subset_vs_reference(space, reference_all, cfg4_batch, refined):
+    from cie_b200.linalg import BatchedConjugateGradients, Statistics, block_diagonal, makeDiagonalOperator
+    probs = cfg4_batch
+    bd, offsets = block_diagonal([p.matrix for p in probs])
+    rhs = torch.cat([p.rhs for p in probs])
+    solver = BatchedConjugateGradients(bd, offsets, space, makeDiagonalOperator(bd, space),
+                                       Statistics(20000, 0.0, 1e-10))
+    if refined:
+        solver.set_refinement(1e-2)
+    x = torch.zeros_like(rhs)
+    solver.product(0.0, rhs, 1.0, x)
+    stats = solver.getStats()
+    xh = x.cpu().numpy()
+    worst = 0.0
+    for s, p in enumerate(probs):
+        rp, col, val = p.host_csr()
+        b = p.rhs.cpu().numpy()
+        xr, sr, err, _ = reference_all.pcg(rp, col, val, b, maxit=20000, abstol=0.0, reltol=1e-10)
+        xs = xh[offsets[s]:offsets[s + 1]]
+        rel = np.linalg.norm(xs - xr) / np.linalg.norm(xr)
+        worst = max(worst, rel)
+        assert err is None
+        assert rel <= TOL, (s, rel)
+        assert true_residual(rp, col, val, xs, b) <= RESIDUAL, s
+        if not refined:
+            assert stats[s].iterationCount == int(sr[0]), (s, stats[s].iterationCount, sr[0])
+    print("cfg4 batch of %d (refined=%s): worst |x - x_ref|/|x_ref| = %.3e" % (len(probs), refined, worst))

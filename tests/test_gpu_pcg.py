@@ -178,6 +178,53 @@ def test_pcg_breakdown_raises(space, loop):
     assert st.iterationCount == 0 and np.all(x == 0)
 
 
+def test_single_launch_wait_timeout_then_reuse(space, reference):
+    """The bounded grid-wide waits of the single-launch solve: with the last block
+    withholding its partial sums at the third exchange, every wait on it runs out
+    (1 ms limit), the solve fails with CIECU_ERR_TIMEOUT, and the same solver then
+    solves normally and matches the reference CG."""
+    from cie_b200._lib import CiecuError
+    from cie_b200.fem import make_poisson
+    from cie_b200.linalg import CSROperator, ConjugateGradients, Statistics, makeDiagonalOperator
+    prob = make_poisson(space, 2, 1, [48, 48], seed=3)
+    A = CSROperator(prob.matrix, space)
+    cg = ConjugateGradients(A, space, makeDiagonalOperator(prob.matrix, space), Statistics(5000, 0.0, 1e-10))
+    cg.set_loop(2)
+    cg.debug_exchange(1_000_000, 3)
+    x = torch.zeros_like(prob.rhs)
+    with pytest.raises(CiecuError, match="gave up waiting"):
+        cg.product(0, prob.rhs, 1, x)
+    cg.debug_exchange(2_000_000_000, 0)
+    x = torch.zeros_like(prob.rhs)
+    cg.product(0, prob.rhs, 1, x)
+    assert cg.info()["loop"] == "single launch"
+    rp, col, val = prob.host_csr()
+    b = host(prob.rhs)
+    xr, sr, err, _ = reference.pcg(rp, col, val, b, maxit=5000, abstol=0.0, reltol=1e-10)
+    assert err is None and abs(cg.getStats().iterationCount - int(sr[0])) <= 2
+    assert np.linalg.norm(host(x) - xr) <= 1e-9 * np.linalg.norm(xr)
+
+
+def test_pinned_schedule_selects_the_graph_loop(space):
+    """A K1 schedule pinned in the automatic loop mode runs the graph loop (the
+    schedules are its kernels) instead of being ignored by the single launch."""
+    from cie_b200.fem import make_poisson
+    from cie_b200.linalg import CSROperator, ConjugateGradients, Statistics, makeDiagonalOperator
+    prob = make_poisson(space, 2, 1, [32, 32], seed=4)
+    A = CSROperator(prob.matrix, space)
+    cg = ConjugateGradients(A, space, makeDiagonalOperator(prob.matrix, space), Statistics(5000, 0.0, 1e-10))
+    x = torch.zeros_like(prob.rhs)
+    cg.product(0, prob.rhs, 1, x)
+    assert cg.info()["loop"] == "single launch"
+    x1 = host(x)
+    for schedule in (4, 64):
+        cg.set_schedule(schedule)
+        x = torch.zeros_like(prob.rhs)
+        cg.product(0, prob.rhs, 1, x)
+        assert cg.info()["loop"] != "single launch" and cg.info()["spmv_schedule"] == schedule
+        assert np.linalg.norm(host(x) - x1) <= 1e-12 * np.linalg.norm(x1)
+
+
 def test_generic_cg_over_masked_operator_vs_oracle(space, restatement):
     """The reference algorithm composed from operator products (masked operator):
     ConjugateGradients over a MaskedCSROperator, as grid 0 of the p-multigrid."""
