@@ -54,6 +54,7 @@ class Restatement:
             "ora_element_gradient": (None, [_l, _i, _P, _P, _P, _P, _P]),
             "ora_dirichlet_eliminate": (None, [_i, _P, _P, _P, _P, _P]),
             "ora_cut_cell_points": (_i, [_i, _i, _i, _P, _d, _P, _P, _i, _P, _P, _P, _d]),
+            "ora_cut_cell_points_halfspace": (_i, [_i, _i, _i, _P, _d, _P, _P, _i, _P, _P, _P, _d]),
             "ora_random_uniform": (None, [_u64, _l, _P]),
             "ora_random_normal": (None, [_u64, _l, _P]),
             "ora_kappa_field": (None, [_u64, _i, _P, _d, _i, _P]),
@@ -179,6 +180,18 @@ class Restatement:
         assert n >= 0
         return pts[: n * dim].reshape(n, dim), w[:n], s[:n]
 
+    def cut_cell_points_halfspace(self, dim, depth, order, normal, offset, origin, size, alpha,
+                                  maxPoints=1 << 16):
+        pts = np.zeros(maxPoints * dim)
+        w = np.zeros(maxPoints)
+        s = np.zeros(maxPoints)
+        n = self.L.ora_cut_cell_points_halfspace(dim, depth, order, p(np.asarray(normal, dtype=np.float64)),
+                                                 float(offset), p(np.asarray(origin, dtype=np.float64)),
+                                                 p(np.asarray(size, dtype=np.float64)), maxPoints, p(pts), p(w),
+                                                 p(s), alpha)
+        assert n >= 0
+        return pts[: n * dim].reshape(n, dim), w[:n], s[:n]
+
     # -- seeded workload inputs --
     def random_uniform(self, seed, n):
         out = np.zeros(int(n))
@@ -262,6 +275,7 @@ class Reference:
             "cieref_space_dot": (_i, [_P, _l, _P, _P, _P]),
             "cieref_space_op": (_i, [_P, _i, _l, _P, _P, _d]),
             "cieref_gauss_legendre": (_i, [_i, _P, _P]),
+            "cieref_lagrange": (_i, [_i, _P, _i, _i, _P, _P, _P, _P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -343,6 +357,16 @@ class Reference:
         n, w = np.zeros(order), np.zeros(order)
         self._check(self.L.cieref_gauss_legendre(order, p(n), p(w)))
         return n, w
+
+    def lagrange(self, nodes, iBase, points):
+        """The reference's LagrangePolynomial of node iBase: (ascending coefficients,
+        values at points, derivative values at points)."""
+        nodes = np.ascontiguousarray(nodes, dtype=np.float64)
+        points = np.ascontiguousarray(points, dtype=np.float64)
+        c, v, d = np.zeros(len(nodes)), np.zeros(len(points)), np.zeros(len(points))
+        self._check(self.L.cieref_lagrange(len(nodes), p(nodes), int(iBase), len(points), p(points), p(c), p(v),
+                                           p(d)))
+        return c, v, d
 
 
 def reference_available():

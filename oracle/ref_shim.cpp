@@ -17,6 +17,9 @@
 //   * cieref_pmg        -> executables/fem_examples/src/poisson2D/solver.cpp:111-232
 //   * cieref_space_*    -> linalg/packages/solvers/src/DefaultSpace.cpp:50-187
 //   * cieref_gauss_legendre -> fem/packages/numeric/src/GaussLegendreQuadrature.cpp:82-175
+//   * cieref_lagrange   -> fem/packages/maths/src/LagrangePolynomial.cpp:18-72 (coefficients),
+//                          fem/packages/maths/impl/Polynomial_impl.hpp (Horner evaluation,
+//                          makeDerivative)
 #include "packages/solvers/inc/ConjugateGradients.hpp"
 #include "packages/solvers/inc/CSROperator.hpp"
 #include "packages/solvers/inc/MaskedCSROperator.hpp"
@@ -27,6 +30,7 @@
 #include "packages/solvers/inc/DefaultSpace.hpp"
 #include "packages/concurrency/inc/ThreadPoolBase.hpp"
 #include "packages/numeric/inc/GaussLegendreQuadrature.hpp"
+#include "packages/maths/inc/LagrangePolynomial.hpp"
 
 #include <chrono>
 #include <cmath>
@@ -355,6 +359,31 @@ int cieref_gauss_legendre(int order, double* nodes, double* weights) {
         for (int i = 0; i < order; ++i) {
             nodes[i] = quadrature.nodes()[static_cast<std::size_t>(i)];
             weights[i] = quadrature.weights()[static_cast<std::size_t>(i)];
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+// The 1-D Lagrange basis polynomial of node iBase on the given nodes, built by the
+// reference's LagrangePolynomial: its ascending monomial coefficients (count of
+// them), and its value and derivative (Polynomial::evaluate of the polynomial and
+// of makeDerivative()) at each of the npts points.
+int cieref_lagrange(int count, const double* nodes, int iBase, int npts, const double* points,
+                    double* coefficients, double* values, double* derivatives) {
+    try {
+        const fem::maths::LagrangePolynomial<double> basis(std::span<const double>(nodes, static_cast<std::size_t>(count)),
+                                                           static_cast<Size>(iBase));
+        const auto c = basis.coefficients();
+        for (std::size_t k = 0; k < c.size(); ++k) coefficients[k] = c[k];
+        const auto derivative = basis.makeDerivative();
+        for (int i = 0; i < npts; ++i) {
+            double in[1] = {points[i]}, out[1] = {0.0};
+            basis.evaluate(std::span<const double>(in, 1), std::span<double>(out, 1), {});
+            values[i] = out[0];
+            derivative.evaluate(std::span<const double>(in, 1), std::span<double>(out, 1), {});
+            derivatives[i] = out[0];
         }
         return 0;
     } catch (const std::exception& e) {

@@ -549,7 +549,7 @@ void ora_dirichlet_eliminate(int n, const int* rowptr, const int* col, double* v
 }
 
 /* Cut-cell quadrature of fem/packages/numeric/inc/KDTreeQuadraturePointFactory.hpp:67-173
- * for a sphere domain (inside: |x - center|^2 < radius^2), depth range [0, depth],
+ * for a domain given by an inside test of physical points, depth range [0, depth],
  * a (order)^dim Gauss-Legendre base rule per tree node.  Keep rule (:156-160):
  * keep = (homogeneous && inside) || depth == max || (depth == min && homogeneous);
  * descend while not homogeneous.  points: parametric coordinates in [-1,1]^dim,
@@ -557,9 +557,25 @@ void ora_dirichlet_eliminate(int n, const int* rowptr, const int* col, double* v
  * 1 inside, alpha outside (ScaledMultiMaterialIntegrand_impl.hpp:33-60 with the
  * material map {(0, alpha), (1, 1)}).  Returns the number of points, or -1 when
  * maxPoints is exceeded. */
+typedef struct {
+    int kind;               /* 0: sphere |x - c|^2 < r^2;  1: half-space n . x < offset */
+    double center[3], radius;
+    double normal[3], offset;
+} cut_domain;
+
+static int cut_inside(const cut_domain* D, int dim, const double* x) {
+    double acc = 0.0;
+    if (D->kind == 0) {
+        for (int d = 0; d < dim; ++d) acc += (x[d] - D->center[d]) * (x[d] - D->center[d]);
+        return acc < D->radius * D->radius;
+    }
+    for (int d = 0; d < dim; ++d) acc += D->normal[d] * x[d];
+    return acc < D->offset;
+}
+
 static int cut_visit(int dim, int depth, int maxDepth, const double* base, double length,
-                     int order, const double* gn, const double* gw, const double* center,
-                     double radius, const double* cellOrigin, const double* cellSize,
+                     int order, const double* gn, const double* gw, const cut_domain* D,
+                     const double* cellOrigin, const double* cellSize,
                      int maxPoints, int count, double* points, double* weights, double* scales,
                      double alpha) {
     int nbase = 1;
@@ -569,18 +585,17 @@ static int cut_visit(int dim, int depth, int maxDepth, const double* base, doubl
     const double jac = pow(0.5 * length, dim);
     for (int q = 0; q < nbase; ++q) {
         int rest = q;
-        double w = 1.0, r2 = 0.0;
+        double w = 1.0, x[3];
         for (int d = 0; d < dim; ++d) {
             const int i = rest % order;
             rest /= order;
             const double xi = base[d] + 0.5 * length * (gn[i] + 1.0);
             points[(long)(count + q) * dim + d] = xi;
             w *= gw[i];
-            const double x = cellOrigin[d] + 0.5 * (xi + 1.0) * cellSize[d];
-            r2 += (x - center[d]) * (x - center[d]);
+            x[d] = cellOrigin[d] + 0.5 * (xi + 1.0) * cellSize[d];
         }
         weights[count + q] = w * jac;
-        const int inside = r2 < radius * radius;
+        const int inside = cut_inside(D, dim, x);
         scales[count + q] = inside ? 1.0 : alpha;
         if (inside0 < 0) inside0 = inside;
         else if (inside != inside0) homogeneous = 0;
@@ -595,21 +610,42 @@ static int cut_visit(int dim, int depth, int maxDepth, const double* base, doubl
     for (int c = 0; c < children; ++c) {
         double childBase[3];
         for (int d = 0; d < dim; ++d) childBase[d] = base[d] + ((c >> d) & 1) * half;
-        count = cut_visit(dim, depth + 1, maxDepth, childBase, half, order, gn, gw, center, radius,
+        count = cut_visit(dim, depth + 1, maxDepth, childBase, half, order, gn, gw, D,
                           cellOrigin, cellSize, maxPoints, count, points, weights, scales, alpha);
         if (count < 0) return -1;
     }
     return count;
 }
 
+static int cut_points(int dim, int depth, int order, const cut_domain* D, const double* cellOrigin,
+                      const double* cellSize, int maxPoints, double* points, double* weights,
+                      double* scales, double alpha) {
+    double gn[16], gw[16];
+    if (order < 1 || order > 16 || ora_gauss_legendre(order, gn, gw)) return -1;
+    const double base[3] = {-1.0, -1.0, -1.0};
+    return cut_visit(dim, 0, depth, base, 2.0, order, gn, gw, D, cellOrigin, cellSize,
+                     maxPoints, 0, points, weights, scales, alpha);
+}
+
 int ora_cut_cell_points(int dim, int depth, int order, const double* center, double radius,
                         const double* cellOrigin, const double* cellSize, int maxPoints,
                         double* points, double* weights, double* scales, double alpha) {
-    double gn[16], gw[16];
-    if (ora_gauss_legendre(order, gn, gw)) return -1;
-    const double base[3] = {-1.0, -1.0, -1.0};
-    return cut_visit(dim, 0, depth, base, 2.0, order, gn, gw, center, radius, cellOrigin, cellSize,
-                     maxPoints, 0, points, weights, scales, alpha);
+    cut_domain D;
+    memset(&D, 0, sizeof(D));
+    for (int d = 0; d < dim; ++d) D.center[d] = center[d];
+    D.radius = radius;
+    return cut_points(dim, depth, order, &D, cellOrigin, cellSize, maxPoints, points, weights, scales, alpha);
+}
+
+int ora_cut_cell_points_halfspace(int dim, int depth, int order, const double* normal, double offset,
+                                  const double* cellOrigin, const double* cellSize, int maxPoints,
+                                  double* points, double* weights, double* scales, double alpha) {
+    cut_domain D;
+    memset(&D, 0, sizeof(D));
+    D.kind = 1;
+    for (int d = 0; d < dim; ++d) D.normal[d] = normal[d];
+    D.offset = offset;
+    return cut_points(dim, depth, order, &D, cellOrigin, cellSize, maxPoints, points, weights, scales, alpha);
 }
 
 /* ---- seeded workload inputs ------------------------------------------------

@@ -55,6 +55,10 @@ void ora_dirichlet_eliminate(int n, const int* rowptr, const int* col, double* v
 int ora_cut_cell_points(int dim, int depth, int order, const double* center, double radius,
                         const double* cellOrigin, const double* cellSize, int maxPoints,
                         double* points, double* weights, double* scales, double alpha);
+/* The same tree for the half-space normal . x < offset (physical coordinates). */
+int ora_cut_cell_points_halfspace(int dim, int depth, int order, const double* normal, double offset,
+                                  const double* cellOrigin, const double* cellSize, int maxPoints,
+                                  double* points, double* weights, double* scales, double alpha);
 
 /* ---- seeded workload inputs (no CUDA library needed) ------------------ */
 void ora_random_uniform(uint64_t seed, long n, double* out);

@@ -122,6 +122,58 @@ def test_q1_2d_element_matches_closed_form(restatement):
 
 # ---- oracle vs the compiled reference -------------------------------------------
 
+
+def lagrange_nodes(order, kind):
+    """Equispaced nodes -1 + 2i/p (the build's Q_p basis) or Chebyshev-Lobatto
+    nodes -cos(i pi / p) (the reference's Lagrange example), ascending."""
+    i = np.arange(order + 1)
+    return -1.0 + 2.0 * i / order if kind == "equispaced" else -np.cos(i * np.pi / order)
+
+
+@pytest.mark.parametrize("kind", ["equispaced", "chebyshev-lobatto"])
+def test_lagrange_basis_restatement_vs_reference(restatement, reference, kind):
+    """The restated product-form Lagrange values and derivatives against the
+    reference's LagrangePolynomial (coefficients from LagrangePolynomial.cpp:18-72,
+    Horner evaluation and makeDerivative of Polynomial_impl.hpp), Q1..Q5, at the
+    Gauss points of the rules the assembly uses and at random points of [-1, 1]."""
+    import ctypes
+    rng = np.random.default_rng(9)
+    for order in range(1, 6):
+        nodes = lagrange_nodes(order, kind)
+        points = np.concatenate([reference.gauss_legendre(q)[0] for q in range(2, 7)] + [rng.uniform(-1, 1, 16)])
+        for base in range(order + 1):
+            c, v_ref, d_ref = reference.lagrange(nodes, base, points)
+            assert abs(np.polyval(c[::-1], nodes[base]) - 1.0) <= 1e-13
+            for k, x in enumerate(points):
+                vals, ders = np.zeros(order + 1), np.zeros(order + 1)
+                restatement.L.ora_lagrange_1d(order + 1, nodes.ctypes.data_as(ctypes.c_void_p), float(x),
+                                              vals.ctypes.data_as(ctypes.c_void_p),
+                                              ders.ctypes.data_as(ctypes.c_void_p))
+                assert abs(vals[base] - v_ref[k]) <= 1e-13, (order, base, x)
+                assert abs(ders[base] - d_ref[k]) <= 1e-12 * max(1.0, abs(d_ref[k])), (order, base, x)
+
+
+@pytest.mark.parametrize("dim,order", [(2, 2), (2, 3), (3, 2), (3, 3)])
+def test_element_stiffness_with_reference_basis(restatement, reference, dim, order):
+    """Q2/Q3 element matrices of the restatement (the checker of the GPU assembly)
+    against the same integral built from the reference's own basis: the
+    LagrangePolynomial coefficient vectors evaluated by the restated integrand at
+    the reference's Gauss points, K = prod(2/h) sum_q w_q kappa G_q^T G_q."""
+    nodes = lagrange_nodes(order, "equispaced")
+    coefficients = np.array([reference.lagrange(nodes, i, [0.0])[0] for i in range(order + 1)])
+    n1, w1 = reference.gauss_legendre(order + 1)
+    q = np.arange((order + 1) ** dim)
+    idx = (q[:, None] // (order + 1) ** np.arange(dim)[None, :]) % (order + 1)
+    h = [0.25, 0.5, 0.125][:dim]
+    kappa = 1.7
+    K = 0.0
+    for pt, w in zip(n1[idx], np.prod(w1[idx], axis=1)):
+        K = K + w * restatement.stiffness_point(dim, coefficients, pt, kappa)
+    K *= np.prod(2.0 / np.array(h))
+    Kr = restatement.element_stiffness(dim, order, kappa, h)
+    assert np.max(np.abs(K - Kr)) <= 1e-13 * np.abs(Kr).max()
+
+
 def test_reference_matches_goldens(reference, golden):
     c = golden["linalg_space"]["spmv"]
     y = reference.spmv(np.array(c["row_extents"], np.int32), np.array(c["column_indices"], np.int32),
