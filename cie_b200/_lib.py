@@ -119,6 +119,14 @@ SIGNATURES = {
     "ciecu_multi_format": (c_int, [P, P]),
     "ciecu_multi_product": (c_int, [P, c_double, P, c_double, P, P]),
     "ciecu_dirichlet_eliminate": (c_int, [P, P, P, P]),
+    "ciecu_write_matrix_market_host": (c_int, [c_char_p, c_int64, c_int64, P, P, P]),
+    "ciecu_write_matrix_market": (c_int, [P, c_char_p]),
+    "ciecu_write_matrix_market_vector": (c_int, [P, c_int64, P, c_char_p]),
+    "ciecu_write_matrix_market_vector_host": (c_int, [c_char_p, c_int64, P]),
+    "ciecu_make_reordering": (c_int, [P, ctypes.c_int32, P, P, c_int, P]),
+    "ciecu_reorder_csr": (c_int, [P, ctypes.c_int32, P, P, P, P, P, P, P]),
+    "ciecu_reorder_vector": (c_int, [P, c_int64, P, c_int, P, P]),
+    "ciecu_csr_pattern_device": (c_int, [P, c_int64, c_int, P, ctypes.c_int32, P, P, P]),
 }
 
 OPTIONAL = set()

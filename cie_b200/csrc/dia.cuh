@@ -19,6 +19,7 @@
 #pragma once
 
 #include "spmv.cuh"
+#include "sell.cuh"
 
 #include <vector>
 
@@ -69,10 +70,10 @@ __device__ __forceinline__ void dia_rows(const DiaArgs<V>& A, const T* __restric
 
 // Four consecutive rows per thread with 16-byte loads of each diagonal (FP32:
 // a warp reads 512 contiguous bytes per diagonal instead of 128).  Rows past
-// nrows (up to ld, zero-filled) are computed and dropped; the gathers of x stay
-// inside [0, nrows).
-template <int ND, typename Op>
-__device__ __forceinline__ void dia_rows4(const DiaArgs<float>& A, const float* __restrict__ x, Op& op) {
+// nrows (up to ld, zero-filled) are computed and dropped; the gathers stay
+// inside [0, nrows).  The operand entry of column c is gather(c).
+template <int ND, typename Op, typename TGather>
+__device__ __forceinline__ void dia_rows4_gather(const DiaArgs<float>& A, const TGather& gather, Op& op) {
     const long stride = static_cast<long>(gridDim.x) * blockDim.x * 4;
     for (long r0 = (static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x) * 4; r0 < A.nrows; r0 += stride) {
         const int r = static_cast<int>(r0);
@@ -87,7 +88,7 @@ __device__ __forceinline__ void dia_rows4(const DiaArgs<float>& A, const float* 
             float xv[4];
 #pragma unroll
             for (int i = 0; i < 4; ++i)
-                xv[i] = static_cast<unsigned>(c + i) < static_cast<unsigned>(A.nrows) ? __ldg(x + c + i) : 0.f;
+                xv[i] = static_cast<unsigned>(c + i) < static_cast<unsigned>(A.nrows) ? gather(c + i) : 0.f;
             sum[0] = fmaf(v.x, xv[0], sum[0]);
             sum[1] = fmaf(v.y, xv[1], sum[1]);
             sum[2] = fmaf(v.z, xv[2], sum[2]);
@@ -97,6 +98,11 @@ __device__ __forceinline__ void dia_rows4(const DiaArgs<float>& A, const float* 
         for (int i = 0; i < 4; ++i)
             if (r + i < A.nrows) op.post(r + i, pre[i], sum[i]);
     }
+}
+
+template <int ND, typename Op>
+__device__ __forceinline__ void dia_rows4(const DiaArgs<float>& A, const float* __restrict__ x, Op& op) {
+    dia_rows4_gather<ND>(A, LoadGather<float>{x}, op);
 }
 
 // Calls f(std::integral_constant<int, ND>) with ND = 27, 9 or 0 (runtime count).

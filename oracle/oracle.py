@@ -55,6 +55,7 @@ class Restatement:
             "ora_dirichlet_eliminate": (None, [_i, _P, _P, _P, _P, _P]),
             "ora_cut_cell_points": (_i, [_i, _i, _i, _P, _d, _P, _P, _i, _P, _P, _P, _d]),
             "ora_cut_cell_points_halfspace": (_i, [_i, _i, _i, _P, _d, _P, _P, _i, _P, _P, _P, _d]),
+            "ora_cuthill_mckee": (_i, [_i, _P, _P, _i, _P]),
             "ora_random_uniform": (None, [_u64, _l, _P]),
             "ora_random_normal": (None, [_u64, _l, _P]),
             "ora_kappa_field": (None, [_u64, _i, _P, _d, _i, _P]),
@@ -192,6 +193,15 @@ class Restatement:
         assert n >= 0
         return pts[: n * dim].reshape(n, dim), w[:n], s[:n]
 
+    # -- graph --
+    def cuthill_mckee(self, rowptr, col, strategy=1):
+        """(map, largest batch queued at once)."""
+        n = len(rowptr) - 1
+        out = np.zeros(n, dtype=np.int32)
+        largest = self.L.ora_cuthill_mckee(n, p(rowptr), p(col), int(strategy), p(out))
+        assert largest >= 0
+        return out, largest
+
     # -- seeded workload inputs --
     def random_uniform(self, seed, n):
         out = np.zeros(int(n))
@@ -276,6 +286,8 @@ class Reference:
             "cieref_space_op": (_i, [_P, _i, _l, _P, _P, _d]),
             "cieref_gauss_legendre": (_i, [_i, _P, _P]),
             "cieref_lagrange": (_i, [_i, _P, _i, _i, _P, _P, _P, _P]),
+            "cieref_make_reordering": (_i, [_i, _P, _P, _P, _i, _P]),
+            "cieref_reorder": (_i, [_i, _P, _P, _P, _P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -357,6 +369,70 @@ class Reference:
         n, w = np.zeros(order), np.zeros(order)
         self._check(self.L.cieref_gauss_legendre(order, p(n), p(w)))
         return n, w
+
+    def make_reordering(self, rowptr, col, val, strategy):
+        """makeReordering (serial): map[new row] = old row; strategy 1 CM, 2 RCM."""
+        n = len(rowptr) - 1
+        out = np.zeros(n, dtype=np.int32)
+        self._check(self.L.cieref_make_reordering(n, p(rowptr), p(col), p(np.ascontiguousarray(val, np.float64)),
+                                                  int(strategy), p(out)))
+        return out
+
+    def reorder(self, mapping, rowptr, col, val):
+        """reorder<int,double,false> on copies: the permuted (rowptr, col, val)."""
+        rp, c, v = (np.array(a, copy=True) for a in (rowptr, col, val))
+        self._check(self.L.cieref_reorder(len(rp) - 1, p(np.ascontiguousarray(mapping, np.int32)), p(rp), p(c), p(v)))
+        return rp, c, v
+
+    # The reference's stream writer crashes (SIGSEGV in the C++ stream's number
+    # formatting) in a process that has imported numpy, whose bundled runtime
+    # libraries it then shares; so it runs in a child interpreter that loads only
+    # ctypes and the reference library, on arrays passed through a file.
+    _MM_CHILD = """
+import array, ctypes, sys
+lib = ctypes.CDLL(sys.argv[1])
+kind, src, dst = sys.argv[2], sys.argv[3], sys.argv[4].encode()
+with open(src, "rb") as f:
+    head = array.array("q"); head.fromfile(f, 3)
+    ints = array.array("i"); vals = array.array("d")
+    if kind == "csr":
+        ints.fromfile(f, head[0] + 1 + head[2])
+    vals.fromfile(f, head[2])
+ip = (ctypes.c_int * max(len(ints), 1)).from_buffer(ints) if len(ints) else None
+vp = (ctypes.c_double * max(len(vals), 1)).from_buffer(vals) if len(vals) else None
+P = ctypes.c_void_p
+if kind == "csr":
+    base = ctypes.addressof(ip)
+    st = lib.cieref_matrix_market(ctypes.c_char_p(dst), ctypes.c_int(head[0]), ctypes.c_int(head[1]), P(base),
+                                  P(base + 4 * (head[0] + 1)), P(ctypes.addressof(vp) if vp else 0))
+else:
+    st = lib.cieref_matrix_market_vector(ctypes.c_char_p(dst), ctypes.c_long(head[2]),
+                                         P(ctypes.addressof(vp) if vp else 0))
+sys.exit(st)
+"""
+
+    def _matrix_market_child(self, kind, path, head, ints, vals):
+        import sys
+        import tempfile
+        with tempfile.NamedTemporaryFile(suffix=".bin", delete=False) as f:
+            np.asarray(head, dtype=np.int64).tofile(f)
+            if ints is not None:
+                np.ascontiguousarray(ints, dtype=np.int32).tofile(f)
+            np.ascontiguousarray(vals, dtype=np.float64).tofile(f)
+            name = f.name
+        try:
+            subprocess.run([sys.executable, "-c", self._MM_CHILD, REF_PATH, kind, name, str(path)], check=True)
+        finally:
+            os.unlink(name)
+
+    def matrix_market(self, path, rowptr, col, val, columns=None):
+        """cie::io::MatrixMarket::Output for a CSR matrix, written to `path`."""
+        n = len(rowptr) - 1
+        ints = np.concatenate([np.asarray(rowptr, np.int32), np.asarray(col, np.int32)])
+        self._matrix_market_child("csr", path, [n, n if columns is None else columns, len(col)], ints, val)
+
+    def matrix_market_vector(self, path, values):
+        self._matrix_market_child("vector", path, [0, 0, len(values)], None, values)
 
     def lagrange(self, nodes, iBase, points):
         """The reference's LagrangePolynomial of node iBase: (ascending coefficients,

@@ -17,6 +17,9 @@
 //   * cieref_pmg        -> executables/fem_examples/src/poisson2D/solver.cpp:111-232
 //   * cieref_space_*    -> linalg/packages/solvers/src/DefaultSpace.cpp:50-187
 //   * cieref_gauss_legendre -> fem/packages/numeric/src/GaussLegendreQuadrature.cpp:82-175
+//   * cieref_make_reordering -> linalg/packages/utilities/src/reorder.cpp:23-173 (serial: no pool)
+//   * cieref_reorder    -> linalg/packages/utilities/src/reorder.cpp:215-365
+//   * cieref_matrix_market[_vector] -> cieutils/packages/io/src/MatrixMarket.cpp
 //   * cieref_lagrange   -> fem/packages/maths/src/LagrangePolynomial.cpp:18-72 (coefficients),
 //                          fem/packages/maths/impl/Polynomial_impl.hpp (Horner evaluation,
 //                          makeDerivative)
@@ -31,12 +34,15 @@
 #include "packages/concurrency/inc/ThreadPoolBase.hpp"
 #include "packages/numeric/inc/GaussLegendreQuadrature.hpp"
 #include "packages/maths/inc/LagrangePolynomial.hpp"
+#include "packages/utilities/inc/reorder.hpp"
+#include "packages/io/inc/MatrixMarket.hpp"
 
 #include <chrono>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <exception>
+#include <fstream>
 #include <memory>
 #include <span>
 #include <string>
@@ -386,6 +392,61 @@ int cieref_lagrange(int count, const double* nodes, int iBase, int npts, const d
             derivatives[i] = out[0];
         }
         return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+// makeReordering<int,double> without a thread pool (the pool's minimum-degree
+// search combines per-thread minima, which can pick another start row among
+// equal degrees): map[new row] = old row.  strategy 1: Cuthill-McKee, 2: reverse.
+int cieref_make_reordering(int n, const int* rowptr, const int* col, const double* val, int strategy, int* map) {
+    try {
+        const std::size_t nnz = static_cast<std::size_t>(rowptr[n]);
+        makeReordering<int, double>(std::span<int>(map, static_cast<std::size_t>(n)),
+                                    std::span<const int>(rowptr, static_cast<std::size_t>(n) + 1),
+                                    std::span<const int>(col, nnz), std::span<const double>(val, nnz),
+                                    strategy == 2 ? ReorderingStrategy::ReverseCuthillMcKee
+                                                  : ReorderingStrategy::CuthillMcKee,
+                                    {});
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+// reorder<int,double,false>: the CSR matrix permuted in place, new row i = old row
+// map[i], columns renumbered and sorted within each row.
+int cieref_reorder(int n, const int* map, int* rowptr, int* col, double* val) {
+    try {
+        const std::size_t nnz = static_cast<std::size_t>(rowptr[n]);
+        reorder<int, double, false>(std::span<const int>(map, static_cast<std::size_t>(n)),
+                                    std::span<int>(rowptr, static_cast<std::size_t>(n) + 1), std::span<int>(col, nnz),
+                                    std::span<double>(val, nnz), {});
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+int cieref_matrix_market(const char* path, int rows, int columns, const int* rowptr, const int* col,
+                         const double* val) {
+    try {
+        std::ofstream file(path);
+        io::MatrixMarket::Output out(file);
+        out(rows, columns, rowptr[rows], rowptr, col, val);
+        return file.good() ? 0 : 1;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+int cieref_matrix_market_vector(const char* path, long n, const double* values) {
+    try {
+        std::ofstream file(path);
+        io::MatrixMarket::Output out(file);
+        out(values, static_cast<std::size_t>(n));
+        return file.good() ? 0 : 1;
     } catch (const std::exception& e) {
         return fail(e);
     }

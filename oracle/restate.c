@@ -866,3 +866,58 @@ int ora_assemble_structured(int dim, int order, int quadratureOrder, const int* 
     free(gtab); free(wq); free(S);
     return missing;
 }
+
+/* ---- graph ------------------------------------------------------------------ */
+
+/* Cuthill-McKee ordering of linalg/packages/utilities/src/reorder.cpp:23-173,
+ * sequentially: start at the least-degree row (lowest index among equals), visit
+ * rows in FIFO order, queue each visited row's unqueued neighbours in column
+ * order and then order that batch by degree with a stable sort (insertion), and
+ * restart at the least-degree unqueued row when the queue is empty; reverse for
+ * RCM (strategy 2).  map[k] = the row placed at k.  Returns the largest batch
+ * queued at once (the reference's std::sort keeps the column order of equal
+ * degrees only for batches of at most 16 rows), or -1 on a bad column. */
+int ora_cuthill_mckee(int n, const int* rowptr, const int* col, int strategy, int* map) {
+    if (n <= 0) return 0;
+    int* degree = (int*)malloc(sizeof(int) * (size_t)n);
+    char* queued = (char*)calloc((size_t)n, 1);
+    int* queue = (int*)malloc(sizeof(int) * (size_t)n);
+    int head = 0, tail = 0, placed = 0, largest = 0;
+    for (int i = 0; i < n; ++i) degree[i] = rowptr[i + 1] - rowptr[i];
+    while (placed < n) {
+        if (head == tail) {
+            int best = -1;
+            for (int i = 0; i < n; ++i)
+                if (!queued[i] && (best < 0 || degree[i] < degree[best])) best = i;
+            queue[tail++] = best;
+            queued[best] = 1;
+        }
+        const int u = queue[head++];
+        const int batch = tail;
+        for (int e = rowptr[u]; e < rowptr[u + 1]; ++e) {
+            const int v = col[e];
+            if (v < 0 || v >= n) { free(degree); free(queued); free(queue); return -1; }
+            if (!queued[v]) {
+                queued[v] = 1;
+                /* stable insertion by degree into the batch */
+                int pos = tail;
+                while (pos > batch && degree[queue[pos - 1]] > degree[v]) {
+                    queue[pos] = queue[pos - 1];
+                    --pos;
+                }
+                queue[pos] = v;
+                ++tail;
+            }
+        }
+        if (tail - batch > largest) largest = tail - batch;
+        map[placed++] = u;
+    }
+    if (strategy == 2)
+        for (int i = 0; i < n / 2; ++i) {
+            const int t = map[i];
+            map[i] = map[n - 1 - i];
+            map[n - 1 - i] = t;
+        }
+    free(degree); free(queued); free(queue);
+    return largest;
+}

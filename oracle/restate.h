@@ -60,6 +60,9 @@ int ora_cut_cell_points_halfspace(int dim, int depth, int order, const double* n
                                   const double* cellOrigin, const double* cellSize, int maxPoints,
                                   double* points, double* weights, double* scales, double alpha);
 
+/* ---- graph ----------------------------------------------------------- */
+int ora_cuthill_mckee(int n, const int* rowptr, const int* col, int strategy, int* map);
+
 /* ---- seeded workload inputs (no CUDA library needed) ------------------ */
 void ora_random_uniform(uint64_t seed, long n, double* out);
 void ora_random_normal(uint64_t seed, long n, double* out);
