@@ -244,6 +244,51 @@ void convention_factors(int dim, const double* h, int convention, double& scale,
     }
 }
 
+// ---- Dirichlet penalty on boundary faces -------------------------------------
+
+// One thread per (face, a, b) with a and b on the face: the face mass term
+// penalty |J| sum_q w_q N_q[a] N_q[b] added into the CSR entry.  `onFace` lists
+// the local indices of the face's basis functions (the others vanish there).
+__global__ void penalty_matrix_kernel(long faces, int nb, int nf, int nqf, const int* __restrict__ faceCells,
+                                      const int* __restrict__ onFace, const double* __restrict__ table,
+                                      const double* __restrict__ wq, double scale, const int* __restrict__ slots,
+                                      double* __restrict__ val) {
+    const long total = faces * nf * nf;
+    for (long t = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; t < total;
+         t += static_cast<long>(gridDim.x) * blockDim.x) {
+        const long f = t / (nf * nf);
+        const int ij = static_cast<int>(t - f * nf * nf);
+        const int a = onFace[ij / nf], b = onFace[ij % nf];
+        double s = 0.0;
+        for (int q = 0; q < nqf; ++q) s = fma(wq[q] * table[q * nb + a], table[q * nb + b], s);
+        const long e = faceCells[f];
+        const int slot = slots[e * nb * nb + a * nb + b];
+        val[slot] = fma(scale, s, val[slot]);
+    }
+}
+
+// One thread per (face, a) with a on the face: penalty |J| sum_q w_q N_q[a] u_d(x_q),
+// u_d(x_q) = sum_b N_q[b] g[dof_b], added into rhs[dof_a].
+__global__ void penalty_rhs_kernel(long faces, int nb, int nf, int nqf, const int* __restrict__ faceCells,
+                                   const int* __restrict__ onFace, const double* __restrict__ table,
+                                   const double* __restrict__ wq, double scale, const int* __restrict__ dofmap,
+                                   const double* __restrict__ g, double* __restrict__ rhs) {
+    const long total = faces * nf;
+    for (long t = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; t < total;
+         t += static_cast<long>(gridDim.x) * blockDim.x) {
+        const long f = t / nf;
+        const int a = onFace[t - f * nf];
+        const int* dofs = dofmap + static_cast<long>(faceCells[f]) * nb;
+        double s = 0.0;
+        for (int q = 0; q < nqf; ++q) {
+            double ud = 0.0;
+            for (int j = 0; j < nf; ++j) ud = fma(table[q * nb + onFace[j]], g[dofs[onFace[j]]], ud);
+            s = fma(wq[q] * table[q * nb + a], ud, s);
+        }
+        rhs[dofs[a]] = fma(scale, s, rhs[dofs[a]]);
+    }
+}
+
 // ---- embedded (finite-cell) stiffness -----------------------------------------
 
 constexpr int kEmbThreads = 256;
@@ -723,6 +768,154 @@ int ciecu_adjoint_gradient(ciecu_pcg solver, ciecu_assembly P, const double* h_c
         u = uMasked;
     }
     return ciecu_element_gradient(P, h_cellSize, convention, lam, u, d_gradKappa, unit);
+}
+
+int ciecu_assemble_dirichlet_penalty(ciecu_assembly P, const int32_t* h_cells, const double* h_cellSize,
+                                     double penalty, int faceMask, int quadratureOrder,
+                                     const double* d_boundaryValues, double* d_entries, double* d_rhs) {
+    CIECU_REQUIRE(P && h_cells && h_cellSize && d_entries, "assemble_dirichlet_penalty: null argument");
+    CIECU_REQUIRE(quadratureOrder >= 0 && quadratureOrder <= 16, "assemble_dirichlet_penalty: quadrature order in [0, 16]");
+    CIECU_REQUIRE(faceMask >= 0 && faceMask < (1 << (2 * P->dim)), "assemble_dirichlet_penalty: invalid face mask");
+    CIECU_REQUIRE(!d_boundaryValues || d_rhs, "assemble_dirichlet_penalty: boundary values need a right-hand side");
+    const int dim = P->dim, p = P->order, n1 = p + 1, nb = P->nb;
+    long c[3] = {1, 1, 1}, total = 1;
+    for (int d = 0; d < dim; ++d) {
+        CIECU_REQUIRE(h_cells[d] >= 1, "assemble_dirichlet_penalty: empty grid");
+        c[d] = h_cells[d];
+        total *= h_cells[d];
+    }
+    CIECU_REQUIRE(total == P->ncells, "assemble_dirichlet_penalty: grid size differs from the plan's cell count");
+    if (faceMask == 0) faceMask = (1 << (2 * dim)) - 1;
+    const int q1 = quadratureOrder ? quadratureOrder : P->q1;
+    std::vector<double> gn, gw;
+    gauss_legendre(q1, gn, gw);
+    int nqf = 1;
+    for (int d = 1; d < dim; ++d) nqf *= q1;
+    cudaStream_t st = P->csr->space->stream;
+    // per side: face point basis table (nqf x nb), weights, on-face indices, and
+    // the side's cells by colour
+    struct Side {
+        std::vector<double> table, wq;
+        std::vector<int> onFace;
+        std::vector<std::vector<int>> colors;
+        double jac;
+    };
+    std::vector<Side> sides;
+    size_t doubles = 0, ints = 0;
+    for (int side = 0; side < 2 * dim; ++side) {
+        if (!((faceMask >> side) & 1)) continue;
+        const int dn = side / 2, hi = side % 2;
+        Side S;
+        S.jac = 1.0;
+        int tang[2] = {0, 0}, nt = 0;
+        for (int d = 0; d < dim; ++d)
+            if (d != dn) {
+                tang[nt++] = d;
+                S.jac *= 0.5 * h_cellSize[d];
+            }
+        S.table.assign(static_cast<size_t>(nqf) * nb, 0.0);
+        S.wq.assign(static_cast<size_t>(nqf), 1.0);
+        std::vector<double> v(n1), dv(n1);
+        for (int q = 0; q < nqf; ++q) {
+            double xi[3] = {0.0, 0.0, 0.0};
+            int rest = q;
+            for (int t = 0; t < nt; ++t) {
+                const int i = rest % q1;
+                rest /= q1;
+                xi[tang[t]] = gn[i];
+                S.wq[q] *= gw[i];
+            }
+            xi[dn] = hi ? 1.0 : -1.0;
+            double vals[3][16];
+            for (int d = 0; d < dim; ++d) {
+                lagrange(p, xi[d], v.data(), dv.data());
+                for (int i = 0; i < n1; ++i) vals[d][i] = v[i];
+            }
+            for (int a = 0; a < nb; ++a) {
+                int ra = a;
+                double prod = 1.0;
+                for (int d = 0; d < dim; ++d) {
+                    prod *= vals[d][ra % n1];
+                    ra /= n1;
+                }
+                S.table[static_cast<size_t>(q) * nb + a] = prod;
+            }
+        }
+        for (int a = 0; a < nb; ++a) {
+            int ra = a, id = 0;
+            for (int d = 0; d <= dn; ++d) {
+                id = ra % n1;
+                ra /= n1;
+            }
+            if (id == (hi ? p : 0)) S.onFace.push_back(a);
+        }
+        const int ncol = 1 << (dim - 1);
+        S.colors.assign(static_cast<size_t>(ncol), {});
+        for (long e = 0; e < total; ++e) {
+            const long co[3] = {e % c[0], (e / c[0]) % c[1], e / (c[0] * c[1])};
+            if (co[dn] != (hi ? c[dn] - 1 : 0)) continue;
+            int color = 0;
+            for (int t = 0; t < nt; ++t) color |= static_cast<int>(co[tang[t]] & 1) << t;
+            S.colors[static_cast<size_t>(color)].push_back(static_cast<int>(e));
+        }
+        doubles += S.table.size() + S.wq.size();
+        ints += S.onFace.size();
+        for (auto& l : S.colors) ints += l.size();
+        sides.push_back(std::move(S));
+    }
+    if (sides.empty()) return CIECU_OK;
+    // one device buffer for every side's tables and lists
+    std::vector<double> hostDoubles;
+    std::vector<int> hostInts;
+    hostDoubles.reserve(doubles);
+    hostInts.reserve(ints);
+    for (auto& S : sides) {
+        hostDoubles.insert(hostDoubles.end(), S.table.begin(), S.table.end());
+        hostDoubles.insert(hostDoubles.end(), S.wq.begin(), S.wq.end());
+        hostInts.insert(hostInts.end(), S.onFace.begin(), S.onFace.end());
+        for (auto& l : S.colors) hostInts.insert(hostInts.end(), l.begin(), l.end());
+    }
+    void* buf = nullptr;
+    const size_t bytes = sizeof(double) * hostDoubles.size() + sizeof(int) * std::max<size_t>(hostInts.size(), 1);
+    CIECU_CUDA(cudaMalloc(&buf, bytes));
+    double* dd = static_cast<double*>(buf);
+    int* di = reinterpret_cast<int*>(dd + hostDoubles.size());
+    cudaError_t e = cudaMemcpyAsync(dd, hostDoubles.data(), sizeof(double) * hostDoubles.size(), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && !hostInts.empty())
+        e = cudaMemcpyAsync(di, hostInts.data(), sizeof(int) * hostInts.size(), cudaMemcpyHostToDevice, st);
+    size_t od = 0, oi = 0;
+    for (auto& S : sides) {
+        if (e != cudaSuccess) break;
+        const double* table = dd + od;
+        const double* wq = table + S.table.size();
+        const int* onFace = di + oi;
+        od += S.table.size() + S.wq.size();
+        oi += S.onFace.size();
+        const int nf = static_cast<int>(S.onFace.size());
+        const double scale = penalty * S.jac;
+        for (auto& l : S.colors) {
+            const int* faceCells = di + oi;
+            oi += l.size();
+            const long faces = static_cast<long>(l.size());
+            if (faces == 0) continue;
+            penalty_matrix_kernel<<<grid_for(faces * nf * nf, kT, 8), kT, 0, st>>>(
+                faces, nb, nf, nqf, faceCells, onFace, table, wq, scale, P->d_slots, d_entries);
+            count_launch();
+            if (d_boundaryValues) {
+                penalty_rhs_kernel<<<grid_for(faces * nf, kT, 8), kT, 0, st>>>(
+                    faces, nb, nf, nqf, faceCells, onFace, table, wq, scale, P->d_dofmap, d_boundaryValues, d_rhs);
+                count_launch();
+            }
+            e = cudaGetLastError();
+            if (e != cudaSuccess) break;
+        }
+    }
+    // the buffer is in use by the launches above: free after they finish
+    const cudaError_t s2 = cudaStreamSynchronize(st);
+    cudaFree(buf);
+    if (e != cudaSuccess) return cuda_fail(e, "assemble_dirichlet_penalty");
+    if (s2 != cudaSuccess) return cuda_fail(s2, "assemble_dirichlet_penalty");
+    return CIECU_OK;
 }
 
 int ciecu_dirichlet_eliminate(ciecu_csr csr, const uint8_t* d_isBoundary, double* d_entries, double* d_rhs) {

@@ -140,6 +140,21 @@ class Assembler:
         self.space.leave()
         return cut.value
 
+    def dirichlet_penalty(self, penalty, faceMask=0, quadratureOrder=0, boundaryValues=None, rhs=None,
+                          entries=None):
+        """Weak Dirichlet condition by penalty on the box faces selected by faceMask
+        (bit 2d: x_d = 0, bit 2d + 1: x_d = max; 0 = all): the face terms of
+        DirichletPenaltyIntegrand added to the matrix and, for nodal boundary values
+        (a device vector over the DoFs), to rhs (ciecu_assemble_dirichlet_penalty)."""
+        entries = self.matrix.entries if entries is None else entries
+        m = self.mesh
+        h = np.ascontiguousarray(m.h, dtype=np.float64)
+        cells = np.ascontiguousarray(m.cells, dtype=np.int32)
+        self.space.enter()
+        call("ciecu_assemble_dirichlet_penalty", self.handle, _np_ptr(cells), _np_ptr(h), float(penalty),
+             int(faceMask), int(quadratureOrder), _ptr(boundaryValues), _ptr(entries), _ptr(rhs))
+        self.space.leave()
+
     def dirichlet(self, isBoundary, rhs=None, entries=None):
         entries = self.matrix.entries if entries is None else entries
         self.space.enter()

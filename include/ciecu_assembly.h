@@ -80,6 +80,27 @@ int ciecu_adjoint_gradient(ciecu_pcg solver, ciecu_assembly plan, const double* 
                            const uint8_t* d_isBoundary, const double* d_u, const double* d_dJdu, double* d_lambda,
                            double* d_gradKappa, double* d_work, ciecu_statistics* h_stats);
 
+/* Weak Dirichlet condition by penalty on the faces of the box of a structured
+ * grid: DirichletPenaltyIntegrand (fem/packages/integrands/impl/DirichletPenaltyIntegrand_impl.hpp:38-88)
+ * integrated over boundary faces and scattered as in constraints.cpp:306-380.
+ * On every boundary face selected by faceMask (bit 2d: the face x_d = 0 of the
+ * box, bit 2d + 1: the face x_d = max; 0 selects all), at the tensor
+ * Gauss-Legendre points of the face (quadratureOrder per tangential axis; 0 =
+ * the plan's order):
+ *     K_e += penalty |J| w_q N(xi_q) N(xi_q)^T
+ *     f_e += penalty |J| w_q u_d(x_q) N(xi_q)
+ * where N are the cell's Q_p basis functions at the face point's parametric
+ * coordinates, |J| = prod over the face's tangential axes of h_t / 2 (the
+ * embedding's Jacobian, TransformedIntegrand.hpp:73-83), and the prescribed value
+ * u_d = sum_b N_b(xi) g_b interpolates nodal values g (d_boundaryValues, one per
+ * DoF; NULL: u_d = 0, and d_rhs is untouched).  Faces of one side are scattered
+ * by colour (parity of the tangential cell coordinates), sides one after another:
+ * no atomics.  h_cells: the grid's cells per axis (cell e at (e % cells[0], ...)),
+ * matching the plan's cell count. */
+int ciecu_assemble_dirichlet_penalty(ciecu_assembly plan, const int32_t* h_cells, const double* h_cellSize,
+                                     double penalty, int faceMask, int quadratureOrder,
+                                     const double* d_boundaryValues, double* d_entries, double* d_rhs);
+
 /* Symmetric elimination of homogeneous Dirichlet DoFs (fem/test/test_1d.cpp:291-313):
  * rows and columns of boundary DoFs zeroed (structural zeros kept), diagonal 1,
  * d_rhs[boundary] = 0 (d_rhs may be NULL). */

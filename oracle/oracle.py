@@ -56,6 +56,7 @@ class Restatement:
             "ora_cut_cell_points": (_i, [_i, _i, _i, _P, _d, _P, _P, _i, _P, _P, _P, _d]),
             "ora_cut_cell_points_halfspace": (_i, [_i, _i, _i, _P, _d, _P, _P, _i, _P, _P, _P, _d]),
             "ora_cuthill_mckee": (_i, [_i, _P, _P, _i, _P]),
+            "ora_dirichlet_penalty": (_i, [_i, _i, _i, _P, _P, _d, _i, _P, _P, _P, _P, _P, _P]),
             "ora_random_uniform": (None, [_u64, _l, _P]),
             "ora_random_normal": (None, [_u64, _l, _P]),
             "ora_kappa_field": (None, [_u64, _i, _P, _d, _i, _P]),
@@ -192,6 +193,21 @@ class Restatement:
                                                  p(s), alpha)
         assert n >= 0
         return pts[: n * dim].reshape(n, dim), w[:n], s[:n]
+
+    def dirichlet_penalty(self, dim, order, cells, penalty, rowptr, col, val, faceMask=0, g=None, rhs=None,
+                          quadratureOrder=None):
+        """Penalty Dirichlet terms added to copies of val (and rhs when g is given)."""
+        cells = np.ascontiguousarray(cells, dtype=np.int32)
+        h = 1.0 / cells.astype(np.float64)
+        dofmap = self.structured_dofmap(dim, order, cells)
+        val = np.array(val, dtype=np.float64, copy=True)
+        rhs = None if rhs is None else np.array(rhs, dtype=np.float64, copy=True)
+        g = None if g is None else np.ascontiguousarray(g, dtype=np.float64)
+        st = self.L.ora_dirichlet_penalty(dim, order, order + 1 if quadratureOrder is None else quadratureOrder,
+                                          p(cells), p(h), float(penalty), int(faceMask), p(g), p(dofmap), p(rowptr),
+                                          p(col), p(val), p(rhs))
+        assert st == 0
+        return val, rhs
 
     # -- graph --
     def cuthill_mckee(self, rowptr, col, strategy=1):

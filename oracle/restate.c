@@ -921,3 +921,88 @@ int ora_cuthill_mckee(int n, const int* rowptr, const int* col, int strategy, in
     free(degree); free(queued); free(queue);
     return largest;
 }
+
+/* Weak Dirichlet condition by penalty on the faces of the box of a structured
+ * Q_order grid: DirichletPenaltyIntegrand::evaluate
+ * (fem/packages/integrands/impl/DirichletPenaltyIntegrand_impl.hpp:38-88) -- at a
+ * boundary point, LHS = N penalty N^T and RHS = penalty u_d N -- times the
+ * weight and the embedding Jacobian |J| = prod over the tangential axes of h/2
+ * (TransformedIntegrand.hpp:73-83), summed over the tensor Gauss points of every
+ * selected face (faceMask bit 2d: x_d = 0, bit 2d+1: x_d = max; 0 = all) and
+ * scattered like Assembler::addContribution (constraints.cpp:306-380).
+ * u_d = sum_b N_b g_b from nodal values g (NULL: no RHS).  Returns 0, or 1 when
+ * an entry is missing from the pattern. */
+int ora_dirichlet_penalty(int dim, int order, int quadratureOrder, const int* cells, const double* h,
+                          double penalty, int faceMask, const double* g, const int* dofmap, const int* rowptr,
+                          const int* col, double* val, double* rhs) {
+    const int n1 = order + 1;
+    int nb = 1;
+    long c[3] = {1, 1, 1}, ncells = 1;
+    for (int d = 0; d < dim; ++d) {
+        nb *= n1;
+        c[d] = cells[d];
+        ncells *= cells[d];
+    }
+    double gn[16], gw[16], nodes[16];
+    if (ora_gauss_legendre(quadratureOrder, gn, gw)) return 1;
+    for (int i = 0; i < n1; ++i) nodes[i] = -1.0 + 2.0 * i / order;
+    if (faceMask == 0) faceMask = (1 << (2 * dim)) - 1;
+    int nqf = 1;
+    for (int d = 1; d < dim; ++d) nqf *= quadratureOrder;
+    double* N = (double*)malloc(sizeof(double) * (size_t)nb);
+    for (int side = 0; side < 2 * dim; ++side) {
+        if (!((faceMask >> side) & 1)) continue;
+        const int dn = side / 2, hi = side % 2;
+        double jac = 1.0;
+        for (int d = 0; d < dim; ++d)
+            if (d != dn) jac *= 0.5 * h[d];
+        for (long e = 0; e < ncells; ++e) {
+            const long co[3] = {e % c[0], (e / c[0]) % c[1], e / (c[0] * c[1])};
+            if (co[dn] != (hi ? c[dn] - 1 : 0)) continue;
+            const int* dofs = dofmap + e * nb;
+            for (int q = 0; q < nqf; ++q) {
+                double xi[3] = {0.0, 0.0, 0.0}, w = 1.0;
+                int rest = q;
+                for (int d = 0; d < dim; ++d) {
+                    if (d == dn) continue;
+                    const int i = rest % quadratureOrder;
+                    rest /= quadratureOrder;
+                    xi[d] = gn[i];
+                    w *= gw[i];
+                }
+                xi[dn] = hi ? 1.0 : -1.0;
+                double vals[3][16], ders[3][16];
+                for (int d = 0; d < dim; ++d) ora_lagrange_1d(n1, nodes, xi[d], vals[d], ders[d]);
+                for (int a = 0; a < nb; ++a) {
+                    int ra = a;
+                    double prod = 1.0;
+                    for (int d = 0; d < dim; ++d) {
+                        prod *= vals[d][ra % n1];
+                        ra /= n1;
+                    }
+                    N[a] = prod;
+                }
+                const double s = w * jac * penalty;
+                for (int a = 0; a < nb; ++a) {
+                    const int row = dofs[a];
+                    for (int b = 0; b < nb; ++b) {
+                        int lo = rowptr[row], hiE = rowptr[row + 1];
+                        while (lo < hiE) {
+                            const int mid = lo + (hiE - lo) / 2;
+                            if (col[mid] < dofs[b]) lo = mid + 1; else hiE = mid;
+                        }
+                        if (lo == rowptr[row + 1] || col[lo] != dofs[b]) { free(N); return 1; }
+                        val[lo] += s * N[a] * N[b];
+                    }
+                }
+                if (g && rhs) {
+                    double ud = 0.0;
+                    for (int b = 0; b < nb; ++b) ud += N[b] * g[dofs[b]];
+                    for (int a = 0; a < nb; ++a) rhs[dofs[a]] += s * ud * N[a];
+                }
+            }
+        }
+    }
+    free(N);
+    return 0;
+}

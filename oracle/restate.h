@@ -60,6 +60,10 @@ int ora_cut_cell_points_halfspace(int dim, int depth, int order, const double* n
                                   const double* cellOrigin, const double* cellSize, int maxPoints,
                                   double* points, double* weights, double* scales, double alpha);
 
+int ora_dirichlet_penalty(int dim, int order, int quadratureOrder, const int* cells, const double* h,
+                          double penalty, int faceMask, const double* g, const int* dofmap, const int* rowptr,
+                          const int* col, double* val, double* rhs);
+
 /* ---- graph ----------------------------------------------------------- */
 int ora_cuthill_mckee(int n, const int* rowptr, const int* col, int strategy, int* map);
 
