@@ -128,6 +128,8 @@ SIGNATURES = {
     "ciecu_reorder_vector": (c_int, [P, c_int64, P, c_int, P, P]),
     "ciecu_csr_pattern_device": (c_int, [P, c_int64, c_int, P, ctypes.c_int32, P, P, P]),
     "ciecu_assemble_dirichlet_penalty": (c_int, [P, P, P, c_double, c_int, c_int, P, P, P]),
+    "ciecu_assemble_embedded_f32": (c_int, [P, P, P, P, P, P, c_double, c_double, c_int, c_int, c_int, P, P]),
+    "ciecu_dirichlet_eliminate_f32": (c_int, [P, P, P]),
 }
 
 OPTIONAL = set()

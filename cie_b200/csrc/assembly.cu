@@ -14,27 +14,13 @@
 //   K_e[a][b] = scale_e * sum_q w_q sum_d f_d G[q][d][a] G[q][d][b]
 //   reference convention (0): scale_e = kappa_e prod_d 2/h_d, f_d = 1
 //   physical convention  (1): scale_e = kappa_e prod_d h_d/2, f_d = (2/h_d)^2
-#include "ciecu_assembly.h"
-#include "spmv.cuh"
+#include "assembly.cuh"
 #include "space.cuh"
 
 #include <cmath>
 #include <string>
 #include <vector>
 
-struct ciecu_assembly_s {
-    ciecu_csr_s* csr = nullptr;
-    int dim = 0, order = 0, nb = 0, nq = 0;
-    long ncells = 0;
-    const int* d_dofmap = nullptr;
-    int* d_cellOrder = nullptr;       // cells sorted by colour
-    std::vector<long> colorOffsets;   // host
-    int* d_slots = nullptr;           // ncells * nb * nb CSR entry indices
-    double* d_gtab = nullptr;         // nq * dim * nb parametric gradients
-    double* d_wq = nullptr;           // nq weights
-    int q1 = 0;                       // 1-D quadrature points (nq = q1^dim)
-    std::vector<double> gn, gw;       // 1-D Gauss-Legendre rule on [-1, 1]
-};
 
 namespace ciecu {
 
@@ -80,24 +66,6 @@ int gauss_legendre(int order, std::vector<double>& nodes, std::vector<double>& w
     }
     if (order % 2 == 1) nodes[order / 2] = 0.0;
     return CIECU_OK;
-}
-
-// Lagrange basis on equispaced nodes -1 + 2i/p and its derivative at x.
-__host__ __device__ void lagrange(int p, double x, double* v, double* dv) {
-    const int n = p + 1;
-    double nodes[16];
-    for (int i = 0; i < n; ++i) nodes[i] = -1.0 + 2.0 * i / p;
-    for (int i = 0; i < n; ++i) {
-        double value = 1.0, deriv = 0.0;
-        for (int j = 0; j < n; ++j) {
-            if (j == i) continue;
-            const double f = (x - nodes[j]) / (nodes[i] - nodes[j]);
-            deriv = deriv * f + value / (nodes[i] - nodes[j]);
-            value *= f;
-        }
-        v[i] = value;
-        dv[i] = deriv;
-    }
 }
 
 namespace {
@@ -212,13 +180,14 @@ __global__ void element_gradient_kernel(long ncells, int nb, const int* __restri
     }
 }
 
+template <typename V>
 __global__ void dirichlet_kernel(int n, const int* __restrict__ rowptr, const int* __restrict__ col,
-                                 double* __restrict__ val, const uint8_t* __restrict__ bnd, double* __restrict__ rhs) {
+                                 V* __restrict__ val, const uint8_t* __restrict__ bnd, double* __restrict__ rhs) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const bool bi = bnd[i] != 0;
         for (int k = rowptr[i]; k < rowptr[i + 1]; ++k) {
             const int j = col[k];
-            if (bi || bnd[j]) val[k] = (i == j) ? 1.0 : 0.0;
+            if (bi || bnd[j]) val[k] = (i == j) ? V(1) : V(0);
         }
         if (rhs && bi) rhs[i] = 0.0;
     }
@@ -229,19 +198,6 @@ __global__ void interior_kernel(int n, const double* __restrict__ v, const uint8
                                 double* __restrict__ out) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         out[i] = bnd[i] ? 0.0 : v[i];
-}
-
-void convention_factors(int dim, const double* h, int convention, double& scale, double f[3]) {
-    scale = 1.0;
-    for (int d = 0; d < 3; ++d) f[d] = 1.0;
-    for (int d = 0; d < dim; ++d) {
-        if (convention == 1) {
-            scale *= 0.5 * h[d];
-            f[d] = (2.0 / h[d]) * (2.0 / h[d]);
-        } else {
-            scale *= 2.0 / h[d];
-        }
-    }
 }
 
 // ---- Dirichlet penalty on boundary faces -------------------------------------
@@ -289,214 +245,17 @@ __global__ void penalty_rhs_kernel(long faces, int nb, int nf, int nqf, const in
     }
 }
 
-// ---- embedded (finite-cell) stiffness -----------------------------------------
-
-constexpr int kEmbThreads = 256;
-constexpr int kEmbBatch = 16;    // quadrature points per shared-memory batch
-constexpr int kEmbEntries = 16;  // element-matrix entries per thread: nb <= 64
-constexpr int kEmbStack = 64;
-
-struct EmbeddedArgs {
-    int dim, order, nb, q1, nq, maxDepth;
-    int cells[3];
-    double gn[16], gw[16];
-    double origin[3], h[3], center[3];
-    double radius2, alpha, scale;
-    double f[3];
-};
-
-// Inside test of the sphere domain at the parametric point xi of a cell.
-__device__ __forceinline__ bool embedded_inside(const EmbeddedArgs& P, const double* corg, const double* xi) {
-    double r2 = 0.0;
-    for (int d = 0; d < P.dim; ++d) {
-        const double x = corg[d] + 0.5 * (xi[d] + 1.0) * P.h[d];
-        r2 += (x - P.center[d]) * (x - P.center[d]);
-    }
-    return r2 < P.radius2;
-}
-
-// Parametric position and base weight of point q of a tree node (first index fastest).
-__device__ __forceinline__ double embedded_point(const EmbeddedArgs& P, const double* base, double length, int q,
-                                                 double* xi) {
-    int rest = q;
-    double w = 1.0;
-    for (int d = 0; d < P.dim; ++d) {
-        const int i = rest % P.q1;
-        rest /= P.q1;
-        xi[d] = base[d] + 0.5 * length * (P.gn[i] + 1.0);
-        w *= P.gw[i];
-    }
-    return w;
-}
-
-// One CTA per cell of one colour.  A cell whose base points all lie on one side
-// of the boundary is regular: its matrix is s K1 (s = 1 inside, alpha outside;
-// K1 = the standard-rule element matrix).  A cut cell is integrated over the
-// depth-first tree of KDTreeQuadraturePointFactory.hpp:67-173 (node points =
-// the base rule mapped to the node, weights times (length/2)^dim; keep =
-// (homogeneous && inside) || depth == maxDepth || (depth == 0 && homogeneous);
-// descend while not homogeneous), each kept point scaled by its material factor
-// (ScaledMultiMaterialIntegrand_impl.hpp:33-60), and accumulated in FP64:
-// K[a][b] += w s sum_d f_d G[d][a] G[d][b].
-__global__ void __launch_bounds__(kEmbThreads)
-    embedded_stiffness_kernel(EmbeddedArgs P, long count, const int* __restrict__ cellOrder,
-                              const double* __restrict__ K1, const double* __restrict__ kappa,
-                              const int* __restrict__ slots, double* __restrict__ val,
-                              unsigned long long* cutCells) {
-    __shared__ double s_G[kEmbBatch * 3 * 64];
-    __shared__ double s_v[kEmbBatch * 3 * 16], s_dv[kEmbBatch * 3 * 16];
-    __shared__ double s_w[kEmbBatch];
-    __shared__ double s_stack[kEmbStack][4];  // base[3], length
-    __shared__ int s_stackDepth[kEmbStack];
-    __shared__ int s_top;
-    __shared__ double s_node[4];
-    __shared__ int s_nodeDepth;
-    __shared__ int s_inside;
-    const int nb = P.nb, nb2 = nb * nb, dim = P.dim, nq = P.nq, n1 = P.order + 1;
-    const int t = threadIdx.x;
-    for (long le = blockIdx.x; le < count; le += gridDim.x) {
-        const int e = cellOrder[le];
-        double corg[3] = {0.0, 0.0, 0.0};
-        {
-            long rest = e;
-            for (int d = 0; d < dim; ++d) {
-                const long idx = rest % P.cells[d];
-                rest /= P.cells[d];
-                corg[d] = P.origin[d] + idx * P.h[d];
-            }
-        }
-        const double kap = kappa ? kappa[e] : 1.0;
-        const int* eslots = slots + static_cast<long>(e) * nb2;
-        // root classification
-        if (t == 0) s_inside = 0;
-        __syncthreads();
-        {
-            const double rootBase[3] = {-1.0, -1.0, -1.0};
-            int mine = 0;
-            for (int q = t; q < nq; q += kEmbThreads) {
-                double xi[3];
-                embedded_point(P, rootBase, 2.0, q, xi);
-                mine += embedded_inside(P, corg, xi) ? 1 : 0;
-            }
-            if (mine) atomicAdd(&s_inside, mine);
-        }
-        __syncthreads();
-        const int rootInside = s_inside;
-        if ((rootInside == 0 || rootInside == nq) && P.maxDepth >= 0) {
-            const double s = rootInside ? 1.0 : P.alpha;
-            for (int ab = t; ab < nb2; ab += kEmbThreads) val[eslots[ab]] += kap * s * K1[ab];
-            __syncthreads();
-            continue;
-        }
-        if (t == 0) atomicAdd(cutCells, 1ull);
-        double acc[kEmbEntries];
-#pragma unroll
-        for (int i = 0; i < kEmbEntries; ++i) acc[i] = 0.0;
-        if (t == 0) {
-            s_top = 1;
-            s_stack[0][0] = s_stack[0][1] = s_stack[0][2] = -1.0;
-            s_stack[0][3] = 2.0;
-            s_stackDepth[0] = 0;
-        }
-        __syncthreads();
-        for (;;) {
-            const int top = s_top;  // every thread reads before thread 0 pops
-            __syncthreads();
-            if (top == 0) break;
-            if (t == 0) {
-                const int k = --s_top;
-                for (int j = 0; j < 4; ++j) s_node[j] = s_stack[k][j];
-                s_nodeDepth = s_stackDepth[k];
-                s_inside = 0;
-            }
-            __syncthreads();
-            const double base[3] = {s_node[0], s_node[1], s_node[2]};
-            const double length = s_node[3];
-            const int depth = s_nodeDepth;
-            {
-                int mine = 0;
-                for (int q = t; q < nq; q += kEmbThreads) {
-                    double xi[3];
-                    embedded_point(P, base, length, q, xi);
-                    mine += embedded_inside(P, corg, xi) ? 1 : 0;
-                }
-                if (mine) atomicAdd(&s_inside, mine);
-            }
-            __syncthreads();
-            const int inside = s_inside;
-            const bool homogeneous = inside == 0 || inside == nq;
-            const bool keep = (homogeneous && inside == nq) || depth == P.maxDepth || (depth == 0 && homogeneous);
-            if (keep) {
-                double jac = 1.0;
-                for (int d = 0; d < dim; ++d) jac *= 0.5 * length;
-                for (int q0 = 0; q0 < nq; q0 += kEmbBatch) {
-                    const int nbatch = min(kEmbBatch, nq - q0);
-                    // 1-D basis values / derivatives per (point, dimension), weights
-                    if (t < nbatch * dim) {
-                        const int p = t / dim, d = t % dim;
-                        double xi[3];
-                        embedded_point(P, base, length, q0 + p, xi);
-                        lagrange(P.order, xi[d], &s_v[(p * 3 + d) * 16], &s_dv[(p * 3 + d) * 16]);
-                    }
-                    if (t < nbatch) {
-                        double xi[3];
-                        const double w = embedded_point(P, base, length, q0 + t, xi);
-                        s_w[t] = w * jac * (embedded_inside(P, corg, xi) ? 1.0 : P.alpha);
-                    }
-                    __syncthreads();
-                    // G[p][dd][a] = prod_d (d == dd ? derivative : value)
-                    for (int idx = t; idx < nbatch * dim * nb; idx += kEmbThreads) {
-                        const int p = idx / (dim * nb), r = idx - p * dim * nb;
-                        const int dd = r / nb, a = r - dd * nb;
-                        int ra = a;
-                        double g = 1.0;
-                        for (int d = 0; d < dim; ++d) {
-                            const int i = ra % n1;
-                            ra /= n1;
-                            g *= (d == dd) ? s_dv[(p * 3 + d) * 16 + i] : s_v[(p * 3 + d) * 16 + i];
-                        }
-                        s_G[(p * 3 + dd) * 64 + a] = g;
-                    }
-                    __syncthreads();
-                    for (int p = 0; p < nbatch; ++p) {
-                        const double w = s_w[p];
-                        const double* G = s_G + p * 3 * 64;
-#pragma unroll
-                        for (int i = 0; i < kEmbEntries; ++i) {
-                            const int ab = t + i * kEmbThreads;
-                            if (ab < nb2) {
-                                const int a = ab / nb, b = ab - (ab / nb) * nb;
-                                double s = 0.0;
-                                for (int d = 0; d < dim; ++d) s += P.f[d] * G[d * 64 + a] * G[d * 64 + b];
-                                acc[i] += w * s;
-                            }
-                        }
-                    }
-                    __syncthreads();
-                }
-            }
-            if (t == 0 && !homogeneous && depth < P.maxDepth) {
-                const double half = 0.5 * length;
-                const int children = 1 << dim;
-                for (int c = children - 1; c >= 0; --c) {  // pushed in reverse: child 0 is visited first
-                    const int k = s_top++;
-                    for (int d = 0; d < 3; ++d) s_stack[k][d] = d < dim ? base[d] + ((c >> d) & 1) * half : -1.0;
-                    s_stack[k][3] = half;
-                    s_stackDepth[k] = depth + 1;
-                }
-            }
-            __syncthreads();
-        }
-#pragma unroll
-        for (int i = 0; i < kEmbEntries; ++i) {
-            const int ab = t + i * kEmbThreads;
-            if (ab < nb2) val[eslots[ab]] += kap * P.scale * acc[i];
-        }
-        __syncthreads();
-    }
-}
-
 }  // namespace
+
+int unit_element(const ciecu_assembly_s* P, double scale, const double f[3], double* d_out, cudaStream_t st) {
+    const int nb2 = P->nb * P->nb;
+    unit_element_kernel<<<(nb2 + kT - 1) / kT, kT, 0, st>>>(P->nb, P->dim, P->nq, P->d_gtab, P->d_wq, scale, f[0],
+                                                           f[1], f[2], d_out);
+    count_launch();
+    CIECU_CHECK_LAUNCH("unit_element_kernel");
+    return CIECU_OK;
+}
+
 }  // namespace ciecu
 
 using namespace ciecu;
@@ -648,70 +407,6 @@ int ciecu_assemble_stiffness(ciecu_assembly P, const double* d_kappa, const doub
             P->d_slots, d_entries);
         count_launch();
         CIECU_CHECK_LAUNCH("stiffness_scatter_kernel");
-    }
-    return CIECU_OK;
-}
-
-int ciecu_assemble_embedded(ciecu_assembly P, const double* d_kappa, const double* h_cellSize, const int32_t* h_cells,
-                            const double* h_origin, const double* h_center, double radius, double alpha, int maxDepth,
-                            int convention, int accumulate, double* d_entries, double* d_work, int64_t* h_cutCells) {
-    CIECU_REQUIRE(P && h_cellSize && h_cells && h_origin && h_center && d_entries && d_work,
-                  "assemble_embedded: null argument");
-    CIECU_REQUIRE(convention == 0 || convention == 1, "assemble_embedded: convention must be 0 or 1");
-    CIECU_REQUIRE(P->nb <= 64 && P->order + 1 <= 16, "assemble_embedded: at most 64 basis functions per cell");
-    CIECU_REQUIRE(maxDepth >= 0 && maxDepth <= 4, "assemble_embedded: tree depth must be in [0, 4]");
-    CIECU_REQUIRE(radius > 0.0, "assemble_embedded: radius must be positive");
-    long cellsTotal = 1;
-    for (int d = 0; d < P->dim; ++d) {
-        CIECU_REQUIRE(h_cells[d] >= 1, "assemble_embedded: empty grid");
-        cellsTotal *= h_cells[d];
-    }
-    CIECU_REQUIRE(cellsTotal == P->ncells, "assemble_embedded: grid size differs from the plan's cell count");
-    cudaStream_t st = P->csr->space->stream;
-    if (!accumulate) CIECU_CUDA(cudaMemsetAsync(d_entries, 0, sizeof(double) * P->csr->nnz, st));
-    EmbeddedArgs A{};
-    A.dim = P->dim;
-    A.order = P->order;
-    A.nb = P->nb;
-    A.q1 = P->q1;
-    A.nq = P->nq;
-    A.maxDepth = maxDepth;
-    for (int d = 0; d < 3; ++d) {
-        A.cells[d] = d < P->dim ? h_cells[d] : 1;
-        A.origin[d] = d < P->dim ? h_origin[d] : 0.0;
-        A.h[d] = d < P->dim ? h_cellSize[d] : 1.0;
-        A.center[d] = d < P->dim ? h_center[d] : 0.0;
-    }
-    for (int i = 0; i < P->q1; ++i) {
-        A.gn[i] = P->gn[i];
-        A.gw[i] = P->gw[i];
-    }
-    A.radius2 = radius * radius;
-    A.alpha = alpha;
-    double f[3];
-    convention_factors(P->dim, h_cellSize, convention, A.scale, f);
-    for (int d = 0; d < 3; ++d) A.f[d] = f[d];
-    // K1: the standard-rule element matrix with the scale, for the regular cells
-    const int nb2 = P->nb * P->nb;
-    unit_element_kernel<<<(nb2 + kT - 1) / kT, kT, 0, st>>>(P->nb, P->dim, P->nq, P->d_gtab, P->d_wq, A.scale, f[0],
-                                                           f[1], f[2], d_work);
-    count_launch();
-    auto* d_cut = reinterpret_cast<unsigned long long*>(P->csr->space->d_result);
-    CIECU_CUDA(cudaMemsetAsync(d_cut, 0, sizeof(unsigned long long), st));
-    for (size_t c = 0; c + 1 < P->colorOffsets.size(); ++c) {
-        const long begin = P->colorOffsets[c], count = P->colorOffsets[c + 1] - begin;
-        if (count == 0) continue;
-        const int grid = static_cast<int>(std::min<long>(count, static_cast<long>(sm_count()) * 8));
-        embedded_stiffness_kernel<<<grid, kEmbThreads, 0, st>>>(A, count, P->d_cellOrder + begin, d_work, d_kappa,
-                                                                P->d_slots, d_entries, d_cut);
-        count_launch();
-        CIECU_CHECK_LAUNCH("embedded_stiffness_kernel");
-    }
-    if (h_cutCells) {
-        unsigned long long cut = 0;
-        CIECU_CUDA(cudaMemcpyAsync(&cut, d_cut, sizeof(cut), cudaMemcpyDeviceToHost, st));
-        CIECU_CUDA(cudaStreamSynchronize(st));
-        *h_cutCells = static_cast<int64_t>(cut);
     }
     return CIECU_OK;
 }
@@ -922,8 +617,19 @@ int ciecu_dirichlet_eliminate(ciecu_csr csr, const uint8_t* d_isBoundary, double
     CIECU_REQUIRE(csr && d_isBoundary && d_entries, "dirichlet_eliminate: null argument");
     CIECU_REQUIRE(csr->rows == csr->cols, "dirichlet_eliminate: square matrix expected");
     if (csr->rows == 0) return CIECU_OK;
-    dirichlet_kernel<<<grid_for(csr->rows, kT, 8), kT, 0, csr->space->stream>>>(csr->rows, csr->rowptr, csr->col,
-                                                                               d_entries, d_isBoundary, d_rhs);
+    dirichlet_kernel<double><<<grid_for(csr->rows, kT, 8), kT, 0, csr->space->stream>>>(
+        csr->rows, csr->rowptr, csr->col, d_entries, d_isBoundary, d_rhs);
+    count_launch();
+    CIECU_CHECK_LAUNCH("dirichlet_kernel");
+    return CIECU_OK;
+}
+
+int ciecu_dirichlet_eliminate_f32(ciecu_csr csr, const uint8_t* d_isBoundary, float* d_entries32) {
+    CIECU_REQUIRE(csr && d_isBoundary && d_entries32, "dirichlet_eliminate_f32: null argument");
+    CIECU_REQUIRE(csr->rows == csr->cols, "dirichlet_eliminate_f32: square matrix expected");
+    if (csr->rows == 0) return CIECU_OK;
+    dirichlet_kernel<float><<<grid_for(csr->rows, kT, 8), kT, 0, csr->space->stream>>>(
+        csr->rows, csr->rowptr, csr->col, d_entries32, d_isBoundary, nullptr);
     count_launch();
     CIECU_CHECK_LAUNCH("dirichlet_kernel");
     return CIECU_OK;

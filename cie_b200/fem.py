@@ -140,6 +140,30 @@ class Assembler:
         self.space.leave()
         return cut.value
 
+    def assemble_embedded_f32(self, entries32, center, radius, alpha, maxDepth, kappa=None, convention=0,
+                              accumulate=False, origin=None):
+        """The finite-cell matrix in FP32 (values in the same pattern): the cut
+        cells' contractions on the tensor cores in split BF16 with FP32
+        accumulation (ciecu_assemble_embedded_f32).  Returns the number of cut cells."""
+        m = self.mesh
+        h = np.ascontiguousarray(m.h, dtype=np.float64)
+        cells = np.ascontiguousarray(m.cells, dtype=np.int32)
+        org = np.zeros(m.dim) if origin is None else np.asarray(origin, dtype=np.float64)
+        cen = np.ascontiguousarray(center, dtype=np.float64)
+        cut = ctypes.c_int64()
+        self.space.enter()
+        call("ciecu_assemble_embedded_f32", self.handle, _ptr(kappa), _np_ptr(h), _np_ptr(cells), _np_ptr(org),
+             _np_ptr(cen), float(radius), float(alpha), int(maxDepth), int(convention), int(bool(accumulate)),
+             _ptr(entries32), ctypes.byref(cut))
+        self.space.leave()
+        return cut.value
+
+    def dirichlet_f32(self, isBoundary, entries32):
+        """Symmetric elimination on an FP32 copy of the values."""
+        self.space.enter()
+        call("ciecu_dirichlet_eliminate_f32", self.csr.handle, _ptr(isBoundary), _ptr(entries32))
+        self.space.leave()
+
     def dirichlet_penalty(self, penalty, faceMask=0, quadratureOrder=0, boundaryValues=None, rhs=None,
                           entries=None):
         """Weak Dirichlet condition by penalty on the box faces selected by faceMask

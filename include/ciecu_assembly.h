@@ -51,12 +51,27 @@ int ciecu_assemble_stiffness(ciecu_assembly plan, const double* d_kappa, const d
  * homogeneous and inside, at the maximum depth, or homogeneous at depth 0, and
  * refined while not homogeneous.  K_e in FP64, convention as
  * ciecu_assemble_stiffness; d_kappa may be NULL (kappa = 1).  The plan's basis has
- * at most 64 functions.  d_work: nb*nb doubles.  h_cutCells (may be NULL): the
- * number of cut cells (synchronises the stream). */
+ * at most 64 functions.  The cut cells' Gram contractions run on the tensor cores
+ * in FP64 (eight CTAs per cut cell, one per depth-1 tree node); cells of one
+ * colour are scattered together, so the result does not depend on the schedule.
+ * d_work: nb*nb doubles (kept for the interface; the call allocates its own
+ * work arrays).  h_cutCells (may be NULL): the number of cut cells.  The call
+ * synchronises the stream. */
 int ciecu_assemble_embedded(ciecu_assembly plan, const double* d_kappa, const double* h_cellSize,
                             const int32_t* h_cells, const double* h_origin, const double* h_center, double radius,
                             double alpha, int maxDepth, int convention, int accumulate, double* d_entries,
                             double* d_work, int64_t* h_cutCells);
+
+/* The same finite-cell matrix in single precision, for inner or preconditioner
+ * operators: d_entries32 (FP32 values in the plan's CSR pattern) (+)= the element
+ * matrices with the Gram contraction B^T W B on the tensor cores in BF16 with
+ * FP32 accumulation, each operand split into a high and a low BF16 part and the
+ * three significant products summed (about 16 significant bits per product); the
+ * regular cells add the FP64 standard-rule matrix rounded to FP32. */
+int ciecu_assemble_embedded_f32(ciecu_assembly plan, const double* d_kappa, const double* h_cellSize,
+                                const int32_t* h_cells, const double* h_origin, const double* h_center, double radius,
+                                double alpha, int maxDepth, int convention, int accumulate, float* d_entries32,
+                                int64_t* h_cutCells);
 
 /* Adjoint gradient of J(u) with respect to the cell conductivities:
  * d_grad[e] = -lambda_e^T (dK_e/dkappa_e) u_e = -lambda_e^T K_e(kappa = 1) u_e.
@@ -105,6 +120,8 @@ int ciecu_assemble_dirichlet_penalty(ciecu_assembly plan, const int32_t* h_cells
  * rows and columns of boundary DoFs zeroed (structural zeros kept), diagonal 1,
  * d_rhs[boundary] = 0 (d_rhs may be NULL). */
 int ciecu_dirichlet_eliminate(ciecu_csr csr, const uint8_t* d_isBoundary, double* d_entries, double* d_rhs);
+/* The same elimination on an FP32 copy of the values (d_entries32 in the pattern of csr). */
+int ciecu_dirichlet_eliminate_f32(ciecu_csr csr, const uint8_t* d_isBoundary, float* d_entries32);
 
 #ifdef __cplusplus
 }

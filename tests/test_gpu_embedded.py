@@ -43,3 +43,18 @@ def test_embedded_assembly_vs_oracle(space, restatement, dim, order, cells, dept
     print("%dD Q%d %s depth %d: %d cut cells of %d" % (dim, order, cells, depth, cut, mesh.ncells))
     assert 0 < cut < mesh.ncells
     assert np.allclose(got, ref, rtol=1e-12, atol=1e-14 * np.abs(ref).max())
+    # the FP32 copy from the split-BF16 tensor-core contraction, against the FP64 matrix
+    v32 = torch.zeros(col.size, dtype=torch.float32, device="cuda")
+    assert asm.assemble_embedded_f32(v32, center, radius, alpha, depth) == cut
+    err = np.abs(v32.cpu().numpy().astype(np.float64) - got).max() / np.abs(got).max()
+    print("FP32 (split BF16 tensor cores) max entry error relative to the largest entry: %.3e" % err)
+    assert err <= 1e-4
+
+
+def test_embedded_assembly_is_deterministic(space):
+    """Eight CTAs per cut cell, partial matrices summed in tree-node order and
+    scattered by colour: repeated assemblies are bit-identical."""
+    from cie_b200.fem import make_embedded_poisson
+    outs = [make_embedded_poisson(space, 3, 3, [8, 8, 8], radius=0.4, alpha=1e-6, depth=2).matrix.entries.cpu().numpy()
+            for _ in range(2)]
+    assert np.array_equal(outs[0].view(np.uint64), outs[1].view(np.uint64))
