@@ -701,14 +701,38 @@ def extra_workloads(space, A, D, settings, t_fp64, it64, rank=0, world=1):
         "note": "random right-hand sides, boundary rows included (identity rows of the eliminated system)"}
     del mrhs, X, B
 
-    # embedded (finite-cell) Q3 sphere on 32^3 cells: FP64 Jacobi-PCG and the two-level
-    # (Q3 -> Q1) multigrid-preconditioned CG, one solve each
-    from cie_b200.fem import make_embedded_poisson
-    from cie_b200.twolevel import make_two_level
-    t0 = time.perf_counter()
+    # embedded (finite-cell) Q3 sphere on 32^3 cells: set-up (pattern on the host and
+    # on the device, FP64 and FP32 tensor-core assembly), FP64 Jacobi-PCG, and the
+    # device two-level CG with FP64 and with FP32 smoothing (outer iteration FP64)
+    from cie_b200.fem import make_embedded_poisson, csr_pattern
+    from cie_b200.graph import csr_pattern_device
+    from cie_b200.twolevel import make_two_level_cg
     pe = make_embedded_poisson(space, 3, 3, [32, 32, 32], radius=0.4, alpha=1e-6, depth=2, seed=0)
     torch.cuda.synchronize()
-    setup = time.perf_counter() - t0
+    em = pe.mesh
+    t0 = time.perf_counter()
+    csr_pattern(em.ncells, em.nb, em.dofmap, em.ndofs)
+    t_pattern_host = time.perf_counter() - t0
+    d_dofmap = pe.assembler.d_dofmap
+    csr_pattern_device(space, em.ncells, em.nb, d_dofmap, em.ndofs)  # warm-up (module load)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    csr_pattern_device(space, em.ncells, em.nb, d_dofmap, em.ndofs)
+    torch.cuda.synchronize()
+    t_pattern_dev = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    pe.assembler.assemble_embedded([0.5] * 3, 0.4, 1e-6, 2)
+    pe.assembler.dirichlet(pe.boundary)
+    torch.cuda.synchronize()
+    t_asm = time.perf_counter() - t0
+    v32 = torch.zeros(pe.matrix.entries.numel(), dtype=torch.float32, device="cuda")
+    t0 = time.perf_counter()
+    pe.assembler.assemble_embedded_f32(v32, [0.5] * 3, 0.4, 1e-6, 2)
+    torch.cuda.synchronize()
+    t_asm32 = time.perf_counter() - t0
+    pe.assembler.dirichlet_f32(pe.boundary, v32)
+    asm32_err = float((v32.double() - pe.matrix.entries).abs().max() / pe.matrix.entries.abs().max())
+    del v32
     Ae = CSROperator(pe.matrix, space)
     cge = ConjugateGradients(Ae, space, makeDiagonalOperator(pe.matrix, space, csr_handle=Ae.csr),
                              Statistics(200000, 0.0, 1e-10))
@@ -719,22 +743,32 @@ def extra_workloads(space, A, D, settings, t_fp64, it64, rank=0, world=1):
         cge.product(0.0, pe.rhs, 1.0, xe)
     tj = timed(solve_jacobi, 1, warm=0)
     itj = cge.getStats().iterationCount
-    fine, fineD, mg = make_two_level(space, pe, degree=4, coarseSettings=Statistics(5000, 0.0, 1e-4))
-    cgm = ConjugateGradients(fine, space, mg, Statistics(20000, 0.0, 1e-10))
-    xm = torch.zeros_like(pe.rhs)
+    emb = {"dofs": pe.rhs.numel(), "nnz": pe.matrix.nnz(), "cut_cells": pe.cut_cells,
+           "pattern_host_seconds": t_pattern_host, "pattern_device_seconds": t_pattern_dev,
+           "assembly_fp64_seconds": t_asm, "assembly_fp32_tensor_core_seconds": t_asm32,
+           "fp32_matrix_max_rel_entry_error": asm32_err,
+           "jacobi_pcg_seconds": tj, "jacobi_pcg_iterations": itj, "jacobi_us_per_iteration": 1e6 * tj / (itj + 1)}
+    del cge
+    for precision in ("f64", "f32"):
+        solver = make_two_level_cg(space, pe, Statistics(20000, 0.0, 1e-10), degree=2, coarseIterations=8,
+                                   precision=precision)
+        xm = torch.zeros_like(pe.rhs)
 
-    def solve_mg():
-        xm.zero_()
-        cgm.product(0.0, pe.rhs, 1.0, xm)
-    tmg = timed(solve_mg, 1, warm=0)
-    out["embedded_sphere_q3_32^3_fp64"] = {
-        "dofs": pe.rhs.numel(), "nnz": pe.matrix.nnz(), "cut_cells": pe.cut_cells, "setup_seconds": setup,
-        "jacobi_pcg_seconds": tj, "jacobi_pcg_iterations": itj,
-        "jacobi_us_per_iteration": 1e6 * tj / (itj + 1),
-        "two_level_pcg_seconds": tmg, "two_level_pcg_iterations": cgm.getStats().iterationCount,
-        "two_level_rel_diff_vs_jacobi": float(torch.linalg.norm(xm - xe) / torch.linalg.norm(xe)),
-        "note": "FP32-inner mixed precision does not converge on this system (material factor 1e-6)"}
-    del cge, cgm, mg, fine, fineD, Ae, pe, xe, xm
+        def solve_mg():
+            xm.zero_()
+            solver.product(0.0, pe.rhs, 1.0, xm)
+        tmg = timed(solve_mg, 1, warm=1)
+        st = solver.getStats()
+        r = pe.rhs.clone()
+        Ae.product(1.0, xm, -1.0, r)
+        emb["two_level_%s_smoothing" % precision] = {
+            "seconds": tmg, "iterations": st.iterationCount,
+            "true_relative_residual": float(torch.linalg.norm(r) / torch.linalg.norm(pe.rhs)),
+            "rel_diff_vs_jacobi": float(torch.linalg.norm(xm - xe) / torch.linalg.norm(xe)),
+            "speedup_vs_jacobi": tj / tmg}
+        del solver, xm
+    out["embedded_sphere_q3_32^3"] = emb
+    del Ae, pe, xe
 
     # adjoint gradient, 3D Q1 64^3
     cells = [64, 64, 64]

@@ -27,6 +27,11 @@ class MixedOptions(ctypes.Structure):
                 ("scaleInner", c_int)]
 
 
+class MgOptions(ctypes.Structure):
+    _fields_ = [("degree", c_int), ("lambdaMax", c_double), ("ratio", c_double), ("coarseIterations", c_int),
+                ("flexible", c_int)]
+
+
 class MixedStatistics(ctypes.Structure):
     _fields_ = [("iterationCount", c_int64), ("absoluteResidual", c_double), ("relativeResidual", c_double),
                 ("innerIterations", c_int64), ("refinements", c_int64), ("trueRelativeResidual", c_double)]
@@ -130,6 +135,10 @@ SIGNATURES = {
     "ciecu_assemble_dirichlet_penalty": (c_int, [P, P, P, c_double, c_int, c_int, P, P, P]),
     "ciecu_assemble_embedded_f32": (c_int, [P, P, P, P, P, P, c_double, c_double, c_int, c_int, c_int, P, P]),
     "ciecu_dirichlet_eliminate_f32": (c_int, [P, P, P]),
+    "ciecu_mgcg_create": (c_int, [P, P, P, P, P, P, P, MgOptions, Statistics, P]),
+    "ciecu_mgcg_destroy": (c_int, [P]),
+    "ciecu_mgcg_product": (c_int, [P, c_double, P, c_double, P, P]),
+    "ciecu_mgcg_info": (c_int, [P, P, P]),
 }
 
 OPTIONAL = set()

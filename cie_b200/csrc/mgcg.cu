@@ -1,0 +1,652 @@
+// Two-level multigrid-preconditioned conjugate gradients, entirely on the device.
+//
+// One outer iteration (the stopping rule and statistics of
+// ConjugateGradients_impl.hpp:49-201):
+//   M1  q = A p, p^T q, alpha = r^T z / p^T q
+//   M2  x += alpha p, r -= alpha q, ||r|| and the stop decision
+//   z = cycle(r):  z = S r;  t = r - A z;  z += P C(R t);  t = r - A z;  z += S t
+//   M3  r^T z (and r^T z_old: flexible beta), beta
+//   M4  p = z + beta p
+// S is a Chebyshev polynomial smoother in D^-1 A (FP64 on the solver's matrix,
+// or FP32 on a single-precision copy), C a fixed number of Jacobi-PCG
+// iterations on the coarse matrix from zero (kernels on the device scalars, no
+// host round trip).  The body runs under a WHILE conditional node of a CUDA
+// graph; M1 / M2 end the loop.  Every reduction is deterministic (per-block
+// partials summed in block order by the last block).
+#include "ciecu_mg.h"
+#include "graph.cuh"
+#include "pcg.cuh"
+
+#include <cmath>
+#include <string>
+#include <utility>
+
+namespace ciecu {
+namespace {
+
+constexpr int kT = 256;
+
+struct MgScalars {
+    double rz, pq, alpha, beta, rr, r0, absres, relres, absTol, relTol;
+    long long iter, maxIter;
+    int done, error, errorKind, flexible;
+    long long errorIter, chunkIter, chunkLimit, cycles;
+    double crz, calpha, cbeta;  // coarse solve
+};
+
+template <bool COND>
+__device__ __forceinline__ void set_cond(cudaGraphConditionalHandle cond, unsigned value) {
+    if constexpr (COND) cudaGraphSetConditional(cond, value);
+}
+
+__device__ __forceinline__ bool halted(const MgScalars* s) { return *reinterpret_cast<const volatile int*>(&s->done) != 0; }
+
+// ---- outer iteration -----------------------------------------------------------
+
+struct PqOp {
+    using Pre = double;
+    const double* __restrict__ p;
+    double* __restrict__ q;
+    double acc;
+    __device__ __forceinline__ double pre(int r) const { return p[r]; }
+    __device__ __forceinline__ void post(int r, double pr, double sum) {
+        q[r] = sum;
+        acc = fma(pr, sum, acc);
+    }
+};
+
+template <int K, bool COND>
+__global__ void __launch_bounds__(csr_threads<K>())
+    mg_spmv_kernel(CsrArgs<double> A, const double* __restrict__ p, double* __restrict__ q, MgScalars* s,
+                   double* partials, unsigned* counter, cudaGraphConditionalHandle loop) {
+    if (halted(s)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) set_cond<COND>(loop, 0);
+        return;
+    }
+    PqOp op{p, q, 0.0};
+    csr_rows<K, double, double, false>(A, p, op);
+    double mine[1] = {op.acc}, tot[1];
+    if (grid_reduce_last<1, csr_threads<K>()>(mine, partials, counter, tot) && threadIdx.x == 0) {
+        s->pq = tot[0];
+        if (!(0.0 < tot[0])) {
+            s->done = 3;
+            s->error = CIECU_ERR_BREAKDOWN;
+            s->errorKind = 2;
+            s->errorIter = s->iter;
+            set_cond<COND>(loop, 0);
+        } else {
+            s->alpha = s->rz / tot[0];
+        }
+    }
+}
+
+template <bool COND>
+__global__ void __launch_bounds__(kT) mg_update_kernel(long n, double* __restrict__ x, double* __restrict__ r,
+                                                       const double* __restrict__ p, const double* __restrict__ q,
+                                                       MgScalars* s, double* partials, unsigned* counter,
+                                                       cudaGraphConditionalHandle loop) {
+    if (halted(s)) return;
+    const double alpha = s->alpha;
+    double rr = 0.0;
+    for (long i = blockIdx.x * static_cast<long>(kT) + threadIdx.x; i < n; i += static_cast<long>(gridDim.x) * kT) {
+        x[i] = fma(alpha, p[i], x[i]);
+        const double ri = fma(-alpha, q[i], r[i]);
+        r[i] = ri;
+        rr = fma(ri, ri, rr);
+    }
+    double mine[1] = {rr}, tot[1];
+    if (grid_reduce_last<1, kT>(mine, partials, counter, tot) && threadIdx.x == 0) {
+        s->rr = tot[0];
+        s->absres = sqrt(tot[0]);
+        s->relres = s->absres / s->r0;
+        if (float_less(s->absres, s->absTol) || float_less(s->relres, s->relTol)) {
+            s->done = 1;
+        } else {
+            s->iter += 1;
+            if (s->iter >= s->maxIter) s->done = 2;
+        }
+        s->chunkIter += 1;
+        set_cond<COND>(loop, (s->done == 0 && s->chunkIter < s->chunkLimit) ? 1u : 0u);
+    }
+}
+
+// r^T z and r^T z_old (flexible) -> beta; at the start (INIT) r^T z and p = z.
+template <bool INIT>
+__global__ void __launch_bounds__(kT) mg_beta_kernel(long n, const double* __restrict__ r, const double* __restrict__ z,
+                                                     double* __restrict__ zold, double* __restrict__ p, MgScalars* s,
+                                                     double* partials, unsigned* counter) {
+    if (halted(s)) return;
+    double rz = 0.0, rzo = 0.0;
+    for (long i = blockIdx.x * static_cast<long>(kT) + threadIdx.x; i < n; i += static_cast<long>(gridDim.x) * kT) {
+        const double ri = r[i], zi = z[i];
+        rz = fma(ri, zi, rz);
+        if (!INIT) rzo = fma(ri, zold[i], rzo);
+        if (INIT) {
+            p[i] = zi;
+            zold[i] = zi;
+        }
+    }
+    double mine[2] = {rz, rzo}, tot[2];
+    if (grid_reduce_last<2, kT>(mine, partials, counter, tot) && threadIdx.x == 0) {
+        if (!(0.0 < tot[0])) {
+            s->done = 3;
+            s->error = CIECU_ERR_BREAKDOWN;
+            s->errorKind = 1;
+            s->errorIter = s->iter;
+            return;
+        }
+        if (!INIT) s->beta = s->flexible ? (tot[0] - tot[1]) / s->rz : tot[0] / s->rz;
+        s->rz = tot[0];
+    }
+}
+
+__global__ void __launch_bounds__(kT) mg_direction_kernel(long n, const double* __restrict__ z, double* __restrict__ p,
+                                                          double* __restrict__ zold, const MgScalars* s) {
+    if (halted(s)) return;
+    const double beta = s->beta;
+    for (long i = blockIdx.x * static_cast<long>(kT) + threadIdx.x; i < n; i += static_cast<long>(gridDim.x) * kT) {
+        const double zi = z[i];
+        p[i] = fma(beta, p[i], zi);
+        zold[i] = zi;
+    }
+}
+
+// ||r_0||: the initial residual and the start decision of the reference.
+__global__ void __launch_bounds__(kT) mg_init_kernel(long n, const double* __restrict__ r, MgScalars* s,
+                                                     double* partials, unsigned* counter) {
+    double rr = 0.0;
+    for (long i = blockIdx.x * static_cast<long>(kT) + threadIdx.x; i < n; i += static_cast<long>(gridDim.x) * kT)
+        rr = fma(r[i], r[i], rr);
+    double mine[1] = {rr}, tot[1];
+    if (grid_reduce_last<1, kT>(mine, partials, counter, tot) && threadIdx.x == 0) {
+        s->rr = tot[0];
+        s->r0 = sqrt(tot[0]);
+        s->absres = s->r0;
+        s->relres = 1.0;
+        if (float_less(s->absres, s->absTol) || float_less(1.0, s->relTol)) s->done = 1;
+        else if (s->maxIter <= 0) s->done = 2;
+    }
+}
+
+__global__ void mg_output_kernel(long n, double inScale, double outScale, const double* __restrict__ x,
+                                 double* __restrict__ out) {
+    for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long>(gridDim.x) * blockDim.x)
+        out[i] = combine(inScale, out[i], outScale, x[i]);
+}
+
+// ---- Chebyshev smoother (T = double or float vectors and values) ---------------
+
+template <typename T>
+__global__ void cheb_first_kernel(long n, const T* __restrict__ in, const T* __restrict__ dinv, T theta,
+                                  T* __restrict__ r, T* __restrict__ d, T* __restrict__ x) {
+    for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long>(gridDim.x) * blockDim.x) {
+        const T ri = in[i];
+        r[i] = ri;
+        const T di = dinv[i] * ri / theta;
+        d[i] = di;
+        x[i] = di;
+    }
+}
+
+template <typename T>
+struct ChebStep {
+    struct Pre {
+        T r, d, dinv, x;
+    };
+    const T* __restrict__ dinv;
+    T c1, c2;
+    T* __restrict__ r;
+    const T* __restrict__ dold;
+    T* __restrict__ dnew;
+    T* __restrict__ x;
+    __device__ __forceinline__ Pre pre(int i) const { return Pre{r[i], dold[i], dinv[i], x[i]}; }
+    __device__ __forceinline__ void post(int i, const Pre& p, T sum) const {
+        const T ri = p.r - sum;
+        r[i] = ri;
+        const T di = c1 * p.d + c2 * p.dinv * ri;
+        dnew[i] = di;
+        x[i] = p.x + di;
+    }
+};
+
+template <int K, typename T>
+__global__ void __launch_bounds__(csr_threads<K>())
+    cheb_step_kernel(CsrArgs<T> A, const T* __restrict__ dinv, T c1, T c2, T* __restrict__ r,
+                     const T* __restrict__ dold, T* __restrict__ dnew, T* __restrict__ x) {
+    ChebStep<T> op{dinv, c1, c2, r, dold, dnew, x};
+    csr_rows<K, T, T, false>(A, dold, op);
+}
+
+template <typename T>
+__global__ void axpy_out_kernel(long n, const T* __restrict__ x, T* __restrict__ out, int accumulate) {
+    for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long>(gridDim.x) * blockDim.x)
+        out[i] = accumulate ? out[i] + x[i] : x[i];
+}
+
+template <typename A, typename B>
+__global__ void convert_kernel(long n, const A* __restrict__ a, B* __restrict__ b, int accumulate) {
+    for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long>(gridDim.x) * blockDim.x)
+        b[i] = accumulate ? static_cast<B>(static_cast<A>(b[i]) + a[i]) : static_cast<B>(a[i]);
+}
+
+// ---- coarse solve: a fixed number of Jacobi-PCG iterations from zero ----------
+
+__global__ void __launch_bounds__(kT) coarse_init_kernel(long m, const double* __restrict__ b,
+                                                         const double* __restrict__ dinv, double* __restrict__ x,
+                                                         double* __restrict__ r, double* __restrict__ z,
+                                                         double* __restrict__ p, MgScalars* s, double* partials,
+                                                         unsigned* counter) {
+    double rz = 0.0;
+    for (long i = blockIdx.x * static_cast<long>(kT) + threadIdx.x; i < m; i += static_cast<long>(gridDim.x) * kT) {
+        const double ri = b[i], zi = dinv[i] * ri;
+        x[i] = 0.0;
+        r[i] = ri;
+        z[i] = zi;
+        p[i] = zi;
+        rz = fma(ri, zi, rz);
+    }
+    double mine[1] = {rz}, tot[1];
+    if (grid_reduce_last<1, kT>(mine, partials, counter, tot) && threadIdx.x == 0) s->crz = tot[0];
+}
+
+template <int K>
+__global__ void __launch_bounds__(csr_threads<K>())
+    coarse_spmv_kernel(CsrArgs<double> A, const double* __restrict__ p, double* __restrict__ q, MgScalars* s,
+                       double* partials, unsigned* counter) {
+    PqOp op{p, q, 0.0};
+    csr_rows<K, double, double, false>(A, p, op);
+    double mine[1] = {op.acc}, tot[1];
+    if (grid_reduce_last<1, csr_threads<K>()>(mine, partials, counter, tot) && threadIdx.x == 0)
+        s->calpha = (0.0 < tot[0] && 0.0 < s->crz) ? s->crz / tot[0] : 0.0;  // converged or broken down: no step
+}
+
+__global__ void __launch_bounds__(kT) coarse_update_kernel(long m, const double* __restrict__ dinv,
+                                                           double* __restrict__ x, double* __restrict__ r,
+                                                           double* __restrict__ z, const double* __restrict__ p,
+                                                           const double* __restrict__ q, MgScalars* s,
+                                                           double* partials, unsigned* counter) {
+    const double alpha = s->calpha;
+    double rz = 0.0;
+    for (long i = blockIdx.x * static_cast<long>(kT) + threadIdx.x; i < m; i += static_cast<long>(gridDim.x) * kT) {
+        x[i] = fma(alpha, p[i], x[i]);
+        const double ri = fma(-alpha, q[i], r[i]);
+        const double zi = dinv[i] * ri;
+        r[i] = ri;
+        z[i] = zi;
+        rz = fma(ri, zi, rz);
+    }
+    double mine[1] = {rz}, tot[1];
+    if (grid_reduce_last<1, kT>(mine, partials, counter, tot) && threadIdx.x == 0) {
+        s->cbeta = 0.0 < s->crz ? tot[0] / s->crz : 0.0;
+        s->crz = tot[0];
+    }
+}
+
+__global__ void __launch_bounds__(kT) coarse_direction_kernel(long m, const double* __restrict__ z,
+                                                              double* __restrict__ p, const MgScalars* s) {
+    const double beta = s->cbeta;
+    for (long i = blockIdx.x * static_cast<long>(kT) + threadIdx.x; i < m; i += static_cast<long>(gridDim.x) * kT)
+        p[i] = fma(beta, p[i], z[i]);
+}
+
+__global__ void count_cycle_kernel(MgScalars* s) { s->cycles += 1; }
+
+}  // namespace
+}  // namespace ciecu
+
+struct ciecu_mgcg_s {
+    ciecu_csr_s *A = nullptr, *S32 = nullptr, *P = nullptr, *R = nullptr, *Ac = nullptr;
+    const double *dinv = nullptr, *dinvc = nullptr;
+    ciecu_mg_options options{};
+    ciecu_statistics settings{};
+    long n = 0, m = 0;
+    double lambdaMax = 0.0, lambdaMin = 0.0;
+    double *x = nullptr, *r = nullptr, *p = nullptr, *q = nullptr, *z = nullptr, *zold = nullptr, *t = nullptr;
+    double* cheb = nullptr;  // 4n (FP64 smoothing)
+    float *dinv32 = nullptr, *r32 = nullptr, *z32 = nullptr, *t32 = nullptr, *cheb32 = nullptr;  // FP32 smoothing
+    double *rc = nullptr, *cx = nullptr, *cr = nullptr, *cz = nullptr, *cp = nullptr, *cq = nullptr;
+    ciecu::MgScalars* d_s = nullptr;
+    ciecu::MgScalars* h_s = nullptr;
+    double* partials = nullptr;
+    unsigned* counter = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    bool deviceLoop = false;
+};
+
+namespace ciecu {
+namespace {
+
+int grid_of(long n) { return grid_for(n, kT, 8); }
+
+// out (+)= S in: Chebyshev polynomial of degree `degree` in D^-1 A applied to in.
+template <typename T>
+int chebyshev(ciecu_mgcg_s* M, ciecu_csr_s* A, const T* dinv, const T* in, T* out, bool accumulate, T* work,
+              cudaStream_t st) {
+    const long n = M->n;
+    T* r = work;
+    T* da = work + n;
+    T* db = work + 2 * n;
+    T* x = work + 3 * n;
+    const double theta = 0.5 * (M->lambdaMax + M->lambdaMin);
+    const double delta = 0.5 * (M->lambdaMax - M->lambdaMin);
+    const double sigma = theta / delta;
+    double rho = 1.0 / sigma;
+    cheb_first_kernel<T><<<grid_of(n), kT, 0, st>>>(n, in, dinv, static_cast<T>(theta), r, da, x);
+    count_launch();
+    const int grid = csr_grid(A, A->kernel);
+    for (int k = 1; k < M->options.degree; ++k) {
+        const double rhoNew = 1.0 / (2.0 * sigma - rho);
+        const T c1 = static_cast<T>(rhoNew * rho), c2 = static_cast<T>(2.0 * rhoNew / delta);
+        CIECU_TRY(with_schedule(A->kernel, [&](auto kk) -> int {
+            constexpr int K = decltype(kk)::value;
+            cheb_step_kernel<K, T><<<fit_grid(cheb_step_kernel<K, T>, csr_threads<K>(), grid), csr_threads<K>(), 0,
+                                     st>>>(A->args<T>(), dinv, c1, c2, r, da, db, x);
+            return CIECU_OK;
+        }));
+        count_launch();
+        std::swap(da, db);
+        rho = rhoNew;
+    }
+    axpy_out_kernel<T><<<grid_of(n), kT, 0, st>>>(n, x, out, accumulate ? 1 : 0);
+    count_launch();
+    return CIECU_OK;
+}
+
+// ec = C rc: coarseIterations Jacobi-PCG iterations from zero, result in M->cx.
+int coarse_solve(ciecu_mgcg_s* M, cudaStream_t st) {
+    const long m = M->m;
+    ciecu_csr_s* Ac = M->Ac;
+    coarse_init_kernel<<<grid_of(m), kT, 0, st>>>(m, M->rc, M->dinvc, M->cx, M->cr, M->cz, M->cp, M->d_s,
+                                                  M->partials, M->counter);
+    count_launch();
+    const int grid = csr_grid(Ac, Ac->kernel);
+    for (int it = 0; it < M->options.coarseIterations; ++it) {
+        CIECU_TRY(with_schedule(Ac->kernel, [&](auto kk) -> int {
+            constexpr int K = decltype(kk)::value;
+            coarse_spmv_kernel<K><<<fit_grid(coarse_spmv_kernel<K>, csr_threads<K>(), grid), csr_threads<K>(), 0,
+                                    st>>>(Ac->args<double>(), M->cp, M->cq, M->d_s, M->partials, M->counter);
+            return CIECU_OK;
+        }));
+        coarse_update_kernel<<<grid_of(m), kT, 0, st>>>(m, M->dinvc, M->cx, M->cr, M->cz, M->cp, M->cq, M->d_s,
+                                                        M->partials, M->counter);
+        coarse_direction_kernel<<<grid_of(m), kT, 0, st>>>(m, M->cz, M->cp, M->d_s);
+        count_launch(3);
+    }
+    return CIECU_OK;
+}
+
+// z = cycle(r) (the symmetric two-level cycle).
+int cycle(ciecu_mgcg_s* M, cudaStream_t st) {
+    const long n = M->n;
+    ciecu_csr_s* A = M->A;
+    if (!M->S32) {
+        CIECU_TRY(chebyshev<double>(M, A, M->dinv, M->r, M->z, false, M->cheb, st));
+        CIECU_CUDA(cudaMemcpyAsync(M->t, M->r, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+        CIECU_TRY(ciecu_csr_spmv_f64(A, 1.0, M->z, -1.0, M->t));  // t = r - A z
+        CIECU_TRY(ciecu_csr_spmv_f64(M->R, 0.0, M->t, 1.0, M->rc));
+        CIECU_TRY(coarse_solve(M, st));
+        CIECU_TRY(ciecu_csr_spmv_f64(M->P, 1.0, M->cx, 1.0, M->z));
+        CIECU_CUDA(cudaMemcpyAsync(M->t, M->r, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+        CIECU_TRY(ciecu_csr_spmv_f64(A, 1.0, M->z, -1.0, M->t));
+        CIECU_TRY(chebyshev<double>(M, A, M->dinv, M->t, M->z, true, M->cheb, st));
+    } else {
+        ciecu_csr_s* S = M->S32;
+        convert_kernel<double, float><<<grid_of(n), kT, 0, st>>>(n, M->r, M->r32, 0);
+        count_launch();
+        CIECU_TRY(chebyshev<float>(M, S, M->dinv32, M->r32, M->z32, false, M->cheb32, st));
+        CIECU_CUDA(cudaMemcpyAsync(M->t32, M->r32, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+        CIECU_TRY(ciecu_csr_spmv_f32(S, 1.0f, M->z32, -1.0f, M->t32));  // t = r - A32 z (FP32)
+        convert_kernel<float, double><<<grid_of(n), kT, 0, st>>>(n, M->t32, M->t, 0);
+        count_launch();
+        CIECU_TRY(ciecu_csr_spmv_f64(M->R, 0.0, M->t, 1.0, M->rc));
+        CIECU_TRY(coarse_solve(M, st));
+        CIECU_TRY(ciecu_csr_spmv_f64(M->P, 0.0, M->cx, 1.0, M->t));  // t = P ec
+        convert_kernel<double, float><<<grid_of(n), kT, 0, st>>>(n, M->t, M->z32, 1);
+        count_launch();
+        CIECU_CUDA(cudaMemcpyAsync(M->t32, M->r32, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+        CIECU_TRY(ciecu_csr_spmv_f32(S, 1.0f, M->z32, -1.0f, M->t32));
+        CIECU_TRY(chebyshev<float>(M, S, M->dinv32, M->t32, M->z32, true, M->cheb32, st));
+        convert_kernel<float, double><<<grid_of(n), kT, 0, st>>>(n, M->z32, M->z, 0);
+        count_launch();
+    }
+    count_cycle_kernel<<<1, 1, 0, st>>>(M->d_s);
+    count_launch();
+    CIECU_CHECK_LAUNCH("two-level cycle");
+    return CIECU_OK;
+}
+
+template <bool COND>
+int iteration(ciecu_mgcg_s* M, cudaStream_t st, cudaGraphConditionalHandle loop) {
+    const long n = M->n;
+    ciecu_csr_s* A = M->A;
+    const int grid = csr_grid(A, A->kernel);
+    CIECU_TRY(with_schedule(A->kernel, [&](auto kk) -> int {
+        constexpr int K = decltype(kk)::value;
+        mg_spmv_kernel<K, COND><<<fit_grid(mg_spmv_kernel<K, COND>, csr_threads<K>(), grid), csr_threads<K>(), 0,
+                                  st>>>(A->args<double>(), M->p, M->q, M->d_s, M->partials, M->counter, loop);
+        return CIECU_OK;
+    }));
+    mg_update_kernel<COND><<<grid_of(n), kT, 0, st>>>(n, M->x, M->r, M->p, M->q, M->d_s, M->partials, M->counter,
+                                                      loop);
+    count_launch(2);
+    CIECU_TRY(cycle(M, st));
+    mg_beta_kernel<false><<<grid_of(n), kT, 0, st>>>(n, M->r, M->z, M->zold, M->p, M->d_s, M->partials, M->counter);
+    mg_direction_kernel<<<grid_of(n), kT, 0, st>>>(n, M->z, M->p, M->zold, M->d_s);
+    count_launch(2);
+    CIECU_CHECK_LAUNCH("two-level CG iteration");
+    return CIECU_OK;
+}
+
+int build_graph(ciecu_mgcg_s* M) {
+    if (M->graph) return CIECU_OK;
+    cudaStream_t st = M->A->space->stream;
+    int status = CIECU_ERR_ARGUMENT;
+    if (device_loop_enabled())
+        status = build_while_graph(st, [&](cudaGraph_t, cudaGraphConditionalHandle loop) {
+            return iteration<true>(M, st, loop);
+        }, &M->graph);
+    if (status == CIECU_OK) {
+        M->deviceLoop = true;
+        return CIECU_OK;
+    }
+    cudaGetLastError();
+    M->deviceLoop = false;
+    cudaGraph_t g = nullptr;
+    CIECU_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    status = iteration<false>(M, st, 0);
+    cudaError_t e = cudaStreamEndCapture(st, &g);
+    if (status != CIECU_OK) {
+        if (g) cudaGraphDestroy(g);
+        return status;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "two-level CG graph capture");
+    e = cudaGraphInstantiate(&M->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(e, "two-level CG graph instantiate");
+    return CIECU_OK;
+}
+
+__global__ void to_f32_kernel(long n, const double* __restrict__ a, float* __restrict__ b) {
+    for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long>(gridDim.x) * blockDim.x)
+        b[i] = static_cast<float>(a[i]);
+}
+
+}  // namespace
+}  // namespace ciecu
+
+using namespace ciecu;
+
+extern "C" {
+
+int ciecu_mgcg_destroy(ciecu_mgcg M) {
+    if (!M) return CIECU_OK;
+    if (M->graph) cudaGraphExecDestroy(M->graph);
+    for (double* v : {M->x, M->r, M->p, M->q, M->z, M->zold, M->t, M->cheb, M->rc, M->cx, M->cr, M->cz, M->cp, M->cq,
+                      M->partials})
+        cudaFree(v);
+    for (float* v : {M->dinv32, M->r32, M->z32, M->t32, M->cheb32}) cudaFree(v);
+    cudaFree(M->d_s);
+    cudaFree(M->counter);
+    if (M->h_s) cudaFreeHost(M->h_s);
+    delete M;
+    return CIECU_OK;
+}
+
+int ciecu_mgcg_create(ciecu_csr fine, const double* d_fineInverseDiagonal, ciecu_csr smoother32,
+                      ciecu_csr prolongation, ciecu_csr restriction, ciecu_csr coarse,
+                      const double* d_coarseInverseDiagonal, ciecu_mg_options options, ciecu_statistics settings,
+                      ciecu_mgcg* out) {
+    CIECU_REQUIRE(fine && d_fineInverseDiagonal && prolongation && restriction && coarse && d_coarseInverseDiagonal &&
+                      out,
+                  "mgcg_create: null argument");
+    CIECU_REQUIRE(fine->valueType == CIECU_F64 && fine->rows == fine->cols, "mgcg_create: square FP64 fine matrix");
+    CIECU_REQUIRE(coarse->valueType == CIECU_F64 && coarse->rows == coarse->cols,
+                  "mgcg_create: square FP64 coarse matrix");
+    CIECU_REQUIRE(prolongation->valueType == CIECU_F64 && prolongation->rows == fine->rows &&
+                      prolongation->cols == coarse->rows,
+                  "mgcg_create: prolongation must be FP64, fine rows x coarse rows");
+    CIECU_REQUIRE(restriction->valueType == CIECU_F64 && restriction->rows == coarse->rows &&
+                      restriction->cols == fine->rows,
+                  "mgcg_create: restriction must be FP64, coarse rows x fine rows");
+    CIECU_REQUIRE(!smoother32 || (smoother32->valueType == CIECU_F32 && smoother32->rows == fine->rows &&
+                                  smoother32->cols == fine->cols),
+                  "mgcg_create: the FP32 smoother matrix must be FP32 and of the fine matrix's shape");
+    CIECU_REQUIRE(prolongation->space == fine->space && restriction->space == fine->space &&
+                      coarse->space == fine->space && (!smoother32 || smoother32->space == fine->space),
+                  "mgcg_create: every matrix must belong to the fine matrix's space");
+    CIECU_REQUIRE(options.degree >= 1 && options.degree <= 64, "mgcg_create: degree in [1, 64]");
+    CIECU_REQUIRE(options.coarseIterations >= 1 && options.coarseIterations <= 1000,
+                  "mgcg_create: coarse iterations in [1, 1000]");
+    CIECU_REQUIRE(options.ratio > 1.0, "mgcg_create: ratio must exceed 1");
+    CIECU_TRY(ensure_tuned(fine));
+    CIECU_TRY(ensure_tuned(coarse));
+    CIECU_TRY(ensure_tuned(prolongation));
+    CIECU_TRY(ensure_tuned(restriction));
+    if (smoother32) CIECU_TRY(ensure_tuned(smoother32));
+    auto* M = new ciecu_mgcg_s();
+    M->A = fine;
+    M->S32 = smoother32;
+    M->P = prolongation;
+    M->R = restriction;
+    M->Ac = coarse;
+    M->dinv = d_fineInverseDiagonal;
+    M->dinvc = d_coarseInverseDiagonal;
+    M->options = options;
+    M->settings = settings;
+    M->n = fine->rows;
+    M->m = coarse->rows;
+    const size_t n = static_cast<size_t>(std::max<long>(M->n, 1)), m = static_cast<size_t>(std::max<long>(M->m, 1));
+    cudaStream_t st = fine->space->stream;
+    cudaError_t e = cudaSuccess;
+    for (double** v : {&M->x, &M->r, &M->p, &M->q, &M->z, &M->zold, &M->t})
+        if (e == cudaSuccess) e = cudaMalloc(v, sizeof(double) * n);
+    for (double** v : {&M->rc, &M->cx, &M->cr, &M->cz, &M->cp, &M->cq})
+        if (e == cudaSuccess) e = cudaMalloc(v, sizeof(double) * m);
+    if (e == cudaSuccess && !smoother32) e = cudaMalloc(&M->cheb, sizeof(double) * 4 * n);
+    if (e == cudaSuccess && smoother32) {
+        for (float** v : {&M->dinv32, &M->r32, &M->z32, &M->t32})
+            if (e == cudaSuccess) e = cudaMalloc(v, sizeof(float) * n);
+        if (e == cudaSuccess) e = cudaMalloc(&M->cheb32, sizeof(float) * 4 * n);
+    }
+    if (e == cudaSuccess) e = cudaMalloc(&M->partials, sizeof(double) * 2 * kMaxPartials);
+    if (e == cudaSuccess) e = cudaMalloc(&M->counter, sizeof(unsigned) * 4);
+    if (e == cudaSuccess) e = cudaMemsetAsync(M->counter, 0, sizeof(unsigned) * 4, st);
+    if (e == cudaSuccess) e = cudaMalloc(&M->d_s, sizeof(MgScalars));
+    if (e == cudaSuccess) e = cudaMallocHost(&M->h_s, sizeof(MgScalars));
+    if (e != cudaSuccess) {
+        ciecu_mgcg_destroy(M);
+        return cuda_fail(e, "mgcg_create: allocation");
+    }
+    if (smoother32 && M->n > 0) {
+        to_f32_kernel<<<grid_of(M->n), kT, 0, st>>>(M->n, d_fineInverseDiagonal, M->dinv32);
+        count_launch();
+    }
+    M->lambdaMax = options.lambdaMax;
+    if (!(M->lambdaMax > 0.0) && M->n > 0) {
+        double lam = 0.0;
+        // 2n doubles of work: the FP64 Chebyshev buffer, or the FP32 one (4n floats)
+        double* work = M->cheb ? M->cheb : reinterpret_cast<double*>(M->cheb32);
+        const int status = ciecu_power_lambda_max_f64(fine, d_fineInverseDiagonal, 20, 0, work, &lam);
+        if (status != CIECU_OK) {
+            ciecu_mgcg_destroy(M);
+            return status;
+        }
+        M->lambdaMax = 1.1 * lam;
+    }
+    M->lambdaMin = M->lambdaMax / options.ratio;
+    *out = M;
+    return CIECU_OK;
+}
+
+int ciecu_mgcg_product(ciecu_mgcg M, double inScale, const double* d_in, double outScale, double* d_out,
+                       ciecu_statistics* h_stats) {
+    CIECU_REQUIRE(M, "mgcg_product: null solver");
+    const long n = M->n;
+    CIECU_REQUIRE(n == 0 || (d_in && d_out), "mgcg_product: null vector");
+    cudaStream_t st = M->A->space->stream;
+    ciecu_statistics stats{0, 1.7976931348623157e308, 1.7976931348623157e308};
+    if (n == 0) {
+        if (h_stats) *h_stats = ciecu_statistics{0, 0.0, 0.0};
+        return CIECU_OK;
+    }
+    CIECU_CUDA(cudaMemcpyAsync(M->x, d_out, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    if (M->settings.iterationCount > 0) {
+        MgScalars init{};
+        init.maxIter = M->settings.iterationCount;
+        init.absTol = M->settings.absoluteResidual;
+        init.relTol = M->settings.relativeResidual;
+        init.flexible = M->options.flexible ? 1 : 0;
+        *M->h_s = init;
+        CIECU_CUDA(cudaMemcpyAsync(M->d_s, M->h_s, sizeof(MgScalars), cudaMemcpyHostToDevice, st));
+        CIECU_CUDA(cudaMemcpyAsync(M->r, d_in, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+        CIECU_TRY(ciecu_csr_spmv_f64(M->A, 1.0, M->x, -1.0, M->r));  // r = b - A x
+        mg_init_kernel<<<grid_of(n), kT, 0, st>>>(n, M->r, M->d_s, M->partials, M->counter);
+        count_launch();
+        CIECU_TRY(cycle(M, st));
+        mg_beta_kernel<true><<<grid_of(n), kT, 0, st>>>(n, M->r, M->z, M->zold, M->p, M->d_s, M->partials,
+                                                        M->counter);
+        count_launch();
+        CIECU_CHECK_LAUNCH("two-level CG set-up");
+        CIECU_TRY(build_graph(M));
+        const long long limit = M->deviceLoop ? (1LL << 20) : 1;
+        for (;;) {
+            CIECU_CUDA(cudaMemcpyAsync(M->h_s, M->d_s, sizeof(MgScalars), cudaMemcpyDeviceToHost, st));
+            CIECU_CUDA(cudaStreamSynchronize(st));
+            if (M->h_s->done) break;
+            M->h_s->chunkIter = 0;
+            M->h_s->chunkLimit = limit;
+            CIECU_CUDA(cudaMemcpyAsync(&M->d_s->chunkIter, &M->h_s->chunkIter, 2 * sizeof(long long),
+                                       cudaMemcpyHostToDevice, st));
+            CIECU_CUDA(cudaGraphLaunch(M->graph, st));
+        }
+        const MgScalars& s = *M->h_s;
+        if (s.error) {
+            if (h_stats) *h_stats = ciecu_statistics{s.errorIter, s.absres, s.relres};
+            if (s.errorKind == 1)
+                return fail(CIECU_ERR_BREAKDOWN, "preconditioned norm vanished in iteration " +
+                                                     std::to_string(s.errorIter) + " (r^T @ z <= 0)");
+            return fail(CIECU_ERR_BREAKDOWN, "p^T @ A @ p vanished in iteration " + std::to_string(s.errorIter));
+        }
+        stats = ciecu_statistics{s.iter, s.absres, s.relres};
+    }
+    mg_output_kernel<<<grid_of(n), kT, 0, st>>>(n, inScale, outScale, M->x, d_out);
+    count_launch();
+    CIECU_CHECK_LAUNCH("mg_output_kernel");
+    CIECU_CUDA(cudaStreamSynchronize(st));
+    if (h_stats) *h_stats = stats;
+    return CIECU_OK;
+}
+
+int ciecu_mgcg_info(ciecu_mgcg M, double* h_lambdaMax, int64_t* h_cycles) {
+    CIECU_REQUIRE(M, "mgcg_info: null solver");
+    if (h_lambdaMax) *h_lambdaMax = M->lambdaMax;
+    if (h_cycles) *h_cycles = M->h_s ? M->h_s->cycles : 0;
+    return CIECU_OK;
+}
+
+}  // extern "C"

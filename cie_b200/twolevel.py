@@ -13,15 +13,18 @@ reference's operator algebra: CSR operators, diagonal, Chebyshev smoothing, CG).
   a Chebyshev polynomial smoother in D^-1 A and the coarse problem solved by the
   fused Jacobi-PCG to a tight tolerance.
 """
+import ctypes
+
 import numpy as np
 import torch
 
-from ._lib import CiecuError, Statistics
+from . import _lib
+from ._lib import CiecuError, MgOptions, Statistics, call
 from .fem import Assembler, StructuredMesh, csr_pattern
 from .linalg import (ChebyshevOperator, ConjugateGradients, CSRMatrix, CSROperator, LinearOperator,
-                     makeDiagonalOperator)
+                     _CSRHandle, _ptr, makeDiagonalOperator)
 
-__all__ = ["prolongation", "TwoLevelMultigrid", "make_two_level"]
+__all__ = ["prolongation", "TwoLevelMultigrid", "make_two_level", "TwoLevelCG", "make_two_level_cg"]
 
 
 def _csr_from_triplets(nrows, ncols, rows, cols, vals):
@@ -138,3 +141,81 @@ def make_two_level(space, problem, center=None, radius=0.4, alpha=1e-6, depth=2,
                            degree=degree, coarseSettings=coarseSettings)
     mg._keep = (cmat, casm, Pm, Rm)
     return fine, fineD, mg
+
+
+class TwoLevelCG(LinearOperator):
+    """Conjugate gradients preconditioned by the symmetric two-level cycle, run on
+    the device as one CUDA graph (ciecu_mgcg_*): Chebyshev smoothing of `degree`
+    in D^-1 A before and after a coarse correction made of `coarseIterations`
+    Jacobi-PCG iterations.  With `smoother32` (an FP32 CSRMatrix in the fine
+    pattern) the cycle smooths and forms its residuals in FP32; the outer
+    iteration stays FP64.  flexible=True uses the flexible CG beta, which keeps
+    the outer iteration convergent when the cycle is not a fixed linear operator."""
+
+    def __init__(self, fine, fineDiagonal, P, R, coarse, coarseDiagonal, settings, degree=2, coarseIterations=8,
+                 ratio=30.0, lambdaMax=0.0, flexible=True, smoother32=None):
+        self.lhs = fine
+        self.space = fine.space
+        self.settings = settings
+        self._stats = Statistics()
+        self._s32 = _CSRHandle(smoother32, self.space) if smoother32 is not None else None
+        opts = MgOptions(int(degree), float(lambdaMax), float(ratio), int(coarseIterations), int(bool(flexible)))
+        h = ctypes.c_void_p()
+        self.space.enter()
+        call("ciecu_mgcg_create", fine.csr.handle, _ptr(fineDiagonal.inverseDiagonal),
+             self._s32.handle if self._s32 is not None else None, P.csr.handle, R.csr.handle, coarse.csr.handle,
+             _ptr(coarseDiagonal.inverseDiagonal), opts, settings, ctypes.byref(h))
+        self.handle = h
+        self._keep = (fine, fineDiagonal, P, R, coarse, coarseDiagonal, smoother32)
+
+    def __del__(self):
+        try:
+            if getattr(self, "handle", None):
+                _lib.load().ciecu_mgcg_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+    def product(self, inScale, in_, outScale, out):
+        stats = Statistics()
+        self.space.enter()
+        try:
+            call("ciecu_mgcg_product", self.handle, float(inScale), _ptr(in_), float(outScale), _ptr(out),
+                 ctypes.byref(stats))
+        finally:
+            self._stats = stats
+            self.space.leave()
+
+    def getStats(self):
+        return self._stats
+
+    def info(self):
+        lam, cycles = ctypes.c_double(), ctypes.c_int64()
+        call("ciecu_mgcg_info", self.handle, ctypes.byref(lam), ctypes.byref(cycles))
+        return {"lambda_max": lam.value, "cycles": cycles.value}
+
+
+def make_two_level_cg(space, problem, settings, center=None, radius=0.4, alpha=1e-6, depth=2, degree=2,
+                      coarseIterations=8, ratio=30.0, flexible=True, precision="f64"):
+    """The device two-level CG of a finite-cell problem made by
+    make_embedded_poisson (same sphere, factor and tree).  precision "f32"
+    smooths on the FP32 matrix assembled with the tensor-core contraction
+    (ciecu_assemble_embedded_f32) and eliminated like the FP64 one."""
+    fine, fineD, mg = make_two_level(space, problem, center=center, radius=radius, alpha=alpha, depth=depth,
+                                     degree=degree)
+    cmat, casm, Pm, Rm = mg._keep
+    coarse = mg.coarseSolver.lhs
+    coarseD = mg.coarseSolver.preconditioner
+    s32 = None
+    if precision == "f32":
+        m = problem.matrix
+        v32 = torch.zeros(m.entries.numel(), dtype=torch.float32, device=space.device)
+        problem.assembler.assemble_embedded_f32(v32, [0.5] * problem.mesh.dim if center is None else center, radius,
+                                                alpha, depth)
+        problem.assembler.dirichlet_f32(problem.boundary, v32)
+        s32 = CSRMatrix(m.columnCount, m.rowExtents, m.columnIndices, v32)
+    solver = TwoLevelCG(fine, fineD, mg.P, mg.R, coarse, coarseD, settings, degree=degree,
+                        coarseIterations=coarseIterations, ratio=ratio, lambdaMax=mg.smoother.lambdaMax,
+                        flexible=flexible, smoother32=s32)
+    solver._mg = mg
+    return solver

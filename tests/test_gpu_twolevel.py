@@ -35,3 +35,37 @@ def test_two_level_pcg_vs_reference(reference):
     assert np.linalg.norm(r) <= 1.05e-10 * np.linalg.norm(b)
     assert rel <= 1e-9
     assert st.iterationCount < sr[0] / 3
+
+
+@pytest.mark.parametrize("precision,degree,coarse", [("f64", 2, 8), ("f32", 2, 8), ("f64", 4, 20)])
+def test_device_two_level_cg_vs_reference(reference, precision, degree, coarse):
+    """The device two-level CG (one CUDA graph, flexible beta) -- FP64 smoothing,
+    or FP32 smoothing on the matrix assembled by the split-BF16 tensor-core
+    contraction -- reaches the reference's FP64 solution within 1e-9 with the
+    true FP64 residual at 1e-10: the outer FP64 iteration refines whatever the
+    single-precision cycle approximates."""
+    from cie_b200.fem import make_embedded_poisson
+    from cie_b200.linalg import CUDASpace, Statistics
+    from cie_b200.twolevel import make_two_level_cg
+    space = CUDASpace()
+    prob = make_embedded_poisson(space, 3, 3, [7, 7, 7], radius=0.4, alpha=1e-6, depth=2, seed=1)
+    solver = make_two_level_cg(space, prob, Statistics(5000, 0.0, 1e-10), degree=degree, coarseIterations=coarse,
+                               precision=precision)
+    x = torch.zeros_like(prob.rhs)
+    solver.product(0.0, prob.rhs, 1.0, x)
+    st = solver.getStats()
+    rp, col, val = prob.host_csr()
+    b = prob.rhs.cpu().numpy()
+    xr, sr, err, _ = reference.pcg(rp, col, val, b, maxit=200000, abstol=0.0, reltol=1e-10)
+    assert err is None
+    xh = x.cpu().numpy()
+    from oracle.oracle import Restatement
+    r = Restatement().spmv(rp, col, val, 1.0, xh, -1.0, b)
+    rel = np.linalg.norm(xh - xr) / np.linalg.norm(xr)
+    print("device two-level CG (%s smoothing, degree %d, %d coarse iterations): %d iterations, %s; Jacobi-PCG "
+          "reference %d; |x - x_ref|/|x_ref| = %.3e" % (precision, degree, coarse, st.iterationCount, solver.info(),
+                                                        sr[0], rel))
+    assert st.relativeResidual < 1e-10
+    assert np.linalg.norm(r) <= 1.05e-10 * np.linalg.norm(b)
+    assert rel <= 1e-9
+    assert st.iterationCount < sr[0] / 3
