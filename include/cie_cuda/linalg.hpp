@@ -541,6 +541,8 @@ public:
     Statistics getConfiguration() const noexcept { return _settings; }
     std::optional<Statistics> getStats() const noexcept { return _stats; }
     bool fused() const noexcept { return static_cast<bool>(_solver); }
+    // The fused device solver (null for the generic composition).
+    ciecu_pcg handle() const noexcept { return _solver.get(); }
 
     void product(double inScale, Space::ConstVectorView in, double outScale, Space::VectorView out) override {
         require(in.size() == out.size(), "ConjugateGradients::product: incompatible vector sizes");
