@@ -43,6 +43,13 @@ PROFILE_CELLS = [96, 96, 96]
 # 0.1 gives 10 replacements and a solution 2e-11 from the FP64 solver's; 0.01 saves
 # 5 replacements but lands 1.1e-9 away, outside the 1e-9 parity bar.
 DELTA = 0.1
+# Inner-iteration form of the mixed solver: True = the search direction and its
+# product formed by recurrence inside the inner SpMV (two kernels per iteration),
+# False = the separate direction kernel (three).  The other form is timed beside it.
+FUSE = False
+# Two-level CG on the finite-cell Q3 sphere: (smoothing precision, Chebyshev
+# degree, pipelined coarse PCG iterations per cycle)
+TWO_LEVEL = (("f64", 4, 80), ("f32", 6, 150))
 METRIC = "PCG time-to-1e-10 (s), 3D Q1 128^3 Poisson"
 
 
@@ -271,7 +278,7 @@ def main():
             b = rhs_h.to("cuda", non_blocking=True)
             A2 = CSROperator(m, space)
             D2 = makeDiagonalOperator(m, space, csr_handle=A2.csr)
-            M2 = MixedPrecisionCG(A2, D2, settings, mode=0, delta=DELTA)
+            M2 = MixedPrecisionCG(A2, D2, settings, mode=0, delta=DELTA, fuseDirection=FUSE)
             xe = torch.zeros(n, dtype=torch.float64, device="cuda")
             M2.product(0.0, b, 1.0, xe)
             sol_h.copy_(xe, non_blocking=True)
@@ -291,9 +298,9 @@ def main():
         pin_fp64, pin_unroll, pin_csr = (int(v) for v in args.pin.split(","))
         A.csr.set_kernel(pin_csr)
         cg.set_schedule(pin_fp64)
-        mixed = MixedPrecisionCG(A, D, settings, mode=0, delta=DELTA, innerKernel=pin_unroll)
+        mixed = MixedPrecisionCG(A, D, settings, mode=0, delta=DELTA, innerKernel=pin_unroll, fuseDirection=FUSE)
     else:
-        mixed = MixedPrecisionCG(A, D, settings, mode=0, delta=DELTA)
+        mixed = MixedPrecisionCG(A, D, settings, mode=0, delta=DELTA, fuseDirection=FUSE)
     x64 = torch.zeros_like(prob.rhs)
     xmx = torch.zeros_like(prob.rhs)
     stream = torch.cuda.ExternalStream(space.stream.cuda_stream)
@@ -362,6 +369,19 @@ def main():
     t_fp64 = timed(solve_fp64, args.steps)
     launches = launch_count() - launches0
 
+    # the other inner-iteration form on the same system (reported, not the headline)
+    other = MixedPrecisionCG(A, D, settings, mode=0, delta=DELTA, fuseDirection=not FUSE)
+    xother = torch.zeros_like(prob.rhs)
+
+    def solve_other():
+        xother.zero_()
+        other.product(0.0, prob.rhs, 1.0, xother)
+
+    for _ in range(2):
+        solve_other()
+    t_other = timed(solve_other, args.steps)
+    ost = other.getStats()
+
     # dominant kernels, timed live with CUDA events on the launching stream
     lib = _lib.load()
     from cie_b200.linalg import _ptr
@@ -385,7 +405,7 @@ def main():
     clocks = sampler.stop()
 
     from cie_b200.sharding import max_over_ranks
-    t_mixed, t_fp64, t_spmv32, t_spmv64 = max_over_ranks([t_mixed, t_fp64, t_spmv32, t_spmv64])
+    t_mixed, t_fp64, t_spmv32, t_spmv64, t_other = max_over_ranks([t_mixed, t_fp64, t_spmv32, t_spmv64, t_other])
     info = mixed.info()
 
     ndiag = A.csr.diagonals()
@@ -434,7 +454,7 @@ def main():
         r = prob.rhs.clone()
         A.product(1.0, x, -1.0, r)
         return float(torch.linalg.norm(r) / torch.linalg.norm(prob.rhs))
-    rel_mixed, rel_fp64 = true_rel(xmx), true_rel(x64)
+    rel_mixed, rel_fp64, rel_other = true_rel(xmx), true_rel(x64), true_rel(xother)
     agree = float(torch.linalg.norm(xmx - x64) / torch.linalg.norm(x64))
 
     extra = None
@@ -472,8 +492,8 @@ def main():
             "vs_baseline": None, "dtype": "f32 inner / f64 refinement",
             "data": "synthetic (seeded mt19937_64 RHS and kappa field)",
             "config": common_config(world),
-            "solver": {"mixed": "jacobi-pcg, FP32 inner over %s, FP64 reliable updates delta=%g" % (info["format"],
-                                                                                                  DELTA),
+            "solver": {"mixed": "jacobi-pcg, FP32 inner over %s, FP64 reliable updates delta=%g, %s" % (
+                           info["format"], DELTA, "fused direction" if FUSE else "separate direction kernel"),
                        "fp64": "jacobi-pcg over %s" % ("dia" if dia64 else "csr")},
             "gpu_launches": int(launches),
             "clocks": clocks,
@@ -490,6 +510,11 @@ def main():
             "mixed": {"seconds": t_mixed, "inner_iterations": mst.innerIterations,
                       "refinements": mst.refinements, "true_relative_residual": rel_mixed,
                       "rel_diff_vs_fp64_solution": agree, "achieved_gbs": mixed_solve_bytes / t_mixed / 1e9},
+            "mixed_other_form": {"form": "fused direction" if not FUSE else "separate direction kernel",
+                                 "seconds": t_other, "inner_iterations": ost.innerIterations,
+                                 "refinements": ost.refinements, "true_relative_residual": rel_other,
+                                 "achieved_gbs": (ost.innerIterations * inner_bytes +
+                                                  (ost.refinements + 1) * refine_bytes) / t_other / 1e9},
             "speedup_mixed_vs_fp64": t_fp64 / t_mixed,
             "pcg_iteration_roofline": {"fp64_frac": fp64_solve_bytes / t_fp64 / 1e9 / hbm,
                                        "mixed_frac": mixed_solve_bytes / t_mixed / 1e9 / hbm},
@@ -647,18 +672,27 @@ def extra_workloads(space, A, D, settings, t_fp64, it64, rank=0, world=1):
     tb = timed(solveb, 3)
     its = [s.iterationCount for s in batch.getStats()]
     rels = [s.relativeResidual for s in batch.getStats()]
-    # the same batch with FP32 inner solves and FP64 refinement
-    refined = BatchedConjugateGradients(bd, offsets, space, Dbd, tight)
-    refined.set_refinement(1e-2)
+    # the same batch with FP32 inner solves and FP64 refinement, for three drops of
+    # the FP32 residual per refinement round (fewer rounds keep more of each Krylov
+    # space); the fastest is reported
+    refinedByTol = {}
     xr = torch.zeros_like(rhs)
+    best = None
+    for tol in (1e-2, 1e-4, 1e-5):
+        refined = BatchedConjugateGradients(bd, offsets, space, Dbd, tight)
+        refined.set_refinement(tol)
 
-    def solver_refined():
-        xr.zero_()
-        refined.product(0.0, rhs, 1.0, xr)
-    tr = timed(solver_refined, 2)
-    rits = [s.iterationCount for s in refined.getStats()]
-    rrel = max(s.relativeResidual for s in refined.getStats())
-    del refined
+        def solver_refined():
+            xr.zero_()
+            refined.product(0.0, rhs, 1.0, xr)
+        t_tol = timed(solver_refined, 1)
+        its_tol = [s.iterationCount for s in refined.getStats()]
+        refinedByTol["%g" % tol] = {"seconds": t_tol, "inner_iterations_max": int(max(its_tol))}
+        if best is None or t_tol < best[0]:
+            best = (t_tol, tol, its_tol, max(s.relativeResidual for s in refined.getStats()),
+                    float(torch.linalg.norm(xr - xb) / torch.linalg.norm(xb)))
+        del refined
+    tr, rtol, rits, rrel, rdiff = best
     # the same systems one after another (one solver object per system)
     singles = []
     for p in probs:
@@ -677,9 +711,9 @@ def extra_workloads(space, A, D, settings, t_fp64, it64, rank=0, world=1):
         "iterations_min": int(min(its)), "iterations_max": int(max(its)), "max_relative_residual": max(rels),
         "sequential_single_solves_seconds": ts, "speedup_vs_sequential": ts / tb,
         "rel_diff_vs_single_solves": agree, "solver": batch.info(),
-        "fp32_refined_seconds": tr, "fp32_refined_inner_iterations_max": int(max(rits)),
-        "fp32_refined_max_relative_residual": rrel,
-        "fp32_refined_rel_diff_vs_fp64": float(torch.linalg.norm(xr - xb) / torch.linalg.norm(xb))}
+        "fp32_refined_seconds": tr, "fp32_refined_inner_tolerance": rtol,
+        "fp32_refined_inner_iterations_max": int(max(rits)), "fp32_refined_max_relative_residual": rrel,
+        "fp32_refined_rel_diff_vs_fp64": rdiff, "fp32_refined_by_inner_tolerance": refinedByTol}
     del singles, batch, Dbd, bd, rhs, xb, xr, probs
 
     # 32 right-hand sides on the 128^3 matrix
@@ -694,12 +728,28 @@ def extra_workloads(space, A, D, settings, t_fp64, it64, rank=0, world=1):
         mrhs.product(0.0, B, 1.0, X)
     tm = timed(solvem, 2)
     its = [s.iterationCount for s in mrhs.getStats()]
+    fmt = mrhs.info()["spmm_format"]
+    X64 = X.clone()
+    # the FP32-refined form of the same 32 solves (FP32 SpMM iterations, FP64
+    # reliable updates per column)
+    mrhs.set_refinement(DELTA)
+    solvem()
+    tmr = timed(solvem, 2)
+    rits = [s.iterationCount for s in mrhs.getStats()]
+    refs = mrhs.refinements()
+    rres = max(s.relativeResidual for s in mrhs.getStats())
+    rdiff = max(float(torch.linalg.norm(X[:, c] - X64[:, c]) / torch.linalg.norm(X64[:, c])) for c in range(k))
+    mrhs.set_refinement(0.0)
+    solvem()
     out["multi_rhs_32_poisson3d_q1_128^3_fp64_pcg"] = {
-        "seconds": tm, "rhs": k, "iterations_min": int(min(its)), "iterations_max": int(max(its)),
+        "seconds": tm, "rhs": k, "spmm_format": fmt, "iterations_min": int(min(its)), "iterations_max": int(max(its)),
         "max_relative_residual": max(s.relativeResidual for s in mrhs.getStats()),
         "seconds_per_rhs": tm / k, "single_solve_seconds": t_fp64, "speedup_vs_32_single_solves": 32 * t_fp64 / tm,
+        "fp32_refined_seconds": tmr, "fp32_refined_iterations_max": int(max(rits)),
+        "fp32_refined_replacements_max": int(max(refs)), "fp32_refined_max_relative_residual": rres,
+        "fp32_refined_max_rel_diff_vs_fp64": rdiff, "fp32_refined_speedup_vs_fp64": tm / tmr,
         "note": "random right-hand sides, boundary rows included (identity rows of the eliminated system)"}
-    del mrhs, X, B
+    del mrhs, X, B, X64
 
     # embedded (finite-cell) Q3 sphere on 32^3 cells: set-up (pattern on the host and
     # on the device, FP64 and FP32 tensor-core assembly), FP64 Jacobi-PCG, and the
@@ -749,8 +799,8 @@ def extra_workloads(space, A, D, settings, t_fp64, it64, rank=0, world=1):
            "fp32_matrix_max_rel_entry_error": asm32_err,
            "jacobi_pcg_seconds": tj, "jacobi_pcg_iterations": itj, "jacobi_us_per_iteration": 1e6 * tj / (itj + 1)}
     del cge
-    for precision in ("f64", "f32"):
-        solver = make_two_level_cg(space, pe, Statistics(20000, 0.0, 1e-10), degree=2, coarseIterations=8,
+    for precision, degree, coarse in TWO_LEVEL:
+        solver = make_two_level_cg(space, pe, Statistics(20000, 0.0, 1e-10), degree=degree, coarseIterations=coarse,
                                    precision=precision)
         xm = torch.zeros_like(pe.rhs)
 
@@ -762,7 +812,7 @@ def extra_workloads(space, A, D, settings, t_fp64, it64, rank=0, world=1):
         r = pe.rhs.clone()
         Ae.product(1.0, xm, -1.0, r)
         emb["two_level_%s_smoothing" % precision] = {
-            "seconds": tmg, "iterations": st.iterationCount,
+            "seconds": tmg, "iterations": st.iterationCount, "chebyshev_degree": degree, "coarse_iterations": coarse,
             "true_relative_residual": float(torch.linalg.norm(r) / torch.linalg.norm(pe.rhs)),
             "rel_diff_vs_jacobi": float(torch.linalg.norm(xm - xe) / torch.linalg.norm(xe)),
             "speedup_vs_jacobi": tj / tmg}

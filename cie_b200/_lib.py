@@ -24,7 +24,7 @@ class Statistics(ctypes.Structure):
 
 class MixedOptions(ctypes.Structure):
     _fields_ = [("mode", c_int), ("delta", c_double), ("compressColumns", c_int), ("innerKernel", c_int),
-                ("scaleInner", c_int)]
+                ("scaleInner", c_int), ("fuseDirection", c_int)]
 
 
 class MgOptions(ctypes.Structure):
@@ -122,6 +122,8 @@ SIGNATURES = {
     "ciecu_multi_destroy": (c_int, [P]),
     "ciecu_multi_info": (c_int, [P, P, P]),
     "ciecu_multi_format": (c_int, [P, P]),
+    "ciecu_multi_set_refinement": (c_int, [P, c_double]),
+    "ciecu_multi_refinements": (c_int, [P, P]),
     "ciecu_multi_product": (c_int, [P, c_double, P, c_double, P, P]),
     "ciecu_dirichlet_eliminate": (c_int, [P, P, P, P]),
     "ciecu_write_matrix_market_host": (c_int, [c_char_p, c_int64, c_int64, P, P, P]),

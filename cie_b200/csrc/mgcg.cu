@@ -9,8 +9,8 @@
 //   M4  p = z + beta p
 // S is a Chebyshev polynomial smoother in D^-1 A (FP64 on the solver's matrix,
 // or FP32 on a single-precision copy), C a fixed number of Jacobi-PCG
-// iterations on the coarse matrix from zero (kernels on the device scalars, no
-// host round trip).  The body runs under a WHILE conditional node of a CUDA
+// iterations on the coarse matrix from zero in the pipelined form (one kernel per
+// iteration, on the device scalars, no host round trip).  The body runs under a WHILE conditional node of a CUDA
 // graph; M1 / M2 end the loop.  Every reduction is deterministic (per-block
 // partials summed in block order by the last block).
 #include "ciecu_mg.h"
@@ -31,7 +31,8 @@ struct MgScalars {
     long long iter, maxIter;
     int done, error, errorKind, flexible;
     long long errorIter, chunkIter, chunkLimit, cycles;
-    double crz, calpha, cbeta;  // coarse solve
+    double cgamma, calpha, cbeta;  // coarse solve
+    int cfrozen;
 };
 
 template <bool COND>
@@ -234,63 +235,129 @@ __global__ void convert_kernel(long n, const A* __restrict__ a, B* __restrict__ 
 }
 
 // ---- coarse solve: a fixed number of Jacobi-PCG iterations from zero ----------
+//
+// Pipelined form of the preconditioned CG (Ghysels and Vanroose, "Hiding global
+// synchronization latency in the preconditioned conjugate gradient algorithm",
+// Parallel Computing 40 (2014), Alg. 4): with u = D^-1 r, w = A u, m = D^-1 w and
+// n = A m kept by recurrences, the two dot products of an iteration, (r, u) and
+// (w, u), come from the same vectors and are reduced together, so an iteration
+// is ONE kernel: n = A m, then on the own rows
+//   z = n + beta z, q = m + beta q, s = w + beta s, p = u + beta p,
+//   x += alpha p, r -= alpha s, u -= alpha q, w -= alpha z, m' = D^-1 w,
+// and the partial sums of the next (r, u), (w, u); the last block forms the next
+// beta = gamma' / gamma and alpha = gamma' / (delta' - beta gamma' / alpha).  m
+// is double-buffered (a block overwrites its rows of m' while other blocks still
+// gather m).  In exact arithmetic the iterates are those of the Jacobi-PCG.  A
+// non-positive gamma or denominator freezes the solve (alpha = beta = 0: no
+// further steps), as converged or broken-down iterations must not move x.
 
-__global__ void __launch_bounds__(kT) coarse_init_kernel(long m, const double* __restrict__ b,
-                                                         const double* __restrict__ dinv, double* __restrict__ x,
-                                                         double* __restrict__ r, double* __restrict__ z,
-                                                         double* __restrict__ p, MgScalars* s, double* partials,
-                                                         unsigned* counter) {
-    double rz = 0.0;
+struct CoarseVectors {
+    double *x, *r, *u, *w, *z, *q, *s, *p;
+    double* m[2];
+};
+
+__global__ void __launch_bounds__(kT) coarse_start_kernel(long m, const double* __restrict__ b,
+                                                          const double* __restrict__ dinv, CoarseVectors v) {
     for (long i = blockIdx.x * static_cast<long>(kT) + threadIdx.x; i < m; i += static_cast<long>(gridDim.x) * kT) {
-        const double ri = b[i], zi = dinv[i] * ri;
-        x[i] = 0.0;
-        r[i] = ri;
-        z[i] = zi;
-        p[i] = zi;
-        rz = fma(ri, zi, rz);
+        const double bi = b[i];
+        v.x[i] = 0.0;
+        v.r[i] = bi;
+        v.u[i] = dinv[i] * bi;
+        v.z[i] = 0.0;
+        v.q[i] = 0.0;
+        v.s[i] = 0.0;
+        v.p[i] = 0.0;
     }
-    double mine[1] = {rz}, tot[1];
-    if (grid_reduce_last<1, kT>(mine, partials, counter, tot) && threadIdx.x == 0) s->crz = tot[0];
 }
+
+// w = A u, m0 = D^-1 w, gamma = (r, u), delta = (w, u) -> the first alpha.
+struct CoarseFirstOp {
+    struct Pre {
+        double r, u, d;
+    };
+    const double* __restrict__ dinv;
+    CoarseVectors v;
+    double gamma, delta;
+    __device__ __forceinline__ Pre pre(int i) const { return Pre{v.r[i], v.u[i], dinv[i]}; }
+    __device__ __forceinline__ void post(int i, const Pre& pr, double sum) {
+        v.w[i] = sum;
+        v.m[0][i] = pr.d * sum;
+        gamma = fma(pr.r, pr.u, gamma);
+        delta = fma(sum, pr.u, delta);
+    }
+};
 
 template <int K>
 __global__ void __launch_bounds__(csr_threads<K>())
-    coarse_spmv_kernel(CsrArgs<double> A, const double* __restrict__ p, double* __restrict__ q, MgScalars* s,
+    coarse_first_kernel(CsrArgs<double> A, const double* __restrict__ dinv, CoarseVectors v, MgScalars* s,
+                        double* partials, unsigned* counter) {
+    CoarseFirstOp op{dinv, v, 0.0, 0.0};
+    csr_rows<K, double, double, false>(A, v.u, op);
+    double mine[2] = {op.gamma, op.delta}, tot[2];
+    if (grid_reduce_last<2, csr_threads<K>()>(mine, partials, counter, tot) && threadIdx.x == 0) {
+        const bool ok = 0.0 < tot[0] && 0.0 < tot[1];
+        s->cgamma = tot[0];
+        s->calpha = ok ? tot[0] / tot[1] : 0.0;
+        s->cbeta = 0.0;
+        s->cfrozen = ok ? 0 : 1;
+    }
+}
+
+struct CoarsePipeOp {
+    struct Pre {
+        double z, q, s, p, x, r, u, w, m, d;
+    };
+    const double* __restrict__ dinv;
+    CoarseVectors v;
+    const double* __restrict__ mcur;
+    double* __restrict__ mnext;
+    double alpha, beta;
+    double gamma, delta;
+    __device__ __forceinline__ Pre pre(int i) const {
+        return Pre{v.z[i], v.q[i], v.s[i], v.p[i], v.x[i], v.r[i], v.u[i], v.w[i], mcur[i], dinv[i]};
+    }
+    __device__ __forceinline__ void post(int i, const Pre& a, double n) {
+        const double z = fma(beta, a.z, n), q = fma(beta, a.q, a.m), s = fma(beta, a.s, a.w),
+                     p = fma(beta, a.p, a.u);
+        const double r = fma(-alpha, s, a.r), u = fma(-alpha, q, a.u), w = fma(-alpha, z, a.w);
+        v.z[i] = z;
+        v.q[i] = q;
+        v.s[i] = s;
+        v.p[i] = p;
+        v.x[i] = fma(alpha, p, a.x);
+        v.r[i] = r;
+        v.u[i] = u;
+        v.w[i] = w;
+        mnext[i] = a.d * w;
+        gamma = fma(r, u, gamma);
+        delta = fma(w, u, delta);
+    }
+};
+
+template <int K>
+__global__ void __launch_bounds__(csr_threads<K>())
+    coarse_pipe_kernel(CsrArgs<double> A, const double* __restrict__ dinv, CoarseVectors v, int cur, MgScalars* s,
                        double* partials, unsigned* counter) {
-    PqOp op{p, q, 0.0};
-    csr_rows<K, double, double, false>(A, p, op);
-    double mine[1] = {op.acc}, tot[1];
-    if (grid_reduce_last<1, csr_threads<K>()>(mine, partials, counter, tot) && threadIdx.x == 0)
-        s->calpha = (0.0 < tot[0] && 0.0 < s->crz) ? s->crz / tot[0] : 0.0;  // converged or broken down: no step
-}
-
-__global__ void __launch_bounds__(kT) coarse_update_kernel(long m, const double* __restrict__ dinv,
-                                                           double* __restrict__ x, double* __restrict__ r,
-                                                           double* __restrict__ z, const double* __restrict__ p,
-                                                           const double* __restrict__ q, MgScalars* s,
-                                                           double* partials, unsigned* counter) {
-    const double alpha = s->calpha;
-    double rz = 0.0;
-    for (long i = blockIdx.x * static_cast<long>(kT) + threadIdx.x; i < m; i += static_cast<long>(gridDim.x) * kT) {
-        x[i] = fma(alpha, p[i], x[i]);
-        const double ri = fma(-alpha, q[i], r[i]);
-        const double zi = dinv[i] * ri;
-        r[i] = ri;
-        z[i] = zi;
-        rz = fma(ri, zi, rz);
+    const volatile MgScalars* vs = s;
+    double* const m0 = v.m[0];
+    double* const m1 = v.m[1];
+    CoarsePipeOp op{dinv, v, cur ? m1 : m0, cur ? m0 : m1, vs->calpha, vs->cbeta, 0.0, 0.0};
+    csr_rows<K, double, double, false>(A, op.mcur, op);
+    double mine[2] = {op.gamma, op.delta}, tot[2];
+    if (grid_reduce_last<2, csr_threads<K>()>(mine, partials, counter, tot) && threadIdx.x == 0) {
+        if (s->cfrozen) return;
+        const double beta = tot[0] / s->cgamma;
+        const double denom = tot[1] - beta * tot[0] / s->calpha;
+        if (!(0.0 < tot[0]) || !(0.0 < denom)) {  // converged to rounding or broken down: no further steps
+            s->calpha = 0.0;
+            s->cbeta = 0.0;
+            s->cfrozen = 1;
+            return;
+        }
+        s->cbeta = beta;
+        s->calpha = tot[0] / denom;
+        s->cgamma = tot[0];
     }
-    double mine[1] = {rz}, tot[1];
-    if (grid_reduce_last<1, kT>(mine, partials, counter, tot) && threadIdx.x == 0) {
-        s->cbeta = 0.0 < s->crz ? tot[0] / s->crz : 0.0;
-        s->crz = tot[0];
-    }
-}
-
-__global__ void __launch_bounds__(kT) coarse_direction_kernel(long m, const double* __restrict__ z,
-                                                              double* __restrict__ p, const MgScalars* s) {
-    const double beta = s->cbeta;
-    for (long i = blockIdx.x * static_cast<long>(kT) + threadIdx.x; i < m; i += static_cast<long>(gridDim.x) * kT)
-        p[i] = fma(beta, p[i], z[i]);
 }
 
 __global__ void count_cycle_kernel(MgScalars* s) { s->cycles += 1; }
@@ -309,6 +376,7 @@ struct ciecu_mgcg_s {
     double* cheb = nullptr;  // 4n (FP64 smoothing)
     float *dinv32 = nullptr, *r32 = nullptr, *z32 = nullptr, *t32 = nullptr, *cheb32 = nullptr;  // FP32 smoothing
     double *rc = nullptr, *cx = nullptr, *cr = nullptr, *cz = nullptr, *cp = nullptr, *cq = nullptr;
+    double *cu = nullptr, *cw = nullptr, *cs = nullptr, *cm0 = nullptr, *cm1 = nullptr;
     ciecu::MgScalars* d_s = nullptr;
     ciecu::MgScalars* h_s = nullptr;
     double* partials = nullptr;
@@ -356,27 +424,26 @@ int chebyshev(ciecu_mgcg_s* M, ciecu_csr_s* A, const T* dinv, const T* in, T* ou
     return CIECU_OK;
 }
 
-// ec = C rc: coarseIterations Jacobi-PCG iterations from zero, result in M->cx.
+// ec = C rc: coarseIterations Jacobi-PCG iterations from zero (pipelined: one
+// kernel per iteration), result in M->cx.
 int coarse_solve(ciecu_mgcg_s* M, cudaStream_t st) {
     const long m = M->m;
     ciecu_csr_s* Ac = M->Ac;
-    coarse_init_kernel<<<grid_of(m), kT, 0, st>>>(m, M->rc, M->dinvc, M->cx, M->cr, M->cz, M->cp, M->d_s,
-                                                  M->partials, M->counter);
+    const CoarseVectors v{M->cx, M->cr, M->cu, M->cw, M->cz, M->cq, M->cs, M->cp, {M->cm0, M->cm1}};
+    coarse_start_kernel<<<grid_of(m), kT, 0, st>>>(m, M->rc, M->dinvc, v);
     count_launch();
     const int grid = csr_grid(Ac, Ac->kernel);
-    for (int it = 0; it < M->options.coarseIterations; ++it) {
-        CIECU_TRY(with_schedule(Ac->kernel, [&](auto kk) -> int {
-            constexpr int K = decltype(kk)::value;
-            coarse_spmv_kernel<K><<<fit_grid(coarse_spmv_kernel<K>, csr_threads<K>(), grid), csr_threads<K>(), 0,
-                                    st>>>(Ac->args<double>(), M->cp, M->cq, M->d_s, M->partials, M->counter);
-            return CIECU_OK;
-        }));
-        coarse_update_kernel<<<grid_of(m), kT, 0, st>>>(m, M->dinvc, M->cx, M->cr, M->cz, M->cp, M->cq, M->d_s,
-                                                        M->partials, M->counter);
-        coarse_direction_kernel<<<grid_of(m), kT, 0, st>>>(m, M->cz, M->cp, M->d_s);
-        count_launch(3);
-    }
-    return CIECU_OK;
+    return with_schedule(Ac->kernel, [&](auto kk) -> int {
+        constexpr int K = decltype(kk)::value;
+        coarse_first_kernel<K><<<fit_grid(coarse_first_kernel<K>, csr_threads<K>(), grid), csr_threads<K>(), 0,
+                                 st>>>(Ac->args<double>(), M->dinvc, v, M->d_s, M->partials, M->counter);
+        const int g = fit_grid(coarse_pipe_kernel<K>, csr_threads<K>(), grid);
+        for (int it = 0; it < M->options.coarseIterations; ++it)
+            coarse_pipe_kernel<K><<<g, csr_threads<K>(), 0, st>>>(Ac->args<double>(), M->dinvc, v, it & 1, M->d_s,
+                                                                 M->partials, M->counter);
+        count_launch(1 + M->options.coarseIterations);
+        return CIECU_OK;
+    });
 }
 
 // z = cycle(r) (the symmetric two-level cycle).
@@ -487,7 +554,7 @@ int ciecu_mgcg_destroy(ciecu_mgcg M) {
     if (!M) return CIECU_OK;
     if (M->graph) cudaGraphExecDestroy(M->graph);
     for (double* v : {M->x, M->r, M->p, M->q, M->z, M->zold, M->t, M->cheb, M->rc, M->cx, M->cr, M->cz, M->cp, M->cq,
-                      M->partials})
+                      M->cu, M->cw, M->cs, M->cm0, M->cm1, M->partials})
         cudaFree(v);
     for (float* v : {M->dinv32, M->r32, M->z32, M->t32, M->cheb32}) cudaFree(v);
     cudaFree(M->d_s);
@@ -545,7 +612,7 @@ int ciecu_mgcg_create(ciecu_csr fine, const double* d_fineInverseDiagonal, ciecu
     cudaError_t e = cudaSuccess;
     for (double** v : {&M->x, &M->r, &M->p, &M->q, &M->z, &M->zold, &M->t})
         if (e == cudaSuccess) e = cudaMalloc(v, sizeof(double) * n);
-    for (double** v : {&M->rc, &M->cx, &M->cr, &M->cz, &M->cp, &M->cq})
+    for (double** v : {&M->rc, &M->cx, &M->cr, &M->cz, &M->cp, &M->cq, &M->cu, &M->cw, &M->cs, &M->cm0, &M->cm1})
         if (e == cudaSuccess) e = cudaMalloc(v, sizeof(double) * m);
     if (e == cudaSuccess && !smoother32) e = cudaMalloc(&M->cheb, sizeof(double) * 4 * n);
     if (e == cudaSuccess && smoother32) {

@@ -26,14 +26,9 @@
 //
 // The solve stops only on the TRUE FP64 residual: ||b - A64 x64|| <= tol ||r0||.
 //
-// One inner iteration = 2 kernels: M1 forms the search direction
-// p_k = z_k + beta p_{k-1} on the fly for every entry it gathers (z = D^-1 r is
-// kept as a vector), stores p_k of its own rows and computes q = A32 p_k with
-// p^T q; M2 updates x and r, writes z and reduces the dot products.  p is double
-// buffered by the parity of the iteration count, so no block overwrites an entry
-// of p_{k-1} that another block still gathers.  The two refinement kernels (R1
-// fold, R2 FP64 residual) are in the same CUDA graph and run only when M2 asked
-// for a replacement.
+// One inner iteration = 3 kernels (M1 SpMV+p^T q, M2 update+dots+decision,
+// M3 direction); the two refinement kernels (R1 fold, R2 FP64 residual) are in
+// the same CUDA graph and return at once unless M2 asked for a replacement.
 #include "ciecu_mixed.h"
 #include "graph.cuh"
 #include "pcg.cuh"
@@ -160,61 +155,78 @@ __global__ void __launch_bounds__(kT) mixed_apply_kernel(SellArgs<float, CI> A, 
     sell_rows<U, float, float, CI>(A, x, op);
 }
 
-// Search direction of iteration k at entry c: p_k = z_k + beta p_{k-1} in FP32
-// (p_k = z_k when beta == 0: the first iteration and a restart), the same
-// expression in every thread that needs it.
-struct Direction {
-    const float* __restrict__ z;
-    const float* __restrict__ pold;
-    float beta;
-    __device__ __forceinline__ float operator()(int c) const {
-        const float zc = __ldg(z + c);
-        return beta == 0.0f ? zc : fmaf(beta, __ldg(pold + c), zc);
-    }
-};
-
-// The two p buffers of iteration k: p_{k-1} read, p_k written.
-struct DirectionBuffers {
-    float* p0;  // p_k for even k
-    float* p1;  // p_k for odd k
-};
-
-__device__ __forceinline__ long long iteration_of(const MixedScalars* s) {
-    return *reinterpret_cast<const volatile long long*>(&s->iter);
-}
-
-// M1: p_k of the own rows stored, q = A32 p_k, p_k^T q (FP64 accumulation), alpha.
+// M1: q = A32 p, p^T q (FP64 accumulation), alpha.
 struct MixedPqOp {
     using Pre = float;
-    Direction dir;
-    float* __restrict__ pnew;
+    const float* __restrict__ p;
     float* __restrict__ q;
     double acc;
-    __device__ __forceinline__ float pre(int r) const { return dir(r); }
+    __device__ __forceinline__ float pre(int r) const { return p[r]; }
     __device__ __forceinline__ void post(int r, float pr, float sum) {
-        pnew[r] = pr;
         q[r] = sum;
         acc = fma(static_cast<double>(pr), static_cast<double>(sum), acc);
     }
 };
 
-__device__ __forceinline__ MixedPqOp make_pq_op(const float* z, DirectionBuffers P, float* q, const MixedScalars* s) {
-    const bool odd = (iteration_of(s) & 1) != 0;
-    const float beta = static_cast<float>(*reinterpret_cast<const volatile double*>(&s->beta));
-    return MixedPqOp{Direction{z, odd ? P.p0 : P.p1, beta}, odd ? P.p1 : P.p0, q, 0.0};
-}
+// M1 of the fused form (options.fuseDirection): w = A32 z with z = D^-1 r kept as
+// a vector, then on the own rows p = z + beta p and q = w + beta q (the search
+// direction and its product by recurrence; p = z, q = w after a restart,
+// beta = 0), p^T q.  One vector is gathered, and the separate direction pass
+// over p, r and D^-1 is gone.
+struct MixedDirOp {
+    struct Pre {
+        float z, p, q;
+    };
+    const float* __restrict__ z;
+    float* __restrict__ p;
+    float* __restrict__ q;
+    float beta;
+    bool restart;
+    double acc;
+    __device__ __forceinline__ Pre pre(int r) const {
+        return restart ? Pre{z[r], 0.0f, 0.0f} : Pre{z[r], p[r], q[r]};
+    }
+    __device__ __forceinline__ void post(int r, const Pre& pr, float sum) {
+        const float pn = restart ? pr.z : fmaf(beta, pr.p, pr.z);
+        const float qn = restart ? sum : fmaf(beta, pr.q, sum);
+        p[r] = pn;
+        q[r] = qn;
+        acc = fma(static_cast<double>(pn), static_cast<double>(qn), acc);
+    }
+};
 
-template <int U, typename CI, bool COND>
-__global__ void __launch_bounds__(kT) mixed_spmv_kernel(SellArgs<float, CI> A, const float* __restrict__ z,
-                                                        DirectionBuffers P, float* __restrict__ q, MixedScalars* s,
+// The M1 epilogue of either form: q = A32 p (plain: the gathered vector is p) or
+// the recurrences above (fused: the gathered vector is z).
+template <bool FUSED>
+struct M1Op;
+template <>
+struct M1Op<false> {
+    using Type = MixedPqOp;
+    static __device__ __forceinline__ MixedPqOp make(const float* x, float* p, float* q, const MixedScalars*) {
+        (void)p;
+        return MixedPqOp{x, q, 0.0};
+    }
+};
+template <>
+struct M1Op<true> {
+    using Type = MixedDirOp;
+    static __device__ __forceinline__ MixedDirOp make(const float* z, float* p, float* q, const MixedScalars* s) {
+        const double beta = *reinterpret_cast<const volatile double*>(&s->beta);
+        return MixedDirOp{z, p, q, static_cast<float>(beta), beta == 0.0, 0.0};
+    }
+};
+
+template <int U, typename CI, bool COND, bool FUSED>
+__global__ void __launch_bounds__(kT) mixed_spmv_kernel(SellArgs<float, CI> A, const float* __restrict__ x,
+                                                        float* __restrict__ p, float* __restrict__ q, MixedScalars* s,
                                                         double* partials, unsigned* counter,
                                                         cudaGraphConditionalHandle loop) {
     if (*reinterpret_cast<volatile int*>(&s->done)) {
         if (blockIdx.x == 0 && threadIdx.x == 0) set_cond<COND>(loop, 0);
         return;
     }
-    MixedPqOp op = make_pq_op(z, P, q, s);
-    sell_rows_gather<U, float, float, CI>(A, op.dir, op);
+    auto op = M1Op<FUSED>::make(x, p, q, s);
+    sell_rows<U, float, float, CI>(A, x, op);
     double mine[1] = {op.acc}, tot[1];
     if (grid_reduce_last<1, kT>(mine, partials, counter, tot) && threadIdx.x == 0) {
         s->pq = tot[0];
@@ -235,17 +247,17 @@ __global__ void __launch_bounds__(kT) mixed_apply_dia_kernel(DiaArgs<float> A, c
     dia_rows4<ND>(A, x, op);
 }
 
-template <int ND, bool COND>
-__global__ void __launch_bounds__(kT) mixed_spmv_dia_kernel(DiaArgs<float> A, const float* __restrict__ z,
-                                                           DirectionBuffers P, float* __restrict__ q,
+template <int ND, bool COND, bool FUSED>
+__global__ void __launch_bounds__(kT) mixed_spmv_dia_kernel(DiaArgs<float> A, const float* __restrict__ x,
+                                                           float* __restrict__ p, float* __restrict__ q,
                                                            MixedScalars* s, double* partials, unsigned* counter,
                                                            cudaGraphConditionalHandle loop) {
     if (*reinterpret_cast<volatile int*>(&s->done)) {
         if (blockIdx.x == 0 && threadIdx.x == 0) set_cond<COND>(loop, 0);
         return;
     }
-    MixedPqOp op = make_pq_op(z, P, q, s);
-    dia_rows4_gather<ND>(A, op.dir, op);
+    auto op = M1Op<FUSED>::make(x, p, q, s);
+    dia_rows4<ND>(A, x, op);
     double mine[1] = {op.acc}, tot[1];
     if (grid_reduce_last<1, kT>(mine, partials, counter, tot) && threadIdx.x == 0) {
         s->pq = tot[0];
@@ -268,10 +280,10 @@ __global__ void __launch_bounds__(kTmaWarps * 32) mixed_apply_tma_kernel(SellArg
     sell_rows_tma<CI>(A, x, op, tma_smem, error);
 }
 
-template <typename CI, bool COND>
+template <typename CI, bool COND, bool FUSED>
 __global__ void __launch_bounds__(kTmaWarps * 32) mixed_spmv_tma_kernel(SellArgs<float, CI> A,
-                                                                        const float* __restrict__ z,
-                                                                        DirectionBuffers P, float* __restrict__ q,
+                                                                        const float* __restrict__ x,
+                                                                        float* __restrict__ p, float* __restrict__ q,
                                                                         MixedScalars* s, double* partials,
                                                                         unsigned* counter,
                                                                         cudaGraphConditionalHandle loop) {
@@ -280,8 +292,8 @@ __global__ void __launch_bounds__(kTmaWarps * 32) mixed_spmv_tma_kernel(SellArgs
         if (blockIdx.x == 0 && threadIdx.x == 0) set_cond<COND>(loop, 0);
         return;
     }
-    MixedPqOp op = make_pq_op(z, P, q, s);
-    sell_rows_tma_gather<CI>(A, op.dir, op, tma_smem, &s->tmaError);
+    auto op = M1Op<FUSED>::make(x, p, q, s);
+    sell_rows_tma<CI>(A, x, op, tma_smem, &s->tmaError);
     double mine[1] = {op.acc}, tot[1];
     if (grid_reduce_last<1, kTmaWarps * 32>(mine, partials, counter, tot) && threadIdx.x == 0) {
         s->pq = tot[0];
@@ -306,13 +318,12 @@ int allow_tma_smem(K* kernel, int bytes) {
     return CIECU_OK;
 }
 
-// M2: x32 += alpha p_k; r32 -= alpha q; z32 = D^-1 r32; rr, rz in FP64;
-// replacement decision.  Every block reads the iteration count (the p buffer)
-// before the last block increments it.
-template <bool COND>
+// M2: x32 += alpha p; r32 -= alpha q; rr, rz in FP64; replacement decision.  The
+// fused form also stores z = D^-1 r for the next M1.
+template <bool COND, bool FUSED>
 __global__ void __launch_bounds__(kT) mixed_update_kernel(long n, float* __restrict__ x, float* __restrict__ r,
-                                                          float* __restrict__ z, DirectionBuffers P,
-                                                          const float* __restrict__ q,
+                                                          float* __restrict__ z,
+                                                          const float* __restrict__ p, const float* __restrict__ q,
                                                           const float* __restrict__ dinv, MixedScalars* s,
                                                           double* partials, unsigned* counter,
                                                           cudaGraphConditionalHandle loop,
@@ -324,7 +335,6 @@ __global__ void __launch_bounds__(kT) mixed_update_kernel(long n, float* __restr
         }
         return;
     }
-    const float* __restrict__ p = (iteration_of(s) & 1) ? P.p1 : P.p0;
     const float alpha = static_cast<float>(s->alpha);
     const bool step = !s->restart;  // after an FP32 breakdown: no step (p may not be finite)
     double rr = 0.0, rz = 0.0;
@@ -345,7 +355,7 @@ __global__ void __launch_bounds__(kT) mixed_update_kernel(long n, float* __restr
             reinterpret_cast<float4*>(r)[j] = rj;
         }
         const float4 zj = make_float4(rj.x * dj.x, rj.y * dj.y, rj.z * dj.z, rj.w * dj.w);
-        reinterpret_cast<float4*>(z)[j] = zj;
+        if (FUSED) reinterpret_cast<float4*>(z)[j] = zj;
         rr = fma(double(rj.x), double(rj.x), rr); rr = fma(double(rj.y), double(rj.y), rr);
         rr = fma(double(rj.z), double(rj.z), rr); rr = fma(double(rj.w), double(rj.w), rr);
         rz = fma(double(rj.x), double(zj.x), rz); rz = fma(double(rj.y), double(zj.y), rz);
@@ -360,7 +370,7 @@ __global__ void __launch_bounds__(kT) mixed_update_kernel(long n, float* __restr
             r[i] = ri;
         }
         const float zi = ri * dinv[i];
-        z[i] = zi;
+        if (FUSED) z[i] = zi;
         rr = fma(double(ri), double(ri), rr);
         rz = fma(double(ri), double(zi), rz);
     }
@@ -414,7 +424,7 @@ struct ResidualOp {
     const double* __restrict__ b;
     const float* __restrict__ dinv;
     float* __restrict__ r32;
-    float* __restrict__ z32;
+    float* __restrict__ z32;           // the fused form keeps z = D^-1 r (or null)
     const double* __restrict__ sdiag;  // inner scaling (or null)
     double rr, rz;
     __device__ __forceinline__ Pre pre(int row) const { return Pre{b[row], dinv[row], sdiag ? sdiag[row] : 1.0}; }
@@ -423,14 +433,14 @@ struct ResidualOp {
         const float rf = static_cast<float>(sdiag ? ri * p.s : ri);
         const float zf = rf * p.d;
         r32[row] = rf;
-        z32[row] = zf;
+        if (z32) z32[row] = zf;
         rr = fma(ri, ri, rr);
         rz = fma(double(rf), double(zf), rz);
     }
 };
 
-// R2 (and set-up): r = b - A64 x64 in FP64; r32 = float(r), z32 = D^-1 r32;
-// ||r||^2 and r32^T z32 in FP64.  INIT: first residual of a solve.
+// R2 (and set-up): r = b - A64 x64 in FP64; r32 = float(r); ||r||^2 and r32^T z32
+// in FP64.  INIT: first residual of a solve.
 template <int KERNEL, bool INIT, bool COND>
 __global__ void __launch_bounds__(csr_threads<KERNEL>())
     mixed_residual_kernel(CsrArgs<double> A, const double* __restrict__ b, const double* __restrict__ x64,
@@ -499,6 +509,29 @@ __global__ void __launch_bounds__(csr_threads<KERNEL>())
     }
 }
 
+// M3: p = z + beta p, z = D^-1 r (FP32).
+__global__ void __launch_bounds__(kT) mixed_direction_kernel(long n, float* __restrict__ p, const float* __restrict__ r,
+                                                             const float* __restrict__ dinv, const MixedScalars* s) {
+    if (*reinterpret_cast<const volatile int*>(&s->done)) return;
+    const float beta = static_cast<float>(s->beta);
+    const long quads = n >> 2;
+    const long stride = static_cast<long>(gridDim.x) * kT;
+    for (long j = static_cast<long>(blockIdx.x) * kT + threadIdx.x; j < quads; j += stride) {
+        const float4 rj = reinterpret_cast<const float4*>(r)[j];
+        const float4 dj = reinterpret_cast<const float4*>(dinv)[j];
+        float4 pj = reinterpret_cast<const float4*>(p)[j];
+        pj.x = fmaf(beta, pj.x, rj.x * dj.x);
+        pj.y = fmaf(beta, pj.y, rj.y * dj.y);
+        pj.z = fmaf(beta, pj.z, rj.z * dj.z);
+        pj.w = fmaf(beta, pj.w, rj.w * dj.w);
+        reinterpret_cast<float4*>(p)[j] = pj;
+    }
+    if (blockIdx.x == 0 && threadIdx.x < (n & 3)) {
+        const long i = (quads << 2) + threadIdx.x;
+        p[i] = fmaf(beta, p[i], r[i] * dinv[i]);
+    }
+}
+
 __global__ void fill_f32_kernel(long n, float v, float* __restrict__ b) {
     const long stride = static_cast<long>(gridDim.x) * blockDim.x;
     for (long i = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) b[i] = v;
@@ -560,7 +593,8 @@ struct ciecu_mixed_s {
     ciecu::SellArgs<float, int> a32{};
     float* dinv32 = nullptr;
     double* sdiag = nullptr;  // sqrt(D^-1) when the inner system is scaled
-    float *x32 = nullptr, *r32 = nullptr, *z32 = nullptr, *p32 = nullptr, *p32b = nullptr, *q32 = nullptr;
+    float *x32 = nullptr, *r32 = nullptr, *p32 = nullptr, *q32 = nullptr;
+    float* z32 = nullptr;  // z = D^-1 r, kept only by the fused form (options.fuseDirection)
     double* x64 = nullptr;
     const double* b = nullptr;
     ciecu::MixedScalars* d_s = nullptr;
@@ -588,16 +622,18 @@ int with_unroll(int u, F&& f) {
 }
 
 // M1 with the autotuned variant: TMA pipeline (unroll == 0), the DIA copy
-// (unroll == kDiaInner) or U register groups.
-template <bool COND>
-int launch_inner_spmv(ciecu_mixed_s* M, cudaStream_t st, cudaGraphConditionalHandle loop) {
+// (unroll == kDiaInner) or U register groups.  FUSED gathers z (the direction
+// recurrences run in the epilogue), otherwise p.
+template <bool COND, bool FUSED>
+int launch_inner_spmv_form(ciecu_mixed_s* M, cudaStream_t st, cudaGraphConditionalHandle loop) {
     const long needA = (M->n + kT - 1) / kT;
+    const float* x = FUSED ? M->z32 : M->p32;
     if (M->unroll == kDiaInner) {
         CIECU_TRY(with_diagonals(M->dia.ndiag, [&](auto nd) -> int {
             constexpr int ND = decltype(nd)::value;
-            mixed_spmv_dia_kernel<ND, COND><<<fit_grid(mixed_spmv_dia_kernel<ND, COND>, kT, (needA + 3) / 4), kT, 0,
-                                              st>>>(M->dia, M->z32, DirectionBuffers{M->p32, M->p32b}, M->q32,
-                                                    M->d_s, M->d_partials, M->d_counter, loop);
+            auto* kernel = mixed_spmv_dia_kernel<ND, COND, FUSED>;
+            kernel<<<fit_grid(kernel, kT, (needA + 3) / 4), kT, 0, st>>>(M->dia, x, M->p32, M->q32, M->d_s,
+                                                                         M->d_partials, M->d_counter, loop);
             return CIECU_OK;
         }));
         CIECU_CHECK_LAUNCH("mixed_spmv_dia_kernel");
@@ -606,36 +642,36 @@ int launch_inner_spmv(ciecu_mixed_s* M, cudaStream_t st, cudaGraphConditionalHan
     if (M->unroll == 0) {
         if (M->idx16) {
             constexpr int smem = TmaShape<float, short>::SMEM;
-            mixed_spmv_tma_kernel<short, COND><<<fit_grid(mixed_spmv_tma_kernel<short, COND>, kTmaWarps * 32,
-                                                          (M->n + 511) / 512, smem),
-                                                 kTmaWarps * 32, smem, st>>>(M->a16, M->z32,
-                                                                             DirectionBuffers{M->p32, M->p32b},
-                                                                             M->q32, M->d_s, M->d_partials,
-                                                                             M->d_counter, loop);
+            auto* kernel = mixed_spmv_tma_kernel<short, COND, FUSED>;
+            kernel<<<fit_grid(kernel, kTmaWarps * 32, (M->n + 511) / 512, smem), kTmaWarps * 32, smem, st>>>(
+                M->a16, x, M->p32, M->q32, M->d_s, M->d_partials, M->d_counter, loop);
         } else {
             constexpr int smem = TmaShape<float, int>::SMEM;
-            mixed_spmv_tma_kernel<int, COND><<<fit_grid(mixed_spmv_tma_kernel<int, COND>, kTmaWarps * 32,
-                                                        (M->n + 511) / 512, smem),
-                                               kTmaWarps * 32, smem, st>>>(M->a32, M->z32,
-                                                                           DirectionBuffers{M->p32, M->p32b},
-                                                                           M->q32, M->d_s, M->d_partials,
-                                                                           M->d_counter, loop);
+            auto* kernel = mixed_spmv_tma_kernel<int, COND, FUSED>;
+            kernel<<<fit_grid(kernel, kTmaWarps * 32, (M->n + 511) / 512, smem), kTmaWarps * 32, smem, st>>>(
+                M->a32, x, M->p32, M->q32, M->d_s, M->d_partials, M->d_counter, loop);
         }
         CIECU_CHECK_LAUNCH("mixed_spmv_tma_kernel");
         return CIECU_OK;
     }
     return with_unroll(M->unroll, [&](auto uu) -> int {
         constexpr int U = decltype(uu)::value;
-        if (M->idx16)
-            mixed_spmv_kernel<U, short, COND><<<fit_grid(mixed_spmv_kernel<U, short, COND>, kT, needA), kT, 0, st>>>(
-                M->a16, M->z32, DirectionBuffers{M->p32, M->p32b}, M->q32, M->d_s, M->d_partials, M->d_counter,
-                loop);
-        else
-            mixed_spmv_kernel<U, int, COND><<<fit_grid(mixed_spmv_kernel<U, int, COND>, kT, needA), kT, 0, st>>>(
-                M->a32, M->z32, DirectionBuffers{M->p32, M->p32b}, M->q32, M->d_s, M->d_partials, M->d_counter,
-                loop);
+        if (M->idx16) {
+            auto* kernel = mixed_spmv_kernel<U, short, COND, FUSED>;
+            kernel<<<fit_grid(kernel, kT, needA), kT, 0, st>>>(M->a16, x, M->p32, M->q32, M->d_s, M->d_partials,
+                                                               M->d_counter, loop);
+        } else {
+            auto* kernel = mixed_spmv_kernel<U, int, COND, FUSED>;
+            kernel<<<fit_grid(kernel, kT, needA), kT, 0, st>>>(M->a32, x, M->p32, M->q32, M->d_s, M->d_partials,
+                                                               M->d_counter, loop);
+        }
         return CIECU_OK;
     });
+}
+
+template <bool COND>
+int launch_inner_spmv(ciecu_mixed_s* M, cudaStream_t st, cudaGraphConditionalHandle loop) {
+    return M->z32 ? launch_inner_spmv_form<COND, true>(M, st, loop) : launch_inner_spmv_form<COND, false>(M, st, loop);
 }
 
 // One inner iteration.  With conditional nodes (useCond) the refinement pair
@@ -650,9 +686,14 @@ int launch_inner(ciecu_mixed_s* M, cudaStream_t st, cudaGraph_t root, cudaGraphC
     cudaGraphConditionalHandle refine = 0;
     if (useCond) CIECU_CUDA(cudaGraphConditionalHandleCreate(&refine, root, 0, cudaGraphCondAssignDefault));
     CIECU_TRY(launch_inner_spmv<COND>(M, st, loop));
-    mixed_update_kernel<COND><<<fit_grid(mixed_update_kernel<COND>, kT, needV), kT, 0, st>>>(
-        M->n, M->x32, M->r32, M->z32, DirectionBuffers{M->p32, M->p32b}, M->q32, M->dinv32, M->d_s, M->d_partials,
-        M->d_counter, loop, refine);
+    if (M->z32)
+        mixed_update_kernel<COND, true><<<fit_grid(mixed_update_kernel<COND, true>, kT, needV), kT, 0, st>>>(
+            M->n, M->x32, M->r32, M->z32, M->p32, M->q32, M->dinv32, M->d_s, M->d_partials, M->d_counter, loop,
+            refine);
+    else
+        mixed_update_kernel<COND, false><<<fit_grid(mixed_update_kernel<COND, false>, kT, needV), kT, 0, st>>>(
+            M->n, M->x32, M->r32, nullptr, M->p32, M->q32, M->dinv32, M->d_s, M->d_partials, M->d_counter, loop,
+            refine);
     auto refinement = [&](cudaStream_t s2) -> int {
         mixed_fold_kernel<<<fit_grid(mixed_fold_kernel, kT, needA), kT, 0, s2>>>(M->n, M->x64, M->x32, M->sdiag,
                                                                                 M->d_s);
@@ -672,6 +713,9 @@ int launch_inner(ciecu_mixed_s* M, cudaStream_t st, cudaGraph_t root, cudaGraphC
         CIECU_TRY(capture_if(st, M->side, refine, refinement));
     else
         CIECU_TRY(refinement(st));
+    if (!M->z32)
+        mixed_direction_kernel<<<fit_grid(mixed_direction_kernel, kT, needV), kT, 0, st>>>(M->n, M->p32, M->r32,
+                                                                                           M->dinv32, M->d_s);
     CIECU_CHECK_LAUNCH("mixed inner iteration");
     return CIECU_OK;
 }
@@ -832,8 +876,9 @@ int ciecu_mixed_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_sta
     const size_t n = static_cast<size_t>(std::max<long>(M->n, 1)) + 4;
     M->nslices = static_cast<int>((M->n + 31) / 32);
     cudaError_t e = cudaSuccess;
-    for (float** v : {&M->dinv32, &M->x32, &M->r32, &M->z32, &M->p32, &M->p32b, &M->q32})
+    for (float** v : {&M->dinv32, &M->x32, &M->r32, &M->p32, &M->q32})
         if (e == cudaSuccess) e = cudaMalloc(v, sizeof(float) * n);
+    if (e == cudaSuccess && options.fuseDirection) e = cudaMalloc(&M->z32, sizeof(float) * n);
     if (e == cudaSuccess) e = cudaMalloc(&M->x64, sizeof(double) * n);
     if (e == cudaSuccess) e = cudaMalloc(&M->d_s, sizeof(MixedScalars));
     if (e == cudaSuccess) e = cudaMallocHost(&M->h_s, sizeof(MixedScalars));
@@ -905,10 +950,15 @@ int ciecu_mixed_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_sta
         }
     }
     {
-        int st2 = allow_tma_smem(mixed_spmv_tma_kernel<short, false>, TmaShape<float, short>::SMEM);
-        if (st2 == CIECU_OK) st2 = allow_tma_smem(mixed_spmv_tma_kernel<short, true>, TmaShape<float, short>::SMEM);
-        if (st2 == CIECU_OK) st2 = allow_tma_smem(mixed_spmv_tma_kernel<int, false>, TmaShape<float, int>::SMEM);
-        if (st2 == CIECU_OK) st2 = allow_tma_smem(mixed_spmv_tma_kernel<int, true>, TmaShape<float, int>::SMEM);
+        constexpr int s16 = TmaShape<float, short>::SMEM, s32 = TmaShape<float, int>::SMEM;
+        int st2 = allow_tma_smem(mixed_spmv_tma_kernel<short, false, false>, s16);
+        if (st2 == CIECU_OK) st2 = allow_tma_smem(mixed_spmv_tma_kernel<short, true, false>, s16);
+        if (st2 == CIECU_OK) st2 = allow_tma_smem(mixed_spmv_tma_kernel<short, false, true>, s16);
+        if (st2 == CIECU_OK) st2 = allow_tma_smem(mixed_spmv_tma_kernel<short, true, true>, s16);
+        if (st2 == CIECU_OK) st2 = allow_tma_smem(mixed_spmv_tma_kernel<int, false, false>, s32);
+        if (st2 == CIECU_OK) st2 = allow_tma_smem(mixed_spmv_tma_kernel<int, true, false>, s32);
+        if (st2 == CIECU_OK) st2 = allow_tma_smem(mixed_spmv_tma_kernel<int, false, true>, s32);
+        if (st2 == CIECU_OK) st2 = allow_tma_smem(mixed_spmv_tma_kernel<int, true, true>, s32);
         if (st2 == CIECU_OK) st2 = allow_tma_smem(mixed_apply_tma_kernel<short>, TmaShape<float, short>::SMEM);
         if (st2 == CIECU_OK) st2 = allow_tma_smem(mixed_apply_tma_kernel<int>, TmaShape<float, int>::SMEM);
         if (st2 != CIECU_OK) {
@@ -919,17 +969,18 @@ int ciecu_mixed_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_sta
     if (cached != 1000) M->unroll = cached;
     // Autotune the group unroll of the inner SpMV on the solver's own matrix,
     // timing the fused kernel the iteration runs (q = A32 p with the p^T q
-    // reduction) on scratch vectors.
+    // reduction) on scratch vectors p32 = 0 -> q32.
     if (options.innerKernel != 0)
         M->unroll = options.innerKernel == kDiaInner ? kDiaInner : (options.innerKernel < 0 ? 0 : options.innerKernel);
     if (M->n > 0 && options.innerKernel == 0 && cached == 1000) {
-        // z = D^-1 > 0 and beta = 0, so p = z: p^T A p > 0 for an SPD matrix, and no
-        // timed launch trips the breakdown flag (which would make the later
-        // candidates return at once).
+        // p = D^-1 > 0: p^T A p > 0 for an SPD matrix, so no timed launch trips the
+        // breakdown flag (which would make the later candidates return at once).
         MixedScalars scratch{};
         scratch.rz = 1.0;
         e = cudaMemcpyAsync(M->d_s, &scratch, sizeof(MixedScalars), cudaMemcpyHostToDevice, st);
         if (e == cudaSuccess)
+            e = cudaMemcpyAsync(M->p32, M->dinv32, sizeof(float) * M->n, cudaMemcpyDeviceToDevice, st);
+        if (e == cudaSuccess && M->z32)  // the fused form gathers z (beta = 0: p = z, q = A z)
             e = cudaMemcpyAsync(M->z32, M->dinv32, sizeof(float) * M->n, cudaMemcpyDeviceToDevice, st);
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         if (e == cudaSuccess) e = cudaEventCreate(&e0);
@@ -991,10 +1042,9 @@ int ciecu_mixed_destroy(ciecu_mixed M) {
     cudaFree(M->sdiag);
     cudaFree(M->x32);
     cudaFree(M->r32);
-    cudaFree(M->z32);
     cudaFree(M->p32);
-    cudaFree(M->p32b);
     cudaFree(M->q32);
+    cudaFree(M->z32);
     cudaFree(M->x64);
     cudaFree(M->d_s);
     if (M->h_s) cudaFreeHost(M->h_s);
@@ -1107,6 +1157,7 @@ int ciecu_mixed_product(ciecu_mixed M, double inScale, const double* d_in, doubl
         *M->h_s = init;
         CIECU_CUDA(cudaMemcpyAsync(M->d_s, M->h_s, sizeof(MixedScalars), cudaMemcpyHostToDevice, st));
         CIECU_CUDA(cudaMemsetAsync(M->x32, 0, sizeof(float) * n, st));
+        CIECU_CUDA(cudaMemsetAsync(M->p32, 0, sizeof(float) * n, st));
         const int needR = csr_grid(A, A->kernel);
         CIECU_TRY(with_schedule(A->kernel, [&](auto k) -> int {
             constexpr int K = decltype(k)::value;
@@ -1117,6 +1168,11 @@ int ciecu_mixed_product(ciecu_mixed M, double inScale, const double* d_in, doubl
                 M->d_counter, 0);
             return CIECU_OK;
         }));
+        if (!M->z32) {  // the fused form's first M1 forms p = z from the z the residual kernel stored
+            mixed_direction_kernel<<<fit_grid(mixed_direction_kernel, kT, ((n + 3) / 4 + kT - 1) / kT), kT, 0, st>>>(
+                n, M->p32, M->r32, M->dinv32, M->d_s);
+            count_launch();
+        }
         count_launch();
         CIECU_CHECK_LAUNCH("mixed set-up");
         CIECU_TRY(build_mixed_graph(M));
@@ -1133,8 +1189,9 @@ int ciecu_mixed_product(ciecu_mixed M, double inScale, const double* d_in, doubl
             CIECU_CUDA(cudaGraphLaunch(M->graph, st));
             CIECU_CUDA(cudaMemcpyAsync(M->h_s, M->d_s, sizeof(MixedScalars), cudaMemcpyDeviceToHost, st));
             CIECU_CUDA(cudaStreamSynchronize(st));
-            count_launch(M->deviceLoop ? 2LL * (M->h_s->iter - before) + 2LL * (M->h_s->refinements - refBefore)
-                                       : 4LL * M->chunk);
+            const long long perIteration = M->z32 ? 2 : 3;
+            count_launch(M->deviceLoop ? perIteration * (M->h_s->iter - before) + 2LL * (M->h_s->refinements - refBefore)
+                                       : (perIteration + 2) * M->chunk);
             if (M->h_s->done) break;
         }
         const MixedScalars& s = *M->h_s;

@@ -37,14 +37,28 @@ struct ColumnScalars {
     int done;       // 0 running, 1 converged, 2 iteration limit, 3 breakdown
     int errorKind;  // 1: r^T z <= 0 at start, 2: p^T A p <= 0
     long long errorIter;
+    // FP32-refined form: reliable-update state of the column
+    double maxrx, maxrr;  // largest FP32 residual norm since the last x / r replacement
+    double rzPending;     // r^T z of the FP32 recursion when a replacement is due
+    long long refinements;
+    int pending;  // a replacement is due at the end of this iteration
+    int updateX;  // ... and it folds the FP32 solution into the FP64 one
+    int restart;  // an FP32 breakdown: no step, direction restarted after the replacement
+    int breakdowns;
 };
 
 struct MultiGlobal {
     unsigned finished;
-    unsigned pad;
+    unsigned anyPending;  // FP32-refined form: some column requested a replacement
     long long chunkIter, chunkLimit, maxIter;
     double absTol, relTol;
+    double delta;  // FP32-refined form: replacement trigger
+    long long replacements;  // FP32-refined form: residual recomputations (launches of T)
 };
+
+// FP32 breakdowns (p^T A p <= 0 in single precision) a column may recover from
+// by a replacement with a restarted direction before it reports the breakdown.
+constexpr int kMaxColumnBreakdowns = 64;
 
 template <bool COND>
 __device__ __forceinline__ void set_loop(cudaGraphConditionalHandle cond, unsigned value) {
@@ -121,9 +135,10 @@ __device__ __forceinline__ void load_entry(const Entry* e, double& a, int& col) 
 }
 
 // FULL: k == KP, so every lane is active and the row stride of X is the
-// compile-time KP (the gather address is a shift and an add).
-template <int KP, bool FULL, typename Op>
-__device__ __forceinline__ void multi_rows(const CsrArgs<double>& A, int k, const double* __restrict__ X, Op& op) {
+// compile-time KP (the gather address is a shift and an add).  V: stored value
+// type (staged as a double, exactly), T: vector and accumulation type.
+template <int KP, bool FULL, typename V, typename T, typename Op>
+__device__ __forceinline__ void multi_rows(const CsrArgs<V>& A, int k, const T* __restrict__ X, Op& op) {
     __shared__ Entry s_e[kStreamTile];  // one 16-byte broadcast read per entry
     constexpr int RPW = 32 / KP;
     constexpr int UNROLL = 8;
@@ -131,30 +146,32 @@ __device__ __forceinline__ void multi_rows(const CsrArgs<double>& A, int k, cons
     const int slot = lane / KP, c = lane % KP;
     const bool active = FULL || c < k;
     const long ld = FULL ? KP : k;
-    const double* __restrict__ xc = X + c;
+    const T* __restrict__ xc = X + c;
     for (int b = blockIdx.x; b < A.nblocks; b += gridDim.x) {
         const int r0 = A.blocks[b], r1 = A.blocks[b + 1];
         const int e0 = A.rowptr[r0], e1 = A.rowptr[r1];
         const bool staged = e1 - e0 <= kStreamTile;
         if (staged) {
             for (int j = threadIdx.x; j < e1 - e0; j += kT)
-                s_e[j] = Entry{stream_ld(A.val + e0 + j), stream_ld(A.col + e0 + j), 0};
+                s_e[j] = Entry{static_cast<double>(stream_ld(A.val + e0 + j)), stream_ld(A.col + e0 + j), 0};
             __syncthreads();
         }
         for (int rbase = r0 + warp * RPW; rbase < r1; rbase += kWarps * RPW) {
             const int row = rbase + slot;
             if (row >= r1) continue;
             const int k0 = A.rowptr[row] - e0, k1 = A.rowptr[row + 1] - e0;
-            double acc = 0.0;
+            T acc = 0;
             if (staged) {
                 int j = k0;
                 for (; j + UNROLL <= k1; j += UNROLL) {
-                    double av[UNROLL], pv[UNROLL];
+                    T av[UNROLL], pv[UNROLL];
 #pragma unroll
                     for (int u = 0; u < UNROLL; ++u) {
+                        double a;
                         int col;
-                        load_entry(s_e + j + u, av[u], col);
-                        pv[u] = active ? __ldg(xc + static_cast<long>(col) * ld) : 0.0;
+                        load_entry(s_e + j + u, a, col);
+                        av[u] = static_cast<T>(a);
+                        pv[u] = active ? __ldg(xc + static_cast<long>(col) * ld) : T(0);
                     }
 #pragma unroll
                     for (int u = 0; u < UNROLL; ++u) acc = fma(av[u], pv[u], acc);
@@ -163,11 +180,12 @@ __device__ __forceinline__ void multi_rows(const CsrArgs<double>& A, int k, cons
                     double a;
                     int col;
                     load_entry(s_e + j, a, col);
-                    acc = fma(a, active ? __ldg(xc + static_cast<long>(col) * ld) : 0.0, acc);
+                    acc = fma(static_cast<T>(a), active ? __ldg(xc + static_cast<long>(col) * ld) : T(0), acc);
                 }
             } else {
                 for (int j = e0 + k0; j < e0 + k1; ++j)
-                    acc = fma(A.val[j], active ? __ldg(xc + static_cast<long>(A.col[j]) * ld) : 0.0, acc);
+                    acc = fma(static_cast<T>(A.val[j]), active ? __ldg(xc + static_cast<long>(A.col[j]) * ld) : T(0),
+                              acc);
             }
             if (active) op(row, c, acc);
         }
@@ -180,25 +198,24 @@ __device__ __forceinline__ void multi_rows(const CsrArgs<double>& A, int k, cons
 // and X[row + off[d]][c] (k consecutive doubles, coalesced).  No staging, no
 // column indices; the diagonals run in ascending order, i.e. in the CSR column
 // order, so the sums equal those of multi_rows.
-template <int KP, bool FULL, typename Op>
-__device__ __forceinline__ void multi_dia_rows(const DiaArgs<double>& D, int k, const double* __restrict__ X,
-                                               Op& op) {
+template <int KP, bool FULL, typename V, typename T, typename Op>
+__device__ __forceinline__ void multi_dia_rows(const DiaArgs<V>& D, int k, const T* __restrict__ X, Op& op) {
     constexpr int RPW = 32 / KP;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int slot = lane / KP, c = lane % KP;
     const bool active = FULL || c < k;
     const long ld = FULL ? KP : k;
-    const double* __restrict__ xc = X + c;
+    const T* __restrict__ xc = X + c;
     const long stride = static_cast<long>(gridDim.x) * kWarps * RPW;
     for (long row = (static_cast<long>(blockIdx.x) * kWarps + warp) * RPW + slot; row < D.nrows; row += stride) {
-        double acc = 0.0;
+        T acc = 0;
 #pragma unroll 9
         for (int d = 0; d < D.ndiag; ++d) {
             const long col = row + D.off[d];
-            const double a = stream_ld(D.val + static_cast<long>(d) * D.ld + row);
-            const double xv =
+            const T a = static_cast<T>(stream_ld(D.val + static_cast<long>(d) * D.ld + row));
+            const T xv =
                 active && static_cast<unsigned long>(col) < static_cast<unsigned long>(D.nrows) ? __ldg(xc + col * ld)
-                                                                                                 : 0.0;
+                                                                                                 : T(0);
             acc = fma(a, xv, acc);
         }
         if (active) op(row, c, acc);
@@ -413,6 +430,314 @@ __global__ void __launch_bounds__(kT) multi_direction_kernel(long n, int k, doub
     }
 }
 
+// ---- FP32-refined form: FP32 inner iterations, FP64 reliable updates ---------
+//
+// Per column the iteration of the mixed-precision solver: K1 Q32 = A32 P32 and
+// p^T q (FP64 sums); K2 X32 += alpha P32, R32 -= alpha Q32, the FP32 recursion's
+// r^T r and r^T z in FP64 and the replacement decision (the FP32 residual norm
+// fell below delta times its maximum since the last replacement, or below the
+// stopping tolerance, or the iteration limit); when any column asks, F folds
+// X32 into the FP64 solution and T recomputes R = B - A64 X64 in FP64 for those
+// columns, stores float(R) and applies the FP64 stopping test; K3 P32 = D^-1 R32
+// + beta P32.  Columns that are done are left unchanged.
+
+struct PqOp32 {
+    const float* __restrict__ p;
+    float* __restrict__ q;
+    int k;
+    double acc;
+    __device__ __forceinline__ void operator()(long row, int c, float sum) {
+        q[row * k + c] = sum;
+        acc = fma(static_cast<double>(p[row * k + c]), static_cast<double>(sum), acc);
+    }
+};
+
+__device__ __forceinline__ void column_pq(ColumnScalars& s, double pq, MultiGlobal* g) {
+    if (s.done) return;
+    s.pq = pq;
+    if (!(0.0 < pq)) {  // FP32 breakdown: no step, replacement with a restarted direction
+        s.alpha = 0.0;
+        s.restart = 1;
+        s.breakdowns += 1;
+        if (s.breakdowns > kMaxColumnBreakdowns) {
+            s.done = 3;
+            s.errorKind = 2;
+            s.errorIter = s.iter;
+            atomicAdd(&g->finished, 1u);
+        }
+    } else {
+        s.alpha = s.rz / pq;
+    }
+}
+
+template <int KP, bool FULL, bool COND>
+__global__ void __launch_bounds__(kT) multi_spmv32_kernel(CsrArgs<float> A, int k, const float* __restrict__ P,
+                                                          float* __restrict__ Q, ColumnScalars* S, MultiGlobal* g,
+                                                          double* partials, unsigned* counter,
+                                                          cudaGraphConditionalHandle cond) {
+    if (*reinterpret_cast<volatile unsigned*>(&g->finished) >= static_cast<unsigned>(k)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) set_loop<COND>(cond, 0);
+        return;
+    }
+    PqOp32 op{P, Q, k, 0.0};
+    multi_rows<KP, FULL>(A, k, P, op);
+    double mine[1] = {op.acc}, tot[1];
+    if (column_reduce_last<KP, 1>(mine, k, partials, counter, tot) && threadIdx.x < k)
+        column_pq(S[threadIdx.x], tot[0], g);
+}
+
+template <int KP, bool FULL, bool COND>
+__global__ void __launch_bounds__(kT) multi_spmv32_dia_kernel(DiaArgs<float> D, int k, const float* __restrict__ P,
+                                                              float* __restrict__ Q, ColumnScalars* S,
+                                                              MultiGlobal* g, double* partials, unsigned* counter,
+                                                              cudaGraphConditionalHandle cond) {
+    if (*reinterpret_cast<volatile unsigned*>(&g->finished) >= static_cast<unsigned>(k)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) set_loop<COND>(cond, 0);
+        return;
+    }
+    PqOp32 op{P, Q, k, 0.0};
+    multi_dia_rows<KP, FULL>(D, k, P, op);
+    double mine[1] = {op.acc}, tot[1];
+    if (column_reduce_last<KP, 1>(mine, k, partials, counter, tot) && threadIdx.x < k)
+        column_pq(S[threadIdx.x], tot[0], g);
+}
+
+// K2 of the refined form.  IF: the handle of the replacement (set when any column
+// asks for one).
+template <int KP, bool COND>
+__global__ void __launch_bounds__(kT) multi_update32_kernel(long n, int k, float* __restrict__ X,
+                                                            float* __restrict__ R, const float* __restrict__ P,
+                                                            const float* __restrict__ Q,
+                                                            const float* __restrict__ dinv, ColumnScalars* S,
+                                                            MultiGlobal* g, double* partials, unsigned* counter,
+                                                            cudaGraphConditionalHandle replace) {
+    if (*reinterpret_cast<volatile unsigned*>(&g->finished) >= static_cast<unsigned>(k)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) set_loop<COND>(replace, 0);
+        return;
+    }
+    constexpr int RPW = 32 / KP;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int slot = lane / KP, c = lane % KP;
+    double rr = 0.0, rz = 0.0;
+    if (c < k && !S[c].done) {
+        const bool step = !S[c].restart;
+        const float alpha = static_cast<float>(S[c].alpha), malpha = -alpha;
+        const long stride = static_cast<long>(gridDim.x) * kWarps * RPW;
+#pragma unroll 4
+        for (long i = (static_cast<long>(blockIdx.x) * kWarps + warp) * RPW + slot; i < n; i += stride) {
+            const long e = i * k + c;
+            float ri = R[e];
+            if (step) {
+                X[e] = fmaf(alpha, P[e], X[e]);
+                ri = fmaf(malpha, Q[e], ri);
+                R[e] = ri;
+            }
+            rr = fma(static_cast<double>(ri), static_cast<double>(ri), rr);
+            rz = fma(static_cast<double>(ri), static_cast<double>(ri * dinv[i]), rz);
+        }
+    }
+    double mine[2] = {rr, rz}, tot[2];
+    __shared__ unsigned s_any;
+    if (threadIdx.x == 0) s_any = 0u;
+    const bool last = column_reduce_last<KP, 2>(mine, k, partials, counter, tot);
+    if (!last) return;
+    __syncthreads();
+    if (threadIdx.x < k) {
+        ColumnScalars& s = S[threadIdx.x];
+        if (!s.done) {
+            const double rnorm = sqrt(tot[0]);
+            s.iter += 1;
+            if (rnorm > s.maxrx) s.maxrx = rnorm;
+            if (rnorm > s.maxrr) s.maxrr = rnorm;
+            const bool updateX = rnorm < g->delta * s.maxrx;
+            const bool update = updateX || rnorm < g->delta * s.maxrr || rnorm < g->relTol * s.r0 ||
+                                rnorm < g->absTol || s.iter >= g->maxIter || s.restart;
+            s.updateX = updateX ? 1 : 0;
+            if (update) {
+                s.pending = 1;
+                s.rzPending = tot[1];
+                atomicOr(&s_any, 1u);
+            } else {
+                s.beta = tot[1] / s.rz;
+                s.rz = tot[1];
+            }
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        g->anyPending = s_any;
+        set_loop<COND>(replace, s_any);
+    }
+}
+
+// F: X64 += X32, X32 = 0 for the columns with a replacement due.
+template <int KP>
+__global__ void __launch_bounds__(kT) multi_fold32_kernel(long n, int k, double* __restrict__ X64,
+                                                          float* __restrict__ X32, const ColumnScalars* S,
+                                                          const MultiGlobal* g) {
+    if (!*reinterpret_cast<const volatile unsigned*>(&g->anyPending)) return;
+    constexpr int RPW = 32 / KP;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int slot = lane / KP, c = lane % KP;
+    if (c >= k || !S[c].pending) return;
+    const long stride = static_cast<long>(gridDim.x) * kWarps * RPW;
+#pragma unroll 4
+    for (long i = (static_cast<long>(blockIdx.x) * kWarps + warp) * RPW + slot; i < n; i += stride) {
+        const long e = i * k + c;
+        X64[e] += static_cast<double>(X32[e]);
+        X32[e] = 0.0f;
+    }
+}
+
+// T (and the set-up, INIT): R = B - A64 X64 in FP64 for the columns with a
+// replacement due (every column at the set-up); R32 = float(R), ||R|| in FP64,
+// r32^T z32; the FP64 stopping test and the direction's beta.
+struct TrueResidualOp {
+    const double* __restrict__ b;
+    const float* __restrict__ dinv;
+    float* __restrict__ r32;
+    const ColumnScalars* S;
+    int k;
+    bool init;
+    double rr, rz;
+    __device__ __forceinline__ void operator()(long row, int c, double sum) {
+        if (!init && !S[c].pending) return;
+        const double ri = b[row * k + c] - sum;
+        const float rf = static_cast<float>(ri);
+        r32[row * k + c] = rf;
+        rr = fma(ri, ri, rr);
+        rz = fma(static_cast<double>(rf), static_cast<double>(rf * dinv[row]), rz);
+    }
+};
+
+template <bool INIT>
+__device__ __forceinline__ void column_replace(ColumnScalars& s, const double (&tot)[2], MultiGlobal* g) {
+    const double rnorm = sqrt(tot[0]);
+    if (INIT) {
+        s = ColumnScalars{};
+        s.r0 = rnorm;
+        s.absres = rnorm;
+        s.relres = 1.0;
+        s.maxrx = s.maxrr = rnorm;
+        s.beta = 0.0;
+        s.rz = tot[1];
+        if (float_less(s.absres, g->absTol) || float_less(s.relres, g->relTol)) {
+            s.done = 1;
+        } else if (!(0.0 < tot[1])) {
+            s.done = 3;
+            s.errorKind = 1;
+        } else if (g->maxIter <= 0) {
+            s.done = 2;
+        }
+        if (s.done) atomicAdd(&g->finished, 1u);
+        return;
+    }
+    if (s.done || !s.pending) return;
+    s.pending = 0;
+    s.refinements += 1;
+    s.rr = tot[0];
+    s.absres = rnorm;
+    s.relres = rnorm / s.r0;
+    if (float_less(s.absres, g->absTol) || float_less(s.relres, g->relTol)) {
+        s.done = 1;
+    } else if (s.iter >= g->maxIter) {
+        s.done = 2;
+    } else if (!(0.0 < tot[1])) {
+        s.done = 3;
+        s.errorKind = 1;
+        s.errorIter = s.iter;
+    } else {
+        s.maxrr = rnorm;
+        if (s.updateX) s.maxrx = rnorm;
+        s.beta = s.restart ? 0.0 : tot[1] / s.rz;  // after an FP32 breakdown: p = z
+        s.rz = tot[1];
+    }
+    s.restart = 0;
+    if (s.done) atomicAdd(&g->finished, 1u);
+}
+
+template <int KP, bool FULL, bool INIT>
+__global__ void __launch_bounds__(kT) multi_true_residual_kernel(CsrArgs<double> A, int k,
+                                                                 const double* __restrict__ X,
+                                                                 const double* __restrict__ B,
+                                                                 const float* __restrict__ dinv,
+                                                                 float* __restrict__ R32, ColumnScalars* S,
+                                                                 MultiGlobal* g, double* partials,
+                                                                 unsigned* counter) {
+    if (!INIT && !*reinterpret_cast<volatile unsigned*>(&g->anyPending)) return;
+    TrueResidualOp op{B, dinv, R32, S, k, INIT, 0.0, 0.0};
+    multi_rows<KP, FULL>(A, k, X, op);
+    double mine[2] = {op.rr, op.rz}, tot[2];
+    if (column_reduce_last<KP, 2>(mine, k, partials, counter, tot)) {
+        if (threadIdx.x < k) column_replace<INIT>(S[threadIdx.x], tot, g);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            g->anyPending = 0u;
+            if (!INIT) g->replacements += 1;
+        }
+    }
+}
+
+template <int KP, bool FULL, bool INIT>
+__global__ void __launch_bounds__(kT) multi_true_residual_dia_kernel(DiaArgs<double> D, int k,
+                                                                     const double* __restrict__ X,
+                                                                     const double* __restrict__ B,
+                                                                     const float* __restrict__ dinv,
+                                                                     float* __restrict__ R32, ColumnScalars* S,
+                                                                     MultiGlobal* g, double* partials,
+                                                                     unsigned* counter) {
+    if (!INIT && !*reinterpret_cast<volatile unsigned*>(&g->anyPending)) return;
+    TrueResidualOp op{B, dinv, R32, S, k, INIT, 0.0, 0.0};
+    multi_dia_rows<KP, FULL>(D, k, X, op);
+    double mine[2] = {op.rr, op.rz}, tot[2];
+    if (column_reduce_last<KP, 2>(mine, k, partials, counter, tot)) {
+        if (threadIdx.x < k) column_replace<INIT>(S[threadIdx.x], tot, g);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            g->anyPending = 0u;
+            if (!INIT) g->replacements += 1;
+        }
+    }
+}
+
+// K3 of the refined form: P32 = D^-1 R32 + beta P32 per running column; ends the
+// loop when all are done.
+template <int KP, bool COND>
+__global__ void __launch_bounds__(kT) multi_direction32_kernel(long n, int k, float* __restrict__ P,
+                                                               const float* __restrict__ R,
+                                                               const float* __restrict__ dinv,
+                                                               const ColumnScalars* S, MultiGlobal* g,
+                                                               cudaGraphConditionalHandle cond) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        g->chunkIter += 1;
+        const bool more = *reinterpret_cast<volatile unsigned*>(&g->finished) < static_cast<unsigned>(k);
+        set_loop<COND>(cond, (more && g->chunkIter < g->chunkLimit) ? 1u : 0u);
+    }
+    constexpr int RPW = 32 / KP;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int slot = lane / KP, c = lane % KP;
+    if (c >= k || S[c].done) return;
+    const float beta = static_cast<float>(S[c].beta);
+    const long stride = static_cast<long>(gridDim.x) * kWarps * RPW;
+    if (beta == 0.0f) {  // a new direction: the old one may not be finite after a breakdown
+#pragma unroll 4
+        for (long i = (static_cast<long>(blockIdx.x) * kWarps + warp) * RPW + slot; i < n; i += stride)
+            P[i * k + c] = R[i * k + c] * dinv[i];
+        return;
+    }
+#pragma unroll 4
+    for (long i = (static_cast<long>(blockIdx.x) * kWarps + warp) * RPW + slot; i < n; i += stride) {
+        const long e = i * k + c;
+        P[e] = fmaf(beta, P[e], R[e] * dinv[i]);
+    }
+}
+
+__global__ void multi_to_f32_kernel(long n, const double* __restrict__ a, float* __restrict__ b) {
+    const long stride = static_cast<long>(gridDim.x) * blockDim.x;
+    for (long i = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+        b[i] = static_cast<float>(a[i]);
+}
+
 __global__ void multi_output_kernel(long count, double inScale, double outScale, const double* __restrict__ x,
                                     double* __restrict__ out) {
     const long stride = static_cast<long>(gridDim.x) * blockDim.x;
@@ -470,6 +795,19 @@ struct ciecu_multi_s {
     int gridD = 1;
     double* diaBuf = nullptr;
     ciecu::DiaArgs<double> dia{};
+    // FP32-refined form (refineDelta > 0): FP32 copies of the matrix (in the
+    // format of the FP64 solve) and of D^-1, FP32 blocks, its own graph
+    double refineDelta = 0.0;
+    float *x32 = nullptr, *r32 = nullptr, *p32 = nullptr, *q32 = nullptr, *dinv32 = nullptr;
+    float* val32 = nullptr;  // CSR values
+    float* dia32 = nullptr;  // DIA copy
+    ciecu::DiaArgs<float> diaF{};
+    int grid32 = 1, grid32D = 1;
+    cudaGraphExec_t graph32 = nullptr;
+    bool deviceLoop32 = false;
+    cudaStream_t side = nullptr;  // captures the IF body of the replacement
+    const double* graphB = nullptr;  // right-hand sides the refined graph reads
+    std::vector<ciecu::ColumnScalars> last;  // column state of the last solve
 };
 
 namespace ciecu {
@@ -609,6 +947,220 @@ int build_multi_graph(ciecu_multi_s* M) {
     return CIECU_OK;
 }
 
+// T of the refined form (INIT: the set-up residual of every column) in the
+// format of the FP64 solve.
+template <bool INIT>
+int launch_true_residual(ciecu_multi_s* M, cudaStream_t st, const double* B) {
+    return with_group(M->kp, [&](auto kk) -> int {
+        constexpr int KP = decltype(kk)::value;
+        if (M->useDia && M->k == KP)
+            multi_true_residual_dia_kernel<KP, true, INIT><<<M->gridD, kT, 0, st>>>(
+                M->dia, M->k, M->x, B, M->dinv32, M->r32, M->d_s, M->d_g, M->d_partials, M->d_counter);
+        else if (M->useDia)
+            multi_true_residual_dia_kernel<KP, false, INIT><<<M->gridD, kT, 0, st>>>(
+                M->dia, M->k, M->x, B, M->dinv32, M->r32, M->d_s, M->d_g, M->d_partials, M->d_counter);
+        else if (M->k == KP)
+            multi_true_residual_kernel<KP, true, INIT><<<M->grid, kT, 0, st>>>(
+                M->A->args<double>(), M->k, M->x, B, M->dinv32, M->r32, M->d_s, M->d_g, M->d_partials, M->d_counter);
+        else
+            multi_true_residual_kernel<KP, false, INIT><<<M->grid, kT, 0, st>>>(
+                M->A->args<double>(), M->k, M->x, B, M->dinv32, M->r32, M->d_s, M->d_g, M->d_partials, M->d_counter);
+        return CIECU_OK;
+    });
+}
+
+CsrArgs<float> args32(const ciecu_multi_s* M) {
+    const CsrArgs<double> a = M->A->args<double>();
+    return CsrArgs<float>{a.rowptr, a.col, M->val32, a.nrows, a.nnz, a.blocks, a.nblocks, a.mask, a.threshold,
+                          a.aligned16};
+}
+
+template <bool COND>
+int launch_multi_iteration32(ciecu_multi_s* M, cudaStream_t st, cudaGraph_t root, cudaGraphConditionalHandle cond) {
+    cudaGraphConditionalHandle replace = 0;
+    if (COND) CIECU_CUDA(cudaGraphConditionalHandleCreate(&replace, root, 0, cudaGraphCondAssignDefault));
+    CIECU_TRY(with_group(M->kp, [&](auto kk) -> int {
+        constexpr int KP = decltype(kk)::value;
+        if (M->useDia && M->k == KP)
+            multi_spmv32_dia_kernel<KP, true, COND><<<M->grid32D, kT, 0, st>>>(
+                M->diaF, M->k, M->p32, M->q32, M->d_s, M->d_g, M->d_partials, M->d_counter, cond);
+        else if (M->useDia)
+            multi_spmv32_dia_kernel<KP, false, COND><<<M->grid32D, kT, 0, st>>>(
+                M->diaF, M->k, M->p32, M->q32, M->d_s, M->d_g, M->d_partials, M->d_counter, cond);
+        else if (M->k == KP)
+            multi_spmv32_kernel<KP, true, COND><<<M->grid32, kT, 0, st>>>(
+                args32(M), M->k, M->p32, M->q32, M->d_s, M->d_g, M->d_partials, M->d_counter, cond);
+        else
+            multi_spmv32_kernel<KP, false, COND><<<M->grid32, kT, 0, st>>>(
+                args32(M), M->k, M->p32, M->q32, M->d_s, M->d_g, M->d_partials, M->d_counter, cond);
+        multi_update32_kernel<KP, COND><<<M->gridV, kT, 0, st>>>(M->n, M->k, M->x32, M->r32, M->p32, M->q32,
+                                                                  M->dinv32, M->d_s, M->d_g, M->d_partials,
+                                                                  M->d_counter, replace);
+        return CIECU_OK;
+    }));
+    auto replacement = [&](cudaStream_t s2) -> int {
+        CIECU_TRY(with_group(M->kp, [&](auto kk) -> int {
+            constexpr int KP = decltype(kk)::value;
+            multi_fold32_kernel<KP><<<M->gridV, kT, 0, s2>>>(M->n, M->k, M->x, M->x32, M->d_s, M->d_g);
+            return CIECU_OK;
+        }));
+        return launch_true_residual<false>(M, s2, M->graphB);
+    };
+    if (COND)
+        CIECU_TRY(capture_if(st, M->side, replace, replacement));
+    else
+        CIECU_TRY(replacement(st));
+    CIECU_TRY(with_group(M->kp, [&](auto kk) -> int {
+        constexpr int KP = decltype(kk)::value;
+        multi_direction32_kernel<KP, COND><<<M->gridV, kT, 0, st>>>(M->n, M->k, M->p32, M->r32, M->dinv32, M->d_s,
+                                                                    M->d_g, cond);
+        return CIECU_OK;
+    }));
+    CIECU_CHECK_LAUNCH("multi-rhs refined iteration");
+    return CIECU_OK;
+}
+
+// The FP32 copies of the refined form, refreshed from the FP64 arrays at every
+// solve (the caller may change the values between solves): D^-1, and the matrix
+// in the format of the FP64 solve (the DIA copy or the CSR values).
+int prepare32(ciecu_multi_s* M, cudaStream_t st) {
+    const size_t count = std::max<size_t>(1, static_cast<size_t>(M->n) * M->k) + 4;
+    cudaError_t e = cudaSuccess;
+    if (!M->x32) {
+        for (float** v : {&M->x32, &M->r32, &M->p32, &M->q32})
+            if (e == cudaSuccess) e = cudaMalloc(v, sizeof(float) * count);
+        if (e == cudaSuccess) e = cudaMalloc(&M->dinv32, sizeof(float) * (static_cast<size_t>(M->n) + 4));
+        if (e == cudaSuccess && !M->side) e = cudaStreamCreateWithFlags(&M->side, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return cuda_fail(e, "multi: FP32 blocks");
+        with_group(M->kp, [&](auto kk) -> int {
+            constexpr int KP = decltype(kk)::value;
+            const long needed = (M->n + static_cast<long>(kWarps) * (32 / KP) - 1) / (static_cast<long>(kWarps) * (32 / KP));
+            M->grid32 = static_cast<int>(std::max<long>(1, std::min<long>(needed, std::min(
+                resident_blocks(reinterpret_cast<const void*>(multi_spmv32_kernel<KP, true, true>), kT, 0),
+                resident_blocks(reinterpret_cast<const void*>(multi_spmv32_kernel<KP, false, true>), kT, 0)))));
+            M->grid32D = static_cast<int>(std::max<long>(1, std::min<long>(needed, std::min(
+                resident_blocks(reinterpret_cast<const void*>(multi_spmv32_dia_kernel<KP, true, true>), kT, 0),
+                resident_blocks(reinterpret_cast<const void*>(multi_spmv32_dia_kernel<KP, false, true>), kT, 0)))));
+            return CIECU_OK;
+        });
+    }
+    if (M->n > 0) {
+        multi_to_f32_kernel<<<grid_for(M->n, kT, 8), kT, 0, st>>>(M->n, M->dinv, M->dinv32);
+        count_launch();
+    }
+    if (M->useDia) {
+        if (!M->dia32) {
+            DiaArgs<float> a{};
+            a.nrows = M->dia.nrows;
+            a.ndiag = M->dia.ndiag;
+            a.ld = M->dia.ld;
+            for (int d = 0; d < kMaxDiagonals; ++d) a.off[d] = M->dia.off[d];
+            const size_t bytes = sizeof(float) * static_cast<size_t>(a.ndiag) * static_cast<size_t>(a.ld);
+            e = cudaMalloc(&M->dia32, bytes);
+            if (e == cudaSuccess) e = cudaMemsetAsync(M->dia32, 0, bytes, st);
+            if (e != cudaSuccess) return cuda_fail(e, "multi: FP32 diagonal copy");
+            a.val = M->dia32;
+            M->diaF = a;
+        }
+        CIECU_TRY(dia_fill_f32(M->A, M->diaF, M->dia32, nullptr, st));
+    } else {
+        if (!M->val32) {
+            e = cudaMalloc(&M->val32, sizeof(float) * std::max<size_t>(1, static_cast<size_t>(M->A->nnz)));
+            if (e != cudaSuccess) return cuda_fail(e, "multi: FP32 values");
+        }
+        if (M->A->nnz > 0) {
+            multi_to_f32_kernel<<<grid_for(M->A->nnz, kT, 8), kT, 0, st>>>(M->A->nnz, static_cast<const double*>(M->A->val),
+                                                                    M->val32);
+            count_launch();
+        }
+    }
+    CIECU_CHECK_LAUNCH("multi: FP32 copies");
+    return CIECU_OK;
+}
+
+int build_multi_graph32(ciecu_multi_s* M, const double* B) {
+    if (M->graph32 && M->graphB == B) return CIECU_OK;
+    if (M->graph32) {
+        cudaGraphExecDestroy(M->graph32);
+        M->graph32 = nullptr;
+    }
+    M->graphB = B;
+    cudaStream_t st = M->A->space->stream;
+    if (device_loop_enabled()) {
+        const int status = build_while_graph(st, [&](cudaGraph_t root, cudaGraphConditionalHandle cond) {
+            return launch_multi_iteration32<true>(M, st, root, cond);
+        }, &M->graph32);
+        if (status == CIECU_OK) {
+            M->deviceLoop32 = true;
+            return CIECU_OK;
+        }
+        cudaGetLastError();
+    }
+    M->deviceLoop32 = false;
+    cudaGraph_t g = nullptr;
+    CIECU_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int status = CIECU_OK;
+    for (int i = 0; i < M->chunk && status == CIECU_OK; ++i) status = launch_multi_iteration32<false>(M, st, nullptr, 0);
+    cudaError_t e = cudaStreamEndCapture(st, &g);
+    if (status != CIECU_OK) {
+        if (g) cudaGraphDestroy(g);
+        return status;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "multi-rhs refined graph capture");
+    e = cudaGraphInstantiate(&M->graph32, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(e, "multi-rhs refined graph instantiate");
+    return CIECU_OK;
+}
+
+// The solve of the refined form: set-up residual, P = D^-1 R, then the graph
+// until every column is done; the column state lands in s.
+int refined_solve(ciecu_multi_s* M, const double* B, std::vector<ColumnScalars>& s) {
+    cudaStream_t st = M->A->space->stream;
+    const long count = M->n * M->k;
+    MultiGlobal g{};
+    g.maxIter = M->settings.iterationCount;
+    g.absTol = M->settings.absoluteResidual;
+    g.relTol = M->settings.relativeResidual;
+    g.delta = M->refineDelta;
+    *M->h_g = g;
+    CIECU_CUDA(cudaMemcpyAsync(M->d_g, M->h_g, sizeof(MultiGlobal), cudaMemcpyHostToDevice, st));
+    CIECU_TRY(prepare_dia(M, st, B));
+    CIECU_TRY(prepare32(M, st));
+    CIECU_CUDA(cudaMemsetAsync(M->x32, 0, sizeof(float) * count, st));
+    CIECU_CUDA(cudaMemsetAsync(M->p32, 0, sizeof(float) * count, st));
+    CIECU_TRY(launch_true_residual<true>(M, st, B));
+    CIECU_TRY(with_group(M->kp, [&](auto kk) -> int {
+        constexpr int KP = decltype(kk)::value;
+        multi_direction32_kernel<KP, false><<<M->gridV, kT, 0, st>>>(M->n, M->k, M->p32, M->r32, M->dinv32, M->d_s,
+                                                                     M->d_g, 0);
+        return CIECU_OK;
+    }));
+    count_launch(2);
+    CIECU_CHECK_LAUNCH("multi-rhs refined set-up");
+    CIECU_TRY(build_multi_graph32(M, B));
+    const long long limit = M->deviceLoop32 ? 4096 : M->chunk;
+    for (;;) {
+        CIECU_CUDA(cudaMemcpyAsync(M->h_g, M->d_g, sizeof(MultiGlobal), cudaMemcpyDeviceToHost, st));
+        CIECU_CUDA(cudaStreamSynchronize(st));
+        if (M->h_g->finished >= static_cast<unsigned>(M->k)) break;
+        const long long before = M->h_g->replacements;
+        M->h_g->chunkIter = 0;
+        M->h_g->chunkLimit = limit;
+        CIECU_CUDA(cudaMemcpyAsync(&M->d_g->chunkIter, &M->h_g->chunkIter, 2 * sizeof(long long),
+                                   cudaMemcpyHostToDevice, st));
+        CIECU_CUDA(cudaGraphLaunch(M->graph32, st));
+        CIECU_CUDA(cudaMemcpyAsync(M->h_g, M->d_g, sizeof(MultiGlobal), cudaMemcpyDeviceToHost, st));
+        CIECU_CUDA(cudaStreamSynchronize(st));
+        count_launch(M->deviceLoop32 ? 3LL * M->h_g->chunkIter + 2LL * (M->h_g->replacements - before)
+                                     : 5LL * M->chunk);
+        if (M->h_g->finished >= static_cast<unsigned>(M->k)) break;
+    }
+    CIECU_CUDA(cudaMemcpyAsync(s.data(), M->d_s, sizeof(ColumnScalars) * M->k, cudaMemcpyDeviceToHost, st));
+    CIECU_CUDA(cudaStreamSynchronize(st));
+    return CIECU_OK;
+}
+
 }  // namespace
 }  // namespace ciecu
 
@@ -646,7 +1198,22 @@ int ciecu_multi_create(ciecu_csr lhs, int rhsCount, const double* d_inverseDiago
     });
     M->grid = static_cast<int>(std::max<long>(1, std::min<long>(M->grid, needed)));
     M->gridV = static_cast<int>(std::max<long>(1, std::min<long>(M->gridV, needed)));
-    if (e == cudaSuccess) e = cudaMalloc(&M->d_partials, sizeof(double) * 2 * 32 * std::max(M->grid, M->gridV));
+    // partial sums for the widest grid of any kernel of either form (the DIA and
+    // FP32 grids are fixed later, at most their resident blocks), so that the
+    // buffer captured by a graph is never replaced
+    int widest = std::max(M->grid, M->gridV);
+    with_group(M->kp, [&](auto kk) -> int {
+        constexpr int KP = decltype(kk)::value;
+        for (const void* k : {reinterpret_cast<const void*>(multi_spmv_dia_kernel<KP, true, true>),
+                              reinterpret_cast<const void*>(multi_spmv_dia_kernel<KP, false, true>),
+                              reinterpret_cast<const void*>(multi_spmv32_kernel<KP, true, true>),
+                              reinterpret_cast<const void*>(multi_spmv32_kernel<KP, false, true>),
+                              reinterpret_cast<const void*>(multi_spmv32_dia_kernel<KP, true, true>),
+                              reinterpret_cast<const void*>(multi_spmv32_dia_kernel<KP, false, true>)})
+            widest = std::max(widest, resident_blocks(k, kT, 0));
+        return CIECU_OK;
+    });
+    if (e == cudaSuccess) e = cudaMalloc(&M->d_partials, sizeof(double) * 2 * 32 * widest);
     if (e == cudaSuccess) e = cudaMalloc(&M->d_counter, sizeof(unsigned));
     if (e == cudaSuccess) e = cudaMemsetAsync(M->d_counter, 0, sizeof(unsigned), st);
     if (e == cudaSuccess) e = cudaMemsetAsync(M->d_s, 0, sizeof(ColumnScalars) * 32, st);
@@ -671,6 +1238,9 @@ int ciecu_multi_destroy(ciecu_multi M) {
     cudaFree(M->d_partials);
     cudaFree(M->d_counter);
     cudaFree(M->diaBuf);
+    if (M->graph32) cudaGraphExecDestroy(M->graph32);
+    if (M->side) cudaStreamDestroy(M->side);
+    for (float* v : {M->x32, M->r32, M->p32, M->q32, M->dinv32, M->val32, M->dia32}) cudaFree(v);
     delete M;
     return CIECU_OK;
 }
@@ -679,6 +1249,20 @@ int ciecu_multi_info(ciecu_multi M, int* lanesPerRow, int* deviceLoop) {
     CIECU_REQUIRE(M, "multi_info: null solver");
     if (lanesPerRow) *lanesPerRow = M->kp;
     if (deviceLoop) *deviceLoop = M->deviceLoop ? 1 : 0;
+    return CIECU_OK;
+}
+
+int ciecu_multi_set_refinement(ciecu_multi M, double delta) {
+    CIECU_REQUIRE(M, "multi_set_refinement: null solver");
+    CIECU_REQUIRE(delta == 0.0 || (delta > 0.0 && delta < 1.0), "multi_set_refinement: delta must be 0 or in (0, 1)");
+    M->refineDelta = delta;
+    return CIECU_OK;
+}
+
+int ciecu_multi_refinements(ciecu_multi M, int64_t* h_perColumn) {
+    CIECU_REQUIRE(M && h_perColumn, "multi_refinements: null argument");
+    for (int c = 0; c < M->k; ++c)
+        h_perColumn[c] = c < static_cast<int>(M->last.size()) ? M->last[c].refinements : 0;
     return CIECU_OK;
 }
 
@@ -696,7 +1280,9 @@ int ciecu_multi_product(ciecu_multi M, double inScale, const double* d_in, doubl
     const long count = n * M->k;
     CIECU_CUDA(cudaMemcpyAsync(M->x, d_out, sizeof(double) * count, cudaMemcpyDeviceToDevice, st));
     std::vector<ColumnScalars> s(static_cast<size_t>(M->k));
-    if (M->settings.iterationCount > 0) {
+    if (M->settings.iterationCount > 0 && M->refineDelta > 0.0) {
+        CIECU_TRY(refined_solve(M, d_in, s));
+    } else if (M->settings.iterationCount > 0) {
         MultiGlobal g{};
         g.maxIter = M->settings.iterationCount;
         g.absTol = M->settings.absoluteResidual;
@@ -736,6 +1322,7 @@ int ciecu_multi_product(ciecu_multi M, double inScale, const double* d_in, doubl
     count_launch();
     CIECU_CHECK_LAUNCH("multi_output_kernel");
     CIECU_CUDA(cudaStreamSynchronize(st));
+    M->last = s;
     int firstError = -1;
     for (int c = 0; c < M->k; ++c) {
         const ColumnScalars& sc = s[c];

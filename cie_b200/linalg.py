@@ -569,10 +569,12 @@ class MixedPrecisionCG(LinearOperator):
     copy (16-bit column offsets where the bandwidth allows), FP32 vectors with FP64
     dot accumulators, FP64 residual r = b - A x and FP64 solution.  mode 0 =
     reliable updates (delta = replacement trigger), mode 1 = restarted iterative
-    refinement (delta = inner tolerance).  Stops on the true FP64 residual."""
+    refinement (delta = inner tolerance).  Stops on the true FP64 residual.
+    fuseDirection: the search direction and its product formed in the inner SpMV
+    by recurrence (two kernels per inner iteration instead of three)."""
 
     def __init__(self, lhs, inverseDiagonal, settings=None, mode=0, delta=None, compressColumns=True,
-                 innerKernel=0, scaleInner=False):
+                 innerKernel=0, scaleInner=False, fuseDirection=False):
         if type(lhs) is not CSROperator or lhs.space._sfx != "f64":
             raise CiecuError(1, "MixedPrecisionCG needs an FP64 CSROperator")
         self.lhs = lhs
@@ -581,7 +583,7 @@ class MixedPrecisionCG(LinearOperator):
         self.settings = settings if settings is not None else Statistics(5000, 0.0, 1e-10)
         delta = (0.1 if mode == 0 else 1e-4) if delta is None else float(delta)
         self.options = MixedOptions(int(mode), delta, int(bool(compressColumns)), int(innerKernel),
-                                    int(bool(scaleInner)))
+                                    int(bool(scaleInner)), int(bool(fuseDirection)))
         h = ctypes.c_void_p()
         self.space.enter()
         call("ciecu_mixed_create", lhs.csr.handle, _ptr(inverseDiagonal.inverseDiagonal), self.settings, self.options,
@@ -743,13 +745,27 @@ class MultiRHSConjugateGradients(LinearOperator):
         except Exception:
             pass
 
+    def set_refinement(self, delta):
+        """delta in (0, 1): FP32 iterations per column with FP64 reliable updates
+        (replacement when the FP32 residual norm fell below delta times its largest
+        value since the last one); 0: FP64 iterations."""
+        call("ciecu_multi_set_refinement", self._solver, float(delta))
+        self.refinement = float(delta)
+
+    def refinements(self):
+        """FP64 residual recomputations per column in the last refined solve."""
+        out = (ctypes.c_int64 * self.k)()
+        call("ciecu_multi_refinements", self._solver, out)
+        return list(out)
+
     def info(self):
         v, d = ctypes.c_int(), ctypes.c_int()
         call("ciecu_multi_info", self._solver, ctypes.byref(v), ctypes.byref(d))
         f = ctypes.c_int()
         call("ciecu_multi_format", self._solver, ctypes.byref(f))
         return {"lanes_per_row": v.value, "device_loop": bool(d.value),
-                "spmm_format": "dia-%d" % f.value if f.value else "csr"}
+                "spmm_format": "dia-%d" % f.value if f.value else "csr",
+                "refinement": getattr(self, "refinement", 0.0)}
 
     def getStats(self):
         return self._stats

@@ -663,7 +663,7 @@ public:
 
     MixedPrecisionCG(std::shared_ptr<CUDACSROperator<int, double>> pLhs,
                      std::shared_ptr<DiagonalOperator<Space>> pPreconditioner, Statistics settings,
-                     ciecu_mixed_options options = ciecu_mixed_options{0, 0.1, 1, 0, 0})
+                     ciecu_mixed_options options = ciecu_mixed_options{0, 0.1, 1, 0, 0, 0})
         : _pLhs(std::move(pLhs)), _pPreconditioner(std::move(pPreconditioner)) {
         ciecu_mixed raw = nullptr;
         check(ciecu_mixed_create(_pLhs->handle(), _pPreconditioner->inverseDiagonal().data(),

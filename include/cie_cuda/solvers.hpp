@@ -97,6 +97,14 @@ public:
     }
     const std::vector<Statistics>& getStats() const noexcept { return _stats; }
     int rhsCount() const noexcept { return _k; }
+    // delta in (0, 1): FP32 iterations per column with FP64 reliable updates
+    // (ciecu_multi_set_refinement); 0: FP64 iterations.
+    void setRefinement(double delta) { check(ciecu_multi_set_refinement(_solver.get(), delta)); }
+    std::vector<int64_t> refinements() const {
+        std::vector<int64_t> out(static_cast<std::size_t>(_k));
+        check(ciecu_multi_refinements(_solver.get(), out.data()));
+        return out;
+    }
 
 private:
     std::shared_ptr<CUDACSROperator<int, double>> _pLhs;

@@ -42,6 +42,12 @@ typedef struct ciecu_mixed_options {
      * unscaled FP32 copy loses the small couplings and definiteness; the FP64
      * residuals, solution and stopping test are unchanged.  0: the unscaled copy. */
     int scaleInner;
+    /* 1: keep z = D^-1 r as a vector and form the search direction and its
+     * product inside the inner SpMV (w = A32 z, p = z + beta p, q = w + beta q):
+     * two kernels per inner iteration instead of three, same vector traffic, and
+     * q carried by recurrence (FP32 rounding drifts between residual
+     * replacements).  0: q = A32 p after a separate direction kernel. */
+    int fuseDirection;
 } ciecu_mixed_options;
 
 typedef struct ciecu_mixed_statistics {

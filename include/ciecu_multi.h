@@ -10,6 +10,8 @@
 #ifndef CIECU_MULTI_H
 #define CIECU_MULTI_H
 
+#include <stdint.h>
+
 #include "ciecu.h"
 
 #ifdef __cplusplus
@@ -29,6 +31,18 @@ int ciecu_multi_info(ciecu_multi solver, int* lanesPerRow, int* deviceLoop);
  * ciecu_csr_diagonals, whose copy timed faster than the CSR SpMM; the copy is
  * refilled from the CSR values at every solve), or 0 for the CSR SpMM. */
 int ciecu_multi_format(ciecu_multi solver, int* diagonals);
+/* delta in (0, 1): FP32-refined form -- every column iterates in FP32 (FP32
+ * copies of the matrix in the format of the FP64 solve and of D^-1, FP32 blocks,
+ * FP64 dot products) with FP64 reliable updates: when a column's FP32 residual
+ * norm fell below delta times its largest value since the last replacement (or
+ * below the stopping tolerance, or at the iteration limit), its FP32 solution is
+ * added to the FP64 one and its residual recomputed as B - A X in FP64; the
+ * stopping test and the statistics use that FP64 residual (iterationCount =
+ * FP32 iterations).  delta = 0 (default): FP64 iterations as
+ * ConjugateGradients::product. */
+int ciecu_multi_set_refinement(ciecu_multi solver, double delta);
+/* FP64 residual recomputations of each column in the last refined solve. */
+int ciecu_multi_refinements(ciecu_multi solver, int64_t* h_perColumn);
 /* Initial guesses = d_out (n x k); on return out = inScale*out + outScale*X.
  * h_stats (may be NULL): one ciecu_statistics per right-hand side.  A breakdown
  * returns CIECU_ERR_BREAKDOWN naming the first such right-hand side; the others

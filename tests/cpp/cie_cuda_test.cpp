@@ -185,6 +185,20 @@ void solver_classes(const std::shared_ptr<Space>& pSpace) {
             worst = std::fmax(worst, rel_diff(col, want));
         }
         report(worst <= 1e-9, "MultiRHSConjugateGradients per column vs reference PCG", worst);
+        // the FP32-refined form from zero: same bar
+        multi.setRefinement(0.1);
+        pSpace->fill(Space::view(X), 0.0);
+        multi.product(0, Space::view(std::as_const(rhs)), 1, Space::view(X));
+        const std::vector<double> Xr = download(pSpace, X);
+        double worstR = 0.0;
+        for (int c = 0; c < k; ++c) {
+            std::vector<double> col(a.n), want(a.n);
+            for (int i = 0; i < a.n; ++i) col[i] = Xr[i * k + c], want[i] = factor[c] * xref[i];
+            worstR = std::fmax(worstR, rel_diff(col, want));
+        }
+        const auto refinements = multi.refinements();
+        report(worstR <= 1e-9 && refinements[0] > 0, "MultiRHSConjugateGradients FP32-refined vs reference PCG",
+               worstR);
     }
     {
         // two levels with the identity transfer and the fine matrix as coarse matrix

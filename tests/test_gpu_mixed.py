@@ -17,34 +17,39 @@ def space():
     return CUDASpace()
 
 
-def mixed_solve(space, m, b, mode=0, delta=None, compress=True, x0=None, settings=None, inner=0):
+def mixed_solve(space, m, b, mode=0, delta=None, compress=True, x0=None, settings=None, inner=0, fuse=False):
     from cie_b200.linalg import CSROperator, MixedPrecisionCG, Statistics, makeDiagonalOperator
     A = CSROperator(m, space)
     D = makeDiagonalOperator(m, space, csr_handle=A.csr)
     solver = MixedPrecisionCG(A, D, settings or Statistics(20000, 0.0, 1e-10), mode=mode, delta=delta,
-                              compressColumns=compress, innerKernel=inner)
+                              compressColumns=compress, innerKernel=inner, fuseDirection=fuse)
     x = dev(np.zeros(len(b)) if x0 is None else x0)
     solver.product(0.0, dev(b), 1.0, x)
     return host(x), solver.getStats(), solver.info()
 
 
-@pytest.mark.parametrize("mode,compress,inner", [(0, True, 0), (0, False, 0), (1, True, 0), (0, True, -1),
-                                                 (0, False, -1), (1, True, -1), (0, True, 1), (0, True, 4),
-                                                 (0, True, -2), (1, True, -2)])
-def test_mixed_3d_lognormal_vs_reference(space, reference, mode, compress, inner):
+@pytest.mark.parametrize("mode,compress,inner,fuse", [(0, True, 0, False), (0, False, 0, False), (1, True, 0, False),
+                                                      (0, True, -1, False), (0, False, -1, False),
+                                                      (1, True, -1, False), (0, True, 1, False), (0, True, 4, False),
+                                                      (0, True, -2, False), (1, True, -2, False),
+                                                      (0, True, -2, True), (1, True, -2, True), (0, True, -1, True),
+                                                      (0, False, 2, True), (0, True, 0, True)])
+def test_mixed_3d_lognormal_vs_reference(space, reference, mode, compress, inner, fuse):
+    """fuse: the direction and its product formed by recurrence in the inner SpMV
+    (two kernels per inner iteration); same bars as the three-kernel form."""
     from cie_b200.fem import make_poisson
     prob = make_poisson(space, 3, 1, [40, 40, 40], seed=2)
     rp, col, val = prob.host_csr()
     b = host(prob.rhs)
-    x, st, info = mixed_solve(space, prob.matrix, b, mode=mode, compress=compress, inner=inner)
+    x, st, info = mixed_solve(space, prob.matrix, b, mode=mode, compress=compress, inner=inner, fuse=fuse)
     if inner:
         assert info["group_unroll"] == (inner if inner == -2 else max(inner, 0))
     xr, sr, err, _ = reference.pcg(rp, col, val, b, maxit=20000, abstol=0.0, reltol=1e-10)
     rel = np.linalg.norm(x - xr) / np.linalg.norm(xr)
     tr = true_residual(rp, col, val, x, b)
-    print("mixed mode %d compress %s: %d inner iterations, %d refinements (FP64 reference: %d), "
+    print("mixed mode %d compress %s fuse %s: %d inner iterations, %d refinements (FP64 reference: %d), "
           "|x-x_ref|/|x_ref| = %.3e, true rel residual %.3e, %s"
-          % (mode, compress, st.innerIterations, st.refinements, sr[0], rel, tr, info))
+          % (mode, compress, fuse, st.innerIterations, st.refinements, sr[0], rel, tr, info))
     if info["format"] != "dia":  # the SELL copy is not built when the DIA copy is the known choice
         assert info["compressed_columns"] == compress
     assert st.trueRelativeResidual < 1e-10 and tr <= 1.01e-10
