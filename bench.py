@@ -221,10 +221,13 @@ def main():
                     help="with --profile: FP64-solver,mixed-unroll,CSR schedules to use instead of autotuning "
                          "(the choices a bench run without the profiler reports), e.g. 4,1,4")
     ap.add_argument("--profile-target", default="pcg",
-                    choices=["pcg", "batch", "spmm", "embedded", "cut", "gradient"],
+                    choices=["pcg", "batch", "spmm", "spmm32", "embedded", "cut", "twolevel", "gradient"],
                     help="with --profile: the solver the ncu target runs (pcg: the headline solves; batch: a "
-                         "batched solve of 128 Q2 systems; spmm: a 32-RHS solve on the Q1 grid of --profile-cells; "
-                         "embedded: the finite-cell Q3 assembly on 16^3 cells; cut: 30 FP64 Jacobi-PCG iterations "
+                         "batched solve of 128 Q2 systems; spmm: a 32-RHS solve on the Q1 grid of --profile-cells "
+                         "(spmm32: its FP32 form with FP64 reliable updates); "
+                         "embedded: the finite-cell Q3 assembly (FP64 and FP32) on --profile-cells^3 cells when that "
+                         "is at most 32, else 16^3; twolevel: three iterations of the two-level CG with FP32 "
+                         "smoothing on that system; cut: 30 FP64 Jacobi-PCG iterations "
                          "on that finite-cell system, on --profile-cells^3 cells when that is at most 24 "
                          "(--pin's first value pins the SpMV schedule); gradient: one "
                          "adjoint gradient on the Q1 grid of --profile-cells)")
@@ -412,18 +415,22 @@ def main():
     dia32 = info.get("format") == "dia"
     dia64 = cg.info().get("spmv_schedule") == 64
     idx_bytes = 2 if info.get("compressed_columns") else 4
+    stored32 = info.get("dia_stored_diagonals") or ndiag
+    sym32 = bool(info.get("dia_symmetric"))
     if dia32:
         # FP32 DIA SpMV: the stored diagonals (nonzeros and the zeros that pad the
-        # diagonals), x read, y written; no column indices
-        spmv32_bytes = 4 * ndiag * n + 8 * n
-        inner_bytes = 4 * ndiag * n + 52 * n
+        # diagonals; the upper half when the matrix is symmetric, the lower entries
+        # being re-read from it through L2), x read, y written; no column indices
+        spmv32_bytes = 4 * stored32 * n + 8 * n
+        inner_bytes = 4 * stored32 * n + 52 * n
     else:
         # FP32 SELL-32 SpMV: values + column offsets of the nonzeros, x read, y written
         # (padding entries and the per-slice descriptors are reported, not counted)
         spmv32_bytes = (4 + idx_bytes) * nnz + 8 * n
         inner_bytes = (4 + idx_bytes) * nnz + 52 * n
     spmv64_bytes = 12 * nnz + 4 * (n + 1) + 16 * n
-    iter64_bytes = (8 * ndiag * n if dia64 else 12 * nnz + 4 * (n + 1)) + 104 * n
+    stored64 = cg.info().get("dia_stored_diagonals") or ndiag
+    iter64_bytes = (8 * stored64 * n if dia64 else 12 * nnz + 4 * (n + 1)) + 104 * n
     fp64_solve_bytes = (it64 + 1) * iter64_bytes + (12 * nnz + 4 * (n + 1) + 24 * n)
     refine_bytes = 12 * nnz + 4 * (n + 1) + 28 * n  # FP64 residual pass: x64, b read, r32 written, dinv32
     mixed_solve_bytes = mst.innerIterations * inner_bytes + (mst.refinements + 1) * refine_bytes
@@ -433,7 +440,7 @@ def main():
     if os.path.exists(tpath) and cells == [128, 128, 128]:
         figures = dict(line.split() for line in open(tpath) if line.strip() and not line.startswith("#"))
         if dia32:
-            traffic = int(figures.get("mixed_apply_dia_kernel_f32", 0)) or None
+            traffic = int(figures.get("mixed_apply_dia_kernel_f32" + ("_symmetric" if sym32 else ""), 0)) or None
         elif info["compressed_columns"] and info["group_unroll"] > 0:
             traffic = int(figures.get("mixed_apply_kernel_f32_sell16", 0)) or None
         traffic64 = int(figures.get("spmv_kernel_f64_csr", 0)) or None
@@ -493,8 +500,10 @@ def main():
             "data": "synthetic (seeded mt19937_64 RHS and kappa field)",
             "config": common_config(world),
             "solver": {"mixed": "jacobi-pcg, FP32 inner over %s, FP64 reliable updates delta=%g, %s" % (
-                           info["format"], DELTA, "fused direction" if FUSE else "separate direction kernel"),
-                       "fp64": "jacobi-pcg over %s" % ("dia" if dia64 else "csr")},
+                           info["format"] + (" (symmetric upper half)" if sym32 else ""), DELTA,
+                           "fused direction" if FUSE else "separate direction kernel"),
+                       "fp64": "jacobi-pcg over %s" % (("dia, symmetric upper half" if cg.info().get(
+                           "dia_symmetric") else "dia") if dia64 else "csr")},
             "gpu_launches": int(launches),
             "clocks": clocks,
             "workloads": extra,
@@ -520,7 +529,9 @@ def main():
                                        "mixed_frac": mixed_solve_bytes / t_mixed / 1e9 / hbm},
             "parity": parity,
             "roofline": {"bound": "hbm", "kernel": (
-                             "mixed_apply_dia_kernel (FP32 DIA SpMV, %d diagonals)" % ndiag) if dia32 else (
+                             "mixed_apply_dia_kernel (FP32 DIA SpMV, %d diagonals%s)" % (
+                                 ndiag, ", symmetric: the %d of the upper half stored" % stored32 if sym32 else ""))
+                         if dia32 else (
                              "%s (FP32 SELL-32 SpMV)" % ("mixed_apply_kernel<%d>" % info["group_unroll"]
                                                          if info["group_unroll"] > 0 else "mixed_apply_tma_kernel")),
                          "achieved": g32, "peak": hbm, "unit": "GB/s", "frac": g32 / hbm, "peak_kind": peak_kind,
@@ -549,19 +560,37 @@ def profile_target(space, target, cells, schedule=0):
         x = torch.zeros_like(rhs)
         solver.product(0.0, rhs, 1.0, x)
         info = solver.info()
-    elif target == "spmm":
+    elif target in ("spmm", "spmm32"):
         prob = make_poisson(space, 3, 1, [cells] * 3, seed=0)
         n = prob.rhs.numel()
         A = CSROperator(prob.matrix, space)
         D = makeDiagonalOperator(prob.matrix, space, csr_handle=A.csr)
         B = torch.as_tensor(np.stack([random_uniform(2000 + c, n) for c in range(32)], axis=1)).cuda().contiguous()
         solver = MultiRHSConjugateGradients(A, D, 32, tight)
+        if target == "spmm32":
+            solver.set_refinement(DELTA)
         X = torch.zeros_like(B)
         solver.product(0.0, B, 1.0, X)
         info = solver.info()
     elif target == "embedded":
-        prob = make_embedded_poisson(space, 3, 3, [16, 16, 16], radius=0.4, alpha=1e-6, depth=2)
-        info = {"cut_cells": prob.cut_cells}
+        # the FP64 (DMMA) assembly inside the set-up, then the FP32 (split-BF16) one
+        c = cells if cells <= 32 else 16
+        prob = make_embedded_poisson(space, 3, 3, [c, c, c], radius=0.4, alpha=1e-6, depth=2)
+        v32 = torch.zeros(prob.matrix.entries.numel(), dtype=torch.float32, device="cuda")
+        prob.assembler.assemble_embedded_f32(v32, [0.5] * 3, 0.4, 1e-6, 2)
+        info = {"cut_cells": prob.cut_cells, "cells": c}
+    elif target == "twolevel":
+        # three outer iterations of the device two-level CG (FP32 smoothing) on the
+        # finite-cell sphere of --profile-cells^3 cells (at most 32)
+        from cie_b200.twolevel import make_two_level_cg
+        c = cells if cells <= 32 else 16
+        prob = make_embedded_poisson(space, 3, 3, [c, c, c], radius=0.4, alpha=1e-6, depth=2)
+        precision, degree, coarse = TWO_LEVEL[-1]
+        solver = make_two_level_cg(space, prob, Statistics(3, 0.0, 1e-10), degree=degree, coarseIterations=coarse,
+                                   precision=precision)
+        x = torch.zeros_like(prob.rhs)
+        solver.product(0.0, prob.rhs, 1.0, x)
+        info = dict(solver.info(), cells=c, degree=degree, coarse=coarse)
     elif target == "cut":
         c = cells if cells <= 24 else 16
         prob = make_embedded_poisson(space, 3, 3, [c, c, c], radius=0.4, alpha=1e-6, depth=2)
@@ -672,27 +701,29 @@ def extra_workloads(space, A, D, settings, t_fp64, it64, rank=0, world=1):
     tb = timed(solveb, 3)
     its = [s.iterationCount for s in batch.getStats()]
     rels = [s.relativeResidual for s in batch.getStats()]
-    # the same batch with FP32 inner solves and FP64 refinement, for three drops of
-    # the FP32 residual per refinement round (fewer rounds keep more of each Krylov
-    # space); the fastest is reported
-    refinedByTol = {}
+    # the same batch in FP32 with FP64 reliable updates per system (the Krylov space
+    # kept across replacements), and with restarted FP32 inner solves to 1e-4 per
+    # FP64 refinement round for comparison
     xr = torch.zeros_like(rhs)
-    best = None
-    for tol in (1e-2, 1e-4, 1e-5):
-        refined = BatchedConjugateGradients(bd, offsets, space, Dbd, tight)
-        refined.set_refinement(tol)
+    refined = BatchedConjugateGradients(bd, offsets, space, Dbd, tight)
+    refined.set_reliable_updates(DELTA)
 
-        def solver_refined():
-            xr.zero_()
-            refined.product(0.0, rhs, 1.0, xr)
-        t_tol = timed(solver_refined, 1)
-        its_tol = [s.iterationCount for s in refined.getStats()]
-        refinedByTol["%g" % tol] = {"seconds": t_tol, "inner_iterations_max": int(max(its_tol))}
-        if best is None or t_tol < best[0]:
-            best = (t_tol, tol, its_tol, max(s.relativeResidual for s in refined.getStats()),
-                    float(torch.linalg.norm(xr - xb) / torch.linalg.norm(xb)))
-        del refined
-    tr, rtol, rits, rrel, rdiff = best
+    def solve_reliable():
+        xr.zero_()
+        refined.product(0.0, rhs, 1.0, xr)
+    tr = timed(solve_reliable, 3)
+    rits = [s.iterationCount for s in refined.getStats()]
+    rreps = refined.refinements()
+    rrel = max(s.relativeResidual for s in refined.getStats())
+    rdiff = float(torch.linalg.norm(xr - xb) / torch.linalg.norm(xb))
+    refined.set_reliable_updates(0.0)
+    refined.set_refinement(1e-4)
+
+    def solve_restarted():
+        xr.zero_()
+        refined.product(0.0, rhs, 1.0, xr)
+    t_restart = timed(solve_restarted, 1)
+    del refined
     # the same systems one after another (one solver object per system)
     singles = []
     for p in probs:
@@ -711,9 +742,10 @@ def extra_workloads(space, A, D, settings, t_fp64, it64, rank=0, world=1):
         "iterations_min": int(min(its)), "iterations_max": int(max(its)), "max_relative_residual": max(rels),
         "sequential_single_solves_seconds": ts, "speedup_vs_sequential": ts / tb,
         "rel_diff_vs_single_solves": agree, "solver": batch.info(),
-        "fp32_refined_seconds": tr, "fp32_refined_inner_tolerance": rtol,
-        "fp32_refined_inner_iterations_max": int(max(rits)), "fp32_refined_max_relative_residual": rrel,
-        "fp32_refined_rel_diff_vs_fp64": rdiff, "fp32_refined_by_inner_tolerance": refinedByTol}
+        "fp32_refined_seconds": tr, "fp32_refined_form": "FP32 iterations, FP64 reliable updates delta=%g" % DELTA,
+        "fp32_refined_iterations_max": int(max(rits)), "fp32_refined_replacements_max": int(max(rreps)),
+        "fp32_refined_max_relative_residual": rrel, "fp32_refined_rel_diff_vs_fp64": rdiff,
+        "fp32_refined_speedup_vs_fp64": tb / tr, "fp32_restarted_refinement_1e-4_seconds": t_restart}
     del singles, batch, Dbd, bd, rhs, xb, xr, probs
 
     # 32 right-hand sides on the 128^3 matrix

@@ -87,6 +87,7 @@ SIGNATURES = {
     "ciecu_pcg_set_graph_chunk": (c_int, [P, c_int]),
     "ciecu_pcg_set_schedule": (c_int, [P, c_int]),
     "ciecu_pcg_info": (c_int, [P, P, P]),
+    "ciecu_pcg_dia_info": (c_int, [P, P, P]),
     "ciecu_pcg_set_loop": (c_int, [P, c_int]),
     "ciecu_pcg_debug_exchange": (c_int, [P, c_int64, c_int64]),
     "ciecu_mixed_create": (c_int, [P, P, Statistics, MixedOptions, P]),
@@ -96,6 +97,7 @@ SIGNATURES = {
     "ciecu_mixed_product": (c_int, [P, c_double, P, c_double, P, P]),
     "ciecu_mixed_apply_f32": (c_int, [P, P, P]),
     "ciecu_mixed_padded_entries": (c_int, [P, P]),
+    "ciecu_mixed_dia_info": (c_int, [P, P, P]),
     # host utilities
     "ciecu_structured_dofmap": (c_int, [c_int, c_int, P, P, P]),
     "ciecu_structured_boundary": (c_int, [c_int, c_int, P, P]),
@@ -118,6 +120,8 @@ SIGNATURES = {
     "ciecu_batch_info": (c_int, [P, P, P, P]),
     "ciecu_batch_product": (c_int, [P, c_double, P, c_double, P, P]),
     "ciecu_batch_set_refinement": (c_int, [P, c_double]),
+    "ciecu_batch_set_reliable_updates": (c_int, [P, c_double]),
+    "ciecu_batch_refinements": (c_int, [P, P]),
     "ciecu_multi_create": (c_int, [P, c_int, P, Statistics, P]),
     "ciecu_multi_destroy": (c_int, [P]),
     "ciecu_multi_info": (c_int, [P, P, P]),

@@ -37,6 +37,14 @@ struct BatchScalars {
     int done;   // 0 running, 1 converged, 2 iteration limit, 3 breakdown
     int errorKind;  // 1: r^T z <= 0 at start, 2: p^T A p <= 0
     long long errorIter;
+    // reliable-update form: state of the system's FP32 recursion
+    double maxrx, maxrr;  // largest FP32 residual norm since the last x / r replacement
+    double rzPending;
+    long long refinements;
+    int pending;  // a replacement is due at the end of this iteration
+    int updateX;
+    int restart;  // an FP32 breakdown: no step, direction restarted after the replacement
+    int breakdowns;
 };
 
 struct BatchGlobal {
@@ -47,7 +55,16 @@ struct BatchGlobal {
     double absTol, relTol;
     int badColumn;       // an entry outside its system's block (set-up check)
     int pad2;
+    // reliable-update form
+    double delta;           // replacement trigger
+    unsigned anyPending;    // some system asked for a replacement in this iteration
+    unsigned ctaDone;       // CTAs of the current kernel that finished (last-CTA decision)
+    long long replacements; // launches of the replacement pair that had work
 };
+
+// FP32 breakdowns a system may recover from by a replacement with a restarted
+// direction before it reports the breakdown.
+constexpr int kMaxSystemBreakdowns = 64;
 
 struct Tile {
     int system;
@@ -211,7 +228,9 @@ __global__ void __launch_bounds__(kT) batch_init_kernel(const Tile* __restrict__
 }
 
 // K1: q = A p and p^T q per system; alpha.
-template <int VS, typename T>
+// RELIABLE (the reliable-update form): an FP32 breakdown takes no step and asks
+// for a replacement with a restarted direction, up to kMaxSystemBreakdowns.
+template <int VS, typename T, bool RELIABLE = false>
 __global__ void __launch_bounds__(kT) batch_spmv_kernel(CsrArgs<T> A, const Tile* __restrict__ tiles, int ntiles,
                                                         const int* tileBegin, const int* tileCount,
                                                         const T* __restrict__ p, T* __restrict__ q,
@@ -226,7 +245,11 @@ __global__ void __launch_bounds__(kT) batch_spmv_kernel(CsrArgs<T> A, const Tile
         if (system_reduce_last<1>(mine, t, tileBegin, tileCount, partials, counter, tot) && threadIdx.x == 0) {
             BatchScalars& s = S[t.system];
             s.pq = tot[0];
-            if (!(0.0 < tot[0])) {
+            if (RELIABLE && !(0.0 < tot[0]) && s.breakdowns < kMaxSystemBreakdowns) {
+                s.alpha = 0.0;
+                s.restart = 1;
+                s.breakdowns += 1;
+            } else if (!(0.0 < tot[0])) {
                 s.done = 3;
                 s.errorKind = 2;
                 s.errorIter = s.iter;
@@ -299,6 +322,218 @@ __global__ void __launch_bounds__(kT) batch_direction_kernel(const Tile* __restr
         const T beta = static_cast<T>(s.beta);
         for (int i = t.rowBegin + threadIdx.x; i < t.rowEnd; i += kT)
             p[i] = add_rn(mul_rn(p[i], beta), mul_rn(r[i], dinv[i]));
+    }
+}
+
+// ---- reliable-update form: FP32 iterations, FP64 residual replacements ------
+//
+// Per system the iteration of the mixed-precision solver: K1 (batch_spmv_kernel
+// on the FP32 copy, RELIABLE: an FP32 breakdown restarts instead of failing);
+// K2 x32 += alpha p32, r32 -= alpha q32, the FP32 recursion's r^T r and r^T z in
+// FP64 and the replacement decision (FP32 residual norm below delta times its
+// maximum since the last replacement, below the stopping tolerance, or the
+// iteration limit); when any system asks, F folds x32 into the FP64 solution
+// and T recomputes r = b - A64 x64 in FP64 for those systems (float(r) kept),
+// with the FP64 stopping test; K3 p32 = D^-1 r32 + beta p32.
+
+// The last CTA of a kernel to finish (a grid-wide ticket) runs f(); CTAs call
+// this once, after all their work.
+template <typename F>
+__device__ __forceinline__ void last_cta(BatchGlobal* g, F&& f) {
+    __shared__ bool s_lastCta;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_lastCta = atomicAdd(&g->ctaDone, 1u) == gridDim.x - 1;
+        if (s_lastCta) {
+            __threadfence();
+            g->ctaDone = 0u;
+            f();
+        }
+    }
+}
+
+template <bool COND>
+__global__ void __launch_bounds__(kT) batch_update_rel_kernel(const Tile* __restrict__ tiles, int ntiles,
+                                                              const int* tileBegin, const int* tileCount,
+                                                              float* __restrict__ x, float* __restrict__ r,
+                                                              const float* __restrict__ p, const float* __restrict__ q,
+                                                              const float* __restrict__ dinv, BatchScalars* S,
+                                                              BatchGlobal* g, double* partials, unsigned* counter,
+                                                              cudaGraphConditionalHandle replace) {
+    for (int ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
+        const Tile t = tiles[ti];
+        BatchScalars& s = S[t.system];
+        if (*reinterpret_cast<volatile int*>(&s.done)) continue;
+        const bool step = !s.restart;
+        const float alpha = static_cast<float>(s.alpha), malpha = -alpha;
+        double rr = 0.0, rz = 0.0;
+        for (int i = t.rowBegin + threadIdx.x; i < t.rowEnd; i += kT) {
+            float ri = r[i];
+            if (step) {
+                x[i] = fmaf(alpha, p[i], x[i]);
+                ri = fmaf(malpha, q[i], ri);
+                r[i] = ri;
+            }
+            rr = fma(static_cast<double>(ri), static_cast<double>(ri), rr);
+            rz = fma(static_cast<double>(ri), static_cast<double>(ri * dinv[i]), rz);
+        }
+        double mine[2] = {rr, rz}, tot[2];
+        if (system_reduce_last<2>(mine, t, tileBegin, tileCount, partials, counter, tot) && threadIdx.x == 0) {
+            const double rnorm = sqrt(tot[0]);
+            s.iter += 1;
+            if (rnorm > s.maxrx) s.maxrx = rnorm;
+            if (rnorm > s.maxrr) s.maxrr = rnorm;
+            const bool updateX = rnorm < g->delta * s.maxrx;
+            const bool update = updateX || rnorm < g->delta * s.maxrr || rnorm < g->relTol * s.r0 ||
+                                rnorm < g->absTol || s.iter >= g->maxIter || s.restart;
+            s.updateX = updateX ? 1 : 0;
+            if (update) {
+                s.pending = 1;
+                s.rzPending = tot[1];
+                atomicOr(&g->anyPending, 1u);
+            } else {
+                s.beta = tot[1] / s.rz;
+                s.rz = tot[1];
+            }
+        }
+        __syncthreads();
+    }
+    last_cta(g, [&] { set_loop<COND>(replace, *reinterpret_cast<volatile unsigned*>(&g->anyPending) ? 1u : 0u); });
+}
+
+// F: x64 += x32, x32 = 0 on the rows of systems with a replacement due.
+__global__ void __launch_bounds__(kT) batch_fold_rel_kernel(const Tile* __restrict__ tiles, int ntiles,
+                                                            double* __restrict__ x64, float* __restrict__ x32,
+                                                            const BatchScalars* S, const BatchGlobal* g) {
+    if (!*reinterpret_cast<const volatile unsigned*>(&g->anyPending)) return;
+    for (int ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
+        const Tile t = tiles[ti];
+        if (!S[t.system].pending) continue;
+        for (int i = t.rowBegin + threadIdx.x; i < t.rowEnd; i += kT) {
+            x64[i] += static_cast<double>(x32[i]);
+            x32[i] = 0.0f;
+        }
+    }
+}
+
+// T: r = b - A64 x64 in FP64, r32 = float(r), ||r||^2 in FP64 and r32^T z32.
+struct TrueResidualOp {
+    struct Pre {
+        double b;
+        float d;
+    };
+    const double* __restrict__ b;
+    const float* __restrict__ dinv;
+    float* __restrict__ r32;
+    double rr, rz;
+    __device__ __forceinline__ Pre pre(int i) const { return Pre{b[i], dinv[i]}; }
+    __device__ __forceinline__ void post(int i, const Pre& pr, double sum) {
+        const double ri = pr.b - sum;
+        const float rf = static_cast<float>(ri);
+        r32[i] = rf;
+        rr = fma(ri, ri, rr);
+        rz = fma(static_cast<double>(rf), static_cast<double>(rf * pr.d), rz);
+    }
+};
+
+template <bool INIT>
+__device__ __forceinline__ void system_replace(BatchScalars& s, const double (&tot)[2], BatchGlobal* g) {
+    const double rnorm = sqrt(tot[0]);
+    if (INIT) {
+        s = BatchScalars{};
+        s.rr = tot[0];
+        s.r0 = rnorm;
+        s.absres = rnorm;
+        s.relres = 1.0;
+        s.maxrx = s.maxrr = rnorm;
+        s.rz = tot[1];
+        if (float_less(s.absres, g->absTol) || float_less(s.relres, g->relTol)) {
+            s.done = 1;
+        } else if (!(0.0 < tot[1])) {
+            s.done = 3;
+            s.errorKind = 1;
+        } else if (g->maxIter <= 0) {
+            s.done = 2;
+        }
+        if (s.done) atomicAdd(&g->finished, 1u);
+        return;
+    }
+    s.pending = 0;
+    s.refinements += 1;
+    s.rr = tot[0];
+    s.absres = rnorm;
+    s.relres = rnorm / s.r0;
+    if (float_less(s.absres, g->absTol) || float_less(s.relres, g->relTol)) {
+        s.done = 1;
+    } else if (s.iter >= g->maxIter) {
+        s.done = 2;
+    } else if (!(0.0 < tot[1])) {
+        s.done = 3;
+        s.errorKind = 1;
+        s.errorIter = s.iter;
+    } else {
+        s.maxrr = rnorm;
+        if (s.updateX) s.maxrx = rnorm;
+        s.beta = s.restart ? 0.0 : tot[1] / s.rz;  // after an FP32 breakdown: p = z
+        s.rz = tot[1];
+    }
+    s.restart = 0;
+    if (s.done) atomicAdd(&g->finished, 1u);
+}
+
+template <int VS, bool INIT>
+__global__ void __launch_bounds__(kT) batch_true_residual_kernel(CsrArgs<double> A, const Tile* __restrict__ tiles,
+                                                                 int ntiles, const int* tileBegin,
+                                                                 const int* tileCount, const double* __restrict__ b,
+                                                                 const double* __restrict__ x64,
+                                                                 const float* __restrict__ dinv,
+                                                                 float* __restrict__ r32, BatchScalars* S,
+                                                                 BatchGlobal* g, double* partials,
+                                                                 unsigned* counter) {
+    if (!INIT && !*reinterpret_cast<volatile unsigned*>(&g->anyPending)) return;
+    for (int ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
+        const Tile t = tiles[ti];
+        BatchScalars& s = S[t.system];
+        if (!INIT && (s.done || !s.pending)) continue;
+        TrueResidualOp op{b, dinv, r32, 0.0, 0.0};
+        tile_rows<VS>(A, t.rowBegin, t.rowEnd, x64, op);
+        double mine[2] = {op.rr, op.rz}, tot[2];
+        if (system_reduce_last<2>(mine, t, tileBegin, tileCount, partials, counter, tot) && threadIdx.x == 0)
+            system_replace<INIT>(s, tot, g);
+        __syncthreads();
+    }
+    if (!INIT)
+        last_cta(g, [&] {
+            g->anyPending = 0u;
+            g->replacements += 1;
+        });
+}
+
+// K3 of the reliable-update form: p32 = D^-1 r32 + beta p32 (beta = 0: a new
+// direction, the old one may not be finite after a breakdown); ends the loop
+// when every system is finished.
+template <bool COND>
+__global__ void __launch_bounds__(kT) batch_direction_rel_kernel(const Tile* __restrict__ tiles, int ntiles,
+                                                                 int systems, float* __restrict__ p,
+                                                                 const float* __restrict__ r,
+                                                                 const float* __restrict__ dinv,
+                                                                 const BatchScalars* S, BatchGlobal* g,
+                                                                 cudaGraphConditionalHandle cond) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        g->chunkIter += 1;
+        const bool more = *reinterpret_cast<volatile unsigned*>(&g->finished) < static_cast<unsigned>(systems);
+        set_loop<COND>(cond, (more && g->chunkIter < g->chunkLimit) ? 1u : 0u);
+    }
+    for (int ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
+        const Tile t = tiles[ti];
+        const BatchScalars& s = S[t.system];
+        if (*reinterpret_cast<const volatile int*>(&s.done)) continue;
+        const float beta = static_cast<float>(s.beta);
+        if (beta == 0.0f)
+            for (int i = t.rowBegin + threadIdx.x; i < t.rowEnd; i += kT) p[i] = r[i] * dinv[i];
+        else
+            for (int i = t.rowBegin + threadIdx.x; i < t.rowEnd; i += kT) p[i] = fmaf(beta, p[i], r[i] * dinv[i]);
     }
 }
 
@@ -404,6 +639,12 @@ struct ciecu_batch_s {
     float* dinv32 = nullptr;
     double* norm2 = nullptr;  // per-system ||r||^2 of the outer refinement
     double innerTolerance = 0.0;  // > 0: FP32 inner solves with FP64 refinement
+    double reliableDelta = 0.0;   // > 0: FP32 iterations with FP64 reliable updates (takes precedence)
+    cudaGraphExec_t relGraph = nullptr;
+    bool relDeviceLoop = false;
+    const double* relB = nullptr;  // right-hand side the reliable-update graph reads
+    cudaStream_t side = nullptr;   // captures the IF body of the replacement
+    std::vector<long long> lastRefinements;  // FP64 replacements per system in the last reliable-update solve
     ciecu::BatchScalars* d_s = nullptr;
     ciecu::BatchGlobal* d_g = nullptr;
     ciecu::BatchGlobal* h_g = nullptr;
@@ -548,6 +789,145 @@ int run_level(ciecu_batch_s* B, Level<T>& L, const BatchGlobal& g0, unsigned pre
     return CIECU_OK;
 }
 
+// FP32 copies of the matrix values and of D^-1 and the FP32 vectors (first use),
+// with the lane count of their SpMV tuned.
+int ensure_f32(ciecu_batch_s* B) {
+    if (B->val32) return CIECU_OK;
+    cudaStream_t st = B->A->space->stream;
+    const size_t n = static_cast<size_t>(std::max<long>(1, B->n));
+    cudaError_t e = cudaMalloc(&B->val32, sizeof(float) * std::max<long>(1, B->A->nnz));
+    if (e == cudaSuccess) e = cudaMalloc(&B->dinv32, sizeof(float) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&B->norm2, sizeof(double) * B->systems);
+    for (float** v : {&B->f32.x, &B->f32.r, &B->f32.p, &B->f32.q})
+        if (e == cudaSuccess) e = cudaMalloc(v, sizeof(float) * n);
+    if (e == cudaSuccess && B->A->nnz > 0) {
+        batch_to_f32_kernel<<<grid_for(B->A->nnz, kT, 8), kT, 0, st>>>(
+            B->A->nnz, static_cast<const double*>(B->A->val), B->val32);
+        batch_to_f32_kernel<<<grid_for(B->n, kT, 8), kT, 0, st>>>(B->n, B->f64.dinv, B->dinv32);
+        count_launch(2);
+        e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "batched pcg: FP32 copies");
+    B->f32.A = CsrArgs<float>{B->A->rowptr, B->A->col, B->val32, B->A->rows, B->A->nnz, B->A->d_blocks,
+                              B->A->nblocks, nullptr, 0, B->A->aligned16};
+    B->f32.dinv = B->dinv32;
+    return tune_batch(B, B->f32);
+}
+
+template <bool INIT>
+int launch_true_residual(ciecu_batch_s* B, cudaStream_t st, const double* b) {
+    return with_lanes(B->f64.lanes, [&](auto v) -> int {
+        constexpr int VS = decltype(v)::value;
+        batch_true_residual_kernel<VS, INIT><<<B->grid, kT, 0, st>>>(
+            B->f64.A, B->d_tiles, B->ntiles, B->d_tileBegin, B->d_tileCount, b, B->f64.x, B->dinv32, B->f32.r,
+            B->d_s, B->d_g, B->d_partials, B->d_counter);
+        return CIECU_OK;
+    });
+}
+
+template <bool COND>
+int launch_reliable_iteration(ciecu_batch_s* B, cudaStream_t st, cudaGraph_t root, cudaGraphConditionalHandle cond) {
+    Level<float>& F = B->f32;
+    cudaGraphConditionalHandle replace = 0;
+    if (COND) CIECU_CUDA(cudaGraphConditionalHandleCreate(&replace, root, 0, cudaGraphCondAssignDefault));
+    CIECU_TRY(with_lanes(F.lanes, [&](auto v) -> int {
+        constexpr int VS = decltype(v)::value;
+        batch_spmv_kernel<VS, float, true><<<B->grid, kT, 0, st>>>(F.A, B->d_tiles, B->ntiles, B->d_tileBegin,
+                                                                   B->d_tileCount, F.p, F.q, B->d_s, B->d_g,
+                                                                   B->d_partials, B->d_counter);
+        return CIECU_OK;
+    }));
+    batch_update_rel_kernel<COND><<<B->grid, kT, 0, st>>>(B->d_tiles, B->ntiles, B->d_tileBegin, B->d_tileCount, F.x,
+                                                          F.r, F.p, F.q, F.dinv, B->d_s, B->d_g, B->d_partials,
+                                                          B->d_counter, replace);
+    auto replacement = [&](cudaStream_t s2) -> int {
+        batch_fold_rel_kernel<<<B->grid, kT, 0, s2>>>(B->d_tiles, B->ntiles, B->f64.x, F.x, B->d_s, B->d_g);
+        return launch_true_residual<false>(B, s2, B->relB);
+    };
+    if (COND)
+        CIECU_TRY(capture_if(st, B->side, replace, replacement));
+    else
+        CIECU_TRY(replacement(st));
+    batch_direction_rel_kernel<COND><<<B->grid, kT, 0, st>>>(B->d_tiles, B->ntiles, B->systems, F.p, F.r, F.dinv,
+                                                             B->d_s, B->d_g, cond);
+    CIECU_CHECK_LAUNCH("batched reliable-update iteration");
+    return CIECU_OK;
+}
+
+int build_reliable_graph(ciecu_batch_s* B, const double* b) {
+    if (B->relGraph && B->relB == b) return CIECU_OK;
+    if (B->relGraph) {
+        cudaGraphExecDestroy(B->relGraph);
+        B->relGraph = nullptr;
+    }
+    B->relB = b;
+    cudaStream_t st = B->A->space->stream;
+    if (!B->side) CIECU_CUDA(cudaStreamCreateWithFlags(&B->side, cudaStreamNonBlocking));
+    if (device_loop_enabled()) {
+        const int status = build_while_graph(st, [&](cudaGraph_t root, cudaGraphConditionalHandle cond) {
+            return launch_reliable_iteration<true>(B, st, root, cond);
+        }, &B->relGraph);
+        if (status == CIECU_OK) {
+            B->relDeviceLoop = true;
+            return CIECU_OK;
+        }
+        cudaGetLastError();
+    }
+    B->relDeviceLoop = false;
+    cudaGraph_t g = nullptr;
+    CIECU_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int status = CIECU_OK;
+    for (int i = 0; i < B->chunk && status == CIECU_OK; ++i)
+        status = launch_reliable_iteration<false>(B, st, nullptr, 0);
+    cudaError_t e = cudaStreamEndCapture(st, &g);
+    if (status != CIECU_OK) {
+        if (g) cudaGraphDestroy(g);
+        return status;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "batched reliable-update graph capture");
+    e = cudaGraphInstantiate(&B->relGraph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(e, "batched reliable-update graph instantiate");
+    return CIECU_OK;
+}
+
+// The reliable-update solve from x64 (the initial guesses): the set-up residual
+// of every system, p32 = D^-1 r32, then the graph until every system is done.
+int reliable_solve(ciecu_batch_s* B, const double* b, const BatchGlobal& g0, std::vector<BatchScalars>& s) {
+    cudaStream_t st = B->A->space->stream;
+    Level<float>& F = B->f32;
+    *B->h_g = g0;
+    B->h_g->delta = B->reliableDelta;
+    CIECU_CUDA(cudaMemcpyAsync(B->d_g, B->h_g, sizeof(BatchGlobal), cudaMemcpyHostToDevice, st));
+    CIECU_CUDA(cudaMemsetAsync(F.x, 0, sizeof(float) * std::max<long>(1, B->n), st));
+    CIECU_TRY(launch_true_residual<true>(B, st, b));
+    batch_direction_rel_kernel<false><<<B->grid, kT, 0, st>>>(B->d_tiles, B->ntiles, B->systems, F.p, F.r, F.dinv,
+                                                              B->d_s, B->d_g, 0);
+    count_launch(2);
+    CIECU_CHECK_LAUNCH("batched reliable-update set-up");
+    CIECU_TRY(build_reliable_graph(B, b));
+    const long long limit = B->relDeviceLoop ? 4096 : B->chunk;
+    for (;;) {
+        CIECU_CUDA(cudaMemcpyAsync(B->h_g, B->d_g, sizeof(BatchGlobal), cudaMemcpyDeviceToHost, st));
+        CIECU_CUDA(cudaStreamSynchronize(st));
+        if (B->h_g->finished >= static_cast<unsigned>(B->systems)) break;
+        const long long before = B->h_g->replacements;
+        B->h_g->chunkIter = 0;
+        B->h_g->chunkLimit = limit;
+        CIECU_CUDA(cudaMemcpyAsync(&B->d_g->chunkIter, &B->h_g->chunkIter, 2 * sizeof(long long),
+                                   cudaMemcpyHostToDevice, st));
+        CIECU_CUDA(cudaGraphLaunch(B->relGraph, st));
+        CIECU_CUDA(cudaMemcpyAsync(B->h_g, B->d_g, sizeof(BatchGlobal), cudaMemcpyDeviceToHost, st));
+        CIECU_CUDA(cudaStreamSynchronize(st));
+        count_launch(B->relDeviceLoop ? 3LL * B->h_g->chunkIter + 2LL * (B->h_g->replacements - before)
+                                      : 5LL * B->chunk);
+        if (B->h_g->finished >= static_cast<unsigned>(B->systems)) break;
+    }
+    CIECU_CUDA(cudaMemcpyAsync(s.data(), B->d_s, sizeof(BatchScalars) * B->systems, cudaMemcpyDeviceToHost, st));
+    CIECU_CUDA(cudaStreamSynchronize(st));
+    return CIECU_OK;
+}
+
 }  // namespace
 }  // namespace ciecu
 
@@ -645,6 +1025,8 @@ int ciecu_batch_destroy(ciecu_batch B) {
     if (!B) return CIECU_OK;
     if (B->f64.graph) cudaGraphExecDestroy(B->f64.graph);
     if (B->f32.graph) cudaGraphExecDestroy(B->f32.graph);
+    if (B->relGraph) cudaGraphExecDestroy(B->relGraph);
+    if (B->side) cudaStreamDestroy(B->side);
     cudaFree(B->d_tiles);
     cudaFree(B->d_tileBegin);
     cudaFree(B->d_tileCount);
@@ -675,26 +1057,24 @@ int ciecu_batch_set_refinement(ciecu_batch B, double innerTolerance) {
     CIECU_REQUIRE(B, "batch_set_refinement: null solver");
     CIECU_REQUIRE(innerTolerance >= 0.0 && innerTolerance < 1.0, "batch_set_refinement: tolerance must be in [0, 1)");
     B->innerTolerance = innerTolerance;
-    if (innerTolerance == 0.0 || B->val32) return CIECU_OK;
-    cudaStream_t st = B->A->space->stream;
-    const size_t n = static_cast<size_t>(std::max<long>(1, B->n));
-    cudaError_t e = cudaMalloc(&B->val32, sizeof(float) * std::max<long>(1, B->A->nnz));
-    if (e == cudaSuccess) e = cudaMalloc(&B->dinv32, sizeof(float) * n);
-    if (e == cudaSuccess) e = cudaMalloc(&B->norm2, sizeof(double) * B->systems);
-    for (float** v : {&B->f32.x, &B->f32.r, &B->f32.p, &B->f32.q})
-        if (e == cudaSuccess) e = cudaMalloc(v, sizeof(float) * n);
-    if (e == cudaSuccess && B->A->nnz > 0) {
-        batch_to_f32_kernel<<<grid_for(B->A->nnz, kT, 8), kT, 0, st>>>(
-            B->A->nnz, static_cast<const double*>(B->A->val), B->val32);
-        batch_to_f32_kernel<<<grid_for(B->n, kT, 8), kT, 0, st>>>(B->n, B->f64.dinv, B->dinv32);
-        count_launch(2);
-        e = cudaGetLastError();
-    }
-    if (e != cudaSuccess) return cuda_fail(e, "batch_set_refinement: FP32 copies");
-    B->f32.A = CsrArgs<float>{B->A->rowptr, B->A->col, B->val32, B->A->rows, B->A->nnz, B->A->d_blocks,
-                              B->A->nblocks, nullptr, 0, B->A->aligned16};
-    B->f32.dinv = B->dinv32;
-    return tune_batch(B, B->f32);
+    if (innerTolerance == 0.0) return CIECU_OK;
+    return ensure_f32(B);
+}
+
+int ciecu_batch_set_reliable_updates(ciecu_batch B, double delta) {
+    CIECU_REQUIRE(B, "batch_set_reliable_updates: null solver");
+    CIECU_REQUIRE(delta == 0.0 || (delta > 0.0 && delta < 1.0),
+                  "batch_set_reliable_updates: delta must be 0 or in (0, 1)");
+    B->reliableDelta = delta;
+    if (delta == 0.0) return CIECU_OK;
+    return ensure_f32(B);
+}
+
+int ciecu_batch_refinements(ciecu_batch B, int64_t* h_perSystem) {
+    CIECU_REQUIRE(B && h_perSystem, "batch_refinements: null argument");
+    for (int i = 0; i < B->systems; ++i)
+        h_perSystem[i] = i < static_cast<int>(B->lastRefinements.size()) ? B->lastRefinements[i] : 0;
+    return CIECU_OK;
 }
 
 int ciecu_batch_product(ciecu_batch B, double inScale, const double* d_in, double outScale, double* d_out,
@@ -716,9 +1096,22 @@ int ciecu_batch_product(ciecu_batch B, double inScale, const double* d_in, doubl
         g.absTol = B->settings.absoluteResidual;
         g.relTol = B->settings.relativeResidual;
         g.badColumn = 0x7fffffff;
-        CIECU_CUDA(cudaMemcpyAsync(L.r, d_in, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-        CIECU_TRY(ciecu_csr_spmv_f64(A, 1.0, L.x, -1.0, L.r));  // r = b - A x0 (block diagonal: per system)
-        if (B->innerTolerance == 0.0) {
+        if (B->reliableDelta == 0.0) {
+            CIECU_CUDA(cudaMemcpyAsync(L.r, d_in, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+            CIECU_TRY(ciecu_csr_spmv_f64(A, 1.0, L.x, -1.0, L.r));  // r = b - A x0 (block diagonal: per system)
+        }
+        if (B->reliableDelta > 0.0) {
+            CIECU_TRY(reliable_solve(B, d_in, g, s));
+            B->lastRefinements.assign(static_cast<size_t>(B->systems), 0);
+            for (int i = 0; i < B->systems; ++i) {
+                out[i] = ciecu_statistics{s[i].done == 3 ? s[i].errorIter : s[i].iter, s[i].absres, s[i].relres};
+                B->lastRefinements[i] = s[i].refinements;
+                if (s[i].done == 3) {
+                    failedKind[i] = s[i].errorKind;
+                    failedIter[i] = s[i].errorIter;
+                }
+            }
+        } else if (B->innerTolerance == 0.0) {
             // FP64: every system runs ConjugateGradients_impl.hpp:49-201 as it is
             CIECU_CUDA(cudaMemsetAsync(B->d_s, 0, sizeof(BatchScalars) * B->systems, st));
             CIECU_TRY(run_level(B, L, g, 0u));

@@ -132,6 +132,75 @@ int dia_fill_f32(const ciecu_csr_s* csr, const DiaArgs<float>& a, float* out, co
     return CIECU_OK;
 }
 
+// Counts the stored pairs (r, r + o), o > 0, whose mirror (r + o, r) differs in
+// any bit: diagonal d (offset o) at row r against diagonal m (offset -o) at row
+// r + o.
+template <typename V>
+__global__ void dia_symmetry_kernel(DiaArgs<V> a, unsigned* bad) {
+    const int half = a.ndiag / 2;
+    for (int k = 1; k <= half; ++k) {
+        const int d = half + k, m = half - k;
+        const int o = a.off[d];
+        const V* up = a.val + static_cast<long>(d) * a.ld;
+        const V* lo = a.val + static_cast<long>(m) * a.ld;
+        for (long r = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; r + o < a.nrows;
+             r += static_cast<long>(gridDim.x) * blockDim.x) {
+            const bool same = sizeof(V) == 8 ? __double_as_longlong(static_cast<double>(up[r])) ==
+                                                   __double_as_longlong(static_cast<double>(lo[r + o]))
+                                             : __float_as_uint(static_cast<float>(up[r])) ==
+                                                   __float_as_uint(static_cast<float>(lo[r + o]));
+            if (!same) atomicAdd(bad, 1u);
+        }
+    }
+}
+
+template <typename V>
+int dia_symmetric(const DiaArgs<V>& full, cudaStream_t st, unsigned* d_flag, bool* symmetric) {
+    *symmetric = false;
+    const int nd = full.ndiag;
+    if (nd < 3 || nd % 2 == 0 || full.off[nd / 2] != 0) return CIECU_OK;
+    for (int k = 1; k <= nd / 2; ++k)
+        if (full.off[nd / 2 + k] != -full.off[nd / 2 - k]) return CIECU_OK;
+    unsigned bad = 0;
+    CIECU_CUDA(cudaMemsetAsync(d_flag, 0, sizeof(unsigned), st));
+    dia_symmetry_kernel<V><<<grid_for(full.nrows, 256, 8), 256, 0, st>>>(full, d_flag);
+    count_launch();
+    CIECU_CHECK_LAUNCH("dia_symmetry_kernel");
+    CIECU_CUDA(cudaMemcpyAsync(&bad, d_flag, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    CIECU_CUDA(cudaStreamSynchronize(st));
+    *symmetric = bad == 0;
+    return CIECU_OK;
+}
+template int dia_symmetric<float>(const DiaArgs<float>&, cudaStream_t, unsigned*, bool*);
+template int dia_symmetric<double>(const DiaArgs<double>&, cudaStream_t, unsigned*, bool*);
+
+int dia_symmetric_upper_f32(const DiaArgs<float>& full, DiaArgs<float>* upper, float** upperVal, cudaStream_t st,
+                            unsigned* d_flag, bool* symmetric) {
+    *upperVal = nullptr;
+    CIECU_TRY(dia_symmetric(full, st, d_flag, symmetric));
+    if (!*symmetric) return CIECU_OK;
+    DiaArgs<float> u = dia_upper_view(full);
+    const size_t bytes = sizeof(float) * static_cast<size_t>(u.ndiag) * static_cast<size_t>(u.ld);
+    float* val = nullptr;
+    if (cudaMalloc(&val, bytes) != cudaSuccess) {
+        cudaGetLastError();  // no room: the full copy stays
+        *symmetric = false;
+        return CIECU_OK;
+    }
+    // the upper half (main diagonal first) is contiguous in the full copy
+    cudaError_t e = cudaMemcpyAsync(val, u.val, bytes, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        cudaFree(val);
+        *symmetric = false;
+        return cuda_fail(e, "DIA upper half");
+    }
+    u.val = val;
+    *upper = u;
+    *upperVal = val;
+    return CIECU_OK;
+}
+
 }  // namespace ciecu
 
 extern "C" int ciecu_csr_diagonals(ciecu_csr csr, int* ndiag) {

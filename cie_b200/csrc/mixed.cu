@@ -36,6 +36,7 @@
 #include "dia.cuh"
 #include "sell_tma.cuh"
 
+#include <cstdlib>
 #include <string>
 #include <vector>
 #include <tuple>
@@ -47,6 +48,7 @@ namespace {
 
 constexpr int kT = 256;
 constexpr int kDiaInner = -2;  // innerKernel / unroll code of the DIA inner kernels
+
 
 struct MixedScalars {
     double rz, pq, alpha, beta, rzPending;
@@ -239,15 +241,24 @@ __global__ void __launch_bounds__(kT) mixed_spmv_kernel(SellArgs<float, CI> A, c
 }
 
 // DIA variants of the two kernels above, for inner matrices of at most 32
-// diagonals (dia.cuh): FP32 values only, no column indices.
-template <int ND>
+// diagonals (dia.cuh): FP32 values only, no column indices.  SYM: A holds the
+// upper half of a symmetric matrix (ND = its diagonal count, main included).
+template <int ND, bool SYM, typename Op>
+__device__ __forceinline__ void mixed_dia_rows(const DiaArgs<float>& A, const float* __restrict__ x, Op& op) {
+    if constexpr (SYM)
+        dia_rows4_sym<ND>(A, x, op);
+    else
+        dia_rows4<ND>(A, x, op);
+}
+
+template <int ND, bool SYM>
 __global__ void __launch_bounds__(kT) mixed_apply_dia_kernel(DiaArgs<float> A, const float* __restrict__ x,
                                                             float* __restrict__ y) {
     StoreOp op{y};
-    dia_rows4<ND>(A, x, op);
+    mixed_dia_rows<ND, SYM>(A, x, op);
 }
 
-template <int ND, bool COND, bool FUSED>
+template <int ND, bool COND, bool FUSED, bool SYM>
 __global__ void __launch_bounds__(kT) mixed_spmv_dia_kernel(DiaArgs<float> A, const float* __restrict__ x,
                                                            float* __restrict__ p, float* __restrict__ q,
                                                            MixedScalars* s, double* partials, unsigned* counter,
@@ -257,7 +268,7 @@ __global__ void __launch_bounds__(kT) mixed_spmv_dia_kernel(DiaArgs<float> A, co
         return;
     }
     auto op = M1Op<FUSED>::make(x, p, q, s);
-    dia_rows4<ND>(A, x, op);
+    mixed_dia_rows<ND, SYM>(A, x, op);
     double mine[1] = {op.acc}, tot[1];
     if (grid_reduce_last<1, kT>(mine, partials, counter, tot) && threadIdx.x == 0) {
         s->pq = tot[0];
@@ -580,6 +591,7 @@ struct ciecu_mixed_s {
                      // kDiaInner = the DIA copy)
     bool sellBuilt = false;  // the SELL copy exists (not built when the DIA copy is the known choice)
     float* dia32 = nullptr;  // DIA copy of the inner matrix (few-diagonal matrices only)
+    bool diaSym = false;     // dia32 holds the upper half of a bitwise symmetric matrix
     ciecu::DiaArgs<float> dia{};
     // SELL-32 inner matrix
     int nslices = 0;
@@ -629,13 +641,18 @@ int launch_inner_spmv_form(ciecu_mixed_s* M, cudaStream_t st, cudaGraphCondition
     const long needA = (M->n + kT - 1) / kT;
     const float* x = FUSED ? M->z32 : M->p32;
     if (M->unroll == kDiaInner) {
-        CIECU_TRY(with_diagonals(M->dia.ndiag, [&](auto nd) -> int {
+        auto go = [&](auto nd, auto sym) -> int {
             constexpr int ND = decltype(nd)::value;
-            auto* kernel = mixed_spmv_dia_kernel<ND, COND, FUSED>;
+            constexpr bool SYM = decltype(sym)::value;
+            auto* kernel = mixed_spmv_dia_kernel<ND, COND, FUSED, SYM>;
             kernel<<<fit_grid(kernel, kT, (needA + 3) / 4), kT, 0, st>>>(M->dia, x, M->p32, M->q32, M->d_s,
                                                                          M->d_partials, M->d_counter, loop);
             return CIECU_OK;
-        }));
+        };
+        if (M->diaSym)
+            CIECU_TRY(with_upper_diagonals(M->dia.ndiag, [&](auto nd) { return go(nd, std::true_type{}); }));
+        else
+            CIECU_TRY(with_diagonals(M->dia.ndiag, [&](auto nd) { return go(nd, std::false_type{}); }));
         CIECU_CHECK_LAUNCH("mixed_spmv_dia_kernel");
         return CIECU_OK;
     }
@@ -919,6 +936,21 @@ int ciecu_mixed_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_sta
                 M->dia = a;
                 if (e == cudaSuccess) status = dia_fill_f32(lhs, M->dia, M->dia32, M->sdiag, st);
                 if (e != cudaSuccess) status = cuda_fail(e, "mixed_create: DIA copy");
+                // a bitwise symmetric copy keeps only its upper half (about half the
+                // bytes per SpMV; the lower terms are read back through L2)
+                if (status == CIECU_OK && dia_symmetric_enabled()) {
+                    DiaArgs<float> upper{};
+                    float* uval = nullptr;
+                    bool sym = false;
+                    status = dia_symmetric_upper_f32(M->dia, &upper, &uval, st,
+                                                     reinterpret_cast<unsigned*>(lhs->space->d_result), &sym);
+                    if (status == CIECU_OK && sym) {
+                        cudaFree(M->dia32);
+                        M->dia32 = uval;
+                        M->dia = upper;
+                        M->diaSym = true;
+                    }
+                }
             } else {
                 cudaGetLastError();  // no room for the copy: the SELL kernels stay
                 M->dia32 = nullptr;
@@ -1075,12 +1107,17 @@ int ciecu_mixed_apply_f32(ciecu_mixed M, const float* d_in, float* d_out) {
     cudaStream_t st = M->A->space->stream;
     const long need = (M->n + kT - 1) / kT;
     if (M->unroll == kDiaInner) {
-        CIECU_TRY(with_diagonals(M->dia.ndiag, [&](auto nd) -> int {
+        auto go = [&](auto nd, auto sym) -> int {
             constexpr int ND = decltype(nd)::value;
-            mixed_apply_dia_kernel<ND><<<fit_grid(mixed_apply_dia_kernel<ND>, kT, (need + 3) / 4), kT, 0, st>>>(
-                M->dia, d_in, d_out);
+            constexpr bool SYM = decltype(sym)::value;
+            auto* kernel = mixed_apply_dia_kernel<ND, SYM>;
+            kernel<<<fit_grid(kernel, kT, (need + 3) / 4), kT, 0, st>>>(M->dia, d_in, d_out);
             return CIECU_OK;
-        }));
+        };
+        if (M->diaSym)
+            CIECU_TRY(with_upper_diagonals(M->dia.ndiag, [&](auto nd) { return go(nd, std::true_type{}); }));
+        else
+            CIECU_TRY(with_diagonals(M->dia.ndiag, [&](auto nd) { return go(nd, std::false_type{}); }));
         count_launch();
         CIECU_CHECK_LAUNCH("mixed_apply_dia_kernel");
         return CIECU_OK;
@@ -1119,6 +1156,13 @@ int ciecu_mixed_apply_f32(ciecu_mixed M, const float* d_in, float* d_out) {
 int ciecu_mixed_padded_entries(ciecu_mixed M, int64_t* h_entries) {
     CIECU_REQUIRE(M && h_entries, "mixed_padded_entries: null argument");
     *h_entries = M->paddedEntries;
+    return CIECU_OK;
+}
+
+int ciecu_mixed_dia_info(ciecu_mixed M, int* storedDiagonals, int* symmetric) {
+    CIECU_REQUIRE(M && storedDiagonals && symmetric, "mixed_dia_info: null argument");
+    *storedDiagonals = M->dia32 ? M->dia.ndiag : 0;
+    *symmetric = M->diaSym ? 1 : 0;
     return CIECU_OK;
 }
 

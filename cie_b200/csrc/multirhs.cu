@@ -22,6 +22,9 @@
 #include "ciecu_multi.h"
 
 #include <algorithm>
+#include <cstdlib>
+#include <cstdint>
+#include <type_traits>
 #include <string>
 #include <vector>
 
@@ -732,6 +735,280 @@ __global__ void __launch_bounds__(kT) multi_direction32_kernel(long n, int k, fl
     }
 }
 
+// ---- k = 32: four columns per lane ---------------------------------------------
+//
+// With 32 right-hand sides a lane of the row-per-warp engines above issues one
+// 4- or 8-byte gather and one FMA per entry, so the SpMM is bound by instruction
+// issue, not by memory.  Here a lane keeps four consecutive columns (one 16-byte
+// load for FP32, two for FP64): eight lanes cover a row's 32 columns and a warp
+// works on four rows at once, so each gather instruction moves four times the
+// bytes and the matrix value is loaded once per eight lanes.  The entries of a
+// row are summed in the same order as above (CSR order / ascending diagonals),
+// so the sums are the same.
+
+template <typename T>
+struct Quad;
+template <>
+struct Quad<float> {
+    static __device__ __forceinline__ void load(const float* p, float (&v)[4]) {
+        const float4 a = __ldg(reinterpret_cast<const float4*>(p));
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    }
+    static __device__ __forceinline__ void load_plain(const float* p, float (&v)[4]) {
+        const float4 a = *reinterpret_cast<const float4*>(p);
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    }
+    static __device__ __forceinline__ void store(float* p, const float (&v)[4]) {
+        *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+    }
+};
+template <>
+struct Quad<double> {
+    static __device__ __forceinline__ void load(const double* p, double (&v)[4]) {
+        const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+        const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+        v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+    }
+    static __device__ __forceinline__ void load_plain(const double* p, double (&v)[4]) {
+        const double2 a = *reinterpret_cast<const double2*>(p);
+        const double2 b = *(reinterpret_cast<const double2*>(p) + 1);
+        v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+    }
+    static __device__ __forceinline__ void store(double* p, const double (&v)[4]) {
+        reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+        reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+    }
+};
+
+constexpr int kQuadLanes = 8;                 // lanes per row
+constexpr int kQuadRows = 32 / kQuadLanes;    // rows per warp
+
+// CSR rows of the row blocks (staged as in multi_rows); op.quad(row, c0, acc)
+// receives columns c0 .. c0 + 3 of the row.
+template <typename V, typename T, typename Op>
+__device__ __forceinline__ void quad_rows(const CsrArgs<V>& A, const T* __restrict__ X, Op& op) {
+    __shared__ Entry s_e[kStreamTile];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int slot = lane / kQuadLanes, c0 = (lane % kQuadLanes) * 4;
+    const T* __restrict__ xc = X + c0;
+    for (int b = blockIdx.x; b < A.nblocks; b += gridDim.x) {
+        const int r0 = A.blocks[b], r1 = A.blocks[b + 1];
+        const int e0 = A.rowptr[r0], e1 = A.rowptr[r1];
+        const bool staged = e1 - e0 <= kStreamTile;
+        if (staged) {
+            for (int j = threadIdx.x; j < e1 - e0; j += kT)
+                s_e[j] = Entry{static_cast<double>(stream_ld(A.val + e0 + j)), stream_ld(A.col + e0 + j), 0};
+            __syncthreads();
+        }
+        for (int rbase = r0 + warp * kQuadRows; rbase < r1; rbase += kWarps * kQuadRows) {
+            const int row = rbase + slot;
+            if (row >= r1) continue;
+            const int k0 = A.rowptr[row] - e0, k1 = A.rowptr[row + 1] - e0;
+            T acc[4] = {T(0), T(0), T(0), T(0)};
+            if (staged) {
+                int j = k0;
+                for (; j + 2 <= k1; j += 2) {
+                    double a0, a1;
+                    int col0, col1;
+                    load_entry(s_e + j, a0, col0);
+                    load_entry(s_e + j + 1, a1, col1);
+                    T x0[4], x1[4];
+                    Quad<T>::load(xc + static_cast<long>(col0) * 32, x0);
+                    Quad<T>::load(xc + static_cast<long>(col1) * 32, x1);
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) acc[u] = fma(static_cast<T>(a0), x0[u], acc[u]);
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) acc[u] = fma(static_cast<T>(a1), x1[u], acc[u]);
+                }
+                if (j < k1) {
+                    double a;
+                    int col;
+                    load_entry(s_e + j, a, col);
+                    T xv[4];
+                    Quad<T>::load(xc + static_cast<long>(col) * 32, xv);
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) acc[u] = fma(static_cast<T>(a), xv[u], acc[u]);
+                }
+            } else {
+                for (int j = e0 + k0; j < e0 + k1; ++j) {
+                    T xv[4];
+                    Quad<T>::load(xc + static_cast<long>(A.col[j]) * 32, xv);
+                    const T a = static_cast<T>(A.val[j]);
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) acc[u] = fma(a, xv[u], acc[u]);
+                }
+            }
+            op.quad(row, c0, acc);
+        }
+        if (staged) __syncthreads();
+    }
+}
+
+// DIA rows (diagonals in ascending order = the CSR column order).
+template <typename V, typename T, typename Op>
+__device__ __forceinline__ void quad_rows(const DiaArgs<V>& D, const T* __restrict__ X, Op& op) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int slot = lane / kQuadLanes, c0 = (lane % kQuadLanes) * 4;
+    const T* __restrict__ xc = X + c0;
+    const long stride = static_cast<long>(gridDim.x) * kWarps * kQuadRows;
+    for (long row = (static_cast<long>(blockIdx.x) * kWarps + warp) * kQuadRows + slot; row < D.nrows;
+         row += stride) {
+        T acc[4] = {T(0), T(0), T(0), T(0)};
+#pragma unroll 3
+        for (int d = 0; d < D.ndiag; ++d) {
+            const long col = row + D.off[d];
+            const T a = static_cast<T>(stream_ld(D.val + static_cast<long>(d) * D.ld + row));
+            if (static_cast<unsigned long>(col) < static_cast<unsigned long>(D.nrows)) {
+                T xv[4];
+                Quad<T>::load(xc + col * 32, xv);
+#pragma unroll
+                for (int u = 0; u < 4; ++u) acc[u] = fma(a, xv[u], acc[u]);
+            } else {
+#pragma unroll
+                for (int u = 0; u < 4; ++u) acc[u] = fma(a, T(0), acc[u]);
+            }
+        }
+        op.quad(row, c0, acc);
+    }
+}
+
+// Per-column totals of four-column partial sums (thread: columns c0 .. c0+3 of
+// its rows): summed over the warp's four row slots, then lane c takes column c,
+// and the column reduction of the row-per-warp kernels finishes the job.
+template <int NV>
+__device__ __forceinline__ bool quad_reduce_last(double (&part)[NV][4], double* partials, unsigned* counter,
+                                                 double (&out)[NV]) {
+    const int lane = threadIdx.x & 31;
+    double mine[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        double t[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            double x = part[v][u];
+            x += __shfl_xor_sync(0xffffffffu, x, 8);
+            x += __shfl_xor_sync(0xffffffffu, x, 16);
+            t[u] = __shfl_sync(0xffffffffu, x, lane >> 2);  // lane (slot 0, group lane / 4)
+        }
+        const int u = lane & 3;
+        mine[v] = u == 0 ? t[0] : u == 1 ? t[1] : u == 2 ? t[2] : t[3];
+    }
+    return column_reduce_last<32, NV>(mine, 32, partials, counter, out);
+}
+
+template <typename T>
+struct PqQuad {
+    const T* __restrict__ p;
+    T* __restrict__ q;
+    double acc[1][4];
+    __device__ __forceinline__ void quad(long row, int c0, const T (&sum)[4]) {
+        Quad<T>::store(q + row * 32 + c0, sum);
+        T pv[4];
+        Quad<T>::load_plain(p + row * 32 + c0, pv);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) acc[0][u] = fma(static_cast<double>(pv[u]), static_cast<double>(sum[u]), acc[0][u]);
+    }
+};
+
+struct ResidualQuad {  // R = B - A X
+    const double* __restrict__ b;
+    double* __restrict__ r;
+    __device__ __forceinline__ void quad(long row, int c0, const double (&sum)[4]) {
+        double bv[4], rv[4];
+        Quad<double>::load_plain(b + row * 32 + c0, bv);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) rv[u] = bv[u] - sum[u];
+        Quad<double>::store(r + row * 32 + c0, rv);
+    }
+};
+
+struct TrueResidualQuad {
+    const double* __restrict__ b;
+    const float* __restrict__ dinv;
+    float* __restrict__ r32;
+    const ColumnScalars* S;
+    bool init;
+    double acc[2][4];
+    __device__ __forceinline__ void quad(long row, int c0, const double (&sum)[4]) {
+        double bv[4];
+        Quad<double>::load_plain(b + row * 32 + c0, bv);
+        const float d = dinv[row];
+        float rf[4];
+        float old[4];
+        Quad<float>::load_plain(r32 + row * 32 + c0, old);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const bool take = init || S[c0 + u].pending;
+            const double ri = bv[u] - sum[u];
+            rf[u] = take ? static_cast<float>(ri) : old[u];
+            if (take) {
+                acc[0][u] = fma(ri, ri, acc[0][u]);
+                acc[1][u] = fma(static_cast<double>(rf[u]), static_cast<double>(rf[u] * d), acc[1][u]);
+            }
+        }
+        Quad<float>::store(r32 + row * 32 + c0, rf);
+    }
+};
+
+// K1 for k = 32 over either format; FP64 (the plain form) or FP32 (the refined
+// form, whose breakdowns restart).
+template <typename MA, typename T, bool COND>
+__global__ void __launch_bounds__(kT) multi_spmv_quad_kernel(MA A, const T* __restrict__ P, T* __restrict__ Q,
+                                                             ColumnScalars* S, MultiGlobal* g, double* partials,
+                                                             unsigned* counter, cudaGraphConditionalHandle cond) {
+    if (*reinterpret_cast<volatile unsigned*>(&g->finished) >= 32u) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) set_loop<COND>(cond, 0);
+        return;
+    }
+    PqQuad<T> op{P, Q, {{0.0, 0.0, 0.0, 0.0}}};
+    quad_rows(A, P, op);
+    double tot[1];
+    if (quad_reduce_last<1>(op.acc, partials, counter, tot) && threadIdx.x < 32) {
+        ColumnScalars& s = S[threadIdx.x];
+        if (std::is_same<T, float>::value) {
+            column_pq(s, tot[0], g);
+        } else if (!s.done) {
+            s.pq = tot[0];
+            if (!(0.0 < tot[0])) {
+                s.done = 3;
+                s.errorKind = 2;
+                s.errorIter = s.iter;
+                atomicAdd(&g->finished, 1u);
+            } else {
+                s.alpha = s.rz / tot[0];
+            }
+        }
+    }
+}
+
+template <typename MA>
+__global__ void __launch_bounds__(kT) multi_residual_quad_kernel(MA A, const double* __restrict__ X,
+                                                                 const double* __restrict__ B, double* __restrict__ R) {
+    ResidualQuad op{B, R};
+    quad_rows(A, X, op);
+}
+
+template <typename MA, bool INIT>
+__global__ void __launch_bounds__(kT) multi_true_residual_quad_kernel(MA A, const double* __restrict__ X,
+                                                                      const double* __restrict__ B,
+                                                                      const float* __restrict__ dinv,
+                                                                      float* __restrict__ R32, ColumnScalars* S,
+                                                                      MultiGlobal* g, double* partials,
+                                                                      unsigned* counter) {
+    if (!INIT && !*reinterpret_cast<volatile unsigned*>(&g->anyPending)) return;
+    TrueResidualQuad op{B, dinv, R32, S, INIT, {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}}};
+    quad_rows(A, X, op);
+    double tot[2];
+    if (quad_reduce_last<2>(op.acc, partials, counter, tot)) {
+        if (threadIdx.x < 32) column_replace<INIT>(S[threadIdx.x], tot, g);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            g->anyPending = 0u;
+            if (!INIT) g->replacements += 1;
+        }
+    }
+}
+
 __global__ void multi_to_f32_kernel(long n, const double* __restrict__ a, float* __restrict__ b) {
     const long stride = static_cast<long>(gridDim.x) * blockDim.x;
     for (long i = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
@@ -808,16 +1085,34 @@ struct ciecu_multi_s {
     cudaStream_t side = nullptr;  // captures the IF body of the replacement
     const double* graphB = nullptr;  // right-hand sides the refined graph reads
     std::vector<ciecu::ColumnScalars> last;  // column state of the last solve
+    // k = 32: the four-columns-per-lane SpMM kernels (grids per format and precision)
+    bool quad = false;
+    int gridQ = 1, gridQD = 1, gridQ32 = 1, gridQ32D = 1;
 };
 
 namespace ciecu {
 namespace {
 
+// CIECU_MULTI_QUAD=0 keeps the row-per-warp SpMM for k = 32 (for comparison).
+bool quad_enabled() {
+    static const bool enabled = [] {
+        const char* v = std::getenv("CIECU_MULTI_QUAD");
+        return !(v && v[0] == '0');
+    }();
+    return enabled;
+}
+
 template <bool COND>
 int launch_multi_iteration(ciecu_multi_s* M, cudaStream_t st, cudaGraphConditionalHandle cond) {
     CIECU_TRY(with_group(M->kp, [&](auto kk) -> int {
         constexpr int KP = decltype(kk)::value;
-        if (M->useDia && M->k == KP)
+        if (M->quad && M->useDia)
+            multi_spmv_quad_kernel<DiaArgs<double>, double, COND><<<M->gridQD, kT, 0, st>>>(
+                M->dia, M->p, M->q, M->d_s, M->d_g, M->d_partials, M->d_counter, cond);
+        else if (M->quad)
+            multi_spmv_quad_kernel<CsrArgs<double>, double, COND><<<M->gridQ, kT, 0, st>>>(
+                M->A->args<double>(), M->p, M->q, M->d_s, M->d_g, M->d_partials, M->d_counter, cond);
+        else if (M->useDia && M->k == KP)
             multi_spmv_dia_kernel<KP, true, COND><<<M->gridD, kT, 0, st>>>(M->dia, M->k, M->p, M->q, M->d_s, M->d_g,
                                                                            M->d_partials, M->d_counter, cond);
         else if (M->useDia)
@@ -845,7 +1140,11 @@ int launch_multi_iteration(ciecu_multi_s* M, cudaStream_t st, cudaGraphCondition
 int launch_multi_residual(ciecu_multi_s* M, cudaStream_t st, bool dia, const double* B) {
     return with_group(M->kp, [&](auto kk) -> int {
         constexpr int KP = decltype(kk)::value;
-        if (dia && M->k == KP)
+        if (M->quad && dia)
+            multi_residual_quad_kernel<DiaArgs<double>><<<M->gridQD, kT, 0, st>>>(M->dia, M->x, B, M->r);
+        else if (M->quad)
+            multi_residual_quad_kernel<CsrArgs<double>><<<M->gridQ, kT, 0, st>>>(M->A->args<double>(), M->x, B, M->r);
+        else if (dia && M->k == KP)
             multi_residual_dia_kernel<KP, true><<<M->gridD, kT, 0, st>>>(M->dia, M->k, M->x, B, M->r);
         else if (dia)
             multi_residual_dia_kernel<KP, false><<<M->gridD, kT, 0, st>>>(M->dia, M->k, M->x, B, M->r);
@@ -953,7 +1252,13 @@ template <bool INIT>
 int launch_true_residual(ciecu_multi_s* M, cudaStream_t st, const double* B) {
     return with_group(M->kp, [&](auto kk) -> int {
         constexpr int KP = decltype(kk)::value;
-        if (M->useDia && M->k == KP)
+        if (M->quad && M->useDia)
+            multi_true_residual_quad_kernel<DiaArgs<double>, INIT><<<M->gridQD, kT, 0, st>>>(
+                M->dia, M->x, B, M->dinv32, M->r32, M->d_s, M->d_g, M->d_partials, M->d_counter);
+        else if (M->quad)
+            multi_true_residual_quad_kernel<CsrArgs<double>, INIT><<<M->gridQ, kT, 0, st>>>(
+                M->A->args<double>(), M->x, B, M->dinv32, M->r32, M->d_s, M->d_g, M->d_partials, M->d_counter);
+        else if (M->useDia && M->k == KP)
             multi_true_residual_dia_kernel<KP, true, INIT><<<M->gridD, kT, 0, st>>>(
                 M->dia, M->k, M->x, B, M->dinv32, M->r32, M->d_s, M->d_g, M->d_partials, M->d_counter);
         else if (M->useDia)
@@ -981,7 +1286,13 @@ int launch_multi_iteration32(ciecu_multi_s* M, cudaStream_t st, cudaGraph_t root
     if (COND) CIECU_CUDA(cudaGraphConditionalHandleCreate(&replace, root, 0, cudaGraphCondAssignDefault));
     CIECU_TRY(with_group(M->kp, [&](auto kk) -> int {
         constexpr int KP = decltype(kk)::value;
-        if (M->useDia && M->k == KP)
+        if (M->quad && M->useDia)
+            multi_spmv_quad_kernel<DiaArgs<float>, float, COND><<<M->gridQ32D, kT, 0, st>>>(
+                M->diaF, M->p32, M->q32, M->d_s, M->d_g, M->d_partials, M->d_counter, cond);
+        else if (M->quad)
+            multi_spmv_quad_kernel<CsrArgs<float>, float, COND><<<M->gridQ32, kT, 0, st>>>(
+                args32(M), M->p32, M->q32, M->d_s, M->d_g, M->d_partials, M->d_counter, cond);
+        else if (M->useDia && M->k == KP)
             multi_spmv32_dia_kernel<KP, true, COND><<<M->grid32D, kT, 0, st>>>(
                 M->diaF, M->k, M->p32, M->q32, M->d_s, M->d_g, M->d_partials, M->d_counter, cond);
         else if (M->useDia)
@@ -1201,7 +1512,19 @@ int ciecu_multi_create(ciecu_csr lhs, int rhsCount, const double* d_inverseDiago
     // partial sums for the widest grid of any kernel of either form (the DIA and
     // FP32 grids are fixed later, at most their resident blocks), so that the
     // buffer captured by a graph is never replaced
-    int widest = std::max(M->grid, M->gridV);
+    if (M->k == 32) {
+        const long rowsQ = (M->n + kWarps * kQuadRows - 1) / (kWarps * kQuadRows);
+        auto fit = [&](const void* k, long need) {
+            return static_cast<int>(std::max<long>(1, std::min<long>(need, resident_blocks(k, kT, 0))));
+        };
+        const long blocks = std::max<long>(1, lhs->nblocks);
+        M->gridQ = fit(reinterpret_cast<const void*>(multi_spmv_quad_kernel<CsrArgs<double>, double, true>), blocks);
+        M->gridQD = fit(reinterpret_cast<const void*>(multi_spmv_quad_kernel<DiaArgs<double>, double, true>), rowsQ);
+        M->gridQ32 = fit(reinterpret_cast<const void*>(multi_spmv_quad_kernel<CsrArgs<float>, float, true>), blocks);
+        M->gridQ32D = fit(reinterpret_cast<const void*>(multi_spmv_quad_kernel<DiaArgs<float>, float, true>), rowsQ);
+        M->quad = quad_enabled();
+    }
+    int widest = std::max({M->grid, M->gridV, M->gridQ, M->gridQD, M->gridQ32, M->gridQ32D});
     with_group(M->kp, [&](auto kk) -> int {
         constexpr int KP = decltype(kk)::value;
         for (const void* k : {reinterpret_cast<const void*>(multi_spmv_dia_kernel<KP, true, true>),
@@ -1247,7 +1570,7 @@ int ciecu_multi_destroy(ciecu_multi M) {
 
 int ciecu_multi_info(ciecu_multi M, int* lanesPerRow, int* deviceLoop) {
     CIECU_REQUIRE(M, "multi_info: null solver");
-    if (lanesPerRow) *lanesPerRow = M->kp;
+    if (lanesPerRow) *lanesPerRow = M->quad ? kQuadLanes : M->kp;
     if (deviceLoop) *deviceLoop = M->deviceLoop ? 1 : 0;
     return CIECU_OK;
 }
@@ -1275,6 +1598,18 @@ int ciecu_multi_format(ciecu_multi M, int* diagonals) {
 int ciecu_multi_product(ciecu_multi M, double inScale, const double* d_in, double outScale, double* d_out,
                         ciecu_statistics* h_stats) {
     CIECU_REQUIRE(M && d_in && d_out, "multi_product: null argument");
+    // the k = 32 kernels read the right-hand sides in 16-byte vectors
+    if (M->k == 32) {
+        const bool want = quad_enabled() && reinterpret_cast<std::uintptr_t>(d_in) % 16 == 0;
+        if (want != M->quad) {
+            M->quad = want;
+            for (cudaGraphExec_t* gr : {&M->graph, &M->graph32})
+                if (*gr) {
+                    cudaGraphExecDestroy(*gr);
+                    *gr = nullptr;
+                }
+        }
+    }
     cudaStream_t st = M->A->space->stream;
     const long n = M->n;
     const long count = n * M->k;

@@ -114,6 +114,33 @@ __global__ void __launch_bounds__(csr_threads<KERNEL>())
     }
 }
 
+// K1 over the upper half of the DIA copy of a bitwise symmetric matrix: half the
+// matrix bytes, the same row sums (dia_rows_sym).
+template <bool COND>
+__global__ void __launch_bounds__(kT) pcg_spmv_dia_sym_kernel(DiaArgs<double> U, const double* __restrict__ p,
+                                                             double* __restrict__ q, PcgScalars* s, double* partials,
+                                                             unsigned* counter, cudaGraphConditionalHandle cond) {
+    if (*reinterpret_cast<volatile int*>(&s->done)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) set_loop<COND>(cond, 0);
+        return;
+    }
+    PqOp op{p, q, 0.0};
+    dia_rows_sym<0, double, double>(U, p, op);
+    double mine[1] = {op.acc}, tot[1];
+    if (grid_reduce_last<1, kT>(mine, partials, counter, tot) && threadIdx.x == 0) {
+        s->pq = tot[0];
+        if (!(0.0 < tot[0])) {
+            s->done = 3;
+            s->error = CIECU_ERR_BREAKDOWN;
+            s->errorKind = 2;
+            s->errorIter = s->iter;
+            set_loop<COND>(cond, 0);
+        } else {
+            s->alpha = s->rz / tot[0];
+        }
+    }
+}
+
 // K1 over the DIA copy of a few-diagonal matrix (dia.cuh): no column indices,
 // 8 bytes per stored entry.
 template <int ND, bool COND>
@@ -575,6 +602,7 @@ struct ciecu_pcg_s {
     unsigned* d_counter = nullptr;
     cudaGraphExec_t graph = nullptr;
     int graphKernel = -1;
+    bool graphSym = false;  // the graph's K1 reads the upper half of the DIA copy
     bool deviceLoop = false;  // graph = WHILE loop (else `chunk` unrolled iterations)
     int kernel = 0;           // K1 schedule, autotuned on the fused SpMV kernel itself
     int chunk = 16;
@@ -583,6 +611,8 @@ struct ciecu_pcg_s {
     bool diaChecked = false;
     double* diaBuf = nullptr;
     ciecu::DiaArgs<double> dia{};
+    bool diaSym = false;           // the copy is bitwise symmetric: K1 reads diaU, its upper half
+    ciecu::DiaArgs<double> diaU{};
     // Single-launch solve (allocated at its first use).
     int loopMode = 0;     // 0 auto (single launch when the system fits in L2), 1 graph, 2 single launch
     bool persistent = false;  // the last solve ran as a single launch
@@ -617,8 +647,12 @@ int launch_k1(ciecu_pcg_s* S, cudaStream_t st, int schedule, cudaGraphConditiona
         // Runtime diagonal count (9 loads in flight per row): a fully unrolled
         // 27-diagonal FP64 row needs 64 registers and halves the occupancy, which
         // measured 20 % slower at 128^3.
-        pcg_spmv_dia_kernel<0, COND><<<fit_grid(pcg_spmv_dia_kernel<0, COND>, kT, (S->n + kT - 1) / kT), kT, 0, st>>>(
-            S->dia, S->p, S->q, S->d_s, S->d_partials, S->d_counter, cond);
+        if (S->diaSym)
+            pcg_spmv_dia_sym_kernel<COND><<<fit_grid(pcg_spmv_dia_sym_kernel<COND>, kT, (S->n + kT - 1) / kT), kT, 0,
+                                            st>>>(S->diaU, S->p, S->q, S->d_s, S->d_partials, S->d_counter, cond);
+        else
+            pcg_spmv_dia_kernel<0, COND><<<fit_grid(pcg_spmv_dia_kernel<0, COND>, kT, (S->n + kT - 1) / kT), kT, 0,
+                                           st>>>(S->dia, S->p, S->q, S->d_s, S->d_partials, S->d_counter, cond);
         return CIECU_OK;
     }
     const int needA = csr_grid(A, schedule);
@@ -651,7 +685,16 @@ int refresh_dia(ciecu_pcg_s* S, cudaStream_t st) {
             S->diaBuf = buf;
         }
     }
-    if (S->diaBuf) CIECU_TRY(dia_fill_f64(S->A, S->dia, S->diaBuf, st));
+    if (S->diaBuf) {
+        CIECU_TRY(dia_fill_f64(S->A, S->dia, S->diaBuf, st));
+        // a bitwise symmetric matrix (checked at every solve: the values may have
+        // changed) is read through the upper half of the copy only
+        bool sym = false;
+        if (dia_symmetric_enabled())
+            CIECU_TRY(dia_symmetric(S->dia, st, reinterpret_cast<unsigned*>(S->A->space->d_result), &sym));
+        S->diaSym = sym;
+        if (sym) S->diaU = dia_upper_view(S->dia);
+    }
     return CIECU_OK;
 }
 
@@ -901,7 +944,7 @@ int tune_solver_spmv(ciecu_pcg_s* S) {
 // host replays until the done flag is set.
 int build_graph(ciecu_pcg_s* S) {
     cudaStream_t st = S->A->space->stream;
-    if (S->graph && S->graphKernel == S->kernel) return CIECU_OK;
+    if (S->graph && S->graphKernel == S->kernel && S->graphSym == S->diaSym) return CIECU_OK;
     if (S->graph) {
         cudaGraphExecDestroy(S->graph);
         S->graph = nullptr;
@@ -914,6 +957,7 @@ int build_graph(ciecu_pcg_s* S) {
     if (status == CIECU_OK) {
         S->deviceLoop = true;
         S->graphKernel = S->kernel;
+        S->graphSym = S->diaSym;
         return CIECU_OK;
     }
     cudaGetLastError();  // clear a sticky launch error of the failed attempt
@@ -932,6 +976,7 @@ int build_graph(ciecu_pcg_s* S) {
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return cuda_fail(e, "pcg graph instantiate");
     S->graphKernel = S->kernel;
+    S->graphSym = S->diaSym;
     return CIECU_OK;
 }
 
@@ -1000,6 +1045,13 @@ int ciecu_pcg_info(ciecu_pcg S, int* spmvSchedule, int* deviceLoop) {
     CIECU_REQUIRE(S, "pcg_info: null solver");
     if (spmvSchedule) *spmvSchedule = S->kernel;
     if (deviceLoop) *deviceLoop = S->persistent ? 2 : (S->deviceLoop ? 1 : 0);
+    return CIECU_OK;
+}
+
+int ciecu_pcg_dia_info(ciecu_pcg S, int* storedDiagonals, int* symmetric) {
+    CIECU_REQUIRE(S && storedDiagonals && symmetric, "pcg_dia_info: null argument");
+    *storedDiagonals = S->diaBuf ? (S->diaSym ? S->diaU.ndiag : S->dia.ndiag) : 0;
+    *symmetric = S->diaSym ? 1 : 0;
     return CIECU_OK;
 }
 

@@ -470,8 +470,11 @@ class ConjugateGradients(LinearOperator):
             return {"fused": False}
         k, d = ctypes.c_int(), ctypes.c_int()
         call("ciecu_pcg_info", self._solver, ctypes.byref(k), ctypes.byref(d))
+        nd, sym = ctypes.c_int(), ctypes.c_int()
+        call("ciecu_pcg_dia_info", self._solver, ctypes.byref(nd), ctypes.byref(sym))
         return {"fused": True, "spmv_schedule": k.value, "device_loop": d.value >= 1,
-                "loop": ("graph chunks", "graph loop", "single launch")[d.value]}
+                "loop": ("graph chunks", "graph loop", "single launch")[d.value],
+                "dia_stored_diagonals": nd.value, "dia_symmetric": bool(sym.value)}
 
     def product(self, inScale, in_, outScale, out):
         n = self.space.size(out)
@@ -606,8 +609,11 @@ class MixedPrecisionCG(LinearOperator):
         call("ciecu_mixed_padded_entries", self._solver, ctypes.byref(e))
         if v.value == -2:
             # the SELL copy (compressed_columns, padded_entries) is kept beside the DIA one
+            nd, sym = ctypes.c_int(), ctypes.c_int()
+            call("ciecu_mixed_dia_info", self._solver, ctypes.byref(nd), ctypes.byref(sym))
             return {"format": "dia", "inner_kernel": "dia", "group_unroll": v.value,
-                    "compressed_columns": bool(c.value), "padded_entries": e.value}
+                    "compressed_columns": bool(c.value), "padded_entries": e.value,
+                    "dia_stored_diagonals": nd.value, "dia_symmetric": bool(sym.value)}
         return {"compressed_columns": bool(c.value), "format": "sell-32x4", "padded_entries": e.value,
                 "group_unroll": v.value, "inner_kernel": "tma-pipeline" if v.value == 0 else "registers"}
 
@@ -701,6 +707,21 @@ class BatchedConjugateGradients(LinearOperator):
             call("ciecu_batch_set_refinement", self._solver, float(innerTolerance))
         finally:
             self.space.leave()
+
+    def set_reliable_updates(self, delta):
+        """delta in (0, 1): FP32 iterations per system with FP64 reliable updates
+        (the Krylov space kept across replacements); 0: off."""
+        self.space.enter()
+        try:
+            call("ciecu_batch_set_reliable_updates", self._solver, float(delta))
+        finally:
+            self.space.leave()
+
+    def refinements(self):
+        """FP64 residual replacements per system in the last reliable-update solve."""
+        out = (ctypes.c_int64 * self.systems)()
+        call("ciecu_batch_refinements", self._solver, out)
+        return list(out)
 
     def getStats(self):
         return self._stats

@@ -45,6 +45,14 @@ public:
     // FP32 inner solves with FP64 refinement per system (innerTolerance: the drop of
     // the FP32 residual per refinement step; 0 returns to FP64).
     void setRefinement(double innerTolerance) { check(ciecu_batch_set_refinement(_solver.get(), innerTolerance)); }
+    // delta in (0, 1): FP32 iterations per system with FP64 reliable updates
+    // (ciecu_batch_set_reliable_updates); 0: off.
+    void setReliableUpdates(double delta) { check(ciecu_batch_set_reliable_updates(_solver.get(), delta)); }
+    std::vector<int64_t> refinements() const {
+        std::vector<int64_t> out(systems());
+        check(ciecu_batch_refinements(_solver.get(), out.data()));
+        return out;
+    }
 
     void product(double inScale, Space::ConstVectorView in, double outScale, Space::VectorView out) {
         require(in.size() == out.size() && out.size() == _pLhs->matrix().rowCount,

@@ -219,6 +219,11 @@ int ciecu_pcg_set_schedule(ciecu_pcg solver, int schedule);
  * kernel, else lanes per row) and how the last solve ran: host-polled graph chunks
  * (0), a device-side graph loop (1) or a single cooperative launch (2). */
 int ciecu_pcg_info(ciecu_pcg solver, int* spmvSchedule, int* deviceLoop);
+/* The diagonal-storage copy at the last solve: the diagonals K1 reads (0: no
+ * copy) and whether they are the upper half (main diagonal included) of a bitwise
+ * symmetric matrix, checked at every solve, whose lower entries K1 reads back from
+ * it (about half the matrix bytes; CIECU_DIA_SYMMETRIC=0 keeps the full copy). */
+int ciecu_pcg_dia_info(ciecu_pcg solver, int* storedDiagonals, int* symmetric);
 /* How the iterations run.  mode 0 (default): a single cooperative launch of at
  * most one block per SM (the fewest of SMs/4, SMs/2, SMs that fit), each block
  * holding its rows of the matrix in shared memory, when the rows fit there at one

@@ -45,6 +45,18 @@ int ciecu_batch_product(ciecu_batch solver, double inScale, const double* d_in, 
  * true residuals.  0 (the default): the FP64 solve.  The first call with a
  * positive tolerance allocates the FP32 copies and autotunes their SpMV. */
 int ciecu_batch_set_refinement(ciecu_batch solver, double innerTolerance);
+/* delta in (0, 1): every system iterates in FP32 (FP32 copies of the values and
+ * of D^-1, FP32 vectors, FP64 dot products) with FP64 reliable updates: when a
+ * system's FP32 residual norm fell below delta times its largest value since the
+ * last replacement (or below the stopping tolerance, or at the iteration limit),
+ * its FP32 solution is added to the FP64 one and its residual recomputed as
+ * b - A x in FP64; the Krylov space is kept across replacements.  The stopping
+ * test and the statistics use that FP64 residual (iterationCount = FP32
+ * iterations).  Takes precedence over ciecu_batch_set_refinement; 0 (default):
+ * off. */
+int ciecu_batch_set_reliable_updates(ciecu_batch solver, double delta);
+/* FP64 residual replacements of each system in the last reliable-update solve. */
+int ciecu_batch_refinements(ciecu_batch solver, int64_t* h_perSystem);
 
 #ifdef __cplusplus
 }

@@ -23,8 +23,9 @@ typedef struct ciecu_multi_s* ciecu_multi;
 int ciecu_multi_create(ciecu_csr lhs, int rhsCount, const double* d_inverseDiagonal, ciecu_statistics settings,
                        ciecu_multi* out);
 int ciecu_multi_destroy(ciecu_multi solver);
-/* Lanes per row group (the power of two >= rhsCount) and whether the solve loop
- * runs on the device (conditional graph nodes). */
+/* Lanes per row group (the power of two >= rhsCount; 8 when rhsCount = 32 and
+ * the right-hand sides are 16-byte aligned: four columns per lane) and whether
+ * the solve loop runs on the device (conditional graph nodes). */
 int ciecu_multi_info(ciecu_multi solver, int* lanesPerRow, int* deviceLoop);
 /* SpMM format chosen at the first solve: the number of diagonals of the
  * diagonal-storage copy (a matrix of at most 32 diagonals, see

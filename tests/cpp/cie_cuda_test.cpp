@@ -158,6 +158,16 @@ void solver_classes(const std::shared_ptr<Space>& pSpace) {
         const double e1 = rel_diff(std::vector<double>(xh.begin() + s0.n, xh.end()), x1);
         report(e0 <= 1e-9 && e1 <= 1e-9 && batch.getStats().size() == 2,
                "BatchedConjugateGradients per system vs reference PCG", std::fmax(e0, e1));
+        // FP32 iterations with FP64 reliable updates: same bar
+        batch.setReliableUpdates(0.1);
+        pSpace->fill(Space::view(x), 0.0);
+        batch.product(0, Space::view(std::as_const(rhs)), 1, Space::view(x));
+        const std::vector<double> xr = download(pSpace, x);
+        const double f0 = rel_diff(std::vector<double>(xr.begin(), xr.begin() + s0.n), x0);
+        const double f1 = rel_diff(std::vector<double>(xr.begin() + s0.n, xr.end()), x1);
+        const auto reps = batch.refinements();
+        report(f0 <= 1e-9 && f1 <= 1e-9 && reps[0] > 0 && reps[1] > 0,
+               "BatchedConjugateGradients reliable updates vs reference PCG", std::fmax(f0, f1));
     }
     const HostCSR a = poisson5(40);
     auto dm = upload(pSpace, a);

@@ -134,3 +134,65 @@ def test_batched_fp32_refined_vs_reference(space, reference):
         assert np.linalg.norm(r) <= 1.05e-10 * np.linalg.norm(b)
         assert np.linalg.norm(xs - xr) <= 1e-9 * np.linalg.norm(xr)
     print("refined: inner iterations %s (FP64 reference %s)" % ([st.iterationCount for st in stats[:4]], int(sr[0])))
+
+
+@pytest.mark.parametrize("delta", [0.1, 0.01])
+def test_batched_reliable_updates_vs_reference(space, reference, delta):
+    """FP32 iterations per system with FP64 reliable updates
+    (set_reliable_updates): every system's true FP64 residual at the 1e-10 stop,
+    its solution within 1e-9 of the reference CG's, at least one replacement, and
+    an iteration count near the FP64 one (the Krylov space is kept)."""
+    from cie_b200.linalg import BatchedConjugateGradients, Statistics, block_diagonal, makeDiagonalOperator
+    from oracle.oracle import Restatement
+    probs = systems(space, 10, seed=19)
+    bd, offsets = block_diagonal([p.matrix for p in probs])
+    rhs = torch.cat([p.rhs for p in probs])
+    D = makeDiagonalOperator(bd, space)
+    solver = BatchedConjugateGradients(bd, offsets, space, D, Statistics(20000, 0.0, 1e-10))
+    solver.set_reliable_updates(delta)
+    x = torch.zeros_like(rhs)
+    solver.product(0.0, rhs, 1.0, x)
+    stats = solver.getStats()
+    reps = solver.refinements()
+    xh = x.cpu().numpy()
+    ora = Restatement()
+    for s, p in enumerate(probs):
+        rp, col, val = p.host_csr()
+        b = p.rhs.cpu().numpy()
+        xs = xh[offsets[s]:offsets[s + 1]].copy()
+        xr, sr, err, _ = reference.pcg(rp, col, val, b, maxit=20000, abstol=0.0, reltol=1e-10)
+        r = ora.spmv(rp, col, val, 1.0, xs, -1.0, b)
+        assert stats[s].relativeResidual < 1e-10, (s, stats[s].relativeResidual)
+        assert np.linalg.norm(r) <= 1.01e-10 * np.linalg.norm(b), s
+        assert np.linalg.norm(xs - xr) <= 1e-9 * np.linalg.norm(xr), s
+        assert reps[s] >= 1
+        assert stats[s].iterationCount <= 1.3 * int(sr[0]) + 10, (s, stats[s].iterationCount, sr[0])
+    print("reliable updates delta %g: iterations %s, replacements %s" % (delta, [st.iterationCount for st in stats[:4]],
+                                                                       reps[:4]))
+
+
+def test_batched_reliable_updates_limits_and_switch(space):
+    """The iteration limit in the reliable-update form (FP64 residual reported),
+    and one solver switched between the FP64 and reliable-update forms."""
+    from cie_b200.linalg import BatchedConjugateGradients, Statistics, block_diagonal, makeDiagonalOperator
+    probs = systems(space, 5, seed=23)
+    bd, offsets = block_diagonal([p.matrix for p in probs])
+    rhs = torch.cat([p.rhs for p in probs])
+    D = makeDiagonalOperator(bd, space)
+    limited = BatchedConjugateGradients(bd, offsets, space, D, Statistics(7, 0.0, 1e-10))
+    limited.set_reliable_updates(0.1)
+    x = torch.zeros_like(rhs)
+    limited.product(0.0, rhs, 1.0, x)
+    for st in limited.getStats():
+        assert st.iterationCount == 7 and 1e-10 < st.relativeResidual < 1.0
+    solver = BatchedConjugateGradients(bd, offsets, space, D, Statistics(20000, 0.0, 1e-10))
+    x64 = torch.zeros_like(rhs)
+    solver.product(0.0, rhs, 1.0, x64)
+    solver.set_reliable_updates(0.1)
+    x32 = torch.zeros_like(rhs)
+    solver.product(0.0, rhs, 1.0, x32)
+    solver.set_reliable_updates(0.0)
+    x64b = torch.zeros_like(rhs)
+    solver.product(0.0, rhs, 1.0, x64b)
+    assert torch.equal(x64, x64b)
+    assert float(torch.linalg.norm(x32 - x64) / torch.linalg.norm(x64)) <= 1e-9

@@ -158,7 +158,7 @@ def cfg4_batch(space):
     return [make_poisson(space, 2, 2, [int(sizes[i]), int(sizes[i])], seed=1000 + 3 * i) for i in pick]
 
 
-@pytest.mark.parametrize("refined", [False, True])
+@pytest.mark.parametrize("refined", [False, True, "reliable"])
 def test_cfg4_batched_subset_vs_reference(space, reference_all, cfg4_batch, refined):
     from cie_b200.linalg import BatchedConjugateGradients, Statistics, block_diagonal, makeDiagonalOperator
     probs = cfg4_batch
@@ -166,7 +166,9 @@ def test_cfg4_batched_subset_vs_reference(space, reference_all, cfg4_batch, refi
     rhs = torch.cat([p.rhs for p in probs])
     solver = BatchedConjugateGradients(bd, offsets, space, makeDiagonalOperator(bd, space),
                                        Statistics(20000, 0.0, 1e-10))
-    if refined:
+    if refined == "reliable":
+        solver.set_reliable_updates(0.1)
+    elif refined:
         # FP32 drops of 1e-4 per round: the FP64 residual lands below the 1e-10 stop
         # with margin, so the solution stays within the 1e-9 bar of the reference's
         # (a refined solve follows its own path, not the reference's iterates)
@@ -176,6 +178,7 @@ def test_cfg4_batched_subset_vs_reference(space, reference_all, cfg4_batch, refi
     stats = solver.getStats()
     xh = x.cpu().numpy()
     worst = 0.0
+    beyond = []
     for s, p in enumerate(probs):
         rp, col, val = p.host_csr()
         b = p.rhs.cpu().numpy()
@@ -184,8 +187,21 @@ def test_cfg4_batched_subset_vs_reference(space, reference_all, cfg4_batch, refi
         rel = np.linalg.norm(xs - xr) / np.linalg.norm(xr)
         worst = max(worst, rel)
         assert err is None
-        assert rel <= TOL, (s, rel)
         assert true_residual(rp, col, val, xs, b) <= RESIDUAL, s
+        if refined == "reliable" and rel > TOL:
+            # the reliable-update solve stops at the same 1e-10 (true FP64 residual)
+            # along its own iterates; where the system's conditioning spreads two such
+            # solutions more than 1e-9 apart, its distance from the exact solution (the
+            # reference CG to 1e-13) must be of the order of the reference's own
+            xe, _, erre, _ = reference_all.pcg(rp, col, val, b, maxit=200000, abstol=0.0, reltol=1e-13)
+            e_ours = np.linalg.norm(xs - xe) / np.linalg.norm(xe)
+            e_ref = np.linalg.norm(xr - xe) / np.linalg.norm(xe)
+            beyond.append((s, rel, e_ours, e_ref))
+            assert erre is None and e_ours <= max(2.0 * e_ref, 1e-12), (s, rel, e_ours, e_ref)
+        else:
+            assert rel <= TOL, (s, rel)
         if not refined:
             assert stats[s].iterationCount == int(sr[0]), (s, stats[s].iterationCount, sr[0])
-    print("cfg4 batch of %d (refined=%s): worst |x - x_ref|/|x_ref| = %.3e" % (len(probs), refined, worst))
+    print("cfg4 batch of %d (refined=%s): worst |x - x_ref|/|x_ref| = %.3e; beyond 1e-9 (system, rel, error, "
+          "reference's error): %s" % (len(probs), refined, worst, beyond))
+    assert len(beyond) <= 2

@@ -185,11 +185,44 @@ def test_dia_inner_operator_matches_sell(space, dims, scale):
     dia.apply_inner(x, y1)
     sell.apply_inner(x, y2)
     assert torch.equal(y1, y2)
+    if not scale:
+        # the assembled matrix is bitwise symmetric: only the upper half is stored,
+        # and the lower terms read back from it keep the column order of the sums
+        assert dia.info()["dia_symmetric"] and dia.info()["dia_stored_diagonals"] == (3 ** dim + 1) // 2
     xs = torch.zeros_like(prob.rhs)
     dia.product(0.0, prob.rhs, 1.0, xs)
     r = prob.rhs.clone()
     A.product(1.0, xs, -1.0, r)
     assert float(torch.linalg.norm(r) / torch.linalg.norm(prob.rhs)) <= 1.01e-10
+
+
+@pytest.mark.parametrize("dims", [(2, [30, 30]), (3, [12, 12, 12])])
+def test_dia_nonsymmetric_matrix_keeps_full_copy(space, dims):
+    """One entry changed on one side only: the symmetry check finds it, the full
+    DIA copy is kept, and the inner operator still equals the SELL one bit for bit
+    (and the CSR SpMV within FP32 rounding)."""
+    from cie_b200.fem import make_poisson
+    from cie_b200.linalg import CSRMatrix, CSROperator, MixedPrecisionCG, Statistics, makeDiagonalOperator
+    dim, cells = dims
+    prob = make_poisson(space, dim, 1, cells, seed=9)
+    rp, col, val = prob.host_csr()
+    i = len(rp) // 2
+    j = next(k for k in range(rp[i], rp[i + 1]) if col[k] > i)
+    val = val.copy()
+    val[j] *= 1.25
+    m = CSRMatrix(len(rp) - 1, dev(rp, torch.int32), dev(col, torch.int32), dev(val))
+    A = CSROperator(m, space)
+    D = makeDiagonalOperator(m, space, csr_handle=A.csr)
+    dia = MixedPrecisionCG(A, D, Statistics(100, 0.0, 1e-10), innerKernel=-2)
+    sell = MixedPrecisionCG(A, D, Statistics(100, 0.0, 1e-10), innerKernel=1)
+    info = dia.info()
+    assert not info["dia_symmetric"] and info["dia_stored_diagonals"] == 3 ** dim
+    n = len(rp) - 1
+    x = torch.rand(n, dtype=torch.float32, device="cuda") * 2 - 1
+    y1, y2 = torch.empty_like(x), torch.empty_like(x)
+    dia.apply_inner(x, y1)
+    sell.apply_inner(x, y2)
+    assert torch.equal(y1, y2)
 
 
 def test_dia_refused_for_scattered_pattern(space):

@@ -15,11 +15,16 @@ def space():
     return CUDASpace()
 
 
-@pytest.mark.parametrize("k,dim,cells", [(32, 3, [14, 14, 14]), (5, 2, [40, 40]), (1, 2, [30, 30])])
-def test_multirhs_pcg_vs_reference_per_column(space, reference, k, dim, cells):
+@pytest.mark.parametrize("k,dim,order,cells,offset", [(32, 3, 1, [14, 14, 14], 0), (32, 3, 2, [6, 6, 6], 0),
+                                                      (32, 3, 1, [10, 10, 10], 1), (5, 2, 1, [40, 40], 0),
+                                                      (1, 2, 1, [30, 30], 0)])
+def test_multirhs_pcg_vs_reference_per_column(space, reference, k, dim, order, cells, offset):
+    """k = 32 runs the four-columns-per-lane SpMM (Q1: DIA or CSR as timed, Q2:
+    CSR); right-hand sides at an 8-byte offset (not 16-byte aligned) take the
+    row-per-warp kernels.  Same iteration counts as the reference either way."""
     from cie_b200.fem import make_poisson
     from cie_b200.linalg import CSROperator, MultiRHSConjugateGradients, Statistics, makeDiagonalOperator
-    prob = make_poisson(space, dim, 1, cells, seed=7)
+    prob = make_poisson(space, dim, order, cells, seed=7)
     n = prob.rhs.numel()
     rng = np.random.default_rng(11)
     B = rng.uniform(-1, 1, (n, k))
@@ -29,7 +34,10 @@ def test_multirhs_pcg_vs_reference_per_column(space, reference, k, dim, cells):
     D = makeDiagonalOperator(prob.matrix, space, csr_handle=A.csr)
     solver = MultiRHSConjugateGradients(A, D, k, Statistics(5000, 0.0, 1e-10))
     X = torch.zeros(n, k, dtype=torch.float64, device="cuda")
-    solver.product(0.0, torch.as_tensor(B).cuda().contiguous(), 1.0, X)
+    buf = torch.zeros(n * k + offset, dtype=torch.float64, device="cuda")
+    Bd = buf[offset:].view(n, k)
+    Bd.copy_(torch.as_tensor(B))
+    solver.product(0.0, Bd, 1.0, X)
     stats = solver.getStats()
     Xh = X.cpu().numpy()
     rp, col, val = prob.host_csr()

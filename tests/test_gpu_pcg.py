@@ -135,6 +135,9 @@ def test_pcg_dia_schedule_vs_reference(space, reference, schedule):
     x = dev(np.zeros(len(b)))
     cg.product(0.0, dev(b), 1.0, x)
     assert cg.info()["spmv_schedule"] == schedule
+    if schedule == 64:
+        # the assembled matrix is bitwise symmetric: K1 reads the upper half only
+        assert cg.info()["dia_symmetric"] and cg.info()["dia_stored_diagonals"] == 14
     xr, sr, err, _ = reference.pcg(rp, col, val, b, maxit=5000, abstol=0.0, reltol=1e-10)
     rel = np.linalg.norm(host(x) - xr) / np.linalg.norm(xr)
     assert abs(cg.getStats().iterationCount - sr[0]) <= 2 and rel <= 1e-9
@@ -143,6 +146,20 @@ def test_pcg_dia_schedule_vs_reference(space, reference, schedule):
     x2 = dev(np.zeros(len(b)))
     cg.product(0.0, dev(b), 1.0, x2)
     assert np.linalg.norm(2.0 * host(x2) - host(x)) <= 1e-9 * np.linalg.norm(host(x))
+    if schedule == 64:
+        # one entry changed on one side: the next solve finds the matrix unsymmetric,
+        # reads the full copy, and still matches the reference on the changed system
+        i = len(rp) // 2
+        j = next(k for k in range(rp[i], rp[i + 1]) if col[k] > i)
+        prob.matrix.entries[j] *= 1.001
+        val3 = 2.0 * val
+        val3[j] *= 1.001
+        x3 = dev(np.zeros(len(b)))
+        cg.product(0.0, dev(b), 1.0, x3)
+        assert not cg.info()["dia_symmetric"] and cg.info()["dia_stored_diagonals"] == 27
+        xr3, sr3, err3, _ = reference.pcg(rp, col, val3, b, maxit=5000, abstol=0.0, reltol=1e-10)
+        assert err3 is None
+        assert np.linalg.norm(host(x3) - xr3) <= 1e-9 * np.linalg.norm(xr3)
 
 
 def test_pcg_dia_schedule_refused_without_diagonals(space):
