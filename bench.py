@@ -415,14 +415,11 @@ def main():
     dia32 = info.get("format") == "dia"
     dia64 = cg.info().get("spmv_schedule") == 64
     idx_bytes = 2 if info.get("compressed_columns") else 4
-    stored32 = info.get("dia_stored_diagonals") or ndiag
-    sym32 = bool(info.get("dia_symmetric"))
     if dia32:
         # FP32 DIA SpMV: the stored diagonals (nonzeros and the zeros that pad the
-        # diagonals; the upper half when the matrix is symmetric, the lower entries
-        # being re-read from it through L2), x read, y written; no column indices
-        spmv32_bytes = 4 * stored32 * n + 8 * n
-        inner_bytes = 4 * stored32 * n + 52 * n
+        # diagonals), x read, y written; no column indices
+        spmv32_bytes = 4 * ndiag * n + 8 * n
+        inner_bytes = 4 * ndiag * n + 52 * n
     else:
         # FP32 SELL-32 SpMV: values + column offsets of the nonzeros, x read, y written
         # (padding entries and the per-slice descriptors are reported, not counted)
@@ -440,7 +437,7 @@ def main():
     if os.path.exists(tpath) and cells == [128, 128, 128]:
         figures = dict(line.split() for line in open(tpath) if line.strip() and not line.startswith("#"))
         if dia32:
-            traffic = int(figures.get("mixed_apply_dia_kernel_f32" + ("_symmetric" if sym32 else ""), 0)) or None
+            traffic = int(figures.get("mixed_apply_dia_kernel_f32", 0)) or None
         elif info["compressed_columns"] and info["group_unroll"] > 0:
             traffic = int(figures.get("mixed_apply_kernel_f32_sell16", 0)) or None
         traffic64 = int(figures.get("spmv_kernel_f64_csr", 0)) or None
@@ -500,7 +497,7 @@ def main():
             "data": "synthetic (seeded mt19937_64 RHS and kappa field)",
             "config": common_config(world),
             "solver": {"mixed": "jacobi-pcg, FP32 inner over %s, FP64 reliable updates delta=%g, %s" % (
-                           info["format"] + (" (symmetric upper half)" if sym32 else ""), DELTA,
+                           info["format"], DELTA,
                            "fused direction" if FUSE else "separate direction kernel"),
                        "fp64": "jacobi-pcg over %s" % (("dia, symmetric upper half" if cg.info().get(
                            "dia_symmetric") else "dia") if dia64 else "csr")},
@@ -529,9 +526,7 @@ def main():
                                        "mixed_frac": mixed_solve_bytes / t_mixed / 1e9 / hbm},
             "parity": parity,
             "roofline": {"bound": "hbm", "kernel": (
-                             "mixed_apply_dia_kernel (FP32 DIA SpMV, %d diagonals%s)" % (
-                                 ndiag, ", symmetric: the %d of the upper half stored" % stored32 if sym32 else ""))
-                         if dia32 else (
+                             "mixed_apply_dia_kernel (FP32 DIA SpMV, %d diagonals)" % ndiag) if dia32 else (
                              "%s (FP32 SELL-32 SpMV)" % ("mixed_apply_kernel<%d>" % info["group_unroll"]
                                                          if info["group_unroll"] > 0 else "mixed_apply_tma_kernel")),
                          "achieved": g32, "peak": hbm, "unit": "GB/s", "frac": g32 / hbm, "peak_kind": peak_kind,

@@ -97,7 +97,6 @@ SIGNATURES = {
     "ciecu_mixed_product": (c_int, [P, c_double, P, c_double, P, P]),
     "ciecu_mixed_apply_f32": (c_int, [P, P, P]),
     "ciecu_mixed_padded_entries": (c_int, [P, P]),
-    "ciecu_mixed_dia_info": (c_int, [P, P, P]),
     # host utilities
     "ciecu_structured_dofmap": (c_int, [c_int, c_int, P, P, P]),
     "ciecu_structured_boundary": (c_int, [c_int, c_int, P, P]),
@@ -145,6 +144,7 @@ SIGNATURES = {
     "ciecu_mgcg_destroy": (c_int, [P]),
     "ciecu_mgcg_product": (c_int, [P, c_double, P, c_double, P, P]),
     "ciecu_mgcg_info": (c_int, [P, P, P]),
+    "ciecu_mgcg_smoother_info": (c_int, [P, P, P]),
 }
 
 OPTIONAL = set()

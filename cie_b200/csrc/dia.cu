@@ -174,33 +174,6 @@ int dia_symmetric(const DiaArgs<V>& full, cudaStream_t st, unsigned* d_flag, boo
 template int dia_symmetric<float>(const DiaArgs<float>&, cudaStream_t, unsigned*, bool*);
 template int dia_symmetric<double>(const DiaArgs<double>&, cudaStream_t, unsigned*, bool*);
 
-int dia_symmetric_upper_f32(const DiaArgs<float>& full, DiaArgs<float>* upper, float** upperVal, cudaStream_t st,
-                            unsigned* d_flag, bool* symmetric) {
-    *upperVal = nullptr;
-    CIECU_TRY(dia_symmetric(full, st, d_flag, symmetric));
-    if (!*symmetric) return CIECU_OK;
-    DiaArgs<float> u = dia_upper_view(full);
-    const size_t bytes = sizeof(float) * static_cast<size_t>(u.ndiag) * static_cast<size_t>(u.ld);
-    float* val = nullptr;
-    if (cudaMalloc(&val, bytes) != cudaSuccess) {
-        cudaGetLastError();  // no room: the full copy stays
-        *symmetric = false;
-        return CIECU_OK;
-    }
-    // the upper half (main diagonal first) is contiguous in the full copy
-    cudaError_t e = cudaMemcpyAsync(val, u.val, bytes, cudaMemcpyDeviceToDevice, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) {
-        cudaFree(val);
-        *symmetric = false;
-        return cuda_fail(e, "DIA upper half");
-    }
-    u.val = val;
-    *upper = u;
-    *upperVal = val;
-    return CIECU_OK;
-}
-
 }  // namespace ciecu
 
 extern "C" int ciecu_csr_diagonals(ciecu_csr csr, int* ndiag) {

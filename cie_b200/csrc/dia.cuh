@@ -107,141 +107,6 @@ __device__ __forceinline__ void dia_rows4(const DiaArgs<float>& A, const float* 
     dia_rows4_gather<ND>(A, LoadGather<float>{x}, op);
 }
 
-// The same four-rows-per-thread pass over the UPPER HALF of a symmetric matrix:
-// diagonal d of U holds A[r][r + off[d]] with off[0] = 0 and ascending positive
-// offsets after it.  The lower term A[r][r - off[d]] = A[r - off[d]][r] is read
-// back from diagonal d at row r - off[d]: data streamed about off[d] rows earlier,
-// so an L2 (often L1) hit, and only the upper half crosses HBM.  The terms run in
-// ascending column order -- lower diagonals from the farthest, the main diagonal,
-// the upper ones -- the order of the full copy, so for a bitwise symmetric matrix
-// the row sums are those of dia_rows4 on the full copy.
-template <int NU, typename Op, typename TGather>
-__device__ __forceinline__ void dia_rows4_sym_gather(const DiaArgs<float>& U, const TGather& gather, Op& op) {
-    const long stride = static_cast<long>(gridDim.x) * blockDim.x * 4;
-    const int nu = NU > 0 ? NU : U.ndiag;
-    for (long r0 = (static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x) * 4; r0 < U.nrows; r0 += stride) {
-        const int r = static_cast<int>(r0);
-        typename Op::Pre pre[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-            if (r + i < U.nrows) pre[i] = op.pre(r + i);
-        float sum[4] = {0.f, 0.f, 0.f, 0.f};
-        auto lower = [&](int d) {
-            const int o = U.off[d];
-            const float* __restrict__ diag = U.val + static_cast<long>(d) * U.ld;
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                const int c = r + i - o;
-                const bool in = static_cast<unsigned>(c) < static_cast<unsigned>(U.nrows);
-                const float v = in ? __ldg(diag + c) : 0.f;
-                const float xv = in ? gather(c) : 0.f;
-                sum[i] = fmaf(v, xv, sum[i]);
-            }
-        };
-        if constexpr (NU > 0) {
-#pragma unroll
-            for (int d = NU - 1; d >= 1; --d) lower(d);
-        } else {
-            for (int d = nu - 1; d >= 1; --d) lower(d);
-        }
-        for_diagonals<NU>(U, [&](int d) {
-            // evict-first like the full copy: the lower-term re-reads come within
-            // about off[d] rows (a few MB of streaming), well inside L2's reach
-            const float4 v = __ldcs(reinterpret_cast<const float4*>(U.val + static_cast<long>(d) * U.ld + r));
-            const int c = r + U.off[d];
-            float xv[4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-                xv[i] = static_cast<unsigned>(c + i) < static_cast<unsigned>(U.nrows) ? gather(c + i) : 0.f;
-            sum[0] = fmaf(v.x, xv[0], sum[0]);
-            sum[1] = fmaf(v.y, xv[1], sum[1]);
-            sum[2] = fmaf(v.z, xv[2], sum[2]);
-            sum[3] = fmaf(v.w, xv[3], sum[3]);
-        });
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-            if (r + i < U.nrows) op.post(r + i, pre[i], sum[i]);
-    }
-}
-
-template <int NU, typename Op>
-__device__ __forceinline__ void dia_rows4_sym(const DiaArgs<float>& U, const float* __restrict__ x, Op& op) {
-    dia_rows4_sym_gather<NU>(U, LoadGather<float>{x}, op);
-}
-
-// Calls f(std::integral_constant<int, NU>) with NU = 14 or 5 (the upper halves of
-// the 27- and 9-diagonal Q1 stencils, main diagonal included) or 0 (runtime).
-template <typename F>
-int with_upper_diagonals(int nu, F&& f) {
-    switch (nu) {
-        case 14: return f(std::integral_constant<int, 14>{});
-        case 5: return f(std::integral_constant<int, 5>{});
-        default: return f(std::integral_constant<int, 0>{});
-    }
-}
-
-// CIECU_DIA_SYMMETRIC=0 keeps full DIA copies of symmetric matrices (for
-// comparison); by default the solvers read only the upper half of such a copy.
-inline bool dia_symmetric_enabled() {
-    static const bool enabled = [] {
-        const char* v = std::getenv("CIECU_DIA_SYMMETRIC");
-        return !(v && v[0] == '0');
-    }();
-    return enabled;
-}
-
-// Whether the DIA copy `full` (offsets symmetric about 0) is bitwise symmetric:
-// entry (r, r + o) equals entry (r + o, r) for every stored pair.
-template <typename V>
-int dia_symmetric(const DiaArgs<V>& full, cudaStream_t st, unsigned* d_flag, bool* symmetric);
-
-// The upper half of a full copy with offsets symmetric about 0, as a view into
-// it: the ndiag / 2 + 1 diagonals from the main one on are contiguous there.
-template <typename V>
-DiaArgs<V> dia_upper_view(const DiaArgs<V>& full) {
-    DiaArgs<V> u{};
-    u.nrows = full.nrows;
-    u.ld = full.ld;
-    u.ndiag = full.ndiag / 2 + 1;
-    for (int d = 0; d < u.ndiag; ++d) u.off[d] = full.off[full.ndiag / 2 + d];
-    u.val = full.val + static_cast<long>(full.ndiag / 2) * full.ld;
-    return u;
-}
-
-// dia_symmetric for an FP32 copy; when symmetric, its upper half moves to a
-// buffer of its own (`upper`, `upperVal`; the caller frees the full one).
-int dia_symmetric_upper_f32(const DiaArgs<float>& full, DiaArgs<float>* upper, float** upperVal, cudaStream_t st,
-                            unsigned* d_flag, bool* symmetric);
-
-// One thread per row over the upper half of a symmetric matrix (see
-// dia_rows4_sym_gather): lower terms from the farthest diagonal in, the main
-// diagonal, the upper ones -- the column order of dia_rows on the full copy.
-template <int NU, typename T, typename V, typename Op>
-__device__ __forceinline__ void dia_rows_sym(const DiaArgs<V>& U, const T* __restrict__ x, Op& op) {
-    const long stride = static_cast<long>(gridDim.x) * blockDim.x;
-    const int nu = NU > 0 ? NU : U.ndiag;
-    for (long rl = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; rl < U.nrows; rl += stride) {
-        const int r = static_cast<int>(rl);
-        const auto pre = op.pre(r);
-        T sum = T(0);
-#pragma unroll 7
-        for (int d = nu - 1; d >= 1; --d) {
-            const int c = r - U.off[d];
-            const bool in = c >= 0;
-            const V v = in ? __ldg(U.val + static_cast<long>(d) * U.ld + c) : V(0);
-            const T xv = in ? __ldg(x + c) : T(0);
-            sum = fma(static_cast<T>(v), xv, sum);
-        }
-        for_diagonals<NU>(U, [&](int d) {
-            const int c = r + U.off[d];
-            const V v = stream_ld(U.val + static_cast<long>(d) * U.ld + r);
-            const T xv = static_cast<unsigned>(c) < static_cast<unsigned>(U.nrows) ? __ldg(x + c) : T(0);
-            sum = fma(static_cast<T>(v), xv, sum);
-        });
-        op.post(r, pre, sum);
-    }
-}
-
 // Calls f(std::integral_constant<int, ND>) with ND = 27, 9 or 0 (runtime count).
 template <typename F>
 int with_diagonals(int ndiag, F&& f) {
@@ -278,5 +143,66 @@ DiaArgs<V> dia_shape(const ciecu_csr_s* csr, const std::vector<int>& offsets) {
 // solver's inner matrix) before the conversion to V.
 int dia_fill_f64(const ciecu_csr_s* csr, const DiaArgs<double>& a, double* out, cudaStream_t st);
 int dia_fill_f32(const ciecu_csr_s* csr, const DiaArgs<float>& a, float* out, const double* sdiag, cudaStream_t st);
+
+// CIECU_DIA_SYMMETRIC=0 makes the FP64 PCG read every diagonal of a bitwise
+// symmetric DIA copy (for comparison); by default it reads only the upper half.
+inline bool dia_symmetric_enabled() {
+    static const bool enabled = [] {
+        const char* v = std::getenv("CIECU_DIA_SYMMETRIC");
+        return !(v && v[0] == '0');
+    }();
+    return enabled;
+}
+
+// Whether the DIA copy `full` (offsets symmetric about 0) is bitwise symmetric:
+// entry (r, r + o) equals entry (r + o, r) for every stored pair.
+template <typename V>
+int dia_symmetric(const DiaArgs<V>& full, cudaStream_t st, unsigned* d_flag, bool* symmetric);
+
+// The upper half of a full copy with offsets symmetric about 0, as a view into
+// it: the ndiag / 2 + 1 diagonals from the main one on are contiguous there.
+template <typename V>
+DiaArgs<V> dia_upper_view(const DiaArgs<V>& full) {
+    DiaArgs<V> u{};
+    u.nrows = full.nrows;
+    u.ld = full.ld;
+    u.ndiag = full.ndiag / 2 + 1;
+    for (int d = 0; d < u.ndiag; ++d) u.off[d] = full.off[full.ndiag / 2 + d];
+    u.val = full.val + static_cast<long>(full.ndiag / 2) * full.ld;
+    return u;
+}
+
+// One thread per row over the upper half U of a bitwise symmetric matrix
+// (diagonal d of U holds A[r][r + off[d]], off[0] = 0, ascending): the lower term
+// A[r][r - off[d]] = A[r - off[d]][r] is read back from diagonal d at row
+// r - off[d], data streamed about off[d] rows earlier (an L2 hit), so only the
+// upper half crosses HBM.  Lower terms from the farthest diagonal in, the main
+// diagonal, the upper ones: the column order of dia_rows on the full copy, so the
+// row sums are the same.
+template <int NU, typename T, typename V, typename Op>
+__device__ __forceinline__ void dia_rows_sym(const DiaArgs<V>& U, const T* __restrict__ x, Op& op) {
+    const long stride = static_cast<long>(gridDim.x) * blockDim.x;
+    const int nu = NU > 0 ? NU : U.ndiag;
+    for (long rl = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; rl < U.nrows; rl += stride) {
+        const int r = static_cast<int>(rl);
+        const auto pre = op.pre(r);
+        T sum = T(0);
+#pragma unroll 7
+        for (int d = nu - 1; d >= 1; --d) {
+            const int c = r - U.off[d];
+            const bool in = c >= 0;
+            const V v = in ? __ldg(U.val + static_cast<long>(d) * U.ld + c) : V(0);
+            const T xv = in ? __ldg(x + c) : T(0);
+            sum = fma(static_cast<T>(v), xv, sum);
+        }
+        for_diagonals<NU>(U, [&](int d) {
+            const int c = r + U.off[d];
+            const V v = stream_ld(U.val + static_cast<long>(d) * U.ld + r);
+            const T xv = static_cast<unsigned>(c) < static_cast<unsigned>(U.nrows) ? __ldg(x + c) : T(0);
+            sum = fma(static_cast<T>(v), xv, sum);
+        });
+        op.post(r, pre, sum);
+    }
+}
 
 }  // namespace ciecu

@@ -19,6 +19,7 @@
 
 #include <cmath>
 #include <string>
+#include <type_traits>
 #include <utility>
 
 namespace ciecu {
@@ -220,6 +221,53 @@ __global__ void __launch_bounds__(csr_threads<K>())
     csr_rows<K, T, T, false>(A, dold, op);
 }
 
+// The FP32 smoother over 16-bit column offsets from the row (6 bytes per entry
+// instead of 8): a Chebyshev step and the cycle's residual t = t - A32 z.
+template <int VS>
+__global__ void __launch_bounds__(kVectorThreads)
+    cheb_step16_kernel(CsrArgs<float, short> A, const float* __restrict__ dinv, float c1, float c2,
+                       float* __restrict__ r, const float* __restrict__ dold, float* __restrict__ dnew,
+                       float* __restrict__ x) {
+    ChebStep<float> op{dinv, c1, c2, r, dold, dnew, x};
+    vector_rows<float, float, short, VS, kVectorThreads, false>(A, dold, op);
+}
+
+struct SubtractOp {  // t = t - A z
+    using Pre = float;
+    float* __restrict__ t;
+    __device__ __forceinline__ float pre(int i) const { return t[i]; }
+    __device__ __forceinline__ void post(int i, float ti, float sum) const { t[i] = ti - sum; }
+};
+
+template <int VS>
+__global__ void __launch_bounds__(kVectorThreads)
+    residual16_kernel(CsrArgs<float, short> A, const float* __restrict__ z, float* __restrict__ t) {
+    SubtractOp op{t};
+    vector_rows<float, float, short, VS, kVectorThreads, false>(A, z, op);
+}
+
+// 16-bit offsets col - row of every entry; bad[0] counts offsets outside int16.
+__global__ void offsets16_kernel(int n, const int* __restrict__ rowptr, const int* __restrict__ col,
+                                 short* __restrict__ out, unsigned* bad) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+        for (int k = rowptr[r]; k < rowptr[r + 1]; ++k) {
+            const int d = col[k] - r;
+            if (d < -32768 || d > 32767) atomicAdd(bad, 1u);
+            out[k] = static_cast<short>(d);
+        }
+}
+
+// Calls f(std::integral_constant<int, VS>) for VS in {4, 8, 16, 32}.
+template <typename F>
+int with_lanes16(int vs, F&& f) {
+    switch (vs) {
+        case 4: return f(std::integral_constant<int, 4>{});
+        case 8: return f(std::integral_constant<int, 8>{});
+        case 16: return f(std::integral_constant<int, 16>{});
+        default: return f(std::integral_constant<int, 32>{});
+    }
+}
+
 template <typename T>
 __global__ void axpy_out_kernel(long n, const T* __restrict__ x, T* __restrict__ out, int accumulate) {
     for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < n;
@@ -375,6 +423,8 @@ struct ciecu_mgcg_s {
     double *x = nullptr, *r = nullptr, *p = nullptr, *q = nullptr, *z = nullptr, *zold = nullptr, *t = nullptr;
     double* cheb = nullptr;  // 4n (FP64 smoothing)
     float *dinv32 = nullptr, *r32 = nullptr, *z32 = nullptr, *t32 = nullptr, *cheb32 = nullptr;  // FP32 smoothing
+    short* col16 = nullptr;  // 16-bit column offsets of the FP32 smoother matrix (when its bandwidth allows)
+    int lanes16 = 8;         // lanes per row of the 16-bit-offset smoother kernels (timed at creation)
     double *rc = nullptr, *cx = nullptr, *cr = nullptr, *cz = nullptr, *cp = nullptr, *cq = nullptr;
     double *cu = nullptr, *cw = nullptr, *cs = nullptr, *cm0 = nullptr, *cm1 = nullptr;
     ciecu::MgScalars* d_s = nullptr;
@@ -389,6 +439,32 @@ namespace ciecu {
 namespace {
 
 int grid_of(long n) { return grid_for(n, kT, 8); }
+
+// The FP32 smoother matrix with 16-bit column offsets.
+CsrArgs<float, short> args16(const ciecu_mgcg_s* M) {
+    const CsrArgs<float> a = M->S32->args<float>();
+    return CsrArgs<float, short>{a.rowptr, M->col16, a.val, a.nrows, a.nnz, a.blocks, a.nblocks, nullptr, 0,
+                                 a.aligned16};
+}
+
+long grid16(const ciecu_mgcg_s* M, int vs) {
+    const long rowsPerBlock = kVectorThreads / vs;
+    return (M->n + rowsPerBlock - 1) / rowsPerBlock;
+}
+
+// t = t - A32 z with the smoother matrix (16-bit offsets when available).
+int residual32(ciecu_mgcg_s* M, const float* z, float* t, cudaStream_t st) {
+    if (!M->col16) return ciecu_csr_spmv_f32(M->S32, 1.0f, z, -1.0f, t);
+    CIECU_TRY(with_lanes16(M->lanes16, [&](auto vv) -> int {
+        constexpr int VS = decltype(vv)::value;
+        residual16_kernel<VS><<<fit_grid(residual16_kernel<VS>, kVectorThreads, grid16(M, VS)), kVectorThreads, 0,
+                                st>>>(args16(M), z, t);
+        return CIECU_OK;
+    }));
+    count_launch();
+    CIECU_CHECK_LAUNCH("residual16_kernel");
+    return CIECU_OK;
+}
 
 // out (+)= S in: Chebyshev polynomial of degree `degree` in D^-1 A applied to in.
 template <typename T>
@@ -409,6 +485,20 @@ int chebyshev(ciecu_mgcg_s* M, ciecu_csr_s* A, const T* dinv, const T* in, T* ou
     for (int k = 1; k < M->options.degree; ++k) {
         const double rhoNew = 1.0 / (2.0 * sigma - rho);
         const T c1 = static_cast<T>(rhoNew * rho), c2 = static_cast<T>(2.0 * rhoNew / delta);
+        if constexpr (std::is_same<T, float>::value) {
+            if (M->col16) {
+                CIECU_TRY(with_lanes16(M->lanes16, [&](auto vv) -> int {
+                    constexpr int VS = decltype(vv)::value;
+                    cheb_step16_kernel<VS><<<fit_grid(cheb_step16_kernel<VS>, kVectorThreads, grid16(M, VS)),
+                                             kVectorThreads, 0, st>>>(args16(M), dinv, c1, c2, r, da, db, x);
+                    return CIECU_OK;
+                }));
+                count_launch();
+                std::swap(da, db);
+                rho = rhoNew;
+                continue;
+            }
+        }
         CIECU_TRY(with_schedule(A->kernel, [&](auto kk) -> int {
             constexpr int K = decltype(kk)::value;
             cheb_step_kernel<K, T><<<fit_grid(cheb_step_kernel<K, T>, csr_threads<K>(), grid), csr_threads<K>(), 0,
@@ -466,7 +556,7 @@ int cycle(ciecu_mgcg_s* M, cudaStream_t st) {
         count_launch();
         CIECU_TRY(chebyshev<float>(M, S, M->dinv32, M->r32, M->z32, false, M->cheb32, st));
         CIECU_CUDA(cudaMemcpyAsync(M->t32, M->r32, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
-        CIECU_TRY(ciecu_csr_spmv_f32(S, 1.0f, M->z32, -1.0f, M->t32));  // t = r - A32 z (FP32)
+        CIECU_TRY(residual32(M, M->z32, M->t32, st));  // t = r - A32 z (FP32)
         convert_kernel<float, double><<<grid_of(n), kT, 0, st>>>(n, M->t32, M->t, 0);
         count_launch();
         CIECU_TRY(ciecu_csr_spmv_f64(M->R, 0.0, M->t, 1.0, M->rc));
@@ -475,7 +565,7 @@ int cycle(ciecu_mgcg_s* M, cudaStream_t st) {
         convert_kernel<double, float><<<grid_of(n), kT, 0, st>>>(n, M->t, M->z32, 1);
         count_launch();
         CIECU_CUDA(cudaMemcpyAsync(M->t32, M->r32, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
-        CIECU_TRY(ciecu_csr_spmv_f32(S, 1.0f, M->z32, -1.0f, M->t32));
+        CIECU_TRY(residual32(M, M->z32, M->t32, st));
         CIECU_TRY(chebyshev<float>(M, S, M->dinv32, M->t32, M->z32, true, M->cheb32, st));
         convert_kernel<float, double><<<grid_of(n), kT, 0, st>>>(n, M->z32, M->z, 0);
         count_launch();
@@ -543,6 +633,61 @@ __global__ void to_f32_kernel(long n, const double* __restrict__ a, float* __res
         b[i] = static_cast<float>(a[i]);
 }
 
+// 16-bit column offsets of the FP32 smoother matrix when every |col - row| fits,
+// and the lanes per row of its kernels (the residual kernel timed, best of
+// three, on scratch vectors); otherwise the smoother keeps the int32 columns.
+int prepare_offsets16(ciecu_mgcg_s* M, cudaStream_t st) {
+    ciecu_csr_s* S = M->S32;
+    if (S->nnz <= 0) return CIECU_OK;
+    unsigned* d_bad = reinterpret_cast<unsigned*>(S->space->d_result);
+    unsigned bad = 0;
+    if (cudaMalloc(&M->col16, sizeof(short) * static_cast<size_t>(S->nnz)) != cudaSuccess) {
+        cudaGetLastError();  // no room: int32 columns
+        M->col16 = nullptr;
+        return CIECU_OK;
+    }
+    CIECU_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(unsigned), st));
+    offsets16_kernel<<<grid_for(M->n, 256, 8), 256, 0, st>>>(static_cast<int>(M->n), S->rowptr, S->col, M->col16,
+                                                             d_bad);
+    count_launch();
+    CIECU_CHECK_LAUNCH("offsets16_kernel");
+    CIECU_CUDA(cudaMemcpyAsync(&bad, d_bad, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    CIECU_CUDA(cudaStreamSynchronize(st));
+    if (bad) {
+        cudaFree(M->col16);
+        M->col16 = nullptr;
+        return CIECU_OK;
+    }
+    // t32 / z32 as scratch (the solve overwrites both)
+    CIECU_CUDA(cudaMemsetAsync(M->z32, 0, sizeof(float) * M->n, st));
+    cudaEvent_t e0, e1;
+    CIECU_CUDA(cudaEventCreate(&e0));
+    CIECU_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    int bestLanes = 8;
+    cudaError_t e = cudaSuccess;
+    for (int vs : {4, 8, 16, 32}) {
+        M->lanes16 = vs;
+        for (int trial = 0; trial < 4 && e == cudaSuccess; ++trial) {
+            cudaEventRecord(e0, st);
+            residual32(M, M->z32, M->t32, st);
+            cudaEventRecord(e1, st);
+            e = cudaEventSynchronize(e1);
+            float ms = 0.f;
+            if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+            if (trial > 0 && e == cudaSuccess && ms < best) {  // the first run warms up
+                best = ms;
+                bestLanes = vs;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e != cudaSuccess) return cuda_fail(e, "mgcg_create: smoother kernel choice");
+    M->lanes16 = bestLanes;
+    return CIECU_OK;
+}
+
 }  // namespace
 }  // namespace ciecu
 
@@ -557,6 +702,7 @@ int ciecu_mgcg_destroy(ciecu_mgcg M) {
                       M->cu, M->cw, M->cs, M->cm0, M->cm1, M->partials})
         cudaFree(v);
     for (float* v : {M->dinv32, M->r32, M->z32, M->t32, M->cheb32}) cudaFree(v);
+    cudaFree(M->col16);
     cudaFree(M->d_s);
     cudaFree(M->counter);
     if (M->h_s) cudaFreeHost(M->h_s);
@@ -632,6 +778,11 @@ int ciecu_mgcg_create(ciecu_csr fine, const double* d_fineInverseDiagonal, ciecu
     if (smoother32 && M->n > 0) {
         to_f32_kernel<<<grid_of(M->n), kT, 0, st>>>(M->n, d_fineInverseDiagonal, M->dinv32);
         count_launch();
+        const int status = prepare_offsets16(M, st);
+        if (status != CIECU_OK) {
+            ciecu_mgcg_destroy(M);
+            return status;
+        }
     }
     M->lambdaMax = options.lambdaMax;
     if (!(M->lambdaMax > 0.0) && M->n > 0) {
@@ -706,6 +857,13 @@ int ciecu_mgcg_product(ciecu_mgcg M, double inScale, const double* d_in, double 
     CIECU_CHECK_LAUNCH("mg_output_kernel");
     CIECU_CUDA(cudaStreamSynchronize(st));
     if (h_stats) *h_stats = stats;
+    return CIECU_OK;
+}
+
+int ciecu_mgcg_smoother_info(ciecu_mgcg M, int* offsets16, int* lanesPerRow) {
+    CIECU_REQUIRE(M && offsets16 && lanesPerRow, "mgcg_smoother_info: null argument");
+    *offsets16 = M->col16 ? 1 : 0;
+    *lanesPerRow = M->col16 ? M->lanes16 : 0;
     return CIECU_OK;
 }
 

@@ -36,6 +36,7 @@
 #include "dia.cuh"
 #include "sell_tma.cuh"
 
+#include <cstdint>
 #include <cstdlib>
 #include <string>
 #include <vector>
@@ -223,6 +224,7 @@ __global__ void __launch_bounds__(kT) mixed_spmv_kernel(SellArgs<float, CI> A, c
                                                         float* __restrict__ p, float* __restrict__ q, MixedScalars* s,
                                                         double* partials, unsigned* counter,
                                                         cudaGraphConditionalHandle loop) {
+    pdl_launch_dependents();
     if (*reinterpret_cast<volatile int*>(&s->done)) {
         if (blockIdx.x == 0 && threadIdx.x == 0) set_cond<COND>(loop, 0);
         return;
@@ -241,34 +243,29 @@ __global__ void __launch_bounds__(kT) mixed_spmv_kernel(SellArgs<float, CI> A, c
 }
 
 // DIA variants of the two kernels above, for inner matrices of at most 32
-// diagonals (dia.cuh): FP32 values only, no column indices.  SYM: A holds the
-// upper half of a symmetric matrix (ND = its diagonal count, main included).
-template <int ND, bool SYM, typename Op>
-__device__ __forceinline__ void mixed_dia_rows(const DiaArgs<float>& A, const float* __restrict__ x, Op& op) {
-    if constexpr (SYM)
-        dia_rows4_sym<ND>(A, x, op);
-    else
-        dia_rows4<ND>(A, x, op);
-}
-
-template <int ND, bool SYM>
+// diagonals (dia.cuh): FP32 values only, no column indices.  The full copy is read
+// even when it is symmetric: reading the lower half back from the upper one (as
+// the FP64 PCG does) measured slower here, where every row pass is already a
+// four-row, 16-byte-load stream.
+template <int ND>
 __global__ void __launch_bounds__(kT) mixed_apply_dia_kernel(DiaArgs<float> A, const float* __restrict__ x,
                                                             float* __restrict__ y) {
     StoreOp op{y};
-    mixed_dia_rows<ND, SYM>(A, x, op);
+    dia_rows4<ND>(A, x, op);
 }
 
-template <int ND, bool COND, bool FUSED, bool SYM>
+template <int ND, bool COND, bool FUSED>
 __global__ void __launch_bounds__(kT) mixed_spmv_dia_kernel(DiaArgs<float> A, const float* __restrict__ x,
                                                            float* __restrict__ p, float* __restrict__ q,
                                                            MixedScalars* s, double* partials, unsigned* counter,
                                                            cudaGraphConditionalHandle loop) {
+    pdl_launch_dependents();
     if (*reinterpret_cast<volatile int*>(&s->done)) {
         if (blockIdx.x == 0 && threadIdx.x == 0) set_cond<COND>(loop, 0);
         return;
     }
     auto op = M1Op<FUSED>::make(x, p, q, s);
-    mixed_dia_rows<ND, SYM>(A, x, op);
+    dia_rows4<ND>(A, x, op);
     double mine[1] = {op.acc}, tot[1];
     if (grid_reduce_last<1, kT>(mine, partials, counter, tot) && threadIdx.x == 0) {
         s->pq = tot[0];
@@ -339,6 +336,7 @@ __global__ void __launch_bounds__(kT) mixed_update_kernel(long n, float* __restr
                                                           double* partials, unsigned* counter,
                                                           cudaGraphConditionalHandle loop,
                                                           cudaGraphConditionalHandle refine) {
+    pdl_wait();  // launched programmatically after M1: wait for it (no-op otherwise)
     if (*reinterpret_cast<volatile int*>(&s->done)) {
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             set_cond<COND>(loop, 0);
@@ -591,7 +589,6 @@ struct ciecu_mixed_s {
                      // kDiaInner = the DIA copy)
     bool sellBuilt = false;  // the SELL copy exists (not built when the DIA copy is the known choice)
     float* dia32 = nullptr;  // DIA copy of the inner matrix (few-diagonal matrices only)
-    bool diaSym = false;     // dia32 holds the upper half of a bitwise symmetric matrix
     ciecu::DiaArgs<float> dia{};
     // SELL-32 inner matrix
     int nslices = 0;
@@ -633,6 +630,30 @@ int with_unroll(int u, F&& f) {
     }
 }
 
+// Experiment switches of the inner iteration's vector kernels (M2, M3):
+// CIECU_MIXED_VBLOCKS=k caps their grids at k CTAs per SM (default: every
+// resident CTA); CIECU_MIXED_PDL=1 launches M2 programmatically after M1.
+int env_int(const char* name, int fallback) {
+    const char* v = std::getenv(name);
+    return v ? std::atoi(v) : fallback;
+}
+
+bool pdl_enabled() {
+    static const bool enabled = env_int("CIECU_MIXED_PDL", 0) == 1;
+    return enabled;
+}
+
+template <typename K>
+int vector_grid(K* kernel, long need) {
+    static const int perSm = env_int("CIECU_MIXED_VBLOCKS", 0);
+    const int g = fit_grid(kernel, kT, need);
+    if (perSm <= 0) return g;
+    int sms = 0, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return std::max(1, std::min(g, perSm * sms));
+}
+
 // M1 with the autotuned variant: TMA pipeline (unroll == 0), the DIA copy
 // (unroll == kDiaInner) or U register groups.  FUSED gathers z (the direction
 // recurrences run in the epilogue), otherwise p.
@@ -641,18 +662,13 @@ int launch_inner_spmv_form(ciecu_mixed_s* M, cudaStream_t st, cudaGraphCondition
     const long needA = (M->n + kT - 1) / kT;
     const float* x = FUSED ? M->z32 : M->p32;
     if (M->unroll == kDiaInner) {
-        auto go = [&](auto nd, auto sym) -> int {
+        CIECU_TRY(with_diagonals(M->dia.ndiag, [&](auto nd) -> int {
             constexpr int ND = decltype(nd)::value;
-            constexpr bool SYM = decltype(sym)::value;
-            auto* kernel = mixed_spmv_dia_kernel<ND, COND, FUSED, SYM>;
+            auto* kernel = mixed_spmv_dia_kernel<ND, COND, FUSED>;
             kernel<<<fit_grid(kernel, kT, (needA + 3) / 4), kT, 0, st>>>(M->dia, x, M->p32, M->q32, M->d_s,
                                                                          M->d_partials, M->d_counter, loop);
             return CIECU_OK;
-        };
-        if (M->diaSym)
-            CIECU_TRY(with_upper_diagonals(M->dia.ndiag, [&](auto nd) { return go(nd, std::true_type{}); }));
-        else
-            CIECU_TRY(with_diagonals(M->dia.ndiag, [&](auto nd) { return go(nd, std::false_type{}); }));
+        }));
         CIECU_CHECK_LAUNCH("mixed_spmv_dia_kernel");
         return CIECU_OK;
     }
@@ -703,14 +719,29 @@ int launch_inner(ciecu_mixed_s* M, cudaStream_t st, cudaGraph_t root, cudaGraphC
     cudaGraphConditionalHandle refine = 0;
     if (useCond) CIECU_CUDA(cudaGraphConditionalHandleCreate(&refine, root, 0, cudaGraphCondAssignDefault));
     CIECU_TRY(launch_inner_spmv<COND>(M, st, loop));
-    if (M->z32)
-        mixed_update_kernel<COND, true><<<fit_grid(mixed_update_kernel<COND, true>, kT, needV), kT, 0, st>>>(
-            M->n, M->x32, M->r32, M->z32, M->p32, M->q32, M->dinv32, M->d_s, M->d_partials, M->d_counter, loop,
-            refine);
-    else
-        mixed_update_kernel<COND, false><<<fit_grid(mixed_update_kernel<COND, false>, kT, needV), kT, 0, st>>>(
-            M->n, M->x32, M->r32, nullptr, M->p32, M->q32, M->dinv32, M->d_s, M->d_partials, M->d_counter, loop,
-            refine);
+    {
+        auto* kernel = M->z32 ? mixed_update_kernel<COND, true> : mixed_update_kernel<COND, false>;
+        const int grid = vector_grid(kernel, needV);
+        if (pdl_enabled()) {
+            // programmatic launch: M2's CTAs are scheduled while M1 drains and wait
+            // (griddepcontrol.wait) until M1 has completed
+            cudaLaunchConfig_t cfg{};
+            cfg.gridDim = dim3(grid);
+            cfg.blockDim = dim3(kT);
+            cfg.stream = st;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+            attr[0].val.programmaticStreamSerializationAllowed = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            CIECU_CUDA(cudaLaunchKernelEx(&cfg, kernel, M->n, M->x32, M->r32, M->z32, static_cast<const float*>(M->p32),
+                                          static_cast<const float*>(M->q32), static_cast<const float*>(M->dinv32),
+                                          M->d_s, M->d_partials, M->d_counter, loop, refine));
+        } else {
+            kernel<<<grid, kT, 0, st>>>(M->n, M->x32, M->r32, M->z32, M->p32, M->q32, M->dinv32, M->d_s,
+                                        M->d_partials, M->d_counter, loop, refine);
+        }
+    }
     auto refinement = [&](cudaStream_t s2) -> int {
         mixed_fold_kernel<<<fit_grid(mixed_fold_kernel, kT, needA), kT, 0, s2>>>(M->n, M->x64, M->x32, M->sdiag,
                                                                                 M->d_s);
@@ -731,8 +762,8 @@ int launch_inner(ciecu_mixed_s* M, cudaStream_t st, cudaGraph_t root, cudaGraphC
     else
         CIECU_TRY(refinement(st));
     if (!M->z32)
-        mixed_direction_kernel<<<fit_grid(mixed_direction_kernel, kT, needV), kT, 0, st>>>(M->n, M->p32, M->r32,
-                                                                                           M->dinv32, M->d_s);
+        mixed_direction_kernel<<<vector_grid(mixed_direction_kernel, needV), kT, 0, st>>>(M->n, M->p32, M->r32,
+                                                                                          M->dinv32, M->d_s);
     CIECU_CHECK_LAUNCH("mixed inner iteration");
     return CIECU_OK;
 }
@@ -936,21 +967,6 @@ int ciecu_mixed_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_sta
                 M->dia = a;
                 if (e == cudaSuccess) status = dia_fill_f32(lhs, M->dia, M->dia32, M->sdiag, st);
                 if (e != cudaSuccess) status = cuda_fail(e, "mixed_create: DIA copy");
-                // a bitwise symmetric copy keeps only its upper half (about half the
-                // bytes per SpMV; the lower terms are read back through L2)
-                if (status == CIECU_OK && dia_symmetric_enabled()) {
-                    DiaArgs<float> upper{};
-                    float* uval = nullptr;
-                    bool sym = false;
-                    status = dia_symmetric_upper_f32(M->dia, &upper, &uval, st,
-                                                     reinterpret_cast<unsigned*>(lhs->space->d_result), &sym);
-                    if (status == CIECU_OK && sym) {
-                        cudaFree(M->dia32);
-                        M->dia32 = uval;
-                        M->dia = upper;
-                        M->diaSym = true;
-                    }
-                }
             } else {
                 cudaGetLastError();  // no room for the copy: the SELL kernels stay
                 M->dia32 = nullptr;
@@ -1107,17 +1123,12 @@ int ciecu_mixed_apply_f32(ciecu_mixed M, const float* d_in, float* d_out) {
     cudaStream_t st = M->A->space->stream;
     const long need = (M->n + kT - 1) / kT;
     if (M->unroll == kDiaInner) {
-        auto go = [&](auto nd, auto sym) -> int {
+        CIECU_TRY(with_diagonals(M->dia.ndiag, [&](auto nd) -> int {
             constexpr int ND = decltype(nd)::value;
-            constexpr bool SYM = decltype(sym)::value;
-            auto* kernel = mixed_apply_dia_kernel<ND, SYM>;
+            auto* kernel = mixed_apply_dia_kernel<ND>;
             kernel<<<fit_grid(kernel, kT, (need + 3) / 4), kT, 0, st>>>(M->dia, d_in, d_out);
             return CIECU_OK;
-        };
-        if (M->diaSym)
-            CIECU_TRY(with_upper_diagonals(M->dia.ndiag, [&](auto nd) { return go(nd, std::true_type{}); }));
-        else
-            CIECU_TRY(with_diagonals(M->dia.ndiag, [&](auto nd) { return go(nd, std::false_type{}); }));
+        }));
         count_launch();
         CIECU_CHECK_LAUNCH("mixed_apply_dia_kernel");
         return CIECU_OK;
@@ -1156,13 +1167,6 @@ int ciecu_mixed_apply_f32(ciecu_mixed M, const float* d_in, float* d_out) {
 int ciecu_mixed_padded_entries(ciecu_mixed M, int64_t* h_entries) {
     CIECU_REQUIRE(M && h_entries, "mixed_padded_entries: null argument");
     *h_entries = M->paddedEntries;
-    return CIECU_OK;
-}
-
-int ciecu_mixed_dia_info(ciecu_mixed M, int* storedDiagonals, int* symmetric) {
-    CIECU_REQUIRE(M && storedDiagonals && symmetric, "mixed_dia_info: null argument");
-    *storedDiagonals = M->dia32 ? M->dia.ndiag : 0;
-    *symmetric = M->diaSym ? 1 : 0;
     return CIECU_OK;
 }
 

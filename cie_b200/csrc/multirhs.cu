@@ -545,28 +545,37 @@ __global__ void __launch_bounds__(kT) multi_update32_kernel(long n, int k, float
     const bool last = column_reduce_last<KP, 2>(mine, k, partials, counter, tot);
     if (!last) return;
     __syncthreads();
+    // The replacement recomputes B - A X for all columns in one FP64 SpMM, so when
+    // one column asks for it every running column takes it: the columns' triggers
+    // then stay in step (about one replacement per delta-fold drop) instead of one
+    // SpMM for each column's own schedule.
+    bool running = false, updateX = false;
     if (threadIdx.x < k) {
         ColumnScalars& s = S[threadIdx.x];
-        if (!s.done) {
+        running = !s.done;
+        if (running) {
             const double rnorm = sqrt(tot[0]);
             s.iter += 1;
             if (rnorm > s.maxrx) s.maxrx = rnorm;
             if (rnorm > s.maxrr) s.maxrr = rnorm;
-            const bool updateX = rnorm < g->delta * s.maxrx;
+            updateX = rnorm < g->delta * s.maxrx;
             const bool update = updateX || rnorm < g->delta * s.maxrr || rnorm < g->relTol * s.r0 ||
                                 rnorm < g->absTol || s.iter >= g->maxIter || s.restart;
-            s.updateX = updateX ? 1 : 0;
-            if (update) {
-                s.pending = 1;
-                s.rzPending = tot[1];
-                atomicOr(&s_any, 1u);
-            } else {
-                s.beta = tot[1] / s.rz;
-                s.rz = tot[1];
-            }
+            if (update) atomicOr(&s_any, 1u);
         }
     }
     __syncthreads();
+    if (threadIdx.x < k && running) {
+        ColumnScalars& s = S[threadIdx.x];
+        if (s_any) {
+            s.pending = 1;
+            s.updateX = updateX ? 1 : 0;
+            s.rzPending = tot[1];
+        } else {
+            s.beta = tot[1] / s.rz;
+            s.rz = tot[1];
+        }
+    }
     if (threadIdx.x == 0) {
         g->anyPending = s_any;
         set_loop<COND>(replace, s_any);

@@ -192,7 +192,10 @@ class TwoLevelCG(LinearOperator):
     def info(self):
         lam, cycles = ctypes.c_double(), ctypes.c_int64()
         call("ciecu_mgcg_info", self.handle, ctypes.byref(lam), ctypes.byref(cycles))
-        return {"lambda_max": lam.value, "cycles": cycles.value}
+        o16, lanes = ctypes.c_int(), ctypes.c_int()
+        call("ciecu_mgcg_smoother_info", self.handle, ctypes.byref(o16), ctypes.byref(lanes))
+        return {"lambda_max": lam.value, "cycles": cycles.value, "smoother_offsets16": bool(o16.value),
+                "smoother_lanes_per_row": lanes.value}
 
 
 def make_two_level_cg(space, problem, settings, center=None, radius=0.4, alpha=1e-6, depth=2, degree=2,

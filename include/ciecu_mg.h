@@ -50,6 +50,11 @@ int ciecu_mgcg_product(ciecu_mgcg solver, double inScale, const double* d_in, do
                        ciecu_statistics* h_stats);
 /* The smoother's spectral bound and the cycles applied by the last solve. */
 int ciecu_mgcg_info(ciecu_mgcg solver, double* h_lambdaMax, int64_t* h_cycles);
+/* The FP32 smoother's column storage: offsets16 = 1 when it reads 16-bit column
+ * offsets from the row (every |col - row| < 2^15; 6 instead of 8 bytes per entry,
+ * built at creation), with the lanes per row chosen by timing; 0 / 0 otherwise
+ * (int32 columns through the CSR handle's own tuned kernel, or no FP32 smoother). */
+int ciecu_mgcg_smoother_info(ciecu_mgcg solver, int* offsets16, int* lanesPerRow);
 
 #ifdef __cplusplus
 }

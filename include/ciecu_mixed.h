@@ -79,11 +79,6 @@ int ciecu_mixed_set_graph_chunk(ciecu_mixed solver, int iterations);
 int ciecu_mixed_apply_f32(ciecu_mixed solver, const float* d_in, float* d_out);
 /* Stored entries of the SELL-32 inner matrix, padding included (>= nnz). */
 int ciecu_mixed_padded_entries(ciecu_mixed solver, int64_t* h_entries);
-/* The FP32 diagonal-storage copy: its stored diagonals (0: none) and whether it
- * holds only the upper half (main diagonal included) of a bitwise symmetric
- * matrix, the lower entries being read back from it (about half the bytes per
- * inner SpMV; CIECU_DIA_SYMMETRIC=0 in the environment keeps the full copy). */
-int ciecu_mixed_dia_info(ciecu_mixed solver, int* storedDiagonals, int* symmetric);
 /* out = inScale*out + outScale*x, x the refined solution (initial guess = out). */
 int ciecu_mixed_product(ciecu_mixed solver, double inScale, const double* d_in, double outScale, double* d_out,
                         ciecu_mixed_statistics* h_stats);

@@ -36,11 +36,12 @@ int ciecu_multi_format(ciecu_multi solver, int* diagonals);
  * copies of the matrix in the format of the FP64 solve and of D^-1, FP32 blocks,
  * FP64 dot products) with FP64 reliable updates: when a column's FP32 residual
  * norm fell below delta times its largest value since the last replacement (or
- * below the stopping tolerance, or at the iteration limit), its FP32 solution is
- * added to the FP64 one and its residual recomputed as B - A X in FP64; the
- * stopping test and the statistics use that FP64 residual (iterationCount =
- * FP32 iterations).  delta = 0 (default): FP64 iterations as
- * ConjugateGradients::product. */
+ * below the stopping tolerance, or at the iteration limit), every running
+ * column's FP32 solution is added to its FP64 one and its residual recomputed as
+ * B - A X in FP64 (one FP64 SpMM serves all columns, so the columns replace
+ * together); each column keeps its search direction.  The stopping test and the
+ * statistics use that FP64 residual (iterationCount = FP32 iterations).  delta =
+ * 0 (default): FP64 iterations as ConjugateGradients::product. */
 int ciecu_multi_set_refinement(ciecu_multi solver, double delta);
 /* FP64 residual recomputations of each column in the last refined solve. */
 int ciecu_multi_refinements(ciecu_multi solver, int64_t* h_perColumn);

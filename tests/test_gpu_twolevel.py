@@ -82,3 +82,7 @@ def test_device_two_level_cg_vs_reference(reference, precision, degree, coarse):
     assert np.linalg.norm(r) <= bar * np.linalg.norm(b)
     assert rel <= 1e-9
     assert st.iterationCount < sr[0] / 2
+    if precision == "f32":
+        # the Q3 stencil's column offsets fit in 16 bits at this size: the FP32
+        # smoother reads 6 bytes per entry
+        assert solver.info()["smoother_offsets16"] and solver.info()["smoother_lanes_per_row"] in (4, 8, 16, 32)
