@@ -49,7 +49,7 @@ DELTA = 0.1
 FUSE = False
 # Two-level CG on the finite-cell Q3 sphere: (smoothing precision, Chebyshev
 # degree, pipelined coarse PCG iterations per cycle)
-TWO_LEVEL = (("f64", 4, 80), ("f32", 6, 150))
+TWO_LEVEL = (("f64", 4, 80), ("f32", 6, 80))
 METRIC = "PCG time-to-1e-10 (s), 3D Q1 128^3 Poisson"
 
 

@@ -52,13 +52,6 @@ __device__ __forceinline__ T stream_ld(const T* p) {
     return __ldcs(p);
 }
 
-// Programmatic dependent launch (sm_90+ PTX): a kernel lets the next, launched
-// with programmatic stream serialization, start scheduling its CTAs; that kernel
-// waits at pdl_wait() until this one has completed and its writes are visible.
-// Both are no-ops for kernels launched the ordinary way.
-__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;"); }
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-
 // Nanoseconds of the GPU's global timer: a bound on a wait in wall-clock time,
 // independent of the SM clock and of the SM the thread runs on.
 __device__ __forceinline__ unsigned long long global_ns() {

@@ -224,7 +224,6 @@ __global__ void __launch_bounds__(kT) mixed_spmv_kernel(SellArgs<float, CI> A, c
                                                         float* __restrict__ p, float* __restrict__ q, MixedScalars* s,
                                                         double* partials, unsigned* counter,
                                                         cudaGraphConditionalHandle loop) {
-    pdl_launch_dependents();
     if (*reinterpret_cast<volatile int*>(&s->done)) {
         if (blockIdx.x == 0 && threadIdx.x == 0) set_cond<COND>(loop, 0);
         return;
@@ -259,7 +258,6 @@ __global__ void __launch_bounds__(kT) mixed_spmv_dia_kernel(DiaArgs<float> A, co
                                                            float* __restrict__ p, float* __restrict__ q,
                                                            MixedScalars* s, double* partials, unsigned* counter,
                                                            cudaGraphConditionalHandle loop) {
-    pdl_launch_dependents();
     if (*reinterpret_cast<volatile int*>(&s->done)) {
         if (blockIdx.x == 0 && threadIdx.x == 0) set_cond<COND>(loop, 0);
         return;
@@ -336,7 +334,6 @@ __global__ void __launch_bounds__(kT) mixed_update_kernel(long n, float* __restr
                                                           double* partials, unsigned* counter,
                                                           cudaGraphConditionalHandle loop,
                                                           cudaGraphConditionalHandle refine) {
-    pdl_wait();  // launched programmatically after M1: wait for it (no-op otherwise)
     if (*reinterpret_cast<volatile int*>(&s->done)) {
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             set_cond<COND>(loop, 0);
@@ -630,30 +627,6 @@ int with_unroll(int u, F&& f) {
     }
 }
 
-// Experiment switches of the inner iteration's vector kernels (M2, M3):
-// CIECU_MIXED_VBLOCKS=k caps their grids at k CTAs per SM (default: every
-// resident CTA); CIECU_MIXED_PDL=1 launches M2 programmatically after M1.
-int env_int(const char* name, int fallback) {
-    const char* v = std::getenv(name);
-    return v ? std::atoi(v) : fallback;
-}
-
-bool pdl_enabled() {
-    static const bool enabled = env_int("CIECU_MIXED_PDL", 0) == 1;
-    return enabled;
-}
-
-template <typename K>
-int vector_grid(K* kernel, long need) {
-    static const int perSm = env_int("CIECU_MIXED_VBLOCKS", 0);
-    const int g = fit_grid(kernel, kT, need);
-    if (perSm <= 0) return g;
-    int sms = 0, dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    return std::max(1, std::min(g, perSm * sms));
-}
-
 // M1 with the autotuned variant: TMA pipeline (unroll == 0), the DIA copy
 // (unroll == kDiaInner) or U register groups.  FUSED gathers z (the direction
 // recurrences run in the epilogue), otherwise p.
@@ -721,26 +694,8 @@ int launch_inner(ciecu_mixed_s* M, cudaStream_t st, cudaGraph_t root, cudaGraphC
     CIECU_TRY(launch_inner_spmv<COND>(M, st, loop));
     {
         auto* kernel = M->z32 ? mixed_update_kernel<COND, true> : mixed_update_kernel<COND, false>;
-        const int grid = vector_grid(kernel, needV);
-        if (pdl_enabled()) {
-            // programmatic launch: M2's CTAs are scheduled while M1 drains and wait
-            // (griddepcontrol.wait) until M1 has completed
-            cudaLaunchConfig_t cfg{};
-            cfg.gridDim = dim3(grid);
-            cfg.blockDim = dim3(kT);
-            cfg.stream = st;
-            cudaLaunchAttribute attr[1];
-            attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-            attr[0].val.programmaticStreamSerializationAllowed = 1;
-            cfg.attrs = attr;
-            cfg.numAttrs = 1;
-            CIECU_CUDA(cudaLaunchKernelEx(&cfg, kernel, M->n, M->x32, M->r32, M->z32, static_cast<const float*>(M->p32),
-                                          static_cast<const float*>(M->q32), static_cast<const float*>(M->dinv32),
-                                          M->d_s, M->d_partials, M->d_counter, loop, refine));
-        } else {
-            kernel<<<grid, kT, 0, st>>>(M->n, M->x32, M->r32, M->z32, M->p32, M->q32, M->dinv32, M->d_s,
-                                        M->d_partials, M->d_counter, loop, refine);
-        }
+        kernel<<<fit_grid(kernel, kT, needV), kT, 0, st>>>(M->n, M->x32, M->r32, M->z32, M->p32, M->q32, M->dinv32,
+                                                           M->d_s, M->d_partials, M->d_counter, loop, refine);
     }
     auto refinement = [&](cudaStream_t s2) -> int {
         mixed_fold_kernel<<<fit_grid(mixed_fold_kernel, kT, needA), kT, 0, s2>>>(M->n, M->x64, M->x32, M->sdiag,
@@ -762,8 +717,8 @@ int launch_inner(ciecu_mixed_s* M, cudaStream_t st, cudaGraph_t root, cudaGraphC
     else
         CIECU_TRY(refinement(st));
     if (!M->z32)
-        mixed_direction_kernel<<<vector_grid(mixed_direction_kernel, needV), kT, 0, st>>>(M->n, M->p32, M->r32,
-                                                                                          M->dinv32, M->d_s);
+        mixed_direction_kernel<<<fit_grid(mixed_direction_kernel, kT, needV), kT, 0, st>>>(M->n, M->p32, M->r32,
+                                                                                           M->dinv32, M->d_s);
     CIECU_CHECK_LAUNCH("mixed inner iteration");
     return CIECU_OK;
 }
