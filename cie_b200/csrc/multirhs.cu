@@ -545,10 +545,16 @@ __global__ void __launch_bounds__(kT) multi_update32_kernel(long n, int k, float
     const bool last = column_reduce_last<KP, 2>(mine, k, partials, counter, tot);
     if (!last) return;
     __syncthreads();
-    // The replacement recomputes B - A X for all columns in one FP64 SpMM, so when
-    // one column asks for it every running column takes it: the columns' triggers
-    // then stay in step (about one replacement per delta-fold drop) instead of one
-    // SpMM for each column's own schedule.
+    // The replacement recomputes B - A X for all columns in one FP64 SpMM, so it is
+    // taken by every running column at once, and only when it is due for the batch:
+    // when some column must stop or restart (FP32 residual below the tolerance,
+    // iteration limit, FP32 breakdown), or when at least half of the running
+    // columns have seen their FP32 residual drop by delta.  A column whose drop
+    // came early keeps iterating until then (reliable updates bound the drift by
+    // the drop, not by the iteration).
+    __shared__ unsigned s_running, s_wanting;
+    if (threadIdx.x == 0) s_running = s_wanting = 0u;
+    __syncthreads();
     bool running = false, updateX = false;
     if (threadIdx.x < k) {
         ColumnScalars& s = S[threadIdx.x];
@@ -559,11 +565,15 @@ __global__ void __launch_bounds__(kT) multi_update32_kernel(long n, int k, float
             if (rnorm > s.maxrx) s.maxrx = rnorm;
             if (rnorm > s.maxrr) s.maxrr = rnorm;
             updateX = rnorm < g->delta * s.maxrx;
-            const bool update = updateX || rnorm < g->delta * s.maxrr || rnorm < g->relTol * s.r0 ||
-                                rnorm < g->absTol || s.iter >= g->maxIter || s.restart;
-            if (update) atomicOr(&s_any, 1u);
+            const bool want = updateX || rnorm < g->delta * s.maxrr;
+            const bool must = rnorm < g->relTol * s.r0 || rnorm < g->absTol || s.iter >= g->maxIter || s.restart;
+            atomicAdd(&s_running, 1u);
+            if (want) atomicAdd(&s_wanting, 1u);
+            if (must) atomicOr(&s_any, 1u);
         }
     }
+    __syncthreads();
+    if (threadIdx.x == 0 && 2u * s_wanting >= s_running && s_wanting > 0u) s_any = 1u;
     __syncthreads();
     if (threadIdx.x < k && running) {
         ColumnScalars& s = S[threadIdx.x];

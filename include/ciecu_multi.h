@@ -34,14 +34,16 @@ int ciecu_multi_info(ciecu_multi solver, int* lanesPerRow, int* deviceLoop);
 int ciecu_multi_format(ciecu_multi solver, int* diagonals);
 /* delta in (0, 1): FP32-refined form -- every column iterates in FP32 (FP32
  * copies of the matrix in the format of the FP64 solve and of D^-1, FP32 blocks,
- * FP64 dot products) with FP64 reliable updates: when a column's FP32 residual
- * norm fell below delta times its largest value since the last replacement (or
- * below the stopping tolerance, or at the iteration limit), every running
- * column's FP32 solution is added to its FP64 one and its residual recomputed as
- * B - A X in FP64 (one FP64 SpMM serves all columns, so the columns replace
- * together); each column keeps its search direction.  The stopping test and the
- * statistics use that FP64 residual (iterationCount = FP32 iterations).  delta =
- * 0 (default): FP64 iterations as ConjugateGradients::product. */
+ * FP64 dot products) with FP64 reliable updates: every running column's FP32
+ * solution is added to its FP64 one and its residual recomputed as B - A X in
+ * FP64 (one FP64 SpMM serves all columns, so they replace together) when some
+ * column's FP32 residual norm fell below the stopping tolerance, or it hit the
+ * iteration limit or an FP32 breakdown, or when at least half of the running
+ * columns saw their FP32 residual norm fall below delta times its largest value
+ * since the last replacement; each column keeps its search direction.  The
+ * stopping test and the statistics use that FP64 residual (iterationCount = FP32
+ * iterations).  delta = 0 (default): FP64 iterations as
+ * ConjugateGradients::product. */
 int ciecu_multi_set_refinement(ciecu_multi solver, double delta);
 /* FP64 residual recomputations of each column in the last refined solve. */
 int ciecu_multi_refinements(ciecu_multi solver, int64_t* h_perColumn);
