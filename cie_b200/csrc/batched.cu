@@ -1047,8 +1047,13 @@ int ciecu_batch_destroy(ciecu_batch B) {
 
 int ciecu_batch_info(ciecu_batch B, int* lanesPerRow, int* deviceLoop, int64_t* tiles) {
     CIECU_REQUIRE(B, "batch_info: null solver");
-    if (lanesPerRow) *lanesPerRow = B->f64.lanes;
-    if (deviceLoop) *deviceLoop = B->f64.deviceLoop ? 1 : 0;
+    // the form the next solve runs: reliable updates (FP32 lanes, its own graph),
+    // restarted refinement (FP32 lanes) or FP64
+    const bool reliable = B->reliableDelta > 0.0;
+    const bool f32 = reliable || B->innerTolerance > 0.0;
+    if (lanesPerRow) *lanesPerRow = f32 ? B->f32.lanes : B->f64.lanes;
+    if (deviceLoop)
+        *deviceLoop = (reliable ? B->relDeviceLoop : (f32 ? B->f32.deviceLoop : B->f64.deviceLoop)) ? 1 : 0;
     if (tiles) *tiles = B->ntiles;
     return CIECU_OK;
 }

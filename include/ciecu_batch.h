@@ -29,7 +29,9 @@ int ciecu_batch_create(ciecu_csr lhs, int64_t systems, const int64_t* h_rowOffse
                        const double* d_inverseDiagonal, ciecu_statistics settings, ciecu_batch* out);
 int ciecu_batch_destroy(ciecu_batch solver);
 /* Lanes per row chosen by the autotuner, whether the solve loop runs on the device
- * (conditional graph nodes), and the number of row tiles. */
+ * (conditional graph nodes), and the number of row tiles -- of the form the solver
+ * is set to (FP64, restarted FP32 refinement or FP32 with reliable updates; the
+ * loop flag is known once that form has solved). */
 int ciecu_batch_info(ciecu_batch solver, int* lanesPerRow, int* deviceLoop, int64_t* tiles);
 /* All systems at once: initial guess = d_out; on return out = inScale*out +
  * outScale*x per row.  h_stats (may be NULL): one ciecu_statistics per system.
