@@ -125,6 +125,7 @@ SIGNATURES = {
     "ciecu_multi_destroy": (c_int, [P]),
     "ciecu_multi_info": (c_int, [P, P, P]),
     "ciecu_multi_format": (c_int, [P, P]),
+    "ciecu_multi_set_format": (c_int, [P, c_int]),
     "ciecu_multi_set_refinement": (c_int, [P, c_double]),
     "ciecu_multi_refinements": (c_int, [P, P]),
     "ciecu_multi_product": (c_int, [P, c_double, P, c_double, P, P]),

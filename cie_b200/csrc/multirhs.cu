@@ -891,6 +891,87 @@ __device__ __forceinline__ void quad_rows(const DiaArgs<V>& D, const T* __restri
     }
 }
 
+// The DIA pass for stencils whose sorted offsets come in consecutive triples
+// (o - 1, o, o + 1) -- the 27- and 9-diagonal Q1 stencils: a lane keeps its four
+// columns of FOUR consecutive rows (a warp sixteen rows), and for every triple
+// loads the six operand rows r + o - 1 .. r + o + 4 once, where the one-row
+// layout above loads twelve (each of the four rows' three neighbours).  The
+// diagonal values of the four rows are one 16-byte (FP32) or two (FP64) loads,
+// the same address for the eight lanes of a row group.  Triples in ascending
+// order and the three diagonals of a triple in order keep every row sum in the
+// CSR column order (out-of-range operand rows are zeros, as above), so the sums
+// are those of quad_rows.
+template <typename V, typename T, typename Op>
+__device__ __forceinline__ void quad_rows_dia3(const DiaArgs<V>& D, const T* __restrict__ X, Op& op) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int slot = lane / kQuadLanes, c0 = (lane % kQuadLanes) * 4;
+    const T* __restrict__ xc = X + c0;
+    const int n = D.nrows;
+    const int triples = D.ndiag / 3;
+    const long stride = static_cast<long>(gridDim.x) * kWarps * 16;
+    for (long r0l = (static_cast<long>(blockIdx.x) * kWarps + warp) * 16 + 4 * slot; r0l < n; r0l += stride) {
+        const int r0 = static_cast<int>(r0l);
+        T acc[4][4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int u = 0; u < 4; ++u) acc[i][u] = T(0);
+#pragma unroll 1
+        for (int t = 0; t < triples; ++t) {
+            const int o = D.off[3 * t + 1];
+            T xr[6][4];
+#pragma unroll
+            for (int j = 0; j < 6; ++j) {
+                const int c = r0 + o - 1 + j;
+                if (static_cast<unsigned>(c) < static_cast<unsigned>(n)) {
+                    Quad<T>::load(xc + static_cast<long>(c) * 32, xr[j]);
+                } else {
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) xr[j][u] = T(0);
+                }
+            }
+#pragma unroll
+            for (int e = 0; e < 3; ++e) {
+                V v[4];
+                Quad<V>::load(D.val + static_cast<long>(3 * t + e) * D.ld + r0, v);
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) acc[i][u] = fma(static_cast<T>(v[i]), xr[i + e][u], acc[i][u]);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            if (r0 + i < n) op.quad(r0 + i, c0, acc[i]);
+    }
+}
+
+// Whether the sorted offsets come in consecutive triples (o - 1, o, o + 1).
+inline bool dia_triples(const DiaArgs<double>& d) {
+    if (d.ndiag == 0 || d.ndiag % 3 != 0) return false;
+    for (int t = 0; t < d.ndiag / 3; ++t)
+        if (d.off[3 * t] + 1 != d.off[3 * t + 1] || d.off[3 * t + 1] + 1 != d.off[3 * t + 2]) return false;
+    return true;
+}
+
+// The DIA pass of the k = 32 kernels: triples when the stencil has them.
+template <bool TRIPLES, typename V, typename T, typename Op>
+__device__ __forceinline__ void quad_rows_dia(const DiaArgs<V>& D, const T* __restrict__ X, Op& op) {
+    if constexpr (TRIPLES)
+        quad_rows_dia3(D, X, op);
+    else
+        quad_rows(D, X, op);
+}
+
+template <bool TRIPLES, typename V, typename T, typename Op>
+__device__ __forceinline__ void quad_pass(const CsrArgs<V>& A, const T* __restrict__ X, Op& op) {
+    quad_rows(A, X, op);
+}
+template <bool TRIPLES, typename V, typename T, typename Op>
+__device__ __forceinline__ void quad_pass(const DiaArgs<V>& D, const T* __restrict__ X, Op& op) {
+    quad_rows_dia<TRIPLES>(D, X, op);
+}
+
 // Per-column totals of four-column partial sums (thread: columns c0 .. c0+3 of
 // its rows): summed over the warp's four row slots, then lane c takes column c,
 // and the column reduction of the row-per-warp kernels finishes the job.
@@ -971,7 +1052,7 @@ struct TrueResidualQuad {
 
 // K1 for k = 32 over either format; FP64 (the plain form) or FP32 (the refined
 // form, whose breakdowns restart).
-template <typename MA, typename T, bool COND>
+template <typename MA, typename T, bool COND, bool TRIPLES = false>
 __global__ void __launch_bounds__(kT) multi_spmv_quad_kernel(MA A, const T* __restrict__ P, T* __restrict__ Q,
                                                              ColumnScalars* S, MultiGlobal* g, double* partials,
                                                              unsigned* counter, cudaGraphConditionalHandle cond) {
@@ -980,7 +1061,7 @@ __global__ void __launch_bounds__(kT) multi_spmv_quad_kernel(MA A, const T* __re
         return;
     }
     PqQuad<T> op{P, Q, {{0.0, 0.0, 0.0, 0.0}}};
-    quad_rows(A, P, op);
+    quad_pass<TRIPLES>(A, P, op);
     double tot[1];
     if (quad_reduce_last<1>(op.acc, partials, counter, tot) && threadIdx.x < 32) {
         ColumnScalars& s = S[threadIdx.x];
@@ -1000,14 +1081,14 @@ __global__ void __launch_bounds__(kT) multi_spmv_quad_kernel(MA A, const T* __re
     }
 }
 
-template <typename MA>
+template <typename MA, bool TRIPLES = false>
 __global__ void __launch_bounds__(kT) multi_residual_quad_kernel(MA A, const double* __restrict__ X,
                                                                  const double* __restrict__ B, double* __restrict__ R) {
     ResidualQuad op{B, R};
-    quad_rows(A, X, op);
+    quad_pass<TRIPLES>(A, X, op);
 }
 
-template <typename MA, bool INIT>
+template <typename MA, bool INIT, bool TRIPLES = false>
 __global__ void __launch_bounds__(kT) multi_true_residual_quad_kernel(MA A, const double* __restrict__ X,
                                                                       const double* __restrict__ B,
                                                                       const float* __restrict__ dinv,
@@ -1016,7 +1097,7 @@ __global__ void __launch_bounds__(kT) multi_true_residual_quad_kernel(MA A, cons
                                                                       unsigned* counter) {
     if (!INIT && !*reinterpret_cast<volatile unsigned*>(&g->anyPending)) return;
     TrueResidualQuad op{B, dinv, R32, S, INIT, {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}}};
-    quad_rows(A, X, op);
+    quad_pass<TRIPLES>(A, X, op);
     double tot[2];
     if (quad_reduce_last<2>(op.acc, partials, counter, tot)) {
         if (threadIdx.x < 32) column_replace<INIT>(S[threadIdx.x], tot, g);
@@ -1107,6 +1188,9 @@ struct ciecu_multi_s {
     // k = 32: the four-columns-per-lane SpMM kernels (grids per format and precision)
     bool quad = false;
     int gridQ = 1, gridQD = 1, gridQ32 = 1, gridQ32D = 1;
+    bool triples = false;  // the DIA offsets come in consecutive triples: the reuse pass (quad_rows_dia3)
+    int formatPin = -1;    // -1: SpMM format by timing, 0: CSR, 1: the DIA copy (ciecu_multi_set_format)
+    int gridQD3 = 1, gridQ32D3 = 1;
 };
 
 namespace ciecu {
@@ -1125,7 +1209,10 @@ template <bool COND>
 int launch_multi_iteration(ciecu_multi_s* M, cudaStream_t st, cudaGraphConditionalHandle cond) {
     CIECU_TRY(with_group(M->kp, [&](auto kk) -> int {
         constexpr int KP = decltype(kk)::value;
-        if (M->quad && M->useDia)
+        if (M->quad && M->useDia && M->triples)
+            multi_spmv_quad_kernel<DiaArgs<double>, double, COND, true><<<M->gridQD3, kT, 0, st>>>(
+                M->dia, M->p, M->q, M->d_s, M->d_g, M->d_partials, M->d_counter, cond);
+        else if (M->quad && M->useDia)
             multi_spmv_quad_kernel<DiaArgs<double>, double, COND><<<M->gridQD, kT, 0, st>>>(
                 M->dia, M->p, M->q, M->d_s, M->d_g, M->d_partials, M->d_counter, cond);
         else if (M->quad)
@@ -1159,7 +1246,9 @@ int launch_multi_iteration(ciecu_multi_s* M, cudaStream_t st, cudaGraphCondition
 int launch_multi_residual(ciecu_multi_s* M, cudaStream_t st, bool dia, const double* B) {
     return with_group(M->kp, [&](auto kk) -> int {
         constexpr int KP = decltype(kk)::value;
-        if (M->quad && dia)
+        if (M->quad && dia && M->triples)
+            multi_residual_quad_kernel<DiaArgs<double>, true><<<M->gridQD3, kT, 0, st>>>(M->dia, M->x, B, M->r);
+        else if (M->quad && dia)
             multi_residual_quad_kernel<DiaArgs<double>><<<M->gridQD, kT, 0, st>>>(M->dia, M->x, B, M->r);
         else if (M->quad)
             multi_residual_quad_kernel<CsrArgs<double>><<<M->gridQ, kT, 0, st>>>(M->A->args<double>(), M->x, B, M->r);
@@ -1184,7 +1273,7 @@ int prepare_dia(ciecu_multi_s* M, cudaStream_t st, const double* B) {
         M->diaChecked = true;
         const std::vector<int>* offsets = nullptr;
         CIECU_TRY(dia_offsets(M->A, &offsets));
-        if (offsets->empty()) return CIECU_OK;
+        if (offsets->empty() || M->formatPin == 0) return CIECU_OK;
         DiaArgs<double> a = dia_shape<double>(M->A, *offsets);
         const size_t bytes = sizeof(double) * static_cast<size_t>(a.ndiag) * static_cast<size_t>(a.ld);
         if (cudaMalloc(&M->diaBuf, bytes) != cudaSuccess) {
@@ -1195,6 +1284,7 @@ int prepare_dia(ciecu_multi_s* M, cudaStream_t st, const double* B) {
         CIECU_CUDA(cudaMemsetAsync(M->diaBuf, 0, bytes, st));
         a.val = M->diaBuf;
         M->dia = a;
+        M->triples = dia_triples(a);
         const long needed = (M->n + static_cast<long>(kWarps) * (32 / M->kp) - 1) /
                             (static_cast<long>(kWarps) * (32 / M->kp));
         with_group(M->kp, [&](auto kk) -> int {
@@ -1228,10 +1318,11 @@ int prepare_dia(ciecu_multi_s* M, cudaStream_t st, const double* B) {
         cudaEventDestroy(e1);
         if (e == cudaSuccess) e = cudaGetLastError();
         if (e != cudaSuccess) return cuda_fail(e, "multi: SpMM format choice");
-        M->useDia = best[1] < best[0];
+        M->useDia = M->formatPin == 1 ? true : (M->formatPin == 0 ? false : best[1] < best[0]);
         return CIECU_OK;
     }
     if (M->diaBuf) CIECU_TRY(dia_fill_f64(M->A, M->dia, M->diaBuf, st));
+    if (M->formatPin >= 0) M->useDia = M->diaBuf && M->formatPin == 1;
     return CIECU_OK;
 }
 
@@ -1271,7 +1362,10 @@ template <bool INIT>
 int launch_true_residual(ciecu_multi_s* M, cudaStream_t st, const double* B) {
     return with_group(M->kp, [&](auto kk) -> int {
         constexpr int KP = decltype(kk)::value;
-        if (M->quad && M->useDia)
+        if (M->quad && M->useDia && M->triples)
+            multi_true_residual_quad_kernel<DiaArgs<double>, INIT, true><<<M->gridQD3, kT, 0, st>>>(
+                M->dia, M->x, B, M->dinv32, M->r32, M->d_s, M->d_g, M->d_partials, M->d_counter);
+        else if (M->quad && M->useDia)
             multi_true_residual_quad_kernel<DiaArgs<double>, INIT><<<M->gridQD, kT, 0, st>>>(
                 M->dia, M->x, B, M->dinv32, M->r32, M->d_s, M->d_g, M->d_partials, M->d_counter);
         else if (M->quad)
@@ -1305,7 +1399,10 @@ int launch_multi_iteration32(ciecu_multi_s* M, cudaStream_t st, cudaGraph_t root
     if (COND) CIECU_CUDA(cudaGraphConditionalHandleCreate(&replace, root, 0, cudaGraphCondAssignDefault));
     CIECU_TRY(with_group(M->kp, [&](auto kk) -> int {
         constexpr int KP = decltype(kk)::value;
-        if (M->quad && M->useDia)
+        if (M->quad && M->useDia && M->triples)
+            multi_spmv_quad_kernel<DiaArgs<float>, float, COND, true><<<M->gridQ32D3, kT, 0, st>>>(
+                M->diaF, M->p32, M->q32, M->d_s, M->d_g, M->d_partials, M->d_counter, cond);
+        else if (M->quad && M->useDia)
             multi_spmv_quad_kernel<DiaArgs<float>, float, COND><<<M->gridQ32D, kT, 0, st>>>(
                 M->diaF, M->p32, M->q32, M->d_s, M->d_g, M->d_partials, M->d_counter, cond);
         else if (M->quad)
@@ -1541,9 +1638,15 @@ int ciecu_multi_create(ciecu_csr lhs, int rhsCount, const double* d_inverseDiago
         M->gridQD = fit(reinterpret_cast<const void*>(multi_spmv_quad_kernel<DiaArgs<double>, double, true>), rowsQ);
         M->gridQ32 = fit(reinterpret_cast<const void*>(multi_spmv_quad_kernel<CsrArgs<float>, float, true>), blocks);
         M->gridQ32D = fit(reinterpret_cast<const void*>(multi_spmv_quad_kernel<DiaArgs<float>, float, true>), rowsQ);
+        const long rows3 = (M->n + kWarps * 16 - 1) / (kWarps * 16);
+        M->gridQD3 = fit(reinterpret_cast<const void*>(multi_spmv_quad_kernel<DiaArgs<double>, double, true, true>),
+                         rows3);
+        M->gridQ32D3 = fit(reinterpret_cast<const void*>(multi_spmv_quad_kernel<DiaArgs<float>, float, true, true>),
+                           rows3);
         M->quad = quad_enabled();
     }
-    int widest = std::max({M->grid, M->gridV, M->gridQ, M->gridQD, M->gridQ32, M->gridQ32D});
+    int widest = std::max({M->grid, M->gridV, M->gridQ, M->gridQD, M->gridQ32, M->gridQ32D, M->gridQD3,
+                           M->gridQ32D3});
     with_group(M->kp, [&](auto kk) -> int {
         constexpr int KP = decltype(kk)::value;
         for (const void* k : {reinterpret_cast<const void*>(multi_spmv_dia_kernel<KP, true, true>),
@@ -1605,6 +1708,24 @@ int ciecu_multi_refinements(ciecu_multi M, int64_t* h_perColumn) {
     CIECU_REQUIRE(M && h_perColumn, "multi_refinements: null argument");
     for (int c = 0; c < M->k; ++c)
         h_perColumn[c] = c < static_cast<int>(M->last.size()) ? M->last[c].refinements : 0;
+    return CIECU_OK;
+}
+
+int ciecu_multi_set_format(ciecu_multi M, int format) {
+    CIECU_REQUIRE(M, "multi_set_format: null solver");
+    CIECU_REQUIRE(format >= -1 && format <= 1, "multi_set_format: format must be -1 (timed), 0 (CSR) or 1 (DIA)");
+    M->formatPin = format;
+    if (format == 1 && !M->diaBuf) M->diaChecked = false;  // build the copy at the next solve
+    if (format >= 0) {
+        if (M->graph) {
+            cudaGraphExecDestroy(M->graph);
+            M->graph = nullptr;
+        }
+        if (M->graph32) {
+            cudaGraphExecDestroy(M->graph32);
+            M->graph32 = nullptr;
+        }
+    }
     return CIECU_OK;
 }
 

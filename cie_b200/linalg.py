@@ -770,6 +770,11 @@ class MultiRHSConjugateGradients(LinearOperator):
         call("ciecu_multi_set_refinement", self._solver, float(delta))
         self.refinement = float(delta)
 
+    def set_format(self, fmt):
+        """Pins the SpMM format: 1 the DIA copy (when the matrix has one), 0 CSR,
+        -1 timed at the first solve (default)."""
+        call("ciecu_multi_set_format", self._solver, int(fmt))
+
     def refinements(self):
         """FP64 residual recomputations per column in the last refined solve."""
         out = (ctypes.c_int64 * self.k)()

@@ -32,6 +32,13 @@ int ciecu_multi_info(ciecu_multi solver, int* lanesPerRow, int* deviceLoop);
  * ciecu_csr_diagonals, whose copy timed faster than the CSR SpMM; the copy is
  * refilled from the CSR values at every solve), or 0 for the CSR SpMM. */
 int ciecu_multi_format(ciecu_multi solver, int* diagonals);
+/* Pins the SpMM format instead of timing it at the first solve: 1 the DIA copy
+ * (when the matrix has one; CSR otherwise), 0 CSR, -1 timed (default).  For
+ * tests and profiling.  With 32 right-hand sides and a stencil whose offsets come
+ * in consecutive triples (the Q1 stencils), the DIA SpMM keeps four rows per lane
+ * and loads each operand row of a triple once; ciecu_multi_format reports the
+ * diagonal count either way. */
+int ciecu_multi_set_format(ciecu_multi solver, int format);
 /* delta in (0, 1): FP32-refined form -- every column iterates in FP32 (FP32
  * copies of the matrix in the format of the FP64 solve and of D^-1, FP32 blocks,
  * FP64 dot products) with FP64 reliable updates: every running column's FP32

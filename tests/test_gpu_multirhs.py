@@ -15,12 +15,14 @@ def space():
     return CUDASpace()
 
 
-@pytest.mark.parametrize("k,dim,order,cells,offset", [(32, 3, 1, [14, 14, 14], 0), (32, 3, 2, [6, 6, 6], 0),
-                                                      (32, 3, 1, [10, 10, 10], 1), (5, 2, 1, [40, 40], 0),
-                                                      (1, 2, 1, [30, 30], 0)])
-def test_multirhs_pcg_vs_reference_per_column(space, reference, k, dim, order, cells, offset):
-    """k = 32 runs the four-columns-per-lane SpMM (Q1: DIA or CSR as timed, Q2:
-    CSR); right-hand sides at an 8-byte offset (not 16-byte aligned) take the
+@pytest.mark.parametrize("k,dim,order,cells,offset,fmt", [(32, 3, 1, [14, 14, 14], 0, 1), (32, 3, 1, [14, 14, 14], 0, 0),
+                                                          (32, 2, 1, [40, 40], 0, 1), (32, 3, 2, [6, 6, 6], 0, -1),
+                                                          (32, 3, 1, [10, 10, 10], 1, 1), (5, 2, 1, [40, 40], 0, -1),
+                                                          (1, 2, 1, [30, 30], 0, -1)])
+def test_multirhs_pcg_vs_reference_per_column(space, reference, k, dim, order, cells, offset, fmt):
+    """k = 32 runs the four-columns-per-lane SpMM: Q1 over the DIA copy (fmt 1:
+    the triple pass, four rows per lane) or CSR (fmt 0), Q2 over CSR (no DIA
+    copy); right-hand sides at an 8-byte offset (not 16-byte aligned) take the
     row-per-warp kernels.  Same iteration counts as the reference either way."""
     from cie_b200.fem import make_poisson
     from cie_b200.linalg import CSROperator, MultiRHSConjugateGradients, Statistics, makeDiagonalOperator
@@ -33,6 +35,7 @@ def test_multirhs_pcg_vs_reference_per_column(space, reference, k, dim, order, c
     A = CSROperator(prob.matrix, space)
     D = makeDiagonalOperator(prob.matrix, space, csr_handle=A.csr)
     solver = MultiRHSConjugateGradients(A, D, k, Statistics(5000, 0.0, 1e-10))
+    solver.set_format(fmt)
     X = torch.zeros(n, k, dtype=torch.float64, device="cuda")
     buf = torch.zeros(n * k + offset, dtype=torch.float64, device="cuda")
     Bd = buf[offset:].view(n, k)
@@ -42,6 +45,10 @@ def test_multirhs_pcg_vs_reference_per_column(space, reference, k, dim, order, c
     Xh = X.cpu().numpy()
     rp, col, val = prob.host_csr()
     print(solver.info(), [s.iterationCount for s in stats[:4]])
+    if fmt == 1:
+        assert solver.info()["spmm_format"] == "dia-%d" % 3 ** dim
+    elif fmt == 0:
+        assert solver.info()["spmm_format"] == "csr"
     for c in range(k):
         xr, sr, err, _ = reference.pcg(rp, col, val, B[:, c].copy(), maxit=5000, abstol=0.0, reltol=1e-10)
         assert err is None
@@ -74,8 +81,9 @@ def test_multirhs_pcg_scales_guesses_limits(space):
             assert float(torch.linalg.norm(got - o) / torch.linalg.norm(o)) <= 1e-9
 
 
-@pytest.mark.parametrize("k,dim,order,cells", [(32, 3, 1, [14, 14, 14]), (5, 3, 2, [6, 6, 6]), (1, 2, 1, [30, 30])])
-def test_multirhs_fp32_refined_vs_reference_per_column(space, reference, k, dim, order, cells):
+@pytest.mark.parametrize("k,dim,order,cells,fmt", [(32, 3, 1, [14, 14, 14], 1), (32, 3, 1, [14, 14, 14], 0),
+                                                   (5, 3, 2, [6, 6, 6], -1), (1, 2, 1, [30, 30], -1)])
+def test_multirhs_fp32_refined_vs_reference_per_column(space, reference, k, dim, order, cells, fmt):
     """The FP32-refined form (FP32 SpMM iterations per column, FP64 reliable
     updates): every column's solution within 1e-9 of the reference's FP64 CG and
     its true FP64 residual at the 1e-10 stop; Q2 (125 diagonals) runs the FP32 CSR
@@ -93,6 +101,7 @@ def test_multirhs_fp32_refined_vs_reference_per_column(space, reference, k, dim,
     D = makeDiagonalOperator(prob.matrix, space, csr_handle=A.csr)
     solver = MultiRHSConjugateGradients(A, D, k, Statistics(5000, 0.0, 1e-10))
     solver.set_refinement(0.1)
+    solver.set_format(fmt)
     X = torch.zeros(n, k, dtype=torch.float64, device="cuda")
     solver.product(0.0, torch.as_tensor(B).cuda().contiguous(), 1.0, X)
     stats = solver.getStats()
