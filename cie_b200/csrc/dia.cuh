@@ -107,6 +107,69 @@ __device__ __forceinline__ void dia_rows4(const DiaArgs<float>& A, const float* 
     dia_rows4_gather<ND>(A, LoadGather<float>{x}, op);
 }
 
+// dia_rows4 for stencils whose sorted offsets come in consecutive triples
+// (o - 1, o, o + 1), the Q1 stencils: for each triple the thread loads the six
+// operand entries x[r + o - 1 .. r + o + 4] of its four rows once, where
+// dia_rows4 loads twelve.  Triples ascending and the three diagonals of a triple
+// in order keep every row sum in the column order of dia_rows4, bit for bit.
+template <int ND, typename Op>
+__device__ __forceinline__ void dia_rows4_triples(const DiaArgs<float>& A, const float* __restrict__ x, Op& op) {
+    constexpr int NT = ND / 3;
+    const int nt = NT > 0 ? NT : A.ndiag / 3;
+    const long stride = static_cast<long>(gridDim.x) * blockDim.x * 4;
+    for (long r0 = (static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x) * 4; r0 < A.nrows; r0 += stride) {
+        const int r = static_cast<int>(r0);
+        typename Op::Pre pre[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            if (r + i < A.nrows) pre[i] = op.pre(r + i);
+        float sum[4] = {0.f, 0.f, 0.f, 0.f};
+        auto triple = [&](int t) {
+            const int c = r + A.off[3 * t + 1] - 1;
+            float xv[6];
+#pragma unroll
+            for (int j = 0; j < 6; ++j)
+                xv[j] = static_cast<unsigned>(c + j) < static_cast<unsigned>(A.nrows) ? __ldg(x + c + j) : 0.f;
+#pragma unroll
+            for (int e = 0; e < 3; ++e) {
+                const float4 v = __ldcs(reinterpret_cast<const float4*>(A.val + static_cast<long>(3 * t + e) * A.ld + r));
+                sum[0] = fmaf(v.x, xv[e], sum[0]);
+                sum[1] = fmaf(v.y, xv[e + 1], sum[1]);
+                sum[2] = fmaf(v.z, xv[e + 2], sum[2]);
+                sum[3] = fmaf(v.w, xv[e + 3], sum[3]);
+            }
+        };
+        if constexpr (NT > 0) {
+#pragma unroll
+            for (int t = 0; t < NT; ++t) triple(t);
+        } else {
+            for (int t = 0; t < nt; ++t) triple(t);
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            if (r + i < A.nrows) op.post(r + i, pre[i], sum[i]);
+    }
+}
+
+// CIECU_DIA_TRIPLES=0 keeps the plain four-row pass for triple stencils (for
+// comparison).
+inline bool dia_triples_enabled() {
+    static const bool enabled = [] {
+        const char* v = std::getenv("CIECU_DIA_TRIPLES");
+        return !(v && v[0] == '0');
+    }();
+    return enabled;
+}
+
+// Whether the sorted offsets come in consecutive triples (o - 1, o, o + 1).
+template <typename V>
+bool dia_has_triples(const DiaArgs<V>& d) {
+    if (d.ndiag == 0 || d.ndiag % 3 != 0) return false;
+    for (int t = 0; t < d.ndiag / 3; ++t)
+        if (d.off[3 * t] + 1 != d.off[3 * t + 1] || d.off[3 * t + 1] + 1 != d.off[3 * t + 2]) return false;
+    return true;
+}
+
 // Calls f(std::integral_constant<int, ND>) with ND = 27, 9 or 0 (runtime count).
 template <typename F>
 int with_diagonals(int ndiag, F&& f) {

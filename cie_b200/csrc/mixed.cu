@@ -246,14 +246,23 @@ __global__ void __launch_bounds__(kT) mixed_spmv_kernel(SellArgs<float, CI> A, c
 // even when it is symmetric: reading the lower half back from the upper one (as
 // the FP64 PCG does) measured slower here, where every row pass is already a
 // four-row, 16-byte-load stream.
-template <int ND>
+// TRIPLES: the offsets come in consecutive triples (dia_rows4_triples).
+template <int ND, bool TRIPLES, typename Op>
+__device__ __forceinline__ void mixed_dia_rows(const DiaArgs<float>& A, const float* __restrict__ x, Op& op) {
+    if constexpr (TRIPLES)
+        dia_rows4_triples<ND>(A, x, op);
+    else
+        dia_rows4<ND>(A, x, op);
+}
+
+template <int ND, bool TRIPLES>
 __global__ void __launch_bounds__(kT) mixed_apply_dia_kernel(DiaArgs<float> A, const float* __restrict__ x,
                                                             float* __restrict__ y) {
     StoreOp op{y};
-    dia_rows4<ND>(A, x, op);
+    mixed_dia_rows<ND, TRIPLES>(A, x, op);
 }
 
-template <int ND, bool COND, bool FUSED>
+template <int ND, bool COND, bool FUSED, bool TRIPLES>
 __global__ void __launch_bounds__(kT) mixed_spmv_dia_kernel(DiaArgs<float> A, const float* __restrict__ x,
                                                            float* __restrict__ p, float* __restrict__ q,
                                                            MixedScalars* s, double* partials, unsigned* counter,
@@ -263,7 +272,7 @@ __global__ void __launch_bounds__(kT) mixed_spmv_dia_kernel(DiaArgs<float> A, co
         return;
     }
     auto op = M1Op<FUSED>::make(x, p, q, s);
-    dia_rows4<ND>(A, x, op);
+    mixed_dia_rows<ND, TRIPLES>(A, x, op);
     double mine[1] = {op.acc}, tot[1];
     if (grid_reduce_last<1, kT>(mine, partials, counter, tot) && threadIdx.x == 0) {
         s->pq = tot[0];
@@ -586,6 +595,7 @@ struct ciecu_mixed_s {
                      // kDiaInner = the DIA copy)
     bool sellBuilt = false;  // the SELL copy exists (not built when the DIA copy is the known choice)
     float* dia32 = nullptr;  // DIA copy of the inner matrix (few-diagonal matrices only)
+    bool diaTriples = false;  // its offsets come in consecutive triples (dia_rows4_triples)
     ciecu::DiaArgs<float> dia{};
     // SELL-32 inner matrix
     int nslices = 0;
@@ -637,7 +647,8 @@ int launch_inner_spmv_form(ciecu_mixed_s* M, cudaStream_t st, cudaGraphCondition
     if (M->unroll == kDiaInner) {
         CIECU_TRY(with_diagonals(M->dia.ndiag, [&](auto nd) -> int {
             constexpr int ND = decltype(nd)::value;
-            auto* kernel = mixed_spmv_dia_kernel<ND, COND, FUSED>;
+            auto* kernel = M->diaTriples ? mixed_spmv_dia_kernel<ND, COND, FUSED, true>
+                                         : mixed_spmv_dia_kernel<ND, COND, FUSED, false>;
             kernel<<<fit_grid(kernel, kT, (needA + 3) / 4), kT, 0, st>>>(M->dia, x, M->p32, M->q32, M->d_s,
                                                                          M->d_partials, M->d_counter, loop);
             return CIECU_OK;
@@ -921,6 +932,7 @@ int ciecu_mixed_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_sta
                 a.val = M->dia32;
                 M->dia = a;
                 if (e == cudaSuccess) status = dia_fill_f32(lhs, M->dia, M->dia32, M->sdiag, st);
+                M->diaTriples = dia_has_triples(M->dia) && dia_triples_enabled();
                 if (e != cudaSuccess) status = cuda_fail(e, "mixed_create: DIA copy");
             } else {
                 cudaGetLastError();  // no room for the copy: the SELL kernels stay
@@ -1080,7 +1092,7 @@ int ciecu_mixed_apply_f32(ciecu_mixed M, const float* d_in, float* d_out) {
     if (M->unroll == kDiaInner) {
         CIECU_TRY(with_diagonals(M->dia.ndiag, [&](auto nd) -> int {
             constexpr int ND = decltype(nd)::value;
-            auto* kernel = mixed_apply_dia_kernel<ND>;
+            auto* kernel = M->diaTriples ? mixed_apply_dia_kernel<ND, true> : mixed_apply_dia_kernel<ND, false>;
             kernel<<<fit_grid(kernel, kT, (need + 3) / 4), kT, 0, st>>>(M->dia, d_in, d_out);
             return CIECU_OK;
         }));

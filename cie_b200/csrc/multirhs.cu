@@ -946,14 +946,6 @@ __device__ __forceinline__ void quad_rows_dia3(const DiaArgs<V>& D, const T* __r
     }
 }
 
-// Whether the sorted offsets come in consecutive triples (o - 1, o, o + 1).
-inline bool dia_triples(const DiaArgs<double>& d) {
-    if (d.ndiag == 0 || d.ndiag % 3 != 0) return false;
-    for (int t = 0; t < d.ndiag / 3; ++t)
-        if (d.off[3 * t] + 1 != d.off[3 * t + 1] || d.off[3 * t + 1] + 1 != d.off[3 * t + 2]) return false;
-    return true;
-}
-
 // The DIA pass of the k = 32 kernels: triples when the stencil has them.
 template <bool TRIPLES, typename V, typename T, typename Op>
 __device__ __forceinline__ void quad_rows_dia(const DiaArgs<V>& D, const T* __restrict__ X, Op& op) {
@@ -1284,7 +1276,7 @@ int prepare_dia(ciecu_multi_s* M, cudaStream_t st, const double* B) {
         CIECU_CUDA(cudaMemsetAsync(M->diaBuf, 0, bytes, st));
         a.val = M->diaBuf;
         M->dia = a;
-        M->triples = dia_triples(a);
+        M->triples = dia_has_triples(a);
         const long needed = (M->n + static_cast<long>(kWarps) * (32 / M->kp) - 1) /
                             (static_cast<long>(kWarps) * (32 / M->kp));
         with_group(M->kp, [&](auto kk) -> int {
