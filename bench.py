@@ -438,7 +438,8 @@ def main():
     if os.path.exists(tpath) and cells == [128, 128, 128]:
         figures = dict(line.split() for line in open(tpath) if line.strip() and not line.startswith("#"))
         if dia32:
-            traffic = int(figures.get("mixed_apply_dia_kernel_f32", 0)) or None
+            key = "mixed_apply_dia_kernel_f32" + ("_triples" if info.get("dia_triples") else "")
+            traffic = int(figures.get(key, 0)) or None
         elif info["compressed_columns"] and info["group_unroll"] > 0:
             traffic = int(figures.get("mixed_apply_kernel_f32_sell16", 0)) or None
         traffic64 = int(figures.get("spmv_kernel_f64_csr", 0)) or None
@@ -527,7 +528,8 @@ def main():
                                        "mixed_frac": mixed_solve_bytes / t_mixed / 1e9 / hbm},
             "parity": parity,
             "roofline": {"bound": "hbm", "kernel": (
-                             "mixed_apply_dia_kernel (FP32 DIA SpMV, %d diagonals)" % ndiag) if dia32 else (
+                             "mixed_apply_dia_kernel (FP32 DIA SpMV, %d diagonals%s)" % (
+                                 ndiag, ", triple pass" if info.get("dia_triples") else "")) if dia32 else (
                              "%s (FP32 SELL-32 SpMV)" % ("mixed_apply_kernel<%d>" % info["group_unroll"]
                                                          if info["group_unroll"] > 0 else "mixed_apply_tma_kernel")),
                          "achieved": g32, "peak": hbm, "unit": "GB/s", "frac": g32 / hbm, "peak_kind": peak_kind,

@@ -1137,6 +1137,13 @@ int ciecu_mixed_padded_entries(ciecu_mixed M, int64_t* h_entries) {
     return CIECU_OK;
 }
 
+int ciecu_mixed_dia_info(ciecu_mixed M, int* diagonals, int* triples) {
+    CIECU_REQUIRE(M && diagonals && triples, "mixed_dia_info: null argument");
+    *diagonals = M->dia32 ? M->dia.ndiag : 0;
+    *triples = M->dia32 && M->diaTriples ? 1 : 0;
+    return CIECU_OK;
+}
+
 int ciecu_mixed_set_graph_chunk(ciecu_mixed M, int iterations) {
     CIECU_REQUIRE(M && iterations >= 1 && iterations <= 4096, "mixed_set_graph_chunk: chunk must be in [1, 4096]");
     if (M->chunk != iterations && M->graph) {

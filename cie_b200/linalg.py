@@ -609,8 +609,11 @@ class MixedPrecisionCG(LinearOperator):
         call("ciecu_mixed_padded_entries", self._solver, ctypes.byref(e))
         if v.value == -2:
             # the SELL copy (compressed_columns, padded_entries) is kept beside the DIA one
+            nd, tr = ctypes.c_int(), ctypes.c_int()
+            call("ciecu_mixed_dia_info", self._solver, ctypes.byref(nd), ctypes.byref(tr))
             return {"format": "dia", "inner_kernel": "dia", "group_unroll": v.value,
-                    "compressed_columns": bool(c.value), "padded_entries": e.value}
+                    "compressed_columns": bool(c.value), "padded_entries": e.value,
+                    "dia_diagonals": nd.value, "dia_triples": bool(tr.value)}
         return {"compressed_columns": bool(c.value), "format": "sell-32x4", "padded_entries": e.value,
                 "group_unroll": v.value, "inner_kernel": "tma-pipeline" if v.value == 0 else "registers"}
 

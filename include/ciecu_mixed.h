@@ -80,6 +80,10 @@ int ciecu_mixed_set_graph_chunk(ciecu_mixed solver, int iterations);
 int ciecu_mixed_apply_f32(ciecu_mixed solver, const float* d_in, float* d_out);
 /* Stored entries of the SELL-32 inner matrix, padding included (>= nnz). */
 int ciecu_mixed_padded_entries(ciecu_mixed solver, int64_t* h_entries);
+/* The FP32 diagonal-storage copy: its diagonals (0: none) and whether its row pass
+ * loads each operand entry of a consecutive offset triple (o - 1, o, o + 1) once
+ * (the Q1 stencils; CIECU_DIA_TRIPLES=0 in the environment turns it off). */
+int ciecu_mixed_dia_info(ciecu_mixed solver, int* diagonals, int* triples);
 /* out = inScale*out + outScale*x, x the refined solution (initial guess = out). */
 int ciecu_mixed_product(ciecu_mixed solver, double inScale, const double* d_in, double outScale, double* d_out,
                         ciecu_mixed_statistics* h_stats);
