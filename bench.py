@@ -839,13 +839,23 @@ def extra_workloads(space, A, D, settings, t_fp64, it64, rank=0, world=1):
             solver.product(0.0, pe.rhs, 1.0, xm)
         tmg = timed(solve_mg, 1, warm=1)
         st = solver.getStats()
+        info = solver.info()
         r = pe.rhs.clone()
         Ae.product(1.0, xm, -1.0, r)
-        emb["two_level_%s_smoothing" % precision] = {
+        entry = {
             "seconds": tmg, "iterations": st.iterationCount, "chebyshev_degree": degree, "coarse_iterations": coarse,
+            "coarse_cluster_ctas": info["coarse_cluster_ctas"] if info["coarse_cluster_active"] else 0,
             "true_relative_residual": float(torch.linalg.norm(r) / torch.linalg.norm(pe.rhs)),
             "rel_diff_vs_jacobi": float(torch.linalg.norm(xm - xe) / torch.linalg.norm(xe)),
             "speedup_vs_jacobi": tj / tmg}
+        if info["coarse_cluster_active"] and precision == TWO_LEVEL[-1][0]:
+            # the same solver with the pipelined coarse kernels (one launch per coarse iteration)
+            solver.set_coarse_cluster(False)
+            tp = timed(solve_mg, 1, warm=0)
+            entry["pipelined_coarse_seconds"] = tp
+            entry["pipelined_coarse_iterations"] = solver.getStats().iterationCount
+            solver.set_coarse_cluster(True)
+        emb["two_level_%s_smoothing" % precision] = entry
         del solver, xm
     out["embedded_sphere_q3_32^3"] = emb
     del Ae, pe, xe

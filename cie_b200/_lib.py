@@ -147,6 +147,9 @@ SIGNATURES = {
     "ciecu_mgcg_product": (c_int, [P, c_double, P, c_double, P, P]),
     "ciecu_mgcg_info": (c_int, [P, P, P]),
     "ciecu_mgcg_smoother_info": (c_int, [P, P, P]),
+    "ciecu_mgcg_coarse_info": (c_int, [P, P, P]),
+    "ciecu_mgcg_set_coarse_cluster": (c_int, [P, c_int]),
+    "ciecu_mgcg_coarse_apply": (c_int, [P, P, P]),
 }
 
 OPTIONAL = set()

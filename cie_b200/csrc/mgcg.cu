@@ -14,13 +14,17 @@
 // graph; M1 / M2 end the loop.  Every reduction is deterministic (per-block
 // partials summed in block order by the last block).
 #include "ciecu_mg.h"
+#include "dia.cuh"
 #include "graph.cuh"
 #include "pcg.cuh"
+
+#include <cooperative_groups.h>
 
 #include <cmath>
 #include <string>
 #include <type_traits>
 #include <utility>
+#include <vector>
 
 namespace ciecu {
 namespace {
@@ -408,6 +412,214 @@ __global__ void __launch_bounds__(csr_threads<K>())
     }
 }
 
+// ---- coarse solve in one thread-block cluster ---------------------------------
+//
+// For a coarse matrix of a structured Q1 stencil (27 diagonals in 3D, 9 in 2D,
+// lexicographic order) that is bitwise symmetric, the whole coarse solve runs in
+// ONE launch of a cluster of up to 16 CTAs: CTA k owns rows [kC, (k+1)C) and keeps
+// in its shared memory
+//   - the FP32 upper half U of the matrix (diagonal d holds A[r][r + off[d]]) for
+//     rows [kC - H, (k+1)C), H the largest offset, so that the lower entries of
+//     its own rows, A[r][r - o] = U_o[r - o], are local too;
+//   - the operand u (FP64) for rows [kC - H, (k+1)C + H): its own rows and the
+//     halo that the neighbouring CTAs push into it through distributed shared memory.
+// The vectors x, r, p, s and D^-1 of the own rows stay in registers (R consecutive
+// rows per thread).  The iteration is the Jacobi-PCG in the form of Chronopoulos
+// and Gear ("s-step iterative methods for symmetric linear systems", J. Comput.
+// Appl. Math. 25 (1989)): with w = A u, both dot products (r, u) and (w, u) of an
+// iteration come from the same vectors and are reduced together, and
+//   beta = gamma / gamma_old, alpha = gamma / (delta - beta gamma / alpha_old),
+//   p = u + beta p, s = w + beta s, x += alpha p, r -= alpha s, u = D^-1 r;
+// so an iteration costs one row pass over shared memory and two cluster barriers
+// (the reduction, the publication of u).  Its iterates are those of the pipelined
+// kernels above in exact arithmetic; the matrix is read in FP32 (the solve is a
+// preconditioner), everything else is FP64.  Every CTA forms the cluster-wide
+// sums from the per-CTA sums in rank order with the same butterfly, so all
+// threads hold bitwise equal scalars and take the same branches: the barrier
+// sequence is uniform, and a non-positive gamma or denominator ends the loop in
+// every CTA at the same iteration.
+
+constexpr int kClusterThreads = 768;
+constexpr int kClusterMaxTriples = 9;
+constexpr int kClusterMaxCtas = 16;
+
+struct ClusterCoarse {
+    const float* __restrict__ upper;  // diagonal d of U at upper + d * ld
+    long ld;
+    const double* __restrict__ b;
+    const double* __restrict__ dinv;
+    double* __restrict__ x;
+    int m, rowsPerCta, halo, iterations;
+    int center[kClusterMaxTriples];  // triple centres, ascending, centre[NT / 2] = 0
+};
+
+// U diagonals of a stencil with NT triples: the main one, offset 1, then the
+// upper triples (c - 1, c, c + 1).
+template <int NT>
+constexpr int cluster_upper_diagonals() {
+    return 2 + 3 * (NT / 2);
+}
+
+__host__ __device__ constexpr long cluster_align16(long bytes) { return (bytes + 15) / 16 * 16; }
+
+// Shared-memory bytes of a CTA: U rows, operand rows, 32 warp sums x 2 and 2 CTA sums.
+__host__ __device__ constexpr long cluster_smem_bytes(int nu, int rowsPerCta, int halo) {
+    return cluster_align16(4L * nu * (rowsPerCta + halo)) + 8L * (rowsPerCta + 2L * halo) + 8L * 66;
+}
+
+__device__ __forceinline__ double warp_sum_all(double v) {
+#pragma unroll
+    for (int k = 16; k >= 1; k >>= 1) v += __shfl_xor_sync(0xffffffffu, v, k);
+    return v;  // the same bits in every lane: each step adds the same pair in both lanes
+}
+
+// Cluster-wide sums of two values, bitwise equal in every thread of every CTA.
+__device__ __forceinline__ void cluster_sum2(cooperative_groups::cluster_group& cluster, double v0, double v1,
+                                             double* warpSums, double* ctaSums, int nctas, double& t0, double& t1) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    v0 = warp_sum_all(v0);
+    v1 = warp_sum_all(v1);
+    if (lane == 0) {
+        warpSums[warp] = v0;
+        warpSums[32 + warp] = v1;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        constexpr int kWarps = kClusterThreads / 32;
+        const double a = warp_sum_all(lane < kWarps ? warpSums[lane] : 0.0);
+        const double b = warp_sum_all(lane < kWarps ? warpSums[32 + lane] : 0.0);
+        if (lane == 0) {
+            ctaSums[0] = a;
+            ctaSums[1] = b;
+        }
+    }
+    cluster.sync();
+    const double a = lane < nctas ? *cluster.map_shared_rank(ctaSums, lane) : 0.0;
+    const double b = lane < nctas ? *cluster.map_shared_rank(ctaSums + 1, lane) : 0.0;
+    t0 = warp_sum_all(a);
+    t1 = warp_sum_all(b);
+}
+
+// u of the own rows into the CTA's operand, and into the halo of the neighbours
+// whose rows reach them (rows within H of either end of the block).
+template <int R>
+__device__ __forceinline__ void cluster_publish(cooperative_groups::cluster_group& cluster, double* pe,
+                                                const double (&u)[R], int li0, int C, int H, int rank, int nctas) {
+    double* prev = rank > 0 ? cluster.map_shared_rank(pe, rank - 1) : nullptr;
+    double* next = rank + 1 < nctas ? cluster.map_shared_rank(pe, rank + 1) : nullptr;
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+        const int li = li0 + j;
+        pe[H + li] = u[j];
+        if (prev && li < H) prev[C + H + li] = u[j];            // the previous CTA's right halo
+        if (next && li >= C - H) next[li - C + H] = u[j];       // the next CTA's left halo
+    }
+}
+
+// w = A u for the R consecutive own rows starting at operand index e0 (= H + li0;
+// U index of those rows is the same): per triple of diagonals the R + 2 operand
+// entries are loaded once.  Lower entries are read from U at row r + o.
+template <int NT, int R>
+__device__ __forceinline__ void cluster_rows(const float* U, int lu, const double* pe, int e0, const int* center,
+                                             double (&w)[R]) {
+#pragma unroll
+    for (int j = 0; j < R; ++j) w[j] = 0.0;
+#pragma unroll
+    for (int t = 0; t < NT; ++t) {
+        const int c = center[t];
+        double xv[R + 2];
+#pragma unroll
+        for (int k = 0; k < R + 2; ++k) xv[k] = pe[e0 + c - 1 + k];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {  // offset o = c - 1 + k
+#pragma unroll
+            for (int j = 0; j < R; ++j) {
+                float a;
+                if (t < NT / 2)  // o < 0: A[r][r + o] = U_{-o}[r + o], -o = c_mirror + 1 - k
+                    a = U[(2 + 3 * (NT / 2 - 1 - t) + (2 - k)) * lu + e0 + j + c - 1 + k];
+                else if (t == NT / 2)
+                    a = k == 0 ? U[lu + e0 + j - 1] : (k == 1 ? U[e0 + j] : U[lu + e0 + j]);
+                else
+                    a = U[(2 + 3 * (t - NT / 2 - 1) + k) * lu + e0 + j];
+                w[j] = fma(static_cast<double>(a), xv[j + k], w[j]);
+            }
+        }
+    }
+}
+
+template <int NT, int R>
+__global__ void __launch_bounds__(kClusterThreads, 1) coarse_cluster_kernel(ClusterCoarse a) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    constexpr int NU = cluster_upper_diagonals<NT>();
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int C = a.rowsPerCta, H = a.halo, lu = C + H, pl = C + 2 * H;
+    const int nctas = static_cast<int>(cluster.num_blocks());
+    const int rank = static_cast<int>(cluster.block_rank());
+    const long start = static_cast<long>(rank) * C;
+    float* U = reinterpret_cast<float*>(smem);
+    double* pe = reinterpret_cast<double*>(smem + cluster_align16(4L * NU * lu));
+    double* warpSums = pe + pl;
+    double* ctaSums = warpSums + 64;
+
+    for (int d = 0; d < NU; ++d)
+        for (int e = threadIdx.x; e < lu; e += kClusterThreads) {
+            const long r = start - H + e;
+            U[d * lu + e] = (r >= 0 && r < a.m) ? __ldg(a.upper + d * a.ld + r) : 0.0f;
+        }
+    for (int e = threadIdx.x; e < pl; e += kClusterThreads) pe[e] = 0.0;
+    cluster.sync();  // every CTA has zeroed its operand before any halo is pushed
+
+    const int li0 = R * static_cast<int>(threadIdx.x);
+    double xs[R], rs[R], ps[R], ss[R], ds[R], us[R];
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+        const long row = start + li0 + j;
+        const bool in = row < a.m;
+        rs[j] = in ? a.b[row] : 0.0;
+        ds[j] = in ? a.dinv[row] : 0.0;
+        us[j] = ds[j] * rs[j];
+        xs[j] = ps[j] = ss[j] = 0.0;
+    }
+    cluster_publish<R>(cluster, pe, us, li0, C, H, rank, nctas);
+    cluster.sync();
+    double gammaOld = 0.0, alphaOld = 0.0;
+    for (int it = 0; it < a.iterations; ++it) {
+        double w[R];
+        cluster_rows<NT, R>(U, lu, pe, H + li0, a.center, w);
+        double g = 0.0, dl = 0.0;
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+            g = fma(rs[j], us[j], g);
+            dl = fma(w[j], us[j], dl);
+        }
+        cluster_sum2(cluster, g, dl, warpSums, ctaSums, nctas, g, dl);
+        const double beta = it == 0 ? 0.0 : g / gammaOld;
+        const double den = it == 0 ? dl : dl - beta * g / alphaOld;
+        if (!(0.0 < g) || !(0.0 < den)) break;  // converged to rounding or broken down: no further steps
+        const double alpha = g / den;
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+            ps[j] = fma(beta, ps[j], us[j]);
+            ss[j] = fma(beta, ss[j], w[j]);
+            xs[j] = fma(alpha, ps[j], xs[j]);
+            rs[j] = fma(-alpha, ss[j], rs[j]);
+            us[j] = ds[j] * rs[j];
+        }
+        gammaOld = g;
+        alphaOld = alpha;
+        if (it + 1 == a.iterations) break;
+        cluster_publish<R>(cluster, pe, us, li0, C, H, rank, nctas);
+        cluster.sync();
+    }
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+        const long row = start + li0 + j;
+        if (row < a.m) a.x[row] = xs[j];
+    }
+    cluster.sync();  // no CTA leaves while another may still read its CTA sums
+}
+
 __global__ void count_cycle_kernel(MgScalars* s) { s->cycles += 1; }
 
 }  // namespace
@@ -433,6 +645,17 @@ struct ciecu_mgcg_s {
     unsigned* counter = nullptr;
     cudaGraphExec_t graph = nullptr;
     bool deviceLoop = false;
+    // cluster-resident coarse solve (coarse_cluster_kernel): the FP32 DIA copy of the
+    // coarse matrix, refilled at every solve, and the launch shape chosen at creation
+    float* coarse32 = nullptr;
+    ciecu::DiaArgs<float> coarseDia{};
+    ciecu::ClusterCoarse cluster{};
+    int clusterCtas = 0;  // 0: the coarse matrix's shape rules the cluster form out
+    int clusterTriples = 0, clusterRows = 0;
+    size_t clusterSmem = 0;
+    bool clusterAllowed = true;  // ciecu_mgcg_set_coarse_cluster
+    bool clusterActive = false;  // the matrix was bitwise symmetric at the last solve
+    bool graphCluster = false;   // the form captured in `graph`
 };
 
 namespace ciecu {
@@ -514,9 +737,145 @@ int chebyshev(ciecu_mgcg_s* M, ciecu_csr_s* A, const T* dinv, const T* in, T* ou
     return CIECU_OK;
 }
 
-// ec = C rc: coarseIterations Jacobi-PCG iterations from zero (pipelined: one
-// kernel per iteration), result in M->cx.
+using ClusterKernel = void (*)(ClusterCoarse);
+
+ClusterKernel cluster_kernel(int triples, int rows) {
+    if (triples == 9) return rows == 1 ? coarse_cluster_kernel<9, 1> : (rows == 3 ? coarse_cluster_kernel<9, 3>
+                                                                                 : coarse_cluster_kernel<9, 5>);
+    return rows == 1 ? coarse_cluster_kernel<3, 1> : (rows == 3 ? coarse_cluster_kernel<3, 3>
+                                                                : coarse_cluster_kernel<3, 5>);
+}
+
+cudaLaunchConfig_t cluster_config(const ciecu_mgcg_s* M, cudaStream_t st, cudaLaunchAttribute* attr) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(static_cast<unsigned>(M->clusterCtas));
+    cfg.blockDim = dim3(kClusterThreads);
+    cfg.dynamicSmemBytes = M->clusterSmem;
+    cfg.stream = st;
+    attr->id = cudaLaunchAttributeClusterDimension;
+    attr->val.clusterDim.x = static_cast<unsigned>(M->clusterCtas);
+    attr->val.clusterDim.y = 1;
+    attr->val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cfg;
+}
+
+// Whether the coarse matrix has the stencil of coarse_cluster_kernel (27 or 9
+// diagonals symmetric about 0: the main one, +-1 and triples (c - 1, c, c + 1))
+// and fits a cluster: R rows per thread (1, 3 or 5), at most 16 CTAs, a halo
+// no wider than a CTA's rows, the shared memory of one CTA.  Then the FP32 DIA
+// copy is allocated; otherwise the pipelined kernels stay (clusterCtas = 0).
+int prepare_cluster(ciecu_mgcg_s* M, cudaStream_t st) {
+    M->clusterCtas = 0;
+    if (M->m <= 0) return CIECU_OK;
+    const std::vector<int>* offsets = nullptr;
+    CIECU_TRY(dia_offsets(M->Ac, &offsets));
+    const std::vector<int>& off = *offsets;
+    const int nd = static_cast<int>(off.size());
+    if (nd != 27 && nd != 9) return CIECU_OK;
+    const int h = nd / 2, nt = nd / 3;
+    if (off[h] != 0) return CIECU_OK;
+    for (int k = 1; k <= h; ++k)
+        if (off[h + k] != -off[h - k]) return CIECU_OK;
+    const int* up = off.data() + h;  // the h + 1 upper offsets, ascending from 0
+    if (up[1] != 1) return CIECU_OK;
+    ClusterCoarse a{};
+    int last = 1;
+    for (int t = 1; t <= nt / 2; ++t) {
+        const int* tri = up + 2 + 3 * (t - 1);
+        const int c = tri[1];
+        if (tri[0] != c - 1 || tri[2] != c + 1 || c - 1 <= last) return CIECU_OK;
+        last = c + 1;
+        a.center[nt / 2 + t] = c;
+        a.center[nt / 2 - t] = -c;
+    }
+    a.center[nt / 2] = 0;
+    const int halo = up[h];
+    int dev = 0, maxSmem = 0;
+    CIECU_CUDA(cudaGetDevice(&dev));
+    CIECU_CUDA(cudaDeviceGetAttribute(&maxSmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    int rows = 0, ctas = 0;
+    long smem = 0;
+    for (int r : {1, 3, 5}) {
+        const long c = static_cast<long>(r) * kClusterThreads;
+        const long n = (M->m + c - 1) / c;
+        if (n > kClusterMaxCtas || (n > 1 && halo > c)) continue;
+        smem = cluster_smem_bytes(h + 1, static_cast<int>(c), halo);
+        if (smem > maxSmem) break;  // more rows per CTA only need more
+        rows = r;
+        ctas = static_cast<int>(n);
+        break;
+    }
+    if (!rows) return CIECU_OK;
+    const ClusterKernel kern = cluster_kernel(nt, rows);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e == cudaSuccess && ctas > 8) e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    int clusters = 0;
+    if (e == cudaSuccess) {
+        M->clusterCtas = ctas;
+        M->clusterSmem = static_cast<size_t>(smem);
+        cudaLaunchAttribute attr{};
+        const cudaLaunchConfig_t cfg = cluster_config(M, st, &attr);
+        e = cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg);
+        M->clusterCtas = 0;
+    }
+    if (e != cudaSuccess || clusters < 1) {
+        cudaGetLastError();  // no such cluster on this device: the pipelined kernels stay
+        return CIECU_OK;
+    }
+    DiaArgs<float> full = dia_shape<float>(M->Ac, off);
+    const size_t bytes = sizeof(float) * static_cast<size_t>(full.ndiag) * static_cast<size_t>(full.ld);
+    if (cudaMalloc(&M->coarse32, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        M->coarse32 = nullptr;
+        return CIECU_OK;
+    }
+    CIECU_CUDA(cudaMemsetAsync(M->coarse32, 0, bytes, st));
+    full.val = M->coarse32;
+    M->coarseDia = full;
+    a.upper = M->coarse32 + static_cast<long>(h) * full.ld;
+    a.ld = full.ld;
+    a.b = M->rc;
+    a.dinv = M->dinvc;
+    a.x = M->cx;
+    a.m = static_cast<int>(M->m);
+    a.rowsPerCta = rows * kClusterThreads;
+    a.halo = halo;
+    a.iterations = M->options.coarseIterations;
+    M->cluster = a;
+    M->clusterCtas = ctas;
+    M->clusterTriples = nt;
+    M->clusterRows = rows;
+    M->clusterSmem = static_cast<size_t>(smem);
+    return CIECU_OK;
+}
+
+// At every solve: the coarse values into the FP32 copy, and whether they are
+// bitwise symmetric (the cluster kernel reads the upper half only).
+int refresh_cluster(ciecu_mgcg_s* M, cudaStream_t st) {
+    M->clusterActive = false;
+    if (!M->clusterCtas || !M->clusterAllowed) return CIECU_OK;
+    CIECU_TRY(dia_fill_f32(M->Ac, M->coarseDia, M->coarse32, nullptr, st));
+    bool sym = false;
+    CIECU_TRY(dia_symmetric<float>(M->coarseDia, st, reinterpret_cast<unsigned*>(M->Ac->space->d_result), &sym));
+    M->clusterActive = sym;
+    return CIECU_OK;
+}
+
+// ec = C rc: coarseIterations Jacobi-PCG iterations from zero, result in M->cx:
+// one cluster launch when the coarse matrix allows it, else the pipelined form
+// (one kernel per iteration).
 int coarse_solve(ciecu_mgcg_s* M, cudaStream_t st) {
+    if (M->clusterActive) {
+        cudaLaunchAttribute attr{};
+        const cudaLaunchConfig_t cfg = cluster_config(M, st, &attr);
+        const cudaError_t e =
+            cudaLaunchKernelEx(&cfg, cluster_kernel(M->clusterTriples, M->clusterRows), M->cluster);
+        count_launch();
+        if (e != cudaSuccess) return cuda_fail(e, "coarse_cluster_kernel launch");
+        return CIECU_OK;
+    }
     const long m = M->m;
     ciecu_csr_s* Ac = M->Ac;
     const CoarseVectors v{M->cx, M->cr, M->cu, M->cw, M->cz, M->cq, M->cs, M->cp, {M->cm0, M->cm1}};
@@ -608,6 +967,7 @@ int build_graph(ciecu_mgcg_s* M) {
         }, &M->graph);
     if (status == CIECU_OK) {
         M->deviceLoop = true;
+        M->graphCluster = M->clusterActive;
         return CIECU_OK;
     }
     cudaGetLastError();
@@ -624,6 +984,7 @@ int build_graph(ciecu_mgcg_s* M) {
     e = cudaGraphInstantiate(&M->graph, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return cuda_fail(e, "two-level CG graph instantiate");
+    M->graphCluster = M->clusterActive;
     return CIECU_OK;
 }
 
@@ -703,6 +1064,7 @@ int ciecu_mgcg_destroy(ciecu_mgcg M) {
         cudaFree(v);
     for (float* v : {M->dinv32, M->r32, M->z32, M->t32, M->cheb32}) cudaFree(v);
     cudaFree(M->col16);
+    cudaFree(M->coarse32);
     cudaFree(M->d_s);
     cudaFree(M->counter);
     if (M->h_s) cudaFreeHost(M->h_s);
@@ -784,6 +1146,13 @@ int ciecu_mgcg_create(ciecu_csr fine, const double* d_fineInverseDiagonal, ciecu
             return status;
         }
     }
+    {
+        const int status = prepare_cluster(M, st);
+        if (status != CIECU_OK) {
+            ciecu_mgcg_destroy(M);
+            return status;
+        }
+    }
     M->lambdaMax = options.lambdaMax;
     if (!(M->lambdaMax > 0.0) && M->n > 0) {
         double lam = 0.0;
@@ -814,6 +1183,11 @@ int ciecu_mgcg_product(ciecu_mgcg M, double inScale, const double* d_in, double 
     }
     CIECU_CUDA(cudaMemcpyAsync(M->x, d_out, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
     if (M->settings.iterationCount > 0) {
+        CIECU_TRY(refresh_cluster(M, st));
+        if (M->graph && M->graphCluster != M->clusterActive) {  // the coarse form changed: capture again
+            cudaGraphExecDestroy(M->graph);
+            M->graph = nullptr;
+        }
         MgScalars init{};
         init.maxIter = M->settings.iterationCount;
         init.absTol = M->settings.absoluteResidual;
@@ -864,6 +1238,33 @@ int ciecu_mgcg_smoother_info(ciecu_mgcg M, int* offsets16, int* lanesPerRow) {
     CIECU_REQUIRE(M && offsets16 && lanesPerRow, "mgcg_smoother_info: null argument");
     *offsets16 = M->col16 ? 1 : 0;
     *lanesPerRow = M->col16 ? M->lanes16 : 0;
+    return CIECU_OK;
+}
+
+int ciecu_mgcg_coarse_apply(ciecu_mgcg M, const double* d_in, double* d_out) {
+    CIECU_REQUIRE(M, "mgcg_coarse_apply: null solver");
+    CIECU_REQUIRE(M->m == 0 || (d_in && d_out), "mgcg_coarse_apply: null vector");
+    if (M->m == 0) return CIECU_OK;
+    cudaStream_t st = M->A->space->stream;
+    CIECU_TRY(refresh_cluster(M, st));
+    CIECU_CUDA(cudaMemcpyAsync(M->rc, d_in, sizeof(double) * M->m, cudaMemcpyDeviceToDevice, st));
+    CIECU_TRY(coarse_solve(M, st));
+    CIECU_CHECK_LAUNCH("coarse solve");
+    CIECU_CUDA(cudaMemcpyAsync(d_out, M->cx, sizeof(double) * M->m, cudaMemcpyDeviceToDevice, st));
+    CIECU_CUDA(cudaStreamSynchronize(st));
+    return CIECU_OK;
+}
+
+int ciecu_mgcg_set_coarse_cluster(ciecu_mgcg M, int enable) {
+    CIECU_REQUIRE(M, "mgcg_set_coarse_cluster: null solver");
+    M->clusterAllowed = enable != 0;
+    return CIECU_OK;
+}
+
+int ciecu_mgcg_coarse_info(ciecu_mgcg M, int* clusterCtas, int* active) {
+    CIECU_REQUIRE(M && clusterCtas && active, "mgcg_coarse_info: null argument");
+    *clusterCtas = M->clusterCtas;
+    *active = M->clusterActive ? 1 : 0;
     return CIECU_OK;
 }
 

@@ -189,13 +189,30 @@ class TwoLevelCG(LinearOperator):
     def getStats(self):
         return self._stats
 
+    def set_coarse_cluster(self, enable):
+        """False: the pipelined coarse kernels (one launch per coarse iteration) even
+        where the one-launch cluster form applies; True (the default): the cluster
+        form where the coarse matrix allows it.  Takes effect at the next product."""
+        call("ciecu_mgcg_set_coarse_cluster", self.handle, int(bool(enable)))
+
+    def coarse_apply(self, in_, out):
+        """out = C in: the cycle's coarse solve alone (coarse-sized FP64 vectors)."""
+        self.space.enter()
+        try:
+            call("ciecu_mgcg_coarse_apply", self.handle, _ptr(in_), _ptr(out))
+        finally:
+            self.space.leave()
+
     def info(self):
         lam, cycles = ctypes.c_double(), ctypes.c_int64()
         call("ciecu_mgcg_info", self.handle, ctypes.byref(lam), ctypes.byref(cycles))
         o16, lanes = ctypes.c_int(), ctypes.c_int()
         call("ciecu_mgcg_smoother_info", self.handle, ctypes.byref(o16), ctypes.byref(lanes))
+        ctas, active = ctypes.c_int(), ctypes.c_int()
+        call("ciecu_mgcg_coarse_info", self.handle, ctypes.byref(ctas), ctypes.byref(active))
         return {"lambda_max": lam.value, "cycles": cycles.value, "smoother_offsets16": bool(o16.value),
-                "smoother_lanes_per_row": lanes.value}
+                "smoother_lanes_per_row": lanes.value, "coarse_cluster_ctas": ctas.value,
+                "coarse_cluster_active": bool(active.value)}
 
 
 def make_two_level_cg(space, problem, settings, center=None, radius=0.4, alpha=1e-6, depth=2, degree=2,

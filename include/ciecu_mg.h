@@ -55,6 +55,21 @@ int ciecu_mgcg_info(ciecu_mgcg solver, double* h_lambdaMax, int64_t* h_cycles);
  * built at creation), with the lanes per row chosen by timing; 0 / 0 otherwise
  * (int32 columns through the CSR handle's own tuned kernel, or no FP32 smoother). */
 int ciecu_mgcg_smoother_info(ciecu_mgcg solver, int* offsets16, int* lanesPerRow);
+/* The coarse solve's form.  clusterCtas > 0: the coarse matrix has a structured
+ * Q1 stencil (27 diagonals in 3D, 9 in 2D, lexicographic order) small enough for
+ * one thread-block cluster of that many CTAs to hold its FP32 upper half in shared
+ * memory, and every coarse solve of a cycle then runs in one launch (checked at
+ * creation); 0: the pipelined kernels, one launch per coarse iteration.  active =
+ * 1 when the last solve used the cluster (its values were bitwise symmetric in
+ * FP32; checked at every solve). */
+int ciecu_mgcg_coarse_info(ciecu_mgcg solver, int* clusterCtas, int* active);
+/* enable = 0: the pipelined coarse kernels even where the cluster form applies
+ * (for comparison); 1 (the default): the cluster form where it applies.  Takes
+ * effect at the next solve. */
+int ciecu_mgcg_set_coarse_cluster(ciecu_mgcg solver, int enable);
+/* d_out = C d_in: the cycle's coarse solve alone (coarse rows; the form of
+ * ciecu_mgcg_coarse_info, the coarse values read as at a solve). */
+int ciecu_mgcg_coarse_apply(ciecu_mgcg solver, const double* d_in, double* d_out);
 
 #ifdef __cplusplus
 }
