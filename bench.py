@@ -43,11 +43,18 @@ PROFILE_CELLS = [96, 96, 96]
 # 0.1 gives 10 replacements and a solution 2e-11 from the FP64 solver's; 0.01 saves
 # 5 replacements but lands 1.1e-9 away, outside the 1e-9 parity bar.
 DELTA = 0.1
-# Inner-iteration form of the mixed solver: True = the search direction and its
-# product formed by recurrence inside the inner SpMV (two kernels per iteration),
-# False = the separate direction kernel (three).  The other form is timed beside it
-# (over the FP32 DIA copy's triple pass the fused form measured 28.0 against 29.4 ms).
-FUSE = True
+# Inner-iteration form of the mixed solver (MixedPrecisionCG fuseDirection): 1 = the
+# search direction and its product formed by recurrence inside the inner SpMV (two
+# kernels per inner iteration), 2 = one kernel per inner iteration over the FP32 DIA
+# copy (pending step, direction and product in one row pass), 0 = a separate
+# direction kernel (three).  OTHER_FORM is timed beside it on the same system: at
+# 128^3 the one-kernel form measured 38.0 ms against 27.7 ms for the two-kernel
+# form (its row pass gathers r, q, p and D^-1 where the two-kernel pass gathers z).
+FUSE = 1
+OTHER_FORM = 2
+FORM_NAMES = {0: "three kernels per inner iteration (separate direction kernel)",
+              1: "two kernels per inner iteration (fused direction)",
+              2: "one kernel per inner iteration (single pass)"}
 # Two-level CG on the finite-cell Q3 sphere: (smoothing precision, Chebyshev
 # degree, pipelined coarse PCG iterations per cycle)
 TWO_LEVEL = (("f64", 4, 80), ("f32", 6, 80))
@@ -374,7 +381,7 @@ def main():
     launches = launch_count() - launches0
 
     # the other inner-iteration form on the same system (reported, not the headline)
-    other = MixedPrecisionCG(A, D, settings, mode=0, delta=DELTA, fuseDirection=not FUSE)
+    other = MixedPrecisionCG(A, D, settings, mode=0, delta=DELTA, fuseDirection=OTHER_FORM)
     xother = torch.zeros_like(prob.rhs)
 
     def solve_other():
@@ -499,8 +506,7 @@ def main():
             "data": "synthetic (seeded mt19937_64 RHS and kappa field)",
             "config": common_config(world),
             "solver": {"mixed": "jacobi-pcg, FP32 inner over %s, FP64 reliable updates delta=%g, %s" % (
-                           info["format"], DELTA,
-                           "fused direction" if FUSE else "separate direction kernel"),
+                           info["format"], DELTA, FORM_NAMES[3 - mixed.kernels_per_iteration]),
                        "fp64": "jacobi-pcg over %s" % (("dia, symmetric upper half" if cg.info().get(
                            "dia_symmetric") else "dia") if dia64 else "csr")},
             "gpu_launches": int(launches),
@@ -518,7 +524,7 @@ def main():
             "mixed": {"seconds": t_mixed, "inner_iterations": mst.innerIterations,
                       "refinements": mst.refinements, "true_relative_residual": rel_mixed,
                       "rel_diff_vs_fp64_solution": agree, "achieved_gbs": mixed_solve_bytes / t_mixed / 1e9},
-            "mixed_other_form": {"form": "fused direction" if not FUSE else "separate direction kernel",
+            "mixed_other_form": {"form": FORM_NAMES[3 - other.kernels_per_iteration],
                                  "seconds": t_other, "inner_iterations": ost.innerIterations,
                                  "refinements": ost.refinements, "true_relative_residual": rel_other,
                                  "achieved_gbs": (ost.innerIterations * inner_bytes +

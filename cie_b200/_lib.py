@@ -98,6 +98,7 @@ SIGNATURES = {
     "ciecu_mixed_apply_f32": (c_int, [P, P, P]),
     "ciecu_mixed_padded_entries": (c_int, [P, P]),
     "ciecu_mixed_dia_info": (c_int, [P, P, P]),
+    "ciecu_mixed_form": (c_int, [P, P]),
     # host utilities
     "ciecu_structured_dofmap": (c_int, [c_int, c_int, P, P, P]),
     "ciecu_structured_boundary": (c_int, [c_int, c_int, P, P]),

@@ -41,10 +41,10 @@ def headers():
     return hs
 
 
-def build(verbose=False, force=False):
+def build(verbose=False, force=False, jobs=None):
     os.makedirs(BUILD, exist_ok=True)
     newest_header = max((os.path.getmtime(h) for h in headers()), default=0)
-    objects = []
+    objects, commands = [], []
     for src in sources():
         obj = os.path.join(BUILD, os.path.basename(src) + ".o")
         objects.append(obj)
@@ -56,9 +56,19 @@ def build(verbose=False, force=False):
             cmd += ["-x", "cu"]
         if verbose and src.endswith(".cu"):
             cmd += ["-Xptxas", "-v"]
-        print(" ".join(os.path.basename(c) if c == src else c for c in cmd[:1] + ["...", os.path.basename(src)]),
-              flush=True)
-        subprocess.run(cmd, check=True)
+        commands.append((src, cmd))
+    # translation units compile independently: one nvcc per core, at most 8
+    jobs = jobs or max(1, min(8, os.cpu_count() or 1))
+    running = []
+    for src, cmd in commands:
+        print("%s ... %s" % (NVCC, os.path.basename(src)), flush=True)
+        running.append((src, subprocess.Popen(cmd)))
+        while len(running) >= jobs or (running and src == commands[-1][0]):
+            src0, proc = running.pop(0)
+            if proc.wait() != 0:
+                for _, other in running:
+                    other.wait()
+                raise subprocess.CalledProcessError(proc.returncode, "nvcc " + os.path.basename(src0))
     if (force or not os.path.exists(LIB)
             or max(os.path.getmtime(o) for o in objects) > os.path.getmtime(LIB)):
         cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objects + ["-lcudart", "-lcuda"]

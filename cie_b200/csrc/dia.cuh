@@ -73,16 +73,16 @@ __device__ __forceinline__ void dia_rows(const DiaArgs<V>& A, const T* __restric
 // Four consecutive rows per thread with 16-byte loads of each diagonal (FP32:
 // a warp reads 512 contiguous bytes per diagonal instead of 128).  Rows past
 // nrows (up to ld, zero-filled) are computed and dropped; the gathers stay
-// inside [0, nrows).  The operand entry of column c is gather(c).
+// inside [0, nrows).  The operand entry of column c is gather(c); the epilogue
+// takes the four rows at once (op.pre4(r, pre), op.post4(r, pre, sum)) and skips
+// rows past nrows itself.
 template <int ND, typename Op, typename TGather>
 __device__ __forceinline__ void dia_rows4_gather(const DiaArgs<float>& A, const TGather& gather, Op& op) {
     const long stride = static_cast<long>(gridDim.x) * blockDim.x * 4;
     for (long r0 = (static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x) * 4; r0 < A.nrows; r0 += stride) {
         const int r = static_cast<int>(r0);
         typename Op::Pre pre[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-            if (r + i < A.nrows) pre[i] = op.pre(r + i);
+        op.pre4(r, pre);
         float sum[4] = {0.f, 0.f, 0.f, 0.f};
         for_diagonals<ND>(A, [&](int d) {
             const float4 v = __ldcs(reinterpret_cast<const float4*>(A.val + static_cast<long>(d) * A.ld + r));
@@ -96,15 +96,33 @@ __device__ __forceinline__ void dia_rows4_gather(const DiaArgs<float>& A, const 
             sum[2] = fmaf(v.z, xv[2], sum[2]);
             sum[3] = fmaf(v.w, xv[3], sum[3]);
         });
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-            if (r + i < A.nrows) op.post(r + i, pre[i], sum[i]);
+        op.post4(r, pre, sum);
     }
 }
 
+// Row-by-row pre/post of an epilogue of the CSR interface, as the four-row
+// epilogue (pre4 / post4 for rows r .. r + 3) that the four-row passes call.
+template <typename Op>
+struct RowsOf4 {
+    using Pre = typename Op::Pre;
+    Op& op;
+    int nrows;
+    __device__ __forceinline__ void pre4(int r, Pre (&pre)[4]) const {
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            if (r + i < nrows) pre[i] = op.pre(r + i);
+    }
+    __device__ __forceinline__ void post4(int r, Pre (&pre)[4], const float (&sum)[4]) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            if (r + i < nrows) op.post(r + i, pre[i], sum[i]);
+    }
+};
+
 template <int ND, typename Op>
 __device__ __forceinline__ void dia_rows4(const DiaArgs<float>& A, const float* __restrict__ x, Op& op) {
-    dia_rows4_gather<ND>(A, LoadGather<float>{x}, op);
+    RowsOf4<Op> rows{op, A.nrows};
+    dia_rows4_gather<ND>(A, LoadGather<float>{x}, rows);
 }
 
 // dia_rows4 for stencils whose sorted offsets come in consecutive triples
@@ -112,24 +130,22 @@ __device__ __forceinline__ void dia_rows4(const DiaArgs<float>& A, const float* 
 // operand entries x[r + o - 1 .. r + o + 4] of its four rows once, where
 // dia_rows4 loads twelve.  Triples ascending and the three diagonals of a triple
 // in order keep every row sum in the column order of dia_rows4, bit for bit.
-template <int ND, typename Op>
-__device__ __forceinline__ void dia_rows4_triples(const DiaArgs<float>& A, const float* __restrict__ x, Op& op) {
+template <int ND, typename Op, typename TGather>
+__device__ __forceinline__ void dia_rows4_triples_gather(const DiaArgs<float>& A, const TGather& gather, Op& op) {
     constexpr int NT = ND / 3;
     const int nt = NT > 0 ? NT : A.ndiag / 3;
     const long stride = static_cast<long>(gridDim.x) * blockDim.x * 4;
     for (long r0 = (static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x) * 4; r0 < A.nrows; r0 += stride) {
         const int r = static_cast<int>(r0);
         typename Op::Pre pre[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-            if (r + i < A.nrows) pre[i] = op.pre(r + i);
+        op.pre4(r, pre);
         float sum[4] = {0.f, 0.f, 0.f, 0.f};
         auto triple = [&](int t) {
             const int c = r + A.off[3 * t + 1] - 1;
             float xv[6];
 #pragma unroll
             for (int j = 0; j < 6; ++j)
-                xv[j] = static_cast<unsigned>(c + j) < static_cast<unsigned>(A.nrows) ? __ldg(x + c + j) : 0.f;
+                xv[j] = static_cast<unsigned>(c + j) < static_cast<unsigned>(A.nrows) ? gather(c + j) : 0.f;
 #pragma unroll
             for (int e = 0; e < 3; ++e) {
                 const float4 v = __ldcs(reinterpret_cast<const float4*>(A.val + static_cast<long>(3 * t + e) * A.ld + r));
@@ -145,10 +161,92 @@ __device__ __forceinline__ void dia_rows4_triples(const DiaArgs<float>& A, const
         } else {
             for (int t = 0; t < nt; ++t) triple(t);
         }
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-            if (r + i < A.nrows) op.post(r + i, pre[i], sum[i]);
+        op.post4(r, pre, sum);
     }
+}
+
+// dia_rows4_triples_gather for an operand that is costly to gather (formed from
+// several vectors): per triple a lane needs the six operand entries starting at
+// column c = r + o - 1, i.e. offsets s .. s + 5 (s = c mod 4, the same in every
+// lane) of the three aligned 4-column blocks b, b + 1, b + 2 with 4b = c - s.
+// Block b + 1 of lane l is block b of lane l + 1, and block b + 2 that of lane
+// l + 2, so each lane forms ONE block (gather.block(b): the four operand values
+// of columns 4b .. 4b + 3 from 16-byte loads) and takes the others from its
+// neighbours by warp shuffles; the last lanes of the warp form theirs directly.
+// A warp takes this path when all of its 32 lanes hold rows (R + 128 <= nrows)
+// and every block it touches lies inside [0, nrows); otherwise it gathers entry
+// by entry through gather(c) as dia_rows4_triples_gather does.  Values and sums
+// are the same either way.  blockDim.x must be a multiple of 32.
+template <int ND, typename Op, typename TGather>
+__device__ __forceinline__ void dia_rows4_triples_window(const DiaArgs<float>& A, const TGather& gather, Op& op) {
+    constexpr int NT = ND / 3;
+    const int nt = NT > 0 ? NT : A.ndiag / 3;
+    const int lane = threadIdx.x & 31;
+    const long stride = static_cast<long>(gridDim.x) * blockDim.x * 4;
+    const long warpBase = (static_cast<long>(blockIdx.x) * blockDim.x + (threadIdx.x & ~31)) * 4;
+    for (long R = warpBase; R < A.nrows; R += stride) {
+        const bool fullWarp = R + 128 <= A.nrows;  // the same in every lane
+        const int r = static_cast<int>(R) + 4 * lane;
+        if (!fullWarp && r >= A.nrows) continue;  // this warp takes the entry-by-entry path only
+        typename Op::Pre pre[4];
+        op.pre4(r, pre);
+        float sum[4] = {0.f, 0.f, 0.f, 0.f};
+        auto triple = [&](int t) {
+            const int o = A.off[3 * t + 1];
+            const int s = (o - 1) & 3;
+            const long first = R + o - 1 - s;  // first column of lane 0's blocks
+            float xv[6];
+            if (fullWarp && first >= 0 && first + 4 * 31 + 11 < A.nrows) {
+                const int b = static_cast<int>((r + o - 1 - s) >> 2);
+                const float4 p0 = gather.block(b);
+                float4 p1;
+                p1.x = __shfl_down_sync(0xffffffffu, p0.x, 1);
+                p1.y = __shfl_down_sync(0xffffffffu, p0.y, 1);
+                p1.z = __shfl_down_sync(0xffffffffu, p0.z, 1);
+                p1.w = __shfl_down_sync(0xffffffffu, p0.w, 1);
+                if (lane == 31) p1 = gather.block(b + 1);
+                if (s == 3) {
+                    float p2 = __shfl_down_sync(0xffffffffu, p0.x, 2);
+                    const float from31 = __shfl_down_sync(0xffffffffu, p1.x, 1);
+                    if (lane == 30) p2 = from31;
+                    if (lane == 31) p2 = gather.block(b + 2).x;
+                    xv[0] = p0.w; xv[1] = p1.x; xv[2] = p1.y; xv[3] = p1.z; xv[4] = p1.w; xv[5] = p2;
+                } else if (s == 2) {
+                    xv[0] = p0.z; xv[1] = p0.w; xv[2] = p1.x; xv[3] = p1.y; xv[4] = p1.z; xv[5] = p1.w;
+                } else if (s == 1) {
+                    xv[0] = p0.y; xv[1] = p0.z; xv[2] = p0.w; xv[3] = p1.x; xv[4] = p1.y; xv[5] = p1.z;
+                } else {
+                    xv[0] = p0.x; xv[1] = p0.y; xv[2] = p0.z; xv[3] = p0.w; xv[4] = p1.x; xv[5] = p1.y;
+                }
+            } else {
+                const int c = r + o - 1;
+#pragma unroll
+                for (int j = 0; j < 6; ++j)
+                    xv[j] = static_cast<unsigned>(c + j) < static_cast<unsigned>(A.nrows) ? gather(c + j) : 0.f;
+            }
+#pragma unroll
+            for (int e = 0; e < 3; ++e) {
+                const float4 v = __ldcs(reinterpret_cast<const float4*>(A.val + static_cast<long>(3 * t + e) * A.ld + r));
+                sum[0] = fmaf(v.x, xv[e], sum[0]);
+                sum[1] = fmaf(v.y, xv[e + 1], sum[1]);
+                sum[2] = fmaf(v.z, xv[e + 2], sum[2]);
+                sum[3] = fmaf(v.w, xv[e + 3], sum[3]);
+            }
+        };
+        if constexpr (NT > 0) {
+#pragma unroll
+            for (int t = 0; t < NT; ++t) triple(t);
+        } else {
+            for (int t = 0; t < nt; ++t) triple(t);
+        }
+        op.post4(r, pre, sum);
+    }
+}
+
+template <int ND, typename Op>
+__device__ __forceinline__ void dia_rows4_triples(const DiaArgs<float>& A, const float* __restrict__ x, Op& op) {
+    RowsOf4<Op> rows{op, A.nrows};
+    dia_rows4_triples_gather<ND>(A, LoadGather<float>{x}, rows);
 }
 
 // CIECU_DIA_TRIPLES=0 keeps the plain four-row pass for triple stencils (for

@@ -284,6 +284,252 @@ __global__ void __launch_bounds__(kT) mixed_spmv_dia_kernel(DiaArgs<float> A, co
     }
 }
 
+// ---- single-pass inner iteration (options.fuseDirection == 2, DIA inner matrix) ----
+//
+// One kernel per inner iteration instead of two or three.  Kernel k+1 receives
+// alpha_k and beta_{k+1} and, for its own rows,
+//   x += alpha_k p_k,  r_{k+1} = r_k - alpha_k q_k,  z = D^-1 r_{k+1},
+//   p_{k+1} = z + beta_{k+1} p_k,  q_{k+1} = A32 p_{k+1};
+// the operand entries p_{k+1}[j] of the row sums are formed the same way from the
+// gathered r_k[j], q_k[j], p_k[j], D^-1[j] (bit for bit the values the owning row
+// stores).  beta_{k+1} = rho_{k+1} / rho_k needs rho_{k+1} = r_{k+1}^T D^-1 r_{k+1}
+// before r_{k+1} exists; with r_{k+1} = r_k - alpha_k q_k it is the quadratic
+//   rho_{k+1} = (r_k^T D^-1 r_k) - 2 alpha_k (r_k^T D^-1 q_k) + alpha_k^2 (q_k^T D^-1 q_k),
+// whose three sums (and the three of ||r_{k+1}||^2) kernel k reduces in FP64
+// beside p_k^T q_k.  alpha_k = rho_k / p_k^T q_k uses the rho of the stored FP32
+// r_k, as the three-kernel form does; beta and the replacement decision use the
+// expansion, which differs from the FP32-rounded vector's sums by its rounding.
+// A residual replacement due after step k (decided on the expanded ||r_{k+1}||)
+// folds x + alpha_k p_k into x64, recomputes r in FP64 and restarts the step
+// with alpha = 0, so the Krylov direction is kept exactly as in the other forms.
+// r, p and q are double-buffered (set iter & 1 read, the other written): rows of
+// other blocks gather the old values while this block writes the new ones.
+// Over the Q1 triple stencils the operand windows come from 16-byte loads and
+// warp shuffles (dia_rows4_triples_window).  It moves 36N vector bytes per
+// iteration against 52N for the two-kernel form, but the gathers read four
+// vectors instead of one: at 128^3 it measured 38.0 ms per solve against 27.7 ms
+// (33.5 ms on the Jacobi-scaled inner system, which gathers three).
+struct SingleVectors {
+    float* r[2];
+    float* p[2];
+    float* q[2];
+};
+
+template <bool SCALED>
+struct SingleStep {
+    const float* __restrict__ r;
+    const float* __restrict__ q;
+    const float* __restrict__ p;
+    const float* __restrict__ dinv;
+    float alpha, beta;
+    bool step;   // alpha != 0: apply the pending step to x and r
+    bool fresh;  // beta == 0: p = z (first iteration, restart)
+
+    // r_{k+1}, then p_{k+1} from it; the same operations in every caller.
+    __device__ __forceinline__ float residual(float rk, float qk) const { return step ? fmaf(-alpha, qk, rk) : rk; }
+    __device__ __forceinline__ float direction(float rn, float pk, float d) const {
+        const float z = SCALED ? rn : __fmul_rn(rn, d);
+        return fresh ? z : fmaf(beta, pk, z);
+    }
+    // operand entry of column c (inside [0, n))
+    __device__ __forceinline__ float operator()(int c) const {
+        const float rk = __ldg(r + c);
+        const float rn = residual(rk, step ? __ldg(q + c) : 0.f);
+        return direction(rn, fresh ? 0.f : __ldg(p + c), SCALED ? 1.f : __ldg(dinv + c));
+    }
+    // operand entries of columns 4b .. 4b + 3 (inside [0, n)), from 16-byte loads
+    __device__ __forceinline__ float4 block(int b) const {
+        const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f), one = make_float4(1.f, 1.f, 1.f, 1.f);
+        const float4 rk = __ldg(reinterpret_cast<const float4*>(r) + b);
+        const float4 qk = step ? __ldg(reinterpret_cast<const float4*>(q) + b) : zero;
+        const float4 pk = fresh ? zero : __ldg(reinterpret_cast<const float4*>(p) + b);
+        const float4 dk = SCALED ? one : __ldg(reinterpret_cast<const float4*>(dinv) + b);
+        return make_float4(direction(residual(rk.x, qk.x), pk.x, dk.x), direction(residual(rk.y, qk.y), pk.y, dk.y),
+                           direction(residual(rk.z, qk.z), pk.z, dk.z), direction(residual(rk.w, qk.w), pk.w, dk.w));
+    }
+};
+
+template <bool SCALED>
+struct SingleOp {
+    struct Pre {
+        float x, r, p, d;
+    };
+    static constexpr int K = SCALED ? 4 : 7;
+    SingleStep<SCALED> in;
+    float* __restrict__ x;
+    float* __restrict__ r;  // write set
+    float* __restrict__ p;
+    float* __restrict__ q;
+    int n;
+    // p^T q, then ||r||^2, r^T q, ||q||^2, then (unscaled) the same three weighted by D^-1
+    double acc[K];
+
+    __device__ __forceinline__ Pre make(float xk, float rk, float pk, float qk, float d) const {
+        Pre o;
+        o.r = in.residual(rk, qk);
+        o.x = in.step ? fmaf(in.alpha, pk, xk) : xk;
+        o.p = in.direction(o.r, pk, d);
+        o.d = d;
+        return o;
+    }
+    __device__ __forceinline__ void pre4(int row, Pre (&pre)[4]) const {
+        if (row + 3 < n) {
+            const float4 rk = *reinterpret_cast<const float4*>(in.r + row);
+            const float4 qk = in.step ? *reinterpret_cast<const float4*>(in.q + row) : make_float4(0.f, 0.f, 0.f, 0.f);
+            const float4 pk = (in.step || !in.fresh) ? *reinterpret_cast<const float4*>(in.p + row)
+                                                    : make_float4(0.f, 0.f, 0.f, 0.f);
+            const float4 xk = in.step ? *reinterpret_cast<const float4*>(x + row) : make_float4(0.f, 0.f, 0.f, 0.f);
+            const float4 dk = SCALED ? make_float4(1.f, 1.f, 1.f, 1.f) : *reinterpret_cast<const float4*>(in.dinv + row);
+            pre[0] = make(xk.x, rk.x, pk.x, qk.x, dk.x);
+            pre[1] = make(xk.y, rk.y, pk.y, qk.y, dk.y);
+            pre[2] = make(xk.z, rk.z, pk.z, qk.z, dk.z);
+            pre[3] = make(xk.w, rk.w, pk.w, qk.w, dk.w);
+            return;
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            if (row + i < n) {
+                const int j = row + i;
+                pre[i] = make(in.step ? x[j] : 0.f, in.r[j], (in.step || !in.fresh) ? in.p[j] : 0.f,
+                              in.step ? in.q[j] : 0.f, SCALED ? 1.f : in.dinv[j]);
+            }
+    }
+    __device__ __forceinline__ void sums(const Pre& o, float qn) {
+        const double rv = o.r, qv = qn;
+        acc[0] = fma(static_cast<double>(o.p), qv, acc[0]);
+        acc[1] = fma(rv, rv, acc[1]);
+        acc[2] = fma(rv, qv, acc[2]);
+        acc[3] = fma(qv, qv, acc[3]);
+        if constexpr (!SCALED) {
+            const double d = o.d;
+            acc[4] = fma(d * rv, rv, acc[4]);
+            acc[5] = fma(d * rv, qv, acc[5]);
+            acc[6] = fma(d * qv, qv, acc[6]);
+        }
+    }
+    __device__ __forceinline__ void post4(int row, Pre (&pre)[4], const float (&sum)[4]) {
+        if (row + 3 < n) {
+            if (in.step)
+                *reinterpret_cast<float4*>(x + row) = make_float4(pre[0].x, pre[1].x, pre[2].x, pre[3].x);
+            *reinterpret_cast<float4*>(r + row) = make_float4(pre[0].r, pre[1].r, pre[2].r, pre[3].r);
+            *reinterpret_cast<float4*>(p + row) = make_float4(pre[0].p, pre[1].p, pre[2].p, pre[3].p);
+            *reinterpret_cast<float4*>(q + row) = make_float4(sum[0], sum[1], sum[2], sum[3]);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) sums(pre[i], sum[i]);
+            return;
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            if (row + i < n) {
+                const int j = row + i;
+                if (in.step) x[j] = pre[i].x;
+                r[j] = pre[i].r;
+                p[j] = pre[i].p;
+                q[j] = sum[i];
+                sums(pre[i], sum[i]);
+            }
+    }
+};
+
+// Last block of a single-pass iteration: alpha_k, the expanded rho_{k+1} and
+// ||r_{k+1}||, the replacement decision of mixed_update_kernel, beta_{k+1}.
+// tot: p^T q, ||r||^2, r^T q, ||q||^2 and (unscaled) r^T D^-1 r, r^T D^-1 q, q^T D^-1 q.
+template <bool COND, int K>
+__device__ void single_decide(MixedScalars* s, const double (&tot)[K], cudaGraphConditionalHandle loop,
+                              cudaGraphConditionalHandle refine) {
+    const int w = K == 7 ? 4 : 1;  // first of the three D^-1-weighted sums
+    const double rho = tot[w];
+    s->pq = tot[0];
+    s->iter += 1;
+    s->rz = rho;
+    s->updateX = 0;
+    bool update;
+    if (!(0.0 < tot[0])) {  // FP32 breakdown: no step, replacement with a restarted direction
+        s->alpha = 0.0;
+        s->restart = 1;
+        s->breakdowns += 1;
+        if (s->breakdowns > kMaxInnerBreakdowns) {
+            s->done = 3;
+            s->error = CIECU_ERR_BREAKDOWN;
+            set_cond<COND>(refine, 0);
+            set_cond<COND>(loop, 0);
+            return;
+        }
+        update = true;
+    } else {
+        const double alpha = rho / tot[0];
+        const double rr = fma(alpha, fma(alpha, tot[3], -2.0 * tot[2]), tot[1]);
+        const double rhoNext = fma(alpha, fma(alpha, tot[w + 2], -2.0 * tot[w + 1]), tot[w]);
+        const double rnorm = rr > 0.0 ? sqrt(rr) : 0.0;
+        s->alpha = alpha;
+        s->sloppy = rnorm;
+        if (s->mode == 0) {
+            if (rnorm > s->maxrx) s->maxrx = rnorm;
+            if (rnorm > s->maxrr) s->maxrr = rnorm;
+            const bool updateX = rnorm < s->delta * s->maxrx;
+            update = updateX || rnorm < s->delta * s->maxrr;
+            s->updateX = updateX ? 1 : 0;
+        } else {
+            update = rnorm < s->delta * s->cycleStart;
+        }
+        update = update || rnorm < s->relTol * s->r0s || rnorm < s->absTol || s->iter >= s->maxIter ||
+                 !(0.0 < rhoNext);
+        if (!update) s->beta = rhoNext / rho;
+    }
+    if (update) s->update = 1;
+    s->chunkIter += 1;
+    set_cond<COND>(refine, update ? 1u : 0u);
+    set_cond<COND>(loop, s->chunkIter < s->chunkLimit ? 1u : 0u);
+}
+
+template <int ND, bool COND, bool SCALED, bool TRIPLES>
+__global__ void __launch_bounds__(kT, 3) mixed_single_dia_kernel(DiaArgs<float> A, float* __restrict__ x,
+                                                             SingleVectors v, const float* __restrict__ dinv,
+                                                             MixedScalars* s, double* partials, unsigned* counter,
+                                                             cudaGraphConditionalHandle loop,
+                                                             cudaGraphConditionalHandle refine) {
+    if (*reinterpret_cast<volatile int*>(&s->done)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            set_cond<COND>(refine, 0);
+            set_cond<COND>(loop, 0);
+        }
+        return;
+    }
+    const int rd = static_cast<int>(*reinterpret_cast<const volatile long long*>(&s->iter) & 1);
+    const double alpha = *reinterpret_cast<const volatile double*>(&s->alpha);
+    const double beta = *reinterpret_cast<const volatile double*>(&s->beta);
+    // (selects, not an index: a runtime index would put v in local memory)
+    const SingleStep<SCALED> in{rd ? v.r[1] : v.r[0], rd ? v.q[1] : v.q[0], rd ? v.p[1] : v.p[0], dinv,
+                                static_cast<float>(alpha), static_cast<float>(beta), alpha != 0.0, beta == 0.0};
+    SingleOp<SCALED> op{in, x, rd ? v.r[0] : v.r[1], rd ? v.p[0] : v.p[1], rd ? v.q[0] : v.q[1], A.nrows, {}};
+    if constexpr (TRIPLES)
+        dia_rows4_triples_window<ND>(A, in, op);
+    else
+        dia_rows4_gather<ND>(A, in, op);
+    constexpr int K = SingleOp<SCALED>::K;
+    double tot[K];
+    if (grid_reduce_last<K, kT>(op.acc, partials, counter, tot) && threadIdx.x == 0)
+        single_decide<COND, K>(s, tot, loop, refine);
+}
+
+// R1 of the single-pass form: x64 += x32 + alpha p (the step decided but not yet
+// applied; alpha = 0 after an FP32 breakdown), x32 = 0.
+__global__ void __launch_bounds__(kT) mixed_fold_pending_kernel(long n, double* __restrict__ x64,
+                                                                float* __restrict__ x32, SingleVectors v,
+                                                                const double* __restrict__ sdiag,
+                                                                const MixedScalars* s) {
+    if (!*reinterpret_cast<const volatile int*>(&s->update)) return;
+    const float* p = (s->iter & 1) ? v.p[1] : v.p[0];
+    const float alpha = static_cast<float>(s->alpha);
+    const bool step = s->alpha != 0.0;
+    const long stride = static_cast<long>(gridDim.x) * kT;
+    for (long i = static_cast<long>(blockIdx.x) * kT + threadIdx.x; i < n; i += stride) {
+        const float xi = step ? fmaf(alpha, p[i], x32[i]) : x32[i];
+        x64[i] += sdiag ? static_cast<double>(xi) * sdiag[i] : static_cast<double>(xi);
+        x32[i] = 0.0f;
+    }
+}
+
 // TMA-pipelined variants of the two kernels above (sell_tma.cuh): one CTA of
 // kTmaWarps warps per SM, the matrix streamed through shared memory.
 template <typename CI>
@@ -455,16 +701,18 @@ struct ResidualOp {
 };
 
 // R2 (and set-up): r = b - A64 x64 in FP64; r32 = float(r); ||r||^2 and r32^T z32
-// in FP64.  INIT: first residual of a solve.
+// in FP64.  INIT: first residual of a solve.  r32alt (the single-pass form's
+// second residual buffer, else null) takes r when the iteration count is odd.
 template <int KERNEL, bool INIT, bool COND>
 __global__ void __launch_bounds__(csr_threads<KERNEL>())
     mixed_residual_kernel(CsrArgs<double> A, const double* __restrict__ b, const double* __restrict__ x64,
-                          const float* __restrict__ dinv, float* __restrict__ r32, float* __restrict__ z32,
-                          const double* __restrict__ sdiag, MixedScalars* s, double* partials, unsigned* counter,
-                          cudaGraphConditionalHandle loop) {
+                          const float* __restrict__ dinv, float* __restrict__ r32, float* __restrict__ r32alt,
+                          float* __restrict__ z32, const double* __restrict__ sdiag, MixedScalars* s,
+                          double* partials, unsigned* counter, cudaGraphConditionalHandle loop) {
     if (!INIT && !*reinterpret_cast<volatile int*>(&s->update)) return;
     constexpr int T = csr_threads<KERNEL>();
-    ResidualOp op{b, dinv, r32, z32, sdiag, 0.0, 0.0};
+    float* rdst = (r32alt && (*reinterpret_cast<const volatile long long*>(&s->iter) & 1)) ? r32alt : r32;
+    ResidualOp op{b, dinv, rdst, z32, sdiag, 0.0, 0.0};
     csr_rows<KERNEL, double, double, false>(A, x64, op);
     const double rr = op.rr, rz = op.rz;
     double mine[2] = {rr, rz}, tot[2];
@@ -485,6 +733,7 @@ __global__ void __launch_bounds__(csr_threads<KERNEL>())
             s->update = 0;
             s->done = 0;
             s->error = 0;
+            s->alpha = 0.0;
             s->beta = 0.0;
             s->rz = tot[1];
             if (float_less(rnorm, s->absTol) || float_less(1.0, s->relTol)) {
@@ -519,6 +768,7 @@ __global__ void __launch_bounds__(csr_threads<KERNEL>())
             }
             s->rz = tot[1];
         }
+        s->alpha = 0.0;  // the single-pass form's pending step is folded into x64
         s->restart = 0;
         if (s->done) set_cond<COND>(loop, 0);
     }
@@ -611,6 +861,8 @@ struct ciecu_mixed_s {
     double* sdiag = nullptr;  // sqrt(D^-1) when the inner system is scaled
     float *x32 = nullptr, *r32 = nullptr, *p32 = nullptr, *q32 = nullptr;
     float* z32 = nullptr;  // z = D^-1 r, kept only by the fused form (options.fuseDirection)
+    int form = 0;          // options.fuseDirection: kernels per inner iteration 3 (0), 2 (1), 1 (2, DIA inner)
+    float *r32b = nullptr, *p32b = nullptr, *q32b = nullptr;  // second buffers of the single-pass form
     double* x64 = nullptr;
     const double* b = nullptr;
     ciecu::MixedScalars* d_s = nullptr;
@@ -691,6 +943,33 @@ int launch_inner_spmv(ciecu_mixed_s* M, cudaStream_t st, cudaGraphConditionalHan
     return M->z32 ? launch_inner_spmv_form<COND, true>(M, st, loop) : launch_inner_spmv_form<COND, false>(M, st, loop);
 }
 
+// The single-pass form runs over the DIA copy only; with another inner kernel a
+// solver created with fuseDirection = 2 runs the fused two-kernel form.
+bool single_pass(const ciecu_mixed_s* M) { return M->form == 2 && M->unroll == kDiaInner; }
+
+SingleVectors single_vectors(const ciecu_mixed_s* M) {
+    return SingleVectors{{M->r32, M->r32b}, {M->p32, M->p32b}, {M->q32, M->q32b}};
+}
+
+template <bool COND>
+int launch_single(ciecu_mixed_s* M, cudaStream_t st, cudaGraphConditionalHandle loop,
+                  cudaGraphConditionalHandle refine) {
+    const long needA = (M->n + kT - 1) / kT;
+    const bool scaled = M->sdiag != nullptr;
+    CIECU_TRY(with_diagonals(M->dia.ndiag, [&](auto nd) -> int {
+        constexpr int ND = decltype(nd)::value;
+        auto* kernel = M->diaTriples ? (scaled ? mixed_single_dia_kernel<ND, COND, true, true>
+                                               : mixed_single_dia_kernel<ND, COND, false, true>)
+                                     : (scaled ? mixed_single_dia_kernel<ND, COND, true, false>
+                                               : mixed_single_dia_kernel<ND, COND, false, false>);
+        kernel<<<fit_grid(kernel, kT, (needA + 3) / 4), kT, 0, st>>>(M->dia, M->x32, single_vectors(M), M->dinv32,
+                                                                     M->d_s, M->d_partials, M->d_counter, loop, refine);
+        return CIECU_OK;
+    }));
+    CIECU_CHECK_LAUNCH("mixed_single_dia_kernel");
+    return CIECU_OK;
+}
+
 // One inner iteration.  With conditional nodes (useCond) the refinement pair
 // R1/R2 sits under IF(refine); otherwise it is launched unconditionally and
 // returns at once unless M2 requested a replacement.
@@ -702,23 +981,30 @@ int launch_inner(ciecu_mixed_s* M, cudaStream_t st, cudaGraph_t root, cudaGraphC
     ciecu_csr_s* A = M->A;
     cudaGraphConditionalHandle refine = 0;
     if (useCond) CIECU_CUDA(cudaGraphConditionalHandleCreate(&refine, root, 0, cudaGraphCondAssignDefault));
-    CIECU_TRY(launch_inner_spmv<COND>(M, st, loop));
-    {
+    const bool single = single_pass(M);
+    if (single) {
+        CIECU_TRY(launch_single<COND>(M, st, loop, refine));
+    } else {
+        CIECU_TRY(launch_inner_spmv<COND>(M, st, loop));
         auto* kernel = M->z32 ? mixed_update_kernel<COND, true> : mixed_update_kernel<COND, false>;
         kernel<<<fit_grid(kernel, kT, needV), kT, 0, st>>>(M->n, M->x32, M->r32, M->z32, M->p32, M->q32, M->dinv32,
                                                            M->d_s, M->d_partials, M->d_counter, loop, refine);
     }
     auto refinement = [&](cudaStream_t s2) -> int {
-        mixed_fold_kernel<<<fit_grid(mixed_fold_kernel, kT, needA), kT, 0, s2>>>(M->n, M->x64, M->x32, M->sdiag,
-                                                                                M->d_s);
+        if (single)
+            mixed_fold_pending_kernel<<<fit_grid(mixed_fold_pending_kernel, kT, needA), kT, 0, s2>>>(
+                M->n, M->x64, M->x32, single_vectors(M), M->sdiag, M->d_s);
+        else
+            mixed_fold_kernel<<<fit_grid(mixed_fold_kernel, kT, needA), kT, 0, s2>>>(M->n, M->x64, M->x32, M->sdiag,
+                                                                                    M->d_s);
         const int needR = csr_grid(A, A->kernel);
         CIECU_TRY(with_schedule(A->kernel, [&](auto k) -> int {
             constexpr int K = decltype(k)::value;
             mixed_residual_kernel<K, false, COND><<<fit_grid(mixed_residual_kernel<K, false, COND>, csr_threads<K>(),
                                                              needR),
                                                     csr_threads<K>(), 0, s2>>>(
-                A->args<double>(), M->b, M->x64, M->dinv32, M->r32, M->z32, M->sdiag, M->d_s, M->d_partials,
-                M->d_counter, loop);
+                A->args<double>(), M->b, M->x64, M->dinv32, M->r32, single ? M->r32b : nullptr,
+                single ? nullptr : M->z32, M->sdiag, M->d_s, M->d_partials, M->d_counter, loop);
             return CIECU_OK;
         }));
         return CIECU_OK;
@@ -727,7 +1013,7 @@ int launch_inner(ciecu_mixed_s* M, cudaStream_t st, cudaGraph_t root, cudaGraphC
         CIECU_TRY(capture_if(st, M->side, refine, refinement));
     else
         CIECU_TRY(refinement(st));
-    if (!M->z32)
+    if (!M->z32 && !single)
         mixed_direction_kernel<<<fit_grid(mixed_direction_kernel, kT, needV), kT, 0, st>>>(M->n, M->p32, M->r32,
                                                                                            M->dinv32, M->d_s);
     CIECU_CHECK_LAUNCH("mixed inner iteration");
@@ -875,6 +1161,8 @@ int ciecu_mixed_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_sta
     CIECU_REQUIRE(lhs->valueType == CIECU_F64 && lhs->rows == lhs->cols, "mixed_create: square FP64 matrix expected");
     CIECU_REQUIRE(options.mode == 0 || options.mode == 1, "mixed_create: mode must be 0 or 1");
     CIECU_REQUIRE(options.scaleInner == 0 || options.scaleInner == 1, "mixed_create: scaleInner must be 0 or 1");
+    CIECU_REQUIRE(options.fuseDirection >= 0 && options.fuseDirection <= 2,
+                  "mixed_create: fuseDirection must be 0, 1 or 2");
     CIECU_REQUIRE(options.delta > 0.0 && options.delta < 1.0, "mixed_create: delta must be in (0, 1)");
     CIECU_REQUIRE(options.innerKernel == 0 || options.innerKernel == 1 || options.innerKernel == 2 ||
                       options.innerKernel == 4 || options.innerKernel == -1 || options.innerKernel == kDiaInner,
@@ -892,7 +1180,11 @@ int ciecu_mixed_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_sta
     cudaError_t e = cudaSuccess;
     for (float** v : {&M->dinv32, &M->x32, &M->r32, &M->p32, &M->q32})
         if (e == cudaSuccess) e = cudaMalloc(v, sizeof(float) * n);
+    M->form = options.fuseDirection;
     if (e == cudaSuccess && options.fuseDirection) e = cudaMalloc(&M->z32, sizeof(float) * n);
+    if (options.fuseDirection == 2)
+        for (float** v : {&M->r32b, &M->p32b, &M->q32b})
+            if (e == cudaSuccess) e = cudaMalloc(v, sizeof(float) * n);
     if (e == cudaSuccess) e = cudaMalloc(&M->x64, sizeof(double) * n);
     if (e == cudaSuccess) e = cudaMalloc(&M->d_s, sizeof(MixedScalars));
     if (e == cudaSuccess) e = cudaMallocHost(&M->h_s, sizeof(MixedScalars));
@@ -1060,6 +1352,7 @@ int ciecu_mixed_destroy(ciecu_mixed M) {
     cudaFree(M->p32);
     cudaFree(M->q32);
     cudaFree(M->z32);
+    for (float* v : {M->r32b, M->p32b, M->q32b}) cudaFree(v);
     cudaFree(M->x64);
     cudaFree(M->d_s);
     if (M->h_s) cudaFreeHost(M->h_s);
@@ -1144,6 +1437,12 @@ int ciecu_mixed_dia_info(ciecu_mixed M, int* diagonals, int* triples) {
     return CIECU_OK;
 }
 
+int ciecu_mixed_form(ciecu_mixed M, int* kernelsPerIteration) {
+    CIECU_REQUIRE(M && kernelsPerIteration, "mixed_form: null argument");
+    *kernelsPerIteration = single_pass(M) ? 1 : (M->z32 ? 2 : 3);
+    return CIECU_OK;
+}
+
 int ciecu_mixed_set_graph_chunk(ciecu_mixed M, int iterations) {
     CIECU_REQUIRE(M && iterations >= 1 && iterations <= 4096, "mixed_set_graph_chunk: chunk must be in [1, 4096]");
     if (M->chunk != iterations && M->graph) {
@@ -1186,8 +1485,8 @@ int ciecu_mixed_product(ciecu_mixed M, double inScale, const double* d_in, doubl
             mixed_residual_kernel<K, true, false><<<fit_grid(mixed_residual_kernel<K, true, false>, csr_threads<K>(),
                                                              needR),
                                                     csr_threads<K>(), 0, st>>>(
-                A->args<double>(), d_in, M->x64, M->dinv32, M->r32, M->z32, M->sdiag, M->d_s, M->d_partials,
-                M->d_counter, 0);
+                A->args<double>(), d_in, M->x64, M->dinv32, M->r32, nullptr, single_pass(M) ? nullptr : M->z32,
+                M->sdiag, M->d_s, M->d_partials, M->d_counter, 0);
             return CIECU_OK;
         }));
         if (!M->z32) {  // the fused form's first M1 forms p = z from the z the residual kernel stored
@@ -1211,7 +1510,7 @@ int ciecu_mixed_product(ciecu_mixed M, double inScale, const double* d_in, doubl
             CIECU_CUDA(cudaGraphLaunch(M->graph, st));
             CIECU_CUDA(cudaMemcpyAsync(M->h_s, M->d_s, sizeof(MixedScalars), cudaMemcpyDeviceToHost, st));
             CIECU_CUDA(cudaStreamSynchronize(st));
-            const long long perIteration = M->z32 ? 2 : 3;
+            const long long perIteration = single_pass(M) ? 1 : (M->z32 ? 2 : 3);
             count_launch(M->deviceLoop ? perIteration * (M->h_s->iter - before) + 2LL * (M->h_s->refinements - refBefore)
                                        : (perIteration + 2) * M->chunk);
             if (M->h_s->done) break;

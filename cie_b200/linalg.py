@@ -573,8 +573,11 @@ class MixedPrecisionCG(LinearOperator):
     dot accumulators, FP64 residual r = b - A x and FP64 solution.  mode 0 =
     reliable updates (delta = replacement trigger), mode 1 = restarted iterative
     refinement (delta = inner tolerance).  Stops on the true FP64 residual.
-    fuseDirection: the search direction and its product formed in the inner SpMV
-    by recurrence (two kernels per inner iteration instead of three)."""
+    fuseDirection: False/0 = three kernels per inner iteration; True/1 = the search
+    direction and its product formed in the inner SpMV by recurrence (two
+    kernels); 2 = one kernel per inner iteration over the diagonal-storage copy
+    (pending step, direction and product in one row pass; form 1 with any other
+    inner kernel).  `kernels_per_iteration` reports the form that runs."""
 
     def __init__(self, lhs, inverseDiagonal, settings=None, mode=0, delta=None, compressColumns=True,
                  innerKernel=0, scaleInner=False, fuseDirection=False):
@@ -586,7 +589,7 @@ class MixedPrecisionCG(LinearOperator):
         self.settings = settings if settings is not None else Statistics(5000, 0.0, 1e-10)
         delta = (0.1 if mode == 0 else 1e-4) if delta is None else float(delta)
         self.options = MixedOptions(int(mode), delta, int(bool(compressColumns)), int(innerKernel),
-                                    int(bool(scaleInner)), int(bool(fuseDirection)))
+                                    int(bool(scaleInner)), int(fuseDirection))
         h = ctypes.c_void_p()
         self.space.enter()
         call("ciecu_mixed_create", lhs.csr.handle, _ptr(inverseDiagonal.inverseDiagonal), self.settings, self.options,
@@ -616,6 +619,12 @@ class MixedPrecisionCG(LinearOperator):
                     "dia_diagonals": nd.value, "dia_triples": bool(tr.value)}
         return {"compressed_columns": bool(c.value), "format": "sell-32x4", "padded_entries": e.value,
                 "group_unroll": v.value, "inner_kernel": "tma-pipeline" if v.value == 0 else "registers"}
+
+    @property
+    def kernels_per_iteration(self):
+        k = ctypes.c_int()
+        call("ciecu_mixed_form", self._solver, ctypes.byref(k))
+        return k.value
 
     def set_graph_chunk(self, iterations):
         call("ciecu_mixed_set_graph_chunk", self._solver, int(iterations))

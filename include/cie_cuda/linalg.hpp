@@ -654,8 +654,9 @@ private:
 };
 
 // Mixed-precision PCG (no reference counterpart): FP32 inner CG over an FP32
-// SELL-32 copy of the matrix, FP64 reliable updates; stops on the true FP64
-// residual.  Same product semantics and statistics as ConjugateGradients.
+// copy of the matrix (diagonal storage or SELL-32), FP64 reliable updates; stops
+// on the true FP64 residual.  Same product semantics and statistics as
+// ConjugateGradients.
 class MixedPrecisionCG : public LinearOperator<CUDASpace<double>> {
 public:
     using Space = CUDASpace<double>;
@@ -682,6 +683,12 @@ public:
     }
     std::optional<Statistics> getStats() const noexcept { return _stats; }
     std::size_t refinements() const noexcept { return _refinements; }
+    // Kernels per inner iteration of the solver's loop (3, 2 or 1; options.fuseDirection).
+    int kernelsPerIteration() const {
+        int k = 0;
+        check(ciecu_mixed_form(_solver.get(), &k));
+        return k;
+    }
 
 private:
     std::shared_ptr<CUDACSROperator<int, double>> _pLhs;

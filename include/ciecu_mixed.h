@@ -47,7 +47,15 @@ typedef struct ciecu_mixed_options {
      * two kernels per inner iteration instead of three, same vector traffic, and
      * q carried by recurrence (FP32 rounding drifts between residual
      * replacements).  0: q = A32 p after a separate direction kernel.  Measured
-     * at 128^3 over the FP32 DIA copy: 28.0 ms fused against 29.4 ms. */
+     * at 128^3 over the FP32 DIA copy: 28.0 ms fused against 29.4 ms.
+     * 2: one kernel per inner iteration over the diagonal-storage copy: the
+     * pending step x += alpha p, r -= alpha q, the direction p = D^-1 r + beta p
+     * and q = A32 p in one row pass (neighbour rows' p formed from their gathered
+     * r, q, p, D^-1), rho and ||r|| of the next residual expanded from FP64 sums
+     * of r and q; r, p, q double-buffered.  With any other inner kernel it runs
+     * as form 1 (ciecu_mixed_form reports which).  Measured at 128^3: 38.0 ms
+     * against 27.7 ms for form 1 -- the row pass gathers four vectors where form
+     * 1 gathers one, and that traffic into the SMs outweighs the kernel saved. */
     int fuseDirection;
 } ciecu_mixed_options;
 
@@ -84,6 +92,9 @@ int ciecu_mixed_padded_entries(ciecu_mixed solver, int64_t* h_entries);
  * loads each operand entry of a consecutive offset triple (o - 1, o, o + 1) once
  * (the Q1 stencils; CIECU_DIA_TRIPLES=0 in the environment turns it off). */
 int ciecu_mixed_dia_info(ciecu_mixed solver, int* diagonals, int* triples);
+/* Kernels per inner iteration of the solver's loop: 3, 2 (fuseDirection 1, or 2
+ * without the diagonal copy) or 1 (fuseDirection 2 over the diagonal copy). */
+int ciecu_mixed_form(ciecu_mixed solver, int* kernelsPerIteration);
 /* out = inScale*out + outScale*x, x the refined solution (initial guess = out). */
 int ciecu_mixed_product(ciecu_mixed solver, double inScale, const double* d_in, double outScale, double* d_out,
                         ciecu_mixed_statistics* h_stats);

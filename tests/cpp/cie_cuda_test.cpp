@@ -440,6 +440,18 @@ int main() {
                    solver.getStats()->relativeResidual);
         }
         {
+            // one kernel per inner iteration over the diagonal copy (fuseDirection 2)
+            MixedPrecisionCG solver(pLhs, pPreconditioner, settings, ciecu_mixed_options{0, 0.1, 1, -2, 0, 2});
+            pSpace->fill(Space::view(out), 0.0);
+            solver.product(0, Space::view(std::as_const(rhs)), 1, Space::view(out));
+            std::vector<double> x(n);
+            pSpace->assign(std::span<double>(x), Space::view(std::as_const(out)));
+            report(solver.kernelsPerIteration() == 1, "MixedPrecisionCG single pass: kernels per inner iteration",
+                   solver.kernelsPerIteration());
+            report(rel_diff(x, xref) <= 1e-9, "MixedPrecisionCG single pass vs reference PCG, rel diff",
+                   rel_diff(x, xref));
+        }
+        {
             // size mismatch is an exception, as CIE_CHECK is in the reference
             bool thrown = false;
             auto shorter = pSpace->makeVector(n - 1);

@@ -95,13 +95,15 @@ def test_cfg2_fp64_pcg_vs_reference(space, cfg2):
     assert true_residual(rp, col, val, xh, b) <= RESIDUAL
 
 
-@pytest.mark.parametrize("delta", [0.1])
-def test_cfg2_mixed_pcg_vs_reference(space, cfg2, delta):
+@pytest.mark.parametrize("delta,fuse", [(0.1, False), (0.1, 2)])
+def test_cfg2_mixed_pcg_vs_reference(space, cfg2, delta, fuse):
     from cie_b200.linalg import CSROperator, MixedPrecisionCG, Statistics, makeDiagonalOperator
     prob, (rp, col, val, b), xr, sr = cfg2
     A = CSROperator(prob.matrix, space)
     D = makeDiagonalOperator(prob.matrix, space, csr_handle=A.csr)
-    solver = MixedPrecisionCG(A, D, Statistics(20000, 0.0, 1e-10), mode=0, delta=delta)
+    solver = MixedPrecisionCG(A, D, Statistics(20000, 0.0, 1e-10), mode=0, delta=delta, fuseDirection=fuse)
+    if fuse == 2:
+        assert solver.kernels_per_iteration == 1
     x = torch.zeros_like(prob.rhs)
     solver.product(0.0, prob.rhs, 1.0, x)
     xh = x.cpu().numpy()

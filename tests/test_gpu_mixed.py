@@ -25,7 +25,9 @@ def mixed_solve(space, m, b, mode=0, delta=None, compress=True, x0=None, setting
                               compressColumns=compress, innerKernel=inner, fuseDirection=fuse)
     x = dev(np.zeros(len(b)) if x0 is None else x0)
     solver.product(0.0, dev(b), 1.0, x)
-    return host(x), solver.getStats(), solver.info()
+    info = solver.info()
+    info["kernels_per_iteration"] = solver.kernels_per_iteration
+    return host(x), solver.getStats(), info
 
 
 @pytest.mark.parametrize("mode,compress,inner,fuse", [(0, True, 0, False), (0, False, 0, False), (1, True, 0, False),
@@ -33,10 +35,14 @@ def mixed_solve(space, m, b, mode=0, delta=None, compress=True, x0=None, setting
                                                       (1, True, -1, False), (0, True, 1, False), (0, True, 4, False),
                                                       (0, True, -2, False), (1, True, -2, False),
                                                       (0, True, -2, True), (1, True, -2, True), (0, True, -1, True),
-                                                      (0, False, 2, True), (0, True, 0, True)])
+                                                      (0, False, 2, True), (0, True, 0, True),
+                                                      (0, True, -2, 2), (1, True, -2, 2), (0, True, 0, 2),
+                                                      (0, True, 2, 2)])
 def test_mixed_3d_lognormal_vs_reference(space, reference, mode, compress, inner, fuse):
     """fuse: the direction and its product formed by recurrence in the inner SpMV
-    (two kernels per inner iteration); same bars as the three-kernel form."""
+    (two kernels per inner iteration), or (2) the whole inner iteration in one row
+    pass over the DIA copy (two kernels over a SELL copy); same bars as the
+    three-kernel form."""
     from cie_b200.fem import make_poisson
     prob = make_poisson(space, 3, 1, [40, 40, 40], seed=2)
     rp, col, val = prob.host_csr()
@@ -52,6 +58,8 @@ def test_mixed_3d_lognormal_vs_reference(space, reference, mode, compress, inner
           % (mode, compress, fuse, st.innerIterations, st.refinements, sr[0], rel, tr, info))
     if info["format"] != "dia":  # the SELL copy is not built when the DIA copy is the known choice
         assert info["compressed_columns"] == compress
+    expected = 3 if not fuse else (1 if fuse == 2 and info["format"] == "dia" else 2)
+    assert info["kernels_per_iteration"] == expected
     assert st.trueRelativeResidual < 1e-10 and tr <= 1.01e-10
     assert rel <= 1e-9
     if mode == 0:
@@ -204,8 +212,8 @@ def test_dia_refused_for_scattered_pattern(space):
         MixedPrecisionCG(A, makeDiagonalOperator(prob.matrix, space), Statistics(10, 0.0, 1e-10), innerKernel=-2)
 
 
-@pytest.mark.parametrize("embedded", [False, True])
-def test_mixed_scaled_inner_vs_reference(space, reference, embedded):
+@pytest.mark.parametrize("embedded,fuse", [(False, False), (True, False), (False, 2)])
+def test_mixed_scaled_inner_vs_reference(space, reference, embedded, fuse):
     """The Jacobi-scaled FP32 inner system (scaleInner): same accuracy bar, on a
     log-normal problem and on an embedded sphere with material factor 1e-4, whose
     entries span eight orders of magnitude.  (At 1e-6 the FP32 inner iteration sits
@@ -226,7 +234,9 @@ def test_mixed_scaled_inner_vs_reference(space, reference, embedded):
     if embedded:
         A.csr.set_kernel(4)
     solver = MixedPrecisionCG(A, D, Statistics(200000, 0.0, 1e-10), scaleInner=True,
-                              innerKernel=1 if embedded else 0)
+                              innerKernel=1 if embedded else (-2 if fuse == 2 else 0), fuseDirection=fuse)
+    if fuse == 2:
+        assert solver.kernels_per_iteration == 1
     x = dev(np.zeros(len(b)))
     solver.product(0.0, dev(b), 1.0, x)
     x, st = host(x), solver.getStats()
