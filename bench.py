@@ -49,7 +49,8 @@ DELTA = 0.1
 # copy (pending step, direction and product in one row pass), 0 = a separate
 # direction kernel (three).  OTHER_FORM is timed beside it on the same system: at
 # 128^3 the one-kernel form measured 38.0 ms against 27.7 ms for the two-kernel
-# form (its row pass gathers r, q, p and D^-1 where the two-kernel pass gathers z).
+# form (its row pass forms each operand entry from r, q, p and D^-1, where the
+# two-kernel pass gathers z).
 FUSE = 1
 OTHER_FORM = 2
 FORM_NAMES = {0: "three kernels per inner iteration (separate direction kernel)",
@@ -228,6 +229,9 @@ def main():
     ap.add_argument("--pin", default=None,
                     help="with --profile: FP64-solver,mixed-unroll,CSR schedules to use instead of autotuning "
                          "(the choices a bench run without the profiler reports), e.g. 4,1,4")
+    ap.add_argument("--mixed-form", type=int, default=None, choices=[0, 1, 2],
+                    help="with --profile: inner-iteration form of the mixed solver (fuseDirection) instead of the "
+                         "benchmarked one")
     ap.add_argument("--profile-target", default="pcg",
                     choices=["pcg", "batch", "spmm", "spmm32", "embedded", "cut", "twolevel", "gradient"],
                     help="with --profile: the solver the ncu target runs (pcg: the headline solves; batch: a "
@@ -305,11 +309,12 @@ def main():
     A = CSROperator(prob.matrix, space)
     D = makeDiagonalOperator(prob.matrix, space, csr_handle=A.csr)
     cg = ConjugateGradients(A, space, D, settings)
+    form = args.mixed_form if (args.profile and args.mixed_form is not None) else FUSE
     if args.profile and args.pin:
         pin_fp64, pin_unroll, pin_csr = (int(v) for v in args.pin.split(","))
         A.csr.set_kernel(pin_csr)
         cg.set_schedule(pin_fp64)
-        mixed = MixedPrecisionCG(A, D, settings, mode=0, delta=DELTA, innerKernel=pin_unroll, fuseDirection=FUSE)
+        mixed = MixedPrecisionCG(A, D, settings, mode=0, delta=DELTA, innerKernel=pin_unroll, fuseDirection=form)
     else:
         mixed = MixedPrecisionCG(A, D, settings, mode=0, delta=DELTA, fuseDirection=FUSE)
     x64 = torch.zeros_like(prob.rhs)

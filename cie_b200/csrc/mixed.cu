@@ -306,9 +306,11 @@ __global__ void __launch_bounds__(kT) mixed_spmv_dia_kernel(DiaArgs<float> A, co
 // other blocks gather the old values while this block writes the new ones.
 // Over the Q1 triple stencils the operand windows come from 16-byte loads and
 // warp shuffles (dia_rows4_triples_window).  It moves 36N vector bytes per
-// iteration against 52N for the two-kernel form, but the gathers read four
-// vectors instead of one: at 128^3 it measured 38.0 ms per solve against 27.7 ms
-// (33.5 ms on the Jacobi-scaled inner system, which gathers three).
+// iteration against 52N for the two-kernel form, but forming each operand entry
+// from four gathered vectors takes 80 registers and 2.6x the instructions of the
+// fused SpMV, and the pass becomes latency-bound: at 128^3 it measured 38.0 ms
+// per solve against 27.7 ms (33.5 ms on the Jacobi-scaled inner system, which
+// gathers three).
 struct SingleVectors {
     float* r[2];
     float* p[2];

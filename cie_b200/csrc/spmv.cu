@@ -34,8 +34,7 @@ __global__ void __launch_bounds__(csr_threads<KERNEL>())
 
 // Row-block boundaries: greedy, at most kStreamTile entries and kStreamMaxRows
 // rows per block; a row longer than the tile is a block of its own.
-std::vector<int> make_row_blocks(const std::vector<int>& rowptr) {
-    const int n = static_cast<int>(rowptr.size()) - 1;
+std::vector<int> make_row_blocks(const int* rowptr, int n) {
     std::vector<int> blocks{0};
     int r0 = 0;
     while (r0 < n) {
@@ -47,6 +46,25 @@ std::vector<int> make_row_blocks(const std::vector<int>& rowptr) {
         r0 = r1;
     }
     return blocks;
+}
+
+// A page-locked host buffer, grown on demand and kept for the life of the
+// process, through which csr_create reads the row extents back (a copy into
+// pageable memory goes through a driver bounce buffer at a fraction of the
+// rate).  The lock is held while the buffer is in use.
+std::mutex g_stagingMutex;
+void* g_staging = nullptr;
+size_t g_stagingBytes = 0;
+
+cudaError_t staging_reserve(size_t bytes) {
+    if (bytes <= g_stagingBytes) return cudaSuccess;
+    if (g_staging) cudaFreeHost(g_staging);
+    g_staging = nullptr;
+    g_stagingBytes = 0;
+    const size_t grown = std::max(bytes, static_cast<size_t>(1) << 20);
+    const cudaError_t e = cudaMallocHost(&g_staging, grown);
+    if (e == cudaSuccess) g_stagingBytes = grown;
+    return e;
 }
 
 // Column indices outside [0, ncols) are counted; csr_create refuses such a matrix
@@ -195,24 +213,28 @@ int ciecu_csr_create(ciecu_space space, int32_t rowCount, int32_t columnCount, i
     csr->valueType = valueType;
     csr->aligned16 = (reinterpret_cast<uintptr_t>(d_columnIndices) % 16 == 0) &&
                      (reinterpret_cast<uintptr_t>(d_entries) % 16 == 0);
-    // Row extents come back to the host once to build the row-block schedule
-    // and check them (monotone, rowptr[rows] == nnz).
-    std::vector<int> rowptr(static_cast<size_t>(rowCount) + 1);
-    cudaError_t e = cudaMemcpyAsync(rowptr.data(), d_rowExtents, sizeof(int) * rowptr.size(), cudaMemcpyDeviceToHost,
-                                    space->stream);
+    // Row extents come back to the host once (through the pinned staging buffer)
+    // to check them (rowptr[0] == 0, monotone, rowptr[rows] == nnz), find the
+    // longest row and build the row-block schedule.
+    std::unique_lock<std::mutex> staging(g_stagingMutex);
+    const size_t extentBytes = sizeof(int) * (static_cast<size_t>(rowCount) + 1);
+    cudaError_t e = staging_reserve(extentBytes);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(g_staging, d_rowExtents, extentBytes, cudaMemcpyDeviceToHost, space->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(space->stream);
     if (e != cudaSuccess) {
         delete csr;
         return cuda_fail(e, "csr_create: reading row extents");
     }
-    if (rowptr[0] != 0 || rowptr[static_cast<size_t>(rowCount)] != nnz) {
+    const int* rowptr = static_cast<const int*>(g_staging);
+    if (rowptr[0] != 0 || rowptr[rowCount] != nnz) {
         delete csr;
         return fail(CIECU_ERR_ARGUMENT, "number of column indices (" + std::to_string(nnz) +
                                             ") is inconsistent with the row extents of the provided CSR matrix");
     }
     int maxRow = 0;
     for (int r = 0; r < rowCount; ++r) {
-        const int len = rowptr[static_cast<size_t>(r) + 1] - rowptr[static_cast<size_t>(r)];
+        const int len = rowptr[r + 1] - rowptr[r];
         if (len < 0) {
             delete csr;
             return fail(CIECU_ERR_ARGUMENT, "row extents of the provided CSR matrix are not monotone at row " +
@@ -222,6 +244,8 @@ int ciecu_csr_create(ciecu_space space, int32_t rowCount, int32_t columnCount, i
     }
     csr->maxRow = maxRow;
     csr->avgRow = rowCount ? static_cast<double>(nnz) / rowCount : 0.0;
+    const std::vector<int> blocks = make_row_blocks(rowptr, rowCount);
+    staging.unlock();
     if (nnz > 0) {
         unsigned* d_bad = reinterpret_cast<unsigned*>(space->d_result);
         unsigned bad = 0;
@@ -244,7 +268,6 @@ int ciecu_csr_create(ciecu_space space, int32_t rowCount, int32_t columnCount, i
                                                 ") in the provided CSR matrix");
         }
     }
-    const std::vector<int> blocks = make_row_blocks(rowptr);
     csr->nblocks = static_cast<int>(blocks.size()) - 1;
     e = cudaMalloc(&csr->d_blocks, sizeof(int) * blocks.size());
     if (e == cudaSuccess)

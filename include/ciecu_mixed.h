@@ -54,8 +54,9 @@ typedef struct ciecu_mixed_options {
      * r, q, p, D^-1), rho and ||r|| of the next residual expanded from FP64 sums
      * of r and q; r, p, q double-buffered.  With any other inner kernel it runs
      * as form 1 (ciecu_mixed_form reports which).  Measured at 128^3: 38.0 ms
-     * against 27.7 ms for form 1 -- the row pass gathers four vectors where form
-     * 1 gathers one, and that traffic into the SMs outweighs the kernel saved. */
+     * against 27.7 ms for form 1 -- forming each operand entry from four gathered
+     * vectors costs registers and instructions, and the latency-bound pass loses
+     * more than the kernel it saves. */
     int fuseDirection;
 } ciecu_mixed_options;
 
