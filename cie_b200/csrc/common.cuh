@@ -7,6 +7,7 @@
 
 #include <cstdint>
 #include <cstdio>
+#include <initializer_list>
 #include <string>
 #include <utility>
 
@@ -21,6 +22,22 @@ void set_error(const std::string& message);
 int fail(int status, const std::string& message);
 int cuda_fail(cudaError_t error, const char* what);
 int sm_count();
+
+// Stream-ordered device memory for solver set-up: a pool per device, owned by the
+// library, that keeps freed blocks (up to kPoolKeepBytes) for the next
+// allocation instead of returning them to the driver, so that creating and
+// destroying solvers of the same size repeatedly maps no new memory.  pool_alloc
+// memory is usable on `stream` in stream order (and everywhere once the stream
+// has been synchronised).  pool_release waits for the device (the implicit
+// synchronisation of cudaFree) and returns the blocks to the pool; it needs no
+// live stream, so a solver may be destroyed after its space.
+constexpr unsigned long long kPoolKeepBytes = 4ull << 30;
+cudaError_t pool_alloc(void** ptr, size_t bytes, cudaStream_t stream);
+template <typename T>
+cudaError_t pool_alloc(T** ptr, size_t bytes, cudaStream_t stream) {
+    return pool_alloc(reinterpret_cast<void**>(ptr), bytes, stream);
+}
+void pool_release(std::initializer_list<void*> ptrs);
 
 #define CIECU_CUDA(call)                                              \
     do {                                                              \

@@ -89,7 +89,7 @@ int dia_offsets(ciecu_csr_s* csr, const std::vector<int>** out) {
     if (csr->rows != csr->cols || csr->rows == 0 || csr->nnz == 0) return CIECU_OK;
     cudaStream_t st = csr->space->stream;
     int* d_table = nullptr;
-    CIECU_CUDA(cudaMalloc(&d_table, sizeof(int) * (kHashSlots + 1)));
+    CIECU_CUDA(pool_alloc(&d_table, sizeof(int) * (kHashSlots + 1), st));
     std::vector<int> h(kHashSlots + 1, kEmpty);
     h[kHashSlots] = 0;  // reject flag
     cudaError_t e = cudaMemcpyAsync(d_table, h.data(), sizeof(int) * h.size(), cudaMemcpyHostToDevice, st);
@@ -101,7 +101,7 @@ int dia_offsets(ciecu_csr_s* csr, const std::vector<int>** out) {
     }
     if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), d_table, sizeof(int) * h.size(), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    cudaFree(d_table);
+    cudaFreeAsync(d_table, st);  // back to the pool; the stream is idle here
     if (e != cudaSuccess) return cuda_fail(e, "dia: offset analysis");
     if (h[kHashSlots] != 0) return CIECU_OK;
     std::vector<int> offsets;

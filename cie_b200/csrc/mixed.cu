@@ -1180,22 +1180,24 @@ int ciecu_mixed_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_sta
     const size_t n = static_cast<size_t>(std::max<long>(M->n, 1)) + 4;
     M->nslices = static_cast<int>((M->n + 31) / 32);
     cudaError_t e = cudaSuccess;
+    // solver buffers come from the library's stream-ordered pool (pool_alloc): a
+    // solver of a size created before maps no new memory
     for (float** v : {&M->dinv32, &M->x32, &M->r32, &M->p32, &M->q32})
-        if (e == cudaSuccess) e = cudaMalloc(v, sizeof(float) * n);
+        if (e == cudaSuccess) e = pool_alloc(v, sizeof(float) * n, st);
     M->form = options.fuseDirection;
-    if (e == cudaSuccess && options.fuseDirection) e = cudaMalloc(&M->z32, sizeof(float) * n);
+    if (e == cudaSuccess && options.fuseDirection) e = pool_alloc(&M->z32, sizeof(float) * n, st);
     if (options.fuseDirection == 2)
         for (float** v : {&M->r32b, &M->p32b, &M->q32b})
-            if (e == cudaSuccess) e = cudaMalloc(v, sizeof(float) * n);
-    if (e == cudaSuccess) e = cudaMalloc(&M->x64, sizeof(double) * n);
-    if (e == cudaSuccess) e = cudaMalloc(&M->d_s, sizeof(MixedScalars));
-    if (e == cudaSuccess) e = cudaMallocHost(&M->h_s, sizeof(MixedScalars));
-    if (e == cudaSuccess) e = cudaMalloc(&M->d_partials, sizeof(double) * kMaxPartials * 2);
-    if (e == cudaSuccess) e = cudaMalloc(&M->d_counter, sizeof(unsigned) * 4);
+            if (e == cudaSuccess) e = pool_alloc(v, sizeof(float) * n, st);
+    if (e == cudaSuccess) e = pool_alloc(&M->x64, sizeof(double) * n, st);
+    if (e == cudaSuccess) e = pool_alloc(&M->d_s, sizeof(MixedScalars), st);
+    M->h_s = new MixedScalars();  // read back once per graph launch: pageable is enough
+    if (e == cudaSuccess) e = pool_alloc(&M->d_partials, sizeof(double) * kMaxPartials * 2, st);
+    if (e == cudaSuccess) e = pool_alloc(&M->d_counter, sizeof(unsigned) * 4, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(M->d_counter, 0, sizeof(unsigned) * 4, st);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&M->side, cudaStreamNonBlocking);
     if (e == cudaSuccess && options.scaleInner) {
-        e = cudaMalloc(&M->sdiag, sizeof(double) * n);
+        e = pool_alloc(&M->sdiag, sizeof(double) * n, st);
         if (e == cudaSuccess && M->n > 0) {
             sqrt_kernel<<<grid_for(M->n, kT, 8), kT, 0, st>>>(M->n, d_inverseDiagonal, M->sdiag);
             count_launch();
@@ -1221,7 +1223,7 @@ int ciecu_mixed_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_sta
         if (status == CIECU_OK && !offsets->empty()) {
             DiaArgs<float> a = dia_shape<float>(lhs, *offsets);
             const size_t bytes = sizeof(float) * static_cast<size_t>(a.ndiag) * static_cast<size_t>(a.ld);
-            if (cudaMalloc(&M->dia32, bytes) == cudaSuccess) {
+            if (pool_alloc(&M->dia32, bytes, st) == cudaSuccess) {
                 e = cudaMemsetAsync(M->dia32, 0, bytes, st);
                 a.val = M->dia32;
                 M->dia = a;
@@ -1338,7 +1340,8 @@ int ciecu_mixed_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_sta
 
 int ciecu_mixed_destroy(ciecu_mixed M) {
     if (!M) return CIECU_OK;
-    // No access to M->A (it may already be gone); cudaFree synchronises the device.
+    // No access to M->A (it may already be gone); cudaFree and pool_release
+    // synchronise the device.
     if (M->graph) cudaGraphExecDestroy(M->graph);
     if (M->side) cudaStreamDestroy(M->side);
     cudaFree(M->sliceLen);
@@ -1346,20 +1349,9 @@ int ciecu_mixed_destroy(ciecu_mixed M) {
     cudaFree(M->rowLen);
     cudaFree(M->val32);
     cudaFree(M->col32or16);
-    cudaFree(M->dia32);
-    cudaFree(M->dinv32);
-    cudaFree(M->sdiag);
-    cudaFree(M->x32);
-    cudaFree(M->r32);
-    cudaFree(M->p32);
-    cudaFree(M->q32);
-    cudaFree(M->z32);
-    for (float* v : {M->r32b, M->p32b, M->q32b}) cudaFree(v);
-    cudaFree(M->x64);
-    cudaFree(M->d_s);
-    if (M->h_s) cudaFreeHost(M->h_s);
-    cudaFree(M->d_partials);
-    cudaFree(M->d_counter);
+    pool_release({M->dia32, M->dinv32, M->sdiag, M->x32, M->r32, M->p32, M->q32, M->z32, M->r32b, M->p32b,
+                  M->q32b, M->x64, M->d_s, M->d_partials, M->d_counter});
+    delete M->h_s;
     delete M;
     return CIECU_OK;
 }

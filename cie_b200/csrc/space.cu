@@ -40,6 +40,58 @@ int sm_count() {
     return cached;
 }
 
+namespace {
+std::mutex g_poolMutex;
+std::map<int, cudaMemPool_t> g_pools;
+
+cudaError_t device_pool(cudaMemPool_t* pool) {
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(g_poolMutex);
+    auto it = g_pools.find(device);
+    if (it != g_pools.end()) {
+        *pool = it->second;
+        return cudaSuccess;
+    }
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t created = nullptr;
+    e = cudaMemPoolCreate(&created, &props);
+    if (e != cudaSuccess) return e;
+    unsigned long long keep = kPoolKeepBytes;
+    e = cudaMemPoolSetAttribute(created, cudaMemPoolAttrReleaseThreshold, &keep);
+    if (e != cudaSuccess) {
+        cudaMemPoolDestroy(created);
+        return e;
+    }
+    g_pools[device] = created;
+    *pool = created;
+    return cudaSuccess;
+}
+}  // namespace
+
+cudaError_t pool_alloc(void** ptr, size_t bytes, cudaStream_t stream) {
+    *ptr = nullptr;
+    cudaMemPool_t pool = nullptr;
+    const cudaError_t e = device_pool(&pool);
+    if (e != cudaSuccess) return e;
+    return cudaMallocFromPoolAsync(ptr, bytes == 0 ? 1 : bytes, pool, stream);
+}
+
+void pool_release(std::initializer_list<void*> ptrs) {
+    bool any = false;
+    for (void* p : ptrs) any = any || p;
+    if (!any) return;
+    cudaDeviceSynchronize();
+    for (void* p : ptrs)
+        if (p) cudaFreeAsync(p, cudaStreamLegacy);
+    cudaStreamSynchronize(cudaStreamLegacy);  // the blocks are free for any stream from here
+}
+
 int resident_blocks(const void* kernel, int threads, size_t smem) {
     static std::mutex mutex;
     static std::map<std::tuple<const void*, int, size_t>, int> cache;

@@ -269,13 +269,13 @@ int ciecu_csr_create(ciecu_space space, int32_t rowCount, int32_t columnCount, i
         }
     }
     csr->nblocks = static_cast<int>(blocks.size()) - 1;
-    e = cudaMalloc(&csr->d_blocks, sizeof(int) * blocks.size());
+    e = pool_alloc(&csr->d_blocks, sizeof(int) * blocks.size(), space->stream);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(csr->d_blocks, blocks.data(), sizeof(int) * blocks.size(), cudaMemcpyHostToDevice,
                             space->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(space->stream);
     if (e != cudaSuccess) {
-        cudaFree(csr->d_blocks);
+        pool_release({csr->d_blocks});
         delete csr;
         return cuda_fail(e, "csr_create: row-block schedule");
     }
@@ -285,8 +285,8 @@ int ciecu_csr_create(ciecu_space space, int32_t rowCount, int32_t columnCount, i
 
 int ciecu_csr_destroy(ciecu_csr csr) {
     if (!csr) return CIECU_OK;
-    // No access to csr->space (it may already be gone); cudaFree synchronises the device.
-    cudaFree(csr->d_blocks);
+    // No access to csr->space (it may already be gone); pool_release synchronises the device.
+    pool_release({csr->d_blocks});
     delete csr;
     return CIECU_OK;
 }
