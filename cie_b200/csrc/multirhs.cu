@@ -1044,10 +1044,10 @@ struct TrueResidualQuad {
 
 // K1 for k = 32 over either format; FP64 (the plain form) or FP32 (the refined
 // form, whose breakdowns restart).
-template <typename MA, typename T, bool COND, bool TRIPLES = false>
-__global__ void __launch_bounds__(kT) multi_spmv_quad_kernel(MA A, const T* __restrict__ P, T* __restrict__ Q,
-                                                             ColumnScalars* S, MultiGlobal* g, double* partials,
-                                                             unsigned* counter, cudaGraphConditionalHandle cond) {
+template <typename MA, typename T, bool COND, bool TRIPLES>
+__device__ __forceinline__ void multi_spmv_quad(MA A, const T* __restrict__ P, T* __restrict__ Q, ColumnScalars* S,
+                                                MultiGlobal* g, double* partials, unsigned* counter,
+                                                cudaGraphConditionalHandle cond) {
     if (*reinterpret_cast<volatile unsigned*>(&g->finished) >= 32u) {
         if (blockIdx.x == 0 && threadIdx.x == 0) set_loop<COND>(cond, 0);
         return;
@@ -1071,6 +1071,25 @@ __global__ void __launch_bounds__(kT) multi_spmv_quad_kernel(MA A, const T* __re
             }
         }
     }
+}
+
+template <typename MA, typename T, bool COND, bool TRIPLES = false>
+__global__ void __launch_bounds__(kT) multi_spmv_quad_kernel(MA A, const T* __restrict__ P, T* __restrict__ Q,
+                                                             ColumnScalars* S, MultiGlobal* g, double* partials,
+                                                             unsigned* counter, cudaGraphConditionalHandle cond) {
+    multi_spmv_quad<MA, T, COND, TRIPLES>(A, P, Q, S, g, partials, counter, cond);
+}
+
+// The FP32 triple pass of the refined form with up to 85 registers (three CTAs
+// per SM): at the compiler's own 64 the 32-RHS FP32 solve at 128^3 measured
+// 475 against 438 ms.
+template <bool COND>
+__global__ void __launch_bounds__(kT, 3) multi_spmv_quad3_f32_kernel(DiaArgs<float> A, const float* __restrict__ P,
+                                                                     float* __restrict__ Q, ColumnScalars* S,
+                                                                     MultiGlobal* g, double* partials,
+                                                                     unsigned* counter,
+                                                                     cudaGraphConditionalHandle cond) {
+    multi_spmv_quad<DiaArgs<float>, float, COND, true>(A, P, Q, S, g, partials, counter, cond);
 }
 
 template <typename MA, bool TRIPLES = false>
@@ -1392,7 +1411,7 @@ int launch_multi_iteration32(ciecu_multi_s* M, cudaStream_t st, cudaGraph_t root
     CIECU_TRY(with_group(M->kp, [&](auto kk) -> int {
         constexpr int KP = decltype(kk)::value;
         if (M->quad && M->useDia && M->triples)
-            multi_spmv_quad_kernel<DiaArgs<float>, float, COND, true><<<M->gridQ32D3, kT, 0, st>>>(
+            multi_spmv_quad3_f32_kernel<COND><<<M->gridQ32D3, kT, 0, st>>>(
                 M->diaF, M->p32, M->q32, M->d_s, M->d_g, M->d_partials, M->d_counter, cond);
         else if (M->quad && M->useDia)
             multi_spmv_quad_kernel<DiaArgs<float>, float, COND><<<M->gridQ32D, kT, 0, st>>>(
@@ -1633,7 +1652,7 @@ int ciecu_multi_create(ciecu_csr lhs, int rhsCount, const double* d_inverseDiago
         const long rows3 = (M->n + kWarps * 16 - 1) / (kWarps * 16);
         M->gridQD3 = fit(reinterpret_cast<const void*>(multi_spmv_quad_kernel<DiaArgs<double>, double, true, true>),
                          rows3);
-        M->gridQ32D3 = fit(reinterpret_cast<const void*>(multi_spmv_quad_kernel<DiaArgs<float>, float, true, true>),
+        M->gridQ32D3 = fit(reinterpret_cast<const void*>(multi_spmv_quad3_f32_kernel<true>),
                            rows3);
         M->quad = quad_enabled();
     }

@@ -675,7 +675,7 @@ int refresh_dia(ciecu_pcg_s* S, cudaStream_t st) {
             DiaArgs<double> a = dia_shape<double>(S->A, *offsets);
             const size_t bytes = sizeof(double) * static_cast<size_t>(a.ndiag) * static_cast<size_t>(a.ld);
             double* buf = nullptr;
-            if (cudaMalloc(&buf, bytes) != cudaSuccess) {
+            if (pool_alloc(&buf, bytes, st) != cudaSuccess) {
                 cudaGetLastError();  // no room for the copy: the CSR schedules stay
                 return CIECU_OK;
             }
@@ -732,7 +732,7 @@ int plan_persistent(ciecu_pcg_s* S) {
     CIECU_CUDA(cudaGetDevice(&device));
     CIECU_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
     const int sms = sm_count();
-    if (!S->split) CIECU_CUDA(cudaMalloc(&S->split, sizeof(int2) * (sms + 1)));
+    if (!S->split) CIECU_CUDA(pool_alloc(&S->split, sizeof(int2) * (sms + 1), st));
     S->fits = false;
     for (int G : {std::max(1, sms / 4), std::max(1, sms / 2), sms}) {
         persistent_split_kernel<<<(G + 1 + 127) / 128, 128, 0, st>>>(A->rowptr, A->rows, A->nnz, G, S->split);
@@ -777,17 +777,14 @@ int ensure_persistent_buffers(ciecu_pcg_s* S) {
     const size_t bytes = sizeof(double) * static_cast<size_t>(std::max<long>(S->n, 1));
     const size_t slotBytes = sizeof(ExchangeSlot) * 2 * static_cast<size_t>(sm_count());
     cudaStream_t st = S->A->space->stream;
-    cudaError_t e = cudaMalloc(&S->z, bytes);
-    if (e == cudaSuccess) e = cudaMalloc(&S->p2, bytes);
-    if (e == cudaSuccess) e = cudaMalloc(&S->slots, slotBytes);
-    if (e == cudaSuccess) e = cudaMalloc(&S->abortFlag, sizeof(int));
+    cudaError_t e = pool_alloc(&S->z, bytes, st);
+    if (e == cudaSuccess) e = pool_alloc(&S->p2, bytes, st);
+    if (e == cudaSuccess) e = pool_alloc(&S->slots, slotBytes, st);
+    if (e == cudaSuccess) e = pool_alloc(&S->abortFlag, sizeof(int), st);
     if (e == cudaSuccess) e = cudaMemsetAsync(S->slots, 0, slotBytes, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(S->abortFlag, 0, sizeof(int), st);
     if (e != cudaSuccess) {
-        cudaFree(S->z);
-        cudaFree(S->p2);
-        cudaFree(S->slots);
-        cudaFree(S->abortFlag);
+        pool_release({S->z, S->p2, S->slots, S->abortFlag});
         S->z = S->p2 = nullptr;
         S->slots = nullptr;
         S->abortFlag = nullptr;
@@ -1002,12 +999,14 @@ int ciecu_pcg_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_stati
     S->n = lhs->rows;
     const size_t bytes = sizeof(double) * static_cast<size_t>(std::max<long>(S->n, 1));
     cudaError_t e = cudaSuccess;
+    cudaStream_t st = lhs->space->stream;
+    // buffers from the library's stream-ordered pool (pool_alloc)
     for (double** v : {&S->x, &S->r, &S->p, &S->q})
-        if (e == cudaSuccess) e = cudaMalloc(v, bytes);
-    if (e == cudaSuccess) e = cudaMalloc(&S->d_s, sizeof(PcgScalars));
-    if (e == cudaSuccess) e = cudaMallocHost(&S->h_s, sizeof(PcgScalars));
-    if (e == cudaSuccess) e = cudaMalloc(&S->d_partials, sizeof(double) * kMaxPartials * 2);
-    if (e == cudaSuccess) e = cudaMalloc(&S->d_counter, sizeof(unsigned) * 4);
+        if (e == cudaSuccess) e = pool_alloc(v, bytes, st);
+    if (e == cudaSuccess) e = pool_alloc(&S->d_s, sizeof(PcgScalars), st);
+    S->h_s = new PcgScalars();  // read back once per graph launch: pageable is enough
+    if (e == cudaSuccess) e = pool_alloc(&S->d_partials, sizeof(double) * kMaxPartials * 2, st);
+    if (e == cudaSuccess) e = pool_alloc(&S->d_counter, sizeof(unsigned) * 4, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(S->d_counter, 0, sizeof(unsigned) * 4, lhs->space->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(S->q, 0, bytes, lhs->space->stream);
     if (e != cudaSuccess) {
@@ -1020,23 +1019,12 @@ int ciecu_pcg_create(ciecu_csr lhs, const double* d_inverseDiagonal, ciecu_stati
 
 int ciecu_pcg_destroy(ciecu_pcg S) {
     if (!S) return CIECU_OK;
-    // No access to S->A: the matrix handle may already be gone.  cudaFree
+    // No access to S->A: the matrix handle may already be gone.  pool_release
     // synchronises the device before releasing memory.
     if (S->graph) cudaGraphExecDestroy(S->graph);
-    cudaFree(S->x);
-    cudaFree(S->r);
-    cudaFree(S->p);
-    cudaFree(S->q);
-    cudaFree(S->d_s);
-    if (S->h_s) cudaFreeHost(S->h_s);
-    cudaFree(S->d_partials);
-    cudaFree(S->d_counter);
-    cudaFree(S->diaBuf);
-    cudaFree(S->z);
-    cudaFree(S->p2);
-    cudaFree(S->slots);
-    cudaFree(S->abortFlag);
-    cudaFree(S->split);
+    pool_release({S->x, S->r, S->p, S->q, S->d_s, S->d_partials, S->d_counter, S->diaBuf, S->z, S->p2, S->slots,
+                  S->abortFlag, S->split});
+    delete S->h_s;
     delete S;
     return CIECU_OK;
 }
