@@ -230,8 +230,12 @@ __global__ void __launch_bounds__(kT) batch_init_kernel(const Tile* __restrict__
 // K1: q = A p and p^T q per system; alpha.
 // RELIABLE (the reliable-update form): an FP32 breakdown takes no step and asks
 // for a replacement with a restarted direction, up to kMaxSystemBreakdowns.
+// Five CTAs per SM (at most 51 registers, against 60 and four CTAs by the
+// compiler's own choice): over the 512 Q2 systems 970 -> 958 ms in FP64 and
+// 887 -> 842 ms in FP32 with reliable updates on one B200; three CTAs (71
+// registers) measured 1.11 s.
 template <int VS, typename T, bool RELIABLE = false>
-__global__ void __launch_bounds__(kT) batch_spmv_kernel(CsrArgs<T> A, const Tile* __restrict__ tiles, int ntiles,
+__global__ void __launch_bounds__(kT, 5) batch_spmv_kernel(CsrArgs<T> A, const Tile* __restrict__ tiles, int ntiles,
                                                         const int* tileBegin, const int* tileCount,
                                                         const T* __restrict__ p, T* __restrict__ q,
                                                         BatchScalars* S, BatchGlobal* g, double* partials,
