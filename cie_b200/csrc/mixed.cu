@@ -27,8 +27,10 @@
 // The solve stops only on the TRUE FP64 residual: ||b - A64 x64|| <= tol ||r0||.
 //
 // One inner iteration = 3 kernels (M1 SpMV+p^T q, M2 update+dots+decision,
-// M3 direction); the two refinement kernels (R1 fold, R2 FP64 residual) are in
-// the same CUDA graph and return at once unless M2 asked for a replacement.
+// M3 direction), 2 when the direction is formed inside M1 (fuseDirection 1), or
+// 1 over the DIA copy (fuseDirection 2, mixed_single_dia_kernel); the two
+// refinement kernels (R1 fold, R2 FP64 residual) are in the same CUDA graph and
+// return at once unless a replacement was asked for.
 #include "ciecu_mixed.h"
 #include "graph.cuh"
 #include "pcg.cuh"
