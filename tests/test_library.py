@@ -97,3 +97,14 @@ def test_errors_are_reported_without_gpu():
     with pytest.raises(_lib.CiecuError) as e:
         _lib.call("ciecu_structured_dofmap", 4, 1, None, None, None)
     assert e.value.status == 1 and "structured_dofmap" in str(e.value)
+
+
+@pytest.mark.parametrize("name,args", [("ciecu_mixed_form", (None, None)), ("ciecu_mixed_dia_info", (None, None, None)),
+                                       ("ciecu_mixed_set_graph_chunk", (None, 16))])
+def test_mixed_solver_queries_refuse_null_handles(name, args):
+    """Argument checks of the mixed solver's C-ABI run on the host: a null handle is
+    CIECU_ERR_ARGUMENT with a message naming the call, and no CUDA call is made."""
+    from cie_b200 import _lib
+    with pytest.raises(_lib.CiecuError) as e:
+        _lib.call(name, *args)
+    assert e.value.status == 1 and name.replace("ciecu_", "") in str(e.value)
